@@ -1,0 +1,283 @@
+"""Run loop around the sweep: the host side of RunModel (src/CovidSim.cpp:1383-1543).
+
+`Simulation` owns one device context (cs_gpu_*) and drives it step by step:
+InitModel + SeedInfection at the start of a realisation, InfectSweep +
+IncubRecoverySweep per timestep, UpdateProbs(0) whenever the susceptible fraction
+has fallen by 0.2 since the last update, daily counter samples (RecordSample,
+CovidSim.cpp:3024) and, for the intervention configurations, a global trigger on
+weekly ICU admissions that switches case isolation, household quarantine, school
+and university closure and social distancing on for a fixed duration (the role
+TreatSweep plays, Sweep.cpp:1324-2004).
+
+`calibrate_local_beta` restates InitTransmissionCoeffs (src/SetupModel.cpp:640-846):
+the spatial transmission coefficient that makes the household + place + spatial
+reproduction numbers add up to R0.
+"""
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+
+
+class GpuBackend:
+    """The cs_gpu_* entry points of the library, as methods."""
+    prefix = "cs_gpu_"
+
+    def __init__(self, pop_c, params, device=0):
+        self.lib = abi.load_library()
+        self.ctx = C.c_void_p()
+        rc = self.lib.cs_gpu_create(C.byref(pop_c), C.byref(params), device, C.byref(self.ctx))
+        if rc != 0:
+            msg = self.lib.cs_gpu_last_error(self.ctx)
+            self.lib.cs_gpu_destroy(self.ctx)
+            self.ctx = None
+            raise abi.CovidSimError("cs_gpu_create: %s" % (msg.decode() if msg else rc))
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise abi.CovidSimError("%s%s: %s" % (self.prefix, what, self.lib.cs_gpu_last_error(self.ctx).decode()))
+
+    def close(self):
+        if self.ctx:
+            self.lib.cs_gpu_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def begin_run(self, seed, seeds):
+        s = np.ascontiguousarray(seeds, dtype=np.int32)
+        self._ck(self.lib.cs_gpu_begin_run(self.ctx, seed, s.ctypes.data, len(s), 0), "begin_run")
+
+    def seed_infections(self, t, people):
+        s = np.ascontiguousarray(people, dtype=np.int32)
+        self._ck(self.lib.cs_gpu_seed_infections(self.ctx, t, s.ctypes.data, len(s)), "seed_infections")
+
+    def infect_sweep(self, t, run=0):
+        self._ck(self.lib.cs_gpu_infect_sweep(self.ctx, t, run), "infect_sweep")
+
+    def incub_recovery_sweep(self, t):
+        self._ck(self.lib.cs_gpu_incub_recovery_sweep(self.ctx, t), "incub_recovery_sweep")
+
+    def step(self, t, run=0):
+        self._ck(self.lib.cs_gpu_step(self.ctx, t, run), "step")
+
+    def update_probs(self, do_place=0):
+        self._ck(self.lib.cs_gpu_update_probs(self.ctx, do_place), "update_probs")
+
+    def set_params(self, params):
+        self._ck(self.lib.cs_gpu_set_params(self.ctx, C.byref(params)), "set_params")
+
+    def set_interventions(self, iv):
+        self._ck(self.lib.cs_gpu_set_interventions(self.ctx, C.byref(iv)), "set_interventions")
+
+    def close_places(self, place_type, mcells, start, stop):
+        if mcells is None:
+            self._ck(self.lib.cs_gpu_close_places(self.ctx, place_type, None, 0, start, stop), "close_places")
+        else:
+            m = np.ascontiguousarray(mcells, dtype=np.int32)
+            self._ck(self.lib.cs_gpu_close_places(self.ctx, place_type, m.ctypes.data, len(m), start, stop), "close_places")
+
+    def counters(self):
+        out = abi.cs_counters()
+        self._ck(self.lib.cs_gpu_get_counters(self.ctx, C.byref(out)), "get_counters")
+        return out
+
+    def download(self, view):
+        self._ck(self.lib.cs_gpu_download_state(self.ctx, C.byref(view)), "download_state")
+
+    def sync(self):
+        self._ck(self.lib.cs_gpu_sync(self.ctx), "sync")
+
+    def stream(self):
+        return self.lib.cs_gpu_stream(self.ctx)
+
+    def launches(self):
+        return self.lib.cs_gpu_launch_count(self.ctx)
+
+
+def state_arrays(n_people, n_cells):
+    """Host arrays for every field of cs_state_view, and the view over them."""
+    spec = dict(inf=np.int8, severity=np.uint8, flags=np.uint8, infection_time=np.uint16, latent_time=np.uint16,
+                recovery_or_death_time=np.uint16, SARI_time=np.uint16, Critical_time=np.uint16,
+                Stepdown_time=np.uint16, absent_start_time=np.uint16, absent_stop_time=np.uint16,
+                isolation_start_time=np.uint16, quar_start_time=np.uint16, detected_time=np.uint16,
+                infectiousness=np.float32, susc=np.float32, ProbAbsent=np.float32, ProbCare=np.float32,
+                infector=np.int32, infect_type=np.int16, listpos=np.int32, cell_slots=np.int32)
+    cell_spec = dict(cell_S=np.int32, cell_L=np.int32, cell_I=np.int32, cell_R=np.int32, cell_D=np.int32,
+                     cell_S0=np.int32, cell_tot_prob=np.float64)
+    arrs = {k: np.zeros(n_people, dtype=v) for k, v in spec.items()}
+    arrs.update({k: np.zeros(n_cells, dtype=v) for k, v in cell_spec.items()})
+    view = abi.cs_state_view()
+    for k, a in arrs.items():
+        setattr(view, k, a.ctypes.data)
+    return arrs, view
+
+
+# ------------------------------------------------------------ calibration
+def calibrate_local_beta(pop, p, R0, seed=1, sample=400_000):
+    """P.LocalBeta from InitTransmissionCoeffs (src/SetupModel.cpp:640-846), by the
+    same per-person expectation over a sample of the population."""
+    rng = np.random.default_rng(seed)
+    N = pop.n_people
+    idx = rng.choice(N, size=min(N, sample), replace=False) if N > sample else np.arange(N)
+    n = len(idx)
+    dt = p.ModelTimeStep
+    ag = np.minimum(pop.person_age[idx] // 5, abi.CS_NUM_AGE_GROUPS - 1)
+    k = 1.0 / (p.InfectiousnessSD ** 2) if p.InfectiousnessSD > 0 else None
+    infn = np.array([p.AgeInfectiousness[a] for a in range(abi.CS_NUM_AGE_GROUPS)])[ag]
+    if k:
+        infn = infn * rng.gamma(k, 1.0 / k, n)
+    sympt = rng.random(n) < np.array(list(p.ProportionSymptomatic))[ag]
+    infn = np.where(sympt, -infn * p.SymptInfectiousness, infn * p.AsymptInfectiousness)
+    # recovery time in steps from the infectious-period ICDF (constant exp(-1) with a profile)
+    q = rng.random(n) * abi.CS_CDF_RES
+    j = np.floor(q).astype(int)
+    q -= j
+    icdf = np.array(list(p.infectious_icdf.v))
+    rec = np.floor(0.5 - (p.InfectiousPeriod * np.log(q * icdf[j + 1] + (1 - q) * icdf[j]) / dt)).astype(int)
+    prof = np.array(list(p.infectiousness))
+    cum = np.concatenate([[0.0], np.cumsum(prof)])
+    lts = min(int(p.LatentToSymptDelay / dt), 10 ** 6)
+    pre = np.minimum(np.minimum(rec, lts), rec)
+    # household
+    hh = pop.person_hh[idx]
+    nh = pop.hh_nh[hh].astype(int)
+    nhr = pop.hh_nhr[hh].astype(int)
+    hinf = np.abs(infn) * dt * p.HouseholdTrans * np.array(list(p.HouseholdDenomLookup))[nhr - 1]
+    logs = np.log(np.clip(1.0 - hinf[:, None] * prof[None, :200], 1e-300, None))
+    mask = np.arange(200)[None, :] < rec[:, None]
+    surv = np.exp(np.where(mask, logs, 0.0).sum(axis=1))
+    R0hh = ((1 - surv) * np.array(list(p.AgeSusceptibility))[ag] * (nh - 1)).sum() / n
+    # spatial
+    rsc = np.array(list(p.RelativeSpatialContact))[ag]
+    sinf = np.abs(infn) * rsc * dt
+    sp = sinf * cum[pre] + sinf * np.where(infn < 0, p.SymptSpatialContactRate, 1.0) * (cum[rec] - cum[pre])
+    R0sp = sp.sum() / n
+    # places
+    R0pl = 0.0
+    for t in range(pop.num_place_types):
+        link = pop.person_place[t, idx]
+        has = link >= 0
+        if not has.any():
+            continue
+        pl = pop.places[t]
+        li = link[has]
+        gi = pop.person_group[t, idx][has].astype(int)
+        gsz = pl["group_size"][pl["group_ofs"][li] + gi].astype(float)
+        npl = np.diff(pl["member_ofs"])[li].astype(float)
+        infh = np.abs(infn[has])
+        pinf = infh * dt * p.PlaceTypeTrans[t]
+        att = np.where(infn[has] < 0, p.SymptPlaceTypeContactRate[t] * (1 - p.SymptPlaceTypeWithdrawalProp[t]), 1.0)
+        r, pr = rec[has], pre[has]
+        lim = 200
+        days = np.arange(lim)[None, :]
+        fac = np.where(days < pr[:, None], 1.0, att[:, None])
+        live = days < r[:, None]
+
+        def survive(scale):
+            v = 1.0 - scale[:, None] * prof[None, :lim] * fac
+            return np.exp(np.where(live, np.log(np.clip(v, 1e-300, None)), 0.0).sum(axis=1))
+
+        s_grp = survive(pinf / p.PlaceTypeGroupSizeParam1[t])
+        s_btw = survive(p.PlaceTypePropBetweenGroupLinks[t] * pinf / npl)
+        ng = gsz - 1
+        R0pl += ((1 - s_grp * s_btw) * ng + (1 - s_btw) * (npl - 1 - ng)).sum() / n
+    beta = (R0 - R0hh - R0pl) / R0sp if R0sp > 0 else 0.0
+    return max(beta, 0.0), dict(R0household=R0hh, R0places=R0pl, SpatialR0=R0sp)
+
+
+# --------------------------------------------------------------- run loop
+@dataclass
+class InterventionPolicy:
+    """Global ICU trigger (src/CovidSim.cpp:3150-3159 ICU triggers with global
+    thresholds): when admissions to critical care over the last `window` days reach
+    `threshold`, switch the interventions on for `duration` days."""
+    threshold: int = 100
+    window: int = 7
+    duration: float = 90.0
+    close_place_types: tuple = (0, 1, 2)
+    social_distancing: bool = True
+    case_isolation: bool = True
+    household_quarantine: bool = True
+
+
+class Simulation:
+    def __init__(self, pop, params, lookup, hires, backend=None, device=0):
+        self.pop = pop
+        self.params = params
+        self._pop_c = pop.to_c(lookup, hires)
+        self.backend = backend(self._pop_c, params) if backend else GpuBackend(self._pop_c, params, device)
+
+    def close(self):
+        self.backend.close()
+
+    def choose_seeds(self, seed, n_seed):
+        """SeedInfection with random locations: uniformly chosen people (the
+        reference picks a person, then a member of that person's microcell)."""
+        rng = np.random.default_rng(seed ^ 0x5EED)
+        return rng.choice(self.pop.n_people, size=n_seed, replace=False).astype(np.int32)
+
+    def run(self, seed, days, n_seed=100, policy=None, sample_every_day=True, callback=None):
+        """One realisation; returns daily time series of the main counters."""
+        be = self.backend
+        P = self.params
+        be.begin_run(seed, self.choose_seeds(seed, n_seed))
+        spd = int(round(P.TimeStepsPerDay))
+        nsteps = int(days * spd)
+        prev_prop_s = 1.0
+        series = {k: [] for k in ("S", "L", "I", "R", "D", "cumI", "cumC", "cumDC", "Critical", "cumCritical",
+                                  "cumDeath_Critical", "cumDeath_SARI", "cumDeath_ILI", "SARI", "ILI", "Mild")}
+        iv_on_until = -1.0
+        iv_started = False
+        socd = np.zeros(self.pop.n_mcells, dtype=np.uint8)
+        for step in range(nsteps):
+            t = step * P.ModelTimeStep
+            be.step(t, 0)
+            if (step + 1) % spd == 0 or step == nsteps - 1:
+                c = be.counters()
+                for k in series:
+                    series[k].append(int(getattr(c, k)))
+                prop_s = c.S / self.pop.n_people
+                if prev_prop_s - prop_s > 0.2:
+                    prev_prop_s = prop_s
+                    be.update_probs(0)
+                if policy is not None:
+                    day = len(series["cumCritical"])
+                    w = policy.window
+                    recent = series["cumCritical"][-1] - (series["cumCritical"][-w - 1] if day > w else 0)
+                    tn = t + P.ModelTimeStep
+                    if not iv_started and recent >= policy.threshold:
+                        iv_started = True
+                        iv_on_until = tn + policy.duration
+                        self._switch_interventions(tn, policy, True, socd)
+                    elif iv_started and iv_on_until > 0 and tn >= iv_on_until:
+                        iv_on_until = -1.0
+                        self._switch_interventions(tn, policy, False, socd)
+                if callback:
+                    callback(step, c)
+        return {k: np.asarray(v) for k, v in series.items()}
+
+    def _switch_interventions(self, t, policy, on, socd):
+        iv = abi.cs_interventions()
+        big = 1e10
+        iv.CaseIsolationTimeStart = t if (on and policy.case_isolation) else big
+        iv.CaseIsolationPolicyDuration = policy.duration
+        iv.HQuarantineTimeStart = t if (on and policy.household_quarantine) else big
+        iv.HQuarantinePolicyDuration = policy.duration
+        socd[:] = abi.CS_TREAT_TREATED if (on and policy.social_distancing) else abi.CS_TREAT_UNTREATED
+        iv.mcell_socdist = socd.ctypes.data
+        iv.mcell_moverest = None
+        self.backend.set_interventions(iv)
+        if on:
+            ts = int(t * self.params.TimeStepsPerDay)
+            stop = min(65533, ts + int(policy.duration * self.params.TimeStepsPerDay))
+            for pt in policy.close_place_types:
+                if pt < self.pop.num_place_types:
+                    self.backend.close_places(pt, None, ts, stop)

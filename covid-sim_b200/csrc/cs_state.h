@@ -1,0 +1,133 @@
+// Device-resident layout of one population and its dynamic state.
+//
+// People: one 32-byte record per person (PersonHot) holding every field a gather
+// of "another person" reads in the sweeps (infection state, household, microcell,
+// susceptibility, absence/isolation/quarantine times, age, flags), so that a
+// random person costs one 32-byte DRAM sector; fields only the person's own
+// transitions touch live in separate arrays (structure of arrays).
+// Cells: Cell::susceptible lists (src/Models/Cell.h:11-20) concatenated cell by
+// cell in `slots`, each partitioned [S | L | I | R and D] exactly as the
+// reference maintains them.
+#pragma once
+
+#include <cstdint>
+
+#include "covidsim_b200.h"
+
+namespace csb {
+
+struct __align__(16) PersonHot {
+    int32_t hh;                // Person::hh
+    int32_t mcell;             // microcell index
+    float susc;                // Person::susc
+    float infness;             // Person::infectiousness (negative when symptomatic)
+    uint16_t latent_time;      // Person::latent_time
+    uint16_t absent_start;     // Person::absent_start_time
+    uint16_t absent_stop;      // Person::absent_stop_time
+    uint16_t isolation_start;  // Person::isolation_start_time
+    uint16_t quar_start;       // HostsQuarantine[].start_time
+    int8_t inf;                // InfStat
+    uint8_t age;               // Person::age
+    uint8_t pflags;            // CS_PF_* (static)
+    uint8_t dflags;            // CS_DF_* (to_die, detected, quarantine compliance)
+    uint8_t sev;               // Severity_Current | Severity_Final << 4
+    uint8_t pad;
+};
+static_assert(sizeof(PersonHot) == 32, "PersonHot must fill one 32-byte sector");
+
+struct DevPlaces {
+    int32_t n;
+    const int32_t* mcell;
+    const int32_t* member_ofs;
+    const int32_t* members;
+    const int32_t* group_ofs;
+    const int32_t* group_start;
+    const int32_t* group_size;
+    uint16_t* close_start;
+    uint16_t* close_end;
+    float* prob_close;
+};
+
+// Intervention windows set by the host between steps.
+struct DevIv {
+    double ci_start, ci_dur, hq_start, hq_dur;
+};
+
+// Transition flags per person for one IncubRecoverySweep.
+enum : uint8_t { kStepLtoI = 1, kStepItoRD = 2 };
+
+// Everything the kernels need, passed by value.
+struct DevPop {
+    int32_t N, NH, NC, NM, NPT, NB, nbx, nby, bs;
+    const cs_params* P;
+    PersonHot* hot;
+    const int32_t* place;      // [NPT][N]
+    const uint16_t* group;     // [NPT][N]
+    const int32_t* hh_first;
+    const uint16_t* hh_nh;
+    const uint16_t* hh_nhr;
+    const float* hh_x;
+    const float* hh_y;
+    const int32_t* mcell_cell;
+    const int32_t* mcell_adunit;
+    const int32_t* cell_grid;
+    const int32_t* cell_start;
+    const int32_t* cell_members;
+    const double* klookup;
+    const double* khires;
+    DevPlaces pl[CS_MAX_PLACE_TYPES];
+    // cold per-person state
+    uint16_t* infection_time;
+    uint16_t* recovery_time;
+    uint16_t* sari_time;
+    uint16_t* critical_time;
+    uint16_t* stepdown_time;
+    uint16_t* detected_time;
+    float* prob_absent;
+    float* prob_care;
+    int32_t* infector;
+    int32_t* listpos;
+    int16_t* infect_type;
+    uint8_t* pstep;
+    // cells
+    int32_t* S;
+    int32_t* L;
+    int32_t* I;
+    int32_t* R;
+    int32_t* D;
+    int32_t* S0;
+    double* tot_prob;
+    int32_t* slots;
+    uint8_t* mark;
+    // microcells
+    uint8_t* socdist;
+    uint8_t* moverest;
+    DevIv* iv;
+    // spatial proposal blocks
+    const int32_t* cell_block;
+    const int32_t* block_cell_ofs;
+    const int32_t* block_cells;
+    int32_t* block_cum;
+    long long* block_S0;
+    double* block_row_cum;     // [NB][NB]
+    // per-step scratch
+    unsigned long long* claim; // [N], UINT64_MAX when unclaimed
+    int32_t* queue;            // [N] newly infected people
+    int32_t* counts;           // [8] device-side sizes (see kCnt*)
+    int32_t* touched;          // [NC] cells whose lists change this phase
+    uint8_t* cell_flag;        // [NC]
+    int32_t* act_ofs;          // [NC+1] exclusive scan of per-cell active counts
+    int32_t* act;              // [N] active people (infectors / latent+infectious)
+    int32_t* act_cell;         // [N]
+    int32_t* cnt;              // [N] spatial contacts per infector
+    int32_t* cnt_ofs;          // [N+1]
+    uint8_t* act_closed;       // [N] infector's place-closed-and-absent flag
+    uint8_t* hh_flag;          // [NH] deferred household actions
+    int32_t* hh_list;          // [NH]
+    int32_t* scan_tmp;         // scan block sums
+    cs_counters* C;
+};
+
+enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntN = 8 };
+
+}  // namespace csb

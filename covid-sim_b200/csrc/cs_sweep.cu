@@ -1,0 +1,1591 @@
+// B200 (sm_100a) implementation of CovidSim's per-timestep sweep behind the C ABI
+// of include/covidsim_b200.h.
+//
+// One timestep = InfectSweep + IncubRecoverySweep (src/Sweep.cpp:283-979).  The
+// reference walks cells on CPU threads and pushes infections through per-thread
+// queues; here each phase is a handful of grid-stride kernels over compact lists
+// built on the device, with no host round trip inside a step (so a step can be
+// replayed as a CUDA graph):
+//
+//   InfectSweep
+//     k_active_counts + scan + k_gather_active  infectious people of every cell
+//     k_infectors        household + place passes, spatial Poisson count per infector
+//     scan + k_spatial   one thread per spatial contact: block proposal + rejection
+//     k_apply_infections DoInfect for every claimed person (lowest key wins)
+//     k_partition_S      S -> L cell-list moves, one thread per touched cell
+//   IncubRecoverySweep
+//     k_active_counts + scan + k_gather_active  latent + infectious people
+//     k_incub_events     DoIncub / DoCase / severity / recovery / death per person
+//     k_partition_LI     L -> I and I -> R/D cell-list moves per touched cell
+//     k_household_after  deferred adult-carer absence and household quarantine
+//
+// Determinism: all random numbers come from Philox streams keyed by
+// (seed, step, entity, purpose); conflicting infections resolve by atomicMin on a
+// 64-bit key; counters are integer atomics; every floating-point reduction runs
+// in a fixed order.  Results therefore do not depend on launch geometry.
+#include <cuda_runtime.h>
+#include <cooperative_groups.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "covidsim_b200.h"
+#include "cs_device.cuh"
+#include "cs_state.h"
+
+namespace cg = cooperative_groups;
+using namespace csb;
+
+// ------------------------------------------------------------------ helpers
+#define CSB_CTR(field) ((unsigned long long*)&d.C->field)
+
+__device__ __forceinline__ void cnt_add(unsigned long long* p, long long v) { atomicAdd(p, (unsigned long long)v); }
+
+// Warp-aggregated append to a device list.
+__device__ __forceinline__ int32_t append(int32_t* count)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    int32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(count, (int32_t)g.size());
+    base = g.shfl(base, 0);
+    return base + (int32_t)g.thread_rank();
+}
+
+__device__ __forceinline__ void mark_cell(const DevPop& d, int c)
+{
+    // cell_flag is a byte array; use the containing 32-bit word for the atomic.
+    unsigned int* w = (unsigned int*)(d.cell_flag + (c & ~3));
+    unsigned int bit = 1u << ((c & 3) * 8);
+    unsigned int old = atomicOr(w, bit);
+    if (!(old & bit)) d.touched[append(d.counts + kCntTouched)] = c;
+}
+
+__device__ __forceinline__ bool flag_household(const DevPop& d, int h, uint8_t f)
+{
+    unsigned int* w = (unsigned int*)(d.hh_flag + (h & ~3));
+    unsigned int sh = (h & 3) * 8;
+    unsigned int old = atomicOr(w, (unsigned int)f << sh);
+    if (((old >> sh) & 0xffu) == 0) d.hh_list[append(d.counts + kCntHH)] = h;
+    return true;
+}
+
+static int g_grid = 148 * 8;
+constexpr int kThreads = 256;
+
+// ----------------------------------------------------------------- scans
+// Exclusive scan of n int32 (n read from *n_dev when given) into out[0..n],
+// out[n] = total (also written to *total_dev when given).  Fixed grid of
+// kScanBlocks blocks, each scanning one contiguous chunk.
+constexpr int kScanBlocks = 1024;
+
+__global__ void k_scan_reduce(const int32_t* __restrict__ in, int n_host, const int32_t* n_dev, int32_t* sums)
+{
+    int n = n_dev ? *n_dev : n_host;
+    long long chunk = ((long long)n + gridDim.x - 1) / gridDim.x;
+    long long s = blockIdx.x * chunk, e = min((long long)n, s + chunk);
+    int32_t acc = 0;
+    for (long long i = s + threadIdx.x; i < e; i += blockDim.x) acc += in[i];
+    __shared__ int32_t red[32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int32_t v = (threadIdx.x < blockDim.x / 32) ? red[threadIdx.x] : 0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) sums[blockIdx.x] = v;
+    }
+}
+
+__global__ void k_scan_top(int32_t* sums, int nb, int32_t* out, int n_host, const int32_t* n_dev, int32_t* total_dev)
+{
+    // one block of 1024 threads, nb <= 1024
+    __shared__ int32_t sh[1024];
+    int t = threadIdx.x;
+    int32_t v = (t < nb) ? sums[t] : 0;
+    sh[t] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int32_t x = (t >= o) ? sh[t - o] : 0;
+        __syncthreads();
+        sh[t] += x;
+        __syncthreads();
+    }
+    if (t < nb) sums[t] = sh[t] - v;  // exclusive
+    if (t == 1023) {
+        int n = n_dev ? *n_dev : n_host;
+        out[n] = sh[1023];
+        if (total_dev) *total_dev = sh[1023];
+    }
+}
+
+__global__ void k_scan_down(const int32_t* __restrict__ in, int32_t* __restrict__ out, int n_host, const int32_t* n_dev, const int32_t* sums)
+{
+    int n = n_dev ? *n_dev : n_host;
+    long long chunk = ((long long)n + gridDim.x - 1) / gridDim.x;
+    long long s = blockIdx.x * chunk, e = min((long long)n, s + chunk);
+    int32_t carry = sums[blockIdx.x];
+    __shared__ int32_t warp_tot[32];
+    __shared__ int32_t tile_tot;
+    for (long long base = s; base < e; base += blockDim.x) {
+        long long i = base + threadIdx.x;
+        int32_t v = (i < e) ? in[i] : 0;
+        int32_t x = v;
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int32_t t = (lane < (int)(blockDim.x / 32)) ? warp_tot[lane] : 0;
+            int32_t tt = t;
+            for (int o = 1; o < 32; o <<= 1) {
+                int32_t y = __shfl_up_sync(0xffffffffu, tt, o);
+                if (lane >= o) tt += y;
+            }
+            warp_tot[lane] = tt - t;
+            if (lane == 31) tile_tot = tt;
+        }
+        __syncthreads();
+        if (i < e) out[i] = carry + warp_tot[w] + x - v;
+        carry += tile_tot;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------- contexts
+struct cs_gpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    char err[512] = {0};
+    long long launches = 0;
+    DevPop d{};
+    cs_params hp{};                 // host copy of the parameters
+    std::vector<void*> allocs;      // every cudaMalloc of the context
+    cs_params* dP = nullptr;
+    DevIv* dIv = nullptr;
+    cs_counters* dC = nullptr;
+    int32_t* d_seed_list = nullptr;
+    int seed_cap = 0;
+    uint64_t seed = 0;
+    bool run_started = false;
+    int grid = 148 * 8;
+};
+
+static int set_err(cs_gpu_ctx* c, int code, const char* fmt, ...)
+{
+    if (c) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(c->err, sizeof(c->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return set_err(c, CS_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define LAUNCH(kernel, grid, block, ...)                                                           \
+    do {                                                                                           \
+        kernel<<<(grid), (block), 0, c->stream>>>(__VA_ARGS__);                                    \
+        c->launches++;                                                                             \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess) return set_err(c, CS_E_CUDA, "launch %s: %s", #kernel, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+static int dalloc(cs_gpu_ctx* c, T** p, size_t n)
+{
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * (n ? n : 1));
+    if (e != cudaSuccess) return set_err(c, CS_E_CUDA, "cudaMalloc(%zu bytes): %s", sizeof(T) * n, cudaGetErrorString(e));
+    c->allocs.push_back(q);
+    *p = (T*)q;
+    return CS_OK;
+}
+
+template <typename T>
+static int dupload(cs_gpu_ctx* c, T** p, const T* src, size_t n)
+{
+    int r = dalloc(c, p, n);
+    if (r) return r;
+    if (n && src) {
+        cudaError_t e = cudaMemcpyAsync(*p, src, sizeof(T) * n, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) return set_err(c, CS_E_CUDA, "upload: %s", cudaGetErrorString(e));
+    }
+    return CS_OK;
+}
+
+static int scan_excl(cs_gpu_ctx* c, const int32_t* in, int32_t* out, int n_host, const int32_t* n_dev, int32_t* total_dev)
+{
+    LAUNCH(k_scan_reduce, kScanBlocks, kThreads, in, n_host, n_dev, c->d.scan_tmp);
+    LAUNCH(k_scan_top, 1, 1024, c->d.scan_tmp, kScanBlocks, out, n_host, n_dev, total_dev);
+    LAUNCH(k_scan_down, kScanBlocks, kThreads, in, out, n_host, n_dev, c->d.scan_tmp);
+    return CS_OK;
+}
+
+// ================================================================ run start
+__global__ void k_reset_people(DevPop d, uint64_t seed)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.N; p += gridDim.x * blockDim.x) {
+        Stream s(seed, CS_RNG_RUN_INIT, 0, (uint32_t)p, 0);
+        PersonHot h = d.hot[p];
+        h.inf = CS_INF_SUSCEPTIBLE;
+        h.sev = CS_SEV_ASYMPTOMATIC | (CS_SEV_ASYMPTOMATIC << 4);
+        h.dflags = (uint8_t)(2u << CS_DF_QUAR_COMPLY_SHIFT);
+        h.latent_time = 0;
+        h.absent_start = kNever;
+        h.absent_stop = 0;
+        h.isolation_start = kNever;
+        h.quar_start = kNever;
+        h.infness = 0.0f;
+        h.susc = 1.0f;
+        d.hot[p] = h;
+        d.infection_time[p] = 0;
+        d.recovery_time[p] = 0;
+        d.sari_time[p] = d.critical_time[p] = d.stepdown_time[p] = kNever;
+        d.detected_time[p] = 0;
+        d.prob_absent[p] = (float)s.next();
+        d.prob_care[p] = (float)s.next();
+        d.infector[p] = -1;
+        d.infect_type[p] = 0;
+        d.pstep[p] = 0;
+        d.claim[p] = ~0ull;
+    }
+}
+
+__global__ void k_reset_slots(DevPop d)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        int b0 = d.cell_start[c], n = d.cell_start[c + 1] - b0;
+        d.S[c] = n;
+        d.L[c] = d.I[c] = d.R[c] = d.D[c] = 0;
+        d.S0[c] = n;
+        d.tot_prob[c] = 1.0;
+        d.cell_flag[c] = 0;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.N; i += gridDim.x * blockDim.x) {
+        int p = d.cell_members[i];
+        d.slots[i] = p;
+        d.mark[i] = 0;
+    }
+}
+
+__global__ void k_reset_listpos(DevPop d)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        int b0 = d.cell_start[c], n = d.cell_start[c + 1] - b0;
+        for (int i = 0; i < n; i++) d.listpos[d.cell_members[b0 + i]] = i;
+    }
+}
+
+__global__ void k_reset_places(DevPop d, int pt, uint64_t seed)
+{
+    DevPlaces pl = d.pl[pt];
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < pl.n; l += gridDim.x * blockDim.x) {
+        Stream s(seed, CS_RNG_PLACE_INIT, 0, (uint32_t)l, (uint32_t)pt);
+        pl.close_start[l] = kNever;
+        pl.close_end[l] = 0;
+        pl.prob_close[l] = (float)s.next();
+    }
+}
+
+// ============================================================ UpdateProbs
+__global__ void k_update_S0(DevPop d, int do_place)
+{
+    const cs_params& P = *d.P;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.NC; j += gridDim.x * blockDim.x) {
+        int n = d.cell_start[j + 1] - d.cell_start[j];
+        int s0;
+        if (!do_place) {
+            s0 = d.S[j] + d.L[j] + d.I[j];
+            if (P.DoDeathCountsInS0) {
+                s0 += n / 5;
+                if ((n < 100) || (s0 > n)) s0 = n;
+            }
+        } else
+            s0 = d.S[j];
+        d.S0[j] = s0;
+    }
+}
+
+// tot_prob of src/CovidSim.cpp:2779-2791 without the dense tables: one warp per
+// source cell, lane k summing targets m = k (mod 32) in order, then a fixed fold.
+__global__ void k_tot_prob(DevPop d)
+{
+    const cs_params& P = *d.P;
+    int lane = threadIdx.x & 31;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int l = warp; l < d.NC; l += nwarps) {
+        int gl = d.cell_grid[l];
+        double a = 0.0, b = 0.0;
+        for (int m = lane; m < d.NC; m += 32) {
+            double kf = (double)(float)knum(d, P, dist2_cc_min(P, gl, d.cell_grid[m]), CSB_CTR(err_kernel_range));
+            int n = d.cell_start[m + 1] - d.cell_start[m];
+            a = a + (double)d.S0[m] * kf;
+            b = b + (double)n * kf;
+        }
+        for (int off = 16; off >= 1; off >>= 1) {
+            double ao = __shfl_down_sync(0xffffffffu, a, off);
+            double bo = __shfl_down_sync(0xffffffffu, b, off);
+            if (lane < off) { a = a + ao; b = b + bo; }
+        }
+        if (lane == 0) d.tot_prob[l] = (b > 0) ? a / b : 0.0;
+    }
+}
+
+__global__ void k_block_S0(DevPop d)
+{
+    for (int B = blockIdx.x * blockDim.x + threadIdx.x; B < d.NB; B += gridDim.x * blockDim.x) {
+        long long s = 0;
+        for (int k = d.block_cell_ofs[B]; k < d.block_cell_ofs[B + 1]; k++) {
+            s += d.S0[d.block_cells[k]];
+            d.block_cum[k] = (int32_t)s;
+        }
+        d.block_S0[B] = s;
+    }
+}
+
+// Row b of the proposal table: running sum over B of S0_B * bound(b, B), added in
+// B order by lane 0 so the doubles round exactly as a sequential loop.
+__global__ void k_block_rows(DevPop d)
+{
+    const cs_params& P = *d.P;
+    int lane = threadIdx.x & 31;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int b = warp; b < d.NB; b += nwarps) {
+        double* row = d.block_row_cum + (size_t)b * d.NB;
+        double s = 0.0;
+        for (int B0 = 0; B0 < d.NB; B0 += 32) {
+            int B = B0 + lane;
+            double w = 0.0;
+            if (B < d.NB && d.block_S0[B] > 0) w = (double)d.block_S0[B] * block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
+            for (int k = 0; k < 32; k++) {
+                double wk = __shfl_sync(0xffffffffu, w, k);
+                if (B0 + k < d.NB) {
+                    s = s + wk;
+                    if (lane == k) row[B] = s;
+                }
+            }
+        }
+    }
+}
+
+// ======================================================== active-list build
+// mode 0: infectious people [S+L, S+L+I); mode 1: latent + infectious [S, S+L+I).
+__global__ void k_active_counts(DevPop d, int mode)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x)
+        d.cnt[c] = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
+}
+
+__global__ void k_gather_active(DevPop d, int mode)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        int base = d.cell_start[c] + d.S[c] + (mode == 0 ? d.L[c] : 0);
+        int n = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
+        int o = d.act_ofs[c];
+        for (int k = 0; k < n; k++) {
+            d.act[o + k] = d.slots[base + k];
+            d.act_cell[o + k] = c;
+        }
+    }
+}
+
+// =============================================================== InfectSweep
+__device__ __forceinline__ void claim_infection(const DevPop& d, int person, int infector, int code)
+{
+    unsigned long long key = ((unsigned long long)(uint32_t)infector << 8) | (unsigned long long)code;
+    unsigned long long old = atomicMin(d.claim + person, key);
+    if (old == ~0ull) d.queue[append(d.counts + kCntQueue)] = person;
+}
+
+struct StepScalars {
+    double t, fp, seas, sp_beta, hh_beta;
+    int ts;
+};
+
+// Geometric-skip enumeration of the Bernoulli(p) trials over a member list
+// (equivalent to the reference's Binomial count + sample without replacement,
+// src/Sweep.cpp:463-470 and 563-566).
+__device__ void place_candidates(const DevPop& d, const cs_params& P, const StepScalars& st, int i, const PersonHot& hi,
+                                 int pt, int link, double p, bool between, uint64_t seed)
+{
+    const DevPlaces& pl = d.pl[pt];
+    int base = pl.member_ofs[link], n;
+    int gi = group_of(d, pt, i);
+    if (!between) {
+        int g = pl.group_ofs[link] + gi;
+        base += pl.group_start[g];
+        n = pl.group_size[g];
+    } else
+        n = pl.member_ofs[link + 1] - pl.member_ofs[link];
+    if (p <= 0 || n <= 0) return;
+    int mc_place = pl.mcell[link];
+    Stream s(seed, between ? CS_RNG_PLACE_BETWEEN : CS_RNG_PLACE_GROUP, (uint32_t)st.ts, (uint32_t)i, (uint32_t)pt);
+    double logq = (p < 1.0) ? log1p(-p) : 0.0;
+    double pos = -1.0;
+    int iag = age_group(hi);
+    bool ich = is_ch(hi);
+    long long ncand = 0;
+    for (;;) {
+        if (p >= 1.0) pos = pos + 1.0;
+        else pos = pos + 1.0 + floor(log(s.next()) / logq);
+        if (!(pos < (double)n)) break;
+        int m = pl.members[base + (int)pos];
+        ncand++;
+        PersonHot hm = d.hot[m];
+        double sc = calc_place_susc(d, hm, P, pt, st.ts);
+        if (between && ich && is_ch(hm) && gi != group_of(d, pt, m)) sc *= P.CareHomeResidentPlaceScaling;
+        if ((pt == P.CareHomePlaceType) && ((!ich) || (!is_ch(hm)))) sc *= P.CareHomeWorkerGroupScaling;
+        if (hm.inf == CS_INF_SUSCEPTIBLE && !host_absent(hm, st.ts)) {
+            sc *= calc_person_susc(hm, iag, P) * p / p;
+            if (moverest_differs(d, hm.mcell, mc_place)) sc *= P.MoveRestrEffect;
+            if ((sc == 1) || (s.next() < sc)) claim_infection(d, m, i, between ? 2 + pt + CS_MAX_PLACE_TYPES : 2 + pt);
+        }
+    }
+    cnt_add(CSB_CTR(work_place_candidates), ncand);
+}
+
+// Household, place and spatial-count passes for one infector (src/Sweep.cpp:314-691).
+__global__ void __launch_bounds__(kThreads) k_infectors(DevPop d, StepScalars st, uint64_t seed)
+{
+    const cs_params& P = *d.P;
+    int nact = d.counts[kCntAct];
+    long long hh_members = 0;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
+        int i = d.act[idx], ci = d.act_cell[idx];
+        PersonHot hi = d.hot[i];
+        int h = hi.hh;
+        int iag = age_group(hi);
+        // household (src/Sweep.cpp:331-377)
+        uint16_t nh = d.hh_nh[h];
+        if (st.hh_beta > 0 && nh > 1) {
+            int f0 = d.hh_first[h], f1 = f0 + nh;
+            double HI = st.hh_beta * calc_house_inf(hi, d.hh_nhr[h], P, st.ts);
+            bool absent = false;
+            for (int m = f0; (m < f1) && (!absent); m++) {
+                bool ma = host_absent(d.hot[m], st.ts);
+                for (int pt = 0; (pt < d.NPT) && (!absent); pt++) {
+                    int lk = link_of(d, pt, m);
+                    if (lk >= 0) absent = place_closed(d, pt, lk, st.ts) && ma;
+                }
+            }
+            if (absent) HI *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_HOUSE];
+            Stream s(seed, CS_RNG_HOUSEHOLD, (uint32_t)st.ts, (uint32_t)i, 0);
+            for (int m = f0; m < f1; m++) {
+                hh_members++;
+                PersonHot hm = d.hot[m];
+                if (hm.inf == CS_INF_SUSCEPTIBLE) {
+                    double foi = HI * calc_house_susc(d, hm, iag, P);
+                    if (s.next() < foi) claim_infection(d, m, i, 1);
+                }
+            }
+        }
+        // places (src/Sweep.cpp:379-647)
+        if (P.DoPlaces && !host_absent(hi, st.ts)) {
+            for (int pt = 0; pt < d.NPT; pt++) {
+                int link = link_of(d, pt, i);
+                if (link < 0) continue;
+                double PI = st.fp * st.seas * calc_place_inf(hi, P, pt, st.ts);
+                if (moverest_differs(d, hi.mcell, d.pl[pt].mcell[link])) PI *= P.MoveRestrEffect;
+                if (pt != P.HotelPlaceType) {
+                    double p1 = PI;
+                    if (p1 > 1) p1 = 1;
+                    place_candidates(d, P, st, i, hi, pt, link, p1, false, seed);
+                }
+                int n = d.pl[pt].member_ofs[link + 1] - d.pl[pt].member_ofs[link];
+                double p2 = PI * (P.PlaceTypePropBetweenGroupLinks[pt] * P.PlaceTypeGroupSizeParam1[pt] / ((double)n));
+                if (p2 > 1) p2 = 1;
+                place_candidates(d, P, st, i, hi, pt, link, p2, true, seed);
+            }
+        }
+        // spatial infectiousness and per-infector Poisson count (src/Sweep.cpp:656-698)
+        int k = 0;
+        uint8_t closed_i = 0;
+        if (st.sp_beta > 0) {
+            double si = calc_spatial_inf(hi, P, st.ts);
+            bool closed = false;
+            if (P.DoPlaces)
+                for (int pt = 0; (pt < d.NPT) && (!closed); pt++) {
+                    int lk = link_of(d, pt, i);
+                    if (lk >= 0) closed = place_closed(d, pt, lk, st.ts);
+                }
+            if (closed && host_absent(hi, st.ts)) { si *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL]; closed_i = 1; }
+            double lambda = si * st.sp_beta * d.tot_prob[ci];
+            Stream s(seed, CS_RNG_SPATIAL_COUNT, (uint32_t)st.ts, (uint32_t)i, 0);
+            k = sample_poisson(s, lambda, CSB_CTR(err_spatial_tries));
+        }
+        d.cnt[idx] = k;
+        d.act_closed[idx] = closed_i;
+    }
+    cnt_add(CSB_CTR(work_hh_members), hh_members);
+}
+
+// One thread per spatial contact (src/Sweep.cpp:742-856): pick a target block from
+// the infector's block row, a slot uniformly among the block's S0 slots, accept with
+// K(d)/bound, redraw on rejection or a dead target.
+__global__ void __launch_bounds__(kThreads) k_spatial(DevPop d, StepScalars st, uint64_t seed)
+{
+    const cs_params& P = *d.P;
+    int nact = d.counts[kCntAct];
+    int ncont = d.counts[kCntContacts];
+    long long draws = 0;
+    for (int cidx = blockIdx.x * blockDim.x + threadIdx.x; cidx < ncont; cidx += gridDim.x * blockDim.x) {
+        // infector owning contact cidx: last idx with cnt_ofs[idx] <= cidx
+        int lo = 0, hi = nact - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (d.cnt_ofs[mid] <= cidx) lo = mid; else hi = mid - 1;
+        }
+        int idx = lo;
+        int j = cidx - d.cnt_ofs[idx];
+        int i = d.act[idx], ci = d.act_cell[idx];
+        bool closed_i = d.act_closed[idx] != 0;
+        PersonHot hinf = d.hot[i];
+        int b = d.cell_block[ci];
+        const double* row = d.block_row_cum + (size_t)b * d.NB;
+        double total = row[d.NB - 1];
+        if (!(total > 0)) { cnt_add(CSB_CTR(err_spatial_tries), 1); continue; }
+        Stream s(seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)st.ts, (uint32_t)i, (uint32_t)j);
+        int iag = age_group(hinf);
+        for (int tries = 0;; tries++) {
+            if (tries >= kMaxSpatialTries) { cnt_add(CSB_CTR(err_spatial_tries), 1); break; }
+            draws++;
+            double target = s.next() * total;
+            int l0 = 0, l1 = d.NB - 1;
+            while (l0 < l1) {
+                int mid = (l0 + l1) >> 1;
+                if (target < row[mid]) l1 = mid; else l0 = mid + 1;
+            }
+            int B = l0;
+            long long bS0 = d.block_S0[B];
+            if (bS0 <= 0) continue;
+            double r = floor(s.next() * (double)bS0);
+            int k0 = d.block_cell_ofs[B], k1 = d.block_cell_ofs[B + 1] - 1;
+            while (k0 < k1) {
+                int mid = (k0 + k1) >> 1;
+                if (r < (double)d.block_cum[mid]) k1 = mid; else k0 = mid + 1;
+            }
+            int m = d.block_cells[k0];
+            int slot = (int)(r - (double)(d.block_cum[k0] - d.S0[m]));
+            int p = d.slots[d.cell_start[m] + slot];
+            PersonHot hp = d.hot[p];
+            double d2 = dist2_hh(d, P, hinf.hh, hp.hh);
+            double accept = knum(d, P, d2, CSB_CTR(err_kernel_range)) / block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
+            if ((s.next() >= accept) || !is_alive(hp.inf)) continue;
+            if ((ci != m) || (hp.hh != hinf.hh)) {
+                double ss = calc_spatial_susc(d, hp, P, st.ts);
+                if (is_ch(hp) || is_ch(hinf)) ss *= P.CareHomeResidentSpatialScaling;
+                if (slot < d.S[m]) {
+                    ss *= calc_person_susc(hp, iag, P);
+                    ss *= P.WAIFW_Matrix_SpatialOnly[age_group(hp)][iag];
+                    if (moverest_differs(d, hp.mcell, hinf.mcell)) ss *= P.MoveRestrEffect;
+                    if ((!closed_i) && host_absent(hp, st.ts)) {
+                        bool f = false;
+                        for (int pt = 0; (pt < d.NPT) && (!f); pt++) {
+                            int lk = link_of(d, pt, p);
+                            if (lk >= 0) f = place_closed(d, pt, lk, st.ts);
+                        }
+                        if (f) ss *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL];
+                    }
+                    if ((ss == 1) || (s.next() < ss))
+                        if (hp.inf == CS_INF_SUSCEPTIBLE) claim_infection(d, p, i, 2 + 2 * CS_MAX_PLACE_TYPES);
+                }
+            }
+            break;
+        }
+    }
+    cnt_add(CSB_CTR(work_spatial_draws), draws);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt_add(CSB_CTR(work_infectors), nact);
+        cnt_add(CSB_CTR(work_spatial_contacts), ncont);
+    }
+}
+
+// DoInfect (src/Update.cpp:100-195) for every person claimed this step.
+__global__ void k_apply_infections(DevPop d, double t, int ts, uint64_t seed)
+{
+    const cs_params& P = *d.P;
+    int nq = d.counts[kCntQueue];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        int p = d.queue[q];
+        unsigned long long key = d.claim[p];
+        d.claim[p] = ~0ull;
+        int32_t infector = (int32_t)(uint32_t)(key >> 8);
+        int code = (int)(key & 0xff);
+        int16_t it = (infector >= 0)
+            ? (int16_t)(code + CS_INFECT_TYPE_MASK * (1 + d.infect_type[infector] / CS_INFECT_TYPE_MASK))
+            : (int16_t)code;
+        PersonHot h = d.hot[p];
+        h.inf = CS_INF_LATENT;
+        d.infection_time[p] = (uint16_t)ts;
+        d.infector[p] = infector;
+        d.infect_type[p] = it;
+        int cell = d.mcell_cell[h.mcell];
+        atomicSub(d.S + cell, 1);
+        atomicAdd(d.L + cell, 1);
+        d.mark[d.cell_start[cell] + d.listpos[p]] = 1;
+        atomicAdd(d.cnt + cell, 1);  // transitions out of this cell's S block
+        mark_cell(d, cell);
+        cnt_add(CSB_CTR(cumI), 1);
+        cnt_add(CSB_CTR(cumItype[it % CS_INFECT_TYPE_MASK]), 1);
+        cnt_add(CSB_CTR(cumIa[age_group(h)]), 1);
+        cnt_add(CSB_CTR(cumI_keyworker[(h.pflags & CS_PF_KEYWORKER) ? 1 : 0]), 1);
+        int ad = d.mcell_adunit[h.mcell];
+        if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumI_adunit[ad]), 1);
+        if (P.DoLatent) {
+            Stream s(seed, CS_RNG_LATENT, (uint32_t)ts, (uint32_t)p, 0);
+            double qq;
+            int i = (int)floor((qq = s.next() * CS_CDF_RES));
+            qq -= (double)i;
+            h.latent_time = (uint16_t)floor(0.5 + (t - P.LatentPeriod * log(qq * P.latent_icdf.v[i + 1] + (1.0 - qq) * P.latent_icdf.v[i])) * P.TimeStepsPerDay);
+        } else
+            h.latent_time = (uint16_t)(t * P.TimeStepsPerDay);
+        d.hot[p] = h;
+        if (infector >= 0) {
+            cnt_add(CSB_CTR(cumTG), ((int)(uint16_t)ts) - ((int)d.infection_time[infector]));
+            cnt_add(CSB_CTR(cumSI), ((int)h.latent_time) - ((int)d.hot[infector].latent_time));
+            cnt_add(CSB_CTR(nTG), 1);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_new_infections), nq);
+}
+
+// Swap-with-block-end removal of marked slots, high to low (src/Update.cpp:1402-1579
+// UpdateCell sequence).  Returns nothing; moved people get their new listpos.
+__device__ void partition_block(const DevPop& d, int base, int b0, int n, int nmarked, uint8_t want,
+                                bool relay_exit)
+{
+    int cur = n, removed = 0;
+    for (int pos = b0 + n - 1; pos >= b0 && removed < nmarked; pos--) {
+        if (d.mark[pos] != want) continue;
+        cur--;
+        removed++;
+        int end = b0 + cur;
+        if (pos < end) {
+            int a = d.slots[pos], e = d.slots[end];
+            d.slots[pos] = e;
+            d.listpos[e] = pos - base;
+            d.slots[end] = a;
+            d.listpos[a] = end - base;
+        }
+        d.mark[pos] = 0;
+        d.mark[end] = 0;
+        if (relay_exit) {
+            int a = d.slots[end];
+            if (d.pstep[a] & kStepItoRD) d.mark[end] = 2;
+        }
+    }
+}
+
+// S -> L list moves for every cell that gained latent people this step.
+__global__ void k_partition_S(DevPop d)
+{
+    int nt = d.counts[kCntTouched];
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_cells_touched), nt);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+        int c = d.touched[k];
+        int moved = d.cnt[c];
+        int base = d.cell_start[c];
+        partition_block(d, base, base, d.S[c] + moved, moved, 1, false);
+        d.cnt[c] = 0;
+        d.cell_flag[c] = 0;
+    }
+}
+
+// ====================================================== IncubRecoverySweep
+__device__ __forceinline__ void sev_add(const DevPop& d, int ad, int which, int delta, bool cum)
+{
+    bool adok = ad >= 0 && ad < CS_MAX_ADUNITS;
+    switch (which) {
+    case CS_SEV_MILD: cnt_add(CSB_CTR(Mild), delta); if (cum) cnt_add(CSB_CTR(cumMild), 1); break;
+    case CS_SEV_ILI: cnt_add(CSB_CTR(ILI), delta); if (cum) cnt_add(CSB_CTR(cumILI), 1); break;
+    case CS_SEV_SARI: cnt_add(CSB_CTR(SARI), delta); if (cum) cnt_add(CSB_CTR(cumSARI), 1); break;
+    case CS_SEV_CRITICAL:
+        cnt_add(CSB_CTR(Critical), delta);
+        if (adok) cnt_add(CSB_CTR(Critical_adunit[ad]), delta);
+        if (cum) { cnt_add(CSB_CTR(cumCritical), 1); if (adok) cnt_add(CSB_CTR(cumCritical_adunit[ad]), 1); }
+        break;
+    case CS_SEV_STEPDOWN: cnt_add(CSB_CTR(CritRecov), delta); if (cum) cnt_add(CSB_CTR(cumCritRecov), 1); break;
+    default: break;
+    }
+}
+
+// DoIncub (src/Update.cpp:408-523) for one person, on a register copy of the record.
+__device__ void do_incub(const DevPop& d, const cs_params& P, int p, PersonHot& h, int ts, uint64_t seed)
+{
+    int age = age_group(h);
+    if (age >= CS_NUM_AGE_GROUPS) age = CS_NUM_AGE_GROUPS - 1;
+    Stream s(seed, CS_RNG_INCUB, (uint32_t)ts, (uint32_t)p, 0);
+    unsigned long long* err = CSB_CTR(err_spatial_tries);
+    float infn = (float)P.AgeInfectiousness[age];
+    if (P.InfectiousnessSD > 0) {
+        double k = 1 / (P.InfectiousnessSD * P.InfectiousnessSD);
+        infn *= (float)sample_gamma(s, k, k, err);
+    }
+    if (s.next() < P.ProportionSymptomatic[age]) {
+        h.inf = CS_INF_INFECTIOUS_ALMOST_SYMPTOMATIC;
+        infn *= (float)(-P.SymptInfectiousness);
+    } else {
+        h.inf = CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE;
+        infn *= (float)P.AsymptInfectiousness;
+    }
+    h.infness = infn;
+    double spd = P.TimeStepsPerDay;
+    if (!P.DoSeverity || h.inf == CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE) {
+        if (P.DoInfectiousnessProfile)
+            d.recovery_time[p] = (uint16_t)(h.latent_time + (uint16_t)(P.InfectiousPeriod * spd));
+        else
+            d.recovery_time[p] = (uint16_t)(h.latent_time + icdf_choose(P.infectious_icdf, P.InfectiousPeriod, s.next(), spd));
+    } else {
+        int CaseTime = h.latent_time + ((int)(P.LatentToSymptDelay / P.ModelTimeStep));
+        double x = s.next();
+        int fin;
+        if (x < P.Prop_ILI_ByAge[age]) fin = CS_SEV_ILI;
+        else if (x < P.Prop_ILI_ByAge[age] + P.Prop_SARI_ByAge[age]) fin = CS_SEV_SARI;
+        else if (x < P.Prop_ILI_ByAge[age] + P.Prop_SARI_ByAge[age] + P.Prop_Critical_ByAge[age]) fin = CS_SEV_CRITICAL;
+        else fin = CS_SEV_MILD;
+        bool to_die = false;
+        if (fin == CS_SEV_CRITICAL) { if (s.next() < (P.CFR_Critical_ByAge[age] * P.CFR_Critical_Scale_Current)) to_die = true; }
+        else if (fin == CS_SEV_SARI) { if (s.next() < (P.CFR_SARI_ByAge[age] * P.CFR_SARI_Scale_Current)) to_die = true; }
+        else if (fin == CS_SEV_ILI) { if (s.next() < (P.CFR_ILI_ByAge[age] * P.CFR_ILI_Scale_Current)) to_die = true; }
+        if (is_ch(h) && ((fin == CS_SEV_CRITICAL) || (fin == CS_SEV_SARI)) && (s.next() > P.CareHomeRelProbHosp)) {
+            to_die = true;
+            fin = CS_SEV_ILI;
+        }
+        h.sev = (uint8_t)((h.sev & 0x0f) | (fin << 4));
+        if (to_die) h.dflags |= CS_DF_TO_DIE;
+        uint16_t rec;
+        if (fin == CS_SEV_MILD)
+            rec = (uint16_t)(CaseTime + icdf_choose(P.MildToRecovery_icdf, P.Mean_MildToRecovery[age], s.next(), spd));
+        else if (fin == CS_SEV_CRITICAL) {
+            uint16_t sari = (uint16_t)(CaseTime + icdf_choose(P.ILIToSARI_icdf, P.Mean_ILIToSARI[age], s.next(), spd));
+            uint16_t crit = (uint16_t)(sari + icdf_choose(P.SARIToCritical_icdf, P.Mean_SARIToCritical[age], s.next(), spd));
+            d.sari_time[p] = sari;
+            d.critical_time[p] = crit;
+            if (to_die) {
+                if (P.IncludeStepDownToDeath == 1) {
+                    uint16_t sd = (uint16_t)(crit + icdf_choose(P.CriticalToCritRecov_icdf, P.Mean_CriticalToCritRecov[age], s.next(), spd));
+                    d.stepdown_time[p] = sd;
+                    rec = (uint16_t)(sd + icdf_choose(P.StepdownToDeath_icdf, P.Mean_StepdownToDeath[age], s.next(), spd));
+                } else
+                    rec = (uint16_t)(crit + icdf_choose(P.CriticalToDeath_icdf, P.Mean_CriticalToDeath[age], s.next(), spd));
+            } else {
+                uint16_t sd = (uint16_t)(crit + icdf_choose(P.CriticalToCritRecov_icdf, P.Mean_CriticalToCritRecov[age], s.next(), spd));
+                d.stepdown_time[p] = sd;
+                rec = (uint16_t)(sd + icdf_choose(P.CritRecovToRecov_icdf, P.Mean_CritRecovToRecov[age], s.next(), spd));
+            }
+        } else if (fin == CS_SEV_SARI) {
+            uint16_t sari = (uint16_t)(CaseTime + icdf_choose(P.ILIToSARI_icdf, P.Mean_ILIToSARI[age], s.next(), spd));
+            d.sari_time[p] = sari;
+            if (to_die) rec = (uint16_t)(sari + icdf_choose(P.SARIToDeath_icdf, P.Mean_SARIToDeath[age], s.next(), spd));
+            else rec = (uint16_t)(sari + icdf_choose(P.SARIToRecovery_icdf, P.Mean_SARIToRecovery[age], s.next(), spd));
+        } else {
+            if (to_die) rec = (uint16_t)(CaseTime + icdf_choose(P.ILIToDeath_icdf, P.Mean_ILIToDeath[age], s.next(), spd));
+            else rec = (uint16_t)(CaseTime + icdf_choose(P.ILIToRecovery_icdf, P.Mean_ILIToRecovery[age], s.next(), spd));
+        }
+        d.recovery_time[p] = rec;
+    }
+    if (h.inf == CS_INF_INFECTIOUS_ALMOST_SYMPTOMATIC && ((P.ControlPropCasesId == 1) || (s.next() < P.ControlPropCasesId))) {
+        h.dflags |= CS_DF_DETECTED;
+        d.detected_time[p] = (uint16_t)(ts + (uint16_t)(P.LatentToSymptDelay * spd));
+    }
+}
+
+// DoDetectedCase (src/Update.cpp:525-792): case isolation now, household
+// quarantine deferred to the per-household pass.
+__device__ void do_detected_case(const DevPop& d, const cs_params& P, const DevIv& iv, int p, PersonHot& h, double t, int ts,
+                                 uint64_t seed)
+{
+    int ad = d.mcell_adunit[h.mcell];
+    if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumDC_adunit[ad]), 1);
+    if (P.DoHouseholds && t >= iv.hq_start && t < iv.hq_start + iv.hq_dur) flag_household(d, h.hh, 4);
+    if (t >= iv.ci_start && t < iv.ci_start + iv.ci_dur) {
+        Stream s(seed, CS_RNG_DETECTED, (uint32_t)ts, (uint32_t)p, 0);
+        if ((P.CaseIsolationProp == 1) || (s.next() < P.CaseIsolationProp)) {
+            h.isolation_start = (uint16_t)ts;
+            if (host_absent(h, ts)) {
+                if (h.absent_stop < ts + P.usCaseAbsenteeismDelay + P.usCaseIsolationDuration)
+                    h.absent_stop = (uint16_t)(ts + P.usCaseAbsenteeismDelay + P.usCaseIsolationDuration);
+            } else if (P.DoRealSymptWithdrawal) {
+                h.absent_start = (uint16_t)(ts + P.usCaseIsolationDelay);
+                h.absent_stop = (uint16_t)(ts + P.usCaseIsolationDelay + P.usCaseIsolationDuration);
+                if (P.DoPlaces && !host_quarantined(h, P, ts) && link_of(d, P.PlaceTypeNoAirNum - 1, p) >= 0 && h.age >= P.CaseAbsentChildAgeCutoff)
+                    cnt_add(CSB_CTR(cumAC), 1);
+                if (P.DoHouseholds && P.DoPlaces && h.age < P.CaseAbsentChildAgeCutoff) {
+                    if (!host_quarantined(h, P, ts)) cnt_add(CSB_CTR(cumACS), 1);
+                    if (d.prob_care[p] < P.CaseAbsentChildPropAdultCarers) flag_household(d, h.hh, 2);
+                }
+            }
+        }
+    }
+}
+
+// DoCase (src/Update.cpp:794-894).
+__device__ void do_case(const DevPop& d, const cs_params& P, const DevIv& iv, int p, PersonHot& h, double t, int ts, uint64_t seed)
+{
+    int age = age_group(h);
+    if (age >= CS_NUM_AGE_GROUPS) age = CS_NUM_AGE_GROUPS - 1;
+    if (h.inf != CS_INF_INFECTIOUS_ALMOST_SYMPTOMATIC) return;
+    h.inf = CS_INF_CASE;
+    if (host_absent(h, ts)) {
+        if (h.absent_stop < ts + P.usCaseAbsenteeismDelay + P.usCaseAbsenteeismDuration)
+            h.absent_stop = (uint16_t)(ts + P.usCaseAbsenteeismDelay + P.usCaseAbsenteeismDuration);
+    } else if ((P.DoRealSymptWithdrawal) && (P.DoPlaces)) {
+        Stream s(seed, CS_RNG_CASE, (uint32_t)ts, (uint32_t)p, 0);
+        h.absent_start = kNever;
+        for (int j = 0; j < d.NPT; j++)
+            if ((link_of(d, j, p) >= 0) && (j != P.HotelPlaceType) && (!host_absent(h, ts)) && (P.SymptPlaceTypeWithdrawalProp[j] > 0)) {
+                if ((!is_ch(h)) && ((P.SymptPlaceTypeWithdrawalProp[j] == 1) || (s.next() < P.SymptPlaceTypeWithdrawalProp[j]))) {
+                    h.absent_start = (uint16_t)(ts + P.usCaseAbsenteeismDelay);
+                    h.absent_stop = (uint16_t)(ts + P.usCaseAbsenteeismDelay + P.usCaseAbsenteeismDuration);
+                    if ((!host_quarantined(h, P, ts)) && (link_of(d, P.PlaceTypeNoAirNum - 1, p) >= 0) && (h.age >= P.CaseAbsentChildAgeCutoff))
+                        cnt_add(CSB_CTR(cumAC), 1);
+                    if ((P.DoHouseholds) && (h.age < P.CaseAbsentChildAgeCutoff)) {
+                        if (!host_quarantined(h, P, ts)) cnt_add(CSB_CTR(cumACS), 1);
+                        if (d.prob_care[p] < P.CaseAbsentChildPropAdultCarers) flag_household(d, h.hh, 1);
+                    }
+                }
+            }
+    }
+    if (h.dflags & CS_DF_DETECTED) {
+        cnt_add(CSB_CTR(cumDC), 1);
+        do_detected_case(d, P, iv, p, h, t, ts, seed);
+    }
+    cnt_add(CSB_CTR(cumC), 1);
+    cnt_add(CSB_CTR(cumCa[age]), 1);
+    cnt_add(CSB_CTR(cumC_keyworker[(h.pflags & CS_PF_KEYWORKER) ? 1 : 0]), 1);
+    int ad = d.mcell_adunit[h.mcell];
+    if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumC_adunit[ad]), 1);
+    if (P.DoSeverity) {
+        int cur = h.sev & 0x0f, fin = h.sev >> 4;
+        if (cur == CS_SEV_ASYMPTOMATIC) {
+            int to = (fin == CS_SEV_MILD) ? CS_SEV_MILD : CS_SEV_ILI;
+            h.sev = (uint8_t)((h.sev & 0xf0) | to);
+            sev_add(d, ad, to, 1, true);
+        }
+    }
+}
+
+// The infectious-person body of IncubRecoverySweep (src/Sweep.cpp:929-977).
+// Returns bit 0 when the person leaves the infectious block this step and bit 1
+// when any event fired (the record must be written back).
+__device__ int infectious_events(const DevPop& d, const cs_params& P, const DevIv& iv, int p, PersonHot& h, int cell,
+                                 double t, int ts, uint64_t seed)
+{
+    int CaseTime = h.latent_time + ((int)(P.LatentToSymptDelay / P.ModelTimeStep));
+    uint16_t rec = d.recovery_time[p];
+    bool any = (ts == (uint16_t)CaseTime) || (ts == rec) ||
+               (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
+    if (!any) return 0;
+    if (P.DoSymptoms && ts == (uint16_t)CaseTime) do_case(d, P, iv, p, h, t, ts, seed);
+    bool to_die = (h.dflags & CS_DF_TO_DIE) != 0;
+    int ad = d.mcell_adunit[h.mcell];
+    if (P.DoSeverity) {
+        int cur = h.sev & 0x0f;
+        if (ts == d.sari_time[p] && cur == CS_SEV_ILI) { cur = CS_SEV_SARI; sev_add(d, ad, CS_SEV_ILI, -1, false); sev_add(d, ad, CS_SEV_SARI, 1, true); }
+        if (ts == d.critical_time[p] && cur == CS_SEV_SARI) { cur = CS_SEV_CRITICAL; sev_add(d, ad, CS_SEV_SARI, -1, false); sev_add(d, ad, CS_SEV_CRITICAL, 1, true); }
+        if (ts == d.stepdown_time[p] && cur == CS_SEV_CRITICAL && !to_die) { cur = CS_SEV_STEPDOWN; sev_add(d, ad, CS_SEV_CRITICAL, -1, false); sev_add(d, ad, CS_SEV_STEPDOWN, 1, true); }
+        if (ts == rec) {
+            if (to_die) {
+                if (cur == CS_SEV_CRITICAL) { sev_add(d, ad, CS_SEV_CRITICAL, -1, false); cnt_add(CSB_CTR(cumDeath_Critical), 1); cur = CS_SEV_DEAD; }
+                else if (cur == CS_SEV_SARI) { sev_add(d, ad, CS_SEV_SARI, -1, false); cnt_add(CSB_CTR(cumDeath_SARI), 1); cur = CS_SEV_DEAD; }
+                else if (cur == CS_SEV_ILI) { sev_add(d, ad, CS_SEV_ILI, -1, false); cnt_add(CSB_CTR(cumDeath_ILI), 1); cur = CS_SEV_DEAD; }
+            } else if (h.inf == CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE || h.inf == CS_INF_CASE) {
+                if (cur == CS_SEV_MILD) { sev_add(d, ad, CS_SEV_MILD, -1, false); cur = CS_SEV_RECOVERED; }
+                else if (cur == CS_SEV_ILI) { sev_add(d, ad, CS_SEV_ILI, -1, false); cur = CS_SEV_RECOVERED; }
+                else if (cur == CS_SEV_SARI) { sev_add(d, ad, CS_SEV_SARI, -1, false); cur = CS_SEV_RECOVERED; }
+                else if (cur == CS_SEV_STEPDOWN) { sev_add(d, ad, CS_SEV_STEPDOWN, -1, false); cur = CS_SEV_RECOVERED; }
+            }
+        }
+        h.sev = (uint8_t)((h.sev & 0xf0) | cur);
+    }
+    if (ts == rec && (h.inf == CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE || h.inf == CS_INF_CASE)) {
+        atomicSub(d.I + cell, 1);
+        cnt_add(CSB_CTR(work_transitions), 1);
+        if (!to_die) {
+            h.inf = (h.inf == CS_INF_CASE) ? CS_INF_RECOVERED_FROM_SYMP : CS_INF_RECOVERED_FROM_ASYMP;
+            atomicAdd(d.R + cell, 1);
+            cnt_add(CSB_CTR(cumR), 1);
+        } else {
+            h.inf = (h.inf == CS_INF_CASE) ? CS_INF_DEAD_WAS_SYMP : CS_INF_DEAD_WAS_ASYMP;
+            atomicAdd(d.D + cell, 1);
+            cnt_add(CSB_CTR(cumD), 1);
+            cnt_add(CSB_CTR(cumDa[age_group(h)]), 1);
+            if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumD_adunit[ad]), 1);
+        }
+        return 3;
+    }
+    return 2;
+}
+
+// cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
+__global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d, double t, int ts, uint64_t seed)
+{
+    const cs_params& P = *d.P;
+    const DevIv iv = *d.iv;
+    int nact = d.counts[kCntAct];
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
+        int p = d.act[idx], c = d.act_cell[idx];
+        PersonHot h = d.hot[p];
+        int pos = d.cell_start[c] + d.listpos[p];
+        if (h.inf == CS_INF_LATENT) {
+            if (h.latent_time != ts) continue;
+            do_incub(d, P, p, h, ts, seed);
+            atomicSub(d.L + c, 1);
+            atomicAdd(d.I + c, 1);
+            int add = 1;
+            d.mark[pos] = 1;
+            cnt_add(CSB_CTR(work_transitions), 1);
+            if (infectious_events(d, P, iv, p, h, c, t, ts, seed) & 1) {
+                d.pstep[p] = kStepItoRD;
+                add += 1 << 16;
+            }
+            d.hot[p] = h;
+            atomicAdd(d.cnt + c, add);
+            mark_cell(d, c);
+        } else {
+            int r = infectious_events(d, P, iv, p, h, c, t, ts, seed);
+            if (r & 2) d.hot[p] = h;
+            if (r & 1) {
+                d.mark[pos] = 2;
+                atomicAdd(d.cnt + c, 1 << 16);
+                mark_cell(d, c);
+            }
+        }
+    }
+}
+
+__global__ void k_partition_LI(DevPop d)
+{
+    int nt = d.counts[kCntTouched];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+        int c = d.touched[k];
+        int v = d.cnt[c];
+        int nLI = v & 0xffff, nIR = (v >> 16) & 0xffff;
+        int base = d.cell_start[c];
+        int S = d.S[c], L = d.L[c], I = d.I[c];
+        if (nLI) partition_block(d, base, base + S, L + nLI, nLI, 1, true);
+        if (nIR) partition_block(d, base, base + S + L, I + nIR, nIR, 2, false);
+        d.cnt[c] = 0;
+        d.cell_flag[c] = 0;
+    }
+}
+
+__global__ void k_clear_pstep(DevPop d)
+{
+    int nact = d.counts[kCntAct];
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) d.pstep[d.act[idx]] = 0;
+}
+
+// Deferred household actions, once per household, after every per-person
+// transition of the step: the adult-carer absence of DoCase/DoDetectedCase
+// (src/Update.cpp:736-763, 843-868) and household quarantine (src/Update.cpp:676-708).
+__global__ void k_household_after(DevPop d, int ts, uint64_t seed)
+{
+    const cs_params& P = *d.P;
+    int nh = d.counts[kCntHH];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+        int h = d.hh_list[k];
+        uint8_t f = d.hh_flag[h];
+        d.hh_flag[h] = 0;
+        int j1 = d.hh_first[h], j2 = j1 + d.hh_nh[h];
+        if (f & 3) {
+            int wp = P.PlaceTypeNoAirNum - 1;
+            bool ok = false;
+            for (int j = j1; (j < j2) && (!ok); j++) {
+                PersonHot hj = d.hot[j];
+                ok = (is_alive(hj.inf) && (hj.age >= P.CaseAbsentChildAgeCutoff) &&
+                      ((link_of(d, wp, j) < 0) || host_absent(hj, ts) || host_quarantined(hj, P, ts)));
+            }
+            if (!ok) {
+                int kk = -1;
+                for (int j = j1; j < j2; j++) {
+                    PersonHot hj = d.hot[j];
+                    if ((hj.age >= P.CaseAbsentChildAgeCutoff) && is_alive(hj.inf)) { kk = j; break; }
+                }
+                if (kk >= 0) {
+                    PersonHot hk = d.hot[kk];
+                    if ((f & 2) || !host_absent(hk, ts)) d.hot[kk].absent_start = (uint16_t)(ts + P.usCaseIsolationDelay);
+                    d.hot[kk].absent_stop = (uint16_t)(ts + P.usCaseIsolationDelay + P.usCaseIsolationDuration);
+                    cnt_add(CSB_CTR(cumAA), 1);
+                }
+            }
+        }
+        if (f & 4) {
+            if (host_to_be_quarantined(d.hot[j1], P, ts) && !P.DoHQretrigger) continue;
+            Stream s(seed, CS_RNG_HQ, (uint32_t)ts, (uint32_t)h, 0);
+            uint16_t qs = (uint16_t)(ts + ((uint16_t)(P.TimeStepsPerDay * P.HQuarantineDelay)));
+            int kc = (s.next() < P.HQuarantinePropHouseCompliant) ? 1 : 0;
+            if (kc) cnt_add(CSB_CTR(cumHQ), 1);
+            for (int j = j1; j < j2; j++) {
+                int comply = (kc == 0) ? 0 : ((s.next() < P.HQuarantinePropIndivCompliant) ? 1 : 0);
+                PersonHot hj = d.hot[j];
+                hj.quar_start = qs;
+                hj.dflags = (uint8_t)((hj.dflags & ~CS_DF_QUAR_COMPLY_MASK) | (comply << CS_DF_QUAR_COMPLY_SHIFT));
+                d.hot[j] = hj;
+            }
+        }
+    }
+}
+
+// ============================================================ seeding
+__global__ void k_seed_claims(DevPop d, const int32_t* list, int n)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int p = list[k];
+        if (p < 0 || p >= d.N) continue;
+        if (d.hot[p].inf != CS_INF_SUSCEPTIBLE) continue;
+        unsigned long long key = ((unsigned long long)(uint32_t)(-2) << 8) | (unsigned long long)(CS_INFECT_TYPE_MASK - 1);
+        if (atomicCAS(d.claim + p, ~0ull, key) == ~0ull) d.queue[append(d.counts + kCntQueue)] = p;
+    }
+}
+
+// ============================================================ interventions
+__global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop)
+{
+    const cs_params& P = *d.P;
+    DevPlaces pl = d.pl[pt];
+    for (int l = blockIdx.x; l < pl.n; l += gridDim.x) {
+        if (sel && !sel[pl.mcell[l]]) continue;
+        __shared__ int do_members;
+        if (threadIdx.x == 0) {
+            do_members = 0;
+            if (pl.close_end[l] < stop) {
+                if (pl.prob_close[l] >= P.Efficacies[CS_NPI_PLACE_CLOSURE][pt]) {
+                    if (pl.close_start[l] > start) pl.close_start[l] = start;
+                    pl.close_end[l] = stop;
+                    do_members = P.DoRealSymptWithdrawal;
+                } else
+                    pl.close_start[l] = pl.close_end[l] = stop;
+            }
+        }
+        __syncthreads();
+        if (do_members)
+            for (int k = pl.member_ofs[l] + threadIdx.x; k < pl.member_ofs[l + 1]; k += blockDim.x) {
+                int w = pl.members[k];
+                // a person can be a member of only one place per type: no race
+                PersonHot* hw = d.hot + w;
+                if (hw->absent_start > start) hw->absent_start = start;
+                if (hw->absent_stop < stop) hw->absent_stop = stop;
+            }
+        __syncthreads();
+    }
+}
+
+__global__ void k_cell_totals(DevPop d)
+{
+    long long s = 0, l = 0, i = 0, r = 0, dd = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        s += d.S[c]; l += d.L[c]; i += d.I[c]; r += d.R[c]; dd += d.D[c];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        l += __shfl_down_sync(0xffffffffu, l, o);
+        i += __shfl_down_sync(0xffffffffu, i, o);
+        r += __shfl_down_sync(0xffffffffu, r, o);
+        dd += __shfl_down_sync(0xffffffffu, dd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        cnt_add(CSB_CTR(S), s); cnt_add(CSB_CTR(L), l); cnt_add(CSB_CTR(I), i);
+        cnt_add(CSB_CTR(R), r); cnt_add(CSB_CTR(D), dd);
+    }
+}
+
+// ================================================================ host API
+extern "C" {
+
+int cs_abi_version(void) { return CS_ABI_VERSION; }
+size_t cs_sizeof_params(void) { return sizeof(cs_params); }
+size_t cs_sizeof_population(void) { return sizeof(cs_population); }
+size_t cs_sizeof_counters(void) { return sizeof(cs_counters); }
+
+const char* cs_gpu_last_error(const cs_gpu_ctx* c) { return c ? c->err : "null context"; }
+void* cs_gpu_stream(cs_gpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+int64_t cs_gpu_launch_count(const cs_gpu_ctx* c) { return c ? c->launches : 0; }
+
+static int check_params(cs_gpu_ctx* c, const cs_params* P)
+{
+    if (P->FalsePositiveRate != 0) return set_err(c, CS_E_UNSUPPORTED, "FalsePositiveRate must be 0 (false-positive cases are not modelled)");
+    if (P->NumPlaceTypes < 0 || P->NumPlaceTypes > CS_MAX_PLACE_TYPES) return set_err(c, CS_E_ARG, "NumPlaceTypes out of range");
+    if (P->kernel_size < 2 || P->kernel_expansion < 1 || !(P->kernel_delta > 0)) return set_err(c, CS_E_ARG, "kernel table not set");
+    if (P->ncw <= 0 || P->nch <= 0) return set_err(c, CS_E_ARG, "grid size not set");
+    return CS_OK;
+}
+
+int cs_gpu_create(const cs_population* pop, const cs_params* params, int device, cs_gpu_ctx** out)
+{
+    if (!out) return CS_E_ARG;
+    cs_gpu_ctx* c = new cs_gpu_ctx();
+    *out = c;
+    if (!pop || !params) return set_err(c, CS_E_ARG, "null population or parameters");
+    int r = check_params(c, params);
+    if (r) return r;
+    if (pop->num_place_types != params->NumPlaceTypes) return set_err(c, CS_E_ARG, "place type count mismatch");
+    c->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    c->grid = nsm * 8;
+    c->hp = *params;
+    DevPop& d = c->d;
+    d.N = pop->n_people; d.NH = pop->n_households; d.NC = pop->n_cells; d.NM = pop->n_mcells; d.NPT = pop->num_place_types;
+    size_t N = d.N, NH = d.NH, NC = d.NC, NM = d.NM, NPT = d.NPT;
+    if (N == 0 || NC == 0) return set_err(c, CS_E_ARG, "empty population");
+    // people
+    std::vector<PersonHot> hot(N);
+    for (size_t p = 0; p < N; p++) {
+        PersonHot h{};
+        h.hh = pop->person_hh[p];
+        h.mcell = pop->person_mcell[p];
+        h.age = pop->person_age[p];
+        h.pflags = pop->person_flags ? pop->person_flags[p] : 0;
+        h.absent_start = kNever;
+        h.isolation_start = kNever;
+        h.quar_start = kNever;
+        h.susc = 1.0f;
+        h.dflags = (uint8_t)(2u << CS_DF_QUAR_COMPLY_SHIFT);
+        hot[p] = h;
+    }
+#define UP(field, src, n) do { if ((r = dupload(c, &field, src, n))) return r; } while (0)
+#define AL(field, n) do { if ((r = dalloc(c, &field, n))) return r; } while (0)
+    {
+        PersonHot* ph;
+        UP(ph, hot.data(), N);
+        d.hot = ph;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    const int32_t* place_c; const uint16_t* group_c;
+    { int32_t* t; UP(t, pop->person_place, NPT * N); place_c = t; }
+    { uint16_t* t; UP(t, pop->person_group, NPT * N); group_c = t; }
+    d.place = place_c; d.group = group_c;
+    { int32_t* t; UP(t, pop->hh_first, NH); d.hh_first = t; }
+    { uint16_t* t; UP(t, pop->hh_nh, NH); d.hh_nh = t; }
+    { uint16_t* t; UP(t, pop->hh_nhr, NH); d.hh_nhr = t; }
+    { float* t; UP(t, pop->hh_x, NH); d.hh_x = t; }
+    { float* t; UP(t, pop->hh_y, NH); d.hh_y = t; }
+    { int32_t* t; UP(t, pop->mcell_cell, NM); d.mcell_cell = t; }
+    { int32_t* t; UP(t, pop->mcell_adunit, NM); d.mcell_adunit = t; }
+    { int32_t* t; UP(t, pop->cell_grid, NC); d.cell_grid = t; }
+    { int32_t* t; UP(t, pop->cell_start, NC + 1); d.cell_start = t; }
+    { int32_t* t; UP(t, pop->cell_members, N); d.cell_members = t; }
+    size_t ksz = (size_t)params->kernel_size + 1;
+    { double* t; UP(t, pop->kernel_lookup, ksz); d.klookup = t; }
+    { double* t; UP(t, pop->kernel_hi_res, ksz); d.khires = t; }
+    for (size_t pt = 0; pt < NPT; pt++) {
+        DevPlaces& pl = d.pl[pt];
+        pl.n = pop->n_places[pt];
+        size_t np = pl.n;
+        size_t nm = pop->place_member_ofs[pt][np], ng = pop->place_group_ofs[pt][np];
+        { int32_t* t; UP(t, pop->place_mcell[pt], np); pl.mcell = t; }
+        { int32_t* t; UP(t, pop->place_member_ofs[pt], np + 1); pl.member_ofs = t; }
+        { int32_t* t; UP(t, pop->place_members[pt], nm); pl.members = t; }
+        { int32_t* t; UP(t, pop->place_group_ofs[pt], np + 1); pl.group_ofs = t; }
+        { int32_t* t; UP(t, pop->group_start[pt], ng); pl.group_start = t; }
+        { int32_t* t; UP(t, pop->group_size[pt], ng); pl.group_size = t; }
+        AL(pl.close_start, np); AL(pl.close_end, np); AL(pl.prob_close, np);
+    }
+    AL(d.infection_time, N); AL(d.recovery_time, N); AL(d.sari_time, N); AL(d.critical_time, N);
+    AL(d.stepdown_time, N); AL(d.detected_time, N); AL(d.prob_absent, N); AL(d.prob_care, N);
+    AL(d.infector, N); AL(d.listpos, N); AL(d.infect_type, N); AL(d.pstep, N);
+    AL(d.S, NC); AL(d.L, NC); AL(d.I, NC); AL(d.R, NC); AL(d.D, NC); AL(d.S0, NC);
+    AL(d.tot_prob, NC); AL(d.slots, N); AL(d.mark, N);
+    AL(d.socdist, NM); AL(d.moverest, NM);
+    CK(cudaMemsetAsync(d.socdist, 0, NM, c->stream));
+    CK(cudaMemsetAsync(d.moverest, 0, NM, c->stream));
+    // proposal blocks
+    int bs = params->block_cells;
+    if (bs <= 0) {
+        bs = 1;
+        while (((params->ncw + bs - 1) / bs) * ((params->nch + bs - 1) / bs) > 4096) bs++;
+    }
+    d.bs = bs;
+    d.nbx = (params->ncw + bs - 1) / bs;
+    d.nby = (params->nch + bs - 1) / bs;
+    d.NB = d.nbx * d.nby;
+    {
+        std::vector<int32_t> cb(NC), ofs(d.NB + 1, 0), cells(NC), fill(d.NB, 0);
+        for (size_t m = 0; m < NC; m++) {
+            int g = pop->cell_grid[m], x = g / params->nch, y = g % params->nch;
+            cb[m] = (x / bs) * d.nby + (y / bs);
+            ofs[cb[m] + 1]++;
+        }
+        for (int b = 0; b < d.NB; b++) ofs[b + 1] += ofs[b];
+        for (size_t m = 0; m < NC; m++) cells[ofs[cb[m]] + fill[cb[m]]++] = (int32_t)m;
+        { int32_t* t; UP(t, cb.data(), NC); d.cell_block = t; }
+        { int32_t* t; UP(t, ofs.data(), (size_t)d.NB + 1); d.block_cell_ofs = t; }
+        { int32_t* t; UP(t, cells.data(), NC); d.block_cells = t; }
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    AL(d.block_cum, NC); AL(d.block_S0, (size_t)d.NB); AL(d.block_row_cum, (size_t)d.NB * d.NB);
+    // scratch
+    AL(d.claim, N); AL(d.queue, N); AL(d.counts, kCntN); AL(d.touched, NC); AL(d.cell_flag, NC + 4);
+    AL(d.act_ofs, NC + 1); AL(d.act, N); AL(d.act_cell, N); AL(d.cnt, N > NC ? N : NC); AL(d.cnt_ofs, N + 1);
+    AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH); AL(d.scan_tmp, kScanBlocks);
+    CK(cudaMemsetAsync(d.claim, 0xff, sizeof(unsigned long long) * N, c->stream));
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
+    CK(cudaMemsetAsync(d.cell_flag, 0, NC + 4, c->stream));
+    CK(cudaMemsetAsync(d.hh_flag, 0, NH + 4, c->stream));
+    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * (N > NC ? N : NC), c->stream));
+    CK(cudaMemsetAsync(d.pstep, 0, N, c->stream));
+    { cs_params* t; UP(t, params, 1); c->dP = t; d.P = t; }
+    { DevIv iv{1e10, 0, 1e10, 0}; DevIv* t; UP(t, &iv, 1); c->dIv = t; d.iv = t; }
+    { cs_counters* t; AL(t, 1); c->dC = t; d.C = t; CK(cudaMemsetAsync(t, 0, sizeof(cs_counters), c->stream)); }
+#undef UP
+#undef AL
+    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+void cs_gpu_destroy(cs_gpu_ctx* c)
+{
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->d_seed_list) cudaFree(c->d_seed_list);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
+{
+    if (!c || !params) return CS_E_ARG;
+    int r = check_params(c, params);
+    if (r) return r;
+    if (params->kernel_size != c->hp.kernel_size || params->NumPlaceTypes != c->hp.NumPlaceTypes || params->ncw != c->hp.ncw ||
+        params->nch != c->hp.nch)
+        return set_err(c, CS_E_ARG, "set_params may not change the kernel table, grid or place types");
+    c->hp = *params;
+    CK(cudaMemcpyAsync(c->dP, params, sizeof(cs_params), cudaMemcpyHostToDevice, c->stream));
+    return CS_OK;
+}
+
+static int rebuild_blocks(cs_gpu_ctx* c)
+{
+    DevPop& d = c->d;
+    LAUNCH(k_block_S0, (d.NB + kThreads - 1) / kThreads, kThreads, d);
+    LAUNCH(k_block_rows, (d.NB * 32 + kThreads - 1) / kThreads, kThreads, d);
+    return CS_OK;
+}
+
+int cs_gpu_update_probs(cs_gpu_ctx* c, int do_place)
+{
+    if (!c) return CS_E_ARG;
+    DevPop& d = c->d;
+    LAUNCH(k_update_S0, (d.NC + kThreads - 1) / kThreads, kThreads, d, do_place);
+    LAUNCH(k_tot_prob, (d.NC * 32 + kThreads - 1) / kThreads, kThreads, d);
+    return rebuild_blocks(c);
+}
+
+static int apply_queue(cs_gpu_ctx* c, double t, int ts)
+{
+    DevPop& d = c->d;
+    LAUNCH(k_apply_infections, c->grid, kThreads, d, t, ts, c->seed);
+    LAUNCH(k_partition_S, c->grid, kThreads, d);
+    CK(cudaMemsetAsync(d.counts + kCntQueue, 0, sizeof(int32_t) * 2, c->stream));  // queue + touched
+    return CS_OK;
+}
+
+int cs_gpu_seed_infections(cs_gpu_ctx* c, double t, const int32_t* people, int n)
+{
+    if (!c) return CS_E_ARG;
+    if (!c->run_started) return set_err(c, CS_E_STATE, "seed_infections before begin_run");
+    if (n <= 0) return CS_OK;
+    if (n > c->seed_cap) {
+        if (c->d_seed_list) cudaFree(c->d_seed_list);
+        c->d_seed_list = nullptr;
+        CK(cudaMalloc(&c->d_seed_list, sizeof(int32_t) * n));
+        c->seed_cap = n;
+    }
+    CK(cudaMemcpyAsync(c->d_seed_list, people, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
+    int ts = (int)(uint16_t)(c->hp.TimeStepsPerDay * t);
+    LAUNCH(k_seed_claims, (n + kThreads - 1) / kThreads, kThreads, c->d, c->d_seed_list, n);
+    return apply_queue(c, t, ts);
+}
+
+int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, int n_seed, int update_probs)
+{
+    if (!c) return CS_E_ARG;
+    (void)update_probs;  // a fresh run has S0 = n and tot_prob = 1 exactly
+    DevPop& d = c->d;
+    c->seed = seed;
+    CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
+    LAUNCH(k_reset_people, c->grid, kThreads, d, seed);
+    LAUNCH(k_reset_slots, c->grid, kThreads, d);
+    LAUNCH(k_reset_listpos, (d.NC + kThreads - 1) / kThreads, kThreads, d);
+    for (int pt = 0; pt < d.NPT; pt++) LAUNCH(k_reset_places, c->grid, kThreads, d, pt, seed);
+    CK(cudaMemsetAsync(d.socdist, 0, d.NM, c->stream));
+    CK(cudaMemsetAsync(d.moverest, 0, d.NM, c->stream));
+    {
+        DevIv iv{1e10, 0, 1e10, 0};
+        CK(cudaMemcpyAsync(c->dIv, &iv, sizeof(iv), cudaMemcpyHostToDevice, c->stream));
+    }
+    int r = rebuild_blocks(c);
+    if (r) return r;
+    c->run_started = true;
+    return cs_gpu_seed_infections(c, 0.0, seed_people, n_seed);
+}
+
+static StepScalars step_scalars(const cs_params& P, double t)
+{
+    StepScalars st;
+    st.t = t;
+    st.ts = (int)(uint16_t)(P.TimeStepsPerDay * t);
+    st.fp = P.ModelTimeStep / (1 - P.FalsePositiveRate);
+    st.seas = P.Seasonality;
+    st.sp_beta = P.DoSpatial ? st.seas * st.fp * P.LocalBeta : 0.0;
+    st.hh_beta = P.DoHouseholds ? st.seas * st.fp * P.HouseholdTrans : 0.0;
+    return st;
+}
+
+static int gather_active(cs_gpu_ctx* c, int mode)
+{
+    DevPop& d = c->d;
+    LAUNCH(k_active_counts, (d.NC + kThreads - 1) / kThreads, kThreads, d, mode);
+    int r = scan_excl(c, d.cnt, d.act_ofs, d.NC, nullptr, d.counts + kCntAct);
+    if (r) return r;
+    LAUNCH(k_gather_active, (d.NC + kThreads - 1) / kThreads, kThreads, d, mode);
+    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
+    return CS_OK;
+}
+
+int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
+{
+    (void)run;
+    if (!c) return CS_E_ARG;
+    if (!c->run_started) return set_err(c, CS_E_STATE, "infect_sweep before begin_run");
+    DevPop& d = c->d;
+    StepScalars st = step_scalars(c->hp, t);
+    int r = gather_active(c, 0);
+    if (r) return r;
+    LAUNCH(k_infectors, c->grid, kThreads, d, st, c->seed);
+    r = scan_excl(c, d.cnt, d.cnt_ofs, 0, d.counts + kCntAct, d.counts + kCntContacts);
+    if (r) return r;
+    LAUNCH(k_spatial, c->grid, kThreads, d, st, c->seed);
+    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * (d.N > d.NC ? d.N : d.NC), c->stream));
+    return apply_queue(c, t, st.ts);
+}
+
+int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* c, double t)
+{
+    if (!c) return CS_E_ARG;
+    if (!c->run_started) return set_err(c, CS_E_STATE, "incub_recovery_sweep before begin_run");
+    DevPop& d = c->d;
+    int ts = (int)(uint16_t)(c->hp.TimeStepsPerDay * t);
+    int r = gather_active(c, 1);
+    if (r) return r;
+    LAUNCH(k_incub_events, c->grid, kThreads, d, t, ts, c->seed);
+    LAUNCH(k_partition_LI, c->grid, kThreads, d);
+    LAUNCH(k_clear_pstep, c->grid, kThreads, d);
+    LAUNCH(k_household_after, c->grid, kThreads, d, ts, c->seed);
+    CK(cudaMemsetAsync(d.counts + kCntTouched, 0, sizeof(int32_t) * 2, c->stream));  // touched + households
+    return CS_OK;
+}
+
+int cs_gpu_step(cs_gpu_ctx* c, double t, int run)
+{
+    int r = cs_gpu_infect_sweep(c, t, run);
+    if (r) return r;
+    return cs_gpu_incub_recovery_sweep(c, t);
+}
+
+int cs_gpu_set_interventions(cs_gpu_ctx* c, const cs_interventions* iv)
+{
+    if (!c || !iv) return CS_E_ARG;
+    DevIv div{iv->CaseIsolationTimeStart, iv->CaseIsolationPolicyDuration, iv->HQuarantineTimeStart, iv->HQuarantinePolicyDuration};
+    CK(cudaMemcpyAsync(c->dIv, &div, sizeof(div), cudaMemcpyHostToDevice, c->stream));
+    if (iv->mcell_socdist) CK(cudaMemcpyAsync(c->d.socdist, iv->mcell_socdist, c->d.NM, cudaMemcpyHostToDevice, c->stream));
+    if (iv->mcell_moverest) CK(cudaMemcpyAsync(c->d.moverest, iv->mcell_moverest, c->d.NM, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+int cs_gpu_close_places(cs_gpu_ctx* c, int pt, const int32_t* mcells, int n_mcells, uint16_t start, uint16_t stop)
+{
+    if (!c) return CS_E_ARG;
+    if (pt < 0 || pt >= c->d.NPT) return set_err(c, CS_E_ARG, "bad place type %d", pt);
+    uint8_t* sel = nullptr;
+    if (mcells) {
+        std::vector<uint8_t> h(c->d.NM, 0);
+        for (int k = 0; k < n_mcells; k++) if (mcells[k] >= 0 && mcells[k] < c->d.NM) h[mcells[k]] = 1;
+        CK(cudaMalloc(&sel, c->d.NM));
+        CK(cudaMemcpyAsync(sel, h.data(), c->d.NM, cudaMemcpyHostToDevice, c->stream));
+    }
+    LAUNCH(k_close_places, c->grid, kThreads, c->d, pt, sel, start, stop);
+    if (sel) {
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFree(sel);
+    }
+    return CS_OK;
+}
+
+int cs_gpu_sync(cs_gpu_ctx* c)
+{
+    if (!c) return CS_E_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+int cs_gpu_get_counters(cs_gpu_ctx* c, cs_counters* out)
+{
+    if (!c || !out) return CS_E_ARG;
+    DevPop& d = c->d;
+    CK(cudaMemsetAsync(d.C, 0, 5 * sizeof(int64_t), c->stream));  // S..D recomputed below
+    LAUNCH(k_cell_totals, 64, kThreads, d);
+    CK(cudaMemcpyAsync(out, d.C, sizeof(cs_counters), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (out->err_queue_overflow || out->err_spatial_tries || out->err_kernel_range)
+        return set_err(c, CS_E_OVERFLOW, "bounded device loop gave up (spatial %lld, queue %lld, kernel range %lld)",
+                       (long long)out->err_spatial_tries, (long long)out->err_queue_overflow, (long long)out->err_kernel_range);
+    return CS_OK;
+}
+
+int cs_gpu_get_cell_counts(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D)
+{
+    if (!c) return CS_E_ARG;
+    size_t n = sizeof(int32_t) * c->d.NC;
+    if (S) CK(cudaMemcpyAsync(S, c->d.S, n, cudaMemcpyDeviceToHost, c->stream));
+    if (L) CK(cudaMemcpyAsync(L, c->d.L, n, cudaMemcpyDeviceToHost, c->stream));
+    if (I) CK(cudaMemcpyAsync(I, c->d.I, n, cudaMemcpyDeviceToHost, c->stream));
+    if (R) CK(cudaMemcpyAsync(R, c->d.R, n, cudaMemcpyDeviceToHost, c->stream));
+    if (D) CK(cudaMemcpyAsync(D, c->d.D, n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+// ------------------------------------------------------- state transfer
+__global__ void k_unpack_hot(DevPop d, int8_t* inf, uint8_t* sev, uint8_t* fl, uint16_t* lt, uint16_t* as, uint16_t* ae,
+                             uint16_t* iso, uint16_t* qs, float* infn, float* susc)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.N; p += gridDim.x * blockDim.x) {
+        PersonHot h = d.hot[p];
+        if (inf) inf[p] = h.inf;
+        if (sev) sev[p] = h.sev;
+        if (fl) fl[p] = h.dflags;
+        if (lt) lt[p] = h.latent_time;
+        if (as) as[p] = h.absent_start;
+        if (ae) ae[p] = h.absent_stop;
+        if (iso) iso[p] = h.isolation_start;
+        if (qs) qs[p] = h.quar_start;
+        if (infn) infn[p] = h.infness;
+        if (susc) susc[p] = h.susc;
+    }
+}
+
+__global__ void k_pack_hot(DevPop d, const int8_t* inf, const uint8_t* sev, const uint8_t* fl, const uint16_t* lt,
+                           const uint16_t* as, const uint16_t* ae, const uint16_t* iso, const uint16_t* qs,
+                           const float* infn, const float* susc)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.N; p += gridDim.x * blockDim.x) {
+        PersonHot h = d.hot[p];
+        h.inf = inf[p]; h.sev = sev[p]; h.dflags = fl[p]; h.latent_time = lt[p]; h.absent_start = as[p];
+        h.absent_stop = ae[p]; h.isolation_start = iso[p]; h.quar_start = qs[p]; h.infness = infn[p]; h.susc = susc[p];
+        d.hot[p] = h;
+    }
+}
+
+int cs_gpu_download_state(cs_gpu_ctx* c, const cs_state_view* v)
+{
+    if (!c || !v) return CS_E_ARG;
+    DevPop& d = c->d;
+    size_t N = d.N, NC = d.NC;
+    // person record fields go through a staging buffer (10 fields)
+    std::vector<void*> tmp;
+    auto stage = [&](size_t bytes) -> void* { void* p = nullptr; if (cudaMalloc(&p, bytes) == cudaSuccess) tmp.push_back(p); return p; };
+    int8_t* dinf = v->inf ? (int8_t*)stage(N) : nullptr;
+    uint8_t* dsev = v->severity ? (uint8_t*)stage(N) : nullptr;
+    uint8_t* dfl = v->flags ? (uint8_t*)stage(N) : nullptr;
+    uint16_t* dlt = v->latent_time ? (uint16_t*)stage(2 * N) : nullptr;
+    uint16_t* das = v->absent_start_time ? (uint16_t*)stage(2 * N) : nullptr;
+    uint16_t* dae = v->absent_stop_time ? (uint16_t*)stage(2 * N) : nullptr;
+    uint16_t* diso = v->isolation_start_time ? (uint16_t*)stage(2 * N) : nullptr;
+    uint16_t* dqs = v->quar_start_time ? (uint16_t*)stage(2 * N) : nullptr;
+    float* dinfn = v->infectiousness ? (float*)stage(4 * N) : nullptr;
+    float* dsusc = v->susc ? (float*)stage(4 * N) : nullptr;
+    k_unpack_hot<<<c->grid, kThreads, 0, c->stream>>>(d, dinf, dsev, dfl, dlt, das, dae, diso, dqs, dinfn, dsusc);
+    c->launches++;
+    int rc = CS_OK;
+#define DL(dst, src, bytes) do { if (v->dst && src) { cudaError_t e_ = cudaMemcpyAsync(v->dst, src, bytes, cudaMemcpyDeviceToHost, c->stream); if (e_ != cudaSuccess) rc = set_err(c, CS_E_CUDA, "download: %s", cudaGetErrorString(e_)); } } while (0)
+    DL(inf, dinf, N); DL(severity, dsev, N); DL(flags, dfl, N); DL(latent_time, dlt, 2 * N);
+    DL(absent_start_time, das, 2 * N); DL(absent_stop_time, dae, 2 * N); DL(isolation_start_time, diso, 2 * N);
+    DL(quar_start_time, dqs, 2 * N); DL(infectiousness, dinfn, 4 * N); DL(susc, dsusc, 4 * N);
+    DL(infection_time, d.infection_time, 2 * N); DL(recovery_or_death_time, d.recovery_time, 2 * N);
+    DL(SARI_time, d.sari_time, 2 * N); DL(Critical_time, d.critical_time, 2 * N); DL(Stepdown_time, d.stepdown_time, 2 * N);
+    DL(detected_time, d.detected_time, 2 * N); DL(ProbAbsent, d.prob_absent, 4 * N); DL(ProbCare, d.prob_care, 4 * N);
+    DL(infector, d.infector, 4 * N); DL(infect_type, d.infect_type, 2 * N); DL(listpos, d.listpos, 4 * N);
+    DL(cell_S, d.S, 4 * NC); DL(cell_L, d.L, 4 * NC); DL(cell_I, d.I, 4 * NC); DL(cell_R, d.R, 4 * NC);
+    DL(cell_D, d.D, 4 * NC); DL(cell_S0, d.S0, 4 * NC); DL(cell_tot_prob, d.tot_prob, 8 * NC); DL(cell_slots, d.slots, 4 * N);
+#undef DL
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    for (void* p : tmp) cudaFree(p);
+    if (e != cudaSuccess) return set_err(c, CS_E_CUDA, "download sync: %s", cudaGetErrorString(e));
+    return rc;
+}
+
+int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
+{
+    if (!c || !v) return CS_E_ARG;
+    DevPop& d = c->d;
+    size_t N = d.N, NC = d.NC;
+    if (!v->inf || !v->severity || !v->flags || !v->latent_time || !v->absent_start_time || !v->absent_stop_time ||
+        !v->isolation_start_time || !v->quar_start_time || !v->infectiousness || !v->susc || !v->infection_time ||
+        !v->recovery_or_death_time || !v->SARI_time || !v->Critical_time || !v->Stepdown_time || !v->detected_time ||
+        !v->ProbAbsent || !v->ProbCare || !v->infector || !v->infect_type || !v->listpos || !v->cell_S || !v->cell_L ||
+        !v->cell_I || !v->cell_R || !v->cell_D || !v->cell_S0 || !v->cell_tot_prob || !v->cell_slots)
+        return set_err(c, CS_E_ARG, "upload_state needs every field of the view");
+    std::vector<void*> tmp;
+    auto stage = [&](const void* src, size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        tmp.push_back(p);
+        cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
+        return p;
+    };
+    int8_t* dinf = (int8_t*)stage(v->inf, N);
+    uint8_t* dsev = (uint8_t*)stage(v->severity, N);
+    uint8_t* dfl = (uint8_t*)stage(v->flags, N);
+    uint16_t* dlt = (uint16_t*)stage(v->latent_time, 2 * N);
+    uint16_t* das = (uint16_t*)stage(v->absent_start_time, 2 * N);
+    uint16_t* dae = (uint16_t*)stage(v->absent_stop_time, 2 * N);
+    uint16_t* diso = (uint16_t*)stage(v->isolation_start_time, 2 * N);
+    uint16_t* dqs = (uint16_t*)stage(v->quar_start_time, 2 * N);
+    float* dinfn = (float*)stage(v->infectiousness, 4 * N);
+    float* dsusc = (float*)stage(v->susc, 4 * N);
+    if (tmp.size() != 10) { for (void* p : tmp) cudaFree(p); return set_err(c, CS_E_CUDA, "upload staging failed"); }
+    k_pack_hot<<<c->grid, kThreads, 0, c->stream>>>(d, dinf, dsev, dfl, dlt, das, dae, diso, dqs, dinfn, dsusc);
+    c->launches++;
+#define UL(src, dst, bytes) CK(cudaMemcpyAsync(dst, v->src, bytes, cudaMemcpyHostToDevice, c->stream))
+    UL(infection_time, d.infection_time, 2 * N); UL(recovery_or_death_time, d.recovery_time, 2 * N);
+    UL(SARI_time, d.sari_time, 2 * N); UL(Critical_time, d.critical_time, 2 * N); UL(Stepdown_time, d.stepdown_time, 2 * N);
+    UL(detected_time, d.detected_time, 2 * N); UL(ProbAbsent, d.prob_absent, 4 * N); UL(ProbCare, d.prob_care, 4 * N);
+    UL(infector, d.infector, 4 * N); UL(infect_type, d.infect_type, 2 * N); UL(listpos, d.listpos, 4 * N);
+    UL(cell_S, d.S, 4 * NC); UL(cell_L, d.L, 4 * NC); UL(cell_I, d.I, 4 * NC); UL(cell_R, d.R, 4 * NC);
+    UL(cell_D, d.D, 4 * NC); UL(cell_S0, d.S0, 4 * NC); UL(cell_tot_prob, d.tot_prob, 8 * NC); UL(cell_slots, d.slots, 4 * N);
+#undef UL
+    CK(cudaMemsetAsync(d.mark, 0, N, c->stream));
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
+    CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
+    c->seed = seed;
+    int r = rebuild_blocks(c);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    for (void* p : tmp) cudaFree(p);
+    if (r) return r;
+    if (e != cudaSuccess) return set_err(c, CS_E_CUDA, "upload sync: %s", cudaGetErrorString(e));
+    c->run_started = true;
+    return CS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,405 @@
+/*
+ * covidsim_b200.h -- C ABI of the B200 (sm_100a) per-timestep sweep of CovidSim.
+ *
+ * The reference model runs one timestep as (src/CovidSim.cpp:1488-1490):
+ *     InfectSweep(t, run);            // src/Sweep.cpp:283-881
+ *     IncubRecoverySweep(t);          // src/Sweep.cpp:883-979
+ * with UpdateProbs(0) (src/CovidSim.cpp:2752-2802) re-normalising the spatial
+ * sampler whenever the susceptible fraction has fallen by 0.2 (:1515-1521).
+ * This header declares drop-in replacements for those three calls that run on one
+ * GPU, plus the set-up, state transfer and counter entry points a host needs around
+ * them.  Everything here is plain C: pointers, sizes and fixed-width integers.
+ *
+ * Ownership: the host owns every array passed in; the context copies what it needs
+ * to device memory during the call and keeps no host pointer afterwards.  The
+ * context owns the device copies and is authoritative for dynamic per-person state
+ * between cs_gpu_begin_run / cs_gpu_upload_state and cs_gpu_download_state.
+ *
+ * Errors: every function returning int returns CS_OK (0) or a negative CS_E* code;
+ * cs_gpu_last_error() then holds a one-line message.  The reference aborts through
+ * ERR_CRITICAL (src/Error.cpp:13); a host that wants that behaviour maps a non-zero
+ * status to its own fatal error.  No device code traps: bounded loops count their
+ * give-ups in cs_counters.err_* and the next call reports them.
+ *
+ * Threading: one host thread per context; calls on a context are serialised on
+ * the context's own CUDA stream and are not re-entrant.
+ */
+#ifndef COVIDSIM_B200_H
+#define COVIDSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CS_ABI_VERSION 1
+
+/* Sizes fixed by the reference (src/Constants.h, src/Country.h). */
+#define CS_MAX_PLACE_TYPES 5        /* MAX_NUM_PLACE_TYPES   (Country.h:15)   */
+#define CS_NUM_AGE_GROUPS 17        /* NUM_AGE_GROUPS        (Constants.h:77) */
+#define CS_AGE_GROUP_WIDTH 5        /* AGE_GROUP_WIDTH       (Constants.h:78) */
+#define CS_CDF_RES 20               /* CDF_RES               (Constants.h:75) */
+#define CS_MAX_INFECTIOUS_STEPS 2550 /* MAX_INFECTIOUS_STEPS (Constants.h:86) */
+#define CS_INFECT_TYPE_MASK 16      /* INFECT_TYPE_MASK      (Constants.h:80) */
+#define CS_MAX_HOUSEHOLD_SIZE 10    /* MAX_HOUSEHOLD_SIZE    (Country.h:5)    */
+#define CS_NUM_SETTINGS (CS_MAX_PLACE_TYPES + 2) /* place types, House, Spatial (Constants.h:117-118) */
+#define CS_NUM_NPI 6                /* CaseIsolation..DigContactTracing (Constants.h:121-126) */
+#define CS_SETTING_HOUSE CS_MAX_PLACE_TYPES
+#define CS_SETTING_SPATIAL (CS_MAX_PLACE_TYPES + 1)
+#define CS_NPI_CASE_ISOLATION 0
+#define CS_NPI_HOME_QUARANTINE 1
+#define CS_NPI_PLACE_CLOSURE 2
+#define CS_NPI_SOCIAL_DISTANCING 3
+#define CS_NPI_ENHANCED_SOCIAL_DISTANCING 4
+#define CS_NPI_DIG_CONTACT_TRACING 5
+#define CS_MAX_ADUNITS 128          /* counters kept per admin unit on the device */
+#define CS_USHRT_MAX_M1 65534u      /* USHRT_MAX - 1: the reference's "never" time */
+
+/* Status codes. */
+#define CS_OK 0
+#define CS_E_ARG (-1)          /* bad argument or inconsistent sizes            */
+#define CS_E_CUDA (-2)         /* a CUDA runtime call failed                     */
+#define CS_E_UNSUPPORTED (-3)  /* parameter combination outside this sweep       */
+#define CS_E_OVERFLOW (-4)     /* a device queue or bounded loop gave up         */
+#define CS_E_STATE (-5)        /* call order violated (e.g. sweep before run)    */
+#define CS_E_RANGE (-6)        /* kernel distance beyond the lookup table        */
+
+/* Infection states: numeric values of InfStat (src/InfStat.h:12-44). */
+#define CS_INF_SUSCEPTIBLE 0
+#define CS_INF_LATENT 1
+#define CS_INF_INFECTIOUS_ALMOST_SYMPTOMATIC (-1)
+#define CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE 2
+#define CS_INF_CASE (-2)
+#define CS_INF_RECOVERED_FROM_ASYMP 3
+#define CS_INF_RECOVERED_FROM_SYMP (-3)
+#define CS_INF_IMMUNE_AT_START 4
+#define CS_INF_DEAD_WAS_ASYMP 5
+#define CS_INF_DEAD_WAS_SYMP (-5)
+
+/* Severity classes: order of Severity (src/InfStat.h:47-58). */
+#define CS_SEV_ASYMPTOMATIC 0
+#define CS_SEV_MILD 1
+#define CS_SEV_ILI 2
+#define CS_SEV_SARI 3
+#define CS_SEV_CRITICAL 4
+#define CS_SEV_STEPDOWN 5
+#define CS_SEV_DEAD 6
+#define CS_SEV_RECOVERED 7
+
+/*
+ * Random streams.  Every draw comes from Philox4x32-10 (Salmon, Moraes, Dror, Shaw,
+ * "Parallel random numbers: as easy as 1, 2, 3", SC'11) keyed by the run seed
+ * (key = {seed & 0xffffffff, seed >> 32}) with counter
+ *     {block, entity, timestep | purpose << 16, sub}
+ * where entity is a person, place or cell index and sub separates several streams of
+ * one entity in one step (contact number, place type).  Each block yields two
+ * doubles in [0,1) from the 53 high bits of (x1:x0) and (x3:x2).  Results therefore
+ * depend on (seed, step, entity, purpose) only, never on launch geometry or thread
+ * count -- unlike the reference's per-thread streams (src/Rand.cpp:28-46).
+ */
+#define CS_RNG_HOUSEHOLD 1        /* entity infector                      */
+#define CS_RNG_PLACE_GROUP 2      /* entity infector, sub place type      */
+#define CS_RNG_PLACE_BETWEEN 3    /* entity infector, sub place type      */
+#define CS_RNG_SPATIAL_COUNT 4    /* entity infector                      */
+#define CS_RNG_SPATIAL_CONTACT 5  /* entity infector, sub contact number  */
+#define CS_RNG_LATENT 6           /* entity infectee                      */
+#define CS_RNG_INCUB 7            /* entity person                        */
+#define CS_RNG_CASE 8             /* entity person                        */
+#define CS_RNG_DETECTED 9         /* entity person                        */
+#define CS_RNG_HQ 10              /* entity household                     */
+#define CS_RNG_RUN_INIT 11        /* entity person, timestep 0            */
+#define CS_RNG_PLACE_INIT 12      /* entity place, sub place type         */
+
+/* Static per-person flag bits (cs_population.person_flags). */
+#define CS_PF_CARE_HOME_RESIDENT 0x01u
+#define CS_PF_ESOCDIST_COMPLY 0x02u
+#define CS_PF_KEYWORKER 0x04u
+
+/* Dynamic per-person flag bits (cs_person_state.flags). */
+#define CS_DF_TO_DIE 0x01u
+#define CS_DF_DETECTED 0x02u
+#define CS_DF_QUAR_COMPLY_SHIFT 2   /* 2 bits: HostsQuarantine[].comply 0/1/2 */
+#define CS_DF_QUAR_COMPLY_MASK 0x0Cu
+
+/* Microcell intervention status: TreatStat (src/Models/Microcell.h:6-17). */
+#define CS_TREAT_UNTREATED 0
+#define CS_TREAT_TO_BE_TREATED 1
+#define CS_TREAT_TREATED 2
+#define CS_TREAT_DONT_TREAT_AGAIN 3
+
+/*
+ * Inverse CDF table: the reference's InverseCdf after assign_exponent(), i.e. the
+ * values exp(-x_i) that InverseCdf::choose (src/InverseCdf.cpp:60-74) interpolates.
+ */
+typedef struct cs_icdf {
+    double v[CS_CDF_RES + 1];
+} cs_icdf;
+
+/*
+ * Every scalar and table the two sweeps read from the reference's global Param P
+ * (src/Param.h).  Field names follow the reference's.  Only the intervention
+ * settings the sweep itself consumes are here; trigger logic stays on the host and
+ * reaches the device through cs_gpu_set_interventions / cs_gpu_close_places.
+ */
+typedef struct cs_params {
+    /* time */
+    double TimeStepsPerDay;            /* P.TimeStepsPerDay                     */
+    double ModelTimeStep;              /* P.ModelTimeStep                       */
+    /* switches */
+    int32_t DoHouseholds, DoPlaces, DoSpatial, DoSymptoms, DoSeverity, DoLatent;
+    int32_t DoInfectiousnessProfile, NoInfectiousnessSDinHH, DoUTM_coords, DoPeriodicBoundaries;
+    int32_t DoRealSymptWithdrawal, DoDeathCountsInS0;  /* the latter is P.DoDeath (UpdateProbs) */
+    int32_t NumPlaceTypes, HotelPlaceType, CareHomePlaceType, PlaceTypeNoAirNum;
+    int32_t IncludeStepDownToDeath, CaseAbsentChildAgeCutoff, DoHQretrigger, _pad0;
+    /* transmission */
+    double LocalBeta, HouseholdTrans, FalsePositiveRate, Seasonality;
+    double HouseholdDenomLookup[CS_MAX_HOUSEHOLD_SIZE];
+    double infectiousness[CS_MAX_INFECTIOUS_STEPS];     /* P.infectiousness[] */
+    double PlaceTypeTrans[CS_MAX_PLACE_TYPES];
+    double PlaceTypeGroupSizeParam1[CS_MAX_PLACE_TYPES];
+    double PlaceTypePropBetweenGroupLinks[CS_MAX_PLACE_TYPES];
+    double SymptPlaceTypeContactRate[CS_MAX_PLACE_TYPES];
+    double SymptPlaceTypeWithdrawalProp[CS_MAX_PLACE_TYPES];
+    double SymptSpatialContactRate;
+    double RelativeSpatialContact[CS_NUM_AGE_GROUPS];
+    double RelativeSpatialContactSusc[CS_NUM_AGE_GROUPS];
+    double AgeSusceptibility[CS_NUM_AGE_GROUPS];
+    double AgeInfectiousness[CS_NUM_AGE_GROUPS];
+    double WAIFW_Matrix[CS_NUM_AGE_GROUPS][CS_NUM_AGE_GROUPS];
+    double WAIFW_Matrix_SpatialOnly[CS_NUM_AGE_GROUPS][CS_NUM_AGE_GROUPS];
+    double CareHomeResidentHouseholdScaling, CareHomeResidentSpatialScaling;
+    double CareHomeWorkerGroupScaling, CareHomeResidentPlaceScaling, CareHomeRelProbHosp;
+    double Efficacies[CS_NUM_NPI][CS_NUM_SETTINGS];    /* P.Efficacies[npi][setting] */
+    double MoveRestrEffect;
+    /* natural history */
+    double LatentPeriod, InfectiousPeriod, LatentToSymptDelay;
+    double SymptInfectiousness, AsymptInfectiousness, InfectiousnessSD;
+    double ProportionSymptomatic[CS_NUM_AGE_GROUPS];
+    cs_icdf latent_icdf, infectious_icdf;
+    cs_icdf MildToRecovery_icdf, ILIToRecovery_icdf, SARIToRecovery_icdf;
+    cs_icdf CriticalToCritRecov_icdf, CritRecovToRecov_icdf, ILIToSARI_icdf;
+    cs_icdf SARIToCritical_icdf, ILIToDeath_icdf, SARIToDeath_icdf;
+    cs_icdf StepdownToDeath_icdf, CriticalToDeath_icdf;
+    double Mean_MildToRecovery[CS_NUM_AGE_GROUPS], Mean_ILIToRecovery[CS_NUM_AGE_GROUPS];
+    double Mean_SARIToRecovery[CS_NUM_AGE_GROUPS], Mean_CriticalToCritRecov[CS_NUM_AGE_GROUPS];
+    double Mean_CritRecovToRecov[CS_NUM_AGE_GROUPS], Mean_StepdownToDeath[CS_NUM_AGE_GROUPS];
+    double Mean_ILIToSARI[CS_NUM_AGE_GROUPS], Mean_SARIToCritical[CS_NUM_AGE_GROUPS];
+    double Mean_CriticalToDeath[CS_NUM_AGE_GROUPS], Mean_SARIToDeath[CS_NUM_AGE_GROUPS];
+    double Mean_ILIToDeath[CS_NUM_AGE_GROUPS];
+    double Prop_ILI_ByAge[CS_NUM_AGE_GROUPS], Prop_SARI_ByAge[CS_NUM_AGE_GROUPS];
+    double Prop_Critical_ByAge[CS_NUM_AGE_GROUPS];
+    double CFR_SARI_ByAge[CS_NUM_AGE_GROUPS], CFR_Critical_ByAge[CS_NUM_AGE_GROUPS];
+    double CFR_ILI_ByAge[CS_NUM_AGE_GROUPS];
+    double CFR_Critical_Scale_Current, CFR_SARI_Scale_Current, CFR_ILI_Scale_Current;
+    double ControlPropCasesId;
+    /* interventions consumed inside the sweep (DoCase/DoDetectedCase) */
+    double CaseIsolationProp, HQuarantinePropHouseCompliant, HQuarantinePropIndivCompliant;
+    double HQuarantineDelay, CaseAbsentChildPropAdultCarers;
+    uint16_t usCaseIsolationDelay, usCaseIsolationDuration, usCaseAbsenteeismDelay;
+    uint16_t usCaseAbsenteeismDuration, usHQuarantineHouseDuration, _pad1[3];
+    /* geometry: degrees relative to the bounding box's bottom-left corner */
+    int32_t ncw, nch;                  /* cells wide / high                    */
+    double cell_width, cell_height;    /* P.in_cells_ (degrees)                */
+    double width_deg, height_deg;      /* P.in_degrees_                         */
+    double bbox_bottom_left_y;         /* P.SpatialBoundingBox.bottom_left().y */
+    double sinx[361], cosx[361], asin2sqx[1001];  /* P.sinx/cosx/asin2sqx    */
+    /* spatial kernel lookup (KernelLookup, src/Kernels.h:66-119) */
+    int32_t kernel_size, kernel_expansion; /* size_, expansion_factor_          */
+    double kernel_delta;               /* delta_                                */
+    /* sampler blocking: cells per side of a proposal block (0 = choose) */
+    int32_t block_cells, _pad2;
+} cs_params;
+
+/*
+ * Static population structure.  Arrays are host pointers read during
+ * cs_gpu_create only.  Index spaces follow the reference: people are numbered as
+ * Hosts[] (contiguous by household, src/SetupModel.cpp:1224-1253); cells are the
+ * populated cells in CellLookup order; microcells are the populated microcells.
+ */
+typedef struct cs_population {
+    int32_t n_people, n_households, n_cells, n_mcells;
+    int32_t num_place_types, n_adunits;
+    int32_t n_places[CS_MAX_PLACE_TYPES];
+    /* people */
+    const int32_t* person_hh;          /* Person::hh                            */
+    const int32_t* person_mcell;       /* index into the mcell_* arrays         */
+    const uint8_t* person_age;         /* Person::age (years)                   */
+    const uint8_t* person_flags;       /* CS_PF_* bits                          */
+    const int32_t* person_place;       /* [num_place_types][n_people] PlaceLinks */
+    const uint16_t* person_group;      /* [num_place_types][n_people] PlaceGroupLinks */
+    /* households */
+    const int32_t* hh_first;           /* Household::FirstPerson                */
+    const uint16_t* hh_nh;             /* Household::nh                         */
+    const uint16_t* hh_nhr;            /* Household::nhr                        */
+    const float* hh_x;                 /* Household::loc.x                      */
+    const float* hh_y;                 /* Household::loc.y                      */
+    /* microcells */
+    const int32_t* mcell_cell;         /* populated-cell index of the microcell */
+    const int32_t* mcell_adunit;       /* Microcell::adunit                     */
+    /* populated cells */
+    const int32_t* cell_grid;          /* grid index x*nch+y (Cells - CellLookup[i]) */
+    const int32_t* cell_start;         /* [n_cells+1] offsets into cell_members */
+    const int32_t* cell_members;       /* [n_people] Cell::members, cell by cell */
+    /* places of type t: CSR member lists and groups */
+    const int32_t* place_mcell[CS_MAX_PLACE_TYPES];
+    const float* place_x[CS_MAX_PLACE_TYPES];
+    const float* place_y[CS_MAX_PLACE_TYPES];
+    const int32_t* place_member_ofs[CS_MAX_PLACE_TYPES]; /* [n_places+1]             */
+    const int32_t* place_members[CS_MAX_PLACE_TYPES];    /* Place::members            */
+    const int32_t* place_group_ofs[CS_MAX_PLACE_TYPES];  /* [n_places+1] into groups  */
+    const int32_t* group_start[CS_MAX_PLACE_TYPES];      /* Place::group_start        */
+    const int32_t* group_size[CS_MAX_PLACE_TYPES];       /* Place::group_size         */
+    /* spatial kernel table (double[kernel_size+1] each) */
+    const double* kernel_lookup;
+    const double* kernel_hi_res;
+} cs_population;
+
+/*
+ * Dynamic per-person and per-cell state, for cs_gpu_upload_state /
+ * cs_gpu_download_state.  All arrays have n_people (or n_cells) elements; any
+ * pointer may be NULL on download to skip that field.
+ */
+typedef struct cs_state_view {
+    int8_t* inf;                       /* InfStat value                         */
+    uint8_t* severity;                 /* Severity_Current | Severity_Final<<4  */
+    uint8_t* flags;                    /* CS_DF_* bits                          */
+    uint16_t* infection_time;
+    uint16_t* latent_time;
+    uint16_t* recovery_or_death_time;
+    uint16_t* SARI_time;
+    uint16_t* Critical_time;
+    uint16_t* Stepdown_time;
+    uint16_t* absent_start_time;
+    uint16_t* absent_stop_time;
+    uint16_t* isolation_start_time;
+    uint16_t* quar_start_time;         /* HostsQuarantine[].start_time          */
+    uint16_t* detected_time;
+    float* infectiousness;
+    float* susc;
+    float* ProbAbsent;
+    float* ProbCare;
+    int32_t* infector;
+    int16_t* infect_type;
+    int32_t* listpos;
+    /* cells */
+    int32_t* cell_S;
+    int32_t* cell_L;
+    int32_t* cell_I;
+    int32_t* cell_R;
+    int32_t* cell_D;
+    int32_t* cell_S0;
+    double* cell_tot_prob;
+    int32_t* cell_slots;               /* [n_people] Cell::susceptible lists     */
+} cs_state_view;
+
+/* Intervention state the host's trigger logic hands to the sweep. */
+typedef struct cs_interventions {
+    /* windows in days, as AdUnits[].X TimeStart and P.X PolicyDuration */
+    double CaseIsolationTimeStart, CaseIsolationPolicyDuration;
+    double HQuarantineTimeStart, HQuarantinePolicyDuration;
+    /* microcell status arrays (n_mcells) or NULL to leave unchanged */
+    const uint8_t* mcell_socdist;      /* Microcell::socdist (TreatStat)        */
+    const uint8_t* mcell_moverest;     /* Microcell::moverest (TreatStat)       */
+} cs_interventions;
+
+/* Counters: the StateT[] fields RecordSample reduces (src/Model.h:68-122). */
+typedef struct cs_counters {
+    int64_t S, L, I, R, D;
+    int64_t cumI, cumC, cumDC, cumFC, cumR, cumD;
+    int64_t cumTG, cumSI, nTG, cumHQ, cumAC, cumAA, cumACS;
+    int64_t cumItype[CS_INFECT_TYPE_MASK];
+    int64_t cumIa[CS_NUM_AGE_GROUPS], cumCa[CS_NUM_AGE_GROUPS], cumDa[CS_NUM_AGE_GROUPS];
+    int64_t Mild, ILI, SARI, Critical, CritRecov;
+    int64_t cumMild, cumILI, cumSARI, cumCritical, cumCritRecov;
+    int64_t cumDeath_ILI, cumDeath_SARI, cumDeath_Critical;
+    int64_t cumI_keyworker[2], cumC_keyworker[2];
+    int64_t cumI_adunit[CS_MAX_ADUNITS], cumC_adunit[CS_MAX_ADUNITS], cumD_adunit[CS_MAX_ADUNITS];
+    int64_t cumDC_adunit[CS_MAX_ADUNITS], cumCritical_adunit[CS_MAX_ADUNITS];
+    int64_t Critical_adunit[CS_MAX_ADUNITS];
+    /* work done by the sweeps (for the HBM roofline) */
+    int64_t work_infectors, work_hh_members, work_place_candidates;
+    int64_t work_spatial_contacts, work_spatial_draws, work_new_infections;
+    int64_t work_transitions, work_cells_touched;
+    /* give-ups of bounded device loops; non-zero means the results are suspect */
+    int64_t err_spatial_tries, err_queue_overflow, err_kernel_range;
+} cs_counters;
+
+typedef struct cs_gpu_ctx cs_gpu_ctx;
+
+/* Library identification; lets a binding check it loaded the header it expects. */
+int cs_abi_version(void);
+size_t cs_sizeof_params(void);
+size_t cs_sizeof_population(void);
+size_t cs_sizeof_counters(void);
+
+/*
+ * Build the spatial kernel lookup tables exactly as KernelLookup::setup/init
+ * (src/Kernels.cpp:8-46) with norm 1: lookup[i] = K(i*delta), hi_res[i] =
+ * K(i*delta/expansion), delta = longest_d2/size.  kernel_type follows
+ * src/Kernels.cpp:25-40 (1 exponential ... 7 power_exp).  Host-only, no GPU.
+ */
+int cs_build_kernel_table(int kernel_type, double scale, double shape, double p3, double p4,
+                          double longest_d2, int size, int expansion,
+                          double* lookup_out, double* hi_res_out, double* delta_out);
+
+/* Host-side evaluation of KernelLookup::num (src/Kernels.cpp:108-129). */
+double cs_kernel_num(const double* lookup, const double* hi_res, int size, int expansion,
+                     double delta, double r2);
+
+/* Create a context on CUDA device `device`: uploads population and parameters. */
+int cs_gpu_create(const cs_population* pop, const cs_params* params, int device, cs_gpu_ctx** out);
+void cs_gpu_destroy(cs_gpu_ctx* ctx);
+const char* cs_gpu_last_error(const cs_gpu_ctx* ctx);
+
+/* Replace the parameter block (e.g. a new R0 or CFR scale) between steps. */
+int cs_gpu_set_params(cs_gpu_ctx* ctx, const cs_params* params);
+
+/*
+ * Start a realisation: the per-person and per-cell resets of InitModel
+ * (src/CovidSim.cpp:1006-1127, no initial immunity), UpdateProbs(0) when
+ * `update_probs` is set, then DoInfect (src/Update.cpp:100-195) at t = 0 on the
+ * n_seed people in `seed_people` (the host's SeedInfection choices,
+ * src/CovidSim.cpp:1244-1374).  `seed` keys every random stream of the run.
+ */
+int cs_gpu_begin_run(cs_gpu_ctx* ctx, uint64_t seed, const int32_t* seed_people, int n_seed,
+                     int update_probs);
+
+/* Load dynamic state prepared by a host (the reference's own InitModel). */
+int cs_gpu_upload_state(cs_gpu_ctx* ctx, uint64_t seed, const cs_state_view* state);
+int cs_gpu_download_state(cs_gpu_ctx* ctx, const cs_state_view* state);
+
+/* Infect people chosen by the host at time t (importation, SeedInfection). */
+int cs_gpu_seed_infections(cs_gpu_ctx* ctx, double t, const int32_t* people, int n);
+
+/* Drop-in for InfectSweep(t, run)       (src/Sweep.cpp:283-881).  */
+int cs_gpu_infect_sweep(cs_gpu_ctx* ctx, double t, int run);
+/* Drop-in for IncubRecoverySweep(t)     (src/Sweep.cpp:883-979), holidays excluded. */
+int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* ctx, double t);
+/* Drop-in for UpdateProbs(do_place)     (src/CovidSim.cpp:2752-2802). */
+int cs_gpu_update_probs(cs_gpu_ctx* ctx, int do_place);
+/* One full model timestep: the two sweeps back to back. */
+int cs_gpu_step(cs_gpu_ctx* ctx, double t, int run);
+
+int cs_gpu_set_interventions(cs_gpu_ctx* ctx, const cs_interventions* iv);
+/* DoPlaceClose (src/Update.cpp:1095-1258) for every place of type t in the listed
+ * microcells (all when mcells == NULL), closing [start, stop) in timesteps. */
+int cs_gpu_close_places(cs_gpu_ctx* ctx, int place_type, const int32_t* mcells, int n_mcells,
+                        uint16_t start, uint16_t stop);
+
+/* Copy the device counter block (cumulative since the run began). */
+int cs_gpu_get_counters(cs_gpu_ctx* ctx, cs_counters* out);
+/* Per-cell S, L, I, R, D (each n_cells) for RecordSample (src/CovidSim.cpp:3044-3056). */
+int cs_gpu_get_cell_counts(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D);
+/* Wait for the context's stream; returns a deferred device error if any. */
+int cs_gpu_sync(cs_gpu_ctx* ctx);
+/* The CUDA stream the context launches on (a cudaStream_t), for host-side timing. */
+void* cs_gpu_stream(cs_gpu_ctx* ctx);
+/* Number of kernels launched on the context since creation. */
+int64_t cs_gpu_launch_count(const cs_gpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COVIDSIM_B200_H */

@@ -1,0 +1,84 @@
+"""GPU sweep against the CPU oracle, state for state: every per-person field, every
+cell list and every counter must be identical after each step."""
+import numpy as np
+import pytest
+
+from covidsim_b200 import abi, sim
+import oracle_py
+from tests.helpers import tiny_world, snapshot, check_lists, STATE_FIELDS
+
+pytestmark = pytest.mark.gpu
+
+SKIP_COUNTERS = set()
+
+
+def _pair(world):
+    pop, P, lk, hr = world
+    g = sim.Simulation(pop, P, lk, hr)
+    o = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+    return pop, P, g, o
+
+
+def _compare(pop, g, o, where):
+    a, b = snapshot(g.backend, pop), snapshot(o.backend, pop)
+    for k in STATE_FIELDS:
+        if not np.array_equal(a[k], b[k]):
+            bad = np.nonzero(a[k] != b[k])[0]
+            raise AssertionError("%s: field %s differs at %d entries, first %s: gpu %s oracle %s"
+                                 % (where, k, len(bad), bad[:5], a[k][bad[:5]], b[k][bad[:5]]))
+    ca, cb = abi.counters_to_dict(g.backend.counters()), abi.counters_to_dict(o.backend.counters())
+    for k in ca:
+        if k not in SKIP_COUNTERS:
+            assert ca[k] == cb[k], "%s: counter %s gpu %s oracle %s" % (where, k, ca[k], cb[k])
+    return a
+
+
+def _run_pair(world, seed, steps, n_seed=20, check_every=1, policy_day=None, update_every=None):
+    pop, P, g, o = _pair(world)
+    seeds = g.choose_seeds(seed, n_seed)
+    g.backend.begin_run(seed, seeds)
+    o.backend.begin_run(seed, seeds)
+    _compare(pop, g, o, "after seeding")
+    for k in range(steps):
+        t = k * P.ModelTimeStep
+        if policy_day is not None and k == int(policy_day * 4):
+            for s in (g, o):
+                s._switch_interventions(t, sim.InterventionPolicy(duration=20.0), True,
+                                        np.zeros(pop.n_mcells, dtype=np.uint8))
+        if update_every and k and k % update_every == 0:
+            g.backend.update_probs(0)
+            o.backend.update_probs(0)
+        g.backend.infect_sweep(t, 0)
+        o.backend.infect_sweep(t, 0)
+        if k % check_every == 0:
+            _compare(pop, g, o, "step %d infect" % k)
+        g.backend.incub_recovery_sweep(t)
+        o.backend.incub_recovery_sweep(t)
+        if k % check_every == 0:
+            snap = _compare(pop, g, o, "step %d incub" % k)
+    snap = _compare(pop, g, o, "end")
+    check_lists(snap, pop)
+    c = g.backend.counters()
+    g.close()
+    o.close()
+    return c
+
+
+def test_parity_no_interventions():
+    c = _run_pair(tiny_world(), seed=101, steps=240, check_every=4)
+    assert c.cumI > 500
+
+
+def test_parity_with_update_probs():
+    c = _run_pair(tiny_world(), seed=202, steps=200, check_every=10, update_every=60)
+    assert c.cumI > 500
+
+
+def test_parity_with_interventions():
+    c = _run_pair(tiny_world(), seed=303, steps=200, check_every=10, policy_day=20)
+    assert c.cumI > 200 and c.cumHQ > 0
+
+
+def test_parity_planar_coordinates():
+    c = _run_pair(tiny_world(utm=0), seed=404, steps=160, check_every=10)
+    assert c.cumI > 100
