@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 sweep: person-steps/s of whole CovidSim realisations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): 10,000,000 synthetic people on a 2 x 2 degree region of 600 x 600
+cells (10 x 10 microcells each, lognormal density), household / age / four place
+types from the generator, power-law spatial kernel, R0 = 2.4, 100 seed infections,
+365 days at 0.25-day steps, with the global ICU-trigger interventions (case
+isolation 0.7, household quarantine 0.5, school/university closure, social
+distancing) switched on for 90 days.  One "step" of this benchmark is one whole
+realisation (1460 model timesteps, InfectSweep + IncubRecoverySweep each); K timed
+realisations run after W untimed ones, each with its own seed.
+
+value = people x timesteps x realisations (all ranks) / device time (max over
+ranks), timed with CUDA events on the sweep's own stream.  The population (0.7 GB
+of structure plus dynamic state) is far larger than L2, so no flush is needed.
+e2e repeats the realisations through the C ABI from host buffers: the initial state
+is copied host -> device, the daily counters and the final per-person state
+device -> host inside the timed region.  Multi-GPU (torchrun) runs independent
+realisations per rank (replicas, weak scaling): only the barrier and the max of the
+timings cross ranks.
+
+--impl reference times the reference's own CPU sweep (oracle/_ref/CovidSim_timed,
+built from the reference sources by oracle/Makefile) on this host's cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (preset, days, interventions, description)
+    "c1": ("c1", 365, True, "10M people, 600x600 cells, interventions, 365 d"),
+    "c0": ("c0", 120, False, "1M people, 240x240 cells, no interventions, 120 d"),
+}
+METRIC = "person-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-out", default=None, help="write per-kernel times to this JSON file")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        self.f.close()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for name, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+        except OSError:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ roofline
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def kernel_bytes(name, w, n_cells_steps):
+    """Algorithmic bytes a kernel moved over the timed region, from the work counters
+    (per-unit costs: transition scan 16 B per latent/infectious person, infector
+    record 40 B, household member 12 B, place candidate 20 B, spatial draw 33 B,
+    accepted infection 24 B, per-cell counts 24 B)."""
+    if name == "k_infectors":
+        return 40 * w["work_infectors"] + 12 * w["work_hh_members"] + 20 * w["work_place_candidates"]
+    if name == "k_spatial":
+        return 33 * w["work_spatial_draws"]
+    if name in ("k_apply_infections", "k_partition_S"):
+        return 12 * w["work_new_infections"]
+    if name == "k_incub_events":
+        return 16 * w["work_incub_people"]
+    if name in ("k_partition_LI", "k_clear_pstep"):
+        return 8 * w["work_transitions"]
+    if name == "k_gather_active":
+        return 12 * (w["work_infectors"] + w["work_incub_people"]) + 16 * n_cells_steps
+    if name in ("k_active_counts", "k_scan_reduce", "k_scan_down"):
+        return 8 * n_cells_steps
+    return None
+
+
+def load_traffic():
+    """dram bytes per launch from the committed ncu summary, when present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return {}
+
+
+# --------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    else:
+        torch.cuda.set_device(local)
+    from covidsim_b200 import population, params as prm, sim
+
+    preset, days, with_iv, desc = WORKLOADS[args.workload]
+    pop = population.preset(preset)
+    P, lk, hr = prm.build_params(pop.grid)
+    beta, r0parts = sim.calibrate_local_beta(pop, P, 2.4)
+    P.LocalBeta = beta
+    s = sim.Simulation(pop, P, lk, hr, device=local)
+    be = s.backend
+    policy = sim.InterventionPolicy() if with_iv else None
+    steps_per_run = int(days * P.TimeStepsPerDay)
+    base_seed = 17389101 + 7919 * rank
+
+    for w in range(args.warmup):
+        s.run(seed=base_seed + 1000 + w, days=days, policy=policy)
+    be.sync()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    stream = torch.cuda.ExternalStream(be.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    work = None
+    finals = []
+    barrier()
+    launches0 = be.launches()
+    be.profile(2)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for k in range(args.steps):
+            ser = s.run(seed=base_seed + k, days=days, policy=policy)
+            c = sim.abi.counters_to_dict(be.counters())
+            work = c if work is None else {kk: (work[kk] + c[kk]) if not isinstance(c[kk], list) else work[kk]
+                                           for kk in c}
+            finals.append((int(ser["cumI"][-1]), int(ser["D"][-1]), int(ser["I"].argmax())))
+        ev1.record(stream)
+        be.sync()
+        torch.cuda.synchronize()
+    barrier()
+    launches = be.launches() - launches0
+    kernels = be.profile_entries()
+    be.profile(0)
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    person_steps = pop.n_people * steps_per_run * args.steps * world
+    value = person_steps / (ms / 1e3)
+    runs_per_hour = args.steps * world / (ms / 1e3) * 3600.0
+
+    # roofline of the dominant kernel
+    peak, peak_kind = peaks()
+    traffic = load_traffic()
+    n_cells_steps = pop.n_cells * steps_per_run * args.steps
+    rows = []
+    for name, (kms, n) in sorted(kernels.items(), key=lambda kv: -kv[1][0]):
+        b = kernel_bytes(name, work, n_cells_steps)
+        rows.append(dict(kernel=name, ms=kms, launches=n, share=kms / sum(v[0] for v in kernels.values()),
+                         bytes=b, gbs=(b / (kms / 1e3) / 1e9) if b else None))
+    dom = rows[0]
+    dom_traffic = traffic.get(dom["kernel"], {}).get("dram_bytes_per_launch")
+    roofline = {
+        "bound": "hbm", "kernel": dom["kernel"], "achieved": round(dom["gbs"], 2) if dom["gbs"] else None,
+        "peak": peak, "unit": "GB/s", "frac": round(dom["gbs"] / peak, 4) if dom["gbs"] else None,
+        "traffic": dom_traffic, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+        "algorithmic_bytes_per_launch": round(dom["bytes"] / dom["launches"]) if dom["bytes"] else None,
+        "avg_launch_us": round(dom["ms"] / dom["launches"] * 1e3, 3),
+        "share_of_kernel_time": round(dom["share"], 4),
+    }
+    if args.profile_out and rank == 0:
+        json.dump(dict(rows=rows, work=work, timed_ms=ms, steps=args.steps, workload=args.workload),
+                  open(args.profile_out, "w"), indent=1)
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        arrs, view = sim.state_arrays(pop.n_people, pop.n_cells)
+        be.begin_run(base_seed, s.choose_seeds(base_seed, 100))
+        be.download(view)          # the prepared start state, now in host memory
+        cudart = torch.cuda.cudart()
+        for a in arrs.values():
+            cudart.cudaHostRegister(a.ctypes.data, a.nbytes, 0)
+        state_bytes = sum(a.nbytes for a in arrs.values())
+        barrier()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            s.run(seed=base_seed + k, days=days, policy=policy, initial_state=view)
+            be.download(view)
+        be.sync()
+        barrier()
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        for a in arrs.values():
+            cudart.cudaHostUnregister(a.ctypes.data)
+        import ctypes
+        e2e = {"value": round(person_steps / dt, 1), "unit": METRIC, "h2d_bytes_per_step": state_bytes,
+               "d2h_bytes_per_step": state_bytes + days * ctypes.sizeof(sim.abi.cs_counters),
+               "what": "upload prepared start state, run, daily counters, download final state"}
+
+    # CPU baseline: the oracle port on a bounded sample of the same workload
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(s, pop, P, lk, hr, days)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    clocks = clk.summary()
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (f64 probabilities, f32 person state)",
+        "data": "synthetic (seeded generator, reference parameter set)",
+        "config": {"workload": desc, "people": pop.n_people, "cells": pop.n_cells, "timesteps_per_step": steps_per_run,
+                   "realisations_per_rank": args.steps, "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (%.0f MB resident)" % (pop.nbytes() / 1e6),
+                   "local_beta": round(beta, 6), "r0_parts": {k: round(float(v), 4) for k, v in r0parts.items()}},
+        "runs_per_hour": round(runs_per_hour, 1),
+        "outcomes": [{"cumI": a, "deaths": b, "peak_day": c} for a, b, c in finals],
+        "clocks": clocks, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+        "gpu_launches": int(launches),
+        "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in rows[:8]],
+    }
+
+
+def cpu_baseline_port(s, pop, P, lk, hr, days, budget_s=20.0):
+    """The CPU oracle (a single-threaded C restatement of the sweep) timed on a
+    bounded sample: a few timesteps around the epidemic peak of the same
+    population, interventions off, started from the GPU's state at that day."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    from covidsim_b200 import sim
+    seed = 4242
+    be = s.backend
+    be.begin_run(seed, s.choose_seeds(seed, 100))
+    # advance on the GPU to the peak region of an intervention-free epidemic
+    peak_day = None
+    I_prev = -1
+    for step in range(int(days * 4)):
+        be.step(step * P.ModelTimeStep, 0)
+        if step % 4 == 3:
+            c = be.counters()
+            if c.I < I_prev and c.I > 0.02 * pop.n_people:
+                peak_day = (step + 1) // 4
+                break
+            I_prev = c.I
+    start_step = step + 1
+    arrs, view = sim.state_arrays(pop.n_people, pop.n_cells)
+    be.download(view)
+    o = oracle_py.OracleBackend(s._pop_c, P)
+    o.upload(seed, view)
+    n = 0
+    t0 = time.perf_counter()
+    while n < 40:
+        o.step((start_step + n) * P.ModelTimeStep, 0)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": round(pop.n_people * n / dt, 1), "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": "%d timesteps from day %s (epidemic peak, no interventions) of the same population, "
+                      "oracle/cs_oracle.c single-threaded" % (n, peak_day)}
+
+
+# ---------------------------------------------------------------- reference
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    res = refrun.time_reference(args.workload, steps=args.steps, warmup=args.warmup)
+    if "unavailable" in res:
+        return {"impl": "reference", "unavailable": res["unavailable"]}
+    preset, days, with_iv, desc = WORKLOADS[args.workload]
+    v = res["value"]
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "reference_sample": res["sample"]},
+        "cpu_baseline": {"value": round(v, 1), "unit": METRIC, "cores": res["cores"], "kind": "reference",
+                         "sample": res["sample"]},
+        "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -110,11 +110,12 @@ class CovidSimError(RuntimeError):
 
 
 def load_library(path=LIB_PATH):
-    """Load the sm_100a library (building it first if it is missing)."""
+    """Load the sm_100a library, (re)building it first when it is missing or older
+    than its sources."""
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(path):
+    if path == LIB_PATH:
         import importlib.util
         spec = importlib.util.spec_from_file_location("_cs_build", os.path.join(PKG_ROOT, "build.py"))
         mod = importlib.util.module_from_spec(spec)
@@ -148,6 +149,8 @@ def load_library(path=LIB_PATH):
         "cs_gpu_sync": (I, [V]),
         "cs_gpu_stream": (V, [V]),
         "cs_gpu_launch_count": (C.c_int64, [V]),
+        "cs_gpu_profile": (I, [V, I]),
+        "cs_gpu_profile_entry": (I, [V, I, C.c_char_p, I, P(D), P(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

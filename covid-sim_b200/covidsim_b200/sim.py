@@ -101,6 +101,23 @@ class GpuBackend:
     def launches(self):
         return self.lib.cs_gpu_launch_count(self.ctx)
 
+    def upload(self, seed, view):
+        self._ck(self.lib.cs_gpu_upload_state(self.ctx, seed, C.byref(view)), "upload_state")
+
+    def profile(self, enable):
+        self._ck(self.lib.cs_gpu_profile(self.ctx, enable), "profile")
+
+    def profile_entries(self):
+        """{kernel name: (total ms, launches)} recorded since profiling was enabled."""
+        out = {}
+        buf = C.create_string_buffer(128)
+        ms, n = C.c_double(), C.c_int64()
+        i = 0
+        while self.lib.cs_gpu_profile_entry(self.ctx, i, buf, 128, C.byref(ms), C.byref(n)) == 0:
+            out[buf.value.decode()] = (ms.value, n.value)
+            i += 1
+        return out
+
 
 def state_arrays(n_people, n_cells):
     """Host arrays for every field of cs_state_view, and the view over them."""
@@ -224,11 +241,18 @@ class Simulation:
         rng = np.random.default_rng(seed ^ 0x5EED)
         return rng.choice(self.pop.n_people, size=n_seed, replace=False).astype(np.int32)
 
-    def run(self, seed, days, n_seed=100, policy=None, sample_every_day=True, callback=None):
-        """One realisation; returns daily time series of the main counters."""
+    def run(self, seed, days, n_seed=100, policy=None, sample_every_day=True, callback=None, initial_state=None):
+        """One realisation; returns daily time series of the main counters.
+
+        initial_state: a cs_state_view of host arrays holding a prepared start
+        (InitModel + SeedInfection already applied); it is copied to the device
+        instead of resetting and seeding there."""
         be = self.backend
         P = self.params
-        be.begin_run(seed, self.choose_seeds(seed, n_seed))
+        if initial_state is not None:
+            be.upload(seed, initial_state)
+        else:
+            be.begin_run(seed, self.choose_seeds(seed, n_seed))
         spd = int(round(P.TimeStepsPerDay))
         nsteps = int(days * spd)
         prev_prop_s = 1.0

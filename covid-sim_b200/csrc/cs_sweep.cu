@@ -72,7 +72,6 @@ __device__ __forceinline__ bool flag_household(const DevPop& d, int h, uint8_t f
     return true;
 }
 
-static int g_grid = 148 * 8;
 constexpr int kThreads = 256;
 
 // ----------------------------------------------------------------- scans
@@ -174,7 +173,45 @@ struct cs_gpu_ctx {
     uint64_t seed = 0;
     bool run_started = false;
     int grid = 148 * 8;
+    // optional per-launch timing with events on the context's stream
+    bool prof = false;
+    struct Rec { const char* name; cudaEvent_t a, b; };
+    std::vector<Rec> ring;
+    size_t ring_used = 0;
+    std::vector<const char*> prof_names;
+    std::vector<double> prof_ms;
+    std::vector<long long> prof_n;
 };
+
+static void prof_flush(cs_gpu_ctx* c)
+{
+    if (!c->ring_used) return;
+    cudaEventSynchronize(c->ring[c->ring_used - 1].b);
+    for (size_t i = 0; i < c->ring_used; i++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ring[i].a, c->ring[i].b);
+        size_t k = 0;
+        while (k < c->prof_names.size() && std::strcmp(c->prof_names[k], c->ring[i].name) != 0) k++;
+        if (k == c->prof_names.size()) { c->prof_names.push_back(c->ring[i].name); c->prof_ms.push_back(0); c->prof_n.push_back(0); }
+        c->prof_ms[k] += ms;
+        c->prof_n[k]++;
+    }
+    c->ring_used = 0;
+}
+
+static void prof_begin(cs_gpu_ctx* c, const char* name)
+{
+    if (c->ring_used == c->ring.size()) prof_flush(c);
+    cs_gpu_ctx::Rec& r = c->ring[c->ring_used];
+    r.name = name;
+    cudaEventRecord(r.a, c->stream);
+}
+
+static void prof_end(cs_gpu_ctx* c)
+{
+    cudaEventRecord(c->ring[c->ring_used].b, c->stream);
+    c->ring_used++;
+}
 
 static int set_err(cs_gpu_ctx* c, int code, const char* fmt, ...)
 {
@@ -195,7 +232,9 @@ static int set_err(cs_gpu_ctx* c, int code, const char* fmt, ...)
 
 #define LAUNCH(kernel, grid, block, ...)                                                           \
     do {                                                                                           \
+        if (c->prof) prof_begin(c, #kernel);                                                       \
         kernel<<<(grid), (block), 0, c->stream>>>(__VA_ARGS__);                                    \
+        if (c->prof) prof_end(c);                                                                  \
         c->launches++;                                                                             \
         cudaError_t e_ = cudaGetLastError();                                                       \
         if (e_ != cudaSuccess) return set_err(c, CS_E_CUDA, "launch %s: %s", #kernel, cudaGetErrorString(e_)); \
@@ -936,6 +975,7 @@ __global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d, double t, i
     const cs_params& P = *d.P;
     const DevIv iv = *d.iv;
     int nact = d.counts[kCntAct];
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_incub_people), nact);
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
         int p = d.act[idx], c = d.act_cell[idx];
         PersonHot h = d.hot[p];
@@ -1253,6 +1293,7 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
 {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& r : c->ring) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (void* p : c->allocs) cudaFree(p);
     if (c->d_seed_list) cudaFree(c->d_seed_list);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1429,6 +1470,33 @@ int cs_gpu_close_places(cs_gpu_ctx* c, int pt, const int32_t* mcells, int n_mcel
         CK(cudaStreamSynchronize(c->stream));
         cudaFree(sel);
     }
+    return CS_OK;
+}
+
+int cs_gpu_profile(cs_gpu_ctx* c, int enable)
+{
+    if (!c) return CS_E_ARG;
+    if (enable && c->ring.empty()) {
+        c->ring.resize(4096);
+        for (auto& r : c->ring) {
+            CK(cudaEventCreate(&r.a));
+            CK(cudaEventCreate(&r.b));
+        }
+    }
+    if (!enable) prof_flush(c);
+    c->prof = enable != 0;
+    if (enable == 2) { c->prof_names.clear(); c->prof_ms.clear(); c->prof_n.clear(); c->ring_used = 0; }
+    return CS_OK;
+}
+
+int cs_gpu_profile_entry(cs_gpu_ctx* c, int i, char* name, int cap, double* total_ms, int64_t* launches)
+{
+    if (!c) return CS_E_ARG;
+    prof_flush(c);
+    if (i < 0 || i >= (int)c->prof_names.size()) return CS_E_RANGE;
+    if (name && cap > 0) snprintf(name, cap, "%s", c->prof_names[i]);
+    if (total_ms) *total_ms = c->prof_ms[i];
+    if (launches) *launches = c->prof_n[i];
     return CS_OK;
 }
 

@@ -1,0 +1,403 @@
+// Drop-in replacement of the reference's two sweep entry points by the sm_100a
+// library, for linking into the reference executable.
+//
+// The reference's Sweep.cpp is compiled with InfectSweep/IncubRecoverySweep renamed
+// (-DInfectSweep=ref_InfectSweep -DIncubRecoverySweep=ref_IncubRecoverySweep) and
+// this file provides the original symbols (src/Sweep.h:7-8), called by RunModel at
+// src/CovidSim.cpp:1488 and 1490.  Everything else -- parameter files, population
+// set-up, InitModel/SeedInfection, RecordSample and the output files -- stays the
+// reference's own code.
+//
+//   first call           build cs_population / cs_params from the reference's
+//                        globals (Hosts, Households, Mcells, CellLookup, Places, P)
+//                        and create the device context;
+//   first call of a run  copy the host state InitModel + SeedInfection left behind
+//                        (people, cell lists, S0, tot_prob) to the device;
+//   every step           run the device sweeps, then copy back what RecordSample
+//                        reads: per-cell S/L/I/R/D and the StateT counters;
+//   UpdateProbs          noticed through a change of the host cells' S0, then
+//                        recomputed on the device from the device's own counts.
+//
+// Features outside the device sweep (digital contact tracing, airports, blanket
+// movement restrictions, treatment/vaccination, false positives, holidays, and the
+// host's own intervention triggers) stop the run with ERR_CRITICAL, the reference's
+// own failure convention, rather than silently computing something else.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "Constants.h"
+#include "Dist.h"
+#include "Error.h"
+#include "InfStat.h"
+#include "Model.h"
+#include "Param.h"
+#include "Sweep.h"
+
+#include "covidsim_b200.h"
+
+namespace {
+
+cs_gpu_ctx* g_ctx = nullptr;
+int g_run = -1;
+PopVar g_base;  // StateT[0] as InitModel + SeedInfection left it; device counters add to it
+long long g_s0_sig = -1;
+int64_t g_tg_base = 0, g_si_base = 0, g_ntg_base = 0, g_tg_set = 0, g_si_set = 0, g_ntg_set = 0;
+std::vector<int32_t> g_S, g_L, g_I, g_R, g_D;
+cs_params g_params;
+
+void check(int rc, const char* what)
+{
+    if (rc != CS_OK) ERR_CRITICAL_FMT("%s failed (%d): %s\n", what, rc, cs_gpu_last_error(g_ctx));
+}
+
+int8_t inf_of(const Person& a)
+{
+    if (a.is_susceptible()) return CS_INF_SUSCEPTIBLE;
+    if (a.is_latent()) return CS_INF_LATENT;
+    if (a.is_infectious_almost_symptomatic()) return CS_INF_INFECTIOUS_ALMOST_SYMPTOMATIC;
+    if (a.is_infectious_asymptomatic_not_case()) return CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE;
+    if (a.is_case()) return CS_INF_CASE;
+    if (a.is_recovered_symp()) return CS_INF_RECOVERED_FROM_SYMP;
+    if (a.is_recovered()) return CS_INF_RECOVERED_FROM_ASYMP;
+    if (a.is_immune_at_start()) return CS_INF_IMMUNE_AT_START;
+    if (a.is_dead_was_symp()) return CS_INF_DEAD_WAS_SYMP;
+    return CS_INF_DEAD_WAS_ASYMP;
+}
+
+void copy_icdf(cs_icdf& dst, InverseCdf& src)
+{
+    for (int i = 0; i <= CDF_RES; i++) dst.v[i] = src[i];
+}
+
+cs_params params_from_reference()
+{
+    cs_params p;
+    std::memset(&p, 0, sizeof(p));
+    p.TimeStepsPerDay = P.TimeStepsPerDay;
+    p.ModelTimeStep = P.ModelTimeStep;
+    p.DoHouseholds = P.DoHouseholds; p.DoPlaces = P.DoPlaces; p.DoSpatial = 1; p.DoSymptoms = P.DoSymptoms;
+    p.DoSeverity = P.DoSeverity; p.DoLatent = P.DoLatent; p.DoInfectiousnessProfile = P.DoInfectiousnessProfile;
+    p.NoInfectiousnessSDinHH = P.NoInfectiousnessSDinHH; p.DoUTM_coords = P.DoUTM_coords;
+    p.DoPeriodicBoundaries = P.DoPeriodicBoundaries; p.DoRealSymptWithdrawal = P.DoRealSymptWithdrawal;
+    p.DoDeathCountsInS0 = P.DoDeath;
+    p.NumPlaceTypes = P.NumPlaceTypes; p.HotelPlaceType = P.HotelPlaceType; p.CareHomePlaceType = P.CareHomePlaceType;
+    p.PlaceTypeNoAirNum = P.PlaceTypeNoAirNum; p.IncludeStepDownToDeath = P.IncludeStepDownToDeath;
+    p.CaseAbsentChildAgeCutoff = P.CaseAbsentChildAgeCutoff; p.DoHQretrigger = P.DoHQretrigger;
+    p.LocalBeta = P.LocalBeta; p.HouseholdTrans = P.HouseholdTrans; p.FalsePositiveRate = P.FalsePositiveRate;
+    p.Seasonality = 1.0;
+    for (int i = 0; i < MAX_HOUSEHOLD_SIZE; i++) p.HouseholdDenomLookup[i] = P.HouseholdDenomLookup[i];
+    for (int i = 0; i < MAX_INFECTIOUS_STEPS; i++) p.infectiousness[i] = P.infectiousness[i];
+    for (int t = 0; t < MAX_NUM_PLACE_TYPES; t++) {
+        p.PlaceTypeTrans[t] = P.PlaceTypeTrans[t];
+        p.PlaceTypeGroupSizeParam1[t] = (t < P.NumPlaceTypes) ? P.PlaceTypeGroupSizeParam1[t] : 1.0;
+        p.PlaceTypePropBetweenGroupLinks[t] = P.PlaceTypePropBetweenGroupLinks[t];
+        p.SymptPlaceTypeContactRate[t] = P.SymptPlaceTypeContactRate[t];
+        p.SymptPlaceTypeWithdrawalProp[t] = P.SymptPlaceTypeWithdrawalProp[t];
+    }
+    p.SymptSpatialContactRate = P.SymptSpatialContactRate;
+    for (int a = 0; a < NUM_AGE_GROUPS; a++) {
+        p.RelativeSpatialContact[a] = P.RelativeSpatialContact[a];
+        p.RelativeSpatialContactSusc[a] = P.RelativeSpatialContactSusc[a];
+        p.AgeSusceptibility[a] = P.AgeSusceptibility[a];
+        p.AgeInfectiousness[a] = P.AgeInfectiousness[a];
+        p.ProportionSymptomatic[a] = P.ProportionSymptomatic[a];
+        for (int b = 0; b < NUM_AGE_GROUPS; b++) {
+            p.WAIFW_Matrix[a][b] = P.WAIFW_Matrix[a][b];
+            p.WAIFW_Matrix_SpatialOnly[a][b] = P.WAIFW_Matrix_SpatialOnly[a][b];
+        }
+        p.Mean_MildToRecovery[a] = P.Mean_MildToRecovery[a]; p.Mean_ILIToRecovery[a] = P.Mean_ILIToRecovery[a];
+        p.Mean_SARIToRecovery[a] = P.Mean_SARIToRecovery[a]; p.Mean_CriticalToCritRecov[a] = P.Mean_CriticalToCritRecov[a];
+        p.Mean_CritRecovToRecov[a] = P.Mean_CritRecovToRecov[a]; p.Mean_StepdownToDeath[a] = P.Mean_StepdownToDeath[a];
+        p.Mean_ILIToSARI[a] = P.Mean_ILIToSARI[a]; p.Mean_SARIToCritical[a] = P.Mean_SARIToCritical[a];
+        p.Mean_CriticalToDeath[a] = P.Mean_CriticalToDeath[a]; p.Mean_SARIToDeath[a] = P.Mean_SARIToDeath[a];
+        p.Mean_ILIToDeath[a] = P.Mean_ILIToDeath[a];
+        p.Prop_ILI_ByAge[a] = P.Prop_ILI_ByAge[a]; p.Prop_SARI_ByAge[a] = P.Prop_SARI_ByAge[a];
+        p.Prop_Critical_ByAge[a] = P.Prop_Critical_ByAge[a];
+        p.CFR_SARI_ByAge[a] = P.CFR_SARI_ByAge[a]; p.CFR_Critical_ByAge[a] = P.CFR_Critical_ByAge[a];
+        p.CFR_ILI_ByAge[a] = P.CFR_ILI_ByAge[a];
+    }
+    p.CareHomeResidentHouseholdScaling = P.CareHomeResidentHouseholdScaling;
+    p.CareHomeResidentSpatialScaling = P.CareHomeResidentSpatialScaling;
+    p.CareHomeWorkerGroupScaling = P.CareHomeWorkerGroupScaling;
+    p.CareHomeResidentPlaceScaling = P.CareHomeResidentPlaceScaling;
+    p.CareHomeRelProbHosp = P.CareHomeRelProbHosp;
+    for (int i = 0; i < CS_NUM_NPI; i++)
+        for (int j = 0; j < CS_NUM_SETTINGS; j++) p.Efficacies[i][j] = P.Efficacies[i][j];
+    p.MoveRestrEffect = P.MoveRestrEffect;
+    p.LatentPeriod = P.LatentPeriod; p.InfectiousPeriod = P.InfectiousPeriod; p.LatentToSymptDelay = P.LatentToSymptDelay;
+    p.SymptInfectiousness = P.SymptInfectiousness; p.AsymptInfectiousness = P.AsymptInfectiousness;
+    p.InfectiousnessSD = P.InfectiousnessSD;
+    copy_icdf(p.latent_icdf, P.latent_icdf); copy_icdf(p.infectious_icdf, P.infectious_icdf);
+    copy_icdf(p.MildToRecovery_icdf, P.MildToRecovery_icdf); copy_icdf(p.ILIToRecovery_icdf, P.ILIToRecovery_icdf);
+    copy_icdf(p.SARIToRecovery_icdf, P.SARIToRecovery_icdf); copy_icdf(p.CriticalToCritRecov_icdf, P.CriticalToCritRecov_icdf);
+    copy_icdf(p.CritRecovToRecov_icdf, P.CritRecovToRecov_icdf); copy_icdf(p.ILIToSARI_icdf, P.ILIToSARI_icdf);
+    copy_icdf(p.SARIToCritical_icdf, P.SARIToCritical_icdf); copy_icdf(p.ILIToDeath_icdf, P.ILIToDeath_icdf);
+    copy_icdf(p.SARIToDeath_icdf, P.SARIToDeath_icdf); copy_icdf(p.StepdownToDeath_icdf, P.StepdownToDeath_icdf);
+    copy_icdf(p.CriticalToDeath_icdf, P.CriticalToDeath_icdf);
+    p.CFR_Critical_Scale_Current = P.CFR_Critical_Scale_Current; p.CFR_SARI_Scale_Current = P.CFR_SARI_Scale_Current;
+    p.CFR_ILI_Scale_Current = P.CFR_ILI_Scale_Current;
+    p.ControlPropCasesId = P.ControlPropCasesId;
+    p.CaseIsolationProp = P.CaseIsolationProp; p.HQuarantinePropHouseCompliant = P.HQuarantinePropHouseCompliant;
+    p.HQuarantinePropIndivCompliant = P.HQuarantinePropIndivCompliant; p.HQuarantineDelay = P.HQuarantineDelay;
+    p.CaseAbsentChildPropAdultCarers = P.CaseAbsentChildPropAdultCarers;
+    p.usCaseIsolationDelay = P.usCaseIsolationDelay; p.usCaseIsolationDuration = P.usCaseIsolationDuration;
+    p.usCaseAbsenteeismDelay = P.usCaseAbsenteeismDelay; p.usCaseAbsenteeismDuration = P.usCaseAbsenteeismDuration;
+    p.usHQuarantineHouseDuration = P.usHQuarantineHouseDuration;
+    p.ncw = P.ncw; p.nch = P.nch;
+    p.cell_width = P.in_cells_.width; p.cell_height = P.in_cells_.height;
+    p.width_deg = P.in_degrees_.width; p.height_deg = P.in_degrees_.height;
+    p.bbox_bottom_left_y = P.SpatialBoundingBox.bottom_left().y;
+    for (int i = 0; i <= DEGREES_PER_TURN; i++) { p.sinx[i] = P.sinx[i]; p.cosx[i] = P.cosx[i]; }
+    for (int i = 0; i <= 1000; i++) p.asin2sqx[i] = P.asin2sqx[i];
+    p.kernel_size = P.KernelLookup.size_;
+    p.kernel_expansion = P.KernelLookup.expansion_factor_;
+    p.block_cells = 0;
+    return p;
+}
+
+void unsupported_features()
+{
+    if (P.DoDigitalContactTracing) ERR_CRITICAL("GPU sweep: digital contact tracing is not supported\n");
+    if (P.DoAirports) ERR_CRITICAL("GPU sweep: airports / travel are not supported\n");
+    if (P.DoBlanketMoveRestr) ERR_CRITICAL("GPU sweep: blanket movement restrictions are not supported\n");
+    if (P.FalsePositiveRate > 0) ERR_CRITICAL("GPU sweep: false-positive cases are not supported\n");
+    if (P.DoHolidays && P.NumHolidays > 0) ERR_CRITICAL("GPU sweep: holidays are not supported\n");
+}
+
+void create_context()
+{
+    unsupported_features();
+    const int N = P.PopSize, NH = P.NumHouseholds, NC = P.NumPopulatedCells, NM = P.NumMicrocells, NPT = P.NumPlaceTypes;
+    static std::vector<int32_t> hh(N), mc(N), place((size_t)NPT * N), hh_first(NH), mcell_cell(NM, 0), mcell_ad(NM),
+        cell_grid(NC), cell_start(NC + 1), cell_members(N);
+    static std::vector<uint8_t> age(N), flags(N);
+    static std::vector<uint16_t> group((size_t)NPT * N), hh_nh(NH), hh_nhr(NH);
+    static std::vector<float> hx(NH), hy(NH);
+    for (int i = 0; i < N; i++) {
+        hh[i] = Hosts[i].hh;
+        mc[i] = Hosts[i].mcell;
+        age[i] = Hosts[i].age;
+        flags[i] = (Hosts[i].care_home_resident ? CS_PF_CARE_HOME_RESIDENT : 0) |
+                   (Hosts[i].esocdist_comply ? CS_PF_ESOCDIST_COMPLY : 0) | (Hosts[i].keyworker ? CS_PF_KEYWORKER : 0);
+        for (int t = 0; t < NPT; t++) {
+            place[(size_t)t * N + i] = Hosts[i].PlaceLinks[t];
+            group[(size_t)t * N + i] = Hosts[i].PlaceGroupLinks[t];
+        }
+    }
+    for (int h = 0; h < NH; h++) {
+        hh_first[h] = Households[h].FirstPerson;
+        hh_nh[h] = Households[h].nh;
+        hh_nhr[h] = Households[h].nhr;
+        hx[h] = Households[h].loc.x;
+        hy[h] = Households[h].loc.y;
+    }
+    cell_start[0] = 0;
+    for (int c = 0; c < NC; c++) {
+        Cell* ct = CellLookup[c];
+        cell_grid[c] = (int32_t)(ct - Cells);
+        for (int k = 0; k < ct->n; k++) cell_members[cell_start[c] + k] = ct->members[k];
+        cell_start[c + 1] = cell_start[c] + ct->n;
+    }
+    std::vector<int32_t> cell_index_of_grid(P.NumCells, -1);
+    for (int c = 0; c < NC; c++) cell_index_of_grid[cell_grid[c]] = c;
+    for (int m = 0; m < NM; m++) {
+        int x = m / P.total_microcells_high_, y = m % P.total_microcells_high_;
+        int grid = (x / P.NMCL) * P.nch + (y / P.NMCL);
+        mcell_cell[m] = cell_index_of_grid[grid] >= 0 ? cell_index_of_grid[grid] : 0;
+        mcell_ad[m] = Mcells[m].adunit;
+    }
+    static std::vector<int32_t> pl_mcell[MAX_NUM_PLACE_TYPES], pl_mofs[MAX_NUM_PLACE_TYPES], pl_members[MAX_NUM_PLACE_TYPES],
+        pl_gofs[MAX_NUM_PLACE_TYPES], pl_gstart[MAX_NUM_PLACE_TYPES], pl_gsize[MAX_NUM_PLACE_TYPES];
+    static std::vector<float> pl_x[MAX_NUM_PLACE_TYPES], pl_y[MAX_NUM_PLACE_TYPES];
+    cs_population pop;
+    std::memset(&pop, 0, sizeof(pop));
+    for (int t = 0; t < NPT; t++) {
+        int np = P.Nplace[t];
+        pl_mcell[t].resize(np); pl_x[t].resize(np); pl_y[t].resize(np);
+        pl_mofs[t].assign(np + 1, 0); pl_gofs[t].assign(np + 1, 0);
+        for (int l = 0; l < np; l++) {
+            Place& pp = Places[t][l];
+            pl_mcell[t][l] = pp.mcell;
+            pl_x[t][l] = pp.loc.x;
+            pl_y[t][l] = pp.loc.y;
+            pl_mofs[t][l + 1] = pl_mofs[t][l] + pp.n;
+            pl_gofs[t][l + 1] = pl_gofs[t][l] + pp.ng;
+        }
+        pl_members[t].resize(pl_mofs[t][np]);
+        pl_gstart[t].resize(pl_gofs[t][np]);
+        pl_gsize[t].resize(pl_gofs[t][np]);
+        for (int l = 0; l < np; l++) {
+            Place& pp = Places[t][l];
+            for (int k = 0; k < pp.n; k++) pl_members[t][pl_mofs[t][l] + k] = pp.members[k];
+            for (int g = 0; g < pp.ng; g++) {
+                pl_gstart[t][pl_gofs[t][l] + g] = pp.group_start[g];
+                pl_gsize[t][pl_gofs[t][l] + g] = pp.group_size[g];
+            }
+        }
+        pop.n_places[t] = np;
+        pop.place_mcell[t] = pl_mcell[t].data(); pop.place_x[t] = pl_x[t].data(); pop.place_y[t] = pl_y[t].data();
+        pop.place_member_ofs[t] = pl_mofs[t].data(); pop.place_members[t] = pl_members[t].data();
+        pop.place_group_ofs[t] = pl_gofs[t].data(); pop.group_start[t] = pl_gstart[t].data();
+        pop.group_size[t] = pl_gsize[t].data();
+    }
+    // the spatial kernel table exactly as KernelLookup::setup/init built it at the end
+    // of set-up (src/SetupModel.cpp:196-209, 308-309)
+    double longest = dist2_raw(0, 0, P.in_degrees_.width, P.in_degrees_.height);
+    double tw = dist2_raw(0, 0, P.in_degrees_.width, 0), th = dist2_raw(0, 0, 0, P.in_degrees_.height);
+    if (tw > longest) longest = tw;
+    if (th > longest) longest = th;
+    if (P.DoPeriodicBoundaries) longest *= 0.25;
+    static std::vector<double> klook(P.KernelLookup.size_ + 1), khi(P.KernelLookup.size_ + 1);
+    g_params = params_from_reference();
+    if (cs_build_kernel_table(P.Kernel.type_, P.Kernel.scale_, P.Kernel.shape_, P.Kernel.p3_, P.Kernel.p4_, longest,
+                              P.KernelLookup.size_, P.KernelLookup.expansion_factor_, klook.data(), khi.data(),
+                              &g_params.kernel_delta) != CS_OK)
+        ERR_CRITICAL("GPU sweep: kernel table\n");
+    pop.n_people = N; pop.n_households = NH; pop.n_cells = NC; pop.n_mcells = NM; pop.num_place_types = NPT;
+    pop.n_adunits = P.NumAdunits;
+    pop.person_hh = hh.data(); pop.person_mcell = mc.data(); pop.person_age = age.data(); pop.person_flags = flags.data();
+    pop.person_place = place.data(); pop.person_group = group.data();
+    pop.hh_first = hh_first.data(); pop.hh_nh = hh_nh.data(); pop.hh_nhr = hh_nhr.data(); pop.hh_x = hx.data(); pop.hh_y = hy.data();
+    pop.mcell_cell = mcell_cell.data(); pop.mcell_adunit = mcell_ad.data();
+    pop.cell_grid = cell_grid.data(); pop.cell_start = cell_start.data(); pop.cell_members = cell_members.data();
+    pop.kernel_lookup = klook.data(); pop.kernel_hi_res = khi.data();
+    int rc = cs_gpu_create(&pop, &g_params, 0, &g_ctx);
+    check(rc, "cs_gpu_create");
+    g_S.resize(NC); g_L.resize(NC); g_I.resize(NC); g_R.resize(NC); g_D.resize(NC);
+    std::fprintf(stderr, "GPU sweep: %d people, %d populated cells on device\n", N, NC);
+}
+
+long long s0_signature()
+{
+    long long s = 0;
+    for (int c = 0; c < P.NumPopulatedCells; c++) s = s * 1000003 + CellLookup[c]->S0;
+    return s;
+}
+
+void upload_run_state(int run)
+{
+    const int N = P.PopSize, NC = P.NumPopulatedCells;
+    std::vector<int8_t> inf(N);
+    std::vector<uint8_t> sev(N), fl(N);
+    std::vector<uint16_t> it(N), lt(N), rt(N), st(N), ct(N), sd(N), as(N), ae(N), iso(N), qs(N), dt(N);
+    std::vector<float> infn(N), susc(N), pa(N), pc(N);
+    std::vector<int32_t> infector(N), listpos(N), slots(N), S0(NC), cS(NC), cL(NC), cI(NC), cR(NC), cD(NC);
+    std::vector<int16_t> itype(N);
+    std::vector<double> tp(NC);
+    for (int i = 0; i < N; i++) {
+        const Person& a = Hosts[i];
+        inf[i] = inf_of(a);
+        sev[i] = (uint8_t)((int)a.Severity_Current | ((int)a.Severity_Final << 4));
+        fl[i] = (uint8_t)((a.to_die ? CS_DF_TO_DIE : 0) | (a.detected ? CS_DF_DETECTED : 0) |
+                          ((HostsQuarantine[i].comply & 3) << CS_DF_QUAR_COMPLY_SHIFT));
+        it[i] = a.infection_time; lt[i] = a.latent_time; rt[i] = a.recovery_or_death_time;
+        st[i] = a.SARI_time; ct[i] = a.Critical_time; sd[i] = a.Stepdown_time;
+        as[i] = a.absent_start_time; ae[i] = a.absent_stop_time; iso[i] = a.isolation_start_time;
+        qs[i] = HostsQuarantine[i].start_time; dt[i] = a.detected_time;
+        infn[i] = a.infectiousness; susc[i] = a.susc; pa[i] = a.ProbAbsent; pc[i] = a.ProbCare;
+        infector[i] = a.infector; itype[i] = a.infect_type; listpos[i] = a.listpos;
+    }
+    int o = 0;
+    for (int c = 0; c < NC; c++) {
+        Cell* x = CellLookup[c];
+        for (int k = 0; k < x->n; k++) slots[o + k] = x->susceptible[k];
+        o += x->n;
+        cS[c] = x->S; cL[c] = x->L; cI[c] = x->I; cR[c] = x->R; cD[c] = x->D; S0[c] = x->S0; tp[c] = x->tot_prob;
+    }
+    cs_state_view v;
+    std::memset(&v, 0, sizeof(v));
+    v.inf = inf.data(); v.severity = sev.data(); v.flags = fl.data(); v.infection_time = it.data(); v.latent_time = lt.data();
+    v.recovery_or_death_time = rt.data(); v.SARI_time = st.data(); v.Critical_time = ct.data(); v.Stepdown_time = sd.data();
+    v.absent_start_time = as.data(); v.absent_stop_time = ae.data(); v.isolation_start_time = iso.data();
+    v.quar_start_time = qs.data(); v.detected_time = dt.data(); v.infectiousness = infn.data(); v.susc = susc.data();
+    v.ProbAbsent = pa.data(); v.ProbCare = pc.data(); v.infector = infector.data(); v.infect_type = itype.data();
+    v.listpos = listpos.data(); v.cell_S = cS.data(); v.cell_L = cL.data(); v.cell_I = cI.data(); v.cell_R = cR.data();
+    v.cell_D = cD.data(); v.cell_S0 = S0.data(); v.cell_tot_prob = tp.data(); v.cell_slots = slots.data();
+    uint64_t seed = ((uint64_t)(uint32_t)P.runSeed1 << 32) ^ (uint32_t)P.runSeed2 ^ (0x9E3779B97F4A7C15ull * (uint64_t)(run + 1));
+    check(cs_gpu_upload_state(g_ctx, seed, &v), "cs_gpu_upload_state");
+    // seeding ran DoInfect on the host (thread 0's counters); the device counts from zero
+    for (int j = 1; j < P.NumThreads; j++)
+        if (StateT[j].cumI || StateT[j].cumC) ERR_CRITICAL("GPU sweep: host counters outside thread 0 at run start\n");
+    std::memcpy(&g_base, &StateT[0], sizeof(PopVar));
+    g_s0_sig = s0_signature();
+    g_tg_base = g_si_base = g_ntg_base = 0;
+    g_tg_set = g_si_set = g_ntg_set = 0;
+}
+
+// RecordSample (src/CovidSim.cpp:3024-3120) reads per-cell counts and StateT[].
+void sync_back()
+{
+    check(cs_gpu_get_cell_counts(g_ctx, g_S.data(), g_L.data(), g_I.data(), g_R.data(), g_D.data()), "cs_gpu_get_cell_counts");
+    for (int c = 0; c < P.NumPopulatedCells; c++) {
+        Cell* x = CellLookup[c];
+        x->S = g_S[c]; x->L = g_L[c]; x->I = g_I[c]; x->R = g_R[c]; x->D = g_D[c];
+    }
+    cs_counters k;
+    check(cs_gpu_get_counters(g_ctx, &k), "cs_gpu_get_counters");
+    PopVar& s = StateT[0];
+    const PopVar& b = g_base;
+    s.cumI = b.cumI + (int)k.cumI; s.cumC = b.cumC + (int)k.cumC; s.cumDC = b.cumDC + (int)k.cumDC;
+    s.cumFC = b.cumFC + (int)k.cumFC; s.cumHQ = b.cumHQ + (int)k.cumHQ; s.cumAC = b.cumAC + (int)k.cumAC;
+    s.cumAA = b.cumAA + (int)k.cumAA; s.cumACS = b.cumACS + (int)k.cumACS;
+    for (int i = 0; i < INFECT_TYPE_MASK; i++) s.cumItype[i] = b.cumItype[i] + (int)k.cumItype[i];
+    for (int a = 0; a < NUM_AGE_GROUPS; a++) {
+        s.cumIa[a] = b.cumIa[a] + (int)k.cumIa[a];
+        s.cumCa[a] = b.cumCa[a] + (int)k.cumCa[a];
+        s.cumDa[a] = b.cumDa[a] + (int)k.cumDa[a];
+    }
+    s.Mild = b.Mild + (int)k.Mild; s.ILI = b.ILI + (int)k.ILI; s.SARI = b.SARI + (int)k.SARI;
+    s.Critical = b.Critical + (int)k.Critical; s.CritRecov = b.CritRecov + (int)k.CritRecov;
+    s.cumMild = b.cumMild + (int)k.cumMild; s.cumILI = b.cumILI + (int)k.cumILI; s.cumSARI = b.cumSARI + (int)k.cumSARI;
+    s.cumCritical = b.cumCritical + (int)k.cumCritical; s.cumCritRecov = b.cumCritRecov + (int)k.cumCritRecov;
+    s.cumDeath_ILI = b.cumDeath_ILI + (int)k.cumDeath_ILI; s.cumDeath_SARI = b.cumDeath_SARI + (int)k.cumDeath_SARI;
+    s.cumDeath_Critical = b.cumDeath_Critical + (int)k.cumDeath_Critical;
+    for (int i = 0; i < 2; i++) {
+        s.cumI_keyworker[i] = b.cumI_keyworker[i] + (int)k.cumI_keyworker[i];
+        s.cumC_keyworker[i] = b.cumC_keyworker[i] + (int)k.cumC_keyworker[i];
+    }
+    // generation-time sums are read and zeroed by each RecordSample: hand over increments
+    if (s.cumTG != g_tg_set || s.nTG != g_ntg_set) { g_tg_base += g_tg_set; g_si_base += g_si_set; g_ntg_base += g_ntg_set; }
+    g_tg_set = k.cumTG - g_tg_base; g_si_set = k.cumSI - g_si_base; g_ntg_set = k.nTG - g_ntg_base;
+    s.cumTG = (int)g_tg_set; s.cumSI = (int)g_si_set; s.nTG = (int)g_ntg_set;
+}
+
+void interventions_idle()
+{
+    // the host's trigger logic runs in TreatSweep; this drop-in supports runs in which
+    // it never switches an intervention on
+    for (int m = 0; m < P.NumMicrocells; m++)
+        if (Mcells[m].socdist == TreatStat::Treated || Mcells[m].moverest == TreatStat::Treated)
+            ERR_CRITICAL("GPU sweep: microcell interventions switched on by the host are not supported by this drop-in\n");
+}
+
+}  // namespace
+
+void InfectSweep(double t, int run)
+{
+    if (!g_ctx) create_context();
+    if (run != g_run) {
+        upload_run_state(run);
+        g_run = run;
+    } else if (s0_signature() != g_s0_sig) {
+        check(cs_gpu_update_probs(g_ctx, 0), "cs_gpu_update_probs");  // the host ran UpdateProbs(0)
+        g_s0_sig = s0_signature();
+    }
+    if (P.DoSeasonality) {
+        double seas = P.Seasonality[((int)t) % DAYS_PER_YEAR];
+        if (seas != g_params.Seasonality) {
+            g_params.Seasonality = seas;
+            check(cs_gpu_set_params(g_ctx, &g_params), "cs_gpu_set_params");
+        }
+    }
+    if (((int)(t * P.TimeStepsPerDay)) % ((int)P.TimeStepsPerDay) == 0) interventions_idle();
+    check(cs_gpu_infect_sweep(g_ctx, t, run), "cs_gpu_infect_sweep");
+}
+
+void IncubRecoverySweep(double t)
+{
+    check(cs_gpu_incub_recovery_sweep(g_ctx, t), "cs_gpu_incub_recovery_sweep");
+    sync_back();
+}

@@ -321,7 +321,7 @@ typedef struct cs_counters {
     /* work done by the sweeps (for the HBM roofline) */
     int64_t work_infectors, work_hh_members, work_place_candidates;
     int64_t work_spatial_contacts, work_spatial_draws, work_new_infections;
-    int64_t work_transitions, work_cells_touched;
+    int64_t work_transitions, work_cells_touched, work_incub_people;
     /* give-ups of bounded device loops; non-zero means the results are suspect */
     int64_t err_spatial_tries, err_queue_overflow, err_kernel_range;
 } cs_counters;
@@ -398,6 +398,14 @@ int cs_gpu_sync(cs_gpu_ctx* ctx);
 void* cs_gpu_stream(cs_gpu_ctx* ctx);
 /* Number of kernels launched on the context since creation. */
 int64_t cs_gpu_launch_count(const cs_gpu_ctx* ctx);
+/*
+ * Per-kernel device time: with enable = 1 every launch is bracketed by CUDA events
+ * on the context's stream; 2 also clears the totals; 0 stops recording.
+ * cs_gpu_profile_entry reads entry i (name, summed milliseconds, launches) and
+ * returns CS_E_RANGE past the last entry.
+ */
+int cs_gpu_profile(cs_gpu_ctx* ctx, int enable);
+int cs_gpu_profile_entry(cs_gpu_ctx* ctx, int i, char* name, int cap, double* total_ms, int64_t* launches);
 
 #ifdef __cplusplus
 }

@@ -1360,6 +1360,7 @@ int cs_cpu_incub_recovery_sweep(cs_cpu_ctx* c, double t)
     const cs_params* P = &c->P;
     if (!c->run_started) return fail(c, CS_E_STATE, "incub sweep before begin_run");
     int ts = (int)(uint16_t)(P->TimeStepsPerDay * t);
+    for (int ci = 0; ci < c->NC; ci++) c->C.work_incub_people += c->L[ci] + c->I[ci];
     /* latent -> infectious (src/Sweep.cpp:924-927) */
     for (int ci = 0; ci < c->NC; ci++) {
         int b0 = c->cell_start[ci] + c->S[ci];

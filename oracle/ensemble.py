@@ -1,0 +1,67 @@
+"""Statistical equivalence of whole epidemics: the reference executable against the
+same executable with the GPU sweep linked in (oracle/_ref/CovidSim_b200).
+
+TEST INFRASTRUCTURE.  Both binaries read the same parameter and density files, so
+the reference's own set-up builds the same population (same set-up seeds) and its
+own RecordSample writes the outputs; only the sweeps differ.  Per realisation we
+keep the final size (cumulative infections), the peak day of prevalence and the
+daily incidence, critical-care and death curves.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
+sys.path.insert(0, HERE)
+
+CONFIG = dict(people=20000, width_deg=0.2, cell_deg=1.0 / 120, nmcl=10, sigma=1.2, days=120, realisations=200,
+              setup_seed=98798150)
+
+
+def population():
+    from covidsim_b200 import population as popmod
+    c = CONFIG
+    grid = popmod.make_grid(width_deg=c["width_deg"], height_deg=c["width_deg"], cell_deg=c["cell_deg"], nmcl=c["nmcl"])
+    return popmod.generate(c["people"], grid, sigma=c["sigma"], seed=c["setup_seed"])
+
+
+def run(binary, nr=None, threads=None):
+    import refrun
+    c = CONFIG
+    res = refrun.run_reference(population(), c["days"], nr=nr or c["realisations"], threads=threads, binary=binary,
+                               series=True, timeout=5400)
+    return summarise(res["series"]), res
+
+
+def summarise(series):
+    n = len(series)
+    days = len(series[0]["t"])
+    cumI = np.array([s["incI"].sum() for s in series])
+    peak = np.array([int(np.argmax(s["I"])) for s in series])
+    inc = np.stack([s["incI"] for s in series])
+    crit = np.stack([s["Critical"] for s in series])
+    deaths = np.stack([s["cumDeath"] for s in series])
+    return dict(n=n, days=days, final_size=cumI.tolist(), peak_day=peak.tolist(),
+                inc_mean=inc.mean(0).tolist(), inc_var=inc.var(0, ddof=1).tolist(),
+                crit_mean=crit.mean(0).tolist(), crit_var=crit.var(0, ddof=1).tolist(),
+                deaths_mean=deaths.mean(0).tolist(), deaths_var=deaths.var(0, ddof=1).tolist())
+
+
+def compare(a, b):
+    """Two-sample KS on final size and peak day; ensemble means of the daily curves
+    within 2 standard errors on at least 90% of days and 4 on all."""
+    from scipy import stats
+    out = {}
+    out["ks_final_size_p"] = float(stats.ks_2samp(a["final_size"], b["final_size"]).pvalue)
+    out["ks_peak_day_p"] = float(stats.ks_2samp(a["peak_day"], b["peak_day"]).pvalue)
+    for key in ("inc", "crit", "deaths"):
+        ma, mb = np.array(a[key + "_mean"]), np.array(b[key + "_mean"])
+        se = np.sqrt(np.array(a[key + "_var"]) / a["n"] + np.array(b[key + "_var"]) / b["n"])
+        z = np.abs(ma - mb) / np.where(se > 0, se, np.inf)
+        live = se > 0
+        out[key + "_within_2se"] = float((z[live] <= 2).mean()) if live.any() else 1.0
+        out[key + "_max_z"] = float(z[live].max()) if live.any() else 0.0
+    return out

@@ -5,12 +5,13 @@
 // the original symbols declared at src/Sweep.h:7-8 and called from RunModel
 // (src/CovidSim.cpp:1488,1490).  The reference's printed "Model ran in" figure is
 // clock() CPU time summed over threads (src/CovidSim.cpp:418), not wall time, so the
-// baseline is taken from omp_get_wtime() here.  At exit one line is written to
-// stderr:
-//   REFTIMING pop=<N> threads=<T> steps=<k> infect_s=<s> incub_s=<s> first_t=<d> last_t=<d>
+// baseline is taken from omp_get_wtime() here.  At exit one line per realisation
+// is written to stderr:
+//   REFTIMING run=<r> pop=<N> threads=<T> steps=<k> infect_s=<s> incub_s=<s> first_t=<d> last_t=<d>
 #include <cstdio>
 #include <cstdlib>
 #include <omp.h>
+#include <vector>
 
 #include "Param.h"
 #include "Sweep.h"
@@ -19,31 +20,38 @@ void ref_InfectSweep(double t, int run);
 void ref_IncubRecoverySweep(double t);
 
 namespace {
-double g_infect = 0.0, g_incub = 0.0, g_first = -1.0, g_last = -1.0;
-long g_steps = 0;
+struct RunTiming {
+    int run;
+    double infect = 0.0, incub = 0.0, first = -1.0, last = -1.0;
+    long steps = 0;
+};
+std::vector<RunTiming> g_runs;
 bool g_registered = false;
 
 void report()
 {
-	std::fprintf(stderr, "\nREFTIMING pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f first_t=%.4f last_t=%.4f\n",
-		P.PopSize, P.NumThreads, g_steps, g_infect, g_incub, g_first, g_last);
+    for (const RunTiming& r : g_runs)
+        std::fprintf(stderr, "\nREFTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f first_t=%.4f last_t=%.4f\n",
+                     r.run, P.PopSize, P.NumThreads, r.steps, r.infect, r.incub, r.first, r.last);
 }
 }
 
 void InfectSweep(double t, int run)
 {
-	if (!g_registered) { std::atexit(report); g_registered = true; }
-	if (g_first < 0) g_first = t;
-	g_last = t;
-	double t0 = omp_get_wtime();
-	ref_InfectSweep(t, run);
-	g_infect += omp_get_wtime() - t0;
-	g_steps++;
+    if (!g_registered) { std::atexit(report); g_registered = true; }
+    if (g_runs.empty() || g_runs.back().run != run) { g_runs.push_back(RunTiming()); g_runs.back().run = run; }
+    RunTiming& r = g_runs.back();
+    if (r.first < 0) r.first = t;
+    r.last = t;
+    double t0 = omp_get_wtime();
+    ref_InfectSweep(t, run);
+    r.infect += omp_get_wtime() - t0;
+    r.steps++;
 }
 
 void IncubRecoverySweep(double t)
 {
-	double t0 = omp_get_wtime();
-	ref_IncubRecoverySweep(t);
-	g_incub += omp_get_wtime() - t0;
+    double t0 = omp_get_wtime();
+    ref_IncubRecoverySweep(t);
+    if (!g_runs.empty()) g_runs.back().incub += omp_get_wtime() - t0;
 }
