@@ -39,9 +39,12 @@ sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
 import numpy as np  # noqa: E402
 
 WORKLOADS = {
-    # name: (preset, days, interventions, description)
-    "c1": ("c1", 365, True, "10M people, 600x600 cells, interventions, 365 d"),
-    "c0": ("c0", 120, False, "1M people, 240x240 cells, no interventions, 120 d"),
+    # name: (preset, days, interventions, description, initial infections)
+    "c1": ("c1", 365, True, "10M people, 600x600 cells, interventions, 365 d", 100),
+    "c0": ("c0", 120, False, "1M people, 240x240 cells, no interventions, 120 d", 100),
+    # a short case whose sweeps run at epidemic-peak load after a few hundred
+    # launches: the profiling case for the spatial and place kernels
+    "c1_peak": ("c1", 8, False, "10M people, 600x600 cells, 500k initial infections, 8 d", 500000),
 }
 METRIC = "person-steps/s"
 
@@ -128,14 +131,20 @@ def kernel_bytes(name, w, n_cells_steps):
     (per-unit costs: transition scan 16 B per latent/infectious person, infector
     record 40 B, household member 12 B, place candidate 20 B, spatial draw 33 B,
     accepted infection 24 B, per-cell counts 24 B)."""
-    if name == "k_infectors":
-        return 40 * w["work_infectors"] + 12 * w["work_hh_members"] + 20 * w["work_place_candidates"]
+    if name == "k_infector_hh_spatial":
+        return 40 * w["work_infectors"] + 12 * w["work_hh_members"]
+    if name == "k_infector_places":
+        return 20 * w["work_place_candidates"] + 16 * w["work_infectors"]
     if name == "k_spatial":
         return 33 * w["work_spatial_draws"]
+    if name == "k_expand_contacts":
+        return 8 * w["work_spatial_contacts"]
     if name in ("k_apply_infections", "k_partition_S"):
         return 12 * w["work_new_infections"]
-    if name == "k_incub_events":
+    if name == "k_incub_scan":
         return 16 * w["work_incub_people"]
+    if name == "k_incub_events":
+        return 32 * w["work_transitions"]
     if name in ("k_partition_LI", "k_clear_pstep"):
         return 8 * w["work_transitions"]
     if name == "k_gather_active":
@@ -170,7 +179,7 @@ def run_ours(args):
         torch.cuda.set_device(local)
     from covidsim_b200 import population, params as prm, sim
 
-    preset, days, with_iv, desc = WORKLOADS[args.workload]
+    preset, days, with_iv, desc, n_seed = WORKLOADS[args.workload]
     pop = population.preset(preset)
     P, lk, hr = prm.build_params(pop.grid)
     beta, r0parts = sim.calibrate_local_beta(pop, P, 2.4)
@@ -182,7 +191,7 @@ def run_ours(args):
     base_seed = 17389101 + 7919 * rank
 
     for w in range(args.warmup):
-        s.run(seed=base_seed + 1000 + w, days=days, policy=policy)
+        s.run(seed=base_seed + 1000 + w, days=days, n_seed=n_seed, policy=policy)
     be.sync()
 
     def barrier():
@@ -192,26 +201,19 @@ def run_ours(args):
 
     stream = torch.cuda.ExternalStream(be.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    work = None
     finals = []
     barrier()
     launches0 = be.launches()
-    be.profile(2)
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for k in range(args.steps):
-            ser = s.run(seed=base_seed + k, days=days, policy=policy)
-            c = sim.abi.counters_to_dict(be.counters())
-            work = c if work is None else {kk: (work[kk] + c[kk]) if not isinstance(c[kk], list) else work[kk]
-                                           for kk in c}
+            ser = s.run(seed=base_seed + k, days=days, n_seed=n_seed, policy=policy)
             finals.append((int(ser["cumI"][-1]), int(ser["D"][-1]), int(ser["I"].argmax())))
         ev1.record(stream)
         be.sync()
         torch.cuda.synchronize()
     barrier()
     launches = be.launches() - launches0
-    kernels = be.profile_entries()
-    be.profile(0)
     ms = ev0.elapsed_time(ev1)
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -221,10 +223,20 @@ def run_ours(args):
     value = person_steps / (ms / 1e3)
     runs_per_hour = args.steps * world / (ms / 1e3) * 3600.0
 
+    # per-kernel device times: one more realisation of the same workload with every
+    # launch bracketed by CUDA events on the sweep's stream (eager launches)
+    be.profile(2)
+    s.run(seed=base_seed, days=days, n_seed=n_seed, policy=policy)
+    be.sync()
+    kernels = be.profile_entries()
+    be.profile(0)
+    work = sim.abi.counters_to_dict(be.counters())
+    prof_runs = 1
+
     # roofline of the dominant kernel
     peak, peak_kind = peaks()
     traffic = load_traffic()
-    n_cells_steps = pop.n_cells * steps_per_run * args.steps
+    n_cells_steps = pop.n_cells * steps_per_run * prof_runs
     rows = []
     for name, (kms, n) in sorted(kernels.items(), key=lambda kv: -kv[1][0]):
         b = kernel_bytes(name, work, n_cells_steps)
@@ -239,26 +251,31 @@ def run_ours(args):
         "algorithmic_bytes_per_launch": round(dom["bytes"] / dom["launches"]) if dom["bytes"] else None,
         "avg_launch_us": round(dom["ms"] / dom["launches"] * 1e3, 3),
         "share_of_kernel_time": round(dom["share"], 4),
+        "timing": "CUDA events around each launch on the sweep's stream, over one extra realisation of the workload",
     }
     if args.profile_out and rank == 0:
-        json.dump(dict(rows=rows, work=work, timed_ms=ms, steps=args.steps, workload=args.workload),
+        json.dump(dict(rows=rows, work=work, timed_ms=ms, steps=args.steps, workload=args.workload, profiled_runs=prof_runs),
                   open(args.profile_out, "w"), indent=1)
 
     # end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
+        # the prepared start state (input) and the final state (output) in separate
+        # pinned host buffers, so every realisation starts from the same input
         arrs, view = sim.state_arrays(pop.n_people, pop.n_cells)
-        be.begin_run(base_seed, s.choose_seeds(base_seed, 100))
-        be.download(view)          # the prepared start state, now in host memory
+        arrs_out, view_out = sim.state_arrays(pop.n_people, pop.n_cells)
+        be.begin_run(base_seed, s.choose_seeds(base_seed, n_seed))
+        be.download(view)
         cudart = torch.cuda.cudart()
-        for a in arrs.values():
+        pinned = list(arrs.values()) + list(arrs_out.values())
+        for a in pinned:
             cudart.cudaHostRegister(a.ctypes.data, a.nbytes, 0)
         state_bytes = sum(a.nbytes for a in arrs.values())
         barrier()
         t0 = time.perf_counter()
         for k in range(args.steps):
-            s.run(seed=base_seed + k, days=days, policy=policy, initial_state=view)
-            be.download(view)
+            s.run(seed=base_seed + k, days=days, n_seed=n_seed, policy=policy, initial_state=view)
+            be.download(view_out)
         be.sync()
         barrier()
         dt = time.perf_counter() - t0
@@ -266,7 +283,7 @@ def run_ours(args):
             t = torch.tensor([dt], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dt = float(t.item())
-        for a in arrs.values():
+        for a in pinned:
             cudart.cudaHostUnregister(a.ctypes.data)
         import ctypes
         e2e = {"value": round(person_steps / dt, 1), "unit": METRIC, "h2d_bytes_per_step": state_bytes,
@@ -348,10 +365,12 @@ def run_reference(args):
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refrun
+    if args.workload not in refrun.SAMPLES:
+        return {"impl": "reference", "unavailable": "no reference sample defined for workload %s" % args.workload}
     res = refrun.time_reference(args.workload, steps=args.steps, warmup=args.warmup)
     if "unavailable" in res:
         return {"impl": "reference", "unavailable": res["unavailable"]}
-    preset, days, with_iv, desc = WORKLOADS[args.workload]
+    preset, days, with_iv, desc, n_seed = WORKLOADS[args.workload]
     v = res["value"]
     return {
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": METRIC, "n_gpus": args.gpus,

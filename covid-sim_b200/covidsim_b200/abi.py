@@ -142,6 +142,7 @@ def load_library(path=LIB_PATH):
         "cs_gpu_incub_recovery_sweep": (I, [V, D]),
         "cs_gpu_update_probs": (I, [V, I]),
         "cs_gpu_step": (I, [V, D, I]),
+        "cs_gpu_use_graphs": (I, [V, I]),
         "cs_gpu_set_interventions": (I, [V, P(cs_interventions)]),
         "cs_gpu_close_places": (I, [V, I, V, I, C.c_uint16, C.c_uint16]),
         "cs_gpu_get_counters": (I, [V, P(cs_counters)]),

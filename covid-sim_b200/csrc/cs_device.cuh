@@ -202,7 +202,8 @@ __device__ __forceinline__ double periodic_xy(const cs_params& P, double x, doub
 // dist2(Person*, Person*) (src/Dist.cpp:49-61) between two households.
 __device__ __forceinline__ double dist2_hh(const DevPop& d, const cs_params& P, int32_t ha, int32_t hb)
 {
-    float ax = __ldg(d.hh_x + ha), ay = __ldg(d.hh_y + ha), bx = __ldg(d.hh_x + hb), by = __ldg(d.hh_y + hb);
+    float2 a = __ldg(d.hh_xy + ha), b = __ldg(d.hh_xy + hb);
+    float ax = a.x, ay = a.y, bx = b.x, by = b.y;
     if (P.DoUTM_coords) return dist2_utm(P, ax, ay, bx, by);
     float dx = ax - bx, dy = ay - by;
     return periodic_xy(P, fabs(dx), fabs(dy));

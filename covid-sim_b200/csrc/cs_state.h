@@ -53,6 +53,14 @@ struct DevIv {
     double ci_start, ci_dur, hq_start, hq_dur;
 };
 
+// Scalars of the current timestep, written on the device by k_set_step so that a
+// captured step graph needs only that one kernel's arguments changed per replay.
+struct DevStep {
+    double t, fp, seas, sp_beta, hh_beta;
+    int32_t ts, pad;
+    unsigned long long seed;
+};
+
 // Transition flags per person for one IncubRecoverySweep.
 enum : uint8_t { kStepLtoI = 1, kStepItoRD = 2 };
 
@@ -68,6 +76,7 @@ struct DevPop {
     const uint16_t* hh_nhr;
     const float* hh_x;
     const float* hh_y;
+    const float2* hh_xy;       // the two above interleaved, one 8-byte load per household
     const int32_t* mcell_cell;
     const int32_t* mcell_adunit;
     const int32_t* cell_grid;
@@ -103,6 +112,7 @@ struct DevPop {
     uint8_t* socdist;
     uint8_t* moverest;
     DevIv* iv;
+    DevStep* step;
     // spatial proposal blocks
     const int32_t* cell_block;
     const int32_t* block_cell_ofs;
@@ -110,6 +120,9 @@ struct DevPop {
     int32_t* block_cum;
     long long* block_S0;
     double* block_row_cum;     // [NB][NB]
+    double* block_bound_tab;   // [NB][NB] bound(b, B) for target blocks with people
+    int16_t* block_guide;      // [NB][NB] cut points of each row (Chen & Asau guide table)
+    int16_t* cell_guide;       // [NC] cut points of each block's cell list
     // per-step scratch
     unsigned long long* claim; // [N], UINT64_MAX when unclaimed
     int32_t* queue;            // [N] newly infected people
@@ -121,6 +134,8 @@ struct DevPop {
     int32_t* act_cell;         // [N]
     int32_t* cnt;              // [N] spatial contacts per infector
     int32_t* cnt_ofs;          // [N+1]
+    int32_t* cmap;             // [N] infector slot of each spatial contact
+    int32_t cmap_cap;
     uint8_t* act_closed;       // [N] infector's place-closed-and-absent flag
     uint8_t* hh_flag;          // [NH] deferred household actions
     int32_t* hh_list;          // [NH]
@@ -128,6 +143,6 @@ struct DevPop {
     cs_counters* C;
 };
 
-enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntN = 8 };
+enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntEvents = 5, kCntN = 8 };
 
 }  // namespace csb

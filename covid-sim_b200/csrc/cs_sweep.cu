@@ -170,9 +170,18 @@ struct cs_gpu_ctx {
     cs_counters* dC = nullptr;
     int32_t* d_seed_list = nullptr;
     int seed_cap = 0;
+    // dense-grid buffers of UpdateProbs' normaliser
+    double *S0g = nullptr, *Ng = nullptr, *Ag = nullptr, *Bg = nullptr;
+    uint8_t *rowS = nullptr, *rowN = nullptr;
     uint64_t seed = 0;
     bool run_started = false;
     int grid = 148 * 8;
+    // one timestep captured as a CUDA graph and replayed
+    bool use_graph = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<cudaGraphNode_t> set_step_nodes;
+    long long graph_launches = 0;
     // optional per-launch timing with events on the context's stream
     bool prof = false;
     struct Rec { const char* name; cudaEvent_t a, b; };
@@ -271,6 +280,10 @@ static int scan_excl(cs_gpu_ctx* c, const int32_t* in, int32_t* out, int n_host,
     return CS_OK;
 }
 
+extern "C" {
+static int tot_prob_pass(cs_gpu_ctx* c, bool denominators);
+}
+
 // ================================================================ run start
 __global__ void k_reset_people(DevPop d, uint64_t seed)
 {
@@ -356,29 +369,98 @@ __global__ void k_update_S0(DevPop d, int do_place)
     }
 }
 
-// tot_prob of src/CovidSim.cpp:2779-2791 without the dense tables: one warp per
-// source cell, lane k summing targets m = k (mod 32) in order, then a fixed fold.
-__global__ void k_tot_prob(DevPop d)
+// tot_prob of src/CovidSim.cpp:2779-2791 without the dense Ncells^2 tables.
+//
+// tot_prob_l = A_l / B_l with A_l = sum_m S0_m Kmax(l,m), B_l = sum_m n_m Kmax(l,m)
+// and Kmax(l,m) = (float)num(dist2_cc_min(l, m)).  The closest-corner distance
+// between two cells depends only on their column distance |dx| and their two rows,
+// so a block owning source row yl and a run of source columns evaluates the
+// kernel once per (target row ym, |dx|) into shared memory and every thread sums
+// its own source cell from there.  Order of summation (restated by the oracle):
+//   A_l = sum over ym ascending of ( sum over xm ascending of S0(xm,ym) * G(|xm-xl|) ),
+// products exact in double, zero terms skipped (adding +0.0 changes nothing).
+__device__ double row_kernel(const DevPop& d, const cs_params& P, int dx, int yl, int ym, unsigned long long* err)
+{
+    int y1 = yl, y2 = ym;
+    if (ym > yl) y1 = yl + 1;
+    else if (ym < yl) y2 = ym + 1;
+    double d2;
+    if (P.DoUTM_coords) {
+        int cx = (dx == 0) ? 0 : ((P.cell_width * (double)dx > CSB_REF_PI) ? dx + 1 : dx - 1);
+        d2 = dist2_utm(P, 0.0, P.cell_height * (double)y1, P.cell_width * (double)cx, P.cell_height * (double)y2);
+    } else {
+        int cx = (dx == 0) ? 0 : (((P.DoPeriodicBoundaries) && (P.cell_width * (double)dx > P.width_deg * 0.5)) ? dx + 1 : dx - 1);
+        int dy = abs(ym - yl), cy = (dy == 0) ? 0 : dy - 1;
+        if ((P.DoPeriodicBoundaries) && (P.height_deg * (double)dy > P.height_deg * 0.5)) cy = dy + 1;
+        d2 = periodic_xy(P, P.cell_width * (double)cx, P.cell_height * (double)cy);
+    }
+    return (double)(float)knum(d, P, d2, err);
+}
+
+__global__ void k_grid_values(DevPop d, double* S0g, double* Ng, uint8_t* rowS, uint8_t* rowN)
+{
+    int nch = d.P->nch;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        int g = d.cell_grid[c];
+        S0g[g] = (double)d.S0[c];
+        if (d.S0[c] > 0) rowS[g % nch] = 1;
+        if (Ng) {
+            int n = d.cell_start[c + 1] - d.cell_start[c];
+            Ng[g] = (double)n;
+            if (n > 0) rowN[g % nch] = 1;
+        }
+    }
+}
+
+__global__ void k_tot_prob_rows(DevPop d, const double* S0g, const double* Ng, const uint8_t* rowS, const uint8_t* rowN,
+                                double* Ag, double* Bg)
 {
     const cs_params& P = *d.P;
-    int lane = threadIdx.x & 31;
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int l = warp; l < d.NC; l += nwarps) {
-        int gl = d.cell_grid[l];
-        double a = 0.0, b = 0.0;
-        for (int m = lane; m < d.NC; m += 32) {
-            double kf = (double)(float)knum(d, P, dist2_cc_min(P, gl, d.cell_grid[m]), CSB_CTR(err_kernel_range));
-            int n = d.cell_start[m + 1] - d.cell_start[m];
-            a = a + (double)d.S0[m] * kf;
-            b = b + (double)n * kf;
+    const int ncw = P.ncw, nch = P.nch;
+    extern __shared__ double sh[];
+    double* G = sh;
+    double* Srow = sh + ncw;
+    double* Nrow = Srow + ncw;
+    const int xl = blockIdx.x * blockDim.x + threadIdx.x, yl = blockIdx.y;
+    const bool want_b = Ng != nullptr;
+    double A = 0.0, B = 0.0;
+    for (int ym = 0; ym < nch; ym++) {
+        bool useS = rowS[ym] != 0, useN = want_b && rowN[ym] != 0;
+        if (!useS && !useN) continue;
+        __syncthreads();
+        for (int k = threadIdx.x; k < ncw; k += blockDim.x) {
+            G[k] = row_kernel(d, P, k, yl, ym, CSB_CTR(err_kernel_range));
+            Srow[k] = S0g[(size_t)k * nch + ym];
+            if (want_b) Nrow[k] = Ng[(size_t)k * nch + ym];
         }
-        for (int off = 16; off >= 1; off >>= 1) {
-            double ao = __shfl_down_sync(0xffffffffu, a, off);
-            double bo = __shfl_down_sync(0xffffffffu, b, off);
-            if (lane < off) { a = a + ao; b = b + bo; }
+        __syncthreads();
+        if (xl < ncw) {
+            double s = 0.0, sb = 0.0;
+            for (int xm = 0; xm < ncw; xm++) {
+                int dd = xm > xl ? xm - xl : xl - xm;
+                double sv = Srow[xm];
+                if (useS && sv != 0.0) s = s + sv * G[dd];
+                if (useN) {
+                    double nv = Nrow[xm];
+                    if (nv != 0.0) sb = sb + nv * G[dd];
+                }
+            }
+            if (useS) A = A + s;
+            if (useN) B = B + sb;
         }
-        if (lane == 0) d.tot_prob[l] = (b > 0) ? a / b : 0.0;
+    }
+    if (xl < ncw) {
+        Ag[(size_t)xl * nch + yl] = A;
+        if (want_b) Bg[(size_t)xl * nch + yl] = B;
+    }
+}
+
+__global__ void k_tot_prob_finish(DevPop d, const double* Ag, const double* Bg)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        int g = d.cell_grid[c];
+        double b = Bg[g];
+        d.tot_prob[c] = (b > 0) ? Ag[g] / b : 0.0;
     }
 }
 
@@ -386,11 +468,20 @@ __global__ void k_block_S0(DevPop d)
 {
     for (int B = blockIdx.x * blockDim.x + threadIdx.x; B < d.NB; B += gridDim.x * blockDim.x) {
         long long s = 0;
-        for (int k = d.block_cell_ofs[B]; k < d.block_cell_ofs[B + 1]; k++) {
+        int k0 = d.block_cell_ofs[B], k1 = d.block_cell_ofs[B + 1];
+        for (int k = k0; k < k1; k++) {
             s += d.S0[d.block_cells[k]];
             d.block_cum[k] = (int32_t)s;
         }
         d.block_S0[B] = s;
+        // cut points of the block's cells: entry k0+q = first cell whose running S0
+        // exceeds q/nc of the block total
+        int nc = k1 - k0, j = k0;
+        for (int q = 0; q < nc; q++) {
+            double thr = (double)q * (double)s / (double)nc;
+            while (j < k1 - 1 && (double)d.block_cum[j] <= thr) j++;
+            d.cell_guide[k0 + q] = (int16_t)(j - k0);
+        }
     }
 }
 
@@ -408,13 +499,29 @@ __global__ void k_block_rows(DevPop d)
         for (int B0 = 0; B0 < d.NB; B0 += 32) {
             int B = B0 + lane;
             double w = 0.0;
-            if (B < d.NB && d.block_S0[B] > 0) w = (double)d.block_S0[B] * block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
+            if (B < d.NB && d.block_S0[B] > 0) {
+                double bound = block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
+                d.block_bound_tab[(size_t)b * d.NB + B] = bound;
+                w = (double)d.block_S0[B] * bound;
+            }
             for (int k = 0; k < 32; k++) {
                 double wk = __shfl_sync(0xffffffffu, w, k);
                 if (B0 + k < d.NB) {
                     s = s + wk;
                     if (lane == k) row[B] = s;
                 }
+            }
+        }
+        // guide[k] = first B whose running weight exceeds k/NB of the row total
+        __syncwarp();
+        if (lane == 0) {
+            int16_t* guide = d.block_guide + (size_t)b * d.NB;
+            double total = s;
+            int B = 0;
+            for (int k = 0; k < d.NB; k++) {
+                double thr = (double)k * total / (double)d.NB;
+                while (B < d.NB - 1 && row[B] <= thr) B++;
+                guide[k] = (int16_t)B;
             }
         }
     }
@@ -449,10 +556,23 @@ __device__ __forceinline__ void claim_infection(const DevPop& d, int person, int
     if (old == ~0ull) d.queue[append(d.counts + kCntQueue)] = person;
 }
 
-struct StepScalars {
-    double t, fp, seas, sp_beta, hh_beta;
-    int ts;
-};
+typedef DevStep StepScalars;
+
+// The step's scalars from the parameters, on the device (src/Sweep.cpp:292-301).
+__global__ void k_set_step(DevPop d, double t, unsigned long long seed)
+{
+    const cs_params& P = *d.P;
+    DevStep st;
+    st.t = t;
+    st.ts = (int)(uint16_t)(P.TimeStepsPerDay * t);
+    st.pad = 0;
+    st.fp = P.ModelTimeStep / (1 - P.FalsePositiveRate);
+    st.seas = P.Seasonality;
+    st.sp_beta = P.DoSpatial ? st.seas * st.fp * P.LocalBeta : 0.0;
+    st.hh_beta = P.DoHouseholds ? st.seas * st.fp * P.HouseholdTrans : 0.0;
+    st.seed = seed;
+    *d.step = st;
+}
 
 // Geometric-skip enumeration of the Bernoulli(p) trials over a member list
 // (equivalent to the reference's Binomial count + sample without replacement,
@@ -496,10 +616,13 @@ __device__ void place_candidates(const DevPop& d, const cs_params& P, const Step
     cnt_add(CSB_CTR(work_place_candidates), ncand);
 }
 
-// Household, place and spatial-count passes for one infector (src/Sweep.cpp:314-691).
-__global__ void __launch_bounds__(kThreads) k_infectors(DevPop d, StepScalars st, uint64_t seed)
+// Household pass and spatial Poisson count of one infector (src/Sweep.cpp:331-377,
+// 656-698); one thread per infector.
+__global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d)
 {
     const cs_params& P = *d.P;
+    const StepScalars st = *d.step;
+    const uint64_t seed = st.seed;
     int nact = d.counts[kCntAct];
     long long hh_members = 0;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
@@ -507,7 +630,6 @@ __global__ void __launch_bounds__(kThreads) k_infectors(DevPop d, StepScalars st
         PersonHot hi = d.hot[i];
         int h = hi.hh;
         int iag = age_group(hi);
-        // household (src/Sweep.cpp:331-377)
         uint16_t nh = d.hh_nh[h];
         if (st.hh_beta > 0 && nh > 1) {
             int f0 = d.hh_first[h], f1 = f0 + nh;
@@ -531,25 +653,6 @@ __global__ void __launch_bounds__(kThreads) k_infectors(DevPop d, StepScalars st
                 }
             }
         }
-        // places (src/Sweep.cpp:379-647)
-        if (P.DoPlaces && !host_absent(hi, st.ts)) {
-            for (int pt = 0; pt < d.NPT; pt++) {
-                int link = link_of(d, pt, i);
-                if (link < 0) continue;
-                double PI = st.fp * st.seas * calc_place_inf(hi, P, pt, st.ts);
-                if (moverest_differs(d, hi.mcell, d.pl[pt].mcell[link])) PI *= P.MoveRestrEffect;
-                if (pt != P.HotelPlaceType) {
-                    double p1 = PI;
-                    if (p1 > 1) p1 = 1;
-                    place_candidates(d, P, st, i, hi, pt, link, p1, false, seed);
-                }
-                int n = d.pl[pt].member_ofs[link + 1] - d.pl[pt].member_ofs[link];
-                double p2 = PI * (P.PlaceTypePropBetweenGroupLinks[pt] * P.PlaceTypeGroupSizeParam1[pt] / ((double)n));
-                if (p2 > 1) p2 = 1;
-                place_candidates(d, P, st, i, hi, pt, link, p2, true, seed);
-            }
-        }
-        // spatial infectiousness and per-infector Poisson count (src/Sweep.cpp:656-698)
         int k = 0;
         uint8_t closed_i = 0;
         if (st.sp_beta > 0) {
@@ -571,29 +674,75 @@ __global__ void __launch_bounds__(kThreads) k_infectors(DevPop d, StepScalars st
     cnt_add(CSB_CTR(work_hh_members), hh_members);
 }
 
+// Place passes (src/Sweep.cpp:379-647): one thread per (infector, place type).
+__global__ void __launch_bounds__(kThreads) k_infector_places(DevPop d)
+{
+    const cs_params& P = *d.P;
+    const StepScalars st = *d.step;
+    const uint64_t seed = st.seed;
+    if (!P.DoPlaces || d.NPT == 0) return;
+    long long n = (long long)d.counts[kCntAct] * d.NPT;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int idx = (int)(t / d.NPT), pt = (int)(t % d.NPT);
+        int i = d.act[idx];
+        int link = link_of(d, pt, i);
+        if (link < 0) continue;
+        PersonHot hi = d.hot[i];
+        if (host_absent(hi, st.ts)) continue;
+        double PI = st.fp * st.seas * calc_place_inf(hi, P, pt, st.ts);
+        if (moverest_differs(d, hi.mcell, d.pl[pt].mcell[link])) PI *= P.MoveRestrEffect;
+        if (pt != P.HotelPlaceType) {
+            double p1 = PI;
+            if (p1 > 1) p1 = 1;
+            place_candidates(d, P, st, i, hi, pt, link, p1, false, seed);
+        }
+        int np = d.pl[pt].member_ofs[link + 1] - d.pl[pt].member_ofs[link];
+        double p2 = PI * (P.PlaceTypePropBetweenGroupLinks[pt] * P.PlaceTypeGroupSizeParam1[pt] / ((double)np));
+        if (p2 > 1) p2 = 1;
+        place_candidates(d, P, st, i, hi, pt, link, p2, true, seed);
+    }
+}
+
+// Contact -> infector map: infector idx writes its own contacts' slots.
+__global__ void k_expand_contacts(DevPop d)
+{
+    int nact = d.counts[kCntAct];
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
+        int o = d.cnt_ofs[idx], k = d.cnt[idx];
+        for (int j = 0; j < k && o + j < d.cmap_cap; j++) d.cmap[o + j] = idx;
+    }
+}
+
 // One thread per spatial contact (src/Sweep.cpp:742-856): pick a target block from
 // the infector's block row, a slot uniformly among the block's S0 slots, accept with
 // K(d)/bound, redraw on rejection or a dead target.
-__global__ void __launch_bounds__(kThreads) k_spatial(DevPop d, StepScalars st, uint64_t seed)
+__global__ void __launch_bounds__(kThreads) k_spatial(DevPop d)
 {
     const cs_params& P = *d.P;
+    const StepScalars st = *d.step;
+    const uint64_t seed = st.seed;
     int nact = d.counts[kCntAct];
     int ncont = d.counts[kCntContacts];
     long long draws = 0;
     for (int cidx = blockIdx.x * blockDim.x + threadIdx.x; cidx < ncont; cidx += gridDim.x * blockDim.x) {
-        // infector owning contact cidx: last idx with cnt_ofs[idx] <= cidx
-        int lo = 0, hi = nact - 1;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (d.cnt_ofs[mid] <= cidx) lo = mid; else hi = mid - 1;
+        // infector owning contact cidx: from the map, else last idx with cnt_ofs[idx] <= cidx
+        int idx;
+        if (cidx < d.cmap_cap) idx = d.cmap[cidx];
+        else {
+            int lo = 0, hi = nact - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (d.cnt_ofs[mid] <= cidx) lo = mid; else hi = mid - 1;
+            }
+            idx = lo;
         }
-        int idx = lo;
         int j = cidx - d.cnt_ofs[idx];
         int i = d.act[idx], ci = d.act_cell[idx];
         bool closed_i = d.act_closed[idx] != 0;
         PersonHot hinf = d.hot[i];
         int b = d.cell_block[ci];
         const double* row = d.block_row_cum + (size_t)b * d.NB;
+        const int16_t* guide_row = d.block_guide + (size_t)b * d.NB;
         double total = row[d.NB - 1];
         if (!(total > 0)) { cnt_add(CSB_CTR(err_spatial_tries), 1); continue; }
         Stream s(seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)st.ts, (uint32_t)i, (uint32_t)j);
@@ -601,27 +750,27 @@ __global__ void __launch_bounds__(kThreads) k_spatial(DevPop d, StepScalars st, 
         for (int tries = 0;; tries++) {
             if (tries >= kMaxSpatialTries) { cnt_add(CSB_CTR(err_spatial_tries), 1); break; }
             draws++;
-            double target = s.next() * total;
-            int l0 = 0, l1 = d.NB - 1;
-            while (l0 < l1) {
-                int mid = (l0 + l1) >> 1;
-                if (target < row[mid]) l1 = mid; else l0 = mid + 1;
-            }
-            int B = l0;
+            // smallest B with target < row[B]: guide-table start, then walk
+            double u1 = s.next();
+            double target = u1 * total;
+            int B = guide_row[min((int)(u1 * (double)d.NB), d.NB - 1)];
+            while (B > 0 && row[B - 1] > target) B--;
+            while (B < d.NB - 1 && !(target < row[B])) B++;
             long long bS0 = d.block_S0[B];
             if (bS0 <= 0) continue;
-            double r = floor(s.next() * (double)bS0);
-            int k0 = d.block_cell_ofs[B], k1 = d.block_cell_ofs[B + 1] - 1;
-            while (k0 < k1) {
-                int mid = (k0 + k1) >> 1;
-                if (r < (double)d.block_cum[mid]) k1 = mid; else k0 = mid + 1;
-            }
+            double u2 = s.next();
+            double r = floor(u2 * (double)bS0);
+            // smallest cell k in block B with r < cum[k], the same way
+            int kb = d.block_cell_ofs[B], ke = d.block_cell_ofs[B + 1] - 1;
+            int k0 = kb + d.cell_guide[kb + min((int)(u2 * (double)(ke - kb + 1)), ke - kb)];
+            while (k0 > kb && r < (double)d.block_cum[k0 - 1]) k0--;
+            while (k0 < ke && !(r < (double)d.block_cum[k0])) k0++;
             int m = d.block_cells[k0];
             int slot = (int)(r - (double)(d.block_cum[k0] - d.S0[m]));
             int p = d.slots[d.cell_start[m] + slot];
             PersonHot hp = d.hot[p];
             double d2 = dist2_hh(d, P, hinf.hh, hp.hh);
-            double accept = knum(d, P, d2, CSB_CTR(err_kernel_range)) / block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
+            double accept = knum(d, P, d2, CSB_CTR(err_kernel_range)) / d.block_bound_tab[(size_t)b * d.NB + B];
             if ((s.next() >= accept) || !is_alive(hp.inf)) continue;
             if ((ci != m) || (hp.hh != hinf.hh)) {
                 double ss = calc_spatial_susc(d, hp, P, st.ts);
@@ -653,9 +802,12 @@ __global__ void __launch_bounds__(kThreads) k_spatial(DevPop d, StepScalars st, 
 }
 
 // DoInfect (src/Update.cpp:100-195) for every person claimed this step.
-__global__ void k_apply_infections(DevPop d, double t, int ts, uint64_t seed)
+__global__ void k_apply_infections(DevPop d)
 {
     const cs_params& P = *d.P;
+    const double t = d.step->t;
+    const int ts = d.step->ts;
+    const uint64_t seed = d.step->seed;
     int nq = d.counts[kCntQueue];
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
         int p = d.queue[q];
@@ -969,14 +1121,40 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
     return 2;
 }
 
-// cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
-__global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d, double t, int ts, uint64_t seed)
+// Which latent / infectious people have an event this step (latent period ends,
+// case onset, severity change, recovery or death): a light scan that compacts
+// them into cmap so the heavy transition kernel runs only on those.
+__global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d)
 {
     const cs_params& P = *d.P;
-    const DevIv iv = *d.iv;
+    const int ts = d.step->ts;
     int nact = d.counts[kCntAct];
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_incub_people), nact);
+    const int delay = (int)(P.LatentToSymptDelay / P.ModelTimeStep);
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
+        int p = d.act[idx];
+        PersonHot h = d.hot[p];
+        bool ev;
+        if (h.inf == CS_INF_LATENT)
+            ev = h.latent_time == ts;
+        else
+            ev = (ts == (uint16_t)(h.latent_time + delay)) || (ts == d.recovery_time[p]) ||
+                 (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
+        if (ev) d.cmap[append(d.counts + kCntEvents)] = idx;
+    }
+}
+
+// cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
+__global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d)
+{
+    const cs_params& P = *d.P;
+    const double t = d.step->t;
+    const int ts = d.step->ts;
+    const uint64_t seed = d.step->seed;
+    const DevIv iv = *d.iv;
+    int nev = d.counts[kCntEvents];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) {
+        int idx = d.cmap[e];
         int p = d.act[idx], c = d.act_cell[idx];
         PersonHot h = d.hot[p];
         int pos = d.cell_start[c] + d.listpos[p];
@@ -1032,9 +1210,11 @@ __global__ void k_clear_pstep(DevPop d)
 // Deferred household actions, once per household, after every per-person
 // transition of the step: the adult-carer absence of DoCase/DoDetectedCase
 // (src/Update.cpp:736-763, 843-868) and household quarantine (src/Update.cpp:676-708).
-__global__ void k_household_after(DevPop d, int ts, uint64_t seed)
+__global__ void k_household_after(DevPop d)
 {
     const cs_params& P = *d.P;
+    const int ts = d.step->ts;
+    const uint64_t seed = d.step->seed;
     int nh = d.counts[kCntHH];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
         int h = d.hh_list[k];
@@ -1216,6 +1396,14 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     { uint16_t* t; UP(t, pop->hh_nhr, NH); d.hh_nhr = t; }
     { float* t; UP(t, pop->hh_x, NH); d.hh_x = t; }
     { float* t; UP(t, pop->hh_y, NH); d.hh_y = t; }
+    {
+        std::vector<float2> xy(NH);
+        for (size_t h = 0; h < NH; h++) xy[h] = make_float2(pop->hh_x[h], pop->hh_y[h]);
+        float2* t;
+        UP(t, xy.data(), NH);
+        d.hh_xy = t;
+        CK(cudaStreamSynchronize(c->stream));
+    }
     { int32_t* t; UP(t, pop->mcell_cell, NM); d.mcell_cell = t; }
     { int32_t* t; UP(t, pop->mcell_adunit, NM); d.mcell_adunit = t; }
     { int32_t* t; UP(t, pop->cell_grid, NC); d.cell_grid = t; }
@@ -1255,6 +1443,9 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     d.nbx = (params->ncw + bs - 1) / bs;
     d.nby = (params->nch + bs - 1) / bs;
     d.NB = d.nbx * d.nby;
+    // guide tables index blocks and a block's cells with 16-bit entries
+    if (d.NB > 32767 || (long long)bs * bs > 32767)
+        return set_err(c, CS_E_UNSUPPORTED, "proposal blocks: at most 32767 blocks of at most 32767 cells");
     {
         std::vector<int32_t> cb(NC), ofs(d.NB + 1, 0), cells(NC), fill(d.NB, 0);
         for (size_t m = 0; m < NC; m++) {
@@ -1270,9 +1461,17 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         CK(cudaStreamSynchronize(c->stream));
     }
     AL(d.block_cum, NC); AL(d.block_S0, (size_t)d.NB); AL(d.block_row_cum, (size_t)d.NB * d.NB);
+    AL(d.block_bound_tab, (size_t)d.NB * d.NB);
+    AL(d.block_guide, (size_t)d.NB * d.NB); AL(d.cell_guide, NC);
     // scratch
+    {
+        size_t G = (size_t)params->ncw * params->nch;
+        AL(c->S0g, G); AL(c->Ng, G); AL(c->Ag, G); AL(c->Bg, G);
+        AL(c->rowS, (size_t)params->nch); AL(c->rowN, (size_t)params->nch);
+    }
     AL(d.claim, N); AL(d.queue, N); AL(d.counts, kCntN); AL(d.touched, NC); AL(d.cell_flag, NC + 4);
     AL(d.act_ofs, NC + 1); AL(d.act, N); AL(d.act_cell, N); AL(d.cnt, N > NC ? N : NC); AL(d.cnt_ofs, N + 1);
+    AL(d.cmap, N); d.cmap_cap = (int32_t)N;
     AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH); AL(d.scan_tmp, kScanBlocks);
     CK(cudaMemsetAsync(d.claim, 0xff, sizeof(unsigned long long) * N, c->stream));
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
@@ -1282,9 +1481,13 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     CK(cudaMemsetAsync(d.pstep, 0, N, c->stream));
     { cs_params* t; UP(t, params, 1); c->dP = t; d.P = t; }
     { DevIv iv{1e10, 0, 1e10, 0}; DevIv* t; UP(t, &iv, 1); c->dIv = t; d.iv = t; }
+    { DevStep* t; AL(t, 1); d.step = t; CK(cudaMemsetAsync(t, 0, sizeof(DevStep), c->stream)); }
     { cs_counters* t; AL(t, 1); c->dC = t; d.C = t; CK(cudaMemsetAsync(t, 0, sizeof(cs_counters), c->stream)); }
 #undef UP
 #undef AL
+    CK(cudaStreamSynchronize(c->stream));
+    r = tot_prob_pass(c, true);  // the n-weighted denominators never change
+    if (r) return r;
     CK(cudaStreamSynchronize(c->stream));
     return CS_OK;
 }
@@ -1294,6 +1497,8 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& r : c->ring) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
     for (void* p : c->allocs) cudaFree(p);
     if (c->d_seed_list) cudaFree(c->d_seed_list);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1313,6 +1518,32 @@ int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
     return CS_OK;
 }
 
+// One pass of the tot_prob row kernel: A from the current S0 (and, at creation,
+// B from the cell populations).
+static int tot_prob_pass(cs_gpu_ctx* c, bool denominators)
+{
+    DevPop& d = c->d;
+    const cs_params& P = c->hp;
+    size_t G = (size_t)P.ncw * P.nch;
+    CK(cudaMemsetAsync(c->S0g, 0, sizeof(double) * G, c->stream));
+    CK(cudaMemsetAsync(c->rowS, 0, P.nch, c->stream));
+    if (denominators) {
+        CK(cudaMemsetAsync(c->Ng, 0, sizeof(double) * G, c->stream));
+        CK(cudaMemsetAsync(c->rowN, 0, P.nch, c->stream));
+    }
+    LAUNCH(k_grid_values, (d.NC + kThreads - 1) / kThreads, kThreads, d, c->S0g, denominators ? c->Ng : nullptr, c->rowS, c->rowN);
+    const int tpb = 128;
+    dim3 grid((P.ncw + tpb - 1) / tpb, P.nch);
+    size_t smem = sizeof(double) * 3 * P.ncw;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (c->prof) prof_begin(c, "k_tot_prob_rows");
+    k_tot_prob_rows<<<grid, tpb, smem, c->stream>>>(d, c->S0g, denominators ? c->Ng : nullptr, c->rowS, c->rowN, c->Ag, c->Bg);
+    if (c->prof) prof_end(c);
+    c->launches++;
+    CK(cudaGetLastError());
+    return CS_OK;
+}
+
 static int rebuild_blocks(cs_gpu_ctx* c)
 {
     DevPop& d = c->d;
@@ -1326,14 +1557,16 @@ int cs_gpu_update_probs(cs_gpu_ctx* c, int do_place)
     if (!c) return CS_E_ARG;
     DevPop& d = c->d;
     LAUNCH(k_update_S0, (d.NC + kThreads - 1) / kThreads, kThreads, d, do_place);
-    LAUNCH(k_tot_prob, (d.NC * 32 + kThreads - 1) / kThreads, kThreads, d);
+    int r = tot_prob_pass(c, false);
+    if (r) return r;
+    LAUNCH(k_tot_prob_finish, (d.NC + kThreads - 1) / kThreads, kThreads, d, c->Ag, c->Bg);
     return rebuild_blocks(c);
 }
 
-static int apply_queue(cs_gpu_ctx* c, double t, int ts)
+static int apply_queue(cs_gpu_ctx* c)
 {
     DevPop& d = c->d;
-    LAUNCH(k_apply_infections, c->grid, kThreads, d, t, ts, c->seed);
+    LAUNCH(k_apply_infections, c->grid, kThreads, d);
     LAUNCH(k_partition_S, c->grid, kThreads, d);
     CK(cudaMemsetAsync(d.counts + kCntQueue, 0, sizeof(int32_t) * 2, c->stream));  // queue + touched
     return CS_OK;
@@ -1351,9 +1584,9 @@ int cs_gpu_seed_infections(cs_gpu_ctx* c, double t, const int32_t* people, int n
         c->seed_cap = n;
     }
     CK(cudaMemcpyAsync(c->d_seed_list, people, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
-    int ts = (int)(uint16_t)(c->hp.TimeStepsPerDay * t);
+    LAUNCH(k_set_step, 1, 1, c->d, t, (unsigned long long)c->seed);
     LAUNCH(k_seed_claims, (n + kThreads - 1) / kThreads, kThreads, c->d, c->d_seed_list, n);
-    return apply_queue(c, t, ts);
+    return apply_queue(c);
 }
 
 int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, int n_seed, int update_probs)
@@ -1380,18 +1613,6 @@ int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, i
     return cs_gpu_seed_infections(c, 0.0, seed_people, n_seed);
 }
 
-static StepScalars step_scalars(const cs_params& P, double t)
-{
-    StepScalars st;
-    st.t = t;
-    st.ts = (int)(uint16_t)(P.TimeStepsPerDay * t);
-    st.fp = P.ModelTimeStep / (1 - P.FalsePositiveRate);
-    st.seas = P.Seasonality;
-    st.sp_beta = P.DoSpatial ? st.seas * st.fp * P.LocalBeta : 0.0;
-    st.hh_beta = P.DoHouseholds ? st.seas * st.fp * P.HouseholdTrans : 0.0;
-    return st;
-}
-
 static int gather_active(cs_gpu_ctx* c, int mode)
 {
     DevPop& d = c->d;
@@ -1409,15 +1630,17 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
     if (!c) return CS_E_ARG;
     if (!c->run_started) return set_err(c, CS_E_STATE, "infect_sweep before begin_run");
     DevPop& d = c->d;
-    StepScalars st = step_scalars(c->hp, t);
+    LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
     int r = gather_active(c, 0);
     if (r) return r;
-    LAUNCH(k_infectors, c->grid, kThreads, d, st, c->seed);
+    LAUNCH(k_infector_hh_spatial, c->grid, kThreads, d);
+    LAUNCH(k_infector_places, c->grid, kThreads, d);
     r = scan_excl(c, d.cnt, d.cnt_ofs, 0, d.counts + kCntAct, d.counts + kCntContacts);
     if (r) return r;
-    LAUNCH(k_spatial, c->grid, kThreads, d, st, c->seed);
+    LAUNCH(k_expand_contacts, c->grid, kThreads, d);
+    LAUNCH(k_spatial, c->grid, kThreads, d);
     CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * (d.N > d.NC ? d.N : d.NC), c->stream));
-    return apply_queue(c, t, st.ts);
+    return apply_queue(c);
 }
 
 int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* c, double t)
@@ -1425,22 +1648,91 @@ int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* c, double t)
     if (!c) return CS_E_ARG;
     if (!c->run_started) return set_err(c, CS_E_STATE, "incub_recovery_sweep before begin_run");
     DevPop& d = c->d;
-    int ts = (int)(uint16_t)(c->hp.TimeStepsPerDay * t);
+    LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
     int r = gather_active(c, 1);
     if (r) return r;
-    LAUNCH(k_incub_events, c->grid, kThreads, d, t, ts, c->seed);
+    CK(cudaMemsetAsync(d.counts + kCntEvents, 0, sizeof(int32_t), c->stream));
+    LAUNCH(k_incub_scan, c->grid, kThreads, d);
+    LAUNCH(k_incub_events, c->grid, kThreads, d);
     LAUNCH(k_partition_LI, c->grid, kThreads, d);
     LAUNCH(k_clear_pstep, c->grid, kThreads, d);
-    LAUNCH(k_household_after, c->grid, kThreads, d, ts, c->seed);
+    LAUNCH(k_household_after, c->grid, kThreads, d);
     CK(cudaMemsetAsync(d.counts + kCntTouched, 0, sizeof(int32_t) * 2, c->stream));  // touched + households
+    return CS_OK;
+}
+
+static int step_eager(cs_gpu_ctx* c, double t, int run)
+{
+    int r = cs_gpu_infect_sweep(c, t, run);
+    if (r) return r;
+    return cs_gpu_incub_recovery_sweep(c, t);
+}
+
+// Capture one whole timestep (both sweeps, ~25 kernels and memsets) as a CUDA graph.
+// Every kernel reads the step's scalars from device memory written by k_set_step,
+// so a replay only needs the two k_set_step nodes' arguments changed.
+static int capture_step(cs_gpu_ctx* c, double t, int run)
+{
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    long long l0 = c->launches;
+    int r = step_eager(c, t, run);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (r || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        c->use_graph = false;  // fall back to eager launches for this context
+        return r ? r : set_err(c, CS_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    }
+    size_t n = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    CK(cudaGraphGetNodes(g, nodes.data(), &n));
+    c->set_step_nodes.clear();
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        CK(cudaGraphNodeGetType(nd, &ty));
+        if (ty != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        CK(cudaGraphKernelNodeGetParams(nd, &kp));
+        if (kp.func == (void*)k_set_step) c->set_step_nodes.push_back(nd);
+    }
+    CK(cudaGraphInstantiate(&c->graph_exec, g, 0));
+    c->graph = g;
+    c->graph_launches = c->launches - l0;
+    c->launches = l0;
     return CS_OK;
 }
 
 int cs_gpu_step(cs_gpu_ctx* c, double t, int run)
 {
-    int r = cs_gpu_infect_sweep(c, t, run);
-    if (r) return r;
-    return cs_gpu_incub_recovery_sweep(c, t);
+    if (!c) return CS_E_ARG;
+    if (!c->run_started) return set_err(c, CS_E_STATE, "step before begin_run");
+    if (!c->use_graph || c->prof) return step_eager(c, t, run);
+    if (!c->graph_exec) {
+        int r = capture_step(c, t, run);
+        if (r) return r;
+    }
+    DevPop d = c->d;
+    unsigned long long seed = c->seed;
+    for (cudaGraphNode_t nd : c->set_step_nodes) {
+        void* args[] = {&d, &t, &seed};
+        cudaKernelNodeParams kp;
+        CK(cudaGraphKernelNodeGetParams(nd, &kp));
+        kp.kernelParams = args;
+        kp.extra = nullptr;
+        CK(cudaGraphExecKernelNodeSetParams(c->graph_exec, nd, &kp));
+    }
+    CK(cudaGraphLaunch(c->graph_exec, c->stream));
+    c->launches += c->graph_launches;
+    return CS_OK;
+}
+
+int cs_gpu_use_graphs(cs_gpu_ctx* c, int enable)
+{
+    if (!c) return CS_E_ARG;
+    c->use_graph = enable != 0;
+    return CS_OK;
 }
 
 int cs_gpu_set_interventions(cs_gpu_ctx* c, const cs_interventions* iv)

@@ -379,8 +379,12 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* ctx, double t, int run);
 int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* ctx, double t);
 /* Drop-in for UpdateProbs(do_place)     (src/CovidSim.cpp:2752-2802). */
 int cs_gpu_update_probs(cs_gpu_ctx* ctx, int do_place);
-/* One full model timestep: the two sweeps back to back. */
+/* One full model timestep: the two sweeps back to back.  The first call captures
+ * the timestep's kernels as a CUDA graph and later calls replay it (unless
+ * cs_gpu_use_graphs(ctx, 0) or per-kernel profiling is on); results are the same
+ * either way. */
 int cs_gpu_step(cs_gpu_ctx* ctx, double t, int run);
+int cs_gpu_use_graphs(cs_gpu_ctx* ctx, int enable);
 
 int cs_gpu_set_interventions(cs_gpu_ctx* ctx, const cs_interventions* iv);
 /* DoPlaceClose (src/Update.cpp:1095-1258) for every place of type t in the listed

@@ -672,9 +672,33 @@ static void rebuild_block_tables(cs_cpu_ctx* c)
 }
 
 /* --------------------------------------------------------- UpdateProbs -- */
-/* UpdateProbs (src/CovidSim.cpp:2752-2802): S0 per cell, tot_prob = sum_m S0_m Kmax /
- * sum_m n_m Kmax with Kmax = (float)num(dist2_cc_min).  Sums run in 32 interleaved
- * partial sums folded pairwise (the order the GPU warp uses), in double. */
+/* Kmax between source row yl and target row ym at column distance dx: the
+ * closest-corner rule of dist2_cc_min (src/Dist.cpp:78-144) written in terms of
+ * (dx, yl, ym), which is all the distance depends on. */
+static double row_kernel(const cs_cpu_ctx* c, int dx, int yl, int ym, int64_t* err)
+{
+    const cs_params* P = &c->P;
+    int y1 = yl, y2 = ym;
+    if (ym > yl) y1 = yl + 1;
+    else if (ym < yl) y2 = ym + 1;
+    double d2;
+    if (P->DoUTM_coords) {
+        int cx = (dx == 0) ? 0 : ((P->cell_width * (double)dx > ORACLE_PI) ? dx + 1 : dx - 1);
+        d2 = dist2_utm(P, 0.0, P->cell_height * (double)y1, P->cell_width * (double)cx, P->cell_height * (double)y2);
+    } else {
+        int cx = (dx == 0) ? 0 : (((P->DoPeriodicBoundaries) && (P->cell_width * (double)dx > P->width_deg * 0.5)) ? dx + 1 : dx - 1);
+        int dy = abs(ym - yl), cy = (dy == 0) ? 0 : dy - 1;
+        if ((P->DoPeriodicBoundaries) && (P->height_deg * (double)dy > P->height_deg * 0.5)) cy = dy + 1;
+        d2 = periodic_xy(P, P->cell_width * (double)cx, P->cell_height * (double)cy);
+    }
+    return (double)(float)knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta, d2, err);
+}
+
+/* UpdateProbs (src/CovidSim.cpp:2752-2802): S0 per cell, then
+ * tot_prob = sum_m S0_m Kmax(l,m) / sum_m n_m Kmax(l,m) with
+ * Kmax = (float)num(dist2_cc_min), summed in double in a fixed order: over target
+ * rows ym ascending, each row's sum over target columns xm ascending formed first;
+ * zero terms are skipped (adding +0.0 changes nothing). */
 int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
 {
     const cs_params* P = &c->P;
@@ -689,20 +713,41 @@ int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
             }
         } else c->S0[j] = c->S[j];
     }
-    for (int l = 0; l < c->NC; l++) {
-        double a[32], b[32];
-        for (int k = 0; k < 32; k++) a[k] = b[k] = 0.0;
-        for (int m = 0; m < c->NC; m++) {
-            double kf = (double)(float)knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta,
-                                           cs_cpu_dist2_cc_min(P, c->cell_grid[l], c->cell_grid[m]), &err);
-            int n = c->cell_start[m + 1] - c->cell_start[m];
-            a[m & 31] = a[m & 31] + (double)c->S0[m] * kf;
-            b[m & 31] = b[m & 31] + (double)n * kf;
-        }
-        for (int off = 16; off >= 1; off >>= 1)
-            for (int k = 0; k < off; k++) { a[k] = a[k] + a[k + off]; b[k] = b[k] + b[k + off]; }
-        c->tot_prob[l] = (b[0] > 0) ? a[0] / b[0] : 0.0;
+    int ncw = P->ncw, nch = P->nch;
+    size_t G = (size_t)ncw * nch;
+    double* S0g = (double*)calloc(G, sizeof(double));
+    double* Ng = (double*)calloc(G, sizeof(double));
+    double* krow = (double*)malloc(sizeof(double) * ncw);
+    for (int m = 0; m < c->NC; m++) {
+        S0g[c->cell_grid[m]] = (double)c->S0[m];
+        Ng[c->cell_grid[m]] = (double)(c->cell_start[m + 1] - c->cell_start[m]);
     }
+    for (int l = 0; l < c->NC; l++) {
+        int xl = c->cell_grid[l] / nch, yl = c->cell_grid[l] % nch;
+        double A = 0.0, B = 0.0;
+        for (int ym = 0; ym < nch; ym++) {
+            int anyS = 0, anyN = 0;
+            for (int xm = 0; xm < ncw; xm++) {
+                anyS |= S0g[(size_t)xm * nch + ym] != 0.0;
+                anyN |= Ng[(size_t)xm * nch + ym] != 0.0;
+            }
+            if (!anyS && !anyN) continue;
+            for (int k = 0; k < ncw; k++) krow[k] = row_kernel(c, k, yl, ym, &err);
+            double s = 0.0, sb = 0.0;
+            for (int xm = 0; xm < ncw; xm++) {
+                int dd = xm > xl ? xm - xl : xl - xm;
+                double sv = S0g[(size_t)xm * nch + ym], nv = Ng[(size_t)xm * nch + ym];
+                if (sv != 0.0) s = s + sv * krow[dd];
+                if (nv != 0.0) sb = sb + nv * krow[dd];
+            }
+            if (anyS) A = A + s;
+            if (anyN) B = B + sb;
+        }
+        c->tot_prob[l] = (B > 0) ? A / B : 0.0;
+    }
+    free(S0g);
+    free(Ng);
+    free(krow);
     rebuild_block_tables(c);
     c->C.err_kernel_range += err;
     return CS_OK;

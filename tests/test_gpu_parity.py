@@ -82,3 +82,32 @@ def test_parity_with_interventions():
 def test_parity_planar_coordinates():
     c = _run_pair(tiny_world(utm=0), seed=404, steps=160, check_every=10)
     assert c.cumI > 100
+
+
+def test_parity_graph_replayed_steps():
+    """cs_gpu_step captures the timestep as a CUDA graph on first use and replays it;
+    the replayed steps must give the oracle's state too."""
+    pop, P, g, o = _pair(tiny_world())
+    seeds = g.choose_seeds(505, 20)
+    g.backend.begin_run(505, seeds)
+    o.backend.begin_run(505, seeds)
+    launches0 = g.backend.launches()
+    for k in range(120):
+        t = k * P.ModelTimeStep
+        g.backend.step(t, 0)
+        o.backend.step(t, 0)
+        if k == 60:
+            g.backend.update_probs(0)
+            o.backend.update_probs(0)
+        if k % 30 == 29:
+            _compare(pop, g, o, "graph step %d" % k)
+    assert g.backend.launches() - launches0 >= 120 * 15
+    # a second run on the same context reuses the captured graph
+    g.backend.begin_run(606, seeds)
+    o.backend.begin_run(606, seeds)
+    for k in range(40):
+        g.backend.step(k * P.ModelTimeStep, 0)
+        o.backend.step(k * P.ModelTimeStep, 0)
+    _compare(pop, g, o, "second run")
+    g.close()
+    o.close()
