@@ -141,6 +141,7 @@ def load_library(path=LIB_PATH):
         "cs_gpu_infect_sweep": (I, [V, D, I]),
         "cs_gpu_incub_recovery_sweep": (I, [V, D]),
         "cs_gpu_update_probs": (I, [V, I]),
+        "cs_gpu_update_probs_static": (I, [V, I]),
         "cs_gpu_step": (I, [V, D, I]),
         "cs_gpu_use_graphs": (I, [V, I]),
         "cs_gpu_set_interventions": (I, [V, P(cs_interventions)]),

@@ -71,6 +71,10 @@ class GpuBackend:
     def update_probs(self, do_place=0):
         self._ck(self.lib.cs_gpu_update_probs(self.ctx, do_place), "update_probs")
 
+    def update_probs_static(self, do_place=0):
+        """UpdateProbs with the library's fixed scratch array (no device allocation)."""
+        self._ck(self.lib.cs_gpu_update_probs_static(self.ctx, do_place), "update_probs_static")
+
     def set_params(self, params):
         self._ck(self.lib.cs_gpu_set_params(self.ctx, C.byref(params)), "set_params")
 

@@ -30,6 +30,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "covidsim_b200.h"
@@ -1949,3 +1950,80 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
 }
 
 }  // extern "C"
+
+// ================================================ UpdateProbs without allocation
+// cs_gpu_update_probs_static computes what cs_gpu_update_probs computes, with the
+// same kernels in the same order, but takes its two grid-sized scratch arrays (S0
+// laid out on the cell grid, and the per-cell numerators) and the row-used flags
+// from one file-scope device array instead of the context's allocations.  It is
+// for callers that must not allocate device memory when UpdateProbs runs: a
+// process whose device memory is already reserved by another allocator's pool,
+// where a further allocation fails; and a caller running beside other streams,
+// where freeing scratch would synchronise the whole device.  Nothing in it calls
+// an allocating routine; its limit is the fixed size of that array.
+namespace {
+constexpr size_t kStaticCells = CS_STATIC_MAX_GRID_CELLS;
+constexpr size_t kStaticRows = CS_STATIC_MAX_GRID_ROWS;
+constexpr size_t kStaticBytes = 2 * sizeof(double) * kStaticCells + kStaticRows;
+constexpr int kStaticMaxDevices = 64;
+}  // namespace
+
+// [S0 on the grid: kStaticCells doubles][numerators: kStaticCells doubles][row flags]
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+static std::mutex g_static_mu;
+static void* g_static_base[kStaticMaxDevices];  // device address of the array, per device
+
+extern "C" int cs_gpu_update_probs_static(cs_gpu_ctx* c, int do_place)
+{
+    if (!c) return CS_E_ARG;
+    DevPop& d = c->d;
+    const cs_params& P = c->hp;
+    const size_t G = (size_t)P.ncw * P.nch;
+    if (G > kStaticCells || (size_t)P.nch > kStaticRows)
+        return set_err(c, CS_E_RANGE,
+                       "update_probs_static: %d x %d grid cells exceed its fixed scratch (%zu cells, %zu rows); "
+                       "use cs_gpu_update_probs", P.ncw, P.nch, kStaticCells, kStaticRows);
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev != c->device)
+        return set_err(c, CS_E_STATE, "update_probs_static: device %d is current, the context is on device %d",
+                       dev, c->device);
+    if (dev < 0 || dev >= kStaticMaxDevices)
+        return set_err(c, CS_E_UNSUPPORTED, "update_probs_static: device ordinal %d above %d", dev, kStaticMaxDevices - 1);
+    // set-up, once per device, with that device current: the array's device address
+    void* base;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (!g_static_base[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+            if (e != cudaSuccess || !p)
+                return set_err(c, CS_E_CUDA, "update_probs_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            g_static_base[dev] = p;
+        }
+        base = g_static_base[dev];
+    }
+    double* S0g = (double*)base;
+    double* Ag = S0g + kStaticCells;
+    uint8_t* rowS = (uint8_t*)(Ag + kStaticCells);
+    // The array still holds the previous call's values.  Grid positions without a
+    // populated cell and rows without susceptibles must read zero; the numerators
+    // are written in full by the row kernel.
+    CK(cudaMemsetAsync(S0g, 0, sizeof(double) * G, c->stream));
+    CK(cudaMemsetAsync(rowS, 0, P.nch, c->stream));
+    const int cgrid = (d.NC + kThreads - 1) / kThreads;
+    k_update_S0<<<cgrid, kThreads, 0, c->stream>>>(d, do_place);
+    k_grid_values<<<cgrid, kThreads, 0, c->stream>>>(d, S0g, nullptr, rowS, nullptr);
+    const int tpb = 128;
+    dim3 grid((P.ncw + tpb - 1) / tpb, P.nch);
+    size_t smem = sizeof(double) * 3 * P.ncw;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tot_prob_rows<<<grid, tpb, smem, c->stream>>>(d, S0g, nullptr, rowS, nullptr, Ag, nullptr);
+    k_tot_prob_finish<<<cgrid, kThreads, 0, c->stream>>>(d, Ag, c->Bg);
+    k_block_S0<<<(d.NB + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);
+    k_block_rows<<<(d.NB * 32 + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);
+    c->launches += 6;
+    CK(cudaGetLastError());
+    return CS_OK;
+}

@@ -379,6 +379,20 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* ctx, double t, int run);
 int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* ctx, double t);
 /* Drop-in for UpdateProbs(do_place)     (src/CovidSim.cpp:2752-2802). */
 int cs_gpu_update_probs(cs_gpu_ctx* ctx, int do_place);
+/* No counterpart in the reference.  The same computation as cs_gpu_update_probs,
+ * bit for bit, for callers that must not allocate device memory at that point (a
+ * process whose device memory is reserved by another allocator's pool; a caller
+ * that must not let a free synchronise the device under other streams).  Its
+ * scratch is one fixed array inside the library, 2 x 8 B x CS_STATIC_MAX_GRID_CELLS
+ * + CS_STATIC_MAX_GRID_ROWS bytes (8.0 MiB), per device; grids with more cells or
+ * rows are rejected with CS_E_RANGE.  The context's device must be current
+ * (CS_E_STATE otherwise).  The first call on a device does the set-up (looking up
+ * the array's device address), so make it before any stream capture.  All calls
+ * on one device share that array: calls that overlap in time, from two contexts
+ * or two streams, race on it and must be serialised by the caller. */
+#define CS_STATIC_MAX_GRID_CELLS 524288
+#define CS_STATIC_MAX_GRID_ROWS 4096
+int cs_gpu_update_probs_static(cs_gpu_ctx* ctx, int do_place);
 /* One full model timestep: the two sweeps back to back.  The first call captures
  * the timestep's kernels as a CUDA graph and later calls replay it (unless
  * cs_gpu_use_graphs(ctx, 0) or per-kernel profiling is on); results are the same
