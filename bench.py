@@ -130,15 +130,13 @@ def kernel_bytes(name, w, n_cells_steps):
     """Algorithmic bytes a kernel moved over the timed region, from the work counters
     (per-unit costs: transition scan 16 B per latent/infectious person, infector
     record 40 B, household member 12 B, place candidate 20 B, spatial draw 33 B,
-    accepted infection 24 B, per-cell counts 24 B)."""
+    accepted infection 24 B, active-list entry 12 B, per-cell counts 16 B)."""
     if name == "k_infector_hh_spatial":
         return 40 * w["work_infectors"] + 12 * w["work_hh_members"]
     if name == "k_infector_places":
         return 20 * w["work_place_candidates"] + 16 * w["work_infectors"]
     if name == "k_spatial":
         return 33 * w["work_spatial_draws"]
-    if name == "k_expand_contacts":
-        return 8 * w["work_spatial_contacts"]
     if name in ("k_apply_infections", "k_partition_S"):
         return 12 * w["work_new_infections"]
     if name == "k_incub_scan":
@@ -147,10 +145,8 @@ def kernel_bytes(name, w, n_cells_steps):
         return 32 * w["work_transitions"]
     if name in ("k_partition_LI", "k_clear_pstep"):
         return 8 * w["work_transitions"]
-    if name == "k_gather_active":
-        return 12 * (w["work_infectors"] + w["work_incub_people"]) + 16 * n_cells_steps
-    if name in ("k_active_counts", "k_scan_reduce", "k_scan_down"):
-        return 8 * n_cells_steps
+    if name == "k_build_active":   # two launches per timestep
+        return 12 * (w["work_infectors"] + w["work_incub_people"]) + 2 * 16 * n_cells_steps
     return None
 
 

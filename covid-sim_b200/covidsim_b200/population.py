@@ -319,7 +319,7 @@ def generate(n_people, grid, sigma=1.2, seed=98798150, blobs=0, blob_share=0.0, 
 
 # ------------------------------------------------------------------ presets
 def preset(name, n_people=None, seed=98798150):
-    """Geography and population of a named workload (see DESIGN.md for the list)."""
+    """Geography and population of a named workload: c0, c1, c1_240, c3 or tiny."""
     if name == "c0":   # 1 M people, 2 x 2 degrees, 240 x 240 cells, 10 x 10 microcells
         grid = make_grid(cell_deg=1.0 / 120, nmcl=10)
         return generate(n_people or 1_000_000, grid, sigma=1.2, seed=seed)

@@ -162,6 +162,25 @@ __device__ __forceinline__ double knum(const DevPop& d, const cs_params& P, doub
     return t;
 }
 
+// KernelLookup::num for a caller that decides later whether the evaluation counts:
+// an out-of-table distance sets *oor instead of counting an error.
+__device__ __forceinline__ double knum_flag(const DevPop& d, const cs_params& P, double r2, int* oor)
+{
+    double t = r2 / P.kernel_delta;
+    if (t > P.kernel_size) { *oor = 1; return 0.0; }
+    double s = t * P.kernel_expansion;
+    if (s < P.kernel_size) {
+        t = s - floor(s);
+        t = (1.0 - t) * __ldg(d.khires + (int)s) + t * __ldg(d.khires + (int)(s + 1.0));
+    } else {
+        int i0 = (int)t, i1 = (int)(t + 1.0);
+        if (i1 > P.kernel_size) i1 = P.kernel_size;
+        s = t - floor(t);
+        t = (1.0 - s) * __ldg(d.klookup + i0) + s * __ldg(d.klookup + i1);
+    }
+    return t;
+}
+
 // dist2UTM (src/Dist.cpp:23-48).
 __device__ inline double dist2_utm(const cs_params& P, double x1, double y1, double x2, double y2)
 {

@@ -129,20 +129,19 @@ struct DevPop {
     int32_t* counts;           // [8] device-side sizes (see kCnt*)
     int32_t* touched;          // [NC] cells whose lists change this phase
     uint8_t* cell_flag;        // [NC]
-    int32_t* act_ofs;          // [NC+1] exclusive scan of per-cell active counts
     int32_t* act;              // [N] active people (infectors / latent+infectious)
     int32_t* act_cell;         // [N]
-    int32_t* cnt;              // [N] spatial contacts per infector
-    int32_t* cnt_ofs;          // [N+1]
-    int32_t* cmap;             // [N] infector slot of each spatial contact
+    int32_t* cnt;              // [NC] per-cell moves of the current phase (zero between phases)
+    int32_t* cnt_ofs;          // [N] first contact-map entry of each active infector
+    int32_t* cmap;             // [2N] active-list index of the infector owning each spatial contact
     int32_t cmap_cap;
     uint8_t* act_closed;       // [N] infector's place-closed-and-absent flag
+    int2* place_work;          // [N * NPT] (active index << 3 | place type, place) of each place pass
     uint8_t* hh_flag;          // [NH] deferred household actions
     int32_t* hh_list;          // [NH]
-    int32_t* scan_tmp;         // scan block sums
     cs_counters* C;
 };
 
-enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntEvents = 5, kCntN = 8 };
+enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntPlaceWork = 5, kCntEvents = 6, kCntN = 8 };
 
 }  // namespace csb

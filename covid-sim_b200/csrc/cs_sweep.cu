@@ -8,14 +8,18 @@
 // replayed as a CUDA graph):
 //
 //   InfectSweep
-//     k_active_counts + scan + k_gather_active  infectious people of every cell
-//     k_infectors        household + place passes, spatial Poisson count per infector
-//     scan + k_spatial   one thread per spatial contact: block proposal + rejection
-//     k_apply_infections DoInfect for every claimed person (lowest key wins)
-//     k_partition_S      S -> L cell-list moves, one thread per touched cell
+//     k_build_active         infectious people of every cell, one list
+//     k_infector_hh_spatial  household pass and spatial Poisson count per infector;
+//                            reserves each infector's entries of the contact map
+//     k_infector_places      place passes, one thread per (infector, place type)
+//     k_spatial              spatial contacts: block proposal + rejection, eight
+//                            draws of a contact evaluated together
+//     k_apply_infections     DoInfect for every claimed person (lowest key wins)
+//     k_partition_S          S -> L cell-list moves, one thread per touched cell
 //   IncubRecoverySweep
-//     k_active_counts + scan + k_gather_active  latent + infectious people
-//     k_incub_events     DoIncub / DoCase / severity / recovery / death per person
+//     k_build_active         latent + infectious people
+//     k_incub_scan           the people with an event this step
+//     k_incub_events         DoIncub / DoCase / severity / recovery / death per person
 //     k_partition_LI     L -> I and I -> R/D cell-list moves per touched cell
 //     k_household_after  deferred adult-carer absence and household quarantine
 //
@@ -25,6 +29,8 @@
 // in a fixed order.  Results therefore do not depend on launch geometry.
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+#include <cooperative_groups/scan.h>
 
 #include <cstdarg>
 #include <cstdio>
@@ -45,6 +51,16 @@ using namespace csb;
 
 __device__ __forceinline__ void cnt_add(unsigned long long* p, long long v) { atomicAdd(p, (unsigned long long)v); }
 
+// Adds every calling thread's v with one atomic per warp, skipping zero sums: the
+// end-of-kernel work tallies would otherwise put one atomic per thread on a
+// single address.
+__device__ __forceinline__ void cnt_add_warp(unsigned long long* p, long long v)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    long long sum = cg::reduce(g, v, cg::plus<long long>());
+    if (g.thread_rank() == 0 && sum != 0) atomicAdd(p, (unsigned long long)sum);
+}
+
 // Warp-aggregated append to a device list.
 __device__ __forceinline__ int32_t append(int32_t* count)
 {
@@ -53,6 +69,18 @@ __device__ __forceinline__ int32_t append(int32_t* count)
     if (g.thread_rank() == 0) base = atomicAdd(count, (int32_t)g.size());
     base = g.shfl(base, 0);
     return base + (int32_t)g.thread_rank();
+}
+
+// Reserves n consecutive entries of a device list for each calling thread, with
+// one atomic per warp; returns the first entry's index.
+__device__ __forceinline__ int32_t reserve(int32_t* count, int32_t n)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    int32_t incl = cg::inclusive_scan(g, n);
+    int32_t base = 0;
+    if (g.thread_rank() == g.size() - 1) base = atomicAdd(count, incl);
+    base = g.shfl(base, g.size() - 1);
+    return base + incl - n;
 }
 
 __device__ __forceinline__ void mark_cell(const DevPop& d, int c)
@@ -74,88 +102,6 @@ __device__ __forceinline__ bool flag_household(const DevPop& d, int h, uint8_t f
 }
 
 constexpr int kThreads = 256;
-
-// ----------------------------------------------------------------- scans
-// Exclusive scan of n int32 (n read from *n_dev when given) into out[0..n],
-// out[n] = total (also written to *total_dev when given).  Fixed grid of
-// kScanBlocks blocks, each scanning one contiguous chunk.
-constexpr int kScanBlocks = 1024;
-
-__global__ void k_scan_reduce(const int32_t* __restrict__ in, int n_host, const int32_t* n_dev, int32_t* sums)
-{
-    int n = n_dev ? *n_dev : n_host;
-    long long chunk = ((long long)n + gridDim.x - 1) / gridDim.x;
-    long long s = blockIdx.x * chunk, e = min((long long)n, s + chunk);
-    int32_t acc = 0;
-    for (long long i = s + threadIdx.x; i < e; i += blockDim.x) acc += in[i];
-    __shared__ int32_t red[32];
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        int32_t v = (threadIdx.x < blockDim.x / 32) ? red[threadIdx.x] : 0;
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) sums[blockIdx.x] = v;
-    }
-}
-
-__global__ void k_scan_top(int32_t* sums, int nb, int32_t* out, int n_host, const int32_t* n_dev, int32_t* total_dev)
-{
-    // one block of 1024 threads, nb <= 1024
-    __shared__ int32_t sh[1024];
-    int t = threadIdx.x;
-    int32_t v = (t < nb) ? sums[t] : 0;
-    sh[t] = v;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        int32_t x = (t >= o) ? sh[t - o] : 0;
-        __syncthreads();
-        sh[t] += x;
-        __syncthreads();
-    }
-    if (t < nb) sums[t] = sh[t] - v;  // exclusive
-    if (t == 1023) {
-        int n = n_dev ? *n_dev : n_host;
-        out[n] = sh[1023];
-        if (total_dev) *total_dev = sh[1023];
-    }
-}
-
-__global__ void k_scan_down(const int32_t* __restrict__ in, int32_t* __restrict__ out, int n_host, const int32_t* n_dev, const int32_t* sums)
-{
-    int n = n_dev ? *n_dev : n_host;
-    long long chunk = ((long long)n + gridDim.x - 1) / gridDim.x;
-    long long s = blockIdx.x * chunk, e = min((long long)n, s + chunk);
-    int32_t carry = sums[blockIdx.x];
-    __shared__ int32_t warp_tot[32];
-    __shared__ int32_t tile_tot;
-    for (long long base = s; base < e; base += blockDim.x) {
-        long long i = base + threadIdx.x;
-        int32_t v = (i < e) ? in[i] : 0;
-        int32_t x = v;
-        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        for (int o = 1; o < 32; o <<= 1) {
-            int32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) warp_tot[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            int32_t t = (lane < (int)(blockDim.x / 32)) ? warp_tot[lane] : 0;
-            int32_t tt = t;
-            for (int o = 1; o < 32; o <<= 1) {
-                int32_t y = __shfl_up_sync(0xffffffffu, tt, o);
-                if (lane >= o) tt += y;
-            }
-            warp_tot[lane] = tt - t;
-            if (lane == 31) tile_tot = tt;
-        }
-        __syncthreads();
-        if (i < e) out[i] = carry + warp_tot[w] + x - v;
-        carry += tile_tot;
-        __syncthreads();
-    }
-}
 
 // ------------------------------------------------------------- contexts
 struct cs_gpu_ctx {
@@ -273,14 +219,6 @@ static int dupload(cs_gpu_ctx* c, T** p, const T* src, size_t n)
     return CS_OK;
 }
 
-static int scan_excl(cs_gpu_ctx* c, const int32_t* in, int32_t* out, int n_host, const int32_t* n_dev, int32_t* total_dev)
-{
-    LAUNCH(k_scan_reduce, kScanBlocks, kThreads, in, n_host, n_dev, c->d.scan_tmp);
-    LAUNCH(k_scan_top, 1, 1024, c->d.scan_tmp, kScanBlocks, out, n_host, n_dev, total_dev);
-    LAUNCH(k_scan_down, kScanBlocks, kThreads, in, out, n_host, n_dev, c->d.scan_tmp);
-    return CS_OK;
-}
-
 extern "C" {
 static int tot_prob_pass(cs_gpu_ctx* c, bool denominators);
 }
@@ -377,9 +315,10 @@ __global__ void k_update_S0(DevPop d, int do_place)
 // between two cells depends only on their column distance |dx| and their two rows,
 // so a block owning source row yl and a run of source columns evaluates the
 // kernel once per (target row ym, |dx|) into shared memory and every thread sums
-// its own source cell from there.  Order of summation (restated by the oracle):
+// its own source cells from there.  Order of summation (restated by the oracle):
 //   A_l = sum over ym ascending of ( sum over xm ascending of S0(xm,ym) * G(|xm-xl|) ),
-// products exact in double, zero terms skipped (adding +0.0 changes nothing).
+// the inner sum by fused multiply-adds (one rounding per term), zero terms
+// skipped (adding +0.0 changes nothing).
 __device__ double row_kernel(const DevPop& d, const cs_params& P, int dx, int yl, int ym, unsigned long long* err)
 {
     int y1 = yl, y2 = ym;
@@ -413,47 +352,130 @@ __global__ void k_grid_values(DevPop d, double* S0g, double* Ng, uint8_t* rowS, 
     }
 }
 
-__global__ void k_tot_prob_rows(DevPop d, const double* S0g, const double* Ng, const uint8_t* rowS, const uint8_t* rowN,
-                                double* Ag, double* Bg)
+// Each thread owns kTotProbCols = 8 consecutive source columns xl0..xl0+7 of
+// source row yl.  Shared memory holds the kernel row mirrored, Gm[off + dx] =
+// G(|dx|), so target column xm of output j reads Gm[off + xm - xl0 - j]: for eight
+// targets xm0..xm0+7 a thread reads one window of 15 values, w[q] =
+// Gm[off - 7 + xm0 - xl0 + q], and does 64 fused multiply-adds from registers.
+// Gm is stored with one pad slot after every 8 values, so the windows of the 16
+// lanes of a half-warp (8 values apart) fall in distinct banks.  Each output's
+// sum still runs over xm ascending; a zero S0 adds +0.0, which changes nothing.
+constexpr int kTotProbCols = 8;
+
+__host__ __device__ constexpr int tp_phys(int i) { return i + (i >> 3); }
+
+struct TotProbGeom {
+    int ncwR;   // target columns rounded up to a multiple of 8 (tail S0 = 0)
+    int off;    // Gm index of dx = 0: ncwR + 7, so off - 7 is a multiple of 8
+    int gphys;  // doubles in the padded Gm array
+    size_t smem(bool denominators) const
+    {
+        return sizeof(double) * ((size_t)gphys + (denominators ? 2 : 1) * (size_t)ncwR);
+    }
+};
+
+static TotProbGeom tot_prob_geom(int ncw)
+{
+    TotProbGeom g;
+    g.ncwR = (ncw + kTotProbCols - 1) / kTotProbCols * kTotProbCols;
+    g.off = g.ncwR + 7;
+    g.gphys = tp_phys(g.off + g.ncwR) + 2;
+    g.gphys += g.gphys & 1;   // keep the arrays after Gm 16-byte aligned
+    return g;
+}
+
+template <bool kDenominators>
+__global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S0g, const double* Ng,
+                                                       const uint8_t* rowS, const uint8_t* rowN,
+                                                       double* Ag, double* Bg, TotProbGeom gm)
 {
     const cs_params& P = *d.P;
     const int ncw = P.ncw, nch = P.nch;
-    extern __shared__ double sh[];
-    double* G = sh;
-    double* Srow = sh + ncw;
-    double* Nrow = Srow + ncw;
-    const int xl = blockIdx.x * blockDim.x + threadIdx.x, yl = blockIdx.y;
-    const bool want_b = Ng != nullptr;
-    double A = 0.0, B = 0.0;
+    extern __shared__ __align__(16) double sh[];
+    double* Gp = sh;                  // padded, mirrored kernel row
+    double* Srow = sh + gm.gphys;     // ncwR
+    double* Nrow = Srow + gm.ncwR;    // ncwR (denominator pass only)
+    const int xl0 = (blockIdx.x * blockDim.x + threadIdx.x) * kTotProbCols, yl = blockIdx.y;
+    for (int k = threadIdx.x; k < gm.gphys; k += blockDim.x) Gp[k] = 0.0;
+    for (int k = ncw + threadIdx.x; k < gm.ncwR; k += blockDim.x) {
+        Srow[k] = 0.0;
+        if (kDenominators) Nrow[k] = 0.0;
+    }
+    double A[kTotProbCols], B[kTotProbCols];
+#pragma unroll
+    for (int j = 0; j < kTotProbCols; j++) A[j] = B[j] = 0.0;
+    // window start of this thread for xm0 = 0, in padded units: phys(off - 7 - xl0 + q)
+    // = 9 * (off - 7 - xl0) / 8 + q + q / 8, with off - 7 - xl0 a multiple of 8
+    const int t0 = 9 * ((gm.off - 7 - xl0) / 8);
     for (int ym = 0; ym < nch; ym++) {
-        bool useS = rowS[ym] != 0, useN = want_b && rowN[ym] != 0;
+        const bool useS = rowS[ym] != 0, useN = kDenominators && rowN[ym] != 0;
         if (!useS && !useN) continue;
         __syncthreads();
         for (int k = threadIdx.x; k < ncw; k += blockDim.x) {
-            G[k] = row_kernel(d, P, k, yl, ym, CSB_CTR(err_kernel_range));
+            double v = row_kernel(d, P, k, yl, ym, CSB_CTR(err_kernel_range));
+            Gp[tp_phys(gm.off + k)] = v;
+            Gp[tp_phys(gm.off - k)] = v;
             Srow[k] = S0g[(size_t)k * nch + ym];
-            if (want_b) Nrow[k] = Ng[(size_t)k * nch + ym];
+            if (kDenominators) Nrow[k] = Ng[(size_t)k * nch + ym];
         }
         __syncthreads();
-        if (xl < ncw) {
-            double s = 0.0, sb = 0.0;
-            for (int xm = 0; xm < ncw; xm++) {
-                int dd = xm > xl ? xm - xl : xl - xm;
-                double sv = Srow[xm];
-                if (useS && sv != 0.0) s = s + sv * G[dd];
-                if (useN) {
-                    double nv = Nrow[xm];
-                    if (nv != 0.0) sb = sb + nv * G[dd];
+        if (xl0 < ncw) {
+            double sa[kTotProbCols], sb[kTotProbCols];
+#pragma unroll
+            for (int j = 0; j < kTotProbCols; j++) sa[j] = sb[j] = 0.0;
+            for (int xm0 = 0, t = t0; xm0 < gm.ncwR; xm0 += kTotProbCols, t += 9) {
+                double w[2 * kTotProbCols - 1];
+#pragma unroll
+                for (int q = 0; q < 2 * kTotProbCols - 1; q++) w[q] = Gp[t + q + (q >> 3)];
+                if (useS) {
+                    const double2* s2 = reinterpret_cast<const double2*>(Srow + xm0);
+#pragma unroll
+                    for (int u2 = 0; u2 < kTotProbCols / 2; u2++) {
+                        double2 sv = s2[u2];
+#pragma unroll
+                        for (int j = 0; j < kTotProbCols; j++) sa[j] = fma(sv.x, w[2 * u2 - j + 7], sa[j]);
+#pragma unroll
+                        for (int j = 0; j < kTotProbCols; j++) sa[j] = fma(sv.y, w[2 * u2 + 1 - j + 7], sa[j]);
+                    }
+                }
+                if (kDenominators && useN) {
+                    const double2* n2 = reinterpret_cast<const double2*>(Nrow + xm0);
+#pragma unroll
+                    for (int u2 = 0; u2 < kTotProbCols / 2; u2++) {
+                        double2 nv = n2[u2];
+#pragma unroll
+                        for (int j = 0; j < kTotProbCols; j++) sb[j] = fma(nv.x, w[2 * u2 - j + 7], sb[j]);
+#pragma unroll
+                        for (int j = 0; j < kTotProbCols; j++) sb[j] = fma(nv.y, w[2 * u2 + 1 - j + 7], sb[j]);
+                    }
                 }
             }
-            if (useS) A = A + s;
-            if (useN) B = B + sb;
+#pragma unroll
+            for (int j = 0; j < kTotProbCols; j++) {
+                if (useS) A[j] = A[j] + sa[j];
+                if (kDenominators && useN) B[j] = B[j] + sb[j];
+            }
         }
     }
-    if (xl < ncw) {
-        Ag[(size_t)xl * nch + yl] = A;
-        if (want_b) Bg[(size_t)xl * nch + yl] = B;
+#pragma unroll
+    for (int j = 0; j < kTotProbCols; j++) {
+        int xl = xl0 + j;
+        if (xl < ncw) {
+            Ag[(size_t)xl * nch + yl] = A[j];
+            if (kDenominators) Bg[(size_t)xl * nch + yl] = B[j];
+        }
     }
+}
+
+// Launch shape of k_tot_prob_rows: ceil(ncw / 8) threads per source row, in
+// blocks of up to 256 threads (whole warps).
+static void tot_prob_launch_shape(int ncw, int nch, dim3* grid, int* threads)
+{
+    int need = (ncw + kTotProbCols - 1) / kTotProbCols;
+    int tpb = ((need + 31) / 32) * 32;
+    if (tpb > 256) tpb = 256;
+    *threads = tpb;
+    *grid = dim3((need + tpb - 1) / tpb, nch);
 }
 
 __global__ void k_tot_prob_finish(DevPop d, const double* Ag, const double* Bg)
@@ -529,19 +551,18 @@ __global__ void k_block_rows(DevPop d)
 }
 
 // ======================================================== active-list build
-// mode 0: infectious people [S+L, S+L+I); mode 1: latent + infectious [S, S+L+I).
-__global__ void k_active_counts(DevPop d, int mode)
-{
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x)
-        d.cnt[c] = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
-}
-
-__global__ void k_gather_active(DevPop d, int mode)
+// The step's active people, cell by cell: infectious, slots [S+L, S+L+I) (mode 0),
+// or latent and infectious, slots [S, S+L+I) (mode 1).  Each cell reserves its
+// entries warp by warp, so the list's order varies from launch to launch; nothing
+// that reads it depends on the order (random streams are keyed by person and
+// contact, conflicting claims resolve by key, tallies are integer sums, and cell
+// lists are reordered by position).
+__global__ void k_build_active(DevPop d, int mode)
 {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
         int base = d.cell_start[c] + d.S[c] + (mode == 0 ? d.L[c] : 0);
         int n = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
-        int o = d.act_ofs[c];
+        int o = reserve(d.counts + kCntAct, n);
         for (int k = 0; k < n; k++) {
             d.act[o + k] = d.slots[base + k];
             d.act_cell[o + k] = c;
@@ -614,7 +635,7 @@ __device__ void place_candidates(const DevPop& d, const cs_params& P, const Step
             if ((sc == 1) || (s.next() < sc)) claim_infection(d, m, i, between ? 2 + pt + CS_MAX_PLACE_TYPES : 2 + pt);
         }
     }
-    cnt_add(CSB_CTR(work_place_candidates), ncand);
+    cnt_add_warp(CSB_CTR(work_place_candidates), ncand);
 }
 
 // Household pass and spatial Poisson count of one infector (src/Sweep.cpp:331-377,
@@ -654,42 +675,53 @@ __global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d)
                 }
             }
         }
+        // the infector's place passes: one work entry per place it attends today
+        int links[CS_MAX_PLACE_TYPES];
+        int nwork = 0;
+        const bool absent_i = host_absent(hi, st.ts);
+        for (int pt = 0; pt < d.NPT; pt++) {
+            links[pt] = P.DoPlaces ? link_of(d, pt, i) : -1;
+            if (links[pt] >= 0 && !absent_i) nwork++;
+        }
+        {
+            int o = reserve(d.counts + kCntPlaceWork, nwork);
+            for (int pt = 0; pt < d.NPT; pt++)
+                if (links[pt] >= 0 && !absent_i) d.place_work[o++] = make_int2((idx << 3) | pt, links[pt]);
+        }
         int k = 0;
         uint8_t closed_i = 0;
         if (st.sp_beta > 0) {
             double si = calc_spatial_inf(hi, P, st.ts);
             bool closed = false;
-            if (P.DoPlaces)
-                for (int pt = 0; (pt < d.NPT) && (!closed); pt++) {
-                    int lk = link_of(d, pt, i);
-                    if (lk >= 0) closed = place_closed(d, pt, lk, st.ts);
-                }
+            for (int pt = 0; (pt < d.NPT) && (!closed); pt++)
+                if (links[pt] >= 0) closed = place_closed(d, pt, links[pt], st.ts);
             if (closed && host_absent(hi, st.ts)) { si *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL]; closed_i = 1; }
             double lambda = si * st.sp_beta * d.tot_prob[ci];
             Stream s(seed, CS_RNG_SPATIAL_COUNT, (uint32_t)st.ts, (uint32_t)i, 0);
             k = sample_poisson(s, lambda, CSB_CTR(err_spatial_tries));
         }
-        d.cnt[idx] = k;
+        // this infector's contacts take entries [o, o + k) of the contact map
+        int o = reserve(d.counts + kCntContacts, k);
+        d.cnt_ofs[idx] = o;
+        for (int jj = 0; jj < k && o + jj < d.cmap_cap; jj++) d.cmap[o + jj] = idx;
         d.act_closed[idx] = closed_i;
     }
-    cnt_add(CSB_CTR(work_hh_members), hh_members);
+    cnt_add_warp(CSB_CTR(work_hh_members), hh_members);
 }
 
-// Place passes (src/Sweep.cpp:379-647): one thread per (infector, place type).
+// Place passes (src/Sweep.cpp:379-647): one thread per (infector, place) work
+// entry, i.e. per place type the infector attends and is not absent from.
 __global__ void __launch_bounds__(kThreads) k_infector_places(DevPop d)
 {
     const cs_params& P = *d.P;
     const StepScalars st = *d.step;
     const uint64_t seed = st.seed;
-    if (!P.DoPlaces || d.NPT == 0) return;
-    long long n = (long long)d.counts[kCntAct] * d.NPT;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        int idx = (int)(t / d.NPT), pt = (int)(t % d.NPT);
+    int n = d.counts[kCntPlaceWork];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        int2 e = d.place_work[t];
+        int idx = e.x >> 3, pt = e.x & 7, link = e.y;
         int i = d.act[idx];
-        int link = link_of(d, pt, i);
-        if (link < 0) continue;
         PersonHot hi = d.hot[i];
-        if (host_absent(hi, st.ts)) continue;
         double PI = st.fp * st.seas * calc_place_inf(hi, P, pt, st.ts);
         if (moverest_differs(d, hi.mcell, d.pl[pt].mcell[link])) PI *= P.MoveRestrEffect;
         if (pt != P.HotelPlaceType) {
@@ -704,39 +736,62 @@ __global__ void __launch_bounds__(kThreads) k_infector_places(DevPop d)
     }
 }
 
-// Contact -> infector map: infector idx writes its own contacts' slots.
-__global__ void k_expand_contacts(DevPop d)
+// Spatial contacts (src/Sweep.cpp:742-856): pick a target block from the infector's
+// block row, a slot uniformly among the block's S0 slots, accept with K(d)/bound,
+// redraw on rejection or a dead target.  Draw t of a contact reads its uniforms
+// from Philox blocks 2t and 2t+1 of the contact's stream, so the draws are
+// independent of one another: kSpatialLanes lanes evaluate draws t0..t0+7
+// together and the lowest accepted one wins, exactly as a sequential loop would.
+constexpr int kSpatialLanes = 8;
+constexpr uint32_t kSpatialBlocksPerDraw = 2;
+
+// One rejection draw; true when accepted (target alive, u < K(d)/bound).
+__device__ __forceinline__ bool spatial_draw(const DevPop& d, const cs_params& P, Stream& s, int b,
+                                             const double* row, const int16_t* guide_row, double total,
+                                             int hh_inf, int& m_out, int& slot_out, int& p_out,
+                                             PersonHot& hp_out, int* oor)
 {
-    int nact = d.counts[kCntAct];
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
-        int o = d.cnt_ofs[idx], k = d.cnt[idx];
-        for (int j = 0; j < k && o + j < d.cmap_cap; j++) d.cmap[o + j] = idx;
-    }
+    // smallest B with target < row[B]: guide-table start, then walk
+    double u1 = s.next();
+    double target = u1 * total;
+    int B = guide_row[min((int)(u1 * (double)d.NB), d.NB - 1)];
+    while (B > 0 && row[B - 1] > target) B--;
+    while (B < d.NB - 1 && !(target < row[B])) B++;
+    long long bS0 = d.block_S0[B];
+    if (bS0 <= 0) return false;
+    double u2 = s.next();
+    double r = floor(u2 * (double)bS0);
+    // smallest cell k in block B with r < cum[k], the same way
+    int kb = d.block_cell_ofs[B], ke = d.block_cell_ofs[B + 1] - 1;
+    int k0 = kb + d.cell_guide[kb + min((int)(u2 * (double)(ke - kb + 1)), ke - kb)];
+    while (k0 > kb && r < (double)d.block_cum[k0 - 1]) k0--;
+    while (k0 < ke && !(r < (double)d.block_cum[k0])) k0++;
+    int m = d.block_cells[k0];
+    int slot = (int)(r - (double)(d.block_cum[k0] - d.S0[m]));
+    int p = d.slots[d.cell_start[m] + slot];
+    PersonHot hp = d.hot[p];
+    double d2 = dist2_hh(d, P, hh_inf, hp.hh);
+    double accept = knum_flag(d, P, d2, oor) / d.block_bound_tab[(size_t)b * d.NB + B];
+    if ((s.next() >= accept) || !is_alive(hp.inf)) return false;
+    m_out = m; slot_out = slot; p_out = p; hp_out = hp;
+    return true;
 }
 
-// One thread per spatial contact (src/Sweep.cpp:742-856): pick a target block from
-// the infector's block row, a slot uniformly among the block's S0 slots, accept with
-// K(d)/bound, redraw on rejection or a dead target.
-__global__ void __launch_bounds__(kThreads) k_spatial(DevPop d)
+__global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d)
 {
     const cs_params& P = *d.P;
     const StepScalars st = *d.step;
     const uint64_t seed = st.seed;
     int nact = d.counts[kCntAct];
-    int ncont = d.counts[kCntContacts];
-    long long draws = 0;
-    for (int cidx = blockIdx.x * blockDim.x + threadIdx.x; cidx < ncont; cidx += gridDim.x * blockDim.x) {
-        // infector owning contact cidx: from the map, else last idx with cnt_ofs[idx] <= cidx
-        int idx;
-        if (cidx < d.cmap_cap) idx = d.cmap[cidx];
-        else {
-            int lo = 0, hi = nact - 1;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (d.cnt_ofs[mid] <= cidx) lo = mid; else hi = mid - 1;
-            }
-            idx = lo;
-        }
+    int nres = d.counts[kCntContacts];
+    int ncont = min(nres, d.cmap_cap);   // contacts beyond the map are counted as overflow
+    auto tile = cg::tiled_partition<kSpatialLanes>(cg::this_thread_block());
+    const int lane = (int)tile.thread_rank();
+    const int group = (blockIdx.x * blockDim.x + threadIdx.x) / kSpatialLanes;
+    const int ngroups = (gridDim.x * blockDim.x) / kSpatialLanes;
+    long long draws = 0, oor_count = 0, give_ups = 0;
+    for (int cidx = group; cidx < ncont; cidx += ngroups) {
+        int idx = d.cmap[cidx];            // the infector owning contact cidx
         int j = cidx - d.cnt_ofs[idx];
         int i = d.act[idx], ci = d.act_cell[idx];
         bool closed_i = d.act_closed[idx] != 0;
@@ -745,60 +800,53 @@ __global__ void __launch_bounds__(kThreads) k_spatial(DevPop d)
         const double* row = d.block_row_cum + (size_t)b * d.NB;
         const int16_t* guide_row = d.block_guide + (size_t)b * d.NB;
         double total = row[d.NB - 1];
-        if (!(total > 0)) { cnt_add(CSB_CTR(err_spatial_tries), 1); continue; }
+        if (!(total > 0)) { if (lane == 0) give_ups++; continue; }
+        int m = 0, slot = 0, p = 0, won = -1;
+        PersonHot hp;
         Stream s(seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)st.ts, (uint32_t)i, (uint32_t)j);
-        int iag = age_group(hinf);
-        for (int tries = 0;; tries++) {
-            if (tries >= kMaxSpatialTries) { cnt_add(CSB_CTR(err_spatial_tries), 1); break; }
-            draws++;
-            // smallest B with target < row[B]: guide-table start, then walk
-            double u1 = s.next();
-            double target = u1 * total;
-            int B = guide_row[min((int)(u1 * (double)d.NB), d.NB - 1)];
-            while (B > 0 && row[B - 1] > target) B--;
-            while (B < d.NB - 1 && !(target < row[B])) B++;
-            long long bS0 = d.block_S0[B];
-            if (bS0 <= 0) continue;
-            double u2 = s.next();
-            double r = floor(u2 * (double)bS0);
-            // smallest cell k in block B with r < cum[k], the same way
-            int kb = d.block_cell_ofs[B], ke = d.block_cell_ofs[B + 1] - 1;
-            int k0 = kb + d.cell_guide[kb + min((int)(u2 * (double)(ke - kb + 1)), ke - kb)];
-            while (k0 > kb && r < (double)d.block_cum[k0 - 1]) k0--;
-            while (k0 < ke && !(r < (double)d.block_cum[k0])) k0++;
-            int m = d.block_cells[k0];
-            int slot = (int)(r - (double)(d.block_cum[k0] - d.S0[m]));
-            int p = d.slots[d.cell_start[m] + slot];
-            PersonHot hp = d.hot[p];
-            double d2 = dist2_hh(d, P, hinf.hh, hp.hh);
-            double accept = knum(d, P, d2, CSB_CTR(err_kernel_range)) / d.block_bound_tab[(size_t)b * d.NB + B];
-            if ((s.next() >= accept) || !is_alive(hp.inf)) continue;
-            if ((ci != m) || (hp.hh != hinf.hh)) {
-                double ss = calc_spatial_susc(d, hp, P, st.ts);
-                if (is_ch(hp) || is_ch(hinf)) ss *= P.CareHomeResidentSpatialScaling;
-                if (slot < d.S[m]) {
-                    ss *= calc_person_susc(hp, iag, P);
-                    ss *= P.WAIFW_Matrix_SpatialOnly[age_group(hp)][iag];
-                    if (moverest_differs(d, hp.mcell, hinf.mcell)) ss *= P.MoveRestrEffect;
-                    if ((!closed_i) && host_absent(hp, st.ts)) {
-                        bool f = false;
-                        for (int pt = 0; (pt < d.NPT) && (!f); pt++) {
-                            int lk = link_of(d, pt, p);
-                            if (lk >= 0) f = place_closed(d, pt, lk, st.ts);
-                        }
-                        if (f) ss *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL];
+        for (int t0 = 0; t0 < kMaxSpatialTries; t0 += kSpatialLanes) {
+            int t = t0 + lane, oor = 0;
+            s = Stream(seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)st.ts, (uint32_t)i, (uint32_t)j);
+            s.block = kSpatialBlocksPerDraw * (uint32_t)t;
+            bool acc = (t < kMaxSpatialTries) && spatial_draw(d, P, s, b, row, guide_row, total, hinf.hh,
+                                                              m, slot, p, hp, &oor);
+            unsigned mask = tile.ballot(acc);
+            int w = mask ? __ffs(mask) - 1 : kSpatialLanes;
+            if (lane < w) oor_count += oor;   // draws up to the winner count, as in a sequential loop
+            if (lane == w) oor_count += oor;
+            if (mask) { won = t0 + w; break; }
+        }
+        if (lane == 0) draws += (won >= 0) ? won + 1 : kMaxSpatialTries;
+        if (won < 0) { if (lane == 0) give_ups++; continue; }
+        if (lane != won % kSpatialLanes) continue;
+        if ((ci != m) || (hp.hh != hinf.hh)) {
+            int iag = age_group(hinf);
+            double ss = calc_spatial_susc(d, hp, P, st.ts);
+            if (is_ch(hp) || is_ch(hinf)) ss *= P.CareHomeResidentSpatialScaling;
+            if (slot < d.S[m]) {
+                ss *= calc_person_susc(hp, iag, P);
+                ss *= P.WAIFW_Matrix_SpatialOnly[age_group(hp)][iag];
+                if (moverest_differs(d, hp.mcell, hinf.mcell)) ss *= P.MoveRestrEffect;
+                if ((!closed_i) && host_absent(hp, st.ts)) {
+                    bool f = false;
+                    for (int pt = 0; (pt < d.NPT) && (!f); pt++) {
+                        int lk = link_of(d, pt, p);
+                        if (lk >= 0) f = place_closed(d, pt, lk, st.ts);
                     }
-                    if ((ss == 1) || (s.next() < ss))
-                        if (hp.inf == CS_INF_SUSCEPTIBLE) claim_infection(d, p, i, 2 + 2 * CS_MAX_PLACE_TYPES);
+                    if (f) ss *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL];
                 }
+                if ((ss == 1) || (s.next() < ss))
+                    if (hp.inf == CS_INF_SUSCEPTIBLE) claim_infection(d, p, i, 2 + 2 * CS_MAX_PLACE_TYPES);
             }
-            break;
         }
     }
-    cnt_add(CSB_CTR(work_spatial_draws), draws);
+    cnt_add_warp(CSB_CTR(work_spatial_draws), draws);
+    cnt_add_warp(CSB_CTR(err_kernel_range), oor_count);
+    cnt_add_warp(CSB_CTR(err_spatial_tries), give_ups);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         cnt_add(CSB_CTR(work_infectors), nact);
         cnt_add(CSB_CTR(work_spatial_contacts), ncont);
+        if (nres > ncont) cnt_add(CSB_CTR(err_queue_overflow), nres - ncont);
     }
 }
 
@@ -810,6 +858,8 @@ __global__ void k_apply_infections(DevPop d)
     const int ts = d.step->ts;
     const uint64_t seed = d.step->seed;
     int nq = d.counts[kCntQueue];
+    // single-address tallies, summed per thread and added once per warp
+    long long n_inf = 0, n_kw = 0, n_tg = 0, sum_tg = 0, sum_si = 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
         int p = d.queue[q];
         unsigned long long key = d.claim[p];
@@ -830,10 +880,10 @@ __global__ void k_apply_infections(DevPop d)
         d.mark[d.cell_start[cell] + d.listpos[p]] = 1;
         atomicAdd(d.cnt + cell, 1);  // transitions out of this cell's S block
         mark_cell(d, cell);
-        cnt_add(CSB_CTR(cumI), 1);
+        n_inf++;
         cnt_add(CSB_CTR(cumItype[it % CS_INFECT_TYPE_MASK]), 1);
         cnt_add(CSB_CTR(cumIa[age_group(h)]), 1);
-        cnt_add(CSB_CTR(cumI_keyworker[(h.pflags & CS_PF_KEYWORKER) ? 1 : 0]), 1);
+        if (h.pflags & CS_PF_KEYWORKER) n_kw++;
         int ad = d.mcell_adunit[h.mcell];
         if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumI_adunit[ad]), 1);
         if (P.DoLatent) {
@@ -846,11 +896,17 @@ __global__ void k_apply_infections(DevPop d)
             h.latent_time = (uint16_t)(t * P.TimeStepsPerDay);
         d.hot[p] = h;
         if (infector >= 0) {
-            cnt_add(CSB_CTR(cumTG), ((int)(uint16_t)ts) - ((int)d.infection_time[infector]));
-            cnt_add(CSB_CTR(cumSI), ((int)h.latent_time) - ((int)d.hot[infector].latent_time));
-            cnt_add(CSB_CTR(nTG), 1);
+            sum_tg += ((int)(uint16_t)ts) - ((int)d.infection_time[infector]);
+            sum_si += ((int)h.latent_time) - ((int)d.hot[infector].latent_time);
+            n_tg++;
         }
     }
+    cnt_add_warp(CSB_CTR(cumI), n_inf);
+    cnt_add_warp(CSB_CTR(cumI_keyworker[1]), n_kw);
+    cnt_add_warp(CSB_CTR(cumI_keyworker[0]), n_inf - n_kw);
+    cnt_add_warp(CSB_CTR(cumTG), sum_tg);
+    cnt_add_warp(CSB_CTR(cumSI), sum_si);
+    cnt_add_warp(CSB_CTR(nTG), n_tg);
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_new_infections), nq);
 }
 
@@ -1364,6 +1420,8 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     DevPop& d = c->d;
     d.N = pop->n_people; d.NH = pop->n_households; d.NC = pop->n_cells; d.NM = pop->n_mcells; d.NPT = pop->num_place_types;
     size_t N = d.N, NH = d.NH, NC = d.NC, NM = d.NM, NPT = d.NPT;
+    if (d.NPT < 0 || d.NPT > CS_MAX_PLACE_TYPES) return set_err(c, CS_E_ARG, "num_place_types out of range");
+    if (N >= (1u << 28)) return set_err(c, CS_E_UNSUPPORTED, "at most 2^28 - 1 people (place work entries pack index << 3)");
     if (N == 0 || NC == 0) return set_err(c, CS_E_ARG, "empty population");
     // people
     std::vector<PersonHot> hot(N);
@@ -1471,14 +1529,15 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         AL(c->rowS, (size_t)params->nch); AL(c->rowN, (size_t)params->nch);
     }
     AL(d.claim, N); AL(d.queue, N); AL(d.counts, kCntN); AL(d.touched, NC); AL(d.cell_flag, NC + 4);
-    AL(d.act_ofs, NC + 1); AL(d.act, N); AL(d.act_cell, N); AL(d.cnt, N > NC ? N : NC); AL(d.cnt_ofs, N + 1);
-    AL(d.cmap, N); d.cmap_cap = (int32_t)N;
-    AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH); AL(d.scan_tmp, kScanBlocks);
+    AL(d.act, N); AL(d.act_cell, N); AL(d.cnt, NC); AL(d.cnt_ofs, N);
+    AL(d.cmap, 2 * N); d.cmap_cap = (int32_t)(2 * N);
+    AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH);
+    AL(d.place_work, N * (size_t)(NPT > 0 ? NPT : 1));
     CK(cudaMemsetAsync(d.claim, 0xff, sizeof(unsigned long long) * N, c->stream));
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
     CK(cudaMemsetAsync(d.cell_flag, 0, NC + 4, c->stream));
     CK(cudaMemsetAsync(d.hh_flag, 0, NH + 4, c->stream));
-    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * (N > NC ? N : NC), c->stream));
+    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * NC, c->stream));
     CK(cudaMemsetAsync(d.pstep, 0, N, c->stream));
     { cs_params* t; UP(t, params, 1); c->dP = t; d.P = t; }
     { DevIv iv{1e10, 0, 1e10, 0}; DevIv* t; UP(t, &iv, 1); c->dIv = t; d.iv = t; }
@@ -1533,12 +1592,19 @@ static int tot_prob_pass(cs_gpu_ctx* c, bool denominators)
         CK(cudaMemsetAsync(c->rowN, 0, P.nch, c->stream));
     }
     LAUNCH(k_grid_values, (d.NC + kThreads - 1) / kThreads, kThreads, d, c->S0g, denominators ? c->Ng : nullptr, c->rowS, c->rowN);
-    const int tpb = 128;
-    dim3 grid((P.ncw + tpb - 1) / tpb, P.nch);
-    size_t smem = sizeof(double) * 3 * P.ncw;
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid;
+    int tpb;
+    tot_prob_launch_shape(P.ncw, P.nch, &grid, &tpb);
+    const TotProbGeom gm = tot_prob_geom(P.ncw);
+    const size_t smem = gm.smem(denominators);
     if (c->prof) prof_begin(c, "k_tot_prob_rows");
-    k_tot_prob_rows<<<grid, tpb, smem, c->stream>>>(d, c->S0g, denominators ? c->Ng : nullptr, c->rowS, c->rowN, c->Ag, c->Bg);
+    if (denominators) {
+        if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_tot_prob_rows<true><<<grid, tpb, smem, c->stream>>>(d, c->S0g, c->Ng, c->rowS, c->rowN, c->Ag, c->Bg, gm);
+    } else {
+        if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, c->S0g, nullptr, c->rowS, nullptr, c->Ag, nullptr, gm);
+    }
     if (c->prof) prof_end(c);
     c->launches++;
     CK(cudaGetLastError());
@@ -1598,6 +1664,7 @@ int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, i
     c->seed = seed;
     CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
+    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
     LAUNCH(k_reset_people, c->grid, kThreads, d, seed);
     LAUNCH(k_reset_slots, c->grid, kThreads, d);
     LAUNCH(k_reset_listpos, (d.NC + kThreads - 1) / kThreads, kThreads, d);
@@ -1614,14 +1681,13 @@ int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, i
     return cs_gpu_seed_infections(c, 0.0, seed_people, n_seed);
 }
 
-static int gather_active(cs_gpu_ctx* c, int mode)
+static int build_active(cs_gpu_ctx* c, int mode)
 {
     DevPop& d = c->d;
-    LAUNCH(k_active_counts, (d.NC + kThreads - 1) / kThreads, kThreads, d, mode);
-    int r = scan_excl(c, d.cnt, d.act_ofs, d.NC, nullptr, d.counts + kCntAct);
-    if (r) return r;
-    LAUNCH(k_gather_active, (d.NC + kThreads - 1) / kThreads, kThreads, d, mode);
-    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
+    static_assert(kCntContacts == kCntAct + 1 && kCntPlaceWork == kCntAct + 2,
+                  "active, contact and place-work counts are reset together");
+    CK(cudaMemsetAsync(d.counts + kCntAct, 0, sizeof(int32_t) * 3, c->stream));
+    LAUNCH(k_build_active, (d.NC + kThreads - 1) / kThreads, kThreads, d, mode);
     return CS_OK;
 }
 
@@ -1632,15 +1698,11 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
     if (!c->run_started) return set_err(c, CS_E_STATE, "infect_sweep before begin_run");
     DevPop& d = c->d;
     LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
-    int r = gather_active(c, 0);
+    int r = build_active(c, 0);
     if (r) return r;
     LAUNCH(k_infector_hh_spatial, c->grid, kThreads, d);
     LAUNCH(k_infector_places, c->grid, kThreads, d);
-    r = scan_excl(c, d.cnt, d.cnt_ofs, 0, d.counts + kCntAct, d.counts + kCntContacts);
-    if (r) return r;
-    LAUNCH(k_expand_contacts, c->grid, kThreads, d);
     LAUNCH(k_spatial, c->grid, kThreads, d);
-    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * (d.N > d.NC ? d.N : d.NC), c->stream));
     return apply_queue(c);
 }
 
@@ -1650,7 +1712,7 @@ int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* c, double t)
     if (!c->run_started) return set_err(c, CS_E_STATE, "incub_recovery_sweep before begin_run");
     DevPop& d = c->d;
     LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
-    int r = gather_active(c, 1);
+    int r = build_active(c, 1);
     if (r) return r;
     CK(cudaMemsetAsync(d.counts + kCntEvents, 0, sizeof(int32_t), c->stream));
     LAUNCH(k_incub_scan, c->grid, kThreads, d);
@@ -1938,6 +2000,7 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
 #undef UL
     CK(cudaMemsetAsync(d.mark, 0, N, c->stream));
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
+    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
     CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
     c->seed = seed;
     int r = rebuild_blocks(c);
@@ -2015,11 +2078,13 @@ extern "C" int cs_gpu_update_probs_static(cs_gpu_ctx* c, int do_place)
     const int cgrid = (d.NC + kThreads - 1) / kThreads;
     k_update_S0<<<cgrid, kThreads, 0, c->stream>>>(d, do_place);
     k_grid_values<<<cgrid, kThreads, 0, c->stream>>>(d, S0g, nullptr, rowS, nullptr);
-    const int tpb = 128;
-    dim3 grid((P.ncw + tpb - 1) / tpb, P.nch);
-    size_t smem = sizeof(double) * 3 * P.ncw;
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tot_prob_rows<<<grid, tpb, smem, c->stream>>>(d, S0g, nullptr, rowS, nullptr, Ag, nullptr);
+    dim3 grid;
+    int tpb;
+    tot_prob_launch_shape(P.ncw, P.nch, &grid, &tpb);
+    const TotProbGeom gm = tot_prob_geom(P.ncw);
+    const size_t smem = gm.smem(false);
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, S0g, nullptr, rowS, nullptr, Ag, nullptr, gm);
     k_tot_prob_finish<<<cgrid, kThreads, 0, c->stream>>>(d, Ag, c->Bg);
     k_block_S0<<<(d.NB + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);
     k_block_rows<<<(d.NB * 32 + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);

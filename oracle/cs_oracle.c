@@ -697,8 +697,9 @@ static double row_kernel(const cs_cpu_ctx* c, int dx, int yl, int ym, int64_t* e
 /* UpdateProbs (src/CovidSim.cpp:2752-2802): S0 per cell, then
  * tot_prob = sum_m S0_m Kmax(l,m) / sum_m n_m Kmax(l,m) with
  * Kmax = (float)num(dist2_cc_min), summed in double in a fixed order: over target
- * rows ym ascending, each row's sum over target columns xm ascending formed first;
- * zero terms are skipped (adding +0.0 changes nothing). */
+ * rows ym ascending, each row's sum over target columns xm ascending formed first
+ * with fused multiply-adds (one rounding per term); zero terms are skipped
+ * (adding +0.0 changes nothing). */
 int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
 {
     const cs_params* P = &c->P;
@@ -737,8 +738,8 @@ int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
             for (int xm = 0; xm < ncw; xm++) {
                 int dd = xm > xl ? xm - xl : xl - xm;
                 double sv = S0g[(size_t)xm * nch + ym], nv = Ng[(size_t)xm * nch + ym];
-                if (sv != 0.0) s = s + sv * krow[dd];
-                if (nv != 0.0) sb = sb + nv * krow[dd];
+                if (sv != 0.0) s = fma(sv, krow[dd], s);
+                if (nv != 0.0) sb = fma(nv, krow[dd], sb);
             }
             if (anyS) A = A + s;
             if (anyN) B = B + sb;
@@ -962,7 +963,41 @@ static void place_candidates(cs_cpu_ctx* c, int i, int pt, int link, double Pinf
     }
 }
 
-/* Spatial contact j of infector i (src/Sweep.cpp:742-856 for one contact). */
+/* Spatial contact j of infector i (src/Sweep.cpp:742-856 for one contact).
+ * Draw t of the rejection loop reads its uniforms from Philox blocks 2t and 2t+1
+ * of the contact's stream (at most four: target block, slot, acceptance, and for
+ * the accepted draw the susceptibility test), so every draw's numbers are fixed
+ * in advance whatever the earlier draws consumed; the first accepted draw wins. */
+#define SPATIAL_BLOCKS_PER_DRAW 2
+static int spatial_draw(cs_cpu_ctx* c, stream* s, int b, int hi_, const double* row, double total,
+                        int* m_out, int* slot_out, int* p_out, int64_t* err)
+{
+    const cs_params* P = &c->P;
+    double target = stream_next(s) * total;
+    int lo = 0, hi = c->NB - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (target < row[mid]) hi = mid; else lo = mid + 1;
+    }
+    int B = lo;
+    if (c->block_S0[B] <= 0) return 0;
+    double r = floor(stream_next(s) * (double)c->block_S0[B]);
+    int k0 = c->block_cell_ofs[B], k1 = c->block_cell_ofs[B + 1] - 1;
+    while (k0 < k1) {
+        int mid = (k0 + k1) >> 1;
+        if (r < (double)c->block_cum[mid]) k1 = mid; else k0 = mid + 1;
+    }
+    int m = c->block_cells[k0];
+    int slot = (int)(r - (double)(c->block_cum[k0] - c->S0[m]));
+    int p = c->slots[c->cell_start[m] + slot];
+    double d2 = dist2_hh(c, hi_, c->hh[p]);
+    double accept = knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta, d2, err)
+        / block_bound(c, b, B, err);
+    if ((stream_next(s) >= accept) || !is_alive(c, p)) return 0;
+    *m_out = m; *slot_out = slot; *p_out = p;
+    return 1;
+}
+
 static void spatial_contact(cs_cpu_ctx* c, int i, int ci, int j, int closed_i, int ts)
 {
     const cs_params* P = &c->P;
@@ -972,52 +1007,33 @@ static void spatial_contact(cs_cpu_ctx* c, int i, int ci, int j, int closed_i, i
     int64_t err = 0;
     if (!(total > 0)) { c->C.err_spatial_tries++; return; }
     stream s;
-    stream_init(&s, c->seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)ts, (uint32_t)i, (uint32_t)j);
     int hi_ = c->hh[i];
-    for (int tries = 0;; tries++) {
-        if (tries >= MAX_SPATIAL_TRIES) { c->C.err_spatial_tries++; return; }
-        c->C.work_spatial_draws++;
-        double target = stream_next(&s) * total;
-        int lo = 0, hi = c->NB - 1;
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (target < row[mid]) hi = mid; else lo = mid + 1;
-        }
-        int B = lo;
-        if (c->block_S0[B] <= 0) continue;
-        double r = floor(stream_next(&s) * (double)c->block_S0[B]);
-        int k0 = c->block_cell_ofs[B], k1 = c->block_cell_ofs[B + 1] - 1;
-        while (k0 < k1) {
-            int mid = (k0 + k1) >> 1;
-            if (r < (double)c->block_cum[mid]) k1 = mid; else k0 = mid + 1;
-        }
-        int m = c->block_cells[k0];
-        int slot = (int)(r - (double)(c->block_cum[k0] - c->S0[m]));
-        int p = c->slots[c->cell_start[m] + slot];
-        double d2 = dist2_hh(c, hi_, c->hh[p]);
-        double accept = knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta, d2, &err)
-            / block_bound(c, b, B, &err);
-        if ((stream_next(&s) >= accept) || !is_alive(c, p)) continue;
-        if ((ci != m) || (c->hh[p] != hi_)) {
-            double ss = calc_spatial_susc(c, p, ts);
-            if (is_ch(c, p) || is_ch(c, i)) ss *= P->CareHomeResidentSpatialScaling;
-            if (slot < c->S[m]) {
-                ss *= calc_person_susc(c, p, i);
-                ss *= P->WAIFW_Matrix_SpatialOnly[age_group(c, p)][age_group(c, i)];
-                if (moverest_differs(c, c->mcell[p], c->mcell[i])) ss *= P->MoveRestrEffect;
-                if ((!closed_i) && host_absent(c, p, ts)) {
-                    int f = 0;
-                    for (int pt = 0; (pt < c->NPT) && (!f); pt++)
-                        if (link_of(c, pt, p) >= 0) f = place_closed(c, pt, link_of(c, pt, p), ts);
-                    if (f) ss *= P->Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL];
-                }
-                if ((ss == 1) || (stream_next(&s) < ss))
-                    if (c->inf[p] == CS_INF_SUSCEPTIBLE) claim(c, p, i, 2 + 2 * CS_MAX_PLACE_TYPES);
-            }
-        }
-        break;
+    int m = 0, slot = 0, p = 0, t;
+    for (t = 0; t < MAX_SPATIAL_TRIES; t++) {
+        stream_init(&s, c->seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)ts, (uint32_t)i, (uint32_t)j);
+        s.block = (uint32_t)(SPATIAL_BLOCKS_PER_DRAW * t);
+        if (spatial_draw(c, &s, b, hi_, row, total, &m, &slot, &p, &err)) break;
     }
+    c->C.work_spatial_draws += (t < MAX_SPATIAL_TRIES) ? t + 1 : t;
     c->C.err_kernel_range += err;
+    if (t >= MAX_SPATIAL_TRIES) { c->C.err_spatial_tries++; return; }
+    if ((ci != m) || (c->hh[p] != hi_)) {
+        double ss = calc_spatial_susc(c, p, ts);
+        if (is_ch(c, p) || is_ch(c, i)) ss *= P->CareHomeResidentSpatialScaling;
+        if (slot < c->S[m]) {
+            ss *= calc_person_susc(c, p, i);
+            ss *= P->WAIFW_Matrix_SpatialOnly[age_group(c, p)][age_group(c, i)];
+            if (moverest_differs(c, c->mcell[p], c->mcell[i])) ss *= P->MoveRestrEffect;
+            if ((!closed_i) && host_absent(c, p, ts)) {
+                int f = 0;
+                for (int pt = 0; (pt < c->NPT) && (!f); pt++)
+                    if (link_of(c, pt, p) >= 0) f = place_closed(c, pt, link_of(c, pt, p), ts);
+                if (f) ss *= P->Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL];
+            }
+            if ((ss == 1) || (stream_next(&s) < ss))
+                if (c->inf[p] == CS_INF_SUSCEPTIBLE) claim(c, p, i, 2 + 2 * CS_MAX_PLACE_TYPES);
+        }
+    }
 }
 
 /* One infector's household, place and spatial passes (src/Sweep.cpp:314-691). */

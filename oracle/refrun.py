@@ -1,6 +1,6 @@
 """Run the reference executable on a synthetic workload and time its sweeps.
 
-TEST / BASELINE INFRASTRUCTURE: bench.py's reference arm and the statistical parity
+TEST AND CPU-BASELINE INFRASTRUCTURE: bench.py's reference arm and the statistical parity
 tests call this; the product never does.  The workload's population is written in
 the reference's input formats (covidsim_b200.refconfig), the reference builds its
 own households and places from it, and oracle/_ref/CovidSim_timed (the reference

@@ -101,7 +101,7 @@ def test_parity_graph_replayed_steps():
             o.backend.update_probs(0)
         if k % 30 == 29:
             _compare(pop, g, o, "graph step %d" % k)
-    assert g.backend.launches() - launches0 >= 120 * 15
+    assert g.backend.launches() - launches0 >= 120 * 10   # replayed kernels are counted
     # a second run on the same context reuses the captured graph
     g.backend.begin_run(606, seeds)
     o.backend.begin_run(606, seeds)
