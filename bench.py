@@ -222,7 +222,14 @@ def run_ours(args):
     # per-kernel device times: one more realisation of the same workload with every
     # launch bracketed by CUDA events on the sweep's stream (eager launches)
     be.profile(2)
-    s.run(seed=base_seed, days=days, n_seed=n_seed, policy=policy)
+    work_daily = []
+
+    def _daily(step, c):
+        work_daily.append({k: int(getattr(c, k)) for k in ("work_infectors", "work_hh_members", "work_place_candidates",
+                                                            "work_spatial_contacts", "work_spatial_draws",
+                                                            "work_new_infections", "work_transitions",
+                                                            "work_incub_people")})
+    s.run(seed=base_seed, days=days, n_seed=n_seed, policy=policy, callback=_daily)
     be.sync()
     kernels = be.profile_entries()
     be.profile(0)
@@ -250,7 +257,8 @@ def run_ours(args):
         "timing": "CUDA events around each launch on the sweep's stream, over one extra realisation of the workload",
     }
     if args.profile_out and rank == 0:
-        json.dump(dict(rows=rows, work=work, timed_ms=ms, steps=args.steps, workload=args.workload, profiled_runs=prof_runs),
+        json.dump(dict(rows=rows, work=work, work_daily=work_daily, timed_ms=ms, steps=args.steps,
+                       workload=args.workload, profiled_runs=prof_runs),
                   open(args.profile_out, "w"), indent=1)
 
     # end to end through the C ABI with host buffers

@@ -221,7 +221,8 @@ __device__ __forceinline__ double periodic_xy(const cs_params& P, double x, doub
 // dist2(Person*, Person*) (src/Dist.cpp:49-61) between two households.
 __device__ __forceinline__ double dist2_hh(const DevPop& d, const cs_params& P, int32_t ha, int32_t hb)
 {
-    float2 a = __ldg(d.hh_xy + ha), b = __ldg(d.hh_xy + hb);
+    float2 a = __ldg(reinterpret_cast<const float2*>(d.hhr + ha));
+    float2 b = __ldg(reinterpret_cast<const float2*>(d.hhr + hb));
     float ax = a.x, ay = a.y, bx = b.x, by = b.y;
     if (P.DoUTM_coords) return dist2_utm(P, ax, ay, bx, by);
     float dx = ax - bx, dy = ay - by;
@@ -313,8 +314,31 @@ __device__ __forceinline__ bool place_closed(const DevPop& d, int pt, int pl, in
 {
     return d.pl[pt].close_start[pl] <= ts && d.pl[pt].close_end[pl] > ts;
 }
-__device__ __forceinline__ int link_of(const DevPop& d, int pt, int p) { return __ldg(d.place + (size_t)pt * d.N + p); }
-__device__ __forceinline__ int group_of(const DevPop& d, int pt, int p) { return __ldg(d.group + (size_t)pt * d.N + p); }
+// False when no place can be closed at ts, so the per-place checks can be skipped.
+__device__ __forceinline__ bool closures_possible(const DevPop& d, int ts)
+{
+    return d.close_window[0] <= ts && ts < d.close_window[1];
+}
+__device__ __forceinline__ int link_of(const DevPop& d, int pt, int p) { return __ldg(&d.links[p].link[pt]); }
+__device__ __forceinline__ int group_of(const DevPop& d, int pt, int p) { return __ldg(&d.links[p].group[pt]); }
+// Whole records, as two and one 16-byte loads.
+__device__ __forceinline__ PersonLinks load_links(const DevPop& d, int p)
+{
+    const int4* q = reinterpret_cast<const int4*>(d.links + p);
+    int4 a = __ldg(q), b = __ldg(q + 1);
+    PersonLinks r;
+    static_assert(sizeof(r) == 2 * sizeof(int4), "layout");
+    reinterpret_cast<int4*>(&r)[0] = a;
+    reinterpret_cast<int4*>(&r)[1] = b;
+    return r;
+}
+__device__ __forceinline__ HouseholdRec load_household(const DevPop& d, int h)
+{
+    int4 a = __ldg(reinterpret_cast<const int4*>(d.hhr + h));
+    HouseholdRec r;
+    reinterpret_cast<int4*>(&r)[0] = a;
+    return r;
+}
 
 // --------------------------------------- CalcInfSusc (src/CalcInfSusc.cpp)
 // Factors that are exactly 1.0 here (digital contact tracing, treatment,

@@ -35,6 +35,24 @@ struct __align__(16) PersonHot {
 };
 static_assert(sizeof(PersonHot) == 32, "PersonHot must fill one 32-byte sector");
 
+// Place memberships of one person, in one 32-byte sector: the place of each type
+// (-1 for none) and the group within it.
+struct __align__(16) PersonLinks {
+    int32_t link[CS_MAX_PLACE_TYPES];
+    uint16_t group[CS_MAX_PLACE_TYPES];
+    uint16_t pad;
+};
+static_assert(sizeof(PersonLinks) == 32, "PersonLinks must fill one 32-byte sector");
+
+// One household: location, first member (members are contiguous), size, and the
+// size the household kernel is normalised by (Household::nhr).
+struct __align__(16) HouseholdRec {
+    float x, y;
+    int32_t first;
+    uint16_t nh, nhr;
+};
+static_assert(sizeof(HouseholdRec) == 16, "HouseholdRec is one 16-byte load");
+
 struct DevPlaces {
     int32_t n;
     const int32_t* mcell;
@@ -69,14 +87,8 @@ struct DevPop {
     int32_t N, NH, NC, NM, NPT, NB, nbx, nby, bs;
     const cs_params* P;
     PersonHot* hot;
-    const int32_t* place;      // [NPT][N]
-    const uint16_t* group;     // [NPT][N]
-    const int32_t* hh_first;
-    const uint16_t* hh_nh;
-    const uint16_t* hh_nhr;
-    const float* hh_x;
-    const float* hh_y;
-    const float2* hh_xy;       // the two above interleaved, one 8-byte load per household
+    const PersonLinks* links;  // [N]
+    const HouseholdRec* hhr;   // [NH]
     const int32_t* mcell_cell;
     const int32_t* mcell_adunit;
     const int32_t* cell_grid;
@@ -113,6 +125,7 @@ struct DevPop {
     uint8_t* moverest;
     DevIv* iv;
     DevStep* step;
+    int32_t* close_window;     // [2] every place closed at ts has [0] <= ts < [1]
     // spatial proposal blocks
     const int32_t* cell_block;
     const int32_t* block_cell_ofs;

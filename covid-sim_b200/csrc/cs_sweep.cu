@@ -30,7 +30,6 @@
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
-#include <cooperative_groups/scan.h>
 
 #include <cstdarg>
 #include <cstdio>
@@ -71,16 +70,37 @@ __device__ __forceinline__ int32_t append(int32_t* count)
     return base + (int32_t)g.thread_rank();
 }
 
-// Reserves n consecutive entries of a device list for each calling thread, with
-// one atomic per warp; returns the first entry's index.
-__device__ __forceinline__ int32_t reserve(int32_t* count, int32_t n)
+// Reserves na entries of list A and nb entries of list B for every thread of the
+// block, with one atomic per list per block.  Every thread of the block must call
+// it at the same point (block-uniform control flow); blockDim.x is a multiple of 32.
+__device__ __forceinline__ int2 block_reserve2(int32_t* count_a, int32_t na, int32_t* count_b, int32_t nb)
 {
-    cg::coalesced_group g = cg::coalesced_threads();
-    int32_t incl = cg::inclusive_scan(g, n);
-    int32_t base = 0;
-    if (g.thread_rank() == g.size() - 1) base = atomicAdd(count, incl);
-    base = g.shfl(base, g.size() - 1);
-    return base + incl - n;
+    __shared__ int2 warp_base[32];
+    __shared__ int2 block_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    int32_t ia = na, ib = nb;
+    for (int o = 1; o < 32; o <<= 1) {
+        int32_t ya = __shfl_up_sync(0xffffffffu, ia, o), yb = __shfl_up_sync(0xffffffffu, ib, o);
+        if (lane >= o) { ia += ya; ib += yb; }
+    }
+    if (lane == 31) warp_base[warp] = make_int2(ia, ib);
+    __syncthreads();
+    if (warp == 0) {
+        int2 v = lane < nwarps ? warp_base[lane] : make_int2(0, 0);
+        int32_t xa = v.x, xb = v.y;
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t ya = __shfl_up_sync(0xffffffffu, xa, o), yb = __shfl_up_sync(0xffffffffu, xb, o);
+            if (lane >= o) { xa += ya; xb += yb; }
+        }
+        int32_t ta = __shfl_sync(0xffffffffu, xa, 31), tb = __shfl_sync(0xffffffffu, xb, 31);
+        if (lane == 0)
+            block_base = make_int2(ta && count_a ? atomicAdd(count_a, ta) : 0, tb && count_b ? atomicAdd(count_b, tb) : 0);
+        if (lane < nwarps) warp_base[lane] = make_int2(xa - v.x, xb - v.y);
+    }
+    __syncthreads();
+    int2 r = make_int2(block_base.x + warp_base[warp].x + ia - na, block_base.y + warp_base[warp].y + ib - nb);
+    __syncthreads();   // the shared slots are reused by the next call
+    return r;
 }
 
 __device__ __forceinline__ void mark_cell(const DevPop& d, int c)
@@ -103,6 +123,9 @@ __device__ __forceinline__ bool flag_household(const DevPop& d, int h, uint8_t f
 
 constexpr int kThreads = 256;
 
+// close_window of a run in which no place has been closed
+static const int32_t kNoClosures[2] = {INT32_MAX, 0};
+
 // ------------------------------------------------------------- contexts
 struct cs_gpu_ctx {
     int device = 0;
@@ -120,6 +143,8 @@ struct cs_gpu_ctx {
     // dense-grid buffers of UpdateProbs' normaliser
     double *S0g = nullptr, *Ng = nullptr, *Ag = nullptr, *Bg = nullptr;
     uint8_t *rowS = nullptr, *rowN = nullptr;
+    float* Gtab = nullptr;   // kernel rows of every (source row, target row) pair, or null
+    double *Apart = nullptr, *Bpart = nullptr;   // per row-chunk partial sums
     uint64_t seed = 0;
     bool run_started = false;
     int grid = 148 * 8;
@@ -221,6 +246,7 @@ static int dupload(cs_gpu_ctx* c, T** p, const T* src, size_t n)
 
 extern "C" {
 static int tot_prob_pass(cs_gpu_ctx* c, bool denominators);
+static int build_kernel_rows(cs_gpu_ctx* c);
 }
 
 // ================================================================ run start
@@ -337,6 +363,21 @@ __device__ double row_kernel(const DevPop& d, const cs_params& P, int dx, int yl
     return (double)(float)knum(d, P, d2, err);
 }
 
+// The kernel rows are geometry only, so they are evaluated once per context:
+// Gtab[(yl * nch + ym) * ncw + dx] = row_kernel(dx, yl, ym), exact in float since
+// row_kernel rounds through float.  *oor counts distances beyond the kernel table.
+__global__ void k_kernel_rows(DevPop d, float* Gtab, unsigned long long* oor)
+{
+    const cs_params& P = *d.P;
+    const size_t ncw = P.ncw, nch = P.nch, n = nch * nch * ncw;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        int dx = (int)(e % ncw);
+        size_t pair = e / ncw;
+        int ym = (int)(pair % nch), yl = (int)(pair / nch);
+        Gtab[e] = (float)row_kernel(d, P, dx, yl, ym, oor);
+    }
+}
+
 __global__ void k_grid_values(DevPop d, double* S0g, double* Ng, uint8_t* rowS, uint8_t* rowN)
 {
     int nch = d.P->nch;
@@ -354,40 +395,55 @@ __global__ void k_grid_values(DevPop d, double* S0g, double* Ng, uint8_t* rowS, 
 
 // Each thread owns kTotProbCols = 8 consecutive source columns xl0..xl0+7 of
 // source row yl.  Shared memory holds the kernel row mirrored, Gm[off + dx] =
-// G(|dx|), so target column xm of output j reads Gm[off + xm - xl0 - j]: for eight
-// targets xm0..xm0+7 a thread reads one window of 15 values, w[q] =
-// Gm[off - 7 + xm0 - xl0 + q], and does 64 fused multiply-adds from registers.
+// G(|dx|), so target column xm of output j reads Gm[off + xm - xl0 - j]: for
+// sixteen targets xm0..xm0+15 a thread reads one window of 23 values, w[q] =
+// Gm[off - 7 + xm0 - xl0 + q], and does 128 fused multiply-adds from registers.
 // Gm is stored with one pad slot after every 8 values, so the windows of the 16
-// lanes of a half-warp (8 values apart) fall in distinct banks.  Each output's
-// sum still runs over xm ascending; a zero S0 adds +0.0, which changes nothing.
+// lanes of a half-warp (8 values apart) fall in distinct banks.
+//
+// Summation order, restated by the oracle: for each output, the row sum over xm
+// ascending (fused multiply-adds, one rounding per term); row sums added in
+// ascending ym within chunks of kTotProbRowChunk target rows; chunk sums added in
+// ascending chunk order.  A zero S0 adds +0.0, which changes nothing.  Blocks
+// cover `chunks_per_block` chunks each: the sweep uses one chunk per block
+// (partial sums, then k_tot_prob_reduce) for parallelism, and the fixed-scratch
+// entry point all chunks in one block; both give the same bits.
 constexpr int kTotProbCols = 8;
+constexpr int kTotProbSpan = 16;          // target columns per register window
+constexpr int kTotProbRowChunk = 32;
 
 __host__ __device__ constexpr int tp_phys(int i) { return i + (i >> 3); }
 
 struct TotProbGeom {
-    int ncwR;   // target columns rounded up to a multiple of 8 (tail S0 = 0)
+    int ncwR;   // target columns rounded up to a multiple of 16 (tail S0 = 0)
     int off;    // Gm index of dx = 0: ncwR + 7, so off - 7 is a multiple of 8
     int gphys;  // doubles in the padded Gm array
+    int nchunks;           // ceil(nch / kTotProbRowChunk)
+    int chunks_per_block;  // 1 (partial sums) or nchunks (final sums)
     size_t smem(bool denominators) const
     {
         return sizeof(double) * ((size_t)gphys + (denominators ? 2 : 1) * (size_t)ncwR);
     }
 };
 
-static TotProbGeom tot_prob_geom(int ncw)
+static TotProbGeom tot_prob_geom(int ncw, int nch, bool partial)
 {
     TotProbGeom g;
-    g.ncwR = (ncw + kTotProbCols - 1) / kTotProbCols * kTotProbCols;
+    g.ncwR = (ncw + kTotProbSpan - 1) / kTotProbSpan * kTotProbSpan;
     g.off = g.ncwR + 7;
-    g.gphys = tp_phys(g.off + g.ncwR) + 2;
+    g.gphys = tp_phys(g.off + g.ncwR + kTotProbSpan) + 2;
     g.gphys += g.gphys & 1;   // keep the arrays after Gm 16-byte aligned
+    g.nchunks = (nch + kTotProbRowChunk - 1) / kTotProbRowChunk;
+    g.chunks_per_block = partial ? 1 : g.nchunks;
     return g;
 }
 
+// Out[(z * ncw + xl) * nch + yl] for block z of the chunk dimension.
 template <bool kDenominators>
 __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S0g, const double* Ng,
                                                        const uint8_t* rowS, const uint8_t* rowN,
-                                                       double* Ag, double* Bg, TotProbGeom gm)
+                                                       double* Aout, double* Bout, TotProbGeom gm,
+                                                       const float* __restrict__ Gtab)
 {
     const cs_params& P = *d.P;
     const int ncw = P.ncw, nch = P.nch;
@@ -396,6 +452,8 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
     double* Srow = sh + gm.gphys;     // ncwR
     double* Nrow = Srow + gm.ncwR;    // ncwR (denominator pass only)
     const int xl0 = (blockIdx.x * blockDim.x + threadIdx.x) * kTotProbCols, yl = blockIdx.y;
+    const int q0 = blockIdx.z * gm.chunks_per_block;
+    const int q1 = min(q0 + gm.chunks_per_block, gm.nchunks);
     for (int k = threadIdx.x; k < gm.gphys; k += blockDim.x) Gp[k] = 0.0;
     for (int k = ncw + threadIdx.x; k < gm.ncwR; k += blockDim.x) {
         Srow[k] = 0.0;
@@ -407,31 +465,37 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
     // window start of this thread for xm0 = 0, in padded units: phys(off - 7 - xl0 + q)
     // = 9 * (off - 7 - xl0) / 8 + q + q / 8, with off - 7 - xl0 a multiple of 8
     const int t0 = 9 * ((gm.off - 7 - xl0) / 8);
-    for (int ym = 0; ym < nch; ym++) {
-        const bool useS = rowS[ym] != 0, useN = kDenominators && rowN[ym] != 0;
-        if (!useS && !useN) continue;
-        __syncthreads();
-        for (int k = threadIdx.x; k < ncw; k += blockDim.x) {
-            double v = row_kernel(d, P, k, yl, ym, CSB_CTR(err_kernel_range));
-            Gp[tp_phys(gm.off + k)] = v;
-            Gp[tp_phys(gm.off - k)] = v;
-            Srow[k] = S0g[(size_t)k * nch + ym];
-            if (kDenominators) Nrow[k] = Ng[(size_t)k * nch + ym];
-        }
-        __syncthreads();
-        if (xl0 < ncw) {
+    for (int q = q0; q < q1; q++) {
+        double a[kTotProbCols], b[kTotProbCols];
+#pragma unroll
+        for (int j = 0; j < kTotProbCols; j++) a[j] = b[j] = 0.0;
+        const int ym1 = min(nch, (q + 1) * kTotProbRowChunk);
+        for (int ym = q * kTotProbRowChunk; ym < ym1; ym++) {
+            const bool useS = rowS[ym] != 0, useN = kDenominators && rowN[ym] != 0;
+            if (!useS && !useN) continue;
+            __syncthreads();
+            const float* grow = Gtab ? Gtab + ((size_t)yl * nch + ym) * ncw : nullptr;
+            for (int k = threadIdx.x; k < ncw; k += blockDim.x) {
+                double v = grow ? (double)grow[k] : row_kernel(d, P, k, yl, ym, CSB_CTR(err_kernel_range));
+                Gp[tp_phys(gm.off + k)] = v;
+                Gp[tp_phys(gm.off - k)] = v;
+                Srow[k] = S0g[(size_t)k * nch + ym];
+                if (kDenominators) Nrow[k] = Ng[(size_t)k * nch + ym];
+            }
+            __syncthreads();
+            if (xl0 >= ncw) continue;
             double sa[kTotProbCols], sb[kTotProbCols];
 #pragma unroll
             for (int j = 0; j < kTotProbCols; j++) sa[j] = sb[j] = 0.0;
-            for (int xm0 = 0, t = t0; xm0 < gm.ncwR; xm0 += kTotProbCols, t += 9) {
-                double w[2 * kTotProbCols - 1];
+            for (int xm0 = 0, t = t0; xm0 < gm.ncwR; xm0 += kTotProbSpan, t += 18) {
+                double w[kTotProbSpan + kTotProbCols - 1];
 #pragma unroll
-                for (int q = 0; q < 2 * kTotProbCols - 1; q++) w[q] = Gp[t + q + (q >> 3)];
+                for (int r = 0; r < kTotProbSpan + kTotProbCols - 1; r++) w[r] = Gp[t + r + (r >> 3)];
                 if (useS) {
                     const double2* s2 = reinterpret_cast<const double2*>(Srow + xm0);
 #pragma unroll
-                    for (int u2 = 0; u2 < kTotProbCols / 2; u2++) {
-                        double2 sv = s2[u2];
+                    for (int u2 = 0; u2 < kTotProbSpan / 2; u2++) {
+                        const double2 sv = s2[u2];
 #pragma unroll
                         for (int j = 0; j < kTotProbCols; j++) sa[j] = fma(sv.x, w[2 * u2 - j + 7], sa[j]);
 #pragma unroll
@@ -441,8 +505,8 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
                 if (kDenominators && useN) {
                     const double2* n2 = reinterpret_cast<const double2*>(Nrow + xm0);
 #pragma unroll
-                    for (int u2 = 0; u2 < kTotProbCols / 2; u2++) {
-                        double2 nv = n2[u2];
+                    for (int u2 = 0; u2 < kTotProbSpan / 2; u2++) {
+                        const double2 nv = n2[u2];
 #pragma unroll
                         for (int j = 0; j < kTotProbCols; j++) sb[j] = fma(nv.x, w[2 * u2 - j + 7], sb[j]);
 #pragma unroll
@@ -452,30 +516,46 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
             }
 #pragma unroll
             for (int j = 0; j < kTotProbCols; j++) {
-                if (useS) A[j] = A[j] + sa[j];
-                if (kDenominators && useN) B[j] = B[j] + sb[j];
+                if (useS) a[j] = a[j] + sa[j];
+                if (kDenominators && useN) b[j] = b[j] + sb[j];
             }
         }
+#pragma unroll
+        for (int j = 0; j < kTotProbCols; j++) {
+            A[j] = A[j] + a[j];
+            if (kDenominators) B[j] = B[j] + b[j];
+        }
     }
+    const size_t zofs = (size_t)blockIdx.z * ncw * nch;
 #pragma unroll
     for (int j = 0; j < kTotProbCols; j++) {
         int xl = xl0 + j;
         if (xl < ncw) {
-            Ag[(size_t)xl * nch + yl] = A[j];
-            if (kDenominators) Bg[(size_t)xl * nch + yl] = B[j];
+            Aout[zofs + (size_t)xl * nch + yl] = A[j];
+            if (kDenominators) Bout[zofs + (size_t)xl * nch + yl] = B[j];
         }
+    }
+}
+
+// Chunk sums added in ascending chunk order: out[g] = sum over z of part[z][g].
+__global__ void k_tot_prob_reduce(const double* __restrict__ part, int nparts, size_t G, double* __restrict__ out)
+{
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < G; g += (size_t)gridDim.x * blockDim.x) {
+        double A = 0.0;
+        for (int z = 0; z < nparts; z++) A = A + part[(size_t)z * G + g];
+        out[g] = A;
     }
 }
 
 // Launch shape of k_tot_prob_rows: ceil(ncw / 8) threads per source row, in
 // blocks of up to 256 threads (whole warps).
-static void tot_prob_launch_shape(int ncw, int nch, dim3* grid, int* threads)
+static void tot_prob_launch_shape(int ncw, int nch, const TotProbGeom& gm, dim3* grid, int* threads)
 {
     int need = (ncw + kTotProbCols - 1) / kTotProbCols;
     int tpb = ((need + 31) / 32) * 32;
     if (tpb > 256) tpb = 256;
     *threads = tpb;
-    *grid = dim3((need + tpb - 1) / tpb, nch);
+    *grid = dim3((need + tpb - 1) / tpb, nch, gm.nchunks / gm.chunks_per_block);
 }
 
 __global__ void k_tot_prob_finish(DevPop d, const double* Ag, const double* Bg)
@@ -559,12 +639,16 @@ __global__ void k_block_rows(DevPop d)
 // lists are reordered by position).
 __global__ void k_build_active(DevPop d, int mode)
 {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
-        int base = d.cell_start[c] + d.S[c] + (mode == 0 ? d.L[c] : 0);
-        int n = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
-        int o = reserve(d.counts + kCntAct, n);
+    for (int c0 = blockIdx.x * blockDim.x; c0 < d.NC; c0 += gridDim.x * blockDim.x) {
+        const int c = c0 + threadIdx.x;
+        int first = 0, n = 0;
+        if (c < d.NC) {
+            first = d.cell_start[c] + d.S[c] + (mode == 0 ? d.L[c] : 0);
+            n = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
+        }
+        const int o = block_reserve2(d.counts + kCntAct, n, nullptr, 0).x;
         for (int k = 0; k < n; k++) {
-            d.act[o + k] = d.slots[base + k];
+            d.act[o + k] = d.slots[first + k];
             d.act_cell[o + k] = c;
         }
     }
@@ -646,65 +730,72 @@ __global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d)
     const StepScalars st = *d.step;
     const uint64_t seed = st.seed;
     int nact = d.counts[kCntAct];
+    const bool anyc = closures_possible(d, st.ts);
     long long hh_members = 0;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
-        int i = d.act[idx], ci = d.act_cell[idx];
-        PersonHot hi = d.hot[i];
-        int h = hi.hh;
-        int iag = age_group(hi);
-        uint16_t nh = d.hh_nh[h];
-        if (st.hh_beta > 0 && nh > 1) {
-            int f0 = d.hh_first[h], f1 = f0 + nh;
-            double HI = st.hh_beta * calc_house_inf(hi, d.hh_nhr[h], P, st.ts);
-            bool absent = false;
-            for (int m = f0; (m < f1) && (!absent); m++) {
-                bool ma = host_absent(d.hot[m], st.ts);
-                for (int pt = 0; (pt < d.NPT) && (!absent); pt++) {
-                    int lk = link_of(d, pt, m);
-                    if (lk >= 0) absent = place_closed(d, pt, lk, st.ts) && ma;
-                }
-            }
-            if (absent) HI *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_HOUSE];
-            Stream s(seed, CS_RNG_HOUSEHOLD, (uint32_t)st.ts, (uint32_t)i, 0);
-            for (int m = f0; m < f1; m++) {
-                hh_members++;
-                PersonHot hm = d.hot[m];
-                if (hm.inf == CS_INF_SUSCEPTIBLE) {
-                    double foi = HI * calc_house_susc(d, hm, iag, P);
-                    if (s.next() < foi) claim_infection(d, m, i, 1);
-                }
-            }
-        }
-        // the infector's place passes: one work entry per place it attends today
+    // block-uniform loop: every thread takes part in the list reservations
+    for (int base = blockIdx.x * blockDim.x; base < nact; base += gridDim.x * blockDim.x) {
+        const int idx = base + threadIdx.x;
         int links[CS_MAX_PLACE_TYPES];
-        int nwork = 0;
-        const bool absent_i = host_absent(hi, st.ts);
-        for (int pt = 0; pt < d.NPT; pt++) {
-            links[pt] = P.DoPlaces ? link_of(d, pt, i) : -1;
-            if (links[pt] >= 0 && !absent_i) nwork++;
-        }
-        {
-            int o = reserve(d.counts + kCntPlaceWork, nwork);
-            for (int pt = 0; pt < d.NPT; pt++)
-                if (links[pt] >= 0 && !absent_i) d.place_work[o++] = make_int2((idx << 3) | pt, links[pt]);
-        }
-        int k = 0;
+        int nwork = 0, k = 0;
         uint8_t closed_i = 0;
-        if (st.sp_beta > 0) {
-            double si = calc_spatial_inf(hi, P, st.ts);
-            bool closed = false;
-            for (int pt = 0; (pt < d.NPT) && (!closed); pt++)
-                if (links[pt] >= 0) closed = place_closed(d, pt, links[pt], st.ts);
-            if (closed && host_absent(hi, st.ts)) { si *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL]; closed_i = 1; }
-            double lambda = si * st.sp_beta * d.tot_prob[ci];
-            Stream s(seed, CS_RNG_SPATIAL_COUNT, (uint32_t)st.ts, (uint32_t)i, 0);
-            k = sample_poisson(s, lambda, CSB_CTR(err_spatial_tries));
+        bool absent_i = true;
+        if (idx < nact) {
+            int i = d.act[idx], ci = d.act_cell[idx];
+            PersonHot hi = d.hot[i];
+            int h = hi.hh;
+            int iag = age_group(hi);
+            const HouseholdRec hr = load_household(d, h);
+            uint16_t nh = hr.nh;
+            if (st.hh_beta > 0 && nh > 1) {
+                int f0 = hr.first, f1 = f0 + nh;
+                double HI = st.hh_beta * calc_house_inf(hi, hr.nhr, P, st.ts);
+                bool absent = false;
+                for (int m = f0; anyc && (m < f1) && (!absent); m++) {
+                    bool ma = host_absent(d.hot[m], st.ts);
+                    for (int pt = 0; (pt < d.NPT) && (!absent); pt++) {
+                        int lk = link_of(d, pt, m);
+                        if (lk >= 0) absent = place_closed(d, pt, lk, st.ts) && ma;
+                    }
+                }
+                if (absent) HI *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_HOUSE];
+                Stream s(seed, CS_RNG_HOUSEHOLD, (uint32_t)st.ts, (uint32_t)i, 0);
+                for (int m = f0; m < f1; m++) {
+                    hh_members++;
+                    PersonHot hm = d.hot[m];
+                    if (hm.inf == CS_INF_SUSCEPTIBLE) {
+                        double foi = HI * calc_house_susc(d, hm, iag, P);
+                        if (s.next() < foi) claim_infection(d, m, i, 1);
+                    }
+                }
+            }
+            // the infector's place passes: one work entry per place it attends today
+            absent_i = host_absent(hi, st.ts);
+            const PersonLinks pli = load_links(d, i);
+            for (int pt = 0; pt < d.NPT; pt++) {
+                links[pt] = P.DoPlaces ? pli.link[pt] : -1;
+                if (links[pt] >= 0 && !absent_i) nwork++;
+            }
+            if (st.sp_beta > 0) {
+                double si = calc_spatial_inf(hi, P, st.ts);
+                bool closed = false;
+                for (int pt = 0; anyc && (pt < d.NPT) && (!closed); pt++)
+                    if (links[pt] >= 0) closed = place_closed(d, pt, links[pt], st.ts);
+                if (closed && absent_i) { si *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL]; closed_i = 1; }
+                double lambda = si * st.sp_beta * d.tot_prob[ci];
+                Stream s(seed, CS_RNG_SPATIAL_COUNT, (uint32_t)st.ts, (uint32_t)i, 0);
+                k = sample_poisson(s, lambda, CSB_CTR(err_spatial_tries));
+            }
         }
-        // this infector's contacts take entries [o, o + k) of the contact map
-        int o = reserve(d.counts + kCntContacts, k);
-        d.cnt_ofs[idx] = o;
-        for (int jj = 0; jj < k && o + jj < d.cmap_cap; jj++) d.cmap[o + jj] = idx;
-        d.act_closed[idx] = closed_i;
+        // place-work entries [ow, ow + nwork) and contact-map entries [oc, oc + k)
+        const int2 o = block_reserve2(d.counts + kCntPlaceWork, nwork, d.counts + kCntContacts, k);
+        if (idx < nact) {
+            int ow = o.x;
+            for (int pt = 0; pt < d.NPT; pt++)
+                if (links[pt] >= 0 && !absent_i) d.place_work[ow++] = make_int2((idx << 3) | pt, links[pt]);
+            d.cnt_ofs[idx] = o.y;
+            for (int jj = 0; jj < k && o.y + jj < d.cmap_cap; jj++) d.cmap[o.y + jj] = idx;
+            d.act_closed[idx] = closed_i;
+        }
     }
     cnt_add_warp(CSB_CTR(work_hh_members), hh_members);
 }
@@ -827,7 +918,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d)
                 ss *= calc_person_susc(hp, iag, P);
                 ss *= P.WAIFW_Matrix_SpatialOnly[age_group(hp)][iag];
                 if (moverest_differs(d, hp.mcell, hinf.mcell)) ss *= P.MoveRestrEffect;
-                if ((!closed_i) && host_absent(hp, st.ts)) {
+                if ((!closed_i) && closures_possible(d, st.ts) && host_absent(hp, st.ts)) {
                     bool f = false;
                     for (int pt = 0; (pt < d.NPT) && (!f); pt++) {
                         int lk = link_of(d, pt, p);
@@ -1188,16 +1279,20 @@ __global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d)
     int nact = d.counts[kCntAct];
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_incub_people), nact);
     const int delay = (int)(P.LatentToSymptDelay / P.ModelTimeStep);
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) {
-        int p = d.act[idx];
-        PersonHot h = d.hot[p];
-        bool ev;
-        if (h.inf == CS_INF_LATENT)
-            ev = h.latent_time == ts;
-        else
-            ev = (ts == (uint16_t)(h.latent_time + delay)) || (ts == d.recovery_time[p]) ||
-                 (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
-        if (ev) d.cmap[append(d.counts + kCntEvents)] = idx;
+    for (int base = blockIdx.x * blockDim.x; base < nact; base += gridDim.x * blockDim.x) {
+        const int idx = base + threadIdx.x;
+        bool ev = false;
+        if (idx < nact) {
+            int p = d.act[idx];
+            PersonHot h = d.hot[p];
+            if (h.inf == CS_INF_LATENT)
+                ev = h.latent_time == ts;
+            else
+                ev = (ts == (uint16_t)(h.latent_time + delay)) || (ts == d.recovery_time[p]) ||
+                     (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
+        }
+        const int o = block_reserve2(d.counts + kCntEvents, ev ? 1 : 0, nullptr, 0).x;
+        if (ev) d.cmap[o] = idx;
     }
 }
 
@@ -1277,7 +1372,8 @@ __global__ void k_household_after(DevPop d)
         int h = d.hh_list[k];
         uint8_t f = d.hh_flag[h];
         d.hh_flag[h] = 0;
-        int j1 = d.hh_first[h], j2 = j1 + d.hh_nh[h];
+        const HouseholdRec hr = load_household(d, h);
+        int j1 = hr.first, j2 = j1 + hr.nh;
         if (f & 3) {
             int wp = P.PlaceTypeNoAirNum - 1;
             bool ok = false;
@@ -1334,6 +1430,11 @@ __global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t st
 {
     const cs_params& P = *d.P;
     DevPlaces pl = d.pl[pt];
+    // every place closed at ts afterwards has close_start >= start and close_end <= stop
+    if (blockIdx.x == 0 && threadIdx.x == 0 && start < stop) {
+        atomicMin(d.close_window, (int32_t)start);
+        atomicMax(d.close_window + 1, (int32_t)stop);
+    }
     for (int l = blockIdx.x; l < pl.n; l += gridDim.x) {
         if (sel && !sel[pl.mcell[l]]) continue;
         __shared__ int do_members;
@@ -1446,21 +1547,28 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         d.hot = ph;
         CK(cudaStreamSynchronize(c->stream));
     }
-    const int32_t* place_c; const uint16_t* group_c;
-    { int32_t* t; UP(t, pop->person_place, NPT * N); place_c = t; }
-    { uint16_t* t; UP(t, pop->person_group, NPT * N); group_c = t; }
-    d.place = place_c; d.group = group_c;
-    { int32_t* t; UP(t, pop->hh_first, NH); d.hh_first = t; }
-    { uint16_t* t; UP(t, pop->hh_nh, NH); d.hh_nh = t; }
-    { uint16_t* t; UP(t, pop->hh_nhr, NH); d.hh_nhr = t; }
-    { float* t; UP(t, pop->hh_x, NH); d.hh_x = t; }
-    { float* t; UP(t, pop->hh_y, NH); d.hh_y = t; }
     {
-        std::vector<float2> xy(NH);
-        for (size_t h = 0; h < NH; h++) xy[h] = make_float2(pop->hh_x[h], pop->hh_y[h]);
-        float2* t;
-        UP(t, xy.data(), NH);
-        d.hh_xy = t;
+        std::vector<PersonLinks> lk(N);
+        for (size_t p = 0; p < N; p++) {
+            PersonLinks& q = lk[p];
+            for (int pt = 0; pt < CS_MAX_PLACE_TYPES; pt++) {
+                q.link[pt] = pt < (int)NPT ? pop->person_place[pt * N + p] : -1;
+                q.group[pt] = pt < (int)NPT ? pop->person_group[pt * N + p] : 0;
+            }
+            q.pad = 0;
+        }
+        PersonLinks* t;
+        UP(t, lk.data(), N);
+        d.links = t;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    {
+        std::vector<HouseholdRec> hh(NH);
+        for (size_t h = 0; h < NH; h++)
+            hh[h] = HouseholdRec{pop->hh_x[h], pop->hh_y[h], pop->hh_first[h], pop->hh_nh[h], pop->hh_nhr[h]};
+        HouseholdRec* t;
+        UP(t, hh.data(), NH);
+        d.hhr = t;
         CK(cudaStreamSynchronize(c->stream));
     }
     { int32_t* t; UP(t, pop->mcell_cell, NM); d.mcell_cell = t; }
@@ -1526,6 +1634,8 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     {
         size_t G = (size_t)params->ncw * params->nch;
         AL(c->S0g, G); AL(c->Ng, G); AL(c->Ag, G); AL(c->Bg, G);
+        const size_t nchunks = (params->nch + kTotProbRowChunk - 1) / kTotProbRowChunk;
+        AL(c->Apart, nchunks * G); AL(c->Bpart, nchunks * G);
         AL(c->rowS, (size_t)params->nch); AL(c->rowN, (size_t)params->nch);
     }
     AL(d.claim, N); AL(d.queue, N); AL(d.counts, kCntN); AL(d.touched, NC); AL(d.cell_flag, NC + 4);
@@ -1533,6 +1643,8 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     AL(d.cmap, 2 * N); d.cmap_cap = (int32_t)(2 * N);
     AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH);
     AL(d.place_work, N * (size_t)(NPT > 0 ? NPT : 1));
+    AL(d.close_window, 2);
+    CK(cudaMemcpyAsync(d.close_window, kNoClosures, sizeof(kNoClosures), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(d.claim, 0xff, sizeof(unsigned long long) * N, c->stream));
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
     CK(cudaMemsetAsync(d.cell_flag, 0, NC + 4, c->stream));
@@ -1546,6 +1658,8 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
 #undef UP
 #undef AL
     CK(cudaStreamSynchronize(c->stream));
+    r = build_kernel_rows(c);
+    if (r) return r;
     r = tot_prob_pass(c, true);  // the n-weighted denominators never change
     if (r) return r;
     CK(cudaStreamSynchronize(c->stream));
@@ -1560,6 +1674,7 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (void* p : c->allocs) cudaFree(p);
+    if (c->Gtab) cudaFree(c->Gtab);
     if (c->d_seed_list) cudaFree(c->d_seed_list);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1573,8 +1688,55 @@ int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
     if (params->kernel_size != c->hp.kernel_size || params->NumPlaceTypes != c->hp.NumPlaceTypes || params->ncw != c->hp.ncw ||
         params->nch != c->hp.nch)
         return set_err(c, CS_E_ARG, "set_params may not change the kernel table, grid or place types");
+    const cs_params& o = c->hp;
+    const bool geometry = params->DoUTM_coords != o.DoUTM_coords || params->DoPeriodicBoundaries != o.DoPeriodicBoundaries ||
+                          params->cell_width != o.cell_width || params->cell_height != o.cell_height ||
+                          params->width_deg != o.width_deg || params->height_deg != o.height_deg ||
+                          params->bbox_bottom_left_y != o.bbox_bottom_left_y || params->kernel_delta != o.kernel_delta ||
+                          params->kernel_expansion != o.kernel_expansion ||
+                          memcmp(params->sinx, o.sinx, sizeof(o.sinx)) || memcmp(params->cosx, o.cosx, sizeof(o.cosx)) ||
+                          memcmp(params->asin2sqx, o.asin2sqx, sizeof(o.asin2sqx));
     c->hp = *params;
     CK(cudaMemcpyAsync(c->dP, params, sizeof(cs_params), cudaMemcpyHostToDevice, c->stream));
+    if (geometry) {   // the kernel rows and the n-weighted denominators depend on it
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->Gtab) cudaFree(c->Gtab);
+        c->Gtab = nullptr;
+        r = build_kernel_rows(c);
+        if (r == CS_OK) r = tot_prob_pass(c, true);
+        if (r) return r;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return CS_OK;
+}
+
+// Kernel rows for UpdateProbs, when they fit in kGtabMaxBytes.  If any distance
+// falls outside the kernel table the rows are dropped again, so that UpdateProbs
+// evaluates (and counts) them on every call as before.
+constexpr size_t kGtabMaxBytes = (size_t)16 << 30;
+
+static int build_kernel_rows(cs_gpu_ctx* c)
+{
+    const cs_params& P = c->hp;
+    size_t n = (size_t)P.nch * P.nch * P.ncw;
+    if (n * sizeof(float) > kGtabMaxBytes) return CS_OK;
+    if (cudaMalloc(&c->Gtab, n * sizeof(float)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        c->Gtab = nullptr;
+        return CS_OK;   // not enough memory: evaluate on the fly
+    }
+    unsigned long long* oor = nullptr;
+    CK(cudaMalloc(&oor, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(oor, 0, sizeof(unsigned long long), c->stream));
+    LAUNCH(k_kernel_rows, c->grid, kThreads, c->d, c->Gtab, oor);
+    unsigned long long h = 0;
+    CK(cudaMemcpyAsync(&h, oor, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(oor);
+    if (h) {
+        cudaFree(c->Gtab);
+        c->Gtab = nullptr;
+    }
     return CS_OK;
 }
 
@@ -1592,22 +1754,25 @@ static int tot_prob_pass(cs_gpu_ctx* c, bool denominators)
         CK(cudaMemsetAsync(c->rowN, 0, P.nch, c->stream));
     }
     LAUNCH(k_grid_values, (d.NC + kThreads - 1) / kThreads, kThreads, d, c->S0g, denominators ? c->Ng : nullptr, c->rowS, c->rowN);
+    const TotProbGeom gm = tot_prob_geom(P.ncw, P.nch, true);
     dim3 grid;
     int tpb;
-    tot_prob_launch_shape(P.ncw, P.nch, &grid, &tpb);
-    const TotProbGeom gm = tot_prob_geom(P.ncw);
+    tot_prob_launch_shape(P.ncw, P.nch, gm, &grid, &tpb);
     const size_t smem = gm.smem(denominators);
     if (c->prof) prof_begin(c, "k_tot_prob_rows");
     if (denominators) {
         if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tot_prob_rows<true><<<grid, tpb, smem, c->stream>>>(d, c->S0g, c->Ng, c->rowS, c->rowN, c->Ag, c->Bg, gm);
+        k_tot_prob_rows<true><<<grid, tpb, smem, c->stream>>>(d, c->S0g, c->Ng, c->rowS, c->rowN, c->Apart, c->Bpart, gm, c->Gtab);
     } else {
         if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, c->S0g, nullptr, c->rowS, nullptr, c->Ag, nullptr, gm);
+        k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, c->S0g, nullptr, c->rowS, nullptr, c->Apart, nullptr, gm, c->Gtab);
     }
     if (c->prof) prof_end(c);
     c->launches++;
     CK(cudaGetLastError());
+    const int rgrid = (int)((G + kThreads - 1) / kThreads);
+    LAUNCH(k_tot_prob_reduce, rgrid, kThreads, c->Apart, gm.nchunks, G, c->Ag);
+    if (denominators) LAUNCH(k_tot_prob_reduce, rgrid, kThreads, c->Bpart, gm.nchunks, G, c->Bg);
     return CS_OK;
 }
 
@@ -1656,6 +1821,22 @@ int cs_gpu_seed_infections(cs_gpu_ctx* c, double t, const int32_t* people, int n
     return apply_queue(c);
 }
 
+// Run-level state outside the per-person view, as InitModel sets it: place
+// closures and each place's closure threshold (src/CovidSim.cpp:1110-1125),
+// social-distancing and movement flags, intervention windows.
+static int reset_run_level(cs_gpu_ctx* c, uint64_t seed)
+{
+    DevPop& d = c->d;
+    for (int pt = 0; pt < d.NPT; pt++) LAUNCH(k_reset_places, c->grid, kThreads, d, pt, seed);
+    CK(cudaMemcpyAsync(d.close_window, kNoClosures, sizeof(kNoClosures), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(d.socdist, 0, d.NM, c->stream));
+    CK(cudaMemsetAsync(d.moverest, 0, d.NM, c->stream));
+    DevIv iv{1e10, 0, 1e10, 0};
+    CK(cudaMemcpyAsync(c->dIv, &iv, sizeof(iv), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));   // iv is a stack copy
+    return CS_OK;
+}
+
 int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, int n_seed, int update_probs)
 {
     if (!c) return CS_E_ARG;
@@ -1668,14 +1849,9 @@ int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, i
     LAUNCH(k_reset_people, c->grid, kThreads, d, seed);
     LAUNCH(k_reset_slots, c->grid, kThreads, d);
     LAUNCH(k_reset_listpos, (d.NC + kThreads - 1) / kThreads, kThreads, d);
-    for (int pt = 0; pt < d.NPT; pt++) LAUNCH(k_reset_places, c->grid, kThreads, d, pt, seed);
-    CK(cudaMemsetAsync(d.socdist, 0, d.NM, c->stream));
-    CK(cudaMemsetAsync(d.moverest, 0, d.NM, c->stream));
-    {
-        DevIv iv{1e10, 0, 1e10, 0};
-        CK(cudaMemcpyAsync(c->dIv, &iv, sizeof(iv), cudaMemcpyHostToDevice, c->stream));
-    }
-    int r = rebuild_blocks(c);
+    int r = reset_run_level(c, seed);
+    if (r) return r;
+    r = rebuild_blocks(c);
     if (r) return r;
     c->run_started = true;
     return cs_gpu_seed_infections(c, 0.0, seed_people, n_seed);
@@ -2003,7 +2179,8 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
     CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
     CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
     c->seed = seed;
-    int r = rebuild_blocks(c);
+    int r = reset_run_level(c, seed);
+    if (r == CS_OK) r = rebuild_blocks(c);
     cudaError_t e = cudaStreamSynchronize(c->stream);
     for (void* p : tmp) cudaFree(p);
     if (r) return r;
@@ -2078,13 +2255,13 @@ extern "C" int cs_gpu_update_probs_static(cs_gpu_ctx* c, int do_place)
     const int cgrid = (d.NC + kThreads - 1) / kThreads;
     k_update_S0<<<cgrid, kThreads, 0, c->stream>>>(d, do_place);
     k_grid_values<<<cgrid, kThreads, 0, c->stream>>>(d, S0g, nullptr, rowS, nullptr);
+    const TotProbGeom gm = tot_prob_geom(P.ncw, P.nch, false);   // all row chunks in one block
     dim3 grid;
     int tpb;
-    tot_prob_launch_shape(P.ncw, P.nch, &grid, &tpb);
-    const TotProbGeom gm = tot_prob_geom(P.ncw);
+    tot_prob_launch_shape(P.ncw, P.nch, gm, &grid, &tpb);
     const size_t smem = gm.smem(false);
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, S0g, nullptr, rowS, nullptr, Ag, nullptr, gm);
+    k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, S0g, nullptr, rowS, nullptr, Ag, nullptr, gm, c->Gtab);
     k_tot_prob_finish<<<cgrid, kThreads, 0, c->stream>>>(d, Ag, c->Bg);
     k_block_S0<<<(d.NB + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);
     k_block_rows<<<(d.NB * 32 + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);

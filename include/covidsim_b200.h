@@ -366,7 +366,9 @@ int cs_gpu_set_params(cs_gpu_ctx* ctx, const cs_params* params);
 int cs_gpu_begin_run(cs_gpu_ctx* ctx, uint64_t seed, const int32_t* seed_people, int n_seed,
                      int update_probs);
 
-/* Load dynamic state prepared by a host (the reference's own InitModel). */
+/* Load dynamic state prepared by a host (the reference's own InitModel).  State
+ * outside the view (place closures and closure thresholds, social-distancing and
+ * movement flags, intervention windows) is reset as cs_gpu_begin_run resets it. */
 int cs_gpu_upload_state(cs_gpu_ctx* ctx, uint64_t seed, const cs_state_view* state);
 int cs_gpu_download_state(cs_gpu_ctx* ctx, const cs_state_view* state);
 

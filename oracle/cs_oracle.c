@@ -698,8 +698,10 @@ static double row_kernel(const cs_cpu_ctx* c, int dx, int yl, int ym, int64_t* e
  * tot_prob = sum_m S0_m Kmax(l,m) / sum_m n_m Kmax(l,m) with
  * Kmax = (float)num(dist2_cc_min), summed in double in a fixed order: over target
  * rows ym ascending, each row's sum over target columns xm ascending formed first
- * with fused multiply-adds (one rounding per term); zero terms are skipped
- * (adding +0.0 changes nothing). */
+ * with fused multiply-adds (one rounding per term); row sums added within chunks
+ * of TOT_PROB_ROW_CHUNK rows, chunk sums added in ascending order; zero terms are
+ * skipped (adding +0.0 changes nothing). */
+#define TOT_PROB_ROW_CHUNK 32
 int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
 {
     const cs_params* P = &c->P;
@@ -726,23 +728,29 @@ int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
     for (int l = 0; l < c->NC; l++) {
         int xl = c->cell_grid[l] / nch, yl = c->cell_grid[l] % nch;
         double A = 0.0, B = 0.0;
-        for (int ym = 0; ym < nch; ym++) {
-            int anyS = 0, anyN = 0;
-            for (int xm = 0; xm < ncw; xm++) {
-                anyS |= S0g[(size_t)xm * nch + ym] != 0.0;
-                anyN |= Ng[(size_t)xm * nch + ym] != 0.0;
+        for (int q0 = 0; q0 < nch; q0 += TOT_PROB_ROW_CHUNK) {
+            double a = 0.0, b = 0.0;
+            int q1 = q0 + TOT_PROB_ROW_CHUNK < nch ? q0 + TOT_PROB_ROW_CHUNK : nch;
+            for (int ym = q0; ym < q1; ym++) {
+                int anyS = 0, anyN = 0;
+                for (int xm = 0; xm < ncw; xm++) {
+                    anyS |= S0g[(size_t)xm * nch + ym] != 0.0;
+                    anyN |= Ng[(size_t)xm * nch + ym] != 0.0;
+                }
+                if (!anyS && !anyN) continue;
+                for (int k = 0; k < ncw; k++) krow[k] = row_kernel(c, k, yl, ym, &err);
+                double s = 0.0, sb = 0.0;
+                for (int xm = 0; xm < ncw; xm++) {
+                    int dd = xm > xl ? xm - xl : xl - xm;
+                    double sv = S0g[(size_t)xm * nch + ym], nv = Ng[(size_t)xm * nch + ym];
+                    if (sv != 0.0) s = fma(sv, krow[dd], s);
+                    if (nv != 0.0) sb = fma(nv, krow[dd], sb);
+                }
+                if (anyS) a = a + s;
+                if (anyN) b = b + sb;
             }
-            if (!anyS && !anyN) continue;
-            for (int k = 0; k < ncw; k++) krow[k] = row_kernel(c, k, yl, ym, &err);
-            double s = 0.0, sb = 0.0;
-            for (int xm = 0; xm < ncw; xm++) {
-                int dd = xm > xl ? xm - xl : xl - xm;
-                double sv = S0g[(size_t)xm * nch + ym], nv = Ng[(size_t)xm * nch + ym];
-                if (sv != 0.0) s = fma(sv, krow[dd], s);
-                if (nv != 0.0) sb = fma(nv, krow[dd], sb);
-            }
-            if (anyS) A = A + s;
-            if (anyN) B = B + sb;
+            A = A + a;
+            B = B + b;
         }
         c->tot_prob[l] = (B > 0) ? A / B : 0.0;
     }
@@ -830,6 +838,25 @@ int cs_cpu_seed_infections(cs_cpu_ctx* c, double t, const int32_t* people, int n
     return CS_OK;
 }
 
+/* Run-level state outside the per-person view, as InitModel sets it: place
+ * closures and each place's closure threshold (src/CovidSim.cpp:1110-1125),
+ * social-distancing and movement flags, intervention windows. */
+static void reset_run_level(cs_cpu_ctx* c, uint64_t seed)
+{
+    for (int t = 0; t < c->NPT; t++)
+        for (int l = 0; l < c->pl[t].n; l++) {
+            stream s;
+            stream_init(&s, seed, CS_RNG_PLACE_INIT, 0, (uint32_t)l, (uint32_t)t);
+            c->pl[t].close_start[l] = USHRT_MAX_M1;
+            c->pl[t].close_end[l] = 0;
+            c->pl[t].prob_close[l] = (float)stream_next(&s);
+        }
+    memset(c->socdist, 0, (size_t)c->NM);
+    memset(c->moverest, 0, (size_t)c->NM);
+    c->ci_start = c->hq_start = 1e10;
+    c->ci_dur = c->hq_dur = 0;
+}
+
 int cs_cpu_begin_run(cs_cpu_ctx* c, uint64_t seed, const int32_t* seed_people, int n_seed, int update_probs)
 {
     c->seed = seed;
@@ -863,19 +890,7 @@ int cs_cpu_begin_run(cs_cpu_ctx* c, uint64_t seed, const int32_t* seed_people, i
         c->S0[j] = n;
         c->tot_prob[j] = 1.0;
     }
-    /* places (src/CovidSim.cpp:1110-1125) */
-    for (int t = 0; t < c->NPT; t++)
-        for (int l = 0; l < c->pl[t].n; l++) {
-            stream s;
-            stream_init(&s, seed, CS_RNG_PLACE_INIT, 0, (uint32_t)l, (uint32_t)t);
-            c->pl[t].close_start[l] = USHRT_MAX_M1;
-            c->pl[t].close_end[l] = 0;
-            c->pl[t].prob_close[l] = (float)stream_next(&s);
-        }
-    memset(c->socdist, 0, (size_t)c->NM);
-    memset(c->moverest, 0, (size_t)c->NM);
-    c->ci_start = c->hq_start = 1e10;
-    c->ci_dur = c->hq_dur = 0;
+    reset_run_level(c, seed);
     c->run_started = 1;
     /* At a run start every cell is wholly susceptible, so UpdateProbs(0) gives
      * S0 = n and tot_prob = 1 exactly; only the proposal tables need rebuilding. */
@@ -1558,6 +1573,7 @@ int cs_cpu_upload_state(cs_cpu_ctx* c, uint64_t seed, const cs_state_view* v)
     memset(c->mark, 0, N);
     memset(&c->C, 0, sizeof(c->C));
     c->seed = seed;
+    reset_run_level(c, seed);
     rebuild_block_tables(c);
     c->run_started = 1;
     return CS_OK;
