@@ -42,6 +42,9 @@ WORKLOADS = {
     # name: (preset, days, interventions, description, initial infections)
     "c1": ("c1", 365, True, "10M people, 600x600 cells, interventions, 365 d", 100),
     "c0": ("c0", 120, False, "1M people, 240x240 cells, no interventions, 120 d", 100),
+    # the same 10M people on the 240x240 grid (coarser cells, as the reference's
+    # own grid limit would force)
+    "c1_240": ("c1_240", 365, True, "10M people, 240x240 cells, interventions, 365 d", 100),
     # a short case whose sweeps run at epidemic-peak load after a few hundred
     # launches: the profiling case for the spatial and place kernels
     "c1_peak": ("c1", 8, False, "10M people, 600x600 cells, 500k initial infections, 8 d", 500000),
@@ -55,7 +58,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["c2"])
+    ap.add_argument("--c2-scale", type=float, default=1.0,
+                    help="c2 only: population sizes times this factor (1.0 = 1/4/10/20 M)")
+    ap.add_argument("--c2-per-size", type=int, default=16, help="c2 only: realisations per population size")
+    ap.add_argument("--c2-days", type=int, default=365, help="c2 only: days per realisation")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-out", default=None, help="write per-kernel times to this JSON file")
@@ -151,7 +158,8 @@ def kernel_bytes(name, w, n_cells_steps):
 
 
 def load_traffic():
-    """dram bytes per launch from the committed ncu summary, when present."""
+    """Per-unit DRAM traffic of the captured kernels from the committed ncu summary
+    (bytes per work unit, e.g. per spatial contact), when present."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         return json.load(open(path))
@@ -246,7 +254,12 @@ def run_ours(args):
         rows.append(dict(kernel=name, ms=kms, launches=n, share=kms / sum(v[0] for v in kernels.values()),
                          bytes=b, gbs=(b / (kms / 1e3) / 1e9) if b else None))
     dom = rows[0]
-    dom_traffic = traffic.get(dom["kernel"], {}).get("dram_bytes_per_launch")
+    # ncu traffic of the same kernel, captured at peak load on the smaller profiling
+    # case and scaled to this workload's average launch by the units it processed
+    dom_traffic = None
+    tr = traffic.get(dom["kernel"])
+    if tr and work.get(tr["unit"]):
+        dom_traffic = round(tr["dram_bytes_per_unit"] * work[tr["unit"]] / dom["launches"])
     roofline = {
         "bound": "hbm", "kernel": dom["kernel"], "achieved": round(dom["gbs"], 2) if dom["gbs"] else None,
         "peak": peak, "unit": "GB/s", "frac": round(dom["gbs"] / peak, 4) if dom["gbs"] else None,
@@ -387,8 +400,84 @@ def run_reference(args):
     }
 
 
+# ------------------------------------------------------------ batched ensemble
+C2_SIZES = (1_000_000, 4_000_000, 10_000_000, 20_000_000)
+
+
+def run_c2(args):
+    """Ensemble of uneven populations stepped together (cs_gpu_batch): per size,
+    `c2-per-size` realisations sharing that population's static device arrays,
+    each with its own seed and R0 drawn uniformly in [1.8, 3.2], C1 interventions.
+    One step = the whole ensemble for c2-days days; one CUDA graph per timestep."""
+    import torch
+    torch.cuda.set_device(0)
+    from covidsim_b200 import population, params as prm, sim
+    grid = population.make_grid(cell_deg=1.0 / 120, nmcl=10)
+    rng = np.random.default_rng(2024)
+    members, people = [], 0
+    for size in C2_SIZES:
+        n = int(size * args.c2_scale)
+        pop = population.generate(n, grid, sigma=1.2, seed=98798150 + n)
+        P, lk, hr = prm.build_params(pop.grid)
+        beta24, _ = sim.calibrate_local_beta(pop, P, 2.4)
+        base = None
+        for k in range(args.c2_per_size):
+            Pk = type(P).from_buffer_copy(P)
+            Pk.LocalBeta = beta24 * float(rng.uniform(1.8, 3.2)) / 2.4   # the coefficient scales R0 linearly
+            if base is None:
+                base = sim.Simulation(pop, Pk, lk, hr)
+                members.append(base)
+            else:
+                members.append(base.replica(Pk))
+            people += n
+    batch = sim.Batch(members)
+    days = args.c2_days
+    policy = sim.InterventionPolicy()
+    stream = torch.cuda.ExternalStream(batch.stream())
+    for w in range(args.warmup):
+        batch.run([9000 + 100 * w + k for k in range(len(members))], min(days, 20), policy=policy)
+    batch.sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    finals = []
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        for k in range(args.steps):
+            out = batch.run([17389101 + 1000 * k + j for j in range(len(members))], days, policy=policy)
+            finals.append(int(sum(o["cumI"][-1] for o in out)))
+        ev1.record(stream)
+        batch.sync()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    steps_per_run = int(days * members[0].params.TimeStepsPerDay)
+    person_steps = people * steps_per_run * args.steps
+    nreal = len(members) * args.steps
+    batch.close()
+    for m in members:
+        m.close()
+    return {
+        "metric": METRIC, "value": round(person_steps / (ms / 1e3), 1), "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64/f32 (f64 probabilities, f32 person state)",
+        "data": "synthetic (seeded generator, reference parameter set)",
+        "config": {"workload": "batched ensemble: %d realisations, %d each of %s people on 240x240 cells, "
+                               "R0 ~ U[1.8, 3.2], interventions, %d d"
+                               % (len(members), args.c2_per_size,
+                                  "/".join("%g" % (x * args.c2_scale) for x in C2_SIZES), days),
+                   "realisations_per_step": len(members), "people_total": people,
+                   "timesteps_per_realisation": steps_per_run, "parallelism": "one graph per timestep, "
+                   "one branch per realisation; static arrays shared per population"},
+        "runs_per_hour": round(nreal / (ms / 1e3) * 3600.0, 1),
+        "ensemble_new_infections": finals,
+        "clocks": clk.summary(), "e2e": None, "gpu_launches": None,
+    }
+
+
 def main():
     args = parse()
+    if args.impl == "ours" and args.workload == "c2":
+        print(json.dumps(run_c2(args)))
+        return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
         print(json.dumps(out))

@@ -144,6 +144,25 @@ def load_library(path=LIB_PATH):
         "cs_gpu_update_probs_static": (I, [V, I]),
         "cs_gpu_step": (I, [V, D, I]),
         "cs_gpu_use_graphs": (I, [V, I]),
+        "cs_gpu_set_grid": (I, [V, I]),
+        "cs_gpu_grid": (I, [V]),
+        "cs_gpu_create_replica": (I, [V, P(V)]),
+        "cs_gpu_batch_create": (I, [P(V), I, P(V)]),
+        "cs_gpu_batch_step": (I, [V, D, I]),
+        "cs_gpu_batch_set_grid": (I, [V, I]),
+        "cs_gpu_batch_sync": (I, [V]),
+        "cs_gpu_batch_stream": (V, [V]),
+        "cs_gpu_batch_last_error": (C.c_char_p, [V]),
+        "cs_gpu_batch_destroy": (None, [V]),
+        "cs_sur_num_params": (C.c_size_t, []),
+        "cs_sur_create": (I, [I, I, P(V)]),
+        "cs_sur_destroy": (None, [V]),
+        "cs_sur_last_error": (C.c_char_p, [V]),
+        "cs_sur_set_params": (I, [V, V]),
+        "cs_sur_get_params": (I, [V, V]),
+        "cs_sur_forward": (I, [V, V, I, V]),
+        "cs_sur_loss_grad": (I, [V, V, V, I, P(C.c_float), V]),
+        "cs_sur_train_step": (I, [V, V, V, I, C.c_float, P(C.c_float)]),
         "cs_gpu_set_interventions": (I, [V, P(cs_interventions)]),
         "cs_gpu_close_places": (I, [V, I, V, I, C.c_uint16, C.c_uint16]),
         "cs_gpu_get_counters": (I, [V, P(cs_counters)]),

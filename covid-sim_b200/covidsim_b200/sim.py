@@ -36,6 +36,23 @@ class GpuBackend:
             self.ctx = None
             raise abi.CovidSimError("cs_gpu_create: %s" % (msg.decode() if msg else rc))
 
+    @classmethod
+    def replica(cls, base):
+        """Another realisation of base's population, sharing its static device arrays."""
+        self = cls.__new__(cls)
+        self.lib = base.lib
+        self.ctx = C.c_void_p()
+        rc = self.lib.cs_gpu_create_replica(base.ctx, C.byref(self.ctx))
+        if rc != 0:
+            msg = self.lib.cs_gpu_last_error(self.ctx)
+            self.lib.cs_gpu_destroy(self.ctx)
+            self.ctx = None
+            raise abi.CovidSimError("cs_gpu_create_replica: %s" % (msg.decode() if msg else rc))
+        return self
+
+    def set_grid(self, blocks):
+        self._ck(self.lib.cs_gpu_set_grid(self.ctx, blocks), "set_grid")
+
     def _ck(self, rc, what):
         if rc != 0:
             raise abi.CovidSimError("%s%s: %s" % (self.prefix, what, self.lib.cs_gpu_last_error(self.ctx).decode()))
@@ -239,6 +256,18 @@ class Simulation:
     def close(self):
         self.backend.close()
 
+    def replica(self, params=None):
+        """A Simulation of another realisation of this population that shares its
+        static device arrays; `params` (same geometry) may differ, e.g. in LocalBeta."""
+        other = Simulation.__new__(Simulation)
+        other.pop = self.pop
+        other.params = params if params is not None else self.params
+        other._pop_c = self._pop_c
+        other.backend = type(self.backend).replica(self.backend)
+        if params is not None:
+            other.backend.set_params(params)
+        return other
+
     def choose_seeds(self, seed, n_seed):
         """SeedInfection with random locations: uniformly chosen people (the
         reference picks a person, then a member of that person's microcell)."""
@@ -252,45 +281,15 @@ class Simulation:
         (InitModel + SeedInfection already applied); it is copied to the device
         instead of resetting and seeding there."""
         be = self.backend
-        P = self.params
         if initial_state is not None:
             be.upload(seed, initial_state)
         else:
             be.begin_run(seed, self.choose_seeds(seed, n_seed))
-        spd = int(round(P.TimeStepsPerDay))
-        nsteps = int(days * spd)
-        prev_prop_s = 1.0
-        series = {k: [] for k in ("S", "L", "I", "R", "D", "cumI", "cumC", "cumDC", "Critical", "cumCritical",
-                                  "cumDeath_Critical", "cumDeath_SARI", "cumDeath_ILI", "SARI", "ILI", "Mild")}
-        iv_on_until = -1.0
-        iv_started = False
-        socd = np.zeros(self.pop.n_mcells, dtype=np.uint8)
-        for step in range(nsteps):
-            t = step * P.ModelTimeStep
-            be.step(t, 0)
-            if (step + 1) % spd == 0 or step == nsteps - 1:
-                c = be.counters()
-                for k in series:
-                    series[k].append(int(getattr(c, k)))
-                prop_s = c.S / self.pop.n_people
-                if prev_prop_s - prop_s > 0.2:
-                    prev_prop_s = prop_s
-                    be.update_probs(0)
-                if policy is not None:
-                    day = len(series["cumCritical"])
-                    w = policy.window
-                    recent = series["cumCritical"][-1] - (series["cumCritical"][-w - 1] if day > w else 0)
-                    tn = t + P.ModelTimeStep
-                    if not iv_started and recent >= policy.threshold:
-                        iv_started = True
-                        iv_on_until = tn + policy.duration
-                        self._switch_interventions(tn, policy, True, socd)
-                    elif iv_started and iv_on_until > 0 and tn >= iv_on_until:
-                        iv_on_until = -1.0
-                        self._switch_interventions(tn, policy, False, socd)
-                if callback:
-                    callback(step, c)
-        return {k: np.asarray(v) for k, v in series.items()}
+        rs = _RunState(self, days, policy, callback)
+        for step in range(rs.nsteps):
+            be.step(step * self.params.ModelTimeStep, 0)
+            rs.after_step(step)
+        return rs.result()
 
     def _switch_interventions(self, t, policy, on, socd):
         iv = abi.cs_interventions()
@@ -309,3 +308,119 @@ class Simulation:
             for pt in policy.close_place_types:
                 if pt < self.pop.num_place_types:
                     self.backend.close_places(pt, None, ts, stop)
+
+
+SERIES = ("S", "L", "I", "R", "D", "cumI", "cumC", "cumDC", "Critical", "cumCritical",
+          "cumDeath_Critical", "cumDeath_SARI", "cumDeath_ILI", "SARI", "ILI", "Mild")
+
+
+class _RunState:
+    """Host side of one realisation between timesteps (src/CovidSim.cpp:1480-1530):
+    daily counters, UpdateProbs when the susceptible fraction has fallen by 0.2,
+    and the global ICU trigger switching interventions on and off."""
+
+    def __init__(self, sim, days, policy, callback):
+        self.sim, self.policy, self.callback = sim, policy, callback
+        P = sim.params
+        self.spd = int(round(P.TimeStepsPerDay))
+        self.nsteps = int(days * self.spd)
+        self.prev_prop_s = 1.0
+        self.series = {k: [] for k in SERIES}
+        self.iv_on_until = -1.0
+        self.iv_started = False
+        self.socd = np.zeros(sim.pop.n_mcells, dtype=np.uint8)
+
+    def after_step(self, step):
+        if not ((step + 1) % self.spd == 0 or step == self.nsteps - 1):
+            return
+        sim, be, P, policy = self.sim, self.sim.backend, self.sim.params, self.policy
+        series = self.series
+        t = step * P.ModelTimeStep
+        c = be.counters()
+        for k in series:
+            series[k].append(int(getattr(c, k)))
+        prop_s = c.S / sim.pop.n_people
+        if self.prev_prop_s - prop_s > 0.2:
+            self.prev_prop_s = prop_s
+            be.update_probs(0)
+        if policy is not None:
+            day = len(series["cumCritical"])
+            w = policy.window
+            recent = series["cumCritical"][-1] - (series["cumCritical"][-w - 1] if day > w else 0)
+            tn = t + P.ModelTimeStep
+            if not self.iv_started and recent >= policy.threshold:
+                self.iv_started = True
+                self.iv_on_until = tn + policy.duration
+                sim._switch_interventions(tn, policy, True, self.socd)
+            elif self.iv_started and self.iv_on_until > 0 and tn >= self.iv_on_until:
+                self.iv_on_until = -1.0
+                sim._switch_interventions(tn, policy, False, self.socd)
+        if self.callback:
+            self.callback(step, c)
+
+    def result(self):
+        return {k: np.asarray(v) for k, v in self.series.items()}
+
+
+class Batch:
+    """Realisations advanced together: one cs_gpu_batch_step per timestep launches
+    one CUDA graph holding every member's step, so the members' kernels share the
+    GPU.  Members are Simulations (replicas of one population via
+    Simulation.replica(), or of different populations); each keeps its own host
+    logic (daily counters, UpdateProbs, interventions)."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        self.lib = abi.load_library()
+        ctxs = (C.c_void_p * len(self.sims))(*[s.backend.ctx for s in self.sims])
+        self.handle = C.c_void_p()
+        rc = self.lib.cs_gpu_batch_create(ctxs, len(self.sims), C.byref(self.handle))
+        if rc != 0:
+            msg = self.lib.cs_gpu_batch_last_error(self.handle)
+            self.lib.cs_gpu_batch_destroy(self.handle)
+            self.handle = None
+            raise abi.CovidSimError("cs_gpu_batch_create: %s" % msg.decode())
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise abi.CovidSimError("cs_gpu_batch_%s: %s" % (what, self.lib.cs_gpu_batch_last_error(self.handle).decode()))
+
+    def step(self, t, run=0):
+        self._ck(self.lib.cs_gpu_batch_step(self.handle, t, run), "step")
+
+    def set_grid(self, blocks):
+        self._ck(self.lib.cs_gpu_batch_set_grid(self.handle, blocks), "set_grid")
+
+    def sync(self):
+        self._ck(self.lib.cs_gpu_batch_sync(self.handle), "sync")
+
+    def stream(self):
+        return self.lib.cs_gpu_batch_stream(self.handle)
+
+    def run(self, seeds, days, n_seed=100, policy=None, callback=None):
+        """One realisation per member (member k with run seed seeds[k] and, when
+        `policy` is a list, policy[k]); returns the members' daily series."""
+        states = []
+        policies = policy if isinstance(policy, (list, tuple)) else [policy] * len(self.sims)
+        for sim, seed, pol in zip(self.sims, seeds, policies):
+            sim.backend.begin_run(seed, sim.choose_seeds(seed, n_seed))
+            cb = (lambda step, c, k=len(states): callback(k, step, c)) if callback else None
+            states.append(_RunState(sim, days, pol, cb))
+        nsteps = max(rs.nsteps for rs in states)
+        dt = self.sims[0].params.ModelTimeStep
+        for step in range(nsteps):
+            self.step(step * dt, 0)
+            for rs in states:
+                rs.after_step(step)
+        return [rs.result() for rs in states]
+
+    def close(self):
+        if self.handle:
+            self.lib.cs_gpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

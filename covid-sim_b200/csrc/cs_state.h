@@ -53,6 +53,17 @@ struct __align__(16) HouseholdRec {
 };
 static_assert(sizeof(HouseholdRec) == 16, "HouseholdRec is one 16-byte load");
 
+// One cell of a proposal block's cell list: running S0 of the block up to and
+// including this cell, the cell, its first slot and its S0 (one 16-byte load).
+struct __align__(16) BlockCell {
+    int32_t cum, m, start, s0;
+};
+// A proposal block: its S0 and its range [kb, ke) of the block cell list.
+struct __align__(16) BlockInfo {
+    long long S0;
+    int32_t kb, ke;
+};
+
 struct DevPlaces {
     int32_t n;
     const int32_t* mcell;
@@ -125,13 +136,15 @@ struct DevPop {
     uint8_t* moverest;
     DevIv* iv;
     DevStep* step;
+    const unsigned long long* seed_src;  // the run's seed, written by begin_run / upload_state
+    const double* t_src;                 // when set (batched graphs), k_set_step takes t from here
     int32_t* close_window;     // [2] every place closed at ts has [0] <= ts < [1]
     // spatial proposal blocks
     const int32_t* cell_block;
     const int32_t* block_cell_ofs;
     const int32_t* block_cells;
-    int32_t* block_cum;
-    long long* block_S0;
+    BlockCell* block_cell_info;  // [NC], rebuilt with S0
+    BlockInfo* block_info;       // [NB], S0 rebuilt with S0
     double* block_row_cum;     // [NB][NB]
     double* block_bound_tab;   // [NB][NB] bound(b, B) for target blocks with people
     int16_t* block_guide;      // [NB][NB] cut points of each row (Chen & Asau guide table)

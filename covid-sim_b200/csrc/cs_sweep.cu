@@ -35,6 +35,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -47,6 +48,35 @@ using namespace csb;
 
 // ------------------------------------------------------------------ helpers
 #define CSB_CTR(field) ((unsigned long long*)&d.C->field)
+
+// Per-block staging of the counters in shared memory, for kernels whose threads
+// hit the same few counters (severity tallies, per-age and per-admin-unit sums):
+// with many items, adds go to shared memory and each block adds its non-zero
+// totals to the global counters once, at its end; with few items the zeroing and
+// flushing would cost more than they save, so adds go straight to the global
+// counters.  CSB_STAGED is valid between stage_begin() and stage_flush() only.
+constexpr int kCtrWords = (int)(sizeof(cs_counters) / sizeof(unsigned long long));
+static_assert(sizeof(cs_counters) % sizeof(unsigned long long) == 0, "counters are 64-bit words");
+constexpr int kStageMinItems = 16384;
+__shared__ unsigned long long s_ctr[kCtrWords];
+__shared__ unsigned long long* s_ctr_base;
+#define CSB_STAGED(field) ((unsigned long long*)((char*)s_ctr_base + offsetof(cs_counters, field)))
+
+__device__ __forceinline__ void stage_begin(cs_counters* C, bool staged)
+{
+    if (staged)
+        for (int i = threadIdx.x; i < kCtrWords; i += blockDim.x) s_ctr[i] = 0ull;
+    if (threadIdx.x == 0) s_ctr_base = staged ? s_ctr : reinterpret_cast<unsigned long long*>(C);
+    __syncthreads();
+}
+__device__ __forceinline__ void stage_flush(cs_counters* C, bool staged)
+{
+    if (!staged) return;
+    __syncthreads();
+    unsigned long long* g = reinterpret_cast<unsigned long long*>(C);
+    for (int i = threadIdx.x; i < kCtrWords; i += blockDim.x)
+        if (s_ctr[i]) atomicAdd(g + i, s_ctr[i]);
+}
 
 __device__ __forceinline__ void cnt_add(unsigned long long* p, long long v) { atomicAdd(p, (unsigned long long)v); }
 
@@ -127,8 +157,27 @@ constexpr int kThreads = 256;
 static const int32_t kNoClosures[2] = {INT32_MAX, 0};
 
 // ------------------------------------------------------------- contexts
+// Device arrays of a population that never change during runs (households,
+// place memberships, cell lists, kernel tables, proposal-block layout, the
+// UpdateProbs kernel rows and denominators).  Contexts made by
+// cs_gpu_create_replica share one store; the last one destroyed frees it.
+struct StaticStore {
+    int device = 0;
+    std::vector<void*> allocs;
+    float* Gtab = nullptr;
+    ~StaticStore()
+    {
+        cudaSetDevice(device);
+        for (void* p : allocs) cudaFree(p);
+        if (Gtab) cudaFree(Gtab);
+    }
+};
+
 struct cs_gpu_ctx {
     int device = 0;
+    std::shared_ptr<StaticStore> stat;     // static population arrays (possibly shared)
+    std::vector<void*>* alloc_to = nullptr;  // where dalloc records allocations (null: allocs)
+    cudaStream_t own_stream = nullptr;     // the context's stream while a batch lends it another
     cudaStream_t stream = nullptr;
     char err[512] = {0};
     long long launches = 0;
@@ -139,11 +188,13 @@ struct cs_gpu_ctx {
     DevIv* dIv = nullptr;
     cs_counters* dC = nullptr;
     int32_t* d_seed_list = nullptr;
+    unsigned long long* d_seed = nullptr;   // device copy of seed (DevPop::seed_src)
     int seed_cap = 0;
     // dense-grid buffers of UpdateProbs' normaliser
     double *S0g = nullptr, *Ng = nullptr, *Ag = nullptr, *Bg = nullptr;
     uint8_t *rowS = nullptr, *rowN = nullptr;
     float* Gtab = nullptr;   // kernel rows of every (source row, target row) pair, or null
+    void* xfer = nullptr;    // state-transfer staging (XferSlices)
     double *Apart = nullptr, *Bpart = nullptr;   // per row-chunk partial sums
     uint64_t seed = 0;
     bool run_started = false;
@@ -227,7 +278,7 @@ static int dalloc(cs_gpu_ctx* c, T** p, size_t n)
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, sizeof(T) * (n ? n : 1));
     if (e != cudaSuccess) return set_err(c, CS_E_CUDA, "cudaMalloc(%zu bytes): %s", sizeof(T) * n, cudaGetErrorString(e));
-    c->allocs.push_back(q);
+    (c->alloc_to ? c->alloc_to : &c->allocs)->push_back(q);
     *p = (T*)q;
     return CS_OK;
 }
@@ -573,16 +624,17 @@ __global__ void k_block_S0(DevPop d)
         long long s = 0;
         int k0 = d.block_cell_ofs[B], k1 = d.block_cell_ofs[B + 1];
         for (int k = k0; k < k1; k++) {
-            s += d.S0[d.block_cells[k]];
-            d.block_cum[k] = (int32_t)s;
+            int m = d.block_cells[k], s0 = d.S0[m];
+            s += s0;
+            d.block_cell_info[k] = BlockCell{(int32_t)s, m, d.cell_start[m], s0};
         }
-        d.block_S0[B] = s;
+        d.block_info[B] = BlockInfo{s, k0, k1};
         // cut points of the block's cells: entry k0+q = first cell whose running S0
         // exceeds q/nc of the block total
         int nc = k1 - k0, j = k0;
         for (int q = 0; q < nc; q++) {
             double thr = (double)q * (double)s / (double)nc;
-            while (j < k1 - 1 && (double)d.block_cum[j] <= thr) j++;
+            while (j < k1 - 1 && (double)d.block_cell_info[j].cum <= thr) j++;
             d.cell_guide[k0 + q] = (int16_t)(j - k0);
         }
     }
@@ -602,10 +654,10 @@ __global__ void k_block_rows(DevPop d)
         for (int B0 = 0; B0 < d.NB; B0 += 32) {
             int B = B0 + lane;
             double w = 0.0;
-            if (B < d.NB && d.block_S0[B] > 0) {
+            if (B < d.NB && d.block_info[B].S0 > 0) {
                 double bound = block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
                 d.block_bound_tab[(size_t)b * d.NB + B] = bound;
-                w = (double)d.block_S0[B] * bound;
+                w = (double)d.block_info[B].S0 * bound;
             }
             for (int k = 0; k < 32; k++) {
                 double wk = __shfl_sync(0xffffffffu, w, k);
@@ -668,6 +720,8 @@ typedef DevStep StepScalars;
 __global__ void k_set_step(DevPop d, double t, unsigned long long seed)
 {
     const cs_params& P = *d.P;
+    if (d.t_src) t = *d.t_src;
+    if (d.seed_src) seed = *d.seed_src;
     DevStep st;
     st.t = t;
     st.ts = (int)(uint16_t)(P.TimeStepsPerDay * t);
@@ -848,18 +902,20 @@ __device__ __forceinline__ bool spatial_draw(const DevPop& d, const cs_params& P
     int B = guide_row[min((int)(u1 * (double)d.NB), d.NB - 1)];
     while (B > 0 && row[B - 1] > target) B--;
     while (B < d.NB - 1 && !(target < row[B])) B++;
-    long long bS0 = d.block_S0[B];
+    const BlockInfo bi = d.block_info[B];
+    long long bS0 = bi.S0;
     if (bS0 <= 0) return false;
     double u2 = s.next();
     double r = floor(u2 * (double)bS0);
     // smallest cell k in block B with r < cum[k], the same way
-    int kb = d.block_cell_ofs[B], ke = d.block_cell_ofs[B + 1] - 1;
+    int kb = bi.kb, ke = bi.ke - 1;
     int k0 = kb + d.cell_guide[kb + min((int)(u2 * (double)(ke - kb + 1)), ke - kb)];
-    while (k0 > kb && r < (double)d.block_cum[k0 - 1]) k0--;
-    while (k0 < ke && !(r < (double)d.block_cum[k0])) k0++;
-    int m = d.block_cells[k0];
-    int slot = (int)(r - (double)(d.block_cum[k0] - d.S0[m]));
-    int p = d.slots[d.cell_start[m] + slot];
+    while (k0 > kb && r < (double)d.block_cell_info[k0 - 1].cum) k0--;
+    while (k0 < ke && !(r < (double)d.block_cell_info[k0].cum)) k0++;
+    const BlockCell bc = d.block_cell_info[k0];
+    int m = bc.m;
+    int slot = (int)(r - (double)(bc.cum - bc.s0));
+    int p = d.slots[bc.start + slot];
     PersonHot hp = d.hot[p];
     double d2 = dist2_hh(d, P, hh_inf, hp.hh);
     double accept = knum_flag(d, P, d2, oor) / d.block_bound_tab[(size_t)b * d.NB + B];
@@ -949,6 +1005,9 @@ __global__ void k_apply_infections(DevPop d)
     const int ts = d.step->ts;
     const uint64_t seed = d.step->seed;
     int nq = d.counts[kCntQueue];
+    if (blockIdx.x * blockDim.x >= nq) return;   // a block without work stages nothing
+    const bool staged = nq >= kStageMinItems;
+    stage_begin(d.C, staged);
     // single-address tallies, summed per thread and added once per warp
     long long n_inf = 0, n_kw = 0, n_tg = 0, sum_tg = 0, sum_si = 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
@@ -972,11 +1031,11 @@ __global__ void k_apply_infections(DevPop d)
         atomicAdd(d.cnt + cell, 1);  // transitions out of this cell's S block
         mark_cell(d, cell);
         n_inf++;
-        cnt_add(CSB_CTR(cumItype[it % CS_INFECT_TYPE_MASK]), 1);
-        cnt_add(CSB_CTR(cumIa[age_group(h)]), 1);
+        cnt_add(CSB_STAGED(cumItype[it % CS_INFECT_TYPE_MASK]), 1);
+        cnt_add(CSB_STAGED(cumIa[age_group(h)]), 1);
         if (h.pflags & CS_PF_KEYWORKER) n_kw++;
         int ad = d.mcell_adunit[h.mcell];
-        if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumI_adunit[ad]), 1);
+        if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_STAGED(cumI_adunit[ad]), 1);
         if (P.DoLatent) {
             Stream s(seed, CS_RNG_LATENT, (uint32_t)ts, (uint32_t)p, 0);
             double qq;
@@ -998,7 +1057,8 @@ __global__ void k_apply_infections(DevPop d)
     cnt_add_warp(CSB_CTR(cumTG), sum_tg);
     cnt_add_warp(CSB_CTR(cumSI), sum_si);
     cnt_add_warp(CSB_CTR(nTG), n_tg);
-    if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_new_infections), nq);
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_STAGED(work_new_infections), nq);
+    stage_flush(d.C, staged);
 }
 
 // Swap-with-block-end removal of marked slots, high to low (src/Update.cpp:1402-1579
@@ -1048,15 +1108,15 @@ __device__ __forceinline__ void sev_add(const DevPop& d, int ad, int which, int 
 {
     bool adok = ad >= 0 && ad < CS_MAX_ADUNITS;
     switch (which) {
-    case CS_SEV_MILD: cnt_add(CSB_CTR(Mild), delta); if (cum) cnt_add(CSB_CTR(cumMild), 1); break;
-    case CS_SEV_ILI: cnt_add(CSB_CTR(ILI), delta); if (cum) cnt_add(CSB_CTR(cumILI), 1); break;
-    case CS_SEV_SARI: cnt_add(CSB_CTR(SARI), delta); if (cum) cnt_add(CSB_CTR(cumSARI), 1); break;
+    case CS_SEV_MILD: cnt_add(CSB_STAGED(Mild), delta); if (cum) cnt_add(CSB_STAGED(cumMild), 1); break;
+    case CS_SEV_ILI: cnt_add(CSB_STAGED(ILI), delta); if (cum) cnt_add(CSB_STAGED(cumILI), 1); break;
+    case CS_SEV_SARI: cnt_add(CSB_STAGED(SARI), delta); if (cum) cnt_add(CSB_STAGED(cumSARI), 1); break;
     case CS_SEV_CRITICAL:
-        cnt_add(CSB_CTR(Critical), delta);
-        if (adok) cnt_add(CSB_CTR(Critical_adunit[ad]), delta);
-        if (cum) { cnt_add(CSB_CTR(cumCritical), 1); if (adok) cnt_add(CSB_CTR(cumCritical_adunit[ad]), 1); }
+        cnt_add(CSB_STAGED(Critical), delta);
+        if (adok) cnt_add(CSB_STAGED(Critical_adunit[ad]), delta);
+        if (cum) { cnt_add(CSB_STAGED(cumCritical), 1); if (adok) cnt_add(CSB_STAGED(cumCritical_adunit[ad]), 1); }
         break;
-    case CS_SEV_STEPDOWN: cnt_add(CSB_CTR(CritRecov), delta); if (cum) cnt_add(CSB_CTR(cumCritRecov), 1); break;
+    case CS_SEV_STEPDOWN: cnt_add(CSB_STAGED(CritRecov), delta); if (cum) cnt_add(CSB_STAGED(cumCritRecov), 1); break;
     default: break;
     }
 }
@@ -1148,7 +1208,7 @@ __device__ void do_detected_case(const DevPop& d, const cs_params& P, const DevI
                                  uint64_t seed)
 {
     int ad = d.mcell_adunit[h.mcell];
-    if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumDC_adunit[ad]), 1);
+    if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_STAGED(cumDC_adunit[ad]), 1);
     if (P.DoHouseholds && t >= iv.hq_start && t < iv.hq_start + iv.hq_dur) flag_household(d, h.hh, 4);
     if (t >= iv.ci_start && t < iv.ci_start + iv.ci_dur) {
         Stream s(seed, CS_RNG_DETECTED, (uint32_t)ts, (uint32_t)p, 0);
@@ -1161,9 +1221,9 @@ __device__ void do_detected_case(const DevPop& d, const cs_params& P, const DevI
                 h.absent_start = (uint16_t)(ts + P.usCaseIsolationDelay);
                 h.absent_stop = (uint16_t)(ts + P.usCaseIsolationDelay + P.usCaseIsolationDuration);
                 if (P.DoPlaces && !host_quarantined(h, P, ts) && link_of(d, P.PlaceTypeNoAirNum - 1, p) >= 0 && h.age >= P.CaseAbsentChildAgeCutoff)
-                    cnt_add(CSB_CTR(cumAC), 1);
+                    cnt_add(CSB_STAGED(cumAC), 1);
                 if (P.DoHouseholds && P.DoPlaces && h.age < P.CaseAbsentChildAgeCutoff) {
-                    if (!host_quarantined(h, P, ts)) cnt_add(CSB_CTR(cumACS), 1);
+                    if (!host_quarantined(h, P, ts)) cnt_add(CSB_STAGED(cumACS), 1);
                     if (d.prob_care[p] < P.CaseAbsentChildPropAdultCarers) flag_household(d, h.hh, 2);
                 }
             }
@@ -1190,23 +1250,23 @@ __device__ void do_case(const DevPop& d, const cs_params& P, const DevIv& iv, in
                     h.absent_start = (uint16_t)(ts + P.usCaseAbsenteeismDelay);
                     h.absent_stop = (uint16_t)(ts + P.usCaseAbsenteeismDelay + P.usCaseAbsenteeismDuration);
                     if ((!host_quarantined(h, P, ts)) && (link_of(d, P.PlaceTypeNoAirNum - 1, p) >= 0) && (h.age >= P.CaseAbsentChildAgeCutoff))
-                        cnt_add(CSB_CTR(cumAC), 1);
+                        cnt_add(CSB_STAGED(cumAC), 1);
                     if ((P.DoHouseholds) && (h.age < P.CaseAbsentChildAgeCutoff)) {
-                        if (!host_quarantined(h, P, ts)) cnt_add(CSB_CTR(cumACS), 1);
+                        if (!host_quarantined(h, P, ts)) cnt_add(CSB_STAGED(cumACS), 1);
                         if (d.prob_care[p] < P.CaseAbsentChildPropAdultCarers) flag_household(d, h.hh, 1);
                     }
                 }
             }
     }
     if (h.dflags & CS_DF_DETECTED) {
-        cnt_add(CSB_CTR(cumDC), 1);
+        cnt_add(CSB_STAGED(cumDC), 1);
         do_detected_case(d, P, iv, p, h, t, ts, seed);
     }
-    cnt_add(CSB_CTR(cumC), 1);
-    cnt_add(CSB_CTR(cumCa[age]), 1);
-    cnt_add(CSB_CTR(cumC_keyworker[(h.pflags & CS_PF_KEYWORKER) ? 1 : 0]), 1);
+    cnt_add(CSB_STAGED(cumC), 1);
+    cnt_add(CSB_STAGED(cumCa[age]), 1);
+    cnt_add(CSB_STAGED(cumC_keyworker[(h.pflags & CS_PF_KEYWORKER) ? 1 : 0]), 1);
     int ad = d.mcell_adunit[h.mcell];
-    if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumC_adunit[ad]), 1);
+    if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_STAGED(cumC_adunit[ad]), 1);
     if (P.DoSeverity) {
         int cur = h.sev & 0x0f, fin = h.sev >> 4;
         if (cur == CS_SEV_ASYMPTOMATIC) {
@@ -1238,9 +1298,9 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
         if (ts == d.stepdown_time[p] && cur == CS_SEV_CRITICAL && !to_die) { cur = CS_SEV_STEPDOWN; sev_add(d, ad, CS_SEV_CRITICAL, -1, false); sev_add(d, ad, CS_SEV_STEPDOWN, 1, true); }
         if (ts == rec) {
             if (to_die) {
-                if (cur == CS_SEV_CRITICAL) { sev_add(d, ad, CS_SEV_CRITICAL, -1, false); cnt_add(CSB_CTR(cumDeath_Critical), 1); cur = CS_SEV_DEAD; }
-                else if (cur == CS_SEV_SARI) { sev_add(d, ad, CS_SEV_SARI, -1, false); cnt_add(CSB_CTR(cumDeath_SARI), 1); cur = CS_SEV_DEAD; }
-                else if (cur == CS_SEV_ILI) { sev_add(d, ad, CS_SEV_ILI, -1, false); cnt_add(CSB_CTR(cumDeath_ILI), 1); cur = CS_SEV_DEAD; }
+                if (cur == CS_SEV_CRITICAL) { sev_add(d, ad, CS_SEV_CRITICAL, -1, false); cnt_add(CSB_STAGED(cumDeath_Critical), 1); cur = CS_SEV_DEAD; }
+                else if (cur == CS_SEV_SARI) { sev_add(d, ad, CS_SEV_SARI, -1, false); cnt_add(CSB_STAGED(cumDeath_SARI), 1); cur = CS_SEV_DEAD; }
+                else if (cur == CS_SEV_ILI) { sev_add(d, ad, CS_SEV_ILI, -1, false); cnt_add(CSB_STAGED(cumDeath_ILI), 1); cur = CS_SEV_DEAD; }
             } else if (h.inf == CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE || h.inf == CS_INF_CASE) {
                 if (cur == CS_SEV_MILD) { sev_add(d, ad, CS_SEV_MILD, -1, false); cur = CS_SEV_RECOVERED; }
                 else if (cur == CS_SEV_ILI) { sev_add(d, ad, CS_SEV_ILI, -1, false); cur = CS_SEV_RECOVERED; }
@@ -1252,17 +1312,17 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
     }
     if (ts == rec && (h.inf == CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE || h.inf == CS_INF_CASE)) {
         atomicSub(d.I + cell, 1);
-        cnt_add(CSB_CTR(work_transitions), 1);
+        cnt_add(CSB_STAGED(work_transitions), 1);
         if (!to_die) {
             h.inf = (h.inf == CS_INF_CASE) ? CS_INF_RECOVERED_FROM_SYMP : CS_INF_RECOVERED_FROM_ASYMP;
             atomicAdd(d.R + cell, 1);
-            cnt_add(CSB_CTR(cumR), 1);
+            cnt_add(CSB_STAGED(cumR), 1);
         } else {
             h.inf = (h.inf == CS_INF_CASE) ? CS_INF_DEAD_WAS_SYMP : CS_INF_DEAD_WAS_ASYMP;
             atomicAdd(d.D + cell, 1);
-            cnt_add(CSB_CTR(cumD), 1);
-            cnt_add(CSB_CTR(cumDa[age_group(h)]), 1);
-            if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_CTR(cumD_adunit[ad]), 1);
+            cnt_add(CSB_STAGED(cumD), 1);
+            cnt_add(CSB_STAGED(cumDa[age_group(h)]), 1);
+            if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_STAGED(cumD_adunit[ad]), 1);
         }
         return 3;
     }
@@ -1297,7 +1357,7 @@ __global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d)
 }
 
 // cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
-__global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d)
+__global__ void __launch_bounds__(kThreads, 3) k_incub_events(DevPop d)
 {
     const cs_params& P = *d.P;
     const double t = d.step->t;
@@ -1305,6 +1365,9 @@ __global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d)
     const uint64_t seed = d.step->seed;
     const DevIv iv = *d.iv;
     int nev = d.counts[kCntEvents];
+    if (blockIdx.x * blockDim.x >= nev) return;   // a block without work stages nothing
+    const bool staged = nev >= kStageMinItems;
+    stage_begin(d.C, staged);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) {
         int idx = d.cmap[e];
         int p = d.act[idx], c = d.act_cell[idx];
@@ -1317,7 +1380,7 @@ __global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d)
             atomicAdd(d.I + c, 1);
             int add = 1;
             d.mark[pos] = 1;
-            cnt_add(CSB_CTR(work_transitions), 1);
+            cnt_add(CSB_STAGED(work_transitions), 1);
             if (infectious_events(d, P, iv, p, h, c, t, ts, seed) & 1) {
                 d.pstep[p] = kStepItoRD;
                 add += 1 << 16;
@@ -1335,6 +1398,7 @@ __global__ void __launch_bounds__(kThreads) k_incub_events(DevPop d)
             }
         }
     }
+    stage_flush(d.C, staged);
 }
 
 __global__ void k_partition_LI(DevPop d)
@@ -1502,6 +1566,63 @@ static int check_params(cs_gpu_ctx* c, const cs_params* P)
     return CS_OK;
 }
 
+// Dynamic state of one realisation and the per-step scratch, for a context whose
+// static arrays (c->stat, and the static pointers in c->d) are in place.
+static int alloc_dynamic(cs_gpu_ctx* c)
+{
+    DevPop& d = c->d;
+    int r;
+    const size_t N = d.N, NH = d.NH, NC = d.NC, NM = d.NM, NPT = d.NPT;
+    const cs_params* params = &c->hp;
+#define UP(field, src, n) do { if ((r = dupload(c, &field, src, n))) return r; } while (0)
+#define AL(field, n) do { if ((r = dalloc(c, &field, n))) return r; } while (0)
+    for (size_t pt = 0; pt < NPT; pt++) {
+        DevPlaces& pl = d.pl[pt];
+        AL(pl.close_start, (size_t)pl.n); AL(pl.close_end, (size_t)pl.n); AL(pl.prob_close, (size_t)pl.n);
+    }
+    AL(d.infection_time, N); AL(d.recovery_time, N); AL(d.sari_time, N); AL(d.critical_time, N);
+    AL(d.stepdown_time, N); AL(d.detected_time, N); AL(d.prob_absent, N); AL(d.prob_care, N);
+    AL(d.infector, N); AL(d.listpos, N); AL(d.infect_type, N); AL(d.pstep, N);
+    AL(d.S, NC); AL(d.L, NC); AL(d.I, NC); AL(d.R, NC); AL(d.D, NC); AL(d.S0, NC);
+    AL(d.tot_prob, NC); AL(d.slots, N); AL(d.mark, N);
+    AL(d.socdist, NM); AL(d.moverest, NM);
+    CK(cudaMemsetAsync(d.socdist, 0, NM, c->stream));
+    CK(cudaMemsetAsync(d.moverest, 0, NM, c->stream));
+    AL(d.block_cell_info, NC); AL(d.block_info, (size_t)d.NB); AL(d.block_row_cum, (size_t)d.NB * d.NB);
+    AL(d.block_bound_tab, (size_t)d.NB * d.NB);
+    AL(d.block_guide, (size_t)d.NB * d.NB); AL(d.cell_guide, NC);
+    {
+        size_t G = (size_t)params->ncw * params->nch;
+        AL(c->S0g, G); AL(c->Ag, G);
+        const size_t nchunks = (params->nch + kTotProbRowChunk - 1) / kTotProbRowChunk;
+        AL(c->Apart, nchunks * G);
+        AL(c->rowS, (size_t)params->nch);
+    }
+    AL(d.claim, N); AL(d.queue, N); AL(d.counts, kCntN); AL(d.touched, NC); AL(d.cell_flag, NC + 4);
+    AL(d.act, N); AL(d.act_cell, N); AL(d.cnt, NC); AL(d.cnt_ofs, N);
+    AL(d.cmap, 2 * N); d.cmap_cap = (int32_t)(2 * N);
+    AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH);
+    AL(d.place_work, N * (size_t)(NPT > 0 ? NPT : 1));
+    AL(d.close_window, 2);
+    CK(cudaMemcpyAsync(d.close_window, kNoClosures, sizeof(kNoClosures), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(d.claim, 0xff, sizeof(unsigned long long) * N, c->stream));
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
+    CK(cudaMemsetAsync(d.cell_flag, 0, NC + 4, c->stream));
+    CK(cudaMemsetAsync(d.hh_flag, 0, NH + 4, c->stream));
+    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * NC, c->stream));
+    CK(cudaMemsetAsync(d.pstep, 0, N, c->stream));
+    { cs_params* t; UP(t, params, 1); c->dP = t; d.P = t; }
+    { DevIv iv{1e10, 0, 1e10, 0}; DevIv* t; UP(t, &iv, 1); c->dIv = t; d.iv = t; }
+    { DevStep* t; AL(t, 1); d.step = t; CK(cudaMemsetAsync(t, 0, sizeof(DevStep), c->stream)); }
+    { unsigned long long* t; AL(t, 1); c->d_seed = t; d.seed_src = t; CK(cudaMemsetAsync(t, 0, sizeof(*t), c->stream)); }
+    d.t_src = nullptr;
+    { cs_counters* t; AL(t, 1); c->dC = t; d.C = t; CK(cudaMemsetAsync(t, 0, sizeof(cs_counters), c->stream)); }
+#undef UP
+#undef AL
+    CK(cudaStreamSynchronize(c->stream));   // the parameter and window copies came from the stack
+    return CS_OK;
+}
+
 int cs_gpu_create(const cs_population* pop, const cs_params* params, int device, cs_gpu_ctx** out)
 {
     if (!out) return CS_E_ARG;
@@ -1518,35 +1639,40 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     c->grid = nsm * 8;
     c->hp = *params;
+    c->stat = std::make_shared<StaticStore>();
+    c->stat->device = device;
     DevPop& d = c->d;
     d.N = pop->n_people; d.NH = pop->n_households; d.NC = pop->n_cells; d.NM = pop->n_mcells; d.NPT = pop->num_place_types;
     size_t N = d.N, NH = d.NH, NC = d.NC, NM = d.NM, NPT = d.NPT;
     if (d.NPT < 0 || d.NPT > CS_MAX_PLACE_TYPES) return set_err(c, CS_E_ARG, "num_place_types out of range");
     if (N >= (1u << 28)) return set_err(c, CS_E_UNSUPPORTED, "at most 2^28 - 1 people (place work entries pack index << 3)");
     if (N == 0 || NC == 0) return set_err(c, CS_E_ARG, "empty population");
-    // people
-    std::vector<PersonHot> hot(N);
-    for (size_t p = 0; p < N; p++) {
-        PersonHot h{};
-        h.hh = pop->person_hh[p];
-        h.mcell = pop->person_mcell[p];
-        h.age = pop->person_age[p];
-        h.pflags = pop->person_flags ? pop->person_flags[p] : 0;
-        h.absent_start = kNever;
-        h.isolation_start = kNever;
-        h.quar_start = kNever;
-        h.susc = 1.0f;
-        h.dflags = (uint8_t)(2u << CS_DF_QUAR_COMPLY_SHIFT);
-        hot[p] = h;
-    }
 #define UP(field, src, n) do { if ((r = dupload(c, &field, src, n))) return r; } while (0)
 #define AL(field, n) do { if ((r = dalloc(c, &field, n))) return r; } while (0)
+    // people: the record mixes static fields (household, microcell, age, flags)
+    // with dynamic ones, so each realisation holds its own copy
     {
+        std::vector<PersonHot> hot(N);
+        for (size_t p = 0; p < N; p++) {
+            PersonHot h{};
+            h.hh = pop->person_hh[p];
+            h.mcell = pop->person_mcell[p];
+            h.age = pop->person_age[p];
+            h.pflags = pop->person_flags ? pop->person_flags[p] : 0;
+            h.absent_start = kNever;
+            h.isolation_start = kNever;
+            h.quar_start = kNever;
+            h.susc = 1.0f;
+            h.dflags = (uint8_t)(2u << CS_DF_QUAR_COMPLY_SHIFT);
+            hot[p] = h;
+        }
         PersonHot* ph;
         UP(ph, hot.data(), N);
         d.hot = ph;
         CK(cudaStreamSynchronize(c->stream));
     }
+    // ---- static arrays, kept in the (shareable) static store
+    c->alloc_to = &c->stat->allocs;
     {
         std::vector<PersonLinks> lk(N);
         for (size_t p = 0; p < N; p++) {
@@ -1590,16 +1716,7 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         { int32_t* t; UP(t, pop->place_group_ofs[pt], np + 1); pl.group_ofs = t; }
         { int32_t* t; UP(t, pop->group_start[pt], ng); pl.group_start = t; }
         { int32_t* t; UP(t, pop->group_size[pt], ng); pl.group_size = t; }
-        AL(pl.close_start, np); AL(pl.close_end, np); AL(pl.prob_close, np);
     }
-    AL(d.infection_time, N); AL(d.recovery_time, N); AL(d.sari_time, N); AL(d.critical_time, N);
-    AL(d.stepdown_time, N); AL(d.detected_time, N); AL(d.prob_absent, N); AL(d.prob_care, N);
-    AL(d.infector, N); AL(d.listpos, N); AL(d.infect_type, N); AL(d.pstep, N);
-    AL(d.S, NC); AL(d.L, NC); AL(d.I, NC); AL(d.R, NC); AL(d.D, NC); AL(d.S0, NC);
-    AL(d.tot_prob, NC); AL(d.slots, N); AL(d.mark, N);
-    AL(d.socdist, NM); AL(d.moverest, NM);
-    CK(cudaMemsetAsync(d.socdist, 0, NM, c->stream));
-    CK(cudaMemsetAsync(d.moverest, 0, NM, c->stream));
     // proposal blocks
     int bs = params->block_cells;
     if (bs <= 0) {
@@ -1627,40 +1744,52 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         { int32_t* t; UP(t, cells.data(), NC); d.block_cells = t; }
         CK(cudaStreamSynchronize(c->stream));
     }
-    AL(d.block_cum, NC); AL(d.block_S0, (size_t)d.NB); AL(d.block_row_cum, (size_t)d.NB * d.NB);
-    AL(d.block_bound_tab, (size_t)d.NB * d.NB);
-    AL(d.block_guide, (size_t)d.NB * d.NB); AL(d.cell_guide, NC);
-    // scratch
-    {
+    {   // UpdateProbs denominators and the buffers only their pass uses
         size_t G = (size_t)params->ncw * params->nch;
-        AL(c->S0g, G); AL(c->Ng, G); AL(c->Ag, G); AL(c->Bg, G);
+        AL(c->Ng, G); AL(c->Bg, G);
         const size_t nchunks = (params->nch + kTotProbRowChunk - 1) / kTotProbRowChunk;
-        AL(c->Apart, nchunks * G); AL(c->Bpart, nchunks * G);
-        AL(c->rowS, (size_t)params->nch); AL(c->rowN, (size_t)params->nch);
+        AL(c->Bpart, nchunks * G);
+        AL(c->rowN, (size_t)params->nch);
     }
-    AL(d.claim, N); AL(d.queue, N); AL(d.counts, kCntN); AL(d.touched, NC); AL(d.cell_flag, NC + 4);
-    AL(d.act, N); AL(d.act_cell, N); AL(d.cnt, NC); AL(d.cnt_ofs, N);
-    AL(d.cmap, 2 * N); d.cmap_cap = (int32_t)(2 * N);
-    AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH);
-    AL(d.place_work, N * (size_t)(NPT > 0 ? NPT : 1));
-    AL(d.close_window, 2);
-    CK(cudaMemcpyAsync(d.close_window, kNoClosures, sizeof(kNoClosures), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(d.claim, 0xff, sizeof(unsigned long long) * N, c->stream));
-    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
-    CK(cudaMemsetAsync(d.cell_flag, 0, NC + 4, c->stream));
-    CK(cudaMemsetAsync(d.hh_flag, 0, NH + 4, c->stream));
-    CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * NC, c->stream));
-    CK(cudaMemsetAsync(d.pstep, 0, N, c->stream));
-    { cs_params* t; UP(t, params, 1); c->dP = t; d.P = t; }
-    { DevIv iv{1e10, 0, 1e10, 0}; DevIv* t; UP(t, &iv, 1); c->dIv = t; d.iv = t; }
-    { DevStep* t; AL(t, 1); d.step = t; CK(cudaMemsetAsync(t, 0, sizeof(DevStep), c->stream)); }
-    { cs_counters* t; AL(t, 1); c->dC = t; d.C = t; CK(cudaMemsetAsync(t, 0, sizeof(cs_counters), c->stream)); }
+    c->alloc_to = nullptr;
 #undef UP
 #undef AL
-    CK(cudaStreamSynchronize(c->stream));
+    // ---- dynamic state of this realisation
+    r = alloc_dynamic(c);
+    if (r) return r;
     r = build_kernel_rows(c);
     if (r) return r;
     r = tot_prob_pass(c, true);  // the n-weighted denominators never change
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+int cs_gpu_create_replica(const cs_gpu_ctx* base, cs_gpu_ctx** out)
+{
+    if (!out) return CS_E_ARG;
+    cs_gpu_ctx* c = new cs_gpu_ctx();
+    *out = c;
+    if (!base || !base->stat) return set_err(c, CS_E_ARG, "replica of a null or unfinished context");
+    int r;
+    c->device = base->device;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->grid = base->grid;
+    c->hp = base->hp;
+    c->stat = base->stat;
+    c->d = base->d;           // static pointers and sizes; dynamic ones are replaced below
+    c->Ng = base->Ng; c->Bg = base->Bg; c->Bpart = base->Bpart; c->rowN = base->rowN;
+    c->Gtab = base->Gtab;
+    DevPop& d = c->d;
+    {
+        PersonHot* ph;
+        if ((r = dalloc(c, &ph, (size_t)d.N))) return r;
+        // static fields of the base's records; begin_run resets the dynamic ones
+        CK(cudaMemcpyAsync(ph, base->d.hot, sizeof(PersonHot) * d.N, cudaMemcpyDeviceToDevice, c->stream));
+        d.hot = ph;
+    }
+    r = alloc_dynamic(c);
     if (r) return r;
     CK(cudaStreamSynchronize(c->stream));
     return CS_OK;
@@ -1674,9 +1803,11 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (void* p : c->allocs) cudaFree(p);
-    if (c->Gtab) cudaFree(c->Gtab);
+    c->stat.reset();   // frees the static arrays when no replica still uses them
+    if (c->xfer) cudaFree(c->xfer);
     if (c->d_seed_list) cudaFree(c->d_seed_list);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    cudaStream_t own = c->own_stream ? c->own_stream : c->stream;   // never a batch's stream
+    if (own) cudaStreamDestroy(own);
     delete c;
 }
 
@@ -1696,12 +1827,14 @@ int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
                           params->kernel_expansion != o.kernel_expansion ||
                           memcmp(params->sinx, o.sinx, sizeof(o.sinx)) || memcmp(params->cosx, o.cosx, sizeof(o.cosx)) ||
                           memcmp(params->asin2sqx, o.asin2sqx, sizeof(o.asin2sqx));
+    if (geometry && c->stat.use_count() > 1)
+        return set_err(c, CS_E_UNSUPPORTED, "set_params may not change the geometry of a population shared by replicas");
     c->hp = *params;
     CK(cudaMemcpyAsync(c->dP, params, sizeof(cs_params), cudaMemcpyHostToDevice, c->stream));
     if (geometry) {   // the kernel rows and the n-weighted denominators depend on it
         CK(cudaStreamSynchronize(c->stream));
-        if (c->Gtab) cudaFree(c->Gtab);
-        c->Gtab = nullptr;
+        if (c->stat->Gtab) cudaFree(c->stat->Gtab);
+        c->stat->Gtab = c->Gtab = nullptr;
         r = build_kernel_rows(c);
         if (r == CS_OK) r = tot_prob_pass(c, true);
         if (r) return r;
@@ -1720,11 +1853,12 @@ static int build_kernel_rows(cs_gpu_ctx* c)
     const cs_params& P = c->hp;
     size_t n = (size_t)P.nch * P.nch * P.ncw;
     if (n * sizeof(float) > kGtabMaxBytes) return CS_OK;
-    if (cudaMalloc(&c->Gtab, n * sizeof(float)) != cudaSuccess) {
+    if (cudaMalloc(&c->stat->Gtab, n * sizeof(float)) != cudaSuccess) {
         (void)cudaGetLastError();
-        c->Gtab = nullptr;
+        c->stat->Gtab = c->Gtab = nullptr;
         return CS_OK;   // not enough memory: evaluate on the fly
     }
+    c->Gtab = c->stat->Gtab;
     unsigned long long* oor = nullptr;
     CK(cudaMalloc(&oor, sizeof(unsigned long long)));
     CK(cudaMemsetAsync(oor, 0, sizeof(unsigned long long), c->stream));
@@ -1734,8 +1868,8 @@ static int build_kernel_rows(cs_gpu_ctx* c)
     CK(cudaStreamSynchronize(c->stream));
     cudaFree(oor);
     if (h) {
-        cudaFree(c->Gtab);
-        c->Gtab = nullptr;
+        cudaFree(c->stat->Gtab);
+        c->stat->Gtab = c->Gtab = nullptr;
     }
     return CS_OK;
 }
@@ -1843,6 +1977,7 @@ int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, i
     (void)update_probs;  // a fresh run has S0 = n and tot_prob = 1 exactly
     DevPop& d = c->d;
     c->seed = seed;
+    CK(cudaMemcpyAsync(c->d_seed, &c->seed, sizeof(c->seed), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
     CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
@@ -1967,11 +2102,200 @@ int cs_gpu_step(cs_gpu_ctx* c, double t, int run)
     return CS_OK;
 }
 
+int cs_gpu_set_grid(cs_gpu_ctx* c, int blocks)
+{
+    if (!c || blocks <= 0) return CS_E_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    c->grid = blocks;
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+    return CS_OK;
+}
+
+int cs_gpu_grid(const cs_gpu_ctx* c) { return c ? c->grid : 0; }
+
 int cs_gpu_use_graphs(cs_gpu_ctx* c, int enable)
 {
     if (!c) return CS_E_ARG;
     c->use_graph = enable != 0;
     return CS_OK;
+}
+
+// ------------------------------------------------------------ batched steps
+// A batch steps many realisations (contexts, each with its own population or a
+// replica sharing one) with one CUDA graph per timestep: the graph holds one
+// branch per member, so the members' kernels run side by side on the GPU.  While
+// the batch exists every member's work goes to the batch's stream, which keeps a
+// member's own calls (UpdateProbs, interventions, counters) ordered with the
+// batched steps.
+struct cs_gpu_batch {
+    int device = 0;
+    std::vector<cs_gpu_ctx*> members;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> branch;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> member_launches;
+    double* d_t = nullptr;   // the timestep's t, read by every member's k_set_step
+    char err[512] = {0};
+};
+
+static int batch_err(cs_gpu_batch* b, int code, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(b->err, sizeof(b->err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define BCK(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return batch_err(b, CS_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static void batch_drop_graph(cs_gpu_batch* b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+int cs_gpu_batch_create(cs_gpu_ctx* const* members, int n, cs_gpu_batch** out)
+{
+    if (!out || !members || n <= 0) return CS_E_ARG;
+    cs_gpu_batch* b = new cs_gpu_batch();
+    *out = b;
+    b->device = members[0] ? members[0]->device : 0;
+    for (int k = 0; k < n; k++) {
+        cs_gpu_ctx* m = members[k];
+        if (!m) return batch_err(b, CS_E_ARG, "member %d is null", k);
+        if (m->device != b->device) return batch_err(b, CS_E_ARG, "member %d is on device %d, not %d", k, m->device, b->device);
+        if (m->own_stream) return batch_err(b, CS_E_STATE, "member %d already belongs to a batch", k);
+        for (int j = 0; j < k; j++)
+            if (members[j] == m) return batch_err(b, CS_E_ARG, "member %d appears twice", k);
+    }
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BCK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    BCK(cudaMalloc(&b->d_t, sizeof(double)));
+    b->members.assign(members, members + n);
+    b->branch.resize(n);
+    b->join.resize(n);
+    b->member_launches.assign(n, 0);
+    for (int k = 0; k < n; k++) {
+        BCK(cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking));
+        BCK(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+        cs_gpu_ctx* m = b->members[k];
+        BCK(cudaStreamSynchronize(m->stream));
+        m->own_stream = m->stream;
+        m->stream = b->stream;
+    }
+    return CS_OK;
+}
+
+const char* cs_gpu_batch_last_error(const cs_gpu_batch* b) { return b ? b->err : "null batch"; }
+
+static int batch_capture(cs_gpu_batch* b, double t, int run)
+{
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    BCK(cudaEventRecord(b->fork, b->stream));
+    int r = CS_OK;
+    const int n = (int)b->members.size();
+    for (int k = 0; k < n && r == CS_OK; k++) {
+        cs_gpu_ctx* m = b->members[k];
+        if (cudaStreamWaitEvent(b->branch[k], b->fork, 0) != cudaSuccess) { r = CS_E_CUDA; break; }
+        m->stream = b->branch[k];
+        m->d.t_src = b->d_t;   // only the captured copies read t from the batch
+        long long l0 = m->launches;
+        r = step_eager(m, t, run);
+        b->member_launches[k] = m->launches - l0;
+        m->launches = l0;
+        m->d.t_src = nullptr;
+        m->stream = b->stream;
+        if (r) {
+            batch_err(b, r, "member %d: %s", k, m->err);
+            break;
+        }
+        if (cudaEventRecord(b->join[k], b->branch[k]) != cudaSuccess ||
+            cudaStreamWaitEvent(b->stream, b->join[k], 0) != cudaSuccess) r = CS_E_CUDA;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (r || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return r ? r : batch_err(b, CS_E_CUDA, "batch capture: %s", cudaGetErrorString(e));
+    }
+    BCK(cudaGraphInstantiate(&b->exec, g, 0));
+    b->graph = g;
+    return CS_OK;
+}
+
+int cs_gpu_batch_step(cs_gpu_batch* b, double t, int run)
+{
+    if (!b) return CS_E_ARG;
+    for (size_t k = 0; k < b->members.size(); k++)
+        if (!b->members[k]->run_started) return batch_err(b, CS_E_STATE, "member %zu: step before begin_run", k);
+    if (!b->exec) {
+        int r = batch_capture(b, t, run);
+        if (r) return r;
+    }
+    // every member's k_set_step reads t (and its run's seed) from device memory
+    BCK(cudaMemcpyAsync(b->d_t, &t, sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaGraphLaunch(b->exec, b->stream));
+    for (size_t k = 0; k < b->members.size(); k++) b->members[k]->launches += b->member_launches[k];
+    return CS_OK;
+}
+
+// Launch shape of every member's grid-stride kernels (blocks); the batch graph is
+// captured again at the next step.  Results do not depend on it.
+int cs_gpu_batch_set_grid(cs_gpu_batch* b, int blocks)
+{
+    if (!b || blocks <= 0) return CS_E_ARG;
+    BCK(cudaStreamSynchronize(b->stream));
+    for (cs_gpu_ctx* m : b->members) {
+        m->grid = blocks;
+        if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
+        if (m->graph) cudaGraphDestroy(m->graph);
+        m->graph_exec = nullptr;
+        m->graph = nullptr;
+    }
+    batch_drop_graph(b);
+    return CS_OK;
+}
+
+void* cs_gpu_batch_stream(cs_gpu_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int cs_gpu_batch_sync(cs_gpu_batch* b)
+{
+    if (!b) return CS_E_ARG;
+    BCK(cudaStreamSynchronize(b->stream));
+    return CS_OK;
+}
+
+void cs_gpu_batch_destroy(cs_gpu_batch* b)
+{
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    for (cs_gpu_ctx* m : b->members)
+        if (m && m->own_stream) {
+            m->stream = m->own_stream;
+            m->own_stream = nullptr;
+        }
+    for (cudaStream_t st : b->branch) if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : b->join) if (ev) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->d_t) cudaFree(b->d_t);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
 }
 
 int cs_gpu_set_interventions(cs_gpu_ctx* c, const cs_interventions* iv)
@@ -2096,24 +2420,47 @@ __global__ void k_pack_hot(DevPop d, const int8_t* inf, const uint8_t* sev, cons
     }
 }
 
+// Device staging of the ten per-person fields that PersonHot packs, for state
+// transfers: one buffer per context, allocated on first use and kept, so repeated
+// uploads and downloads allocate nothing.
+struct XferSlices {
+    int8_t* inf; uint8_t* sev; uint8_t* fl; uint16_t *lt, *as, *ae, *iso, *qs; float *infn, *susc;
+};
+
+static int xfer_slices(cs_gpu_ctx* c, XferSlices* x)
+{
+    const size_t N = c->d.N;
+    const size_t sizes[10] = {N, N, N, 2 * N, 2 * N, 2 * N, 2 * N, 2 * N, 4 * N, 4 * N};
+    size_t ofs[10], total = 0;
+    for (int k = 0; k < 10; k++) { ofs[k] = total; total += (sizes[k] + 255) / 256 * 256; }
+    if (!c->xfer) CK(cudaMalloc(&c->xfer, total));
+    char* b = (char*)c->xfer;
+    x->inf = (int8_t*)(b + ofs[0]); x->sev = (uint8_t*)(b + ofs[1]); x->fl = (uint8_t*)(b + ofs[2]);
+    x->lt = (uint16_t*)(b + ofs[3]); x->as = (uint16_t*)(b + ofs[4]); x->ae = (uint16_t*)(b + ofs[5]);
+    x->iso = (uint16_t*)(b + ofs[6]); x->qs = (uint16_t*)(b + ofs[7]);
+    x->infn = (float*)(b + ofs[8]); x->susc = (float*)(b + ofs[9]);
+    return CS_OK;
+}
+
 int cs_gpu_download_state(cs_gpu_ctx* c, const cs_state_view* v)
 {
     if (!c || !v) return CS_E_ARG;
     DevPop& d = c->d;
     size_t N = d.N, NC = d.NC;
-    // person record fields go through a staging buffer (10 fields)
-    std::vector<void*> tmp;
-    auto stage = [&](size_t bytes) -> void* { void* p = nullptr; if (cudaMalloc(&p, bytes) == cudaSuccess) tmp.push_back(p); return p; };
-    int8_t* dinf = v->inf ? (int8_t*)stage(N) : nullptr;
-    uint8_t* dsev = v->severity ? (uint8_t*)stage(N) : nullptr;
-    uint8_t* dfl = v->flags ? (uint8_t*)stage(N) : nullptr;
-    uint16_t* dlt = v->latent_time ? (uint16_t*)stage(2 * N) : nullptr;
-    uint16_t* das = v->absent_start_time ? (uint16_t*)stage(2 * N) : nullptr;
-    uint16_t* dae = v->absent_stop_time ? (uint16_t*)stage(2 * N) : nullptr;
-    uint16_t* diso = v->isolation_start_time ? (uint16_t*)stage(2 * N) : nullptr;
-    uint16_t* dqs = v->quar_start_time ? (uint16_t*)stage(2 * N) : nullptr;
-    float* dinfn = v->infectiousness ? (float*)stage(4 * N) : nullptr;
-    float* dsusc = v->susc ? (float*)stage(4 * N) : nullptr;
+    // person record fields go through the staging slices (10 fields)
+    XferSlices x;
+    int r0 = xfer_slices(c, &x);
+    if (r0) return r0;
+    int8_t* dinf = v->inf ? x.inf : nullptr;
+    uint8_t* dsev = v->severity ? x.sev : nullptr;
+    uint8_t* dfl = v->flags ? x.fl : nullptr;
+    uint16_t* dlt = v->latent_time ? x.lt : nullptr;
+    uint16_t* das = v->absent_start_time ? x.as : nullptr;
+    uint16_t* dae = v->absent_stop_time ? x.ae : nullptr;
+    uint16_t* diso = v->isolation_start_time ? x.iso : nullptr;
+    uint16_t* dqs = v->quar_start_time ? x.qs : nullptr;
+    float* dinfn = v->infectiousness ? x.infn : nullptr;
+    float* dsusc = v->susc ? x.susc : nullptr;
     k_unpack_hot<<<c->grid, kThreads, 0, c->stream>>>(d, dinf, dsev, dfl, dlt, das, dae, diso, dqs, dinfn, dsusc);
     c->launches++;
     int rc = CS_OK;
@@ -2129,7 +2476,6 @@ int cs_gpu_download_state(cs_gpu_ctx* c, const cs_state_view* v)
     DL(cell_D, d.D, 4 * NC); DL(cell_S0, d.S0, 4 * NC); DL(cell_tot_prob, d.tot_prob, 8 * NC); DL(cell_slots, d.slots, 4 * N);
 #undef DL
     cudaError_t e = cudaStreamSynchronize(c->stream);
-    for (void* p : tmp) cudaFree(p);
     if (e != cudaSuccess) return set_err(c, CS_E_CUDA, "download sync: %s", cudaGetErrorString(e));
     return rc;
 }
@@ -2145,25 +2491,17 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
         !v->ProbAbsent || !v->ProbCare || !v->infector || !v->infect_type || !v->listpos || !v->cell_S || !v->cell_L ||
         !v->cell_I || !v->cell_R || !v->cell_D || !v->cell_S0 || !v->cell_tot_prob || !v->cell_slots)
         return set_err(c, CS_E_ARG, "upload_state needs every field of the view");
-    std::vector<void*> tmp;
-    auto stage = [&](const void* src, size_t bytes) -> void* {
-        void* p = nullptr;
-        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
-        tmp.push_back(p);
-        cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
-        return p;
-    };
-    int8_t* dinf = (int8_t*)stage(v->inf, N);
-    uint8_t* dsev = (uint8_t*)stage(v->severity, N);
-    uint8_t* dfl = (uint8_t*)stage(v->flags, N);
-    uint16_t* dlt = (uint16_t*)stage(v->latent_time, 2 * N);
-    uint16_t* das = (uint16_t*)stage(v->absent_start_time, 2 * N);
-    uint16_t* dae = (uint16_t*)stage(v->absent_stop_time, 2 * N);
-    uint16_t* diso = (uint16_t*)stage(v->isolation_start_time, 2 * N);
-    uint16_t* dqs = (uint16_t*)stage(v->quar_start_time, 2 * N);
-    float* dinfn = (float*)stage(v->infectiousness, 4 * N);
-    float* dsusc = (float*)stage(v->susc, 4 * N);
-    if (tmp.size() != 10) { for (void* p : tmp) cudaFree(p); return set_err(c, CS_E_CUDA, "upload staging failed"); }
+    XferSlices x;
+    int r0 = xfer_slices(c, &x);
+    if (r0) return r0;
+#define STG(dst, src, bytes) CK(cudaMemcpyAsync(dst, v->src, bytes, cudaMemcpyHostToDevice, c->stream))
+    STG(x.inf, inf, N); STG(x.sev, severity, N); STG(x.fl, flags, N); STG(x.lt, latent_time, 2 * N);
+    STG(x.as, absent_start_time, 2 * N); STG(x.ae, absent_stop_time, 2 * N); STG(x.iso, isolation_start_time, 2 * N);
+    STG(x.qs, quar_start_time, 2 * N); STG(x.infn, infectiousness, 4 * N); STG(x.susc, susc, 4 * N);
+#undef STG
+    int8_t* dinf = x.inf; uint8_t* dsev = x.sev; uint8_t* dfl = x.fl;
+    uint16_t *dlt = x.lt, *das = x.as, *dae = x.ae, *diso = x.iso, *dqs = x.qs;
+    float *dinfn = x.infn, *dsusc = x.susc;
     k_pack_hot<<<c->grid, kThreads, 0, c->stream>>>(d, dinf, dsev, dfl, dlt, das, dae, diso, dqs, dinfn, dsusc);
     c->launches++;
 #define UL(src, dst, bytes) CK(cudaMemcpyAsync(dst, v->src, bytes, cudaMemcpyHostToDevice, c->stream))
@@ -2179,10 +2517,10 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
     CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
     CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
     c->seed = seed;
+    CK(cudaMemcpyAsync(c->d_seed, &c->seed, sizeof(c->seed), cudaMemcpyHostToDevice, c->stream));
     int r = reset_run_level(c, seed);
     if (r == CS_OK) r = rebuild_blocks(c);
     cudaError_t e = cudaStreamSynchronize(c->stream);
-    for (void* p : tmp) cudaFree(p);
     if (r) return r;
     if (e != cudaSuccess) return set_err(c, CS_E_CUDA, "upload sync: %s", cudaGetErrorString(e));
     c->run_started = true;

@@ -402,6 +402,67 @@ int cs_gpu_update_probs_static(cs_gpu_ctx* ctx, int do_place);
 int cs_gpu_step(cs_gpu_ctx* ctx, double t, int run);
 int cs_gpu_use_graphs(cs_gpu_ctx* ctx, int enable);
 
+/* Blocks of the grid-stride kernels (default 8 per SM).  Results do not depend
+ * on it: every list the kernels fill is read order-independently.  A captured
+ * step graph is dropped and captured again. */
+int cs_gpu_set_grid(cs_gpu_ctx* ctx, int blocks);
+int cs_gpu_grid(const cs_gpu_ctx* ctx);
+
+/* ---- Realisations stepped together.  No counterpart in the reference, which
+ * runs realisations one after another (src/CovidSim.cpp:371-399).
+ *
+ * cs_gpu_create_replica: a context for another realisation of `base`'s population.
+ * It shares base's static device arrays (households, place memberships, cell
+ * lists, kernel tables, proposal-block layout, UpdateProbs rows) and allocates
+ * only dynamic state; the shared arrays live until the last sharing context is
+ * destroyed.  Its parameters start as base's; cs_gpu_set_params may change them
+ * except the geometry.
+ *
+ * cs_gpu_batch: n member contexts (replicas, or contexts of other populations,
+ * on one device) advanced by one CUDA graph per timestep with one branch per
+ * member, so their kernels run side by side.  While the batch exists, members'
+ * own calls run on the batch's stream, ordered with the batched steps.  Destroy
+ * the batch before its members. */
+int cs_gpu_create_replica(const cs_gpu_ctx* base, cs_gpu_ctx** out);
+
+typedef struct cs_gpu_batch cs_gpu_batch;
+int cs_gpu_batch_create(cs_gpu_ctx* const* members, int n, cs_gpu_batch** out);
+/* One timestep (InfectSweep + IncubRecoverySweep) of every member at time t. */
+int cs_gpu_batch_step(cs_gpu_batch* batch, double t, int run);
+/* cs_gpu_set_grid for every member. */
+int cs_gpu_batch_set_grid(cs_gpu_batch* batch, int blocks);
+int cs_gpu_batch_sync(cs_gpu_batch* batch);
+void* cs_gpu_batch_stream(cs_gpu_batch* batch);
+const char* cs_gpu_batch_last_error(const cs_gpu_batch* batch);
+void cs_gpu_batch_destroy(cs_gpu_batch* batch);
+
+/* ---- Scenario surrogate.  No counterpart in the reference, which has no learned
+ * model.  A network mapping 8 scenario parameters (scaled to [0, 1]) to 365
+ * days x 4 daily outputs, trained on the simulator's own trajectories and used
+ * to screen scenario sweeps; the simulator re-runs what it ranks highly.
+ *   x [n, 8] -> 4 x (Linear 512 + ReLU) -> Linear 256 + ReLU -> Linear 2944 + ReLU
+ *   -> [n, 46, 64] -> 3 x (nearest upsample x2, Conv1d k=5 pad 2): 64 -> 64 -> 32 -> 4,
+ *      ReLU after the first two -> first 365 time points -> y [n, 365, 4]
+ * Matrix products run on the tensor cores in BF16 with FP32 accumulation; master
+ * weights, gradients and Adam moments are FP32.  Parameters travel as one flat
+ * FP32 array: per layer its weight [out, in] (a convolution's [out, tap * in + c])
+ * then its bias [out], layers in the order above. */
+typedef struct cs_sur cs_sur;
+size_t cs_sur_num_params(void);
+int cs_sur_create(int max_batch, int device, cs_sur** out);
+void cs_sur_destroy(cs_sur* sur);
+const char* cs_sur_last_error(const cs_sur* sur);
+/* Set the FP32 weights (and reset the Adam moments); read them back. */
+int cs_sur_set_params(cs_sur* sur, const float* flat);
+int cs_sur_get_params(cs_sur* sur, float* flat);
+/* y [n, 365, 4] for x [n, 8]; any n (processed in batches of max_batch). */
+int cs_sur_forward(cs_sur* sur, const float* x, int n, float* y);
+/* Mean squared error against target [n, 365, 4] and, when grad is not NULL, its
+ * gradient in the flat layout; n <= max_batch. */
+int cs_sur_loss_grad(cs_sur* sur, const float* x, const float* target, int n, float* loss, float* grad);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on a batch; loss may be NULL. */
+int cs_sur_train_step(cs_sur* sur, const float* x, const float* target, int n, float lr, float* loss);
+
 int cs_gpu_set_interventions(cs_gpu_ctx* ctx, const cs_interventions* iv);
 /* DoPlaceClose (src/Update.cpp:1095-1258) for every place of type t in the listed
  * microcells (all when mcells == NULL), closing [start, stop) in timesteps. */

@@ -26,10 +26,15 @@ STOCK = os.path.join(HERE, "_ref", "CovidSim")
 # 1207-1216): 8 bytes per cell pair.  Its sample grids are chosen to fit in memory
 # and set up in seconds.
 SAMPLES = {
-    "c1": dict(people=1_000_000, cell_deg=1.0 / 60, days=365, interventions=True,
-               note="1M people of the 10M workload's generator on the 120x120 grid the reference can allocate "
-                    "(its dense cell tables need 8 B x cells^2: 1.04 TB at 600x600), C1 interventions, 365 d"),
-    "c0": dict(people=1_000_000, cell_deg=1.0 / 120, days=120, interventions=False,
+    # The 10M-person workload scaled down to what the reference sets up in about a
+    # minute: its dense cell tables (8 B x cells^2) rule out the 600x600 grid
+    # (1.04 TB) and its set-up time grows with people and with cells^2.  The
+    # sample keeps the workload's generator, its 28 people per cell and its
+    # interventions, with the ICU trigger scaled per head (100 per 10M).
+    "c1": dict(people=115_000, cell_deg=1.0 / 32, days=365, interventions=True, threshold=1,
+               note="115k people of the 10M workload's generator on 64x64 cells (28 people per cell, as the "
+                    "10M workload), C1 interventions with the ICU trigger scaled per head, 365 d"),
+    "c0": dict(people=1_000_000, cell_deg=1.0 / 120, days=120, interventions=False, threshold=100,
                note="1M people, 240x240 cells (26.5 GB of dense cell tables), 120 d"),
 }
 
@@ -42,7 +47,8 @@ def parse_timing(stderr):
     return rows
 
 
-def run_reference(pop, days, nr=1, threads=None, interventions=False, workdir=None, seeds=(98798150, 729101, 17389101, 4797132),
+def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=100, workdir=None,
+                  seeds=(98798150, 729101, 17389101, 4797132),
                   binary=BIN, keep=False, timeout=3000, series=False):
     sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
     from covidsim_b200 import refconfig
@@ -50,7 +56,7 @@ def run_reference(pop, days, nr=1, threads=None, interventions=False, workdir=No
     wd = workdir or tempfile.mkdtemp(prefix="csref_")
     try:
         f = refconfig.write_workload(wd, pop, days, interventions=interventions)
-        params = refconfig.intervention_params(interventions)
+        params = refconfig.intervention_params(interventions, threshold=threshold)
         pre = refconfig.pre_params(days, pop.grid, 2.4, 100)
         pre["Number of realisations"] = nr
         pre["Number of non-extinct realisations"] = nr
@@ -94,7 +100,7 @@ def time_reference(workload, steps=3, warmup=3):
     s = SAMPLES[workload]
     grid = population.make_grid(cell_deg=s["cell_deg"], nmcl=10)
     pop = population.generate(s["people"], grid, sigma=1.2, seed=98798150)
-    res = run_reference(pop, s["days"], nr=warmup + steps, interventions=s["interventions"])
+    res = run_reference(pop, s["days"], nr=warmup + steps, interventions=s["interventions"], threshold=s["threshold"])
     rows = res["rows"][warmup:warmup + steps]
     if len(rows) < steps:
         return {"unavailable": "reference produced %d timed realisations" % len(rows)}
