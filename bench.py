@@ -58,11 +58,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["c2"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["c2", "c4"])
     ap.add_argument("--c2-scale", type=float, default=1.0,
                     help="c2 only: population sizes times this factor (1.0 = 1/4/10/20 M)")
     ap.add_argument("--c2-per-size", type=int, default=16, help="c2 only: realisations per population size")
     ap.add_argument("--c2-days", type=int, default=365, help="c2 only: days per realisation")
+    ap.add_argument("--c4-train", type=int, default=256, help="c4 only: training scenarios")
+    ap.add_argument("--c4-seeds", type=int, default=4, help="c4 only: seeds per training scenario")
+    ap.add_argument("--c4-sweep", type=int, default=100_000, help="c4 only: scenarios screened")
+    ap.add_argument("--c4-rerun", type=int, default=100, help="c4 only: top scenarios re-run by the simulator")
+    ap.add_argument("--c4-people", type=int, default=1_000_000, help="c4 only: population size")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-out", default=None, help="write per-kernel times to this JSON file")
@@ -473,10 +478,85 @@ def run_c2(args):
     }
 
 
+# -------------------------------------------------------- surrogate sweep
+def run_c4(args):
+    """Scenario sweep with the surrogate: simulate training scenarios (batched,
+    several seeds each), train the network, screen the sweep, re-run the
+    scenarios ranked best (lowest critical-care peak) with 8 seeds each, and
+    report the network's error on those against the simulator's ensemble mean.
+    The plain method (every sweep scenario simulated one realisation at a time
+    with 8 seeds) is timed on a sample and extrapolated."""
+    import torch
+    torch.cuda.set_device(0)
+    from covidsim_b200 import population, params as prm, sim, surrogate
+    grid = population.make_grid(cell_deg=1.0 / 120, nmcl=10)
+    pop = population.generate(args.c4_people, grid, sigma=1.2, seed=98798150)
+    P, lk, hr = prm.build_params(pop.grid)
+    t_all = time.perf_counter()
+    # 1. training trajectories
+    train = surrogate.sample_scenarios(args.c4_train, seed=101)
+    t0 = time.perf_counter()
+    idx, ys = surrogate.simulate(pop, P, lk, hr, train, args.c4_seeds, batch_size=64)
+    t_sim = time.perf_counter() - t0
+    xs = surrogate.to_unit(train[idx]).astype(np.float32)
+    # 2. training
+    net = surrogate.Surrogate(max_batch=256, seed=5)
+    t0 = time.perf_counter()
+    hist = net.fit(xs, ys, epochs=300, lr=1e-3, batch=256)
+    t_train = time.perf_counter() - t0
+    # 3. screening
+    sweep = surrogate.sample_scenarios(args.c4_sweep, seed=202)
+    t0 = time.perf_counter()
+    pred = net.predict(surrogate.to_unit(sweep).astype(np.float32))
+    t_screen = time.perf_counter() - t0
+    top = np.argsort(np.expm1(pred[:, :, 2]).max(axis=1))[:args.c4_rerun]
+    # 4. the simulator judges the top scenarios: 8 seeds each
+    t0 = time.perf_counter()
+    ridx, rys = surrogate.simulate(pop, P, lk, hr, sweep[top], 8, batch_size=64, seed0=777)
+    t_rerun = time.perf_counter() - t0
+    t_pipeline = time.perf_counter() - t_all
+    ens = np.stack([np.expm1(rys[ridx == k]).mean(axis=0) for k in range(len(top))])   # natural scale
+    pr = np.expm1(pred[top])
+    icu_err = np.linalg.norm(pr[:, :, 2] - ens[:, :, 2], axis=1) / np.maximum(np.linalg.norm(ens[:, :, 2], axis=1), 1e-12)
+    # 5. the plain method: one realisation at a time, timed on a sample
+    s1 = sim.Simulation(pop, P, lk, hr)
+    beta24, _ = sim.calibrate_local_beta(pop, P, 2.4)
+    n_plain = 8
+    t0 = time.perf_counter()
+    for k in range(n_plain):
+        q, pol = surrogate.scenario_params(P, beta24, sweep[k])
+        s1.backend.set_params(q)
+        s1.params = q
+        s1.run(9000 + k, surrogate.DAYS, policy=pol)
+    s1.backend.sync()
+    t_one = (time.perf_counter() - t0) / n_plain
+    s1.close()
+    t_plain = t_one * args.c4_sweep * 8
+    net.close()
+    return {
+        "metric": "scenario-sweep speed-up over one-at-a-time simulation", "value": round(t_plain / t_pipeline, 1),
+        "unit": "x", "n_gpus": 1, "higher_is_better": True, "dtype": "bf16 network (fp32 accumulate), f64/f32 simulator",
+        "data": "synthetic (seeded generator, reference parameter set)",
+        "config": {"workload": "surrogate sweep: %d people, %d training scenarios x %d seeds, %d screened, top %d "
+                               "re-run x 8 seeds" % (args.c4_people, args.c4_train, args.c4_seeds, args.c4_sweep,
+                                                     args.c4_rerun)},
+        "seconds": {"simulate_training": round(t_sim, 2), "train": round(t_train, 2), "screen": round(t_screen, 3),
+                    "rerun_top": round(t_rerun, 2), "pipeline": round(t_pipeline, 2),
+                    "one_realisation_plain": round(t_one, 4), "plain_sweep_estimate": round(t_plain, 1)},
+        "train_loss": [round(float(hist[0]), 5), round(float(hist[-1]), 5)],
+        "icu_rel_l2_vs_ensemble_mean": {"median": round(float(np.median(icu_err)), 4),
+                                        "mean": round(float(icu_err.mean()), 4),
+                                        "p90": round(float(np.quantile(icu_err, 0.9)), 4)},
+    }
+
+
 def main():
     args = parse()
     if args.impl == "ours" and args.workload == "c2":
         print(json.dumps(run_c2(args)))
+        return
+    if args.impl == "ours" and args.workload == "c4":
+        print(json.dumps(run_c4(args)))
         return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:
