@@ -146,6 +146,7 @@ def load_library(path=LIB_PATH):
         "cs_gpu_use_graphs": (I, [V, I]),
         "cs_gpu_set_grid": (I, [V, I]),
         "cs_gpu_grid": (I, [V]),
+        "cs_gpu_set_spatial_lanes": (I, [V, I]),
         "cs_gpu_create_replica": (I, [V, P(V)]),
         "cs_gpu_batch_create": (I, [P(V), I, P(V)]),
         "cs_gpu_batch_step": (I, [V, D, I]),

@@ -53,6 +53,9 @@ class GpuBackend:
     def set_grid(self, blocks):
         self._ck(self.lib.cs_gpu_set_grid(self.ctx, blocks), "set_grid")
 
+    def set_spatial_lanes(self, lanes):
+        self._ck(self.lib.cs_gpu_set_spatial_lanes(self.ctx, lanes), "set_spatial_lanes")
+
     def _ck(self, rc, what):
         if rc != 0:
             raise abi.CovidSimError("%s%s: %s" % (self.prefix, what, self.lib.cs_gpu_last_error(self.ctx).decode()))

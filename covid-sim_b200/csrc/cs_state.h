@@ -146,7 +146,9 @@ struct DevPop {
     BlockCell* block_cell_info;  // [NC], rebuilt with S0
     BlockInfo* block_info;       // [NB], S0 rebuilt with S0
     double* block_row_cum;     // [NB][NB]
-    double* block_bound_tab;   // [NB][NB] bound(b, B) for target blocks with people
+    double* block_bound_tab;   // [NB][NB] bound(b, B)
+    int32_t bounds_static;     // 1: all of block_bound_tab was filled once (geometry only);
+                               // 0: k_block_rows fills the entries of blocks with people
     int16_t* block_guide;      // [NB][NB] cut points of each row (Chen & Asau guide table)
     int16_t* cell_guide;       // [NC] cut points of each block's cell list
     // per-step scratch

@@ -199,6 +199,7 @@ struct cs_gpu_ctx {
     uint64_t seed = 0;
     bool run_started = false;
     int grid = 148 * 8;
+    int spatial_lanes = 8;   // lanes per spatial contact (4, 8 or 16)
     // one timestep captured as a CUDA graph and replayed
     bool use_graph = true;
     cudaGraph_t graph = nullptr;
@@ -298,6 +299,7 @@ static int dupload(cs_gpu_ctx* c, T** p, const T* src, size_t n)
 extern "C" {
 static int tot_prob_pass(cs_gpu_ctx* c, bool denominators);
 static int build_kernel_rows(cs_gpu_ctx* c);
+static int build_block_bounds(cs_gpu_ctx* c);
 }
 
 // ================================================================ run start
@@ -471,9 +473,11 @@ struct TotProbGeom {
     int gphys;  // doubles in the padded Gm array
     int nchunks;           // ceil(nch / kTotProbRowChunk)
     int chunks_per_block;  // 1 (partial sums) or nchunks (final sums)
+    int need;              // threads per source row: ceil(ncw / 8)
+    int rpb;               // source rows per block: 2 when two rows fit 256 threads, else 1
     size_t smem(bool denominators) const
     {
-        return sizeof(double) * ((size_t)gphys + (denominators ? 2 : 1) * (size_t)ncwR);
+        return sizeof(double) * ((size_t)rpb * gphys + (denominators ? 2 : 1) * (size_t)ncwR);
     }
 };
 
@@ -486,6 +490,8 @@ static TotProbGeom tot_prob_geom(int ncw, int nch, bool partial)
     g.gphys += g.gphys & 1;   // keep the arrays after Gm 16-byte aligned
     g.nchunks = (nch + kTotProbRowChunk - 1) / kTotProbRowChunk;
     g.chunks_per_block = partial ? 1 : g.nchunks;
+    g.need = (ncw + kTotProbCols - 1) / kTotProbCols;
+    g.rpb = (2 * g.need <= 256) ? 2 : 1;
     return g;
 }
 
@@ -499,13 +505,19 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
     const cs_params& P = *d.P;
     const int ncw = P.ncw, nch = P.nch;
     extern __shared__ __align__(16) double sh[];
-    double* Gp = sh;                  // padded, mirrored kernel row
-    double* Srow = sh + gm.gphys;     // ncwR
-    double* Nrow = Srow + gm.ncwR;    // ncwR (denominator pass only)
-    const int xl0 = (blockIdx.x * blockDim.x + threadIdx.x) * kTotProbCols, yl = blockIdx.y;
+    double* Srow = sh + gm.rpb * gm.gphys;   // ncwR
+    double* Nrow = Srow + gm.ncwR;           // ncwR (denominator pass only)
+    // rpb == 2: threads [0, need) own source row 2*blockIdx.y, [need, 2*need) the
+    // next one, each with its own kernel row Gp; the rest only help fill shared memory
+    const int sub = gm.rpb == 2 ? (int)threadIdx.x / gm.need : 0;
+    const int jcol = gm.rpb == 2 ? (int)threadIdx.x % gm.need : (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int yl0 = blockIdx.y * gm.rpb;
+    const int yl = yl0 + sub;
+    double* Gp = sh + (size_t)min(sub, gm.rpb - 1) * gm.gphys;   // this thread's padded, mirrored kernel row
+    const int xl0 = (sub < gm.rpb && yl < nch) ? jcol * kTotProbCols : ncw;   // ncw: no outputs
     const int q0 = blockIdx.z * gm.chunks_per_block;
     const int q1 = min(q0 + gm.chunks_per_block, gm.nchunks);
-    for (int k = threadIdx.x; k < gm.gphys; k += blockDim.x) Gp[k] = 0.0;
+    for (int k = threadIdx.x; k < gm.rpb * gm.gphys; k += blockDim.x) sh[k] = 0.0;
     for (int k = ncw + threadIdx.x; k < gm.ncwR; k += blockDim.x) {
         Srow[k] = 0.0;
         if (kDenominators) Nrow[k] = 0.0;
@@ -525,13 +537,19 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
             const bool useS = rowS[ym] != 0, useN = kDenominators && rowN[ym] != 0;
             if (!useS && !useN) continue;
             __syncthreads();
-            const float* grow = Gtab ? Gtab + ((size_t)yl * nch + ym) * ncw : nullptr;
-            for (int k = threadIdx.x; k < ncw; k += blockDim.x) {
-                double v = grow ? (double)grow[k] : row_kernel(d, P, k, yl, ym, CSB_CTR(err_kernel_range));
-                Gp[tp_phys(gm.off + k)] = v;
-                Gp[tp_phys(gm.off - k)] = v;
-                Srow[k] = S0g[(size_t)k * nch + ym];
-                if (kDenominators) Nrow[k] = Ng[(size_t)k * nch + ym];
+            for (int e = threadIdx.x; e < gm.rpb * ncw; e += blockDim.x) {
+                const int r = e / ncw, k = e % ncw, ylr = yl0 + r;
+                if (ylr < nch) {
+                    double v = Gtab ? (double)Gtab[((size_t)ylr * nch + ym) * ncw + k]
+                                    : row_kernel(d, P, k, ylr, ym, CSB_CTR(err_kernel_range));
+                    double* G = sh + (size_t)r * gm.gphys;
+                    G[tp_phys(gm.off + k)] = v;
+                    G[tp_phys(gm.off - k)] = v;
+                }
+                if (r == 0) {
+                    Srow[k] = S0g[(size_t)k * nch + ym];
+                    if (kDenominators) Nrow[k] = Ng[(size_t)k * nch + ym];
+                }
             }
             __syncthreads();
             if (xl0 >= ncw) continue;
@@ -602,11 +620,12 @@ __global__ void k_tot_prob_reduce(const double* __restrict__ part, int nparts, s
 // blocks of up to 256 threads (whole warps).
 static void tot_prob_launch_shape(int ncw, int nch, const TotProbGeom& gm, dim3* grid, int* threads)
 {
-    int need = (ncw + kTotProbCols - 1) / kTotProbCols;
-    int tpb = ((need + 31) / 32) * 32;
+    (void)ncw;
+    int tpb = ((gm.rpb * gm.need + 31) / 32) * 32;
     if (tpb > 256) tpb = 256;
     *threads = tpb;
-    *grid = dim3((need + tpb - 1) / tpb, nch, gm.nchunks / gm.chunks_per_block);
+    const int xblocks = gm.rpb == 2 ? 1 : (gm.need + tpb - 1) / tpb;
+    *grid = dim3(xblocks, (nch + gm.rpb - 1) / gm.rpb, gm.nchunks / gm.chunks_per_block);
 }
 
 __global__ void k_tot_prob_finish(DevPop d, const double* Ag, const double* Bg)
@@ -640,8 +659,19 @@ __global__ void k_block_S0(DevPop d)
     }
 }
 
+// Every bound(b, B) of the geometry, once per population; *oor counts distances
+// beyond the kernel table (then the bounds are evaluated per call instead, so that
+// the error counts stay those of the per-call evaluation).
+__global__ void k_block_bounds_all(DevPop d, unsigned long long* oor)
+{
+    const cs_params& P = *d.P;
+    const size_t n = (size_t)d.NB * d.NB;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        d.block_bound_tab[e] = block_bound(d, P, (int)(e / d.NB), (int)(e % d.NB), oor);
+}
+
 // Row b of the proposal table: running sum over B of S0_B * bound(b, B), added in
-// B order by lane 0 so the doubles round exactly as a sequential loop.
+// B order so the doubles round exactly as a sequential loop.
 __global__ void k_block_rows(DevPop d)
 {
     const cs_params& P = *d.P;
@@ -650,13 +680,15 @@ __global__ void k_block_rows(DevPop d)
     int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int b = warp; b < d.NB; b += nwarps) {
         double* row = d.block_row_cum + (size_t)b * d.NB;
+        double* btab = d.block_bound_tab + (size_t)b * d.NB;
         double s = 0.0;
         for (int B0 = 0; B0 < d.NB; B0 += 32) {
             int B = B0 + lane;
             double w = 0.0;
             if (B < d.NB && d.block_info[B].S0 > 0) {
-                double bound = block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
-                d.block_bound_tab[(size_t)b * d.NB + B] = bound;
+                double bound;
+                if (d.bounds_static) bound = btab[B];
+                else btab[B] = bound = block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
                 w = (double)d.block_info[B].S0 * bound;
             }
             for (int k = 0; k < 32; k++) {
@@ -667,17 +699,20 @@ __global__ void k_block_rows(DevPop d)
                 }
             }
         }
-        // guide[k] = first B whose running weight exceeds k/NB of the row total
+        // guide[k] = first B whose running weight exceeds k/NB of the row total (the
+        // last block if none): thresholds and the row both ascend, so each lane
+        // finds its entries by binary search
         __syncwarp();
-        if (lane == 0) {
-            int16_t* guide = d.block_guide + (size_t)b * d.NB;
-            double total = s;
-            int B = 0;
-            for (int k = 0; k < d.NB; k++) {
-                double thr = (double)k * total / (double)d.NB;
-                while (B < d.NB - 1 && row[B] <= thr) B++;
-                guide[k] = (int16_t)B;
+        int16_t* guide = d.block_guide + (size_t)b * d.NB;
+        const double total = s;
+        for (int k = lane; k < d.NB; k += 32) {
+            double thr = (double)k * total / (double)d.NB;
+            int lo = 0, hi = d.NB - 1;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (row[mid] <= thr) lo = mid + 1; else hi = mid;
             }
+            guide[k] = (int16_t)lo;
         }
     }
 }
@@ -885,9 +920,9 @@ __global__ void __launch_bounds__(kThreads) k_infector_places(DevPop d)
 // block row, a slot uniformly among the block's S0 slots, accept with K(d)/bound,
 // redraw on rejection or a dead target.  Draw t of a contact reads its uniforms
 // from Philox blocks 2t and 2t+1 of the contact's stream, so the draws are
-// independent of one another: kSpatialLanes lanes evaluate draws t0..t0+7
-// together and the lowest accepted one wins, exactly as a sequential loop would.
-constexpr int kSpatialLanes = 8;
+// independent of one another: LANES lanes (4, 8 or 16, a tuning choice that does
+// not change results) evaluate draws t0..t0+LANES-1 together and the lowest
+// accepted one wins, exactly as a sequential loop would.
 constexpr uint32_t kSpatialBlocksPerDraw = 2;
 
 // One rejection draw; true when accepted (target alive, u < K(d)/bound).
@@ -924,6 +959,7 @@ __device__ __forceinline__ bool spatial_draw(const DevPop& d, const cs_params& P
     return true;
 }
 
+template <int kSpatialLanes>
 __global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d)
 {
     const cs_params& P = *d.P;
@@ -1417,12 +1453,6 @@ __global__ void k_partition_LI(DevPop d)
     }
 }
 
-__global__ void k_clear_pstep(DevPop d)
-{
-    int nact = d.counts[kCntAct];
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nact; idx += gridDim.x * blockDim.x) d.pstep[d.act[idx]] = 0;
-}
-
 // Deferred household actions, once per household, after every per-person
 // transition of the step: the adult-carer absence of DoCase/DoDetectedCase
 // (src/Update.cpp:736-763, 843-868) and household quarantine (src/Update.cpp:676-708).
@@ -1431,6 +1461,9 @@ __global__ void k_household_after(DevPop d)
     const cs_params& P = *d.P;
     const int ts = d.step->ts;
     const uint64_t seed = d.step->seed;
+    // the step's transition flags are only set on event people: clear them
+    int nev = d.counts[kCntEvents];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) d.pstep[d.act[d.cmap[e]]] = 0;
     int nh = d.counts[kCntHH];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
         int h = d.hh_list[k];
@@ -1589,7 +1622,7 @@ static int alloc_dynamic(cs_gpu_ctx* c)
     CK(cudaMemsetAsync(d.socdist, 0, NM, c->stream));
     CK(cudaMemsetAsync(d.moverest, 0, NM, c->stream));
     AL(d.block_cell_info, NC); AL(d.block_info, (size_t)d.NB); AL(d.block_row_cum, (size_t)d.NB * d.NB);
-    AL(d.block_bound_tab, (size_t)d.NB * d.NB);
+    if (!d.bounds_static) AL(d.block_bound_tab, (size_t)d.NB * d.NB);   // else shared, filled once
     AL(d.block_guide, (size_t)d.NB * d.NB); AL(d.cell_guide, NC);
     {
         size_t G = (size_t)params->ncw * params->nch;
@@ -1751,11 +1784,15 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         AL(c->Bpart, nchunks * G);
         AL(c->rowN, (size_t)params->nch);
     }
+    AL(d.block_bound_tab, (size_t)d.NB * d.NB);
+    d.bounds_static = 1;
     c->alloc_to = nullptr;
 #undef UP
 #undef AL
     // ---- dynamic state of this realisation
     r = alloc_dynamic(c);
+    if (r) return r;
+    r = build_block_bounds(c);
     if (r) return r;
     r = build_kernel_rows(c);
     if (r) return r;
@@ -1836,9 +1873,33 @@ int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
         if (c->stat->Gtab) cudaFree(c->stat->Gtab);
         c->stat->Gtab = c->Gtab = nullptr;
         r = build_kernel_rows(c);
+        if (r == CS_OK) r = build_block_bounds(c);
         if (r == CS_OK) r = tot_prob_pass(c, true);
         if (r) return r;
         CK(cudaStreamSynchronize(c->stream));
+    }
+    return CS_OK;
+}
+
+// bound(b, B) for every pair of proposal blocks, into the table the population's
+// contexts share.  If a distance falls outside the kernel table, this context
+// evaluates the bounds per call into its own table instead.
+static int build_block_bounds(cs_gpu_ctx* c)
+{
+    DevPop& d = c->d;
+    if (!d.bounds_static) return CS_OK;
+    unsigned long long* oor = nullptr;
+    CK(cudaMalloc(&oor, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(oor, 0, sizeof(unsigned long long), c->stream));
+    LAUNCH(k_block_bounds_all, c->grid, kThreads, d, oor);
+    unsigned long long h = 0;
+    CK(cudaMemcpyAsync(&h, oor, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(oor);
+    if (h) {
+        d.bounds_static = 0;
+        int r = dalloc(c, &d.block_bound_tab, (size_t)d.NB * d.NB);
+        if (r) return r;
     }
     return CS_OK;
 }
@@ -1934,7 +1995,8 @@ static int apply_queue(cs_gpu_ctx* c)
     DevPop& d = c->d;
     LAUNCH(k_apply_infections, c->grid, kThreads, d);
     LAUNCH(k_partition_S, c->grid, kThreads, d);
-    CK(cudaMemsetAsync(d.counts + kCntQueue, 0, sizeof(int32_t) * 2, c->stream));  // queue + touched
+    // every sweep leaves all list counters at zero for the next one
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
     return CS_OK;
 }
 
@@ -1995,9 +2057,8 @@ int cs_gpu_begin_run(cs_gpu_ctx* c, uint64_t seed, const int32_t* seed_people, i
 static int build_active(cs_gpu_ctx* c, int mode)
 {
     DevPop& d = c->d;
-    static_assert(kCntContacts == kCntAct + 1 && kCntPlaceWork == kCntAct + 2,
-                  "active, contact and place-work counts are reset together");
-    CK(cudaMemsetAsync(d.counts + kCntAct, 0, sizeof(int32_t) * 3, c->stream));
+    // the list counters are zero here: every sweep (and begin_run, upload_state,
+    // seed_infections) ends by zeroing them
     LAUNCH(k_build_active, (d.NC + kThreads - 1) / kThreads, kThreads, d, mode);
     return CS_OK;
 }
@@ -2013,33 +2074,42 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
     if (r) return r;
     LAUNCH(k_infector_hh_spatial, c->grid, kThreads, d);
     LAUNCH(k_infector_places, c->grid, kThreads, d);
-    LAUNCH(k_spatial, c->grid, kThreads, d);
+    switch (c->spatial_lanes) {
+    case 4: LAUNCH(k_spatial<4>, c->grid, kThreads, d); break;
+    case 16: LAUNCH(k_spatial<16>, c->grid, kThreads, d); break;
+    default: LAUNCH(k_spatial<8>, c->grid, kThreads, d); break;
+    }
     return apply_queue(c);
+}
+
+// IncubRecoverySweep; set_step false when the infect sweep of the same timestep has
+// just written the step's scalars.
+static int incub_sweep(cs_gpu_ctx* c, double t, bool set_step)
+{
+    DevPop& d = c->d;
+    if (set_step) LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
+    int r = build_active(c, 1);
+    if (r) return r;
+    LAUNCH(k_incub_scan, c->grid, kThreads, d);
+    LAUNCH(k_incub_events, c->grid, kThreads, d);
+    LAUNCH(k_partition_LI, c->grid, kThreads, d);
+    LAUNCH(k_household_after, c->grid, kThreads, d);
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));   // all list counters
+    return CS_OK;
 }
 
 int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* c, double t)
 {
     if (!c) return CS_E_ARG;
     if (!c->run_started) return set_err(c, CS_E_STATE, "incub_recovery_sweep before begin_run");
-    DevPop& d = c->d;
-    LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
-    int r = build_active(c, 1);
-    if (r) return r;
-    CK(cudaMemsetAsync(d.counts + kCntEvents, 0, sizeof(int32_t), c->stream));
-    LAUNCH(k_incub_scan, c->grid, kThreads, d);
-    LAUNCH(k_incub_events, c->grid, kThreads, d);
-    LAUNCH(k_partition_LI, c->grid, kThreads, d);
-    LAUNCH(k_clear_pstep, c->grid, kThreads, d);
-    LAUNCH(k_household_after, c->grid, kThreads, d);
-    CK(cudaMemsetAsync(d.counts + kCntTouched, 0, sizeof(int32_t) * 2, c->stream));  // touched + households
-    return CS_OK;
+    return incub_sweep(c, t, true);
 }
 
 static int step_eager(cs_gpu_ctx* c, double t, int run)
 {
     int r = cs_gpu_infect_sweep(c, t, run);
     if (r) return r;
-    return cs_gpu_incub_recovery_sweep(c, t);
+    return incub_sweep(c, t, false);
 }
 
 // Capture one whole timestep (both sweeps, ~25 kernels and memsets) as a CUDA graph.
@@ -2115,6 +2185,19 @@ int cs_gpu_set_grid(cs_gpu_ctx* c, int blocks)
 }
 
 int cs_gpu_grid(const cs_gpu_ctx* c) { return c ? c->grid : 0; }
+
+int cs_gpu_set_spatial_lanes(cs_gpu_ctx* c, int lanes)
+{
+    if (!c) return CS_E_ARG;
+    if (lanes != 4 && lanes != 8 && lanes != 16) return set_err(c, CS_E_ARG, "spatial lanes must be 4, 8 or 16");
+    CK(cudaStreamSynchronize(c->stream));
+    c->spatial_lanes = lanes;
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+    return CS_OK;
+}
 
 int cs_gpu_use_graphs(cs_gpu_ctx* c, int enable)
 {

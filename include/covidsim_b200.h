@@ -407,6 +407,9 @@ int cs_gpu_use_graphs(cs_gpu_ctx* ctx, int enable);
  * step graph is dropped and captured again. */
 int cs_gpu_set_grid(cs_gpu_ctx* ctx, int blocks);
 int cs_gpu_grid(const cs_gpu_ctx* ctx);
+/* Lanes that test one spatial contact's candidate draws together: 4, 8 (default)
+ * or 16.  Also a launch-shape choice: results do not depend on it. */
+int cs_gpu_set_spatial_lanes(cs_gpu_ctx* ctx, int lanes);
 
 /* ---- Realisations stepped together.  No counterpart in the reference, which
  * runs realisations one after another (src/CovidSim.cpp:371-399).

@@ -87,12 +87,26 @@ def test_batch_matches_lone_contexts():
 def test_launch_shape_does_not_change_results():
     pop, P, lk, hr = tiny_world()
     ref = sim.Simulation(pop, P, lk, hr)
-    alt = ref.replica()
-    alt.backend.set_grid(148 * 2)
-    out = []
-    for s in (ref, alt):
-        s.run(31, days=15, n_seed=20)
-        out.append(snapshot(s.backend, pop))
-    _same(out[0], out[1], "grid 8 vs 2 blocks per SM")
-    alt.close()
+    ref.run(31, days=15, n_seed=20)
+    want = snapshot(ref.backend, pop)
+    for grid, lanes in ((148 * 2, 8), (148 * 8, 4), (148 * 16, 16)):
+        alt = ref.replica()
+        alt.backend.set_grid(grid)
+        alt.backend.set_spatial_lanes(lanes)
+        alt.run(31, days=15, n_seed=20)
+        _same(snapshot(alt.backend, pop), want, "grid %d, %d spatial lanes" % (grid, lanes))
+        alt.close()
     ref.close()
+
+
+def test_autotuner_picks_a_setting_and_keeps_results():
+    from covidsim_b200 import tune
+    pop, P, lk, hr = tiny_world()
+    s = sim.Simulation(pop, P, lk, hr)
+    s.run(41, days=10, n_seed=20)
+    want = snapshot(s.backend, pop)
+    best = tune.autotune(s, steps=8)
+    assert best["grid"] % 148 == 0 and best["spatial_lanes"] in (4, 8, 16) and len(best["ms"]) == 12
+    s.run(41, days=10, n_seed=20)
+    _same(snapshot(s.backend, pop), want, "after tuning")
+    s.close()
