@@ -63,8 +63,8 @@ def parse():
                     help="c2 only: population sizes times this factor (1.0 = 1/4/10/20 M)")
     ap.add_argument("--c2-per-size", type=int, default=16, help="c2 only: realisations per population size")
     ap.add_argument("--c2-days", type=int, default=365, help="c2 only: days per realisation")
-    ap.add_argument("--c4-train", type=int, default=2048, help="c4 only: training scenarios")
-    ap.add_argument("--c4-seeds", type=int, default=2, help="c4 only: seeds per training scenario")
+    ap.add_argument("--c4-train", type=int, default=4096, help="c4 only: training scenarios")
+    ap.add_argument("--c4-seeds", type=int, default=1, help="c4 only: seeds per training scenario")
     ap.add_argument("--c4-epochs", type=int, default=800, help="c4 only: training epochs")
     ap.add_argument("--c4-sweep", type=int, default=100_000, help="c4 only: scenarios screened")
     ap.add_argument("--c4-rerun", type=int, default=100, help="c4 only: top scenarios re-run by the simulator")
@@ -455,6 +455,8 @@ def run_c2(args):
                 members.append(base.replica(Pk))
             people += n
     batch = sim.Batch(members)
+    from covidsim_b200 import tune
+    tuned = tune.autotune_batch(batch, n_sm=torch.cuda.get_device_properties(0).multi_processor_count)
     days = args.c2_days
     policy = sim.InterventionPolicy()
     stream = torch.cuda.ExternalStream(batch.stream())
@@ -489,8 +491,10 @@ def run_c2(args):
                                % (len(members), args.c2_per_size,
                                   "/".join("%g" % (x * args.c2_scale) for x in C2_SIZES), days),
                    "realisations_per_step": len(members), "people_total": people,
-                   "timesteps_per_realisation": steps_per_run, "parallelism": "one graph per timestep, "
-                   "one branch per realisation; static arrays shared per population"},
+                   "timesteps_per_realisation": steps_per_run,
+                   "parallelism": "one graph per timestep; each kernel launched once for all realisations "
+                                  "(one grid row each); static arrays shared per population",
+                   "tuned": tuned},
         "runs_per_hour": round(nreal / (ms / 1e3) * 3600.0, 1),
         "ensemble_new_infections": finals,
         "clocks": clk.summary(), "e2e": None, "gpu_launches": None,
@@ -525,7 +529,7 @@ def run_c4(args):
     # 2. training
     net = surrogate.Surrogate(max_batch=256, seed=5)
     t0 = time.perf_counter()
-    hist = net.fit(xs, ys, epochs=args.c4_epochs, lr=1e-3, batch=256)
+    hist = net.fit(xs, ys, epochs=args.c4_epochs, lr=1e-3, batch=256, holdout=0.1)
     t_train = time.perf_counter() - t0
     # 3. screening
     sweep = surrogate.sample_scenarios(args.c4_sweep, seed=202)
@@ -587,6 +591,7 @@ def run_c4(args):
                     "rerun_top": round(t_rerun, 2), "pipeline": round(t_pipeline, 2),
                     "one_realisation_plain": round(t_one, 4), "plain_sweep_estimate": round(t_plain, 1)},
         "train_loss": [round(float(hist[0]), 5), round(float(hist[-1]), 5)],
+        "heldout_loss_best": round(float(min(v for _, v in net.val_history)), 5) if net.val_history else None,
         "icu_rel_l2_vs_ensemble_mean": {"top_ranked": err_top, "random_sweep_sample": err_rnd},
     }
 

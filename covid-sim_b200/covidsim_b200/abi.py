@@ -151,6 +151,7 @@ def load_library(path=LIB_PATH):
         "cs_gpu_batch_create": (I, [P(V), I, P(V)]),
         "cs_gpu_batch_step": (I, [V, D, I]),
         "cs_gpu_batch_set_grid": (I, [V, I]),
+        "cs_gpu_batch_set_spatial_lanes": (I, [V, I]),
         "cs_gpu_batch_sync": (I, [V]),
         "cs_gpu_batch_stream": (V, [V]),
         "cs_gpu_batch_last_error": (C.c_char_p, [V]),

@@ -367,8 +367,7 @@ class _RunState:
 
 class Batch:
     """Realisations advanced together: one cs_gpu_batch_step per timestep launches
-    one CUDA graph holding every member's step, so the members' kernels share the
-    GPU.  Members are Simulations (replicas of one population via
+    one CUDA graph whose kernels each run the step's work of every member.  Members are Simulations (replicas of one population via
     Simulation.replica(), or of different populations); each keeps its own host
     logic (daily counters, UpdateProbs, interventions)."""
 
@@ -393,6 +392,9 @@ class Batch:
 
     def set_grid(self, blocks):
         self._ck(self.lib.cs_gpu_batch_set_grid(self.handle, blocks), "set_grid")
+
+    def set_spatial_lanes(self, lanes):
+        self._ck(self.lib.cs_gpu_batch_set_spatial_lanes(self.handle, lanes), "set_spatial_lanes")
 
     def sync(self):
         self._ck(self.lib.cs_gpu_batch_sync(self.handle), "sync")

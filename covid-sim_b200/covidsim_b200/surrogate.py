@@ -172,16 +172,30 @@ class Surrogate:
                  "train_step")
         return float(loss.value)
 
-    def fit(self, x_unit, y, epochs=200, lr=1e-3, batch=None, seed=0, lr_final=1e-5):
-        """Minibatch Adam with a cosine learning-rate decay; returns the epoch losses."""
+    def loss(self, x_unit, y):
+        """Mean squared error of the predictions (no update)."""
+        p = self.predict(x_unit)
+        return float(np.mean((p - y) ** 2))
+
+    def fit(self, x_unit, y, epochs=200, lr=1e-3, batch=None, seed=0, lr_final=1e-5, holdout=0.0, check_every=10):
+        """Minibatch Adam with a cosine learning-rate decay; returns the epoch losses.
+        With `holdout` > 0 that fraction of the samples is kept out of training and
+        the weights with the lowest held-out loss (checked every `check_every`
+        epochs) are kept at the end."""
         batch = batch or self.max_batch
         rng = np.random.default_rng(seed)
-        n = x_unit.shape[0]
+        n_all = x_unit.shape[0]
+        perm = rng.permutation(n_all)
+        n_val = int(n_all * holdout)
+        val, tr = perm[:n_val], perm[n_val:]
+        n = len(tr)
         hist = []
         steps = max(1, epochs * ((n + batch - 1) // batch))
         k = 0
+        best, best_w = np.inf, None
+        self.val_history = []
         for ep in range(epochs):
-            order = rng.permutation(n)
+            order = tr[rng.permutation(n)]
             tot, cnt = 0.0, 0
             for b0 in range(0, n, batch):
                 sel = order[b0:b0 + batch]
@@ -190,6 +204,13 @@ class Surrogate:
                 cnt += len(sel)
                 k += 1
             hist.append(tot / cnt)
+            if n_val and ((ep + 1) % check_every == 0 or ep == epochs - 1):
+                v = self.loss(x_unit[val], y[val])
+                self.val_history.append((ep + 1, v))
+                if v < best:
+                    best, best_w = v, self.get_params()
+        if best_w is not None:
+            self.set_params(best_w)
         return hist
 
     def close(self):

@@ -724,7 +724,7 @@ __global__ void k_block_rows(DevPop d)
 // that reads it depends on the order (random streams are keyed by person and
 // contact, conflicting claims resolve by key, tallies are integer sums, and cell
 // lists are reordered by position).
-__global__ void k_build_active(DevPop d, int mode)
+__device__ __forceinline__ void k_build_active_body(const DevPop& d, int mode)
 {
     for (int c0 = blockIdx.x * blockDim.x; c0 < d.NC; c0 += gridDim.x * blockDim.x) {
         const int c = c0 + threadIdx.x;
@@ -740,6 +740,8 @@ __global__ void k_build_active(DevPop d, int mode)
         }
     }
 }
+__global__ void k_build_active(DevPop d, int mode) { k_build_active_body(d, mode); }
+__global__ void k_build_active_multi(const DevPop* __restrict__ pops, int mode) { k_build_active_body(pops[blockIdx.y], mode); }
 
 // =============================================================== InfectSweep
 __device__ __forceinline__ void claim_infection(const DevPop& d, int person, int infector, int code)
@@ -752,7 +754,7 @@ __device__ __forceinline__ void claim_infection(const DevPop& d, int person, int
 typedef DevStep StepScalars;
 
 // The step's scalars from the parameters, on the device (src/Sweep.cpp:292-301).
-__global__ void k_set_step(DevPop d, double t, unsigned long long seed)
+__device__ __forceinline__ void k_set_step_body(const DevPop& d, double t, unsigned long long seed)
 {
     const cs_params& P = *d.P;
     if (d.t_src) t = *d.t_src;
@@ -768,6 +770,8 @@ __global__ void k_set_step(DevPop d, double t, unsigned long long seed)
     st.seed = seed;
     *d.step = st;
 }
+__global__ void k_set_step(DevPop d, double t, unsigned long long seed) { k_set_step_body(d, t, seed); }
+__global__ void k_set_step_multi(const DevPop* __restrict__ pops, double t, unsigned long long seed) { k_set_step_body(pops[blockIdx.y], t, seed); }
 
 // Geometric-skip enumeration of the Bernoulli(p) trials over a member list
 // (equivalent to the reference's Binomial count + sample without replacement,
@@ -813,7 +817,7 @@ __device__ void place_candidates(const DevPop& d, const cs_params& P, const Step
 
 // Household pass and spatial Poisson count of one infector (src/Sweep.cpp:331-377,
 // 656-698); one thread per infector.
-__global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d)
+__device__ __forceinline__ void k_infector_hh_spatial_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const StepScalars st = *d.step;
@@ -888,10 +892,12 @@ __global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d)
     }
     cnt_add_warp(CSB_CTR(work_hh_members), hh_members);
 }
+__global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d) { k_infector_hh_spatial_body(d); }
+__global__ void __launch_bounds__(kThreads) k_infector_hh_spatial_multi(const DevPop* __restrict__ pops) { k_infector_hh_spatial_body(pops[blockIdx.y]); }
 
 // Place passes (src/Sweep.cpp:379-647): one thread per (infector, place) work
 // entry, i.e. per place type the infector attends and is not absent from.
-__global__ void __launch_bounds__(kThreads) k_infector_places(DevPop d)
+__device__ __forceinline__ void k_infector_places_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const StepScalars st = *d.step;
@@ -915,6 +921,8 @@ __global__ void __launch_bounds__(kThreads) k_infector_places(DevPop d)
         place_candidates(d, P, st, i, hi, pt, link, p2, true, seed);
     }
 }
+__global__ void __launch_bounds__(kThreads) k_infector_places(DevPop d) { k_infector_places_body(d); }
+__global__ void __launch_bounds__(kThreads) k_infector_places_multi(const DevPop* __restrict__ pops) { k_infector_places_body(pops[blockIdx.y]); }
 
 // Spatial contacts (src/Sweep.cpp:742-856): pick a target block from the infector's
 // block row, a slot uniformly among the block's S0 slots, accept with K(d)/bound,
@@ -960,7 +968,7 @@ __device__ __forceinline__ bool spatial_draw(const DevPop& d, const cs_params& P
 }
 
 template <int kSpatialLanes>
-__global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d)
+__device__ __forceinline__ void k_spatial_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const StepScalars st = *d.step;
@@ -1032,9 +1040,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d)
         if (nres > ncont) cnt_add(CSB_CTR(err_queue_overflow), nres - ncont);
     }
 }
+template <int kSpatialLanes>
+__global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d) { k_spatial_body<kSpatialLanes>(d); }
+template <int kSpatialLanes>
+__global__ void __launch_bounds__(kThreads, 3) k_spatial_multi(const DevPop* __restrict__ pops) { k_spatial_body<kSpatialLanes>(pops[blockIdx.y]); }
 
 // DoInfect (src/Update.cpp:100-195) for every person claimed this step.
-__global__ void k_apply_infections(DevPop d)
+__device__ __forceinline__ void k_apply_infections_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const double t = d.step->t;
@@ -1096,6 +1108,8 @@ __global__ void k_apply_infections(DevPop d)
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_STAGED(work_new_infections), nq);
     stage_flush(d.C, staged);
 }
+__global__ void k_apply_infections(DevPop d) { k_apply_infections_body(d); }
+__global__ void k_apply_infections_multi(const DevPop* __restrict__ pops) { k_apply_infections_body(pops[blockIdx.y]); }
 
 // Swap-with-block-end removal of marked slots, high to low (src/Update.cpp:1402-1579
 // UpdateCell sequence).  Returns nothing; moved people get their new listpos.
@@ -1125,7 +1139,7 @@ __device__ void partition_block(const DevPop& d, int base, int b0, int n, int nm
 }
 
 // S -> L list moves for every cell that gained latent people this step.
-__global__ void k_partition_S(DevPop d)
+__device__ __forceinline__ void k_partition_S_body(const DevPop& d)
 {
     int nt = d.counts[kCntTouched];
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_cells_touched), nt);
@@ -1138,6 +1152,8 @@ __global__ void k_partition_S(DevPop d)
         d.cell_flag[c] = 0;
     }
 }
+__global__ void k_partition_S(DevPop d) { k_partition_S_body(d); }
+__global__ void k_partition_S_multi(const DevPop* __restrict__ pops) { k_partition_S_body(pops[blockIdx.y]); }
 
 // ====================================================== IncubRecoverySweep
 __device__ __forceinline__ void sev_add(const DevPop& d, int ad, int which, int delta, bool cum)
@@ -1368,7 +1384,7 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
 // Which latent / infectious people have an event this step (latent period ends,
 // case onset, severity change, recovery or death): a light scan that compacts
 // them into cmap so the heavy transition kernel runs only on those.
-__global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d)
+__device__ __forceinline__ void k_incub_scan_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const int ts = d.step->ts;
@@ -1391,9 +1407,11 @@ __global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d)
         if (ev) d.cmap[o] = idx;
     }
 }
+__global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d) { k_incub_scan_body(d); }
+__global__ void __launch_bounds__(kThreads) k_incub_scan_multi(const DevPop* __restrict__ pops) { k_incub_scan_body(pops[blockIdx.y]); }
 
 // cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
-__global__ void __launch_bounds__(kThreads, 3) k_incub_events(DevPop d)
+__device__ __forceinline__ void k_incub_events_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const double t = d.step->t;
@@ -1436,8 +1454,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_incub_events(DevPop d)
     }
     stage_flush(d.C, staged);
 }
+__global__ void __launch_bounds__(kThreads, 3) k_incub_events(DevPop d) { k_incub_events_body(d); }
+__global__ void __launch_bounds__(kThreads, 3) k_incub_events_multi(const DevPop* __restrict__ pops) { k_incub_events_body(pops[blockIdx.y]); }
 
-__global__ void k_partition_LI(DevPop d)
+__device__ __forceinline__ void k_partition_LI_body(const DevPop& d)
 {
     int nt = d.counts[kCntTouched];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
@@ -1452,11 +1472,13 @@ __global__ void k_partition_LI(DevPop d)
         d.cell_flag[c] = 0;
     }
 }
+__global__ void k_partition_LI(DevPop d) { k_partition_LI_body(d); }
+__global__ void k_partition_LI_multi(const DevPop* __restrict__ pops) { k_partition_LI_body(pops[blockIdx.y]); }
 
 // Deferred household actions, once per household, after every per-person
 // transition of the step: the adult-carer absence of DoCase/DoDetectedCase
 // (src/Update.cpp:736-763, 843-868) and household quarantine (src/Update.cpp:676-708).
-__global__ void k_household_after(DevPop d)
+__device__ __forceinline__ void k_household_after_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const int ts = d.step->ts;
@@ -1509,6 +1531,8 @@ __global__ void k_household_after(DevPop d)
         }
     }
 }
+__global__ void k_household_after(DevPop d) { k_household_after_body(d); }
+__global__ void k_household_after_multi(const DevPop* __restrict__ pops) { k_household_after_body(pops[blockIdx.y]); }
 
 // ============================================================ seeding
 __global__ void k_seed_claims(DevPop d, const int32_t* list, int n)
@@ -2206,24 +2230,30 @@ int cs_gpu_use_graphs(cs_gpu_ctx* c, int enable)
     return CS_OK;
 }
 
+// List counters of every member of a batch back to zero (the end-of-sweep reset).
+__global__ void k_zero_counts_multi(const DevPop* __restrict__ pops)
+{
+    if (threadIdx.x < kCntN) pops[blockIdx.x].counts[threadIdx.x] = 0;
+}
+
 // ------------------------------------------------------------ batched steps
 // A batch steps many realisations (contexts, each with its own population or a
-// replica sharing one) with one CUDA graph per timestep: the graph holds one
-// branch per member, so the members' kernels run side by side on the GPU.  While
-// the batch exists every member's work goes to the batch's stream, which keeps a
-// member's own calls (UpdateProbs, interventions, counters) ordered with the
-// batched steps.
+// replica sharing one) with one CUDA graph per timestep.  Each of the step's
+// kernels is launched once for all members: blockIdx.y selects the member, whose
+// DevPop the kernel reads from a device array, so a timestep is the same 11
+// kernels and 2 counter resets whatever the number of members.  While the batch
+// exists every member's work goes to the batch's stream, which keeps a member's
+// own calls (UpdateProbs, interventions, counters) ordered with the batched steps.
 struct cs_gpu_batch {
     int device = 0;
     std::vector<cs_gpu_ctx*> members;
     cudaStream_t stream = nullptr;
-    std::vector<cudaStream_t> branch;
-    cudaEvent_t fork = nullptr;
-    std::vector<cudaEvent_t> join;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<long long> member_launches;
     double* d_t = nullptr;   // the timestep's t, read by every member's k_set_step
+    DevPop* d_pops = nullptr; // members' DevPop (t taken from d_t)
+    int lanes = 8;            // spatial lanes of the batched launches
     char err[512] = {0};
 };
 
@@ -2266,15 +2296,11 @@ int cs_gpu_batch_create(cs_gpu_ctx* const* members, int n, cs_gpu_batch** out)
     }
     BCK(cudaSetDevice(b->device));
     BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    BCK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     BCK(cudaMalloc(&b->d_t, sizeof(double)));
+    BCK(cudaMalloc(&b->d_pops, sizeof(DevPop) * n));
     b->members.assign(members, members + n);
-    b->branch.resize(n);
-    b->join.resize(n);
     b->member_launches.assign(n, 0);
     for (int k = 0; k < n; k++) {
-        BCK(cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking));
-        BCK(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
         cs_gpu_ctx* m = b->members[k];
         BCK(cudaStreamSynchronize(m->stream));
         m->own_stream = m->stream;
@@ -2285,30 +2311,60 @@ int cs_gpu_batch_create(cs_gpu_ctx* const* members, int n, cs_gpu_batch** out)
 
 const char* cs_gpu_batch_last_error(const cs_gpu_batch* b) { return b ? b->err : "null batch"; }
 
+#define BLAUNCH(kernel, grid, block, ...)                                                          \
+    do {                                                                                           \
+        kernel<<<(grid), (block), 0, b->stream>>>(__VA_ARGS__);                                    \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess) return batch_err(b, CS_E_CUDA, "launch %s: %s", #kernel, cudaGetErrorString(e_)); \
+    } while (0)
+
+// The batched timestep, in the order of step_eager (InfectSweep, then
+// IncubRecoverySweep without a second k_set_step).
+static int batch_enqueue(cs_gpu_batch* b)
+{
+    const int R = (int)b->members.size();
+    const int grid = b->members[0]->grid;
+    const dim3 g(grid, R), one(1, R);
+    const DevPop* pops = b->d_pops;
+    BLAUNCH(k_set_step_multi, one, 1, pops, 0.0, 0ull);
+    BLAUNCH(k_build_active_multi, g, kThreads, pops, 0);
+    BLAUNCH(k_infector_hh_spatial_multi, g, kThreads, pops);
+    BLAUNCH(k_infector_places_multi, g, kThreads, pops);
+    switch (b->lanes) {
+    case 4: BLAUNCH(k_spatial_multi<4>, g, kThreads, pops); break;
+    case 16: BLAUNCH(k_spatial_multi<16>, g, kThreads, pops); break;
+    default: BLAUNCH(k_spatial_multi<8>, g, kThreads, pops); break;
+    }
+    BLAUNCH(k_apply_infections_multi, g, kThreads, pops);
+    BLAUNCH(k_partition_S_multi, g, kThreads, pops);
+    BLAUNCH(k_zero_counts_multi, R, 32, pops);
+    BLAUNCH(k_build_active_multi, g, kThreads, pops, 1);
+    BLAUNCH(k_incub_scan_multi, g, kThreads, pops);
+    BLAUNCH(k_incub_events_multi, g, kThreads, pops);
+    BLAUNCH(k_partition_LI_multi, g, kThreads, pops);
+    BLAUNCH(k_household_after_multi, g, kThreads, pops);
+    BLAUNCH(k_zero_counts_multi, R, 32, pops);
+    return CS_OK;
+}
+
 static int batch_capture(cs_gpu_batch* b, double t, int run)
 {
-    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    BCK(cudaEventRecord(b->fork, b->stream));
-    int r = CS_OK;
+    (void)t;
+    (void)run;
     const int n = (int)b->members.size();
-    for (int k = 0; k < n && r == CS_OK; k++) {
-        cs_gpu_ctx* m = b->members[k];
-        if (cudaStreamWaitEvent(b->branch[k], b->fork, 0) != cudaSuccess) { r = CS_E_CUDA; break; }
-        m->stream = b->branch[k];
-        m->d.t_src = b->d_t;   // only the captured copies read t from the batch
-        long long l0 = m->launches;
-        r = step_eager(m, t, run);
-        b->member_launches[k] = m->launches - l0;
-        m->launches = l0;
-        m->d.t_src = nullptr;
-        m->stream = b->stream;
-        if (r) {
-            batch_err(b, r, "member %d: %s", k, m->err);
-            break;
-        }
-        if (cudaEventRecord(b->join[k], b->branch[k]) != cudaSuccess ||
-            cudaStreamWaitEvent(b->stream, b->join[k], 0) != cudaSuccess) r = CS_E_CUDA;
+    for (int k = 1; k < n; k++)
+        if (b->members[k]->grid != b->members[0]->grid)
+            return batch_err(b, CS_E_ARG, "members use different launch shapes; set one with cs_gpu_batch_set_grid");
+    // members' DevPop, each taking t from the batch
+    std::vector<DevPop> hp(n);
+    for (int k = 0; k < n; k++) {
+        hp[k] = b->members[k]->d;
+        hp[k].t_src = b->d_t;
     }
+    BCK(cudaMemcpyAsync(b->d_pops, hp.data(), sizeof(DevPop) * n, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int r = batch_enqueue(b);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (r || e != cudaSuccess) {
@@ -2318,6 +2374,7 @@ static int batch_capture(cs_gpu_batch* b, double t, int run)
     }
     BCK(cudaGraphInstantiate(&b->exec, g, 0));
     b->graph = g;
+    for (int k = 0; k < n; k++) b->member_launches[k] = 11;   // kernels run for each member per step
     return CS_OK;
 }
 
@@ -2354,6 +2411,16 @@ int cs_gpu_batch_set_grid(cs_gpu_batch* b, int blocks)
     return CS_OK;
 }
 
+int cs_gpu_batch_set_spatial_lanes(cs_gpu_batch* b, int lanes)
+{
+    if (!b) return CS_E_ARG;
+    if (lanes != 4 && lanes != 8 && lanes != 16) return batch_err(b, CS_E_ARG, "spatial lanes must be 4, 8 or 16");
+    BCK(cudaStreamSynchronize(b->stream));
+    b->lanes = lanes;
+    batch_drop_graph(b);
+    return CS_OK;
+}
+
 void* cs_gpu_batch_stream(cs_gpu_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 int cs_gpu_batch_sync(cs_gpu_batch* b)
@@ -2373,10 +2440,8 @@ void cs_gpu_batch_destroy(cs_gpu_batch* b)
             m->stream = m->own_stream;
             m->own_stream = nullptr;
         }
-    for (cudaStream_t st : b->branch) if (st) cudaStreamDestroy(st);
-    for (cudaEvent_t ev : b->join) if (ev) cudaEventDestroy(ev);
-    if (b->fork) cudaEventDestroy(b->fork);
     if (b->d_t) cudaFree(b->d_t);
+    if (b->d_pops) cudaFree(b->d_pops);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }

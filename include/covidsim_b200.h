@@ -422,18 +422,20 @@ int cs_gpu_set_spatial_lanes(cs_gpu_ctx* ctx, int lanes);
  * except the geometry.
  *
  * cs_gpu_batch: n member contexts (replicas, or contexts of other populations,
- * on one device) advanced by one CUDA graph per timestep with one branch per
- * member, so their kernels run side by side.  While the batch exists, members'
- * own calls run on the batch's stream, ordered with the batched steps.  Destroy
- * the batch before its members. */
+ * on one device) advanced by one CUDA graph per timestep in which each of the
+ * step's kernels is launched once for all members (one grid row per member).
+ * While the batch exists, members' own calls run on the batch's stream, ordered
+ * with the batched steps.  Destroy the batch before its members. */
 int cs_gpu_create_replica(const cs_gpu_ctx* base, cs_gpu_ctx** out);
 
 typedef struct cs_gpu_batch cs_gpu_batch;
 int cs_gpu_batch_create(cs_gpu_ctx* const* members, int n, cs_gpu_batch** out);
 /* One timestep (InfectSweep + IncubRecoverySweep) of every member at time t. */
 int cs_gpu_batch_step(cs_gpu_batch* batch, double t, int run);
-/* cs_gpu_set_grid for every member. */
+/* cs_gpu_set_grid for every member (members must share one launch shape). */
 int cs_gpu_batch_set_grid(cs_gpu_batch* batch, int blocks);
+/* Spatial lanes of the batched launches (4, 8 or 16). */
+int cs_gpu_batch_set_spatial_lanes(cs_gpu_batch* batch, int lanes);
 int cs_gpu_batch_sync(cs_gpu_batch* batch);
 void* cs_gpu_batch_stream(cs_gpu_batch* batch);
 const char* cs_gpu_batch_last_error(const cs_gpu_batch* batch);
