@@ -63,8 +63,8 @@ def parse():
                     help="c2 only: population sizes times this factor (1.0 = 1/4/10/20 M)")
     ap.add_argument("--c2-per-size", type=int, default=16, help="c2 only: realisations per population size")
     ap.add_argument("--c2-days", type=int, default=365, help="c2 only: days per realisation")
-    ap.add_argument("--c4-train", type=int, default=4096, help="c4 only: training scenarios")
-    ap.add_argument("--c4-seeds", type=int, default=1, help="c4 only: seeds per training scenario")
+    ap.add_argument("--c4-train", type=int, default=2048, help="c4 only: training scenarios")
+    ap.add_argument("--c4-seeds", type=int, default=2, help="c4 only: seeds per training scenario")
     ap.add_argument("--c4-epochs", type=int, default=800, help="c4 only: training epochs")
     ap.add_argument("--c4-sweep", type=int, default=100_000, help="c4 only: scenarios screened")
     ap.add_argument("--c4-rerun", type=int, default=100, help="c4 only: top scenarios re-run by the simulator")
@@ -529,7 +529,7 @@ def run_c4(args):
     # 2. training
     net = surrogate.Surrogate(max_batch=256, seed=5)
     t0 = time.perf_counter()
-    hist = net.fit(xs, ys, epochs=args.c4_epochs, lr=1e-3, batch=256, holdout=0.1)
+    hist = net.fit(xs, ys, epochs=args.c4_epochs, lr=1e-3, batch=256, holdout=0.1, weight_decay=1e-4)
     t_train = time.perf_counter() - t0
     # 3. screening
     sweep = surrogate.sample_scenarios(args.c4_sweep, seed=202)

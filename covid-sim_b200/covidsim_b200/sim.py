@@ -113,6 +113,14 @@ class GpuBackend:
         self._ck(self.lib.cs_gpu_get_counters(self.ctx, C.byref(out)), "get_counters")
         return out
 
+    def run_device(self, days, policy):
+        """cs_gpu_run: `days` days from t = 0 with the run loop's logic on the device
+        (policy: a cs_run_policy); returns the day-end counter blocks as an int64
+        array [days, sizeof(cs_counters) / 8]."""
+        out = np.empty((days, C.sizeof(abi.cs_counters) // 8), np.int64)   # every field is int64
+        self._ck(self.lib.cs_gpu_run(self.ctx, days, C.byref(policy), out.ctypes.data), "run")
+        return out
+
     def download(self, view):
         self._ck(self.lib.cs_gpu_download_state(self.ctx, C.byref(view)), "download_state")
 
@@ -249,6 +257,22 @@ class InterventionPolicy:
     household_quarantine: bool = True
 
 
+def run_policy(policy, n_place_types, probs_every_step=False):
+    """The cs_run_policy of cs_gpu_run for an InterventionPolicy (or None)."""
+    p = abi.cs_run_policy()
+    p.probs_every_step = int(bool(probs_every_step))
+    if policy is not None:
+        p.icu_trigger = 1
+        p.icu_threshold = int(policy.threshold)
+        p.icu_window = int(policy.window)
+        p.case_isolation = int(bool(policy.case_isolation))
+        p.household_quarantine = int(bool(policy.household_quarantine))
+        p.social_distancing = int(bool(policy.social_distancing))
+        p.close_place_types = sum(1 << pt for pt in set(policy.close_place_types) if 0 <= pt < n_place_types)
+        p.duration = float(policy.duration)
+    return p
+
+
 class Simulation:
     def __init__(self, pop, params, lookup, hires, backend=None, device=0):
         self.pop = pop
@@ -277,18 +301,32 @@ class Simulation:
         rng = np.random.default_rng(seed ^ 0x5EED)
         return rng.choice(self.pop.n_people, size=n_seed, replace=False).astype(np.int32)
 
-    def run(self, seed, days, n_seed=100, policy=None, sample_every_day=True, callback=None, initial_state=None):
+    def run(self, seed, days, n_seed=100, policy=None, sample_every_day=True, callback=None, initial_state=None,
+            probs_every_step=False, device_loop=None):
         """One realisation; returns daily time series of the main counters.
 
         initial_state: a cs_state_view of host arrays holding a prepared start
         (InitModel + SeedInfection already applied); it is copied to the device
-        instead of resetting and seeding there."""
+        instead of resetting and seeding there.
+        probs_every_step: test the susceptible fraction for UpdateProbs after every
+        timestep, as the reference does, rather than at day ends.
+        device_loop: run the logic between timesteps on the device (cs_gpu_run), one
+        host round trip per run; the default uses it whenever the backend has it, the
+        run has whole days and there is no per-day callback.  Results are the same."""
         be = self.backend
         if initial_state is not None:
             be.upload(seed, initial_state)
         else:
             be.begin_run(seed, self.choose_seeds(seed, n_seed))
-        rs = _RunState(self, days, policy, callback)
+        rs = _RunState(self, days, policy, callback, probs_every_step)
+        whole = rs.nsteps == int(days) * rs.spd and float(days) == int(days)
+        if device_loop is None:
+            device_loop = hasattr(be, "run_device") and callback is None and whole
+        if device_loop:
+            if not whole or callback is not None:
+                raise ValueError("the device run loop takes whole days and no callback")
+            daily = be.run_device(int(days), run_policy(policy, self.pop.num_place_types, probs_every_step))
+            return {k: daily[:, _COUNTER_INDEX[k]].copy() for k in SERIES}
         for step in range(rs.nsteps):
             be.step(step * self.params.ModelTimeStep, 0)
             rs.after_step(step)
@@ -315,6 +353,7 @@ class Simulation:
 
 SERIES = ("S", "L", "I", "R", "D", "cumI", "cumC", "cumDC", "Critical", "cumCritical",
           "cumDeath_Critical", "cumDeath_SARI", "cumDeath_ILI", "SARI", "ILI", "Mild")
+_COUNTER_INDEX = {k: getattr(abi.cs_counters, k).offset // 8 for k in SERIES}
 
 
 class _RunState:
@@ -322,8 +361,9 @@ class _RunState:
     daily counters, UpdateProbs when the susceptible fraction has fallen by 0.2,
     and the global ICU trigger switching interventions on and off."""
 
-    def __init__(self, sim, days, policy, callback):
+    def __init__(self, sim, days, policy, callback, probs_every_step=False):
         self.sim, self.policy, self.callback = sim, policy, callback
+        self.every_step = probs_every_step
         P = sim.params
         self.spd = int(round(P.TimeStepsPerDay))
         self.nsteps = int(days * self.spd)
@@ -334,18 +374,22 @@ class _RunState:
         self.socd = np.zeros(sim.pop.n_mcells, dtype=np.uint8)
 
     def after_step(self, step):
-        if not ((step + 1) % self.spd == 0 or step == self.nsteps - 1):
+        day_end = (step + 1) % self.spd == 0 or step == self.nsteps - 1
+        if not (day_end or self.every_step):
             return
         sim, be, P, policy = self.sim, self.sim.backend, self.sim.params, self.policy
         series = self.series
         t = step * P.ModelTimeStep
         c = be.counters()
-        for k in series:
-            series[k].append(int(getattr(c, k)))
+        if day_end:
+            for k in series:
+                series[k].append(int(getattr(c, k)))
         prop_s = c.S / sim.pop.n_people
         if self.prev_prop_s - prop_s > 0.2:
             self.prev_prop_s = prop_s
             be.update_probs(0)
+        if not day_end:
+            return
         if policy is not None:
             day = len(series["cumCritical"])
             w = policy.window

@@ -164,12 +164,12 @@ class Surrogate:
                                            g.ctypes.data), "loss_grad")
         return float(loss.value), g
 
-    def train_step(self, x_unit, target, lr):
+    def train_step(self, x_unit, target, lr, weight_decay=0.0):
         x = np.ascontiguousarray(x_unit, np.float32)
         t = np.ascontiguousarray(target, np.float32)
         loss = C.c_float()
-        self._ck(self.lib.cs_sur_train_step(self.h, x.ctypes.data, t.ctypes.data, x.shape[0], lr, C.byref(loss)),
-                 "train_step")
+        self._ck(self.lib.cs_sur_train_step(self.h, x.ctypes.data, t.ctypes.data, x.shape[0], lr, weight_decay,
+                                            C.byref(loss)), "train_step")
         return float(loss.value)
 
     def loss(self, x_unit, y):
@@ -177,7 +177,8 @@ class Surrogate:
         p = self.predict(x_unit)
         return float(np.mean((p - y) ** 2))
 
-    def fit(self, x_unit, y, epochs=200, lr=1e-3, batch=None, seed=0, lr_final=1e-5, holdout=0.0, check_every=10):
+    def fit(self, x_unit, y, epochs=200, lr=1e-3, batch=None, seed=0, lr_final=1e-5, holdout=0.0, check_every=10,
+            weight_decay=0.0):
         """Minibatch Adam with a cosine learning-rate decay; returns the epoch losses.
         With `holdout` > 0 that fraction of the samples is kept out of training and
         the weights with the lowest held-out loss (checked every `check_every`
@@ -200,7 +201,7 @@ class Surrogate:
             for b0 in range(0, n, batch):
                 sel = order[b0:b0 + batch]
                 lr_k = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / steps))
-                tot += self.train_step(x_unit[sel], y[sel], lr_k) * len(sel)
+                tot += self.train_step(x_unit[sel], y[sel], lr_k, weight_decay) * len(sel)
                 cnt += len(sel)
                 k += 1
             hist.append(tot / cnt)

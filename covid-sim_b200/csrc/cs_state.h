@@ -138,6 +138,8 @@ struct DevPop {
     DevStep* step;
     const unsigned long long* seed_src;  // the run's seed, written by begin_run / upload_state
     const double* t_src;                 // when set (batched graphs), k_set_step takes t from here
+    int32_t* step_clock;                 // when set (day graphs), k_set_step takes t = clock * dt and advances it
+    const int32_t* gate;                 // when set (day graphs), UpdateProbs kernels run only if *gate
     int32_t* close_window;     // [2] every place closed at ts has [0] <= ts < [1]
     // spatial proposal blocks
     const int32_t* cell_block;

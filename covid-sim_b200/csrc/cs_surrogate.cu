@@ -223,7 +223,7 @@ __global__ void k_mse(const float* __restrict__ y, const float* __restrict__ tar
 
 // Adam (Kingma & Ba, 2015) on FP32 master weights; refreshes the BF16 copy.
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v, const float* __restrict__ g,
-                       bf16* __restrict__ wb, size_t n, float lr, float b1, float b2, float eps, float c1, float c2)
+                       bf16* __restrict__ wb, size_t n, float lr, float b1, float b2, float eps, float c1, float c2, float wd)
 {
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         float gi = g[e];
@@ -231,7 +231,8 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
         float vi = b2 * v[e] + (1.f - b2) * gi * gi;
         m[e] = mi;
         v[e] = vi;
-        float wi = w[e] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        // decoupled weight decay (Loshchilov & Hutter, "Decoupled weight decay regularization", 2019)
+        float wi = w[e] * (1.f - lr * wd) - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
         w[e] = wi;
         if (wb) wb[e] = __float2bfloat16(wi);
     }
@@ -622,7 +623,7 @@ int cs_sur_loss_grad(cs_sur* s, const float* x, const float* target, int n, floa
     return CS_OK;
 }
 
-int cs_sur_train_step(cs_sur* s, const float* x, const float* target, int n, float lr, float* loss)
+int cs_sur_train_step(cs_sur* s, const float* x, const float* target, int n, float lr, float weight_decay, float* loss)
 {
     if (!s || !x || !target) return CS_E_ARG;
     int r = loss_grad(s, x, target, n, loss);
@@ -630,7 +631,7 @@ int cs_sur_train_step(cs_sur* s, const float* x, const float* target, int n, flo
     s->t++;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - powf(b1, (float)s->t), c2 = 1.f - powf(b2, (float)s->t);
-    sur::k_adam<<<1184, 256, 0, s->stream>>>(s->w, s->m, s->v, s->g, s->wb, s->np, lr, b1, b2, 1e-8f, c1, c2);
+    sur::k_adam<<<1184, 256, 0, s->stream>>>(s->w, s->m, s->v, s->g, s->wb, s->np, lr, b1, b2, 1e-8f, c1, c2, weight_decay);
     SCK(cudaGetLastError());
     if (!loss) SCK(cudaStreamSynchronize(s->stream));
     return CS_OK;

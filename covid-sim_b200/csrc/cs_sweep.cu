@@ -31,6 +31,8 @@
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -173,6 +175,8 @@ struct StaticStore {
     }
 };
 
+struct DayCtl;
+
 struct cs_gpu_ctx {
     int device = 0;
     std::shared_ptr<StaticStore> stat;     // static population arrays (possibly shared)
@@ -206,6 +210,16 @@ struct cs_gpu_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<cudaGraphNode_t> set_step_nodes;
     long long graph_launches = 0;
+    // device-side run loop: one graph per day (cs_gpu_run)
+    DayCtl* d_ctl = nullptr;
+    int32_t* d_clock = nullptr;
+    cs_counters* d_series = nullptr;
+    int series_cap = 0;
+    int day_every_step = -1;    // the probs_every_step the day graph was captured with
+    size_t tp_smem[2] = {0, 0}; // dynamic shared memory enabled for k_tot_prob_rows<false>, <true>
+    cudaGraph_t day_graph = nullptr;
+    cudaGraphExec_t day_exec = nullptr;
+    long long day_launches = 0;
     // optional per-launch timing with events on the context's stream
     bool prof = false;
     struct Rec { const char* name; cudaEvent_t a, b; };
@@ -215,6 +229,14 @@ struct cs_gpu_ctx {
     std::vector<double> prof_ms;
     std::vector<long long> prof_n;
 };
+
+static void drop_day_graph(cs_gpu_ctx* c)
+{
+    if (c->day_exec) cudaGraphExecDestroy(c->day_exec);
+    if (c->day_graph) cudaGraphDestroy(c->day_graph);
+    c->day_exec = nullptr;
+    c->day_graph = nullptr;
+}
 
 static void prof_flush(cs_gpu_ctx* c)
 {
@@ -371,6 +393,7 @@ __global__ void k_reset_places(DevPop d, int pt, uint64_t seed)
 // ============================================================ UpdateProbs
 __global__ void k_update_S0(DevPop d, int do_place)
 {
+    if (d.gate && !*d.gate) return;
     const cs_params& P = *d.P;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < d.NC; j += gridDim.x * blockDim.x) {
         int n = d.cell_start[j + 1] - d.cell_start[j];
@@ -433,6 +456,7 @@ __global__ void k_kernel_rows(DevPop d, float* Gtab, unsigned long long* oor)
 
 __global__ void k_grid_values(DevPop d, double* S0g, double* Ng, uint8_t* rowS, uint8_t* rowN)
 {
+    if (d.gate && !*d.gate) return;
     int nch = d.P->nch;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
         int g = d.cell_grid[c];
@@ -502,6 +526,7 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
                                                        double* Aout, double* Bout, TotProbGeom gm,
                                                        const float* __restrict__ Gtab)
 {
+    if (d.gate && !*d.gate) return;
     const cs_params& P = *d.P;
     const int ncw = P.ncw, nch = P.nch;
     extern __shared__ __align__(16) double sh[];
@@ -607,8 +632,10 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
 }
 
 // Chunk sums added in ascending chunk order: out[g] = sum over z of part[z][g].
-__global__ void k_tot_prob_reduce(const double* __restrict__ part, int nparts, size_t G, double* __restrict__ out)
+__global__ void k_tot_prob_reduce(const double* __restrict__ part, int nparts, size_t G, double* __restrict__ out,
+                                  const int32_t* gate)
 {
+    if (gate && !*gate) return;
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < G; g += (size_t)gridDim.x * blockDim.x) {
         double A = 0.0;
         for (int z = 0; z < nparts; z++) A = A + part[(size_t)z * G + g];
@@ -630,6 +657,7 @@ static void tot_prob_launch_shape(int ncw, int nch, const TotProbGeom& gm, dim3*
 
 __global__ void k_tot_prob_finish(DevPop d, const double* Ag, const double* Bg)
 {
+    if (d.gate && !*d.gate) return;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
         int g = d.cell_grid[c];
         double b = Bg[g];
@@ -639,6 +667,7 @@ __global__ void k_tot_prob_finish(DevPop d, const double* Ag, const double* Bg)
 
 __global__ void k_block_S0(DevPop d)
 {
+    if (d.gate && !*d.gate) return;
     for (int B = blockIdx.x * blockDim.x + threadIdx.x; B < d.NB; B += gridDim.x * blockDim.x) {
         long long s = 0;
         int k0 = d.block_cell_ofs[B], k1 = d.block_cell_ofs[B + 1];
@@ -674,6 +703,7 @@ __global__ void k_block_bounds_all(DevPop d, unsigned long long* oor)
 // B order so the doubles round exactly as a sequential loop.
 __global__ void k_block_rows(DevPop d)
 {
+    if (d.gate && !*d.gate) return;
     const cs_params& P = *d.P;
     int lane = threadIdx.x & 31;
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -758,6 +788,11 @@ __device__ __forceinline__ void k_set_step_body(const DevPop& d, double t, unsig
 {
     const cs_params& P = *d.P;
     if (d.t_src) t = *d.t_src;
+    if (d.step_clock) {
+        int k = *d.step_clock;
+        t = (double)k * P.ModelTimeStep;
+        *d.step_clock = k + 1;
+    }
     if (d.seed_src) seed = *d.seed_src;
     DevStep st;
     st.t = t;
@@ -1547,8 +1582,29 @@ __global__ void k_seed_claims(DevPop d, const int32_t* list, int n)
 }
 
 // ============================================================ interventions
-__global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop)
+// State of the device-side run loop (cs_gpu_run): its policy, the host loop's
+// variables between timesteps (src/CovidSim.cpp:1517-1526 PreviousProportionSusceptible,
+// the ICU trigger's switch state) and what the day's logic decided for the
+// kernels gated on it.
+struct DayCtl {
+    cs_run_policy pol;
+    cs_counters* series;        // [days] counters at each day's end
+    double prev_prop_s, on_until;
+    int32_t day, started;
+    int32_t update;             // UpdateProbs runs (gate of its kernels)
+    int32_t socd_write;         // every microcell's social-distancing flag becomes socd_value
+    int32_t close;              // places of the policy's types close over [close_start, close_stop)
+    uint16_t close_start, close_stop;
+    uint8_t socd_value, pad[3];
+};
+
+__global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop, const DayCtl* ctl)
 {
+    if (ctl) {   // a day graph's closure: only on the day the trigger fired, window from the device
+        if (!ctl->close || !((ctl->pol.close_place_types >> pt) & 1u)) return;
+        start = ctl->close_start;
+        stop = ctl->close_stop;
+    }
     const cs_params& P = *d.P;
     DevPlaces pl = d.pl[pt];
     // every place closed at ts afterwards has close_start >= start and close_end <= stop
@@ -1581,6 +1637,77 @@ __global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t st
             }
         __syncthreads();
     }
+}
+
+// The test after a timestep whether the susceptible fraction fell by more than 0.2
+// since UpdateProbs last ran (src/CovidSim.cpp:1520-1526); S is fresh from k_cell_totals.
+__global__ void k_probs_check(DevPop d, DayCtl* ctl)
+{
+    const double prop_s = (double)d.C->S / (double)d.N;
+    int up = 0;
+    if (ctl->prev_prop_s - prop_s > 0.2) {
+        ctl->prev_prop_s = prop_s;
+        up = 1;
+    }
+    ctl->update = up;
+}
+
+// End of a day of the run loop: the day's counters into the series, and the global
+// ICU trigger (src/CovidSim.cpp:3150-3159 with global thresholds) switching case
+// isolation, household quarantine, social distancing and place closure on for
+// pol.duration days, then off.  The switch takes effect from the next timestep.
+__global__ void k_day_logic(DevPop d, DayCtl* ctl, const int32_t* clock, DevIv* iv)
+{
+    const int day = ctl->day;
+    {
+        const unsigned long long* src = (const unsigned long long*)d.C;
+        unsigned long long* dst = (unsigned long long*)(ctl->series + day);
+        for (int k = threadIdx.x; k < (int)(sizeof(cs_counters) / 8); k += blockDim.x) dst[k] = src[k];
+    }
+    if (threadIdx.x) return;
+    const cs_params& P = *d.P;
+    const cs_run_policy& pol = ctl->pol;
+    ctl->socd_write = 0;
+    ctl->close = 0;
+    if (pol.icu_trigger) {
+        const int w = pol.icu_window;
+        const long long recent = (long long)d.C->cumCritical - (day + 1 > w ? (long long)ctl->series[day - w].cumCritical : 0ll);
+        const double t = (double)(*clock - 1) * P.ModelTimeStep;   // the day's last timestep
+        const double tn = t + P.ModelTimeStep;
+        int sw = -1;
+        if (!ctl->started && recent >= pol.icu_threshold) {
+            ctl->started = 1;
+            ctl->on_until = tn + pol.duration;
+            sw = 1;
+        } else if (ctl->started && ctl->on_until > 0 && tn >= ctl->on_until) {
+            ctl->on_until = -1.0;
+            sw = 0;
+        }
+        if (sw >= 0) {
+            DevIv v;
+            v.ci_start = (sw && pol.case_isolation) ? tn : 1e10;
+            v.ci_dur = pol.duration;
+            v.hq_start = (sw && pol.household_quarantine) ? tn : 1e10;
+            v.hq_dur = pol.duration;
+            *iv = v;
+            ctl->socd_write = 1;
+            ctl->socd_value = (sw && pol.social_distancing) ? CS_TREAT_TREATED : CS_TREAT_UNTREATED;
+            if (sw) {
+                const int ts = (int)(tn * P.TimeStepsPerDay);
+                const int stop = min(65533, ts + (int)(pol.duration * P.TimeStepsPerDay));
+                ctl->close = 1;
+                ctl->close_start = (uint16_t)ts;
+                ctl->close_stop = (uint16_t)stop;
+            }
+        }
+    }
+    ctl->day = day + 1;
+}
+
+__global__ void k_socdist_fill(DevPop d, const DayCtl* ctl)
+{
+    if (!ctl->socd_write) return;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < d.NM; m += gridDim.x * blockDim.x) d.socdist[m] = ctl->socd_value;
 }
 
 __global__ void k_cell_totals(DevPop d)
@@ -1863,6 +1990,11 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     for (auto& r : c->ring) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->day_exec) cudaGraphExecDestroy(c->day_exec);
+    if (c->day_graph) cudaGraphDestroy(c->day_graph);
+    if (c->d_ctl) cudaFree(c->d_ctl);
+    if (c->d_clock) cudaFree(c->d_clock);
+    if (c->d_series) cudaFree(c->d_series);
     for (void* p : c->allocs) cudaFree(p);
     c->stat.reset();   // frees the static arrays when no replica still uses them
     if (c->xfer) cudaFree(c->xfer);
@@ -1890,6 +2022,7 @@ int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
                           memcmp(params->asin2sqx, o.asin2sqx, sizeof(o.asin2sqx));
     if (geometry && c->stat.use_count() > 1)
         return set_err(c, CS_E_UNSUPPORTED, "set_params may not change the geometry of a population shared by replicas");
+    drop_day_graph(c);   // captured with this kernel-row table and steps per day
     c->hp = *params;
     CK(cudaMemcpyAsync(c->dP, params, sizeof(cs_params), cudaMemcpyHostToDevice, c->stream));
     if (geometry) {   // the kernel rows and the n-weighted denominators depend on it
@@ -1959,6 +2092,32 @@ static int build_kernel_rows(cs_gpu_ctx* c)
     return CS_OK;
 }
 
+// bytes of p to zero (a kernel rather than a memset so that a day graph can gate it)
+__global__ void k_zero_gated(unsigned char* p, size_t bytes, const int32_t* gate)
+{
+    if (gate && !*gate) return;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < bytes; e += (size_t)gridDim.x * blockDim.x) p[e] = 0;
+}
+
+// The dynamic shared memory the row kernel needs, raised above the default before
+// its first launch (and so never inside a graph capture that follows one).
+static int tot_prob_smem(cs_gpu_ctx* c, bool denominators, size_t smem)
+{
+    size_t& have = c->tp_smem[denominators ? 1 : 0];
+    if (smem <= 48 * 1024 || smem <= have) return CS_OK;
+    if (denominators) CK(cudaFuncSetAttribute(k_tot_prob_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else CK(cudaFuncSetAttribute(k_tot_prob_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    have = smem;
+    return CS_OK;
+}
+
+static int tot_prob_prepare(cs_gpu_ctx* c)
+{
+    const cs_params& P = c->hp;
+    const TotProbGeom gm = tot_prob_geom(P.ncw, P.nch, true);
+    return tot_prob_smem(c, false, gm.smem(false));
+}
+
 // One pass of the tot_prob row kernel: A from the current S0 (and, at creation,
 // B from the cell populations).
 static int tot_prob_pass(cs_gpu_ctx* c, bool denominators)
@@ -1966,8 +2125,13 @@ static int tot_prob_pass(cs_gpu_ctx* c, bool denominators)
     DevPop& d = c->d;
     const cs_params& P = c->hp;
     size_t G = (size_t)P.ncw * P.nch;
-    CK(cudaMemsetAsync(c->S0g, 0, sizeof(double) * G, c->stream));
-    CK(cudaMemsetAsync(c->rowS, 0, P.nch, c->stream));
+    if (d.gate) {
+        LAUNCH(k_zero_gated, c->grid, kThreads, (unsigned char*)c->S0g, sizeof(double) * G, d.gate);
+        LAUNCH(k_zero_gated, 4, kThreads, c->rowS, (size_t)P.nch, d.gate);
+    } else {
+        CK(cudaMemsetAsync(c->S0g, 0, sizeof(double) * G, c->stream));
+        CK(cudaMemsetAsync(c->rowS, 0, P.nch, c->stream));
+    }
     if (denominators) {
         CK(cudaMemsetAsync(c->Ng, 0, sizeof(double) * G, c->stream));
         CK(cudaMemsetAsync(c->rowN, 0, P.nch, c->stream));
@@ -1978,20 +2142,20 @@ static int tot_prob_pass(cs_gpu_ctx* c, bool denominators)
     int tpb;
     tot_prob_launch_shape(P.ncw, P.nch, gm, &grid, &tpb);
     const size_t smem = gm.smem(denominators);
+    int r = tot_prob_smem(c, denominators, smem);
+    if (r) return r;
     if (c->prof) prof_begin(c, "k_tot_prob_rows");
     if (denominators) {
-        if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_tot_prob_rows<true><<<grid, tpb, smem, c->stream>>>(d, c->S0g, c->Ng, c->rowS, c->rowN, c->Apart, c->Bpart, gm, c->Gtab);
     } else {
-        if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, c->S0g, nullptr, c->rowS, nullptr, c->Apart, nullptr, gm, c->Gtab);
     }
     if (c->prof) prof_end(c);
     c->launches++;
     CK(cudaGetLastError());
     const int rgrid = (int)((G + kThreads - 1) / kThreads);
-    LAUNCH(k_tot_prob_reduce, rgrid, kThreads, c->Apart, gm.nchunks, G, c->Ag);
-    if (denominators) LAUNCH(k_tot_prob_reduce, rgrid, kThreads, c->Bpart, gm.nchunks, G, c->Bg);
+    LAUNCH(k_tot_prob_reduce, rgrid, kThreads, c->Apart, gm.nchunks, G, c->Ag, d.gate);
+    if (denominators) LAUNCH(k_tot_prob_reduce, rgrid, kThreads, c->Bpart, gm.nchunks, G, c->Bg, d.gate);
     return CS_OK;
 }
 
@@ -2201,6 +2365,7 @@ int cs_gpu_set_grid(cs_gpu_ctx* c, int blocks)
     if (!c || blocks <= 0) return CS_E_ARG;
     CK(cudaStreamSynchronize(c->stream));
     c->grid = blocks;
+    drop_day_graph(c);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     c->graph_exec = nullptr;
@@ -2216,6 +2381,7 @@ int cs_gpu_set_spatial_lanes(cs_gpu_ctx* c, int lanes)
     if (lanes != 4 && lanes != 8 && lanes != 16) return set_err(c, CS_E_ARG, "spatial lanes must be 4, 8 or 16");
     CK(cudaStreamSynchronize(c->stream));
     c->spatial_lanes = lanes;
+    drop_day_graph(c);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     c->graph_exec = nullptr;
@@ -2227,6 +2393,138 @@ int cs_gpu_use_graphs(cs_gpu_ctx* c, int enable)
 {
     if (!c) return CS_E_ARG;
     c->use_graph = enable != 0;
+    return CS_OK;
+}
+
+// ------------------------------------------------------- device run loop
+// S..D of the counter block from the cells, as cs_gpu_get_counters does.
+static int enqueue_totals(cs_gpu_ctx* c)
+{
+    CK(cudaMemsetAsync(c->d.C, 0, 5 * sizeof(int64_t), c->stream));
+    LAUNCH(k_cell_totals, 64, kThreads, c->d);
+    return CS_OK;
+}
+
+// One day of the run loop on the context's stream.  c->d carries the step clock
+// (k_set_step takes t from it) and the UpdateProbs gate (&ctl->update), so the
+// same launches serve every day and can be captured once.  Order as the host loop:
+// the timesteps; after each (or the day's last) the counters and the UpdateProbs
+// test; at the day's end the series and the trigger, then the gated UpdateProbs,
+// and the switch's social-distancing flags and closures.
+static int enqueue_day(cs_gpu_ctx* c, int spd, bool every_step)
+{
+    DevPop& d = c->d;
+    for (int s = 0; s < spd; s++) {
+        int r = step_eager(c, 0.0, 0);
+        if (r) return r;
+        if (!every_step && s < spd - 1) continue;
+        r = enqueue_totals(c);
+        if (r) return r;
+        LAUNCH(k_probs_check, 1, 1, d, c->d_ctl);
+        if (s == spd - 1) LAUNCH(k_day_logic, 1, kThreads, d, c->d_ctl, (const int32_t*)c->d_clock, c->dIv);
+        r = cs_gpu_update_probs(c, 0);
+        if (r) return r;
+    }
+    const int mgrid = std::max(1, std::min(c->grid, (d.NM + kThreads - 1) / kThreads));
+    LAUNCH(k_socdist_fill, mgrid, kThreads, d, (const DayCtl*)c->d_ctl);
+    for (int pt = 0; pt < d.NPT; pt++)
+        LAUNCH(k_close_places, c->grid, kThreads, d, pt, (const uint8_t*)nullptr, (uint16_t)0, (uint16_t)0, (const DayCtl*)c->d_ctl);
+    return CS_OK;
+}
+
+static int capture_day(cs_gpu_ctx* c, int spd, bool every_step)
+{
+    int r = tot_prob_prepare(c);
+    if (r) return r;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    long long l0 = c->launches;
+    r = enqueue_day(c, spd, every_step);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (r || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        c->launches = l0;
+        return r ? r : set_err(c, CS_E_CUDA, "day graph capture: %s", cudaGetErrorString(e));
+    }
+    cudaError_t ei = cudaGraphInstantiate(&c->day_exec, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        c->day_exec = nullptr;
+        c->launches = l0;
+        return set_err(c, CS_E_CUDA, "day graph instantiate: %s", cudaGetErrorString(ei));
+    }
+    c->day_graph = g;
+    c->day_launches = c->launches - l0;
+    c->day_every_step = every_step ? 1 : 0;
+    c->launches = l0;
+    return CS_OK;
+}
+
+static int run_days(cs_gpu_ctx* c, int days, int spd, bool every_step)
+{
+    const bool graph = c->use_graph && !c->prof;
+    if (graph && (!c->day_exec || c->day_every_step != (every_step ? 1 : 0))) {
+        drop_day_graph(c);
+        int r = capture_day(c, spd, every_step);
+        if (r) return r;
+    }
+    for (int k = 0; k < days; k++) {
+        if (graph) {
+            CK(cudaGraphLaunch(c->day_exec, c->stream));
+            c->launches += c->day_launches;
+        } else {
+            int r = enqueue_day(c, spd, every_step);
+            if (r) return r;
+        }
+    }
+    return CS_OK;
+}
+
+int cs_gpu_run(cs_gpu_ctx* c, int days, const cs_run_policy* policy, cs_counters* daily)
+{
+    if (!c || days < 0) return CS_E_ARG;
+    if (!c->run_started) return set_err(c, CS_E_STATE, "run before begin_run");
+    if (days == 0) return CS_OK;
+    const int spd = (int)std::lround(c->hp.TimeStepsPerDay);
+    if (spd < 1 || (double)spd != c->hp.TimeStepsPerDay)
+        return set_err(c, CS_E_ARG, "the run loop needs a whole number of timesteps per day");
+    cs_run_policy pol{};
+    if (policy) pol = *policy;
+    if (pol.icu_trigger && pol.icu_window < 1) return set_err(c, CS_E_ARG, "icu_window must be at least 1 day");
+    if (!c->d_ctl) {
+        CK(cudaMalloc(&c->d_ctl, sizeof(DayCtl)));
+        CK(cudaMalloc(&c->d_clock, sizeof(int32_t)));
+    }
+    if (days > c->series_cap) {
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->d_series) cudaFree(c->d_series);
+        c->d_series = nullptr;
+        c->series_cap = 0;
+        CK(cudaMalloc(&c->d_series, sizeof(cs_counters) * (size_t)days));
+        c->series_cap = days;
+    }
+    DayCtl h{};
+    h.pol = pol;
+    h.series = c->d_series;
+    h.prev_prop_s = 1.0;
+    h.on_until = -1.0;
+    const int32_t zero = 0;
+    CK(cudaMemcpyAsync(c->d_ctl, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_clock, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->stream));
+    c->d.step_clock = c->d_clock;
+    c->d.gate = &c->d_ctl->update;
+    int r = run_days(c, days, spd, pol.probs_every_step != 0);
+    c->d.step_clock = nullptr;
+    c->d.gate = nullptr;
+    if (r) return r;
+    cs_counters last;
+    CK(cudaMemcpyAsync(&last, c->d_series + (days - 1), sizeof(last), cudaMemcpyDeviceToHost, c->stream));
+    if (daily) CK(cudaMemcpyAsync(daily, c->d_series, sizeof(cs_counters) * (size_t)days, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (last.err_queue_overflow || last.err_spatial_tries || last.err_kernel_range)
+        return set_err(c, CS_E_OVERFLOW, "bounded device loop gave up (spatial %lld, queue %lld, kernel range %lld)",
+                       (long long)last.err_spatial_tries, (long long)last.err_queue_overflow, (long long)last.err_kernel_range);
     return CS_OK;
 }
 
@@ -2402,6 +2700,7 @@ int cs_gpu_batch_set_grid(cs_gpu_batch* b, int blocks)
     BCK(cudaStreamSynchronize(b->stream));
     for (cs_gpu_ctx* m : b->members) {
         m->grid = blocks;
+        drop_day_graph(m);
         if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
         if (m->graph) cudaGraphDestroy(m->graph);
         m->graph_exec = nullptr;
@@ -2468,7 +2767,7 @@ int cs_gpu_close_places(cs_gpu_ctx* c, int pt, const int32_t* mcells, int n_mcel
         CK(cudaMalloc(&sel, c->d.NM));
         CK(cudaMemcpyAsync(sel, h.data(), c->d.NM, cudaMemcpyHostToDevice, c->stream));
     }
-    LAUNCH(k_close_places, c->grid, kThreads, c->d, pt, sel, start, stop);
+    LAUNCH(k_close_places, c->grid, kThreads, c->d, pt, sel, start, stop, (const DayCtl*)nullptr);
     if (sel) {
         CK(cudaStreamSynchronize(c->stream));
         cudaFree(sel);

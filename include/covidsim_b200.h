@@ -465,8 +465,10 @@ int cs_sur_forward(cs_sur* sur, const float* x, int n, float* y);
 /* Mean squared error against target [n, 365, 4] and, when grad is not NULL, its
  * gradient in the flat layout; n <= max_batch. */
 int cs_sur_loss_grad(cs_sur* sur, const float* x, const float* target, int n, float* loss, float* grad);
-/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on a batch; loss may be NULL. */
-int cs_sur_train_step(cs_sur* sur, const float* x, const float* target, int n, float lr, float* loss);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8; weight_decay applied to the
+ * weights directly, as AdamW) on a batch; loss may be NULL. */
+int cs_sur_train_step(cs_sur* sur, const float* x, const float* target, int n, float lr, float weight_decay,
+                      float* loss);
 
 int cs_gpu_set_interventions(cs_gpu_ctx* ctx, const cs_interventions* iv);
 /* DoPlaceClose (src/Update.cpp:1095-1258) for every place of type t in the listed
@@ -476,6 +478,34 @@ int cs_gpu_close_places(cs_gpu_ctx* ctx, int place_type, const int32_t* mcells, 
 
 /* Copy the device counter block (cumulative since the run began). */
 int cs_gpu_get_counters(cs_gpu_ctx* ctx, cs_counters* out);
+
+/* What the run loop between timesteps does (the host side of RunModel,
+ * src/CovidSim.cpp:1420-1527): the UpdateProbs test on the susceptible fraction,
+ * and a global critical-care trigger (src/CovidSim.cpp:3150-3159, global
+ * thresholds) that switches interventions on for `duration` days. */
+typedef struct cs_run_policy {
+    int32_t icu_trigger;            /* 1: the trigger below is active */
+    int32_t icu_threshold;          /* critical-care admissions over icu_window days that fire it */
+    int32_t icu_window;             /* days */
+    int32_t case_isolation;         /* 1: case isolation switches with the trigger */
+    int32_t household_quarantine;   /* 1: household quarantine switches with the trigger */
+    int32_t social_distancing;      /* 1: every microcell's social distancing switches with it */
+    uint32_t close_place_types;     /* bit t set: places of type t close when it fires */
+    int32_t probs_every_step;       /* 1: test the susceptible fraction after every timestep,
+                                       as the reference does; 0: at the end of each day */
+    double duration;                /* days the interventions stay on */
+} cs_run_policy;
+
+/* A whole realisation on the device: `days` days of timesteps from t = 0 (after
+ * cs_gpu_begin_run or cs_gpu_upload_state), with the run loop's logic between
+ * timesteps evaluated by kernels rather than the host, so no host round trip
+ * happens until the run ends.  daily[d] (days entries, may be NULL) receives the
+ * counters at the end of day d, as cs_gpu_get_counters would return them there.
+ * policy NULL: no trigger, UpdateProbs tested at day ends.  Gives the same state
+ * and counters as stepping with cs_gpu_step and applying the same logic on the
+ * host (cs_gpu_get_counters, cs_gpu_update_probs(ctx, 0), cs_gpu_set_interventions,
+ * cs_gpu_close_places). */
+int cs_gpu_run(cs_gpu_ctx* ctx, int days, const cs_run_policy* policy, cs_counters* daily);
 /* Per-cell S, L, I, R, D (each n_cells) for RecordSample (src/CovidSim.cpp:3044-3056). */
 int cs_gpu_get_cell_counts(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D);
 /* Wait for the context's stream; returns a deferred device error if any. */

@@ -1,0 +1,120 @@
+"""The run loop on the device (cs_gpu_run): the logic between timesteps (day-end
+counters, the UpdateProbs test on the susceptible fraction, the critical-care
+trigger switching interventions on and off) evaluated by kernels in one graph per
+day.  Day for day and state for state it must give what the same logic gives on
+the host, and what the oracle gives under that host logic."""
+import numpy as np
+import pytest
+
+from covidsim_b200 import abi, sim
+import oracle_py
+from tests.helpers import tiny_world, snapshot, STATE_FIELDS
+
+pytestmark = pytest.mark.gpu
+
+DAYS = 60
+
+
+def _policy():
+    # fires early in the tiny world's epidemic and switches off again inside the run
+    return sim.InterventionPolicy(threshold=3, window=7, duration=12.0)
+
+
+def _same_state(a, b, where):
+    for k in STATE_FIELDS:
+        assert np.array_equal(a[k], b[k]), "%s: %s differs at %d entries" % (where, k, int(np.sum(a[k] != b[k])))
+
+
+def _same_series(a, b, where):
+    for k in sim.SERIES:
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), "%s: series %s differs" % (where, k)
+
+
+def _instrument(s):
+    """Record the host loop's UpdateProbs calls and intervention switches."""
+    log = {"update": 0, "switch": []}
+    up = s.backend.update_probs
+
+    def update_probs(do_place=0):
+        log["update"] += 1
+        up(do_place)
+    s.backend.update_probs = update_probs
+    sw = s._switch_interventions
+
+    def switch(t, policy, on, socd):
+        log["switch"].append((t, on))
+        sw(t, policy, on, socd)
+    s._switch_interventions = switch
+    return log
+
+
+@pytest.mark.parametrize("every_step", [False, True])
+def test_device_loop_matches_host_loop(every_step):
+    pop, P, lk, hr = tiny_world()
+    host = sim.Simulation(pop, P, lk, hr)
+    log = _instrument(host)
+    want = host.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step, device_loop=False)
+    want_state = snapshot(host.backend, pop)
+    # the run exercised what the loop decides
+    assert log["update"] >= 1, log
+    assert [on for _, on in log["switch"]] == [True, False], log
+    dev = host.replica()
+    got = dev.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step, device_loop=True)
+    _same_series(got, want, "device loop")
+    _same_state(snapshot(dev.backend, pop), want_state, "device loop")
+    # a second run on the same context replays the same graph from a fresh start
+    again = dev.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step)
+    _same_series(again, want, "second device run")
+    _same_state(snapshot(dev.backend, pop), want_state, "second device run")
+    dev.close()
+    host.close()
+
+
+def test_device_loop_matches_oracle():
+    pop, P, lk, hr = tiny_world()
+    o = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+    log = _instrument(o)
+    g = sim.Simulation(pop, P, lk, hr)
+    want = o.run(606, DAYS, n_seed=20, policy=_policy(), probs_every_step=True)
+    assert log["update"] >= 1 and [on for _, on in log["switch"]] == [True, False], log
+    got = g.run(606, DAYS, n_seed=20, policy=_policy(), probs_every_step=True)
+    _same_series(got, want, "device loop vs oracle")
+    _same_state(snapshot(g.backend, pop), snapshot(o.backend, pop), "device loop vs oracle")
+    assert abi.counters_to_dict(g.backend.counters()) == abi.counters_to_dict(o.backend.counters())
+    g.close()
+    o.close()
+
+
+def test_graph_and_eager_day_loops_agree():
+    pop, P, lk, hr = tiny_world()
+    a = sim.Simulation(pop, P, lk, hr)
+    b = a.replica()
+    b.backend.lib.cs_gpu_use_graphs(b.backend.ctx, 0)
+    n0 = a.backend.launches()
+    ra = a.run(707, 30, n_seed=20, policy=_policy())
+    per_day_graph = (a.backend.launches() - n0) / 30
+    n0 = b.backend.launches()
+    rb = b.run(707, 30, n_seed=20, policy=_policy())
+    per_day_eager = (b.backend.launches() - n0) / 30
+    _same_series(ra, rb, "graph vs eager")
+    _same_state(snapshot(a.backend, pop), snapshot(b.backend, pop), "graph vs eager")
+    # both count the same kernels: four timesteps, the totals, the gated UpdateProbs,
+    # the trigger, the flags and one closure kernel per place type
+    assert per_day_graph == per_day_eager > 4 * 10
+    b.close()
+    a.close()
+
+
+def test_run_loop_errors():
+    pop, P, lk, hr = tiny_world()
+    s = sim.Simulation(pop, P, lk, hr)
+    with pytest.raises(abi.CovidSimError):
+        s.backend.run_device(3, sim.run_policy(None, pop.num_place_types))   # before begin_run
+    s.backend.begin_run(1, s.choose_seeds(1, 10))
+    bad = sim.run_policy(_policy(), pop.num_place_types)
+    bad.icu_window = 0
+    with pytest.raises(abi.CovidSimError):
+        s.backend.run_device(3, bad)
+    # a run of no days does nothing
+    assert s.backend.run_device(0, sim.run_policy(None, pop.num_place_types)).shape[0] == 0
+    s.close()
