@@ -63,11 +63,14 @@ def parse():
                     help="c2 only: population sizes times this factor (1.0 = 1/4/10/20 M)")
     ap.add_argument("--c2-per-size", type=int, default=16, help="c2 only: realisations per population size")
     ap.add_argument("--c2-days", type=int, default=365, help="c2 only: days per realisation")
-    ap.add_argument("--c4-train", type=int, default=2048, help="c4 only: training scenarios")
-    ap.add_argument("--c4-seeds", type=int, default=2, help="c4 only: seeds per training scenario")
+    ap.add_argument("--c4-train", type=int, default=2500, help="c4 only: training scenarios")
+    ap.add_argument("--c4-seeds", type=int, default=8, help="c4 only: seeds per training scenario")
     ap.add_argument("--c4-epochs", type=int, default=800, help="c4 only: training epochs")
     ap.add_argument("--c4-sweep", type=int, default=100_000, help="c4 only: scenarios screened")
-    ap.add_argument("--c4-rerun", type=int, default=100, help="c4 only: top scenarios re-run by the simulator")
+    ap.add_argument("--c4-rerun", type=int, default=1000, help="c4 only: top scenarios re-run by the simulator")
+    ap.add_argument("--c4-check", type=int, default=100,
+                    help="c4 only: scenarios drawn at random from the sweep to measure accuracy on")
+    ap.add_argument("--c4-save", default=None, help="c4 only: write the simulated data sets to this .npz")
     ap.add_argument("--c4-people", type=int, default=1_000_000, help="c4 only: population size")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -554,7 +557,7 @@ def run_c4(args):
                 "ensemble_icu_peak_per_million_median": round(float(np.median(ens[:, :, 2].max(axis=1))), 2)}
     err_top = icu_errors(top, ridx, rys)
     # accuracy on scenarios drawn at random from the sweep (not part of the timed pipeline)
-    rnd = np.random.default_rng(303).choice(len(sweep), args.c4_rerun, replace=False)
+    rnd = np.random.default_rng(303).choice(len(sweep), args.c4_check, replace=False)
     qidx, qys = surrogate.simulate(pop, P, lk, hr, sweep[rnd], 8, batch_size=64, seed0=888)
     err_rnd = icu_errors(rnd, qidx, qys)
     # the simulator against itself: a second, independent 8-seed ensemble of the same
@@ -565,6 +568,12 @@ def run_c4(args):
     floor = np.linalg.norm(e1[:, :, 2] - e2[:, :, 2], axis=1) / np.maximum(np.linalg.norm(e2[:, :, 2], axis=1), 1e-12)
     err_rnd["simulator_vs_itself_median"] = round(float(np.median(floor)), 4)
     err_rnd["simulator_vs_itself_mean"] = round(float(floor.mean()), 4)
+    if args.c4_save:
+        def ens(sel, i_r, y_r):   # per-scenario ensemble means, log1p
+            return np.stack([np.log1p(np.expm1(y_r[i_r == k]).mean(axis=0)) for k in range(len(sel))]).astype(np.float32)
+        np.savez_compressed(args.c4_save, train=train, train_targets=ym, sweep_top=sweep[top],
+                            top_mean=ens(top, ridx, rys), sweep_rnd=sweep[rnd], rnd_mean=ens(rnd, qidx, qys),
+                            rnd_mean2=ens(rnd, q2idx, q2ys), net=net.get_params())
     # 5. the plain method: one realisation at a time, timed on a sample
     s1 = sim.Simulation(pop, P, lk, hr)
     beta24, _ = sim.calibrate_local_beta(pop, P, 2.4)

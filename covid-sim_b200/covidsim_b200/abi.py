@@ -166,10 +166,12 @@ def load_library(path=LIB_PATH):
         "cs_sur_forward": (I, [V, V, I, V]),
         "cs_sur_loss_grad": (I, [V, V, V, I, P(C.c_float), V]),
         "cs_sur_train_step": (I, [V, V, V, I, C.c_float, C.c_float, P(C.c_float)]),
+        "cs_sur_set_gemm": (I, [V, I]),
         "cs_gpu_set_interventions": (I, [V, P(cs_interventions)]),
         "cs_gpu_close_places": (I, [V, I, V, I, C.c_uint16, C.c_uint16]),
         "cs_gpu_get_counters": (I, [V, P(cs_counters)]),
         "cs_gpu_run": (I, [V, I, P(cs_run_policy), V]),
+        "cs_gpu_batch_run": (I, [V, I, V, V]),
         "cs_gpu_get_cell_counts": (I, [V, V, V, V, V, V]),
         "cs_gpu_sync": (I, [V]),
         "cs_gpu_stream": (V, [V]),

@@ -446,15 +446,31 @@ class Batch:
     def stream(self):
         return self.lib.cs_gpu_batch_stream(self.handle)
 
-    def run(self, seeds, days, n_seed=100, policy=None, callback=None):
+    def run(self, seeds, days, n_seed=100, policy=None, callback=None, probs_every_step=False, device_loop=None):
         """One realisation per member (member k with run seed seeds[k] and, when
-        `policy` is a list, policy[k]); returns the members' daily series."""
+        `policy` is a list, policy[k]); returns the members' daily series.
+        device_loop as Simulation.run: by default the logic between timesteps runs
+        on the device (cs_gpu_batch_run) whenever there is no callback and the run
+        has whole days.  probs_every_step may be a list (one flag per member)."""
         states = []
         policies = policy if isinstance(policy, (list, tuple)) else [policy] * len(self.sims)
-        for sim, seed, pol in zip(self.sims, seeds, policies):
+        every = probs_every_step if isinstance(probs_every_step, (list, tuple)) else [probs_every_step] * len(self.sims)
+        for sim, seed, pol, ev in zip(self.sims, seeds, policies, every):
             sim.backend.begin_run(seed, sim.choose_seeds(seed, n_seed))
             cb = (lambda step, c, k=len(states): callback(k, step, c)) if callback else None
-            states.append(_RunState(sim, days, pol, cb))
+            states.append(_RunState(sim, days, pol, cb, ev))
+        whole = float(days) == int(days) and all(rs.nsteps == int(days) * rs.spd for rs in states)
+        if device_loop is None:
+            device_loop = callback is None and whole
+        if device_loop:
+            if not whole or callback is not None:
+                raise ValueError("the device run loop takes whole days and no callback")
+            n, nd = len(self.sims), int(days)
+            pols = (abi.cs_run_policy * n)(*[run_policy(p, s.pop.num_place_types, ev)
+                                             for p, s, ev in zip(policies, self.sims, every)])
+            out = np.empty((n, max(nd, 1), C.sizeof(abi.cs_counters) // 8), np.int64)
+            self._ck(self.lib.cs_gpu_batch_run(self.handle, nd, C.addressof(pols), out.ctypes.data), "run")
+            return [{k: out[j, :nd, _COUNTER_INDEX[k]].copy() for k in SERIES} for j in range(n)]
         nsteps = max(rs.nsteps for rs in states)
         dt = self.sims[0].params.ModelTimeStep
         for step in range(nsteps):

@@ -117,7 +117,7 @@ def simulate(pop, P, lk, hr, thetas, seeds_per, days=DAYS, batch_size=64, n_seed
 
 class Surrogate:
     """The cs_sur_* network: FP32 master weights on the device, BF16 tensor-core
-    forward and backward with FP32 accumulation, Adam."""
+    (tcgen05) forward and backward with FP32 accumulation, Adam."""
 
     def __init__(self, max_batch=256, device=0, seed=0, params=None):
         self.lib = abi.load_library()
@@ -138,6 +138,10 @@ class Surrogate:
     @staticmethod
     def n_params():
         return abi.load_library().cs_sur_num_params()
+
+    def set_gemm(self, impl):
+        """Matrix products on tcgen05 ("tcgen05", the default) or mma.sync ("mma.sync")."""
+        self._ck(self.lib.cs_sur_set_gemm(self.h, {"tcgen05": 0, "mma.sync": 1}[impl]), "set_gemm")
 
     def set_params(self, flat):
         f = np.ascontiguousarray(flat, np.float32)

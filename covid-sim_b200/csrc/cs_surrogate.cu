@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -48,10 +49,19 @@ __device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
+// Split K (gridDim.z > 1): slice z covers k in [z * kchunk, min(K, (z + 1) * kchunk))
+// and writes its partial product to C + z * cstride (no bias, ReLU or BF16 output).
 __global__ void __launch_bounds__(128) k_gemm_nt(const bf16* __restrict__ A, int lda, const bf16* __restrict__ B, int ldb,
                                                  float* __restrict__ C, int ldc, bf16* __restrict__ Cb, int ldcb,
-                                                 const float* __restrict__ bias, int relu, int K)
+                                                 const float* __restrict__ bias, int relu, int K, int kchunk, size_t cstride)
 {
+    if (gridDim.z > 1) {
+        const int z = blockIdx.z;
+        A += (size_t)z * kchunk;
+        B += (size_t)z * kchunk;
+        C += (size_t)z * cstride;
+        K = min(kchunk, K - z * kchunk);
+    }
     __shared__ __align__(16) bf16 As[64][40];
     __shared__ __align__(16) bf16 Bs[64][40];
     const int bm = blockIdx.y * 64, bn = blockIdx.x * 64;
@@ -110,6 +120,201 @@ __global__ void __launch_bounds__(128) k_gemm_nt(const bf16* __restrict__ A, int
                 if (C) { C[(size_t)r * ldc + c] = v0; C[(size_t)r * ldc + c + 1] = v1; }
                 if (Cb) *reinterpret_cast<__nv_bfloat162*>(Cb + (size_t)r * ldcb + c) = __floats2bfloat162_rn(v0, v1);
             }
+}
+
+// ------------------------------------------------------- tcgen05 GEMM
+// The same product on the 5th-generation tensor cores.  A block computes a 128 x BN
+// tile: its 128 threads stage 64-wide K slices of A and B in shared memory in the
+// K-major 128-byte-swizzled layout (two stages, so the loads of slice k+1 overlap
+// the products of slice k), one thread issues the tcgen05.mma instructions
+// (M = 128, N = BN, K = 16 each, BF16 in, FP32 accumulator in tensor memory) and
+// commits them to the stage's mbarrier, and after the last slice every warp reads
+// its 32 accumulator rows from tensor memory for the epilogue (bias, ReLU, FP32
+// and/or BF16 stores).  Rows of A past M are staged as zeros and not stored.
+// Every wait is bounded: on a give-up the block records it in *err, waits (bounded)
+// for its issued products, frees its tensor memory and returns.
+namespace tc {
+
+constexpr int BM = 128, BK = 64;          // BK bf16 = 128 bytes, one swizzle row
+constexpr unsigned kSpin = 1u << 22;      // try_wait rounds before a wait gives up
+
+__host__ __device__ constexpr size_t smem_bytes(int BN) { return 1024 + 2 * (size_t)(BM + BN) * BK * 2; }
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled operand: start
+// address, leading offset 16 B (unused by this layout), 8-row groups 1024 B apart,
+// descriptor version 1, layout SWIZZLE_128B.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major.
+__host__ __device__ constexpr uint32_t idesc(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(saddr(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for (unsigned i = 0; i < kSpin; i++)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                 :: "r"(d_tmem), "l"(a), "l"(b), "r"(id), "r"(accumulate) : "memory");
+}
+
+__device__ __forceinline__ void commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(saddr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+                   "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                   "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// rows x 64 BF16 of a row-major matrix (row stride ld elements, rows from r0, k from
+// k0) into a 128-byte-swizzled stage: 16-byte chunk j of row r lands at
+// r * 128 + ((j ^ (r & 7)) * 16).  Rows at or past nrows are zero.
+__device__ __forceinline__ void stage_rows(unsigned char* dst, const bf16* __restrict__ src, int ld, int r0, int nrows,
+                                           int k0, int rows)
+{
+    for (int i = threadIdx.x; i < rows * 8; i += blockDim.x) {
+        const int r = i >> 3, j = i & 7;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (r0 + r < nrows) v = *reinterpret_cast<const uint4*>(src + (size_t)(r0 + r) * ld + k0 + j * 8);
+        *reinterpret_cast<uint4*>(dst + r * 128 + ((j ^ (r & 7)) << 4)) = v;
+    }
+}
+
+}  // namespace tc
+
+// C[M,N] = A[M,K] B[N,K]^T (+ bias) (ReLU) on tcgen05; N a multiple of BN, K of 64;
+// split K as k_gemm_nt (gridDim.z slices of kchunk, partial products at C + z * cstride).
+template <int BN>
+__global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, int lda, const bf16* __restrict__ B, int ldb,
+                                                 float* __restrict__ C, int ldc, bf16* __restrict__ Cb, int ldcb,
+                                                 const float* __restrict__ bias, int relu, int M, int K, int kchunk,
+                                                 size_t cstride, int* err)
+{
+    using namespace tc;
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_ok;
+    unsigned char* base = smem_raw + ((1024 - (saddr(smem_raw) & 1023)) & 1023);
+    unsigned char* As = base;                          // [2][BM * 128 B]
+    unsigned char* Bs = base + 2 * BM * BK * 2;        // [2][BN * 128 B]
+    if (gridDim.z > 1) {
+        const int z = blockIdx.z;
+        A += (size_t)z * kchunk;
+        B += (size_t)z * kchunk;
+        C += (size_t)z * cstride;
+        K = min(kchunk, K - z * kchunk);
+    }
+    const int bm = blockIdx.y * BM, bn = blockIdx.x * BN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(saddr(&tmem_base)), "r"(BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(saddr(&bar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(saddr(&bar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_ok = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tm = tmem_base;
+    const int nk = K / BK;
+    int issued = 0;                    // slices whose products were committed
+    for (int kc = 0; kc < nk; kc++) {
+        const int st = kc & 1;
+        if (kc >= 2) {                 // the products that read this stage are done
+            if (threadIdx.x == 0 && !mbar_wait(&bar[st], ((kc - 2) >> 1) & 1)) s_ok = 0;
+            __syncthreads();
+            if (!s_ok) break;
+        }
+        stage_rows(As + st * BM * 128, A, lda, bm, M, kc * BK, BM);
+        stage_rows(Bs + st * BN * 128, B, ldb, bn, 1 << 30, kc * BK, BN);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = saddr(As + st * BM * 128), b0 = saddr(Bs + st * BN * 128);
+#pragma unroll
+            for (int k = 0; k < BK / 16; k++)
+                tc::mma(tm, sdesc(a0 + 32 * k), sdesc(b0 + 32 * k), idesc(BM, BN), (kc | k) != 0);
+            commit(&bar[st]);
+        }
+        issued = kc + 1;
+    }
+    // the last committed slice's barrier completes after all earlier products
+    if (threadIdx.x == 0 && issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) s_ok = 0;
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (s_ok && issued == nk) {
+        const int row = bm + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            uint32_t r[32];
+            ld32(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+            if (row < M) {
+                const int col = bn + c0;
+#pragma unroll
+                for (int j = 0; j < 32; j += 2) {
+                    float v0 = __uint_as_float(r[j]), v1 = __uint_as_float(r[j + 1]);
+                    if (nk == 0) v0 = v1 = 0.f;
+                    if (bias) { v0 += bias[col + j]; v1 += bias[col + j + 1]; }
+                    if (relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                    if (C) *reinterpret_cast<float2*>(C + (size_t)row * ldc + col + j) = make_float2(v0, v1);
+                    if (Cb) *reinterpret_cast<__nv_bfloat162*>(Cb + (size_t)row * ldcb + col + j) = __floats2bfloat162_rn(v0, v1);
+                }
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tm), "r"(BN));
+}
+
+// C[r, c] = sum over the slices z, in ascending order, of part[z][r, c] ([M, N] each).
+__global__ void k_splitk_reduce(const float* __restrict__ part, int nsplit, int M, int N, float* __restrict__ C, int ldc)
+{
+    const size_t MN = (size_t)M * N;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < MN; e += (size_t)gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        for (int z = 0; z < nsplit; z++) acc += part[z * MN + e];
+        C[(e / N) * ldc + e % N] = acc;
+    }
 }
 
 // out[c, r] = in[r, c] for an R x Cc block (both multiples of 32).
@@ -222,6 +427,29 @@ __global__ void k_mse(const float* __restrict__ y, const float* __restrict__ tar
 }
 
 // Adam (Kingma & Ba, 2015) on FP32 master weights; refreshes the BF16 copy.
+// Sum of v[0..n) in a fixed order: block b sums its contiguous range (strided by
+// thread, then a shared-memory tree), the final pass adds the blocks in order.
+__global__ void k_sum_part(const float* __restrict__ v, size_t n, double* __restrict__ part)
+{
+    __shared__ double sh[256];
+    const size_t per = (n + gridDim.x - 1) / gridDim.x, b0 = blockIdx.x * per, e0 = min(n, b0 + per);
+    double acc = 0.0;
+    for (size_t e = b0 + threadIdx.x; e < e0; e += blockDim.x) acc += v[e];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+__global__ void k_sum_final(const double* __restrict__ part, int n, double* __restrict__ out)
+{
+    double a = 0.0;
+    for (int i = 0; i < n; i++) a += part[i];
+    *out = a;
+}
+
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v, const float* __restrict__ g,
                        bf16* __restrict__ wb, size_t n, float lr, float b1, float b2, float eps, float c1, float c2, float wd)
 {
@@ -293,6 +521,11 @@ struct cs_sur {
     bf16 *cols[3] = {nullptr, nullptr, nullptr};
     bf16 *colsT = nullptr, *dzT = nullptr, *wT = nullptr, *hT = nullptr;
     float *dz = nullptr, *dh = nullptr, *dcols = nullptr, *part = nullptr;
+    float* kpart = nullptr;                 // split-K partial products
+    size_t kpart_n = 0;
+    double *lpart = nullptr, *lsum = nullptr;   // loss reduction
+    int* d_err = nullptr;                   // set by a tensor-core GEMM whose wait gave up
+    int gemm_impl = 0;                      // 0: tcgen05, 1: mma.sync
     bf16* dzb = nullptr;
     float *xdev = nullptr, *tdev = nullptr, *sq = nullptr, *ydev = nullptr;
     std::vector<void*> allocs;
@@ -350,12 +583,47 @@ static void build_layers(cs_sur* s)
     s->np = ofs;
 }
 
+constexpr int kLossBlocks = 296;
+
+// One product (or, with nsplit > 1, its K slices of kchunk) on the selected path.
+static int gemm_launch(cs_sur* s, const bf16* A, int lda, const bf16* B, int ldb, float* C, int ldc, bf16* Cb, int ldcb,
+                       const float* bias, int relu, int M, int N, int K, int nsplit, int kchunk, size_t cstride)
+{
+    if (s->gemm_impl == 0 && K % 64 == 0 && kchunk % 64 == 0) {
+        dim3 grid(N / 64, (M + tc::BM - 1) / tc::BM, nsplit);
+        k_gemm_tc<64><<<grid, 128, tc::smem_bytes(64), s->stream>>>(A, lda, B, ldb, C, ldc, Cb, ldcb, bias, relu, M, K,
+                                                                    kchunk, cstride, s->d_err);
+    } else {
+        dim3 grid(N / 64, M / 64, nsplit);
+        sur::k_gemm_nt<<<grid, 128, 0, s->stream>>>(A, lda, B, ldb, C, ldc, Cb, ldcb, bias, relu, K, kchunk, cstride);
+    }
+    SCK(cudaGetLastError());
+    return CS_OK;
+}
+
 static int gemm(cs_sur* s, const bf16* A, int lda, const bf16* B, int ldb, float* C, int ldc, bf16* Cb, int ldcb,
                 const float* bias, int relu, int M, int N, int K)
 {
     if (M % 64 || N % 64 || K % 32) return sur_err(s, CS_E_ARG, "gemm shape %d x %d x %d not padded", M, N, K);
-    dim3 grid(N / 64, M / 64);
-    sur::k_gemm_nt<<<grid, 128, 0, s->stream>>>(A, lda, B, ldb, C, ldc, Cb, ldcb, bias, relu, K);
+    return gemm_launch(s, A, lda, B, ldb, C, ldc, Cb, ldcb, bias, relu, M, N, K, 1, K, 0);
+}
+
+// C = A B^T for a product with few output tiles and a long K (the convolutions'
+// weight gradients, K = batch x time points): K is split into slices so that about
+// two blocks per SM run, and the slices' partial products are summed in a fixed order.
+constexpr int kMaxSplit = 64;
+
+static int gemm_splitk(cs_sur* s, const bf16* A, int lda, const bf16* B, int ldb, float* C, int ldc, int M, int N, int K)
+{
+    if (M % 64 || N % 64 || K % 32) return sur_err(s, CS_E_ARG, "gemm shape %d x %d x %d not padded", M, N, K);
+    const int tiles = (M / 64) * (N / 64);
+    int nsplit = std::min(kMaxSplit, std::max(1, std::min((K + 255) / 256, 296 / tiles)));
+    if (nsplit == 1 || (size_t)M * N * kMaxSplit > s->kpart_n) return gemm(s, A, lda, B, ldb, C, ldc, nullptr, 0, nullptr, 0, M, N, K);
+    const int kchunk = ((K + nsplit - 1) / nsplit + 63) / 64 * 64;
+    nsplit = (K + kchunk - 1) / kchunk;
+    int r = gemm_launch(s, A, lda, B, ldb, s->kpart, N, nullptr, 0, nullptr, 0, M, N, K, nsplit, kchunk, (size_t)M * N);
+    if (r) return r;
+    sur::k_splitk_reduce<<<std::min(1184, (M * N + 255) / 256), 256, 0, s->stream>>>(s->kpart, nsplit, M, N, C, ldc);
     SCK(cudaGetLastError());
     return CS_OK;
 }
@@ -424,6 +692,15 @@ int cs_sur_create(int max_batch, int device, cs_sur** out)
     SA(s->dz, maxz); SA(s->dzb, maxz); SA(s->dzT, maxz); SA(s->dh, maxz); SA(s->hT, maxz);
     SA(s->wT, maxw);
     SA(s->part, (size_t)((B * 8 * kT0 + 255) / 256 + 1) * 3000);
+    {
+        size_t mn = 0;
+        for (int i = 0; i < 3; i++) mn = std::max(mn, (size_t)s->L[6 + i].outP * s->L[6 + i].inP);
+        s->kpart_n = mn * kMaxSplit;
+        SA(s->kpart, s->kpart_n);
+    }
+    SA(s->lpart, (size_t)kLossBlocks); SA(s->lsum, (size_t)1); SA(s->d_err, (size_t)1);
+    SCK(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+    SCK(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::smem_bytes(64)));
     SA(s->xdev, (size_t)B * kIn); SA(s->tdev, (size_t)B * kTOut * kNOut); SA(s->sq, (size_t)B * kTOut * kNOut);
     SA(s->ydev, (size_t)B * kTOut * kNOut);
 #undef SA
@@ -529,7 +806,7 @@ static int backward(cs_sur* s, int Bp)
         // dW = dz^T cols: A = dz^T [outP, M], B = cols^T [inP, M]
         if ((r = transpose(s, s->dzb, kCh, s->dzT, M, M, l.outP))) return r;
         if ((r = transpose(s, s->cols[ci], l.inP, s->colsT, M, M, l.inP))) return r;
-        if ((r = gemm(s, s->dzT, M, s->colsT, M, s->g + l.wofs, l.inP, nullptr, 0, nullptr, 0, l.outP, l.inP, M))) return r;
+        if ((r = gemm_splitk(s, s->dzT, M, s->colsT, M, s->g + l.wofs, l.inP, l.outP, l.inP, M))) return r;
         if ((r = colsum(s, s->dz, M, kCh, s->g + l.bofs))) return r;
         // dcols = dz W: A = dz [M, outP], B = W^T [inP, outP]
         if ((r = transpose(s, s->wb + l.wofs, l.inP, s->wT, l.outP, l.outP, l.inP))) return r;
@@ -555,6 +832,19 @@ static int backward(cs_sur* s, int Bp)
     return CS_OK;
 }
 
+// Wait for the stream; an error if a tensor-core GEMM's bounded wait gave up.
+static int sync_check(cs_sur* s)
+{
+    int e = 0;
+    SCK(cudaMemcpyAsync(&e, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
+    if (e) {
+        SCK(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+        return sur_err(s, CS_E_CUDA, "a tensor-core GEMM gave up waiting for its products");
+    }
+    return CS_OK;
+}
+
 static int load_batch(cs_sur* s, const float* x, const float* target, int n, int* Bp)
 {
     if (n <= 0 || n > s->bmax) return sur_err(s, CS_E_RANGE, "batch of %d outside 1..%d", n, s->bmax);
@@ -576,12 +866,14 @@ static int loss_grad(cs_sur* s, const float* x, const float* target, int n, floa
     SCK(cudaGetLastError());
     if ((r = backward(s, Bp))) return r;
     if (loss) {
-        std::vector<float> sq((size_t)n * kTOut * kNOut);
-        SCK(cudaMemcpyAsync(sq.data(), s->sq, sizeof(float) * sq.size(), cudaMemcpyDeviceToHost, s->stream));
-        SCK(cudaStreamSynchronize(s->stream));
+        const size_t nsq = (size_t)n * kTOut * kNOut;
+        sur::k_sum_part<<<kLossBlocks, 256, 0, s->stream>>>(s->sq, nsq, s->lpart);
+        sur::k_sum_final<<<1, 1, 0, s->stream>>>(s->lpart, kLossBlocks, s->lsum);
+        SCK(cudaGetLastError());
         double acc = 0.0;
-        for (float v : sq) acc += v;
-        *loss = (float)(acc / (double)sq.size());
+        SCK(cudaMemcpyAsync(&acc, s->lsum, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        if ((r = sync_check(s))) return r;
+        *loss = (float)(acc / (double)nsq);
     }
     return CS_OK;
 }
@@ -600,8 +892,7 @@ int cs_sur_forward(cs_sur* s, const float* x, int n, float* y)
         SCK(cudaMemcpyAsync(y + (size_t)b0 * kTOut * kNOut, s->ydev, sizeof(float) * nb * kTOut * kNOut,
                             cudaMemcpyDeviceToHost, s->stream));
     }
-    SCK(cudaStreamSynchronize(s->stream));
-    return CS_OK;
+    return sync_check(s);
 }
 
 int cs_sur_loss_grad(cs_sur* s, const float* x, const float* target, int n, float* loss, float* grad)
@@ -612,7 +903,7 @@ int cs_sur_loss_grad(cs_sur* s, const float* x, const float* target, int n, floa
     if (grad) {
         std::vector<float> h(s->np);
         SCK(cudaMemcpyAsync(h.data(), s->g, sizeof(float) * s->np, cudaMemcpyDeviceToHost, s->stream));
-        SCK(cudaStreamSynchronize(s->stream));
+        if ((r = sync_check(s))) return r;
         size_t k = 0;
         for (auto& l : s->L) {
             for (int o = 0; o < l.out; o++)
@@ -633,7 +924,16 @@ int cs_sur_train_step(cs_sur* s, const float* x, const float* target, int n, flo
     const float c1 = 1.f - powf(b1, (float)s->t), c2 = 1.f - powf(b2, (float)s->t);
     sur::k_adam<<<1184, 256, 0, s->stream>>>(s->w, s->m, s->v, s->g, s->wb, s->np, lr, b1, b2, 1e-8f, c1, c2, weight_decay);
     SCK(cudaGetLastError());
-    if (!loss) SCK(cudaStreamSynchronize(s->stream));
+    if (!loss) return sync_check(s);
+    return CS_OK;
+}
+
+int cs_sur_set_gemm(cs_sur* s, int impl)
+{
+    if (!s) return CS_E_ARG;
+    if (impl != 0 && impl != 1) return sur_err(s, CS_E_ARG, "GEMM path must be 0 (tcgen05) or 1 (mma.sync)");
+    SCK(cudaStreamSynchronize(s->stream));
+    s->gemm_impl = impl;
     return CS_OK;
 }
 

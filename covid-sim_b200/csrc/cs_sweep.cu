@@ -216,6 +216,7 @@ struct cs_gpu_ctx {
     cs_counters* d_series = nullptr;
     int series_cap = 0;
     int day_every_step = -1;    // the probs_every_step the day graph was captured with
+    long long geometry_gen = 0; // bumped when set_params replaces the kernel-row table
     size_t tp_smem[2] = {0, 0}; // dynamic shared memory enabled for k_tot_prob_rows<false>, <true>
     cudaGraph_t day_graph = nullptr;
     cudaGraphExec_t day_exec = nullptr;
@@ -1598,7 +1599,8 @@ struct DayCtl {
     uint8_t socd_value, pad[3];
 };
 
-__global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop, const DayCtl* ctl)
+__device__ void k_close_places_body(const DevPop& d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop,
+                                    const DayCtl* ctl)
 {
     if (ctl) {   // a day graph's closure: only on the day the trigger fired, window from the device
         if (!ctl->close || !((ctl->pol.close_place_types >> pt) & 1u)) return;
@@ -1638,11 +1640,24 @@ __global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t st
         __syncthreads();
     }
 }
+__global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop, const DayCtl* ctl)
+{
+    k_close_places_body(d, pt, sel, start, stop, ctl);
+}
+__global__ void k_close_places_multi(const DevPop* __restrict__ pops, int pt, DayCtl* const* ctls)
+{
+    const DevPop& d = pops[blockIdx.y];
+    if (pt < d.NPT) k_close_places_body(d, pt, nullptr, 0, 0, ctls[blockIdx.y]);
+}
 
 // The test after a timestep whether the susceptible fraction fell by more than 0.2
 // since UpdateProbs last ran (src/CovidSim.cpp:1520-1526); S is fresh from k_cell_totals.
-__global__ void k_probs_check(DevPop d, DayCtl* ctl)
+__device__ __forceinline__ void k_probs_check_body(const DevPop& d, DayCtl* ctl, int day_end)
 {
+    if (!day_end && !ctl->pol.probs_every_step) {   // this realisation tests at day ends only
+        ctl->update = 0;
+        return;
+    }
     const double prop_s = (double)d.C->S / (double)d.N;
     int up = 0;
     if (ctl->prev_prop_s - prop_s > 0.2) {
@@ -1651,12 +1666,17 @@ __global__ void k_probs_check(DevPop d, DayCtl* ctl)
     }
     ctl->update = up;
 }
+__global__ void k_probs_check(DevPop d, DayCtl* ctl, int day_end) { k_probs_check_body(d, ctl, day_end); }
+__global__ void k_probs_check_multi(const DevPop* __restrict__ pops, DayCtl* const* ctls, int day_end)
+{
+    k_probs_check_body(pops[blockIdx.x], ctls[blockIdx.x], day_end);
+}
 
 // End of a day of the run loop: the day's counters into the series, and the global
 // ICU trigger (src/CovidSim.cpp:3150-3159 with global thresholds) switching case
 // isolation, household quarantine, social distancing and place closure on for
 // pol.duration days, then off.  The switch takes effect from the next timestep.
-__global__ void k_day_logic(DevPop d, DayCtl* ctl, const int32_t* clock, DevIv* iv)
+__device__ void k_day_logic_body(const DevPop& d, DayCtl* ctl, const int32_t* clock, DevIv* iv)
 {
     const int day = ctl->day;
     {
@@ -1703,14 +1723,27 @@ __global__ void k_day_logic(DevPop d, DayCtl* ctl, const int32_t* clock, DevIv* 
     }
     ctl->day = day + 1;
 }
+__global__ void k_day_logic(DevPop d, DayCtl* ctl, const int32_t* clock, DevIv* iv) { k_day_logic_body(d, ctl, clock, iv); }
+// one block per member; the window struct is the member's own (written only here and
+// by cs_gpu_set_interventions)
+__global__ void k_day_logic_multi(const DevPop* __restrict__ pops, DayCtl* const* ctls)
+{
+    const DevPop& d = pops[blockIdx.x];
+    k_day_logic_body(d, ctls[blockIdx.x], d.step_clock, const_cast<DevIv*>(d.iv));
+}
 
-__global__ void k_socdist_fill(DevPop d, const DayCtl* ctl)
+__device__ __forceinline__ void k_socdist_fill_body(const DevPop& d, const DayCtl* ctl)
 {
     if (!ctl->socd_write) return;
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < d.NM; m += gridDim.x * blockDim.x) d.socdist[m] = ctl->socd_value;
 }
+__global__ void k_socdist_fill(DevPop d, const DayCtl* ctl) { k_socdist_fill_body(d, ctl); }
+__global__ void k_socdist_fill_multi(const DevPop* __restrict__ pops, DayCtl* const* ctls)
+{
+    k_socdist_fill_body(pops[blockIdx.y], ctls[blockIdx.y]);
+}
 
-__global__ void k_cell_totals(DevPop d)
+__device__ __forceinline__ void k_cell_totals_body(const DevPop& d)
 {
     long long s = 0, l = 0, i = 0, r = 0, dd = 0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
@@ -1727,6 +1760,13 @@ __global__ void k_cell_totals(DevPop d)
         cnt_add(CSB_CTR(S), s); cnt_add(CSB_CTR(L), l); cnt_add(CSB_CTR(I), i);
         cnt_add(CSB_CTR(R), r); cnt_add(CSB_CTR(D), dd);
     }
+}
+__global__ void k_cell_totals(DevPop d) { k_cell_totals_body(d); }
+__global__ void k_cell_totals_multi(const DevPop* __restrict__ pops) { k_cell_totals_body(pops[blockIdx.y]); }
+// S..D of each member's counter block to zero before k_cell_totals_multi
+__global__ void k_zero_totals_multi(const DevPop* __restrict__ pops)
+{
+    if (threadIdx.x < 5) (&pops[blockIdx.x].C->S)[threadIdx.x] = 0;
 }
 
 // ================================================================ host API
@@ -2026,6 +2066,7 @@ int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
     c->hp = *params;
     CK(cudaMemcpyAsync(c->dP, params, sizeof(cs_params), cudaMemcpyHostToDevice, c->stream));
     if (geometry) {   // the kernel rows and the n-weighted denominators depend on it
+        c->geometry_gen++;
         CK(cudaStreamSynchronize(c->stream));
         if (c->stat->Gtab) cudaFree(c->stat->Gtab);
         c->stat->Gtab = c->Gtab = nullptr;
@@ -2420,7 +2461,7 @@ static int enqueue_day(cs_gpu_ctx* c, int spd, bool every_step)
         if (!every_step && s < spd - 1) continue;
         r = enqueue_totals(c);
         if (r) return r;
-        LAUNCH(k_probs_check, 1, 1, d, c->d_ctl);
+        LAUNCH(k_probs_check, 1, 1, d, c->d_ctl, s == spd - 1 ? 1 : 0);
         if (s == spd - 1) LAUNCH(k_day_logic, 1, kThreads, d, c->d_ctl, (const int32_t*)c->d_clock, c->dIv);
         r = cs_gpu_update_probs(c, 0);
         if (r) return r;
@@ -2481,16 +2522,17 @@ static int run_days(cs_gpu_ctx* c, int days, int spd, bool every_step)
     return CS_OK;
 }
 
-int cs_gpu_run(cs_gpu_ctx* c, int days, const cs_run_policy* policy, cs_counters* daily)
+// Timesteps per day of the context's parameters, or 0 when not a whole number.
+static int steps_per_day(const cs_gpu_ctx* c)
 {
-    if (!c || days < 0) return CS_E_ARG;
-    if (!c->run_started) return set_err(c, CS_E_STATE, "run before begin_run");
-    if (days == 0) return CS_OK;
     const int spd = (int)std::lround(c->hp.TimeStepsPerDay);
-    if (spd < 1 || (double)spd != c->hp.TimeStepsPerDay)
-        return set_err(c, CS_E_ARG, "the run loop needs a whole number of timesteps per day");
-    cs_run_policy pol{};
-    if (policy) pol = *policy;
+    return (spd >= 1 && (double)spd == c->hp.TimeStepsPerDay) ? spd : 0;
+}
+
+// The run loop's device state for a run of `days` days from t = 0 under pol: the
+// control block, the step clock at 0, and room for the day-end series.
+static int day_ctl_start(cs_gpu_ctx* c, int days, const cs_run_policy& pol)
+{
     if (pol.icu_trigger && pol.icu_window < 1) return set_err(c, CS_E_ARG, "icu_window must be at least 1 day");
     if (!c->d_ctl) {
         CK(cudaMalloc(&c->d_ctl, sizeof(DayCtl)));
@@ -2512,20 +2554,49 @@ int cs_gpu_run(cs_gpu_ctx* c, int days, const cs_run_policy* policy, cs_counters
     const int32_t zero = 0;
     CK(cudaMemcpyAsync(c->d_ctl, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_clock, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->stream));
-    c->d.step_clock = c->d_clock;
-    c->d.gate = &c->d_ctl->update;
-    int r = run_days(c, days, spd, pol.probs_every_step != 0);
-    c->d.step_clock = nullptr;
-    c->d.gate = nullptr;
-    if (r) return r;
-    cs_counters last;
-    CK(cudaMemcpyAsync(&last, c->d_series + (days - 1), sizeof(last), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));   // h and zero live on this stack frame
+    return CS_OK;
+}
+
+// The day-end series of a finished run into daily (may be NULL); the stream is
+// synchronised afterwards, so *last holds the final day's counters.
+static int day_series_out(cs_gpu_ctx* c, int days, cs_counters* daily, cs_counters* last)
+{
+    CK(cudaMemcpyAsync(last, c->d_series + (days - 1), sizeof(*last), cudaMemcpyDeviceToHost, c->stream));
     if (daily) CK(cudaMemcpyAsync(daily, c->d_series, sizeof(cs_counters) * (size_t)days, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+static int check_give_ups(cs_gpu_ctx* c, const cs_counters& last)
+{
     if (last.err_queue_overflow || last.err_spatial_tries || last.err_kernel_range)
         return set_err(c, CS_E_OVERFLOW, "bounded device loop gave up (spatial %lld, queue %lld, kernel range %lld)",
                        (long long)last.err_spatial_tries, (long long)last.err_queue_overflow, (long long)last.err_kernel_range);
     return CS_OK;
+}
+
+int cs_gpu_run(cs_gpu_ctx* c, int days, const cs_run_policy* policy, cs_counters* daily)
+{
+    if (!c || days < 0) return CS_E_ARG;
+    if (!c->run_started) return set_err(c, CS_E_STATE, "run before begin_run");
+    if (days == 0) return CS_OK;
+    const int spd = steps_per_day(c);
+    if (!spd) return set_err(c, CS_E_ARG, "the run loop needs a whole number of timesteps per day");
+    cs_run_policy pol{};
+    if (policy) pol = *policy;
+    int r = day_ctl_start(c, days, pol);
+    if (r) return r;
+    c->d.step_clock = c->d_clock;
+    c->d.gate = &c->d_ctl->update;
+    r = run_days(c, days, spd, pol.probs_every_step != 0);
+    c->d.step_clock = nullptr;
+    c->d.gate = nullptr;
+    if (r) return r;
+    cs_counters last;
+    r = day_series_out(c, days, daily, &last);
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    return check_give_ups(c, last);
 }
 
 // List counters of every member of a batch back to zero (the end-of-sweep reset).
@@ -2552,6 +2623,19 @@ struct cs_gpu_batch {
     double* d_t = nullptr;   // the timestep's t, read by every member's k_set_step
     DevPop* d_pops = nullptr; // members' DevPop (t taken from d_t)
     int lanes = 8;            // spatial lanes of the batched launches
+    // device run loop (cs_gpu_batch_run): members' DevPop with step clocks and
+    // UpdateProbs gates, their control blocks, one graph per day
+    DevPop* d_pops_day = nullptr;
+    DayCtl** d_ctls = nullptr;
+    cudaGraph_t day_graph = nullptr;
+    cudaGraphExec_t day_exec = nullptr;
+    int day_every_step = -1;
+    int day_spd = 0;
+    std::vector<long long> day_geometry;       // members' geometry_gen when the day graph was captured
+    std::vector<long long> member_day_launches;
+    static constexpr int kSide = 8;            // streams the members' UpdateProbs chains fan out to
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kSide] = {};
     char err[512] = {0};
 };
 
@@ -2576,6 +2660,10 @@ static void batch_drop_graph(cs_gpu_batch* b)
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
+    if (b->day_exec) cudaGraphExecDestroy(b->day_exec);
+    if (b->day_graph) cudaGraphDestroy(b->day_graph);
+    b->day_exec = nullptr;
+    b->day_graph = nullptr;
 }
 
 int cs_gpu_batch_create(cs_gpu_ctx* const* members, int n, cs_gpu_batch** out)
@@ -2618,12 +2706,11 @@ const char* cs_gpu_batch_last_error(const cs_gpu_batch* b) { return b ? b->err :
 
 // The batched timestep, in the order of step_eager (InfectSweep, then
 // IncubRecoverySweep without a second k_set_step).
-static int batch_enqueue(cs_gpu_batch* b)
+static int batch_enqueue(cs_gpu_batch* b, const DevPop* pops)
 {
     const int R = (int)b->members.size();
     const int grid = b->members[0]->grid;
     const dim3 g(grid, R), one(1, R);
-    const DevPop* pops = b->d_pops;
     BLAUNCH(k_set_step_multi, one, 1, pops, 0.0, 0ull);
     BLAUNCH(k_build_active_multi, g, kThreads, pops, 0);
     BLAUNCH(k_infector_hh_spatial_multi, g, kThreads, pops);
@@ -2645,14 +2732,20 @@ static int batch_enqueue(cs_gpu_batch* b)
     return CS_OK;
 }
 
+static int batch_same_grid(cs_gpu_batch* b)
+{
+    for (size_t k = 1; k < b->members.size(); k++)
+        if (b->members[k]->grid != b->members[0]->grid)
+            return batch_err(b, CS_E_ARG, "members use different launch shapes; set one with cs_gpu_batch_set_grid");
+    return CS_OK;
+}
+
 static int batch_capture(cs_gpu_batch* b, double t, int run)
 {
     (void)t;
     (void)run;
     const int n = (int)b->members.size();
-    for (int k = 1; k < n; k++)
-        if (b->members[k]->grid != b->members[0]->grid)
-            return batch_err(b, CS_E_ARG, "members use different launch shapes; set one with cs_gpu_batch_set_grid");
+    if (int r = batch_same_grid(b)) return r;
     // members' DevPop, each taking t from the batch
     std::vector<DevPop> hp(n);
     for (int k = 0; k < n; k++) {
@@ -2662,7 +2755,7 @@ static int batch_capture(cs_gpu_batch* b, double t, int run)
     BCK(cudaMemcpyAsync(b->d_pops, hp.data(), sizeof(DevPop) * n, cudaMemcpyHostToDevice, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    int r = batch_enqueue(b);
+    int r = batch_enqueue(b, b->d_pops);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (r || e != cudaSuccess) {
@@ -2729,11 +2822,178 @@ int cs_gpu_batch_sync(cs_gpu_batch* b)
     return CS_OK;
 }
 
+// ------------------------------------------------------- batched run loop
+// The single-context day (enqueue_day) for every member at once: the batched
+// timesteps, then the members' totals, UpdateProbs tests and day logic as one
+// launch each (blockIdx selects the member), and each member's gated UpdateProbs
+// chain on one of kSide side streams, forked from and joined back into the
+// batch's stream, so that the chains' mostly empty launches overlap.
+static int batch_updates(cs_gpu_batch* b)
+{
+    BCK(cudaEventRecord(b->ev_fork, b->stream));
+    for (int i = 0; i < cs_gpu_batch::kSide; i++) BCK(cudaStreamWaitEvent(b->side[i], b->ev_fork, 0));
+    int r = CS_OK;
+    for (size_t k = 0; k < b->members.size() && !r; k++) {
+        cs_gpu_ctx* m = b->members[k];
+        m->stream = b->side[k % cs_gpu_batch::kSide];
+        const long long l0 = m->launches;
+        r = cs_gpu_update_probs(m, 0);
+        b->member_day_launches[k] += m->launches - l0;
+        m->launches = l0;
+        m->stream = b->stream;
+        if (r) batch_err(b, r, "member %zu UpdateProbs: %s", k, m->err);
+    }
+    // joined even after an error, so that the capture can end
+    for (int i = 0; i < cs_gpu_batch::kSide; i++) {
+        cudaEventRecord(b->ev_join[i], b->side[i]);
+        cudaStreamWaitEvent(b->stream, b->ev_join[i], 0);
+    }
+    return r;
+}
+
+static int batch_enqueue_day(cs_gpu_batch* b, int spd, bool every_step)
+{
+    const int R = (int)b->members.size();
+    const DevPop* pops = b->d_pops_day;
+    int npt = 0;
+    for (cs_gpu_ctx* m : b->members) npt = std::max(npt, m->d.NPT);
+    for (int s = 0; s < spd; s++) {
+        int r = batch_enqueue(b, pops);
+        if (r) return r;
+        for (int k = 0; k < R; k++) b->member_day_launches[k] += 11;
+        if (!every_step && s < spd - 1) continue;
+        const int day_end = s == spd - 1 ? 1 : 0;
+        BLAUNCH(k_zero_totals_multi, R, 32, pops);
+        BLAUNCH(k_cell_totals_multi, dim3(64, R), kThreads, pops);
+        BLAUNCH(k_probs_check_multi, R, 1, pops, b->d_ctls, day_end);
+        if (day_end) BLAUNCH(k_day_logic_multi, R, kThreads, pops, b->d_ctls);
+        for (int k = 0; k < R; k++) b->member_day_launches[k] += 2 + day_end;
+        r = batch_updates(b);
+        if (r) return r;
+    }
+    const dim3 g(b->members[0]->grid, R);
+    BLAUNCH(k_socdist_fill_multi, g, kThreads, pops, b->d_ctls);
+    for (int pt = 0; pt < npt; pt++) BLAUNCH(k_close_places_multi, g, kThreads, pops, pt, b->d_ctls);
+    for (int k = 0; k < R; k++) b->member_day_launches[k] += 1 + b->members[k]->d.NPT;
+    return CS_OK;
+}
+
+static int batch_capture_day(cs_gpu_batch* b, int spd, bool every_step)
+{
+    const int n = (int)b->members.size();
+    if (!b->ev_fork) {
+        BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        for (int i = 0; i < cs_gpu_batch::kSide; i++) {
+            BCK(cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking));
+            BCK(cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming));
+        }
+    }
+    for (cs_gpu_ctx* m : b->members)
+        if (int r = tot_prob_prepare(m)) return batch_err(b, r, "%s", m->err);
+    b->member_day_launches.assign(n, 0);
+    // the members' own launches (their UpdateProbs chains) read the clock and gate too
+    for (cs_gpu_ctx* m : b->members) {
+        m->d.step_clock = m->d_clock;
+        m->d.gate = &m->d_ctl->update;
+    }
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int r = batch_enqueue_day(b, spd, every_step);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    for (cs_gpu_ctx* m : b->members) {
+        m->d.step_clock = nullptr;
+        m->d.gate = nullptr;
+    }
+    if (r || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return r ? r : batch_err(b, CS_E_CUDA, "batch day graph capture: %s", cudaGetErrorString(e));
+    }
+    cudaError_t ei = cudaGraphInstantiate(&b->day_exec, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        b->day_exec = nullptr;
+        return batch_err(b, CS_E_CUDA, "batch day graph instantiate: %s", cudaGetErrorString(ei));
+    }
+    b->day_graph = g;
+    b->day_every_step = every_step ? 1 : 0;
+    b->day_spd = spd;
+    b->day_geometry.resize(n);
+    for (int k = 0; k < n; k++) b->day_geometry[k] = b->members[k]->geometry_gen;
+    return CS_OK;
+}
+
+int cs_gpu_batch_run(cs_gpu_batch* b, int days, const cs_run_policy* policies, cs_counters* daily)
+{
+    if (!b || days < 0) return CS_E_ARG;
+    const int n = (int)b->members.size();
+    for (int k = 0; k < n; k++)
+        if (!b->members[k]->run_started) return batch_err(b, CS_E_STATE, "member %d: run before begin_run", k);
+    if (days == 0) return CS_OK;
+    if (int r = batch_same_grid(b)) return r;
+    for (int k = 0; k < n; k++)
+        if (b->members[k]->prof) return batch_err(b, CS_E_STATE, "member %d has per-launch timing on", k);
+    const int spd = steps_per_day(b->members[0]);
+    for (int k = 0; k < n; k++)
+        if (!spd || steps_per_day(b->members[k]) != spd)
+            return batch_err(b, CS_E_ARG, "the batched run loop needs the same whole number of timesteps per day in every member");
+    bool every = false;
+    for (int k = 0; k < n; k++) {
+        cs_gpu_ctx* m = b->members[k];
+        cs_run_policy pol{};
+        if (policies) pol = policies[k];
+        every = every || pol.probs_every_step;
+        if (int r = day_ctl_start(m, days, pol)) return batch_err(b, r, "member %d: %s", k, m->err);
+    }
+    if (!b->d_pops_day) {
+        BCK(cudaMalloc(&b->d_pops_day, sizeof(DevPop) * n));
+        BCK(cudaMalloc(&b->d_ctls, sizeof(DayCtl*) * n));
+    }
+    std::vector<DevPop> hp(n);
+    std::vector<DayCtl*> hc(n);
+    for (int k = 0; k < n; k++) {
+        cs_gpu_ctx* m = b->members[k];
+        hp[k] = m->d;
+        hp[k].step_clock = m->d_clock;
+        hp[k].gate = &m->d_ctl->update;
+        hc[k] = m->d_ctl;
+    }
+    BCK(cudaMemcpyAsync(b->d_pops_day, hp.data(), sizeof(DevPop) * n, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->d_ctls, hc.data(), sizeof(DayCtl*) * n, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    bool stale = !b->day_exec || b->day_every_step != (every ? 1 : 0) || b->day_spd != spd;
+    for (int k = 0; k < n && !stale; k++) stale = b->day_geometry[k] != b->members[k]->geometry_gen;
+    if (stale) {
+        if (b->day_exec) cudaGraphExecDestroy(b->day_exec);
+        if (b->day_graph) cudaGraphDestroy(b->day_graph);
+        b->day_exec = nullptr;
+        b->day_graph = nullptr;
+        if (int r = batch_capture_day(b, spd, every)) return r;
+    }
+    for (int d = 0; d < days; d++) BCK(cudaGraphLaunch(b->day_exec, b->stream));
+    for (int k = 0; k < n; k++) b->members[k]->launches += b->member_day_launches[k] * days;
+    std::vector<cs_counters> last(n);
+    for (int k = 0; k < n; k++)
+        if (int r = day_series_out(b->members[k], days, daily ? daily + (size_t)k * days : nullptr, &last[k]))
+            return batch_err(b, r, "member %d: %s", k, b->members[k]->err);
+    BCK(cudaStreamSynchronize(b->stream));
+    for (int k = 0; k < n; k++)
+        if (int r = check_give_ups(b->members[k], last[k])) return batch_err(b, r, "member %d: %s", k, b->members[k]->err);
+    return CS_OK;
+}
+
 void cs_gpu_batch_destroy(cs_gpu_batch* b)
 {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
     batch_drop_graph(b);
+    for (int i = 0; i < cs_gpu_batch::kSide; i++) {
+        if (b->side[i]) cudaStreamDestroy(b->side[i]);
+        if (b->ev_join[i]) cudaEventDestroy(b->ev_join[i]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->d_pops_day) cudaFree(b->d_pops_day);
+    if (b->d_ctls) cudaFree(b->d_ctls);
     for (cs_gpu_ctx* m : b->members)
         if (m && m->own_stream) {
             m->stream = m->own_stream;

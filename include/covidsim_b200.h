@@ -469,6 +469,10 @@ int cs_sur_loss_grad(cs_sur* sur, const float* x, const float* target, int n, fl
  * weights directly, as AdamW) on a batch; loss may be NULL. */
 int cs_sur_train_step(cs_sur* sur, const float* x, const float* target, int n, float lr, float weight_decay,
                       float* loss);
+/* Matrix products on tcgen05 (0, the default: tensor memory accumulators, one
+ * thread issuing the MMAs) or on mma.sync.m16n8k16 (1).  Both accumulate in FP32
+ * from the same BF16 operands; only the summation order differs. */
+int cs_sur_set_gemm(cs_sur* sur, int impl);
 
 int cs_gpu_set_interventions(cs_gpu_ctx* ctx, const cs_interventions* iv);
 /* DoPlaceClose (src/Update.cpp:1095-1258) for every place of type t in the listed
@@ -506,6 +510,11 @@ typedef struct cs_run_policy {
  * host (cs_gpu_get_counters, cs_gpu_update_probs(ctx, 0), cs_gpu_set_interventions,
  * cs_gpu_close_places). */
 int cs_gpu_run(cs_gpu_ctx* ctx, int days, const cs_run_policy* policy, cs_counters* daily);
+/* cs_gpu_run for every member of a batch at once, one graph per day: policies[k]
+ * (n entries, or NULL for none) is member k's; daily (n * days entries, may be
+ * NULL) receives member k's day d at daily[k * days + d].  Members need the same
+ * whole number of timesteps per day. */
+int cs_gpu_batch_run(cs_gpu_batch* batch, int days, const cs_run_policy* policies, cs_counters* daily);
 /* Per-cell S, L, I, R, D (each n_cells) for RecordSample (src/CovidSim.cpp:3044-3056). */
 int cs_gpu_get_cell_counts(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D);
 /* Wait for the context's stream; returns a deferred device error if any. */

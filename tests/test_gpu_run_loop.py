@@ -118,3 +118,35 @@ def test_run_loop_errors():
     # a run of no days does nothing
     assert s.backend.run_device(0, sim.run_policy(None, pop.num_place_types)).shape[0] == 0
     s.close()
+
+
+@pytest.mark.parametrize("every_step", [[False, False, False], [False, True, False]])
+def test_batch_device_loop_matches_lone_host_loops(every_step):
+    w1 = tiny_world()
+    w2 = tiny_world(n_people=12000, seed=4711)
+    a = sim.Simulation(*w1)
+    P2 = abi.cs_params.from_buffer_copy(w1[1])
+    P2.LocalBeta = w1[1].LocalBeta * 1.3
+    b = a.replica(P2)
+    c = sim.Simulation(*w2)
+    members = [a, b, c]
+    policies = [_policy(), None, sim.InterventionPolicy(threshold=2, window=5, duration=8.0, close_place_types=(1, 3))]
+    seeds = [21, 22, 23]
+    batch = sim.Batch(members)
+    got = batch.run(seeds, DAYS, n_seed=20, policy=policies, probs_every_step=every_step)
+    snaps = [snapshot(m.backend, m.pop) for m in members]
+    # the batch graph is kept and replayed by a second run
+    again = batch.run(seeds, DAYS, n_seed=20, policy=policies, probs_every_step=every_step)
+    batch.close()
+    lone = [sim.Simulation(*w1), sim.Simulation(w1[0], P2, w1[2], w1[3]), sim.Simulation(*w2)]
+    for k, (m, seed) in enumerate(zip(lone, seeds)):
+        log = _instrument(m)
+        want = m.run(seed, DAYS, n_seed=20, policy=policies[k], probs_every_step=every_step[k], device_loop=False)
+        if policies[k] is not None:
+            assert log["switch"], "member %d: the trigger never fired" % k
+        _same_series(got[k], want, "member %d" % k)
+        _same_series(again[k], want, "member %d, second run" % k)
+        _same_state(snapshot(m.backend, m.pop), snaps[k], "member %d" % k)
+        m.close()
+    for m in members:
+        m.close()

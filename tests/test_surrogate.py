@@ -74,6 +74,32 @@ def test_gradients_match_reference():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [64, 200])
+def test_tcgen05_and_mma_sync_agree(n):
+    """The two GEMM paths on the same BF16 operands: only FP32 summation order
+    differs (n = 64 pads the batch to one 128-row tile half full; 200 to 256 rows)."""
+    from covidsim_b200 import surrogate
+    flat, x, target = _case(n, 11)
+    out = {}
+    for impl in ("tcgen05", "mma.sync"):
+        net = surrogate.Surrogate(max_batch=256, params=flat.astype(np.float32))
+        net.set_gemm(impl)
+        y = net.predict(x.astype(np.float32))
+        loss, g = net.loss_grad(x.astype(np.float32), target.astype(np.float32))
+        out[impl] = (y, loss, g)
+        net.close()
+    (y1, l1, g1), (y2, l2, g2) = out["tcgen05"], out["mma.sync"]
+    assert _rel(y1, y2) < 2e-3, _rel(y1, y2)
+    assert abs(l1 - l2) <= 1e-4 * abs(l2)
+    k = 0
+    for name, (o, i) in ref.layer_shapes():
+        for part, m in (("W", o * i), ("b", o)):
+            e = _rel(g1[k:k + m], g2[k:k + m])
+            assert e < 1e-2, (name, part, e)
+            k += m
+
+
+@pytest.mark.gpu
 def test_training_reduces_loss():
     from covidsim_b200 import surrogate
     rng = np.random.default_rng(3)
