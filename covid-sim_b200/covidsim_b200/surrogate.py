@@ -230,6 +230,42 @@ class Surrogate:
             pass
 
 
+class Ensemble:
+    """n Surrogates trained on the same scenarios from different initial weights,
+    held-out splits and minibatch orders; their predictions are averaged on the
+    natural scale (expm1 of the log1p outputs), which cuts the variance a single
+    network shows between neighbouring scenarios."""
+
+    def __init__(self, n, max_batch=256, seed=0):
+        self.nets = []
+        try:
+            for k in range(n):
+                self.nets.append(Surrogate(max_batch=max_batch, seed=seed + k))
+        except Exception:
+            self.close()
+            raise
+
+    def fit(self, x_unit, y, **kw):
+        """Surrogate.fit for each member (member k splits and shuffles with seed k);
+        returns the members' epoch losses."""
+        kw.pop("seed", None)
+        return [net.fit(x_unit, y, seed=k, **kw) for k, net in enumerate(self.nets)]
+
+    def predict(self, x_unit):
+        return np.log1p(np.mean([np.expm1(net.predict(x_unit)) for net in self.nets], axis=0)).astype(np.float32)
+
+    def close(self):
+        for net in self.nets:
+            net.close()
+        self.nets = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def relative_l2(pred, ref):
     """||pred - ref|| / ||ref|| per scenario, on the natural scale (expm1 of the
     log1p outputs)."""
@@ -249,3 +285,39 @@ def he_init(seed):
         parts.append(rng.uniform(-lim, lim, size=o * i).astype(np.float32))
         parts.append(np.zeros(o, np.float32))
     return np.concatenate(parts)
+
+
+def time_training(steps=50, batch=256, sweep=100_000, impl="tcgen05", seed=0):
+    """Milliseconds per training step (batch rows, random data) and seconds to screen
+    `sweep` scenarios, on the given GEMM path."""
+    import time
+    rng = np.random.default_rng(seed)
+    x = rng.random((batch, N_PARAMS)).astype(np.float32)
+    y = rng.normal(0.0, 1.0, (batch, DAYS, len(OUTPUTS))).astype(np.float32)
+    net = Surrogate(max_batch=batch, seed=seed)
+    try:
+        net.set_gemm(impl)
+        for _ in range(3):
+            net.train_step(x, y, 1e-3, 1e-4)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            net.train_step(x, y, 1e-3, 1e-4)
+        step_ms = (time.perf_counter() - t0) / max(steps, 1) * 1e3
+        xs = rng.random((sweep, N_PARAMS)).astype(np.float32)
+        t0 = time.perf_counter()
+        net.predict(xs)
+        screen_s = time.perf_counter() - t0
+    finally:
+        net.close()
+    return step_ms, screen_s
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="time the surrogate's training step and screening")
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--sweep", type=int, default=100_000)
+    ap.add_argument("--gemm", default="tcgen05", choices=["tcgen05", "mma.sync"])
+    a = ap.parse_args()
+    ms, sc = time_training(a.steps, sweep=a.sweep, impl=a.gemm)
+    print("%s: %.3f ms per training step (256 rows), %.3f s to screen %d scenarios" % (a.gemm, ms, sc, a.sweep))

@@ -211,15 +211,38 @@ __device__ __forceinline__ void stage_rows(unsigned char* dst, const bf16* __res
     }
 }
 
+// The A operand of a convolution read straight from its input H [Bn*T, kCh] (no
+// column matrix): row m = b*2T + t, column k = tap*Cin + c holds
+// H[b*T + (t+tap-2)/2, c] when 0 <= t+tap-2 < 2T, else zero (as k_im2col_up).  Cin is
+// a multiple of 8, so a 16-byte chunk never straddles two taps.
+__device__ __forceinline__ void stage_conv_rows(unsigned char* dst, const bf16* __restrict__ H, int T, int Cin, int r0,
+                                                int nrows, int k0)
+{
+    for (int i = threadIdx.x; i < BM * 8; i += blockDim.x) {
+        const int r = i >> 3, j = i & 7;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        const int m = r0 + r, k = k0 + j * 8;
+        const int tap = k / Cin;
+        if (m < nrows && tap < kTap) {
+            const int b = m / (2 * T), t = m - b * 2 * T, u = t + tap - kTap / 2;
+            if (u >= 0 && u < 2 * T)
+                v = *reinterpret_cast<const uint4*>(H + ((size_t)b * T + (u >> 1)) * kCh + (k - tap * Cin));
+        }
+        *reinterpret_cast<uint4*>(dst + r * 128 + ((j ^ (r & 7)) << 4)) = v;
+    }
+}
+
 }  // namespace tc
 
 // C[M,N] = A[M,K] B[N,K]^T (+ bias) (ReLU) on tcgen05; N a multiple of BN, K of 64;
 // split K as k_gemm_nt (gridDim.z slices of kchunk, partial products at C + z * cstride).
+// With H set, A is the column matrix of a convolution of H (hT time points, hCin
+// channels), generated while staging (not split).
 template <int BN>
 __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, int lda, const bf16* __restrict__ B, int ldb,
                                                  float* __restrict__ C, int ldc, bf16* __restrict__ Cb, int ldcb,
                                                  const float* __restrict__ bias, int relu, int M, int K, int kchunk,
-                                                 size_t cstride, int* err)
+                                                 size_t cstride, int* err, const bf16* __restrict__ H, int hT, int hCin)
 {
     using namespace tc;
     extern __shared__ unsigned char smem_raw[];
@@ -261,7 +284,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, int
             __syncthreads();
             if (!s_ok) break;
         }
-        stage_rows(As + st * BM * 128, A, lda, bm, M, kc * BK, BM);
+        if (H) stage_conv_rows(As + st * BM * 128, H, hT, hCin, bm, M, kc * BK);
+        else stage_rows(As + st * BM * 128, A, lda, bm, M, kc * BK, BM);
         stage_rows(Bs + st * BN * 128, B, ldb, bn, 1 << 30, kc * BK, BN);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -306,14 +330,20 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, int
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tm), "r"(BN));
 }
 
-// C[r, c] = sum over the slices z, in ascending order, of part[z][r, c] ([M, N] each).
-__global__ void k_splitk_reduce(const float* __restrict__ part, int nsplit, int M, int N, float* __restrict__ C, int ldc)
+// C[r, c] = sum over the slices z, in ascending order, of part[z][r, c] ([M, N] each),
+// then the product's epilogue (bias, ReLU, FP32 and/or BF16 stores).
+__global__ void k_splitk_reduce(const float* __restrict__ part, int nsplit, int M, int N, float* __restrict__ C, int ldc,
+                                bf16* __restrict__ Cb, int ldcb, const float* __restrict__ bias, int relu)
 {
     const size_t MN = (size_t)M * N;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < MN; e += (size_t)gridDim.x * blockDim.x) {
         float acc = 0.f;
         for (int z = 0; z < nsplit; z++) acc += part[z * MN + e];
-        C[(e / N) * ldc + e % N] = acc;
+        const size_t r = e / N, c = e % N;
+        if (bias) acc += bias[c];
+        if (relu) acc = fmaxf(acc, 0.f);
+        if (C) C[r * ldc + c] = acc;
+        if (Cb) Cb[r * ldcb + c] = __float2bfloat16_rn(acc);
     }
 }
 
@@ -345,6 +375,28 @@ __global__ void k_im2col_up(const bf16* __restrict__ H, int Bn, int T, int Cin, 
         }
         cols[e] = v;
     }
+}
+
+// The transposed column matrix, colsT[k, m] = cols[m, k] of k_im2col_up, for m < M
+// (= Bn*2T) and k < ldk (columns past kTap*Cin zero), through a 32 x 32 shared tile
+// so that both the reads of H and the writes are coalesced.
+__global__ void k_im2colT_up(const bf16* __restrict__ H, int T, int Cin, bf16* __restrict__ colsT, int M)
+{
+    __shared__ bf16 tile[32][34];
+    const int m0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+        const int m = m0 + q, k = k0 + threadIdx.x;
+        bf16 v = __float2bfloat16(0.f);
+        const int tap = k / Cin;
+        if (tap < kTap) {
+            const int b = m / (2 * T), t = m - b * 2 * T, u = t + tap - kTap / 2;
+            if (u >= 0 && u < 2 * T) v = H[((size_t)b * T + (u >> 1)) * kCh + (k - tap * Cin)];
+        }
+        tile[q][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int q = threadIdx.y; q < 32; q += blockDim.y)
+        colsT[(size_t)(k0 + q) * M + m0 + threadIdx.x] = tile[threadIdx.x][q];
 }
 
 // Adjoint of k_im2col_up, fused with the ReLU mask of H: for channel c < Cin,
@@ -387,22 +439,41 @@ __global__ void k_relu_back(const float* __restrict__ dh, const bf16* __restrict
 
 // Column sums of dz [rows, ld] in a fixed order: part[chunk, col] over row chunks
 // of 256, then the chunks in ascending order.
+// Column sums of dz [rows, ld] in a fixed order.  Block (x, y) covers 32 columns
+// and row chunk y of kColChunk rows; its 8 row lanes each sum every 8th row, then
+// a shared-memory tree adds the lanes: part[y, col].  The final pass adds the
+// chunks the same way.
+constexpr int kColChunk = 2048;
+__device__ __forceinline__ float lanes_tree(float v, float (*sh)[33])
+{
+    sh[threadIdx.y][threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 4; o > 0; o >>= 1) {
+        if ((int)threadIdx.y < o) sh[threadIdx.y][threadIdx.x] += sh[threadIdx.y + o][threadIdx.x];
+        __syncthreads();
+    }
+    return sh[0][threadIdx.x];
+}
 __global__ void k_colsum_part(const float* __restrict__ dz, int rows, int ld, float* __restrict__ part)
 {
-    int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ld) return;
-    int r0 = blockIdx.y * 256, r1 = min(rows, r0 + 256);
-    float s = 0.f;
-    for (int r = r0; r < r1; r++) s += dz[(size_t)r * ld + col];
-    part[(size_t)blockIdx.y * ld + col] = s;
+    __shared__ float sh[8][33];
+    const int col = blockIdx.x * 32 + threadIdx.x;
+    const int r0 = blockIdx.y * kColChunk, r1 = min(rows, r0 + kColChunk);
+    float v = 0.f;
+    if (col < ld)
+        for (int r = r0 + threadIdx.y; r < r1; r += 8) v += dz[(size_t)r * ld + col];
+    v = lanes_tree(v, sh);
+    if (threadIdx.y == 0 && col < ld) part[(size_t)blockIdx.y * ld + col] = v;
 }
 __global__ void k_colsum_final(const float* __restrict__ part, int nchunks, int ld, float* __restrict__ out)
 {
-    int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ld) return;
-    float s = 0.f;
-    for (int q = 0; q < nchunks; q++) s += part[(size_t)q * ld + col];
-    out[col] = s;
+    __shared__ float sh[8][33];
+    const int col = blockIdx.x * 32 + threadIdx.x;
+    float v = 0.f;
+    if (col < ld)
+        for (int q = threadIdx.y; q < nchunks; q += 8) v += part[(size_t)q * ld + col];
+    v = lanes_tree(v, sh);
+    if (threadIdx.y == 0 && col < ld) out[col] = v;
 }
 
 // Loss terms and the output gradient: y is [B*368, 64] (channels < 4 used), target
@@ -445,9 +516,16 @@ __global__ void k_sum_part(const float* __restrict__ v, size_t n, double* __rest
 }
 __global__ void k_sum_final(const double* __restrict__ part, int n, double* __restrict__ out)
 {
+    __shared__ double sh[256];
     double a = 0.0;
-    for (int i = 0; i < n; i++) a += part[i];
-    *out = a;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a += part[i];
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
 }
 
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v, const float* __restrict__ g,
@@ -592,7 +670,7 @@ static int gemm_launch(cs_sur* s, const bf16* A, int lda, const bf16* B, int ldb
     if (s->gemm_impl == 0 && K % 64 == 0 && kchunk % 64 == 0) {
         dim3 grid(N / 64, (M + tc::BM - 1) / tc::BM, nsplit);
         k_gemm_tc<64><<<grid, 128, tc::smem_bytes(64), s->stream>>>(A, lda, B, ldb, C, ldc, Cb, ldcb, bias, relu, M, K,
-                                                                    kchunk, cstride, s->d_err);
+                                                                    kchunk, cstride, s->d_err, nullptr, 0, 0);
     } else {
         dim3 grid(N / 64, M / 64, nsplit);
         sur::k_gemm_nt<<<grid, 128, 0, s->stream>>>(A, lda, B, ldb, C, ldc, Cb, ldcb, bias, relu, K, kchunk, cstride);
@@ -601,32 +679,35 @@ static int gemm_launch(cs_sur* s, const bf16* A, int lda, const bf16* B, int ldb
     return CS_OK;
 }
 
+// C = A B^T (+ bias) (ReLU).  A product with few output tiles and a long K (the
+// convolutions' weight gradients, K = batch x time points; the linear layers at
+// batch sizes of a few hundred) is split along K so that about two blocks per SM
+// run; the slices' partial products are then summed in a fixed order and the
+// epilogue applied.
+constexpr int kMaxSplit = 64;
+
 static int gemm(cs_sur* s, const bf16* A, int lda, const bf16* B, int ldb, float* C, int ldc, bf16* Cb, int ldcb,
                 const float* bias, int relu, int M, int N, int K)
 {
     if (M % 64 || N % 64 || K % 32) return sur_err(s, CS_E_ARG, "gemm shape %d x %d x %d not padded", M, N, K);
+    const int tiles = (s->gemm_impl == 0 ? (M + tc::BM - 1) / tc::BM : M / 64) * (N / 64);
+    int nsplit = tiles < 74 ? std::min(kMaxSplit, std::max(1, std::min(K / 128, 296 / tiles))) : 1;
+    if (nsplit > 1 && K % 64 == 0) {
+        const int kchunk = ((K + nsplit - 1) / nsplit + 63) / 64 * 64;
+        nsplit = (K + kchunk - 1) / kchunk;
+        if (nsplit > 1 && (size_t)nsplit * M * N <= s->kpart_n) {
+            int r = gemm_launch(s, A, lda, B, ldb, s->kpart, N, nullptr, 0, nullptr, 0, M, N, K, nsplit, kchunk,
+                                (size_t)M * N);
+            if (r) return r;
+            const int rg = (int)std::min<size_t>(1184, ((size_t)M * N + 255) / 256);
+            sur::k_splitk_reduce<<<rg, 256, 0, s->stream>>>(s->kpart, nsplit, M, N, C, ldc, Cb, ldcb, bias, relu);
+            SCK(cudaGetLastError());
+            return CS_OK;
+        }
+    }
     return gemm_launch(s, A, lda, B, ldb, C, ldc, Cb, ldcb, bias, relu, M, N, K, 1, K, 0);
 }
 
-// C = A B^T for a product with few output tiles and a long K (the convolutions'
-// weight gradients, K = batch x time points): K is split into slices so that about
-// two blocks per SM run, and the slices' partial products are summed in a fixed order.
-constexpr int kMaxSplit = 64;
-
-static int gemm_splitk(cs_sur* s, const bf16* A, int lda, const bf16* B, int ldb, float* C, int ldc, int M, int N, int K)
-{
-    if (M % 64 || N % 64 || K % 32) return sur_err(s, CS_E_ARG, "gemm shape %d x %d x %d not padded", M, N, K);
-    const int tiles = (M / 64) * (N / 64);
-    int nsplit = std::min(kMaxSplit, std::max(1, std::min((K + 255) / 256, 296 / tiles)));
-    if (nsplit == 1 || (size_t)M * N * kMaxSplit > s->kpart_n) return gemm(s, A, lda, B, ldb, C, ldc, nullptr, 0, nullptr, 0, M, N, K);
-    const int kchunk = ((K + nsplit - 1) / nsplit + 63) / 64 * 64;
-    nsplit = (K + kchunk - 1) / kchunk;
-    int r = gemm_launch(s, A, lda, B, ldb, s->kpart, N, nullptr, 0, nullptr, 0, M, N, K, nsplit, kchunk, (size_t)M * N);
-    if (r) return r;
-    sur::k_splitk_reduce<<<std::min(1184, (M * N + 255) / 256), 256, 0, s->stream>>>(s->kpart, nsplit, M, N, C, ldc);
-    SCK(cudaGetLastError());
-    return CS_OK;
-}
 
 static int transpose(cs_sur* s, const bf16* in, int ldi, bf16* out, int ldo, int R, int Cc)
 {
@@ -695,7 +776,7 @@ int cs_sur_create(int max_batch, int device, cs_sur** out)
     {
         size_t mn = 0;
         for (int i = 0; i < 3; i++) mn = std::max(mn, (size_t)s->L[6 + i].outP * s->L[6 + i].inP);
-        s->kpart_n = mn * kMaxSplit;
+        s->kpart_n = std::max(mn * kMaxSplit, (size_t)4 << 20);
         SA(s->kpart, s->kpart_n);
     }
     SA(s->lpart, (size_t)kLossBlocks); SA(s->lsum, (size_t)1); SA(s->d_err, (size_t)1);
@@ -768,22 +849,33 @@ static int forward(cs_sur* s, int Bp)
     int T = kT0;
     for (int ci = 0; ci < 3; ci++) {
         const Layer& l = s->L[6 + ci];
-        sur::k_im2col_up<<<1184, 256, 0, s->stream>>>(s->act[6 + ci], Bp, T, l.cin, s->cols[ci], l.inP);
-        SCK(cudaGetLastError());
-        T *= 2;
         const bool last = ci == 2;
-        if ((r = gemm(s, s->cols[ci], l.inP, s->wb + l.wofs, l.inP, last ? s->yout : nullptr, kCh,
-                      last ? nullptr : s->act[7 + ci], kCh, s->w + l.bofs, l.relu ? 1 : 0, Bp * T, l.outP, l.inP))) return r;
+        float* C = last ? s->yout : nullptr;
+        bf16* Cb = last ? nullptr : s->act[7 + ci];
+        const int M = Bp * 2 * T;
+        if (s->gemm_impl == 0) {   // the column matrix is generated while staging
+            dim3 grid(l.outP / 64, (M + tc::BM - 1) / tc::BM, 1);
+            k_gemm_tc<64><<<grid, 128, tc::smem_bytes(64), s->stream>>>(nullptr, 0, s->wb + l.wofs, l.inP, C, kCh, Cb, kCh,
+                                                                        s->w + l.bofs, l.relu ? 1 : 0, M, l.inP, l.inP, 0,
+                                                                        s->d_err, s->act[6 + ci], T, l.cin);
+            SCK(cudaGetLastError());
+        } else {
+            sur::k_im2col_up<<<1184, 256, 0, s->stream>>>(s->act[6 + ci], Bp, T, l.cin, s->cols[ci], l.inP);
+            SCK(cudaGetLastError());
+            if ((r = gemm(s, s->cols[ci], l.inP, s->wb + l.wofs, l.inP, C, kCh, Cb, kCh, s->w + l.bofs, l.relu ? 1 : 0,
+                          M, l.outP, l.inP))) return r;
+        }
+        T *= 2;
     }
     return CS_OK;
 }
 
 static int colsum(cs_sur* s, const float* dz, int rows, int ld, float* out)
 {
-    int nch = (rows + 255) / 256;
-    dim3 g1((ld + 127) / 128, nch);
-    sur::k_colsum_part<<<g1, 128, 0, s->stream>>>(dz, rows, ld, s->part);
-    sur::k_colsum_final<<<(ld + 127) / 128, 128, 0, s->stream>>>(s->part, nch, ld, out);
+    const int nch = (rows + kColChunk - 1) / kColChunk;
+    const dim3 blk(32, 8);
+    sur::k_colsum_part<<<dim3((ld + 31) / 32, nch), blk, 0, s->stream>>>(dz, rows, ld, s->part);
+    sur::k_colsum_final<<<(ld + 31) / 32, blk, 0, s->stream>>>(s->part, nch, ld, out);
     SCK(cudaGetLastError());
     return CS_OK;
 }
@@ -805,8 +897,12 @@ static int backward(cs_sur* s, int Bp)
         const int M = Bp * T;
         // dW = dz^T cols: A = dz^T [outP, M], B = cols^T [inP, M]
         if ((r = transpose(s, s->dzb, kCh, s->dzT, M, M, l.outP))) return r;
-        if ((r = transpose(s, s->cols[ci], l.inP, s->colsT, M, M, l.inP))) return r;
-        if ((r = gemm_splitk(s, s->dzT, M, s->colsT, M, s->g + l.wofs, l.inP, l.outP, l.inP, M))) return r;
+        {   // the transposed column matrix of this convolution's input, from the input itself
+            dim3 grid(l.inP / 32, M / 32), blk(32, 8);
+            sur::k_im2colT_up<<<grid, blk, 0, s->stream>>>(s->act[6 + ci], T / 2, l.cin, s->colsT, M);
+            SCK(cudaGetLastError());
+        }
+        if ((r = gemm(s, s->dzT, M, s->colsT, M, s->g + l.wofs, l.inP, nullptr, 0, nullptr, 0, l.outP, l.inP, M))) return r;
         if ((r = colsum(s, s->dz, M, kCh, s->g + l.bofs))) return r;
         // dcols = dz W: A = dz [M, outP], B = W^T [inP, outP]
         if ((r = transpose(s, s->wb + l.wofs, l.inP, s->wT, l.outP, l.outP, l.inP))) return r;
@@ -868,7 +964,7 @@ static int loss_grad(cs_sur* s, const float* x, const float* target, int n, floa
     if (loss) {
         const size_t nsq = (size_t)n * kTOut * kNOut;
         sur::k_sum_part<<<kLossBlocks, 256, 0, s->stream>>>(s->sq, nsq, s->lpart);
-        sur::k_sum_final<<<1, 1, 0, s->stream>>>(s->lpart, kLossBlocks, s->lsum);
+        sur::k_sum_final<<<1, 256, 0, s->stream>>>(s->lpart, kLossBlocks, s->lsum);
         SCK(cudaGetLastError());
         double acc = 0.0;
         SCK(cudaMemcpyAsync(&acc, s->lsum, sizeof(double), cudaMemcpyDeviceToHost, s->stream));

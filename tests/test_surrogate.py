@@ -100,6 +100,19 @@ def test_tcgen05_and_mma_sync_agree(n):
 
 
 @pytest.mark.gpu
+def test_ensemble_averages_members_on_the_natural_scale():
+    from covidsim_b200 import surrogate
+    x = np.random.default_rng(4).random((30, ref.N_IN)).astype(np.float32)
+    ens = surrogate.Ensemble(3, max_batch=64, seed=7)
+    members = [net.predict(x) for net in ens.nets]
+    want = np.log1p(np.mean([np.expm1(p) for p in members], axis=0))
+    assert np.allclose(ens.predict(x), want, rtol=1e-6, atol=1e-6)
+    # distinct initial weights give distinct members
+    assert not np.array_equal(members[0], members[1])
+    ens.close()
+
+
+@pytest.mark.gpu
 def test_training_reduces_loss():
     from covidsim_b200 import surrogate
     rng = np.random.default_rng(3)
