@@ -48,6 +48,9 @@ WORKLOADS = {
     # a short case whose sweeps run at epidemic-peak load after a few hundred
     # launches: the profiling case for the spatial and place kernels
     "c1_peak": ("c1", 8, False, "10M people, 600x600 cells, 500k initial infections, 8 d", 500000),
+    # 66 M people, 1500x1500 cells, 30 urban blobs, 100 admin units whose triggers
+    # fire on their own admissions (staggered)
+    "c3": ("c3", 365, "adunit", "66M people, 1500x1500 cells, 100 admin units, staggered triggers, 365 d", 100),
 }
 METRIC = "person-steps/s"
 
@@ -215,7 +218,8 @@ def run_ours(args):
     P.LocalBeta = beta
     s = sim.Simulation(pop, P, lk, hr, device=local)
     be = s.backend
-    policy = sim.InterventionPolicy() if with_iv else None
+    policy = (sim.InterventionPolicy(per_adunit=True) if with_iv == "adunit" else
+              sim.InterventionPolicy() if with_iv else None)
     steps_per_run = int(days * P.TimeStepsPerDay)
     base_seed = replica_seed(rank)
 

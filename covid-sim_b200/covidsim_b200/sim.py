@@ -255,6 +255,10 @@ class InterventionPolicy:
     social_distancing: bool = True
     case_isolation: bool = True
     household_quarantine: bool = True
+    # one trigger per admin unit (the reference's DoAdminTriggers) on the unit's own
+    # admissions, firing above the threshold and switching that unit's windows,
+    # microcells and places
+    per_adunit: bool = False
 
 
 def run_policy(policy, n_place_types, probs_every_step=False):
@@ -269,6 +273,7 @@ def run_policy(policy, n_place_types, probs_every_step=False):
         p.household_quarantine = int(bool(policy.household_quarantine))
         p.social_distancing = int(bool(policy.social_distancing))
         p.close_place_types = sum(1 << pt for pt in set(policy.close_place_types) if 0 <= pt < n_place_types)
+        p.per_adunit = int(bool(policy.per_adunit))
         p.duration = float(policy.duration)
     return p
 
@@ -372,6 +377,14 @@ class _RunState:
         self.iv_on_until = -1.0
         self.iv_started = False
         self.socd = np.zeros(sim.pop.n_mcells, dtype=np.uint8)
+        if policy is not None and policy.per_adunit:
+            na = min(max(sim.pop.n_adunits, 1), abi.CS_MAX_ADUNITS)
+            self.ad_started = np.zeros(na, bool)
+            self.ad_on_until = np.full(na, -1.0)
+            self.ad_ci = np.full(max(sim.pop.n_adunits, 1), 1e10)
+            self.ad_hq = np.full(max(sim.pop.n_adunits, 1), 1e10)
+            self.ad_cum = []
+            self.ad_mcells = [np.nonzero(sim.pop.mcell_adunit == a)[0].astype(np.int32) for a in range(na)]
 
     def after_step(self, step):
         day_end = (step + 1) % self.spd == 0 or step == self.nsteps - 1
@@ -390,7 +403,9 @@ class _RunState:
             be.update_probs(0)
         if not day_end:
             return
-        if policy is not None:
+        if policy is not None and policy.per_adunit:
+            self._per_adunit(c, t + P.ModelTimeStep)
+        elif policy is not None:
             day = len(series["cumCritical"])
             w = policy.window
             recent = series["cumCritical"][-1] - (series["cumCritical"][-w - 1] if day > w else 0)
@@ -404,6 +419,52 @@ class _RunState:
                 sim._switch_interventions(tn, policy, False, self.socd)
         if self.callback:
             self.callback(step, c)
+
+    def _per_adunit(self, c, tn):
+        """One trigger per admin unit on its own critical-care admissions over the
+        window (src/CovidSim.cpp:3442-3446 trigDC_adunit with ICU triggers), firing
+        when they exceed the threshold (src/Sweep.cpp:1478-1482); a switch sets that
+        unit's windows and microcells and closes its places."""
+        sim, policy, P = self.sim, self.policy, self.sim.params
+        na = len(self.ad_started)
+        cum = np.array(c.cumCritical_adunit[:na], dtype=np.int64)
+        self.ad_cum.append(cum)
+        w = policy.window
+        recent = cum - (self.ad_cum[-w - 1] if len(self.ad_cum) > w else 0)
+        switched, closing = False, []
+        for a in range(na):
+            sw = -1
+            if not self.ad_started[a] and recent[a] > policy.threshold:
+                self.ad_started[a] = True
+                self.ad_on_until[a] = tn + policy.duration
+                sw = 1
+            elif self.ad_started[a] and self.ad_on_until[a] > 0 and tn >= self.ad_on_until[a]:
+                self.ad_on_until[a] = -1.0
+                sw = 0
+            if sw < 0:
+                continue
+            switched = True
+            self.ad_ci[a] = tn if (sw and policy.case_isolation) else 1e10
+            self.ad_hq[a] = tn if (sw and policy.household_quarantine) else 1e10
+            self.socd[self.ad_mcells[a]] = abi.CS_TREAT_TREATED if (sw and policy.social_distancing) else abi.CS_TREAT_UNTREATED
+            if sw:
+                closing.append(a)
+        if not switched:
+            return
+        iv = abi.cs_interventions()
+        iv.CaseIsolationTimeStart = iv.HQuarantineTimeStart = 1e10
+        iv.CaseIsolationPolicyDuration = iv.HQuarantinePolicyDuration = policy.duration
+        iv.mcell_socdist = self.socd.ctypes.data
+        iv.mcell_moverest = None
+        iv.adunit_CaseIsolationTimeStart = self.ad_ci.ctypes.data
+        iv.adunit_HQuarantineTimeStart = self.ad_hq.ctypes.data
+        sim.backend.set_interventions(iv)
+        ts = int(tn * P.TimeStepsPerDay)
+        stop = min(65533, ts + int(policy.duration * P.TimeStepsPerDay))
+        for a in closing:
+            for pt in policy.close_place_types:
+                if pt < sim.pop.num_place_types:
+                    sim.backend.close_places(pt, self.ad_mcells[a], ts, stop)
 
     def result(self):
         return {k: np.asarray(v) for k, v in self.series.items()}

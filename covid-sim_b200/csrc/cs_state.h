@@ -77,9 +77,12 @@ struct DevPlaces {
     float* prob_close;
 };
 
-// Intervention windows set by the host between steps.
+// Intervention windows: the policy durations, and each admin unit's start times
+// (AdUnits[a].CaseIsolationTimeStart and .HQuarantineTimeStart), NA entries each.
 struct DevIv {
-    double ci_start, ci_dur, hq_start, hq_dur;
+    double ci_dur, hq_dur;
+    double* ci_start;
+    double* hq_start;
 };
 
 // Scalars of the current timestep, written on the device by k_set_step so that a
@@ -96,6 +99,7 @@ enum : uint8_t { kStepLtoI = 1, kStepItoRD = 2 };
 // Everything the kernels need, passed by value.
 struct DevPop {
     int32_t N, NH, NC, NM, NPT, NB, nbx, nby, bs;
+    int32_t NA;                // admin units with intervention windows (at least 1)
     const cs_params* P;
     PersonHot* hot;
     const PersonLinks* links;  // [N]

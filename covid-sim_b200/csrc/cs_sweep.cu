@@ -190,6 +190,7 @@ struct cs_gpu_ctx {
     std::vector<void*> allocs;      // every cudaMalloc of the context
     cs_params* dP = nullptr;
     DevIv* dIv = nullptr;
+    double *iv_ci = nullptr, *iv_hq = nullptr;   // the windows' per-admin-unit start times
     cs_counters* dC = nullptr;
     int32_t* d_seed_list = nullptr;
     unsigned long long* d_seed = nullptr;   // device copy of seed (DevPop::seed_src)
@@ -1297,8 +1298,10 @@ __device__ void do_detected_case(const DevPop& d, const cs_params& P, const DevI
 {
     int ad = d.mcell_adunit[h.mcell];
     if (ad >= 0 && ad < CS_MAX_ADUNITS) cnt_add(CSB_STAGED(cumDC_adunit[ad]), 1);
-    if (P.DoHouseholds && t >= iv.hq_start && t < iv.hq_start + iv.hq_dur) flag_household(d, h.hh, 4);
-    if (t >= iv.ci_start && t < iv.ci_start + iv.ci_dur) {
+    const int aw = (ad >= 0 && ad < d.NA) ? ad : 0;   // the person's admin unit's windows
+    const double hq0 = iv.hq_start[aw], ci0 = iv.ci_start[aw];
+    if (P.DoHouseholds && t >= hq0 && t < hq0 + iv.hq_dur) flag_household(d, h.hh, 4);
+    if (t >= ci0 && t < ci0 + iv.ci_dur) {
         Stream s(seed, CS_RNG_DETECTED, (uint32_t)ts, (uint32_t)p, 0);
         if ((P.CaseIsolationProp == 1) || (s.next() < P.CaseIsolationProp)) {
             h.isolation_start = (uint16_t)ts;
@@ -1583,6 +1586,13 @@ __global__ void k_seed_claims(DevPop d, const int32_t* list, int n)
 }
 
 // ============================================================ interventions
+// No intervention windows: every admin unit's start times at 1e10, durations 0.
+__global__ void k_iv_reset(DevIv* iv, int na)
+{
+    for (int a = threadIdx.x; a < na; a += blockDim.x) iv->ci_start[a] = iv->hq_start[a] = 1e10;
+    if (threadIdx.x == 0) iv->ci_dur = iv->hq_dur = 0.0;
+}
+
 // State of the device-side run loop (cs_gpu_run): its policy, the host loop's
 // variables between timesteps (src/CovidSim.cpp:1517-1526 PreviousProportionSusceptible,
 // the ICU trigger's switch state) and what the day's logic decided for the
@@ -1595,37 +1605,51 @@ struct DayCtl {
     int32_t update;             // UpdateProbs runs (gate of its kernels)
     int32_t socd_write;         // every microcell's social-distancing flag becomes socd_value
     int32_t close;              // places of the policy's types close over [close_start, close_stop)
-    uint16_t close_start, close_stop;
+    uint16_t close_start, close_stop;   // per admin unit: the envelope of the units' windows
     uint8_t socd_value, pad[3];
+    // per admin unit triggers (pol.per_adunit)
+    int32_t a_started[CS_MAX_ADUNITS];
+    double a_on_until[CS_MAX_ADUNITS];
+    int8_t a_switch[CS_MAX_ADUNITS];    // this day: -1 none, 1 on, 0 off
+    uint16_t a_close_start[CS_MAX_ADUNITS], a_close_stop[CS_MAX_ADUNITS];
 };
 
 __device__ void k_close_places_body(const DevPop& d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop,
                                     const DayCtl* ctl)
 {
-    if (ctl) {   // a day graph's closure: only on the day the trigger fired, window from the device
+    if (ctl) {   // a day graph's closure: only on the day a trigger fired, window from the device
         if (!ctl->close || !((ctl->pol.close_place_types >> pt) & 1u)) return;
         start = ctl->close_start;
         stop = ctl->close_stop;
     }
+    const bool per_unit = ctl && ctl->pol.per_adunit;
     const cs_params& P = *d.P;
     DevPlaces pl = d.pl[pt];
     // every place closed at ts afterwards has close_start >= start and close_end <= stop
-    if (blockIdx.x == 0 && threadIdx.x == 0 && start < stop) {
-        atomicMin(d.close_window, (int32_t)start);
-        atomicMax(d.close_window + 1, (int32_t)stop);
+    const uint16_t start0 = start, stop0 = stop;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && start0 < stop0) {
+        atomicMin(d.close_window, (int32_t)start0);
+        atomicMax(d.close_window + 1, (int32_t)stop0);
     }
     for (int l = blockIdx.x; l < pl.n; l += gridDim.x) {
         if (sel && !sel[pl.mcell[l]]) continue;
+        uint16_t ws = start0, we = stop0;   // this place's closure window
+        if (per_unit) {   // the window of the place's admin unit, if it switched on today
+            const int a = d.mcell_adunit[pl.mcell[l]];
+            if (a < 0 || a >= CS_MAX_ADUNITS || ctl->a_switch[a] != 1) continue;
+            ws = ctl->a_close_start[a];
+            we = ctl->a_close_stop[a];
+        }
         __shared__ int do_members;
         if (threadIdx.x == 0) {
             do_members = 0;
-            if (pl.close_end[l] < stop) {
+            if (pl.close_end[l] < we) {
                 if (pl.prob_close[l] >= P.Efficacies[CS_NPI_PLACE_CLOSURE][pt]) {
-                    if (pl.close_start[l] > start) pl.close_start[l] = start;
-                    pl.close_end[l] = stop;
+                    if (pl.close_start[l] > ws) pl.close_start[l] = ws;
+                    pl.close_end[l] = we;
                     do_members = P.DoRealSymptWithdrawal;
                 } else
-                    pl.close_start[l] = pl.close_end[l] = stop;
+                    pl.close_start[l] = pl.close_end[l] = we;
             }
         }
         __syncthreads();
@@ -1634,8 +1658,8 @@ __device__ void k_close_places_body(const DevPop& d, int pt, const uint8_t* sel,
                 int w = pl.members[k];
                 // a person can be a member of only one place per type: no race
                 PersonHot* hw = d.hot + w;
-                if (hw->absent_start > start) hw->absent_start = start;
-                if (hw->absent_stop < stop) hw->absent_stop = stop;
+                if (hw->absent_start > ws) hw->absent_start = ws;
+                if (hw->absent_stop < we) hw->absent_stop = we;
             }
         __syncthreads();
     }
@@ -1676,52 +1700,108 @@ __global__ void k_probs_check_multi(const DevPop* __restrict__ pops, DayCtl* con
 // ICU trigger (src/CovidSim.cpp:3150-3159 with global thresholds) switching case
 // isolation, household quarantine, social distancing and place closure on for
 // pol.duration days, then off.  The switch takes effect from the next timestep.
+// One trigger (the global one, or one admin unit's) at the end of a day, as the host
+// loop decides it: 1 switches on (for pol.duration days), 0 switches off, -1 nothing.
+// A global trigger fires at recent >= threshold (src/Sweep.cpp:1476), an admin unit's
+// at recent > threshold (src/Sweep.cpp:1478-1482).
+__device__ __forceinline__ int trigger_step(const cs_run_policy& pol, long long recent, double tn, int32_t& started,
+                                            double& on_until, bool strict)
+{
+    if (!started && (strict ? recent > pol.icu_threshold : recent >= pol.icu_threshold)) {
+        started = 1;
+        on_until = tn + pol.duration;
+        return 1;
+    }
+    if (started && on_until > 0 && tn >= on_until) {
+        on_until = -1.0;
+        return 0;
+    }
+    return -1;
+}
+
 __device__ void k_day_logic_body(const DevPop& d, DayCtl* ctl, const int32_t* clock, DevIv* iv)
 {
+    __shared__ int s_sw, s_any, s_cmin, s_cmax;
     const int day = ctl->day;
     {
         const unsigned long long* src = (const unsigned long long*)d.C;
         unsigned long long* dst = (unsigned long long*)(ctl->series + day);
         for (int k = threadIdx.x; k < (int)(sizeof(cs_counters) / 8); k += blockDim.x) dst[k] = src[k];
     }
-    if (threadIdx.x) return;
     const cs_params& P = *d.P;
     const cs_run_policy& pol = ctl->pol;
-    ctl->socd_write = 0;
-    ctl->close = 0;
-    if (pol.icu_trigger) {
-        const int w = pol.icu_window;
-        const long long recent = (long long)d.C->cumCritical - (day + 1 > w ? (long long)ctl->series[day - w].cumCritical : 0ll);
-        const double t = (double)(*clock - 1) * P.ModelTimeStep;   // the day's last timestep
-        const double tn = t + P.ModelTimeStep;
-        int sw = -1;
-        if (!ctl->started && recent >= pol.icu_threshold) {
-            ctl->started = 1;
-            ctl->on_until = tn + pol.duration;
-            sw = 1;
-        } else if (ctl->started && ctl->on_until > 0 && tn >= ctl->on_until) {
-            ctl->on_until = -1.0;
-            sw = 0;
+    const double t = (double)(*clock - 1) * P.ModelTimeStep;   // the day's last timestep
+    const double tn = t + P.ModelTimeStep;
+    const int w = pol.icu_window;
+    const cs_counters* past = day + 1 > w ? ctl->series + (day - w) : nullptr;
+    const int ts = (int)(tn * P.TimeStepsPerDay);
+    const int stop = min(65533, ts + (int)(pol.duration * P.TimeStepsPerDay));
+    if (threadIdx.x == 0) {
+        ctl->socd_write = 0;
+        ctl->close = 0;
+        s_sw = -1;
+        s_any = 0;
+        s_cmin = INT_MAX;
+        s_cmax = 0;
+        if (pol.icu_trigger && !pol.per_adunit) {
+            const long long recent = (long long)d.C->cumCritical - (past ? (long long)past->cumCritical : 0ll);
+            s_sw = trigger_step(pol, recent, tn, ctl->started, ctl->on_until, false);
         }
-        if (sw >= 0) {
-            DevIv v;
-            v.ci_start = (sw && pol.case_isolation) ? tn : 1e10;
-            v.ci_dur = pol.duration;
-            v.hq_start = (sw && pol.household_quarantine) ? tn : 1e10;
-            v.hq_dur = pol.duration;
-            *iv = v;
+    }
+    __syncthreads();
+    if (pol.icu_trigger && !pol.per_adunit && s_sw >= 0) {   // every admin unit's windows
+        const int sw = s_sw;
+        for (int a = threadIdx.x; a < d.NA; a += blockDim.x) {
+            iv->ci_start[a] = (sw && pol.case_isolation) ? tn : 1e10;
+            iv->hq_start[a] = (sw && pol.household_quarantine) ? tn : 1e10;
+        }
+        if (threadIdx.x == 0) {
+            iv->ci_dur = iv->hq_dur = pol.duration;
             ctl->socd_write = 1;
             ctl->socd_value = (sw && pol.social_distancing) ? CS_TREAT_TREATED : CS_TREAT_UNTREATED;
             if (sw) {
-                const int ts = (int)(tn * P.TimeStepsPerDay);
-                const int stop = min(65533, ts + (int)(pol.duration * P.TimeStepsPerDay));
                 ctl->close = 1;
                 ctl->close_start = (uint16_t)ts;
                 ctl->close_stop = (uint16_t)stop;
             }
         }
     }
-    ctl->day = day + 1;
+    if (pol.icu_trigger && pol.per_adunit) {   // one trigger per admin unit
+        const int na = min(d.NA, CS_MAX_ADUNITS);
+        for (int a = threadIdx.x; a < CS_MAX_ADUNITS; a += blockDim.x) {
+            int sw = -1;
+            if (a < na) {
+                const long long recent = (long long)d.C->cumCritical_adunit[a] -
+                                         (past ? (long long)past->cumCritical_adunit[a] : 0ll);
+                sw = trigger_step(pol, recent, tn, ctl->a_started[a], ctl->a_on_until[a], true);
+            }
+            ctl->a_switch[a] = (int8_t)sw;
+            if (sw < 0) continue;
+            iv->ci_start[a] = (sw && pol.case_isolation) ? tn : 1e10;
+            iv->hq_start[a] = (sw && pol.household_quarantine) ? tn : 1e10;
+            atomicOr(&s_any, 1);
+            if (sw) {
+                ctl->a_close_start[a] = (uint16_t)ts;
+                ctl->a_close_stop[a] = (uint16_t)stop;
+                if ((uint16_t)ts < (uint16_t)stop) {
+                    atomicMin(&s_cmin, (int)(uint16_t)ts);
+                    atomicMax(&s_cmax, (int)(uint16_t)stop);
+                }
+                atomicOr(&s_any, 2);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_any) {
+            iv->ci_dur = iv->hq_dur = pol.duration;
+            ctl->socd_write = 1;
+            if (s_any & 2) {
+                ctl->close = 1;
+                ctl->close_start = (uint16_t)(s_cmin == INT_MAX ? 0 : s_cmin);
+                ctl->close_stop = (uint16_t)s_cmax;
+            }
+        }
+    }
+    if (threadIdx.x == 0) ctl->day = day + 1;
 }
 __global__ void k_day_logic(DevPop d, DayCtl* ctl, const int32_t* clock, DevIv* iv) { k_day_logic_body(d, ctl, clock, iv); }
 // one block per member; the window struct is the member's own (written only here and
@@ -1735,7 +1815,17 @@ __global__ void k_day_logic_multi(const DevPop* __restrict__ pops, DayCtl* const
 __device__ __forceinline__ void k_socdist_fill_body(const DevPop& d, const DayCtl* ctl)
 {
     if (!ctl->socd_write) return;
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < d.NM; m += gridDim.x * blockDim.x) d.socdist[m] = ctl->socd_value;
+    const bool per_unit = ctl->pol.per_adunit != 0;
+    const uint8_t on = ctl->pol.social_distancing ? CS_TREAT_TREATED : CS_TREAT_UNTREATED;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < d.NM; m += gridDim.x * blockDim.x) {
+        if (!per_unit) {
+            d.socdist[m] = ctl->socd_value;
+            continue;
+        }
+        const int a = d.mcell_adunit[m];
+        if (a < 0 || a >= CS_MAX_ADUNITS || ctl->a_switch[a] < 0) continue;
+        d.socdist[m] = ctl->a_switch[a] ? on : (uint8_t)CS_TREAT_UNTREATED;
+    }
 }
 __global__ void k_socdist_fill(DevPop d, const DayCtl* ctl) { k_socdist_fill_body(d, ctl); }
 __global__ void k_socdist_fill_multi(const DevPop* __restrict__ pops, DayCtl* const* ctls)
@@ -1836,7 +1926,14 @@ static int alloc_dynamic(cs_gpu_ctx* c)
     CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * NC, c->stream));
     CK(cudaMemsetAsync(d.pstep, 0, N, c->stream));
     { cs_params* t; UP(t, params, 1); c->dP = t; d.P = t; }
-    { DevIv iv{1e10, 0, 1e10, 0}; DevIv* t; UP(t, &iv, 1); c->dIv = t; d.iv = t; }
+    {
+        double *ci, *hq;
+        AL(ci, d.NA); AL(hq, d.NA);
+        DevIv iv{0, 0, ci, hq};
+        DevIv* t; UP(t, &iv, 1); c->dIv = t; d.iv = t;
+        c->iv_ci = ci; c->iv_hq = hq;
+        LAUNCH(k_iv_reset, 1, kThreads, t, d.NA);
+    }
     { DevStep* t; AL(t, 1); d.step = t; CK(cudaMemsetAsync(t, 0, sizeof(DevStep), c->stream)); }
     { unsigned long long* t; AL(t, 1); c->d_seed = t; d.seed_src = t; CK(cudaMemsetAsync(t, 0, sizeof(*t), c->stream)); }
     d.t_src = nullptr;
@@ -1867,6 +1964,7 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     c->stat->device = device;
     DevPop& d = c->d;
     d.N = pop->n_people; d.NH = pop->n_households; d.NC = pop->n_cells; d.NM = pop->n_mcells; d.NPT = pop->num_place_types;
+    d.NA = pop->n_adunits > 0 ? pop->n_adunits : 1;
     size_t N = d.N, NH = d.NH, NC = d.NC, NM = d.NM, NPT = d.NPT;
     if (d.NPT < 0 || d.NPT > CS_MAX_PLACE_TYPES) return set_err(c, CS_E_ARG, "num_place_types out of range");
     if (N >= (1u << 28)) return set_err(c, CS_E_UNSUPPORTED, "at most 2^28 - 1 people (place work entries pack index << 3)");
@@ -2256,9 +2354,7 @@ static int reset_run_level(cs_gpu_ctx* c, uint64_t seed)
     CK(cudaMemcpyAsync(d.close_window, kNoClosures, sizeof(kNoClosures), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(d.socdist, 0, d.NM, c->stream));
     CK(cudaMemsetAsync(d.moverest, 0, d.NM, c->stream));
-    DevIv iv{1e10, 0, 1e10, 0};
-    CK(cudaMemcpyAsync(c->dIv, &iv, sizeof(iv), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));   // iv is a stack copy
+    LAUNCH(k_iv_reset, 1, kThreads, c->dIv, d.NA);
     return CS_OK;
 }
 
@@ -3008,7 +3104,15 @@ void cs_gpu_batch_destroy(cs_gpu_batch* b)
 int cs_gpu_set_interventions(cs_gpu_ctx* c, const cs_interventions* iv)
 {
     if (!c || !iv) return CS_E_ARG;
-    DevIv div{iv->CaseIsolationTimeStart, iv->CaseIsolationPolicyDuration, iv->HQuarantineTimeStart, iv->HQuarantinePolicyDuration};
+    const int na = c->d.NA;
+    std::vector<double> ci(na), hq(na);
+    for (int a = 0; a < na; a++) {
+        ci[a] = iv->adunit_CaseIsolationTimeStart ? iv->adunit_CaseIsolationTimeStart[a] : iv->CaseIsolationTimeStart;
+        hq[a] = iv->adunit_HQuarantineTimeStart ? iv->adunit_HQuarantineTimeStart[a] : iv->HQuarantineTimeStart;
+    }
+    DevIv div{iv->CaseIsolationPolicyDuration, iv->HQuarantinePolicyDuration, c->iv_ci, c->iv_hq};
+    CK(cudaMemcpyAsync(c->iv_ci, ci.data(), sizeof(double) * na, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->iv_hq, hq.data(), sizeof(double) * na, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->dIv, &div, sizeof(div), cudaMemcpyHostToDevice, c->stream));
     if (iv->mcell_socdist) CK(cudaMemcpyAsync(c->d.socdist, iv->mcell_socdist, c->d.NM, cudaMemcpyHostToDevice, c->stream));
     if (iv->mcell_moverest) CK(cudaMemcpyAsync(c->d.moverest, iv->mcell_moverest, c->d.NM, cudaMemcpyHostToDevice, c->stream));

@@ -302,6 +302,10 @@ typedef struct cs_interventions {
     /* microcell status arrays (n_mcells) or NULL to leave unchanged */
     const uint8_t* mcell_socdist;      /* Microcell::socdist (TreatStat)        */
     const uint8_t* mcell_moverest;     /* Microcell::moverest (TreatStat)       */
+    /* per admin unit start times (n_adunits entries, AdUnits[a].CaseIsolationTimeStart
+       and .HQuarantineTimeStart), or NULL for the scalar start in every admin unit */
+    const double* adunit_CaseIsolationTimeStart;
+    const double* adunit_HQuarantineTimeStart;
 } cs_interventions;
 
 /* Counters: the StateT[] fields RecordSample reduces (src/Model.h:68-122). */
@@ -497,6 +501,11 @@ typedef struct cs_run_policy {
     uint32_t close_place_types;     /* bit t set: places of type t close when it fires */
     int32_t probs_every_step;       /* 1: test the susceptible fraction after every timestep,
                                        as the reference does; 0: at the end of each day */
+    int32_t per_adunit;             /* 1: one trigger per admin unit (the first CS_MAX_ADUNITS;
+                                       DoAdminTriggers, src/Sweep.cpp:1478-1482) on its own
+                                       admissions, firing when they exceed icu_threshold and
+                                       switching its case isolation, household quarantine,
+                                       microcells and places only */
     double duration;                /* days the interventions stay on */
 } cs_run_policy;
 

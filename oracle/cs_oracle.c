@@ -77,7 +77,8 @@ struct cs_cpu_ctx {
     uint8_t* mark;
     /* microcell interventions */
     uint8_t *socdist, *moverest;
-    double ci_start, ci_dur, hq_start, hq_dur;
+    double ci_dur, hq_dur;
+    double *ci_start, *hq_start;   /* [max(1, NAD)]: AdUnits[a].CaseIsolationTimeStart, HQuarantineTimeStart */
     /* spatial proposal blocks */
     int32_t bs, nbx, nby, NB;
     int32_t *cell_block, *block_cell_ofs, *block_cells, *block_cum;
@@ -610,6 +611,8 @@ int cs_cpu_create(const cs_population* pop, const cs_params* params, cs_cpu_ctx*
     ALLOC(c->socdist, c->NM, uint8_t); ALLOC(c->moverest, c->NM, uint8_t);
     ALLOC(c->claim, c->N, uint64_t);
     ALLOC(c->hh_carer, c->NH, uint8_t); ALLOC(c->hh_hq, c->NH, uint8_t);
+    ALLOC(c->ci_start, c->NAD, double); ALLOC(c->hq_start, c->NAD, double);
+    for (int a = 0; a <= c->NAD; a++) c->ci_start[a] = c->hq_start[a] = 1e10;
     for (int i = 0; i < c->N; i++) c->claim[i] = UINT64_MAX;
     build_blocks(c);
     *out = c;
@@ -627,7 +630,7 @@ void cs_cpu_destroy(cs_cpu_ctx* c)
                     c->prob_absent, c->prob_care, c->infector, c->listpos, c->infect_type, c->S, c->L, c->I,
                     c->R, c->D, c->S0, c->tot_prob, c->slots, c->mark, c->socdist, c->moverest, c->claim,
                     c->hh_carer, c->hh_hq, c->cell_block, c->block_cell_ofs, c->block_cells, c->block_cum,
-                    c->block_S0, c->block_row_cum};
+                    c->block_S0, c->block_row_cum, c->ci_start, c->hq_start};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     for (int t = 0; t < c->NPT; t++) {
         place_arrays* p = &c->pl[t];
@@ -853,7 +856,7 @@ static void reset_run_level(cs_cpu_ctx* c, uint64_t seed)
         }
     memset(c->socdist, 0, (size_t)c->NM);
     memset(c->moverest, 0, (size_t)c->NM);
-    c->ci_start = c->hq_start = 1e10;
+    for (int a = 0; a <= c->NAD; a++) c->ci_start[a] = c->hq_start[a] = 1e10;
     c->ci_dur = c->hq_dur = 0;
 }
 
@@ -1307,8 +1310,10 @@ static void do_detected_case(cs_cpu_ctx* c, int p, double t, int ts)
     const cs_params* P = &c->P;
     int ad = c->mcell_adunit[c->mcell[p]];
     if (ad >= 0 && ad < CS_MAX_ADUNITS) c->C.cumDC_adunit[ad]++;
-    if (P->DoHouseholds && t >= c->hq_start && t < c->hq_start + c->hq_dur) c->hh_hq[c->hh[p]] = 1;
-    if (t >= c->ci_start && t < c->ci_start + c->ci_dur) {
+    const int aw = (ad >= 0 && ad < c->NAD) ? ad : 0;   /* the person's admin unit's windows */
+    const double hq0 = c->hq_start[aw], ci0 = c->ci_start[aw];
+    if (P->DoHouseholds && t >= hq0 && t < hq0 + c->hq_dur) c->hh_hq[c->hh[p]] = 1;
+    if (t >= ci0 && t < ci0 + c->ci_dur) {
         stream s;
         stream_init(&s, c->seed, CS_RNG_DETECTED, (uint32_t)ts, (uint32_t)p, 0);
         if ((P->CaseIsolationProp == 1) || (stream_next(&s) < P->CaseIsolationProp)) {
@@ -1483,9 +1488,11 @@ int cs_cpu_step(cs_cpu_ctx* c, double t, int run)
 /* --------------------------------------------------------- interventions -- */
 int cs_cpu_set_interventions(cs_cpu_ctx* c, const cs_interventions* iv)
 {
-    c->ci_start = iv->CaseIsolationTimeStart;
+    for (int a = 0; a < (c->NAD > 0 ? c->NAD : 1); a++) {
+        c->ci_start[a] = iv->adunit_CaseIsolationTimeStart ? iv->adunit_CaseIsolationTimeStart[a] : iv->CaseIsolationTimeStart;
+        c->hq_start[a] = iv->adunit_HQuarantineTimeStart ? iv->adunit_HQuarantineTimeStart[a] : iv->HQuarantineTimeStart;
+    }
     c->ci_dur = iv->CaseIsolationPolicyDuration;
-    c->hq_start = iv->HQuarantineTimeStart;
     c->hq_dur = iv->HQuarantinePolicyDuration;
     if (iv->mcell_socdist) memcpy(c->socdist, iv->mcell_socdist, (size_t)c->NM);
     if (iv->mcell_moverest) memcpy(c->moverest, iv->mcell_moverest, (size_t)c->NM);

@@ -7,8 +7,8 @@ from covidsim_b200 import population, params as prm, sim
 
 
 @functools.lru_cache(maxsize=None)
-def tiny_world(n_people=20000, seed=98798150, kernel_size=200000, r0=2.4, utm=1):
-    pop = population.preset("tiny", n_people=n_people, seed=seed)
+def tiny_world(n_people=20000, seed=98798150, kernel_size=200000, r0=2.4, utm=1, adunit_grid=None):
+    pop = population.preset("tiny", n_people=n_people, seed=seed, adunit_grid=adunit_grid)
     P, lk, hr = prm.build_params(pop.grid, kernel_size=kernel_size)
     P.DoUTM_coords = utm
     if not utm:

@@ -150,3 +150,51 @@ def test_batch_device_loop_matches_lone_host_loops(every_step):
         m.close()
     for m in members:
         m.close()
+
+
+def _unit_policy():
+    # staggered: each of the 9 admin units fires on its own admissions
+    return sim.InterventionPolicy(threshold=1, window=7, duration=12.0, per_adunit=True)
+
+
+@pytest.mark.parametrize("every_step", [False, True])
+def test_per_adunit_device_loop_matches_host_loop_and_oracle(every_step):
+    pop, P, lk, hr = tiny_world(adunit_grid=3)
+    host = sim.Simulation(pop, P, lk, hr)
+    calls = []
+    orig = host.backend.set_interventions
+    host.backend.set_interventions = lambda iv: (calls.append(1), orig(iv))
+    want = host.run(505, DAYS, n_seed=20, policy=_unit_policy(), probs_every_step=every_step, device_loop=False)
+    want_state = snapshot(host.backend, pop)
+    assert len(calls) >= 3, "the admin units' triggers did not switch on different days"
+    dev = host.replica()
+    got = dev.run(505, DAYS, n_seed=20, policy=_unit_policy(), probs_every_step=every_step, device_loop=True)
+    _same_series(got, want, "per admin unit, device loop")
+    _same_state(snapshot(dev.backend, pop), want_state, "per admin unit, device loop")
+    if every_step:
+        o = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+        ow = o.run(505, DAYS, n_seed=20, policy=_unit_policy(), probs_every_step=True)
+        _same_series(got, ow, "per admin unit, device loop vs oracle")
+        _same_state(snapshot(dev.backend, pop), snapshot(o.backend, pop), "per admin unit, device loop vs oracle")
+        o.close()
+    dev.close()
+    host.close()
+
+
+def test_batch_with_per_adunit_member():
+    pop, P, lk, hr = tiny_world(adunit_grid=3)
+    a = sim.Simulation(pop, P, lk, hr)
+    b = a.replica()
+    policies = [_unit_policy(), sim.InterventionPolicy(threshold=3, window=7, duration=12.0)]
+    batch = sim.Batch([a, b])
+    got = batch.run([31, 32], DAYS, n_seed=20, policy=policies)
+    snaps = [snapshot(m.backend, pop) for m in (a, b)]
+    batch.close()
+    for k, seed in enumerate([31, 32]):
+        m = sim.Simulation(pop, P, lk, hr)
+        want = m.run(seed, DAYS, n_seed=20, policy=policies[k], device_loop=False)
+        _same_series(got[k], want, "member %d" % k)
+        _same_state(snapshot(m.backend, pop), snaps[k], "member %d" % k)
+        m.close()
+    a.close()
+    b.close()
