@@ -196,11 +196,11 @@ struct cs_gpu_ctx {
     unsigned long long* d_seed = nullptr;   // device copy of seed (DevPop::seed_src)
     int seed_cap = 0;
     // dense-grid buffers of UpdateProbs' normaliser
-    double *S0g = nullptr, *Ng = nullptr, *Ag = nullptr, *Bg = nullptr;
+    float *S0g = nullptr, *Ng = nullptr, *Ag = nullptr, *Bg = nullptr;
     uint8_t *rowS = nullptr, *rowN = nullptr;
     float* Gtab = nullptr;   // kernel rows of every (source row, target row) pair, or null
     void* xfer = nullptr;    // state-transfer staging (XferSlices)
-    double *Apart = nullptr, *Bpart = nullptr;   // per row-chunk partial sums
+    float *Apart = nullptr, *Bpart = nullptr;   // per row-chunk partial sums
     uint64_t seed = 0;
     bool run_started = false;
     int grid = 148 * 8;
@@ -456,17 +456,17 @@ __global__ void k_kernel_rows(DevPop d, float* Gtab, unsigned long long* oor)
     }
 }
 
-__global__ void k_grid_values(DevPop d, double* S0g, double* Ng, uint8_t* rowS, uint8_t* rowN)
+__global__ void k_grid_values(DevPop d, float* S0g, float* Ng, uint8_t* rowS, uint8_t* rowN)
 {
     if (d.gate && !*d.gate) return;
     int nch = d.P->nch;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
         int g = d.cell_grid[c];
-        S0g[g] = (double)d.S0[c];
+        S0g[g] = (float)d.S0[c];
         if (d.S0[c] > 0) rowS[g % nch] = 1;
         if (Ng) {
             int n = d.cell_start[c + 1] - d.cell_start[c];
-            Ng[g] = (double)n;
+            Ng[g] = (float)n;
             if (n > 0) rowN[g % nch] = 1;
         }
     }
@@ -477,9 +477,10 @@ __global__ void k_grid_values(DevPop d, double* S0g, double* Ng, uint8_t* rowS, 
 // G(|dx|), so target column xm of output j reads Gm[off + xm - xl0 - j]: for
 // sixteen targets xm0..xm0+15 a thread reads one window of 23 values, w[q] =
 // Gm[off - 7 + xm0 - xl0 + q], and does 128 fused multiply-adds from registers.
-// Gm is stored with one pad slot after every 8 values, so the windows of the 16
-// lanes of a half-warp (8 values apart) fall in distinct banks.
+// Gm is stored with one pad slot after every 8 values, so the windows of the 32
+// lanes of a warp (9 slots apart) fall in distinct banks.
 //
+// Arithmetic: FP32, as the reference's float cum_trans sums (src/CovidSim.cpp:2785-2795).
 // Summation order, restated by the oracle: for each output, the row sum over xm
 // ascending (fused multiply-adds, one rounding per term); row sums added in
 // ascending ym within chunks of kTotProbRowChunk target rows; chunk sums added in
@@ -496,14 +497,14 @@ __host__ __device__ constexpr int tp_phys(int i) { return i + (i >> 3); }
 struct TotProbGeom {
     int ncwR;   // target columns rounded up to a multiple of 16 (tail S0 = 0)
     int off;    // Gm index of dx = 0: ncwR + 7, so off - 7 is a multiple of 8
-    int gphys;  // doubles in the padded Gm array
+    int gphys;  // values in the padded Gm array
     int nchunks;           // ceil(nch / kTotProbRowChunk)
     int chunks_per_block;  // 1 (partial sums) or nchunks (final sums)
     int need;              // threads per source row: ceil(ncw / 8)
     int rpb;               // source rows per block: 2 when two rows fit 256 threads, else 1
     size_t smem(bool denominators) const
     {
-        return sizeof(double) * ((size_t)rpb * gphys + (denominators ? 2 : 1) * (size_t)ncwR);
+        return sizeof(float) * ((size_t)rpb * gphys + (denominators ? 2 : 1) * (size_t)ncwR);
     }
 };
 
@@ -513,7 +514,7 @@ static TotProbGeom tot_prob_geom(int ncw, int nch, bool partial)
     g.ncwR = (ncw + kTotProbSpan - 1) / kTotProbSpan * kTotProbSpan;
     g.off = g.ncwR + 7;
     g.gphys = tp_phys(g.off + g.ncwR + kTotProbSpan) + 2;
-    g.gphys += g.gphys & 1;   // keep the arrays after Gm 16-byte aligned
+    g.gphys += g.gphys & 1;   // keep the arrays after Gm 8-byte aligned (float2 reads)
     g.nchunks = (nch + kTotProbRowChunk - 1) / kTotProbRowChunk;
     g.chunks_per_block = partial ? 1 : g.nchunks;
     g.need = (ncw + kTotProbCols - 1) / kTotProbCols;
@@ -523,42 +524,42 @@ static TotProbGeom tot_prob_geom(int ncw, int nch, bool partial)
 
 // Out[(z * ncw + xl) * nch + yl] for block z of the chunk dimension.
 template <bool kDenominators>
-__global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S0g, const double* Ng,
+__global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const float* S0g, const float* Ng,
                                                        const uint8_t* rowS, const uint8_t* rowN,
-                                                       double* Aout, double* Bout, TotProbGeom gm,
+                                                       float* Aout, float* Bout, TotProbGeom gm,
                                                        const float* __restrict__ Gtab)
 {
     if (d.gate && !*d.gate) return;
     const cs_params& P = *d.P;
     const int ncw = P.ncw, nch = P.nch;
-    extern __shared__ __align__(16) double sh[];
-    double* Srow = sh + gm.rpb * gm.gphys;   // ncwR
-    double* Nrow = Srow + gm.ncwR;           // ncwR (denominator pass only)
+    extern __shared__ __align__(16) float sh[];
+    float* Srow = sh + gm.rpb * gm.gphys;   // ncwR
+    float* Nrow = Srow + gm.ncwR;           // ncwR (denominator pass only)
     // rpb == 2: threads [0, need) own source row 2*blockIdx.y, [need, 2*need) the
     // next one, each with its own kernel row Gp; the rest only help fill shared memory
     const int sub = gm.rpb == 2 ? (int)threadIdx.x / gm.need : 0;
     const int jcol = gm.rpb == 2 ? (int)threadIdx.x % gm.need : (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int yl0 = blockIdx.y * gm.rpb;
     const int yl = yl0 + sub;
-    double* Gp = sh + (size_t)min(sub, gm.rpb - 1) * gm.gphys;   // this thread's padded, mirrored kernel row
+    float* Gp = sh + (size_t)min(sub, gm.rpb - 1) * gm.gphys;   // this thread's padded, mirrored kernel row
     const int xl0 = (sub < gm.rpb && yl < nch) ? jcol * kTotProbCols : ncw;   // ncw: no outputs
     const int q0 = blockIdx.z * gm.chunks_per_block;
     const int q1 = min(q0 + gm.chunks_per_block, gm.nchunks);
-    for (int k = threadIdx.x; k < gm.rpb * gm.gphys; k += blockDim.x) sh[k] = 0.0;
+    for (int k = threadIdx.x; k < gm.rpb * gm.gphys; k += blockDim.x) sh[k] = 0.f;
     for (int k = ncw + threadIdx.x; k < gm.ncwR; k += blockDim.x) {
-        Srow[k] = 0.0;
-        if (kDenominators) Nrow[k] = 0.0;
+        Srow[k] = 0.f;
+        if (kDenominators) Nrow[k] = 0.f;
     }
-    double A[kTotProbCols], B[kTotProbCols];
+    float A[kTotProbCols], B[kTotProbCols];
 #pragma unroll
-    for (int j = 0; j < kTotProbCols; j++) A[j] = B[j] = 0.0;
+    for (int j = 0; j < kTotProbCols; j++) A[j] = B[j] = 0.f;
     // window start of this thread for xm0 = 0, in padded units: phys(off - 7 - xl0 + q)
     // = 9 * (off - 7 - xl0) / 8 + q + q / 8, with off - 7 - xl0 a multiple of 8
     const int t0 = 9 * ((gm.off - 7 - xl0) / 8);
     for (int q = q0; q < q1; q++) {
-        double a[kTotProbCols], b[kTotProbCols];
+        float a[kTotProbCols], b[kTotProbCols];
 #pragma unroll
-        for (int j = 0; j < kTotProbCols; j++) a[j] = b[j] = 0.0;
+        for (int j = 0; j < kTotProbCols; j++) a[j] = b[j] = 0.f;
         const int ym1 = min(nch, (q + 1) * kTotProbRowChunk);
         for (int ym = q * kTotProbRowChunk; ym < ym1; ym++) {
             const bool useS = rowS[ym] != 0, useN = kDenominators && rowN[ym] != 0;
@@ -567,9 +568,9 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
             for (int e = threadIdx.x; e < gm.rpb * ncw; e += blockDim.x) {
                 const int r = e / ncw, k = e % ncw, ylr = yl0 + r;
                 if (ylr < nch) {
-                    double v = Gtab ? (double)Gtab[((size_t)ylr * nch + ym) * ncw + k]
-                                    : row_kernel(d, P, k, ylr, ym, CSB_CTR(err_kernel_range));
-                    double* G = sh + (size_t)r * gm.gphys;
+                    float v = Gtab ? Gtab[((size_t)ylr * nch + ym) * ncw + k]
+                                   : (float)row_kernel(d, P, k, ylr, ym, CSB_CTR(err_kernel_range));
+                    float* G = sh + (size_t)r * gm.gphys;
                     G[tp_phys(gm.off + k)] = v;
                     G[tp_phys(gm.off - k)] = v;
                 }
@@ -580,33 +581,33 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
             }
             __syncthreads();
             if (xl0 >= ncw) continue;
-            double sa[kTotProbCols], sb[kTotProbCols];
+            float sa[kTotProbCols], sb[kTotProbCols];
 #pragma unroll
-            for (int j = 0; j < kTotProbCols; j++) sa[j] = sb[j] = 0.0;
+            for (int j = 0; j < kTotProbCols; j++) sa[j] = sb[j] = 0.f;
             for (int xm0 = 0, t = t0; xm0 < gm.ncwR; xm0 += kTotProbSpan, t += 18) {
-                double w[kTotProbSpan + kTotProbCols - 1];
+                float w[kTotProbSpan + kTotProbCols - 1];
 #pragma unroll
                 for (int r = 0; r < kTotProbSpan + kTotProbCols - 1; r++) w[r] = Gp[t + r + (r >> 3)];
                 if (useS) {
-                    const double2* s2 = reinterpret_cast<const double2*>(Srow + xm0);
+                    const float2* s2 = reinterpret_cast<const float2*>(Srow + xm0);
 #pragma unroll
                     for (int u2 = 0; u2 < kTotProbSpan / 2; u2++) {
-                        const double2 sv = s2[u2];
+                        const float2 sv = s2[u2];
 #pragma unroll
-                        for (int j = 0; j < kTotProbCols; j++) sa[j] = fma(sv.x, w[2 * u2 - j + 7], sa[j]);
+                        for (int j = 0; j < kTotProbCols; j++) sa[j] = fmaf(sv.x, w[2 * u2 - j + 7], sa[j]);
 #pragma unroll
-                        for (int j = 0; j < kTotProbCols; j++) sa[j] = fma(sv.y, w[2 * u2 + 1 - j + 7], sa[j]);
+                        for (int j = 0; j < kTotProbCols; j++) sa[j] = fmaf(sv.y, w[2 * u2 + 1 - j + 7], sa[j]);
                     }
                 }
                 if (kDenominators && useN) {
-                    const double2* n2 = reinterpret_cast<const double2*>(Nrow + xm0);
+                    const float2* n2 = reinterpret_cast<const float2*>(Nrow + xm0);
 #pragma unroll
                     for (int u2 = 0; u2 < kTotProbSpan / 2; u2++) {
-                        const double2 nv = n2[u2];
+                        const float2 nv = n2[u2];
 #pragma unroll
-                        for (int j = 0; j < kTotProbCols; j++) sb[j] = fma(nv.x, w[2 * u2 - j + 7], sb[j]);
+                        for (int j = 0; j < kTotProbCols; j++) sb[j] = fmaf(nv.x, w[2 * u2 - j + 7], sb[j]);
 #pragma unroll
-                        for (int j = 0; j < kTotProbCols; j++) sb[j] = fma(nv.y, w[2 * u2 + 1 - j + 7], sb[j]);
+                        for (int j = 0; j < kTotProbCols; j++) sb[j] = fmaf(nv.y, w[2 * u2 + 1 - j + 7], sb[j]);
                     }
                 }
             }
@@ -634,12 +635,12 @@ __global__ void __launch_bounds__(256) k_tot_prob_rows(DevPop d, const double* S
 }
 
 // Chunk sums added in ascending chunk order: out[g] = sum over z of part[z][g].
-__global__ void k_tot_prob_reduce(const double* __restrict__ part, int nparts, size_t G, double* __restrict__ out,
+__global__ void k_tot_prob_reduce(const float* __restrict__ part, int nparts, size_t G, float* __restrict__ out,
                                   const int32_t* gate)
 {
     if (gate && !*gate) return;
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < G; g += (size_t)gridDim.x * blockDim.x) {
-        double A = 0.0;
+        float A = 0.f;
         for (int z = 0; z < nparts; z++) A = A + part[(size_t)z * G + g];
         out[g] = A;
     }
@@ -657,13 +658,13 @@ static void tot_prob_launch_shape(int ncw, int nch, const TotProbGeom& gm, dim3*
     *grid = dim3(xblocks, (nch + gm.rpb - 1) / gm.rpb, gm.nchunks / gm.chunks_per_block);
 }
 
-__global__ void k_tot_prob_finish(DevPop d, const double* Ag, const double* Bg)
+__global__ void k_tot_prob_finish(DevPop d, const float* Ag, const float* Bg)
 {
     if (d.gate && !*d.gate) return;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
         int g = d.cell_grid[c];
-        double b = Bg[g];
-        d.tot_prob[c] = (b > 0) ? Ag[g] / b : 0.0;
+        const double b = (double)Bg[g];
+        d.tot_prob[c] = (b > 0) ? (double)Ag[g] / b : 0.0;
     }
 }
 
@@ -2265,14 +2266,14 @@ static int tot_prob_pass(cs_gpu_ctx* c, bool denominators)
     const cs_params& P = c->hp;
     size_t G = (size_t)P.ncw * P.nch;
     if (d.gate) {
-        LAUNCH(k_zero_gated, c->grid, kThreads, (unsigned char*)c->S0g, sizeof(double) * G, d.gate);
+        LAUNCH(k_zero_gated, c->grid, kThreads, (unsigned char*)c->S0g, sizeof(float) * G, d.gate);
         LAUNCH(k_zero_gated, 4, kThreads, c->rowS, (size_t)P.nch, d.gate);
     } else {
-        CK(cudaMemsetAsync(c->S0g, 0, sizeof(double) * G, c->stream));
+        CK(cudaMemsetAsync(c->S0g, 0, sizeof(float) * G, c->stream));
         CK(cudaMemsetAsync(c->rowS, 0, P.nch, c->stream));
     }
     if (denominators) {
-        CK(cudaMemsetAsync(c->Ng, 0, sizeof(double) * G, c->stream));
+        CK(cudaMemsetAsync(c->Ng, 0, sizeof(float) * G, c->stream));
         CK(cudaMemsetAsync(c->rowN, 0, P.nch, c->stream));
     }
     LAUNCH(k_grid_values, (d.NC + kThreads - 1) / kThreads, kThreads, d, c->S0g, denominators ? c->Ng : nullptr, c->rowS, c->rowN);
@@ -3353,11 +3354,11 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
 namespace {
 constexpr size_t kStaticCells = CS_STATIC_MAX_GRID_CELLS;
 constexpr size_t kStaticRows = CS_STATIC_MAX_GRID_ROWS;
-constexpr size_t kStaticBytes = 2 * sizeof(double) * kStaticCells + kStaticRows;
+constexpr size_t kStaticBytes = 2 * sizeof(float) * kStaticCells + kStaticRows;
 constexpr int kStaticMaxDevices = 64;
 }  // namespace
 
-// [S0 on the grid: kStaticCells doubles][numerators: kStaticCells doubles][row flags]
+// [S0 on the grid: kStaticCells floats][numerators: kStaticCells floats][row flags]
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
 static std::mutex g_static_mu;
@@ -3393,13 +3394,13 @@ extern "C" int cs_gpu_update_probs_static(cs_gpu_ctx* c, int do_place)
         }
         base = g_static_base[dev];
     }
-    double* S0g = (double*)base;
-    double* Ag = S0g + kStaticCells;
+    float* S0g = (float*)base;
+    float* Ag = S0g + kStaticCells;
     uint8_t* rowS = (uint8_t*)(Ag + kStaticCells);
     // The array still holds the previous call's values.  Grid positions without a
     // populated cell and rows without susceptibles must read zero; the numerators
     // are written in full by the row kernel.
-    CK(cudaMemsetAsync(S0g, 0, sizeof(double) * G, c->stream));
+    CK(cudaMemsetAsync(S0g, 0, sizeof(float) * G, c->stream));
     CK(cudaMemsetAsync(rowS, 0, P.nch, c->stream));
     const int cgrid = (d.NC + kThreads - 1) / kThreads;
     k_update_S0<<<cgrid, kThreads, 0, c->stream>>>(d, do_place);

@@ -389,8 +389,8 @@ int cs_gpu_update_probs(cs_gpu_ctx* ctx, int do_place);
  * bit for bit, for callers that must not allocate device memory at that point (a
  * process whose device memory is reserved by another allocator's pool; a caller
  * that must not let a free synchronise the device under other streams).  Its
- * scratch is one fixed array inside the library, 2 x 8 B x CS_STATIC_MAX_GRID_CELLS
- * + CS_STATIC_MAX_GRID_ROWS bytes (8.0 MiB), per device; grids with more cells or
+ * scratch is one fixed array inside the library, 2 x 4 B x CS_STATIC_MAX_GRID_CELLS
+ * + CS_STATIC_MAX_GRID_ROWS bytes (4.0 MiB), per device; grids with more cells or
  * rows are rejected with CS_E_RANGE.  The context's device must be current
  * (CS_E_STATE otherwise).  The first call on a device does the set-up (looking up
  * the array's device address), so make it before any stream capture.  All calls

@@ -699,7 +699,8 @@ static double row_kernel(const cs_cpu_ctx* c, int dx, int yl, int ym, int64_t* e
 
 /* UpdateProbs (src/CovidSim.cpp:2752-2802): S0 per cell, then
  * tot_prob = sum_m S0_m Kmax(l,m) / sum_m n_m Kmax(l,m) with
- * Kmax = (float)num(dist2_cc_min), summed in double in a fixed order: over target
+ * Kmax = (float)num(dist2_cc_min), summed in float (as the reference's float
+ * cum_trans sums, src/CovidSim.cpp:2785-2795) in a fixed order: over target
  * rows ym ascending, each row's sum over target columns xm ascending formed first
  * with fused multiply-adds (one rounding per term); row sums added within chunks
  * of TOT_PROB_ROW_CHUNK rows, chunk sums added in ascending order; zero terms are
@@ -721,33 +722,33 @@ int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
     }
     int ncw = P->ncw, nch = P->nch;
     size_t G = (size_t)ncw * nch;
-    double* S0g = (double*)calloc(G, sizeof(double));
-    double* Ng = (double*)calloc(G, sizeof(double));
-    double* krow = (double*)malloc(sizeof(double) * ncw);
+    float* S0g = (float*)calloc(G, sizeof(float));
+    float* Ng = (float*)calloc(G, sizeof(float));
+    float* krow = (float*)malloc(sizeof(float) * ncw);
     for (int m = 0; m < c->NC; m++) {
-        S0g[c->cell_grid[m]] = (double)c->S0[m];
-        Ng[c->cell_grid[m]] = (double)(c->cell_start[m + 1] - c->cell_start[m]);
+        S0g[c->cell_grid[m]] = (float)c->S0[m];
+        Ng[c->cell_grid[m]] = (float)(c->cell_start[m + 1] - c->cell_start[m]);
     }
     for (int l = 0; l < c->NC; l++) {
         int xl = c->cell_grid[l] / nch, yl = c->cell_grid[l] % nch;
-        double A = 0.0, B = 0.0;
+        float A = 0.f, B = 0.f;
         for (int q0 = 0; q0 < nch; q0 += TOT_PROB_ROW_CHUNK) {
-            double a = 0.0, b = 0.0;
+            float a = 0.f, b = 0.f;
             int q1 = q0 + TOT_PROB_ROW_CHUNK < nch ? q0 + TOT_PROB_ROW_CHUNK : nch;
             for (int ym = q0; ym < q1; ym++) {
                 int anyS = 0, anyN = 0;
                 for (int xm = 0; xm < ncw; xm++) {
-                    anyS |= S0g[(size_t)xm * nch + ym] != 0.0;
-                    anyN |= Ng[(size_t)xm * nch + ym] != 0.0;
+                    anyS |= S0g[(size_t)xm * nch + ym] != 0.f;
+                    anyN |= Ng[(size_t)xm * nch + ym] != 0.f;
                 }
                 if (!anyS && !anyN) continue;
-                for (int k = 0; k < ncw; k++) krow[k] = row_kernel(c, k, yl, ym, &err);
-                double s = 0.0, sb = 0.0;
+                for (int k = 0; k < ncw; k++) krow[k] = (float)row_kernel(c, k, yl, ym, &err);
+                float s = 0.f, sb = 0.f;
                 for (int xm = 0; xm < ncw; xm++) {
                     int dd = xm > xl ? xm - xl : xl - xm;
-                    double sv = S0g[(size_t)xm * nch + ym], nv = Ng[(size_t)xm * nch + ym];
-                    if (sv != 0.0) s = fma(sv, krow[dd], s);
-                    if (nv != 0.0) sb = fma(nv, krow[dd], sb);
+                    float sv = S0g[(size_t)xm * nch + ym], nv = Ng[(size_t)xm * nch + ym];
+                    if (sv != 0.f) s = fmaf(sv, krow[dd], s);
+                    if (nv != 0.f) sb = fmaf(nv, krow[dd], sb);
                 }
                 if (anyS) a = a + s;
                 if (anyN) b = b + sb;
@@ -755,7 +756,7 @@ int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
             A = A + a;
             B = B + b;
         }
-        c->tot_prob[l] = (B > 0) ? A / B : 0.0;
+        c->tot_prob[l] = (B > 0) ? (double)A / (double)B : 0.0;
     }
     free(S0g);
     free(Ng);
