@@ -352,7 +352,7 @@ def run_ours(args):
     return {
         "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (f64 probabilities, f32 person state)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (f64 infection probabilities, f32 normaliser sums and person state)",
         "data": "synthetic (seeded generator, reference parameter set)",
         "config": {"workload": desc, "people": pop.n_people, "cells": pop.n_cells, "timesteps_per_step": steps_per_run,
                    "realisations_per_rank": args.steps, "parallelism": "replicas x%d" % world,
@@ -492,7 +492,7 @@ def run_c2(args):
         "metric": METRIC, "value": round(person_steps / (ms / 1e3), 1), "unit": METRIC, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64/f32 (f64 probabilities, f32 person state)",
+        "dtype": "f64/f32 (f64 infection probabilities, f32 normaliser sums and person state)",
         "data": "synthetic (seeded generator, reference parameter set)",
         "config": {"workload": "batched ensemble: %d realisations, %d each of %s people on 240x240 cells, "
                                "R0 ~ U[1.8, 3.2], interventions, %d d"
