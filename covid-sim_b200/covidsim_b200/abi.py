@@ -129,6 +129,8 @@ def load_library(path=LIB_PATH):
         "cs_sizeof_params": (C.c_size_t, []),
         "cs_sizeof_population": (C.c_size_t, []),
         "cs_sizeof_counters": (C.c_size_t, []),
+        "cs_sizeof_interventions": (C.c_size_t, []),
+        "cs_sizeof_run_policy": (C.c_size_t, []),
         "cs_build_kernel_table": (I, [I, D, D, D, D, D, I, I, V, V, P(D)]),
         "cs_kernel_num": (D, [V, V, I, I, D, D]),
         "cs_gpu_create": (I, [P(cs_population), P(cs_params), I, P(V)]),
@@ -185,7 +187,8 @@ def load_library(path=LIB_PATH):
     if lib.cs_abi_version() != CONST["CS_ABI_VERSION"]:
         raise CovidSimError("library ABI version %d, header %d" % (lib.cs_abi_version(), CONST["CS_ABI_VERSION"]))
     for fn, st in (("cs_sizeof_params", cs_params), ("cs_sizeof_population", cs_population),
-                   ("cs_sizeof_counters", cs_counters)):
+                   ("cs_sizeof_counters", cs_counters), ("cs_sizeof_interventions", cs_interventions),
+                   ("cs_sizeof_run_policy", cs_run_policy)):
         if getattr(lib, fn)() != C.sizeof(st):
             raise CovidSimError("%s: library %d bytes, Python mirror %d" % (fn, getattr(lib, fn)(), C.sizeof(st)))
     _lib = lib

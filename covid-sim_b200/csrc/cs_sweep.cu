@@ -1867,6 +1867,8 @@ int cs_abi_version(void) { return CS_ABI_VERSION; }
 size_t cs_sizeof_params(void) { return sizeof(cs_params); }
 size_t cs_sizeof_population(void) { return sizeof(cs_population); }
 size_t cs_sizeof_counters(void) { return sizeof(cs_counters); }
+size_t cs_sizeof_interventions(void) { return sizeof(cs_interventions); }
+size_t cs_sizeof_run_policy(void) { return sizeof(cs_run_policy); }
 
 const char* cs_gpu_last_error(const cs_gpu_ctx* c) { return c ? c->err : "null context"; }
 void* cs_gpu_stream(cs_gpu_ctx* c) { return c ? (void*)c->stream : nullptr; }

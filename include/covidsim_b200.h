@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define CS_ABI_VERSION 1
+#define CS_ABI_VERSION 2            /* 2: per admin unit windows in cs_interventions, cs_run_policy */
 
 /* Sizes fixed by the reference (src/Constants.h, src/Country.h). */
 #define CS_MAX_PLACE_TYPES 5        /* MAX_NUM_PLACE_TYPES   (Country.h:15)   */
@@ -337,6 +337,8 @@ int cs_abi_version(void);
 size_t cs_sizeof_params(void);
 size_t cs_sizeof_population(void);
 size_t cs_sizeof_counters(void);
+size_t cs_sizeof_interventions(void);
+size_t cs_sizeof_run_policy(void);
 
 /*
  * Build the spatial kernel lookup tables exactly as KernelLookup::setup/init
