@@ -76,6 +76,8 @@ def parse():
                     help="c4 only: scenarios drawn at random from the sweep to measure accuracy on")
     ap.add_argument("--c4-save", default=None, help="c4 only: write the simulated data sets to this .npz")
     ap.add_argument("--c4-people", type=int, default=1_000_000, help="c4 only: population size")
+    ap.add_argument("--population-cache", default=None,
+                    help="directory keeping generated populations (.npz) for later runs")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-out", default=None, help="write per-kernel times to this JSON file")
@@ -212,7 +214,7 @@ def run_ours(args):
     from covidsim_b200 import population, params as prm, sim
 
     preset, days, with_iv, desc, n_seed = WORKLOADS[args.workload]
-    pop = population.preset(preset)
+    pop = population.cached(args.population_cache, preset, lambda: population.preset(preset))
     P, lk, hr = prm.build_params(pop.grid)
     beta, r0parts = sim.calibrate_local_beta(pop, P, 2.4)
     P.LocalBeta = beta

@@ -337,3 +337,97 @@ def preset(name, n_people=None, seed=98798150, adunit_grid=None):
         grid = make_grid(width_deg=0.2, height_deg=0.2, cell_deg=1.0 / 60, nmcl=4)
         return generate(n_people or 20_000, grid, sigma=1.0, seed=seed, adunit_grid=adunit_grid)
     raise ValueError("unknown preset %r" % name)
+
+
+# ------------------------------------------------------------ files
+_ARRAYS = ("person_hh", "person_mcell", "person_age", "person_flags", "person_place", "person_group",
+           "hh_first", "hh_nh", "hh_nhr", "hh_x", "hh_y", "mcell_cell", "mcell_adunit", "mcell_grid",
+           "cell_grid", "cell_start", "cell_members")
+_PLACE_ARRAYS = ("mcell", "x", "y", "member_ofs", "members", "group_ofs", "group_start", "group_size")
+
+
+def save(pop, path):
+    """Write a generated population to one .npz file, so that it is generated once
+    and reused across runs and batches (load() reads it back)."""
+    import json
+    out = {k: getattr(pop, k) for k in _ARRAYS}
+    for t, pl in enumerate(pop.places):
+        for k in _PLACE_ARRAYS:
+            out["place%d_%s" % (t, k)] = pl[k]
+    meta = dict(n_people=int(pop.n_people), n_adunits=int(pop.n_adunits), num_place_types=len(pop.places),
+                grid={k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in pop.grid.items()})
+    out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez(path, **out)
+
+
+def load(path):
+    """A population written by save()."""
+    import json
+    with np.load(path) as z:
+        meta = json.loads(bytes(z["meta"]).decode())
+        kw = {k: z[k] for k in _ARRAYS}
+        places = [{k: z["place%d_%s" % (t, k)] for k in _PLACE_ARRAYS} for t in range(meta["num_place_types"])]
+    grid = {k: (np.asarray(v) if isinstance(v, list) else v) for k, v in meta["grid"].items()}
+    return Population(n_people=meta["n_people"], grid=grid, places=places, n_adunits=meta["n_adunits"], **kw)
+
+
+# The reference's network file (SavePeopleToPlaces / LoadPeopleToPlaces,
+# src/SetupModel.cpp:2603-2690): int32 file version (NETWORK_FILE_VERSION,
+# src/SetupModel.h:96), number of place types, population size, the two set-up
+# seeds, then each person's place index per place type (int32, person-major);
+# -1 where a person has no place of that type.
+NETWORK_FILE_VERSION = 1
+
+
+def save_network_file(pop, path, setup_seed1, setup_seed2):
+    npt = len(pop.places)
+    links = np.asarray(pop.person_place, np.int32).reshape(npt, pop.n_people)
+    for t, pl in enumerate(pop.places):
+        if np.any(links[t] >= len(pl["mcell"])):
+            raise ValueError("out of bounds place link for place type %d" % t)
+    head = np.array([NETWORK_FILE_VERSION, npt, pop.n_people, setup_seed1, setup_seed2], dtype="<i4")
+    with open(path, "wb") as f:
+        f.write(head.tobytes())
+        f.write(np.ascontiguousarray(links.T, dtype="<i4").tobytes())
+
+
+def load_network_file(path, n_people, n_places, setup_seed1, setup_seed2):
+    """Place links [place types, people] from a network file, checked as the
+    reference checks them (version, place types, population size, seeds, bounds);
+    n_places: places per type."""
+    with open(path, "rb") as f:
+        head = np.frombuffer(f.read(20), dtype="<i4")
+        if len(head) < 5 or head[0] != NETWORK_FILE_VERSION:
+            raise ValueError("incompatible network file")
+        npt = len(n_places)
+        if head[1] != npt:
+            raise ValueError("number of place types does not match saved value")
+        if head[2] != n_people:
+            raise ValueError("population size does not match saved value")
+        if head[3] != setup_seed1 or head[4] != setup_seed2:
+            raise ValueError("random number seeds do not match saved values")
+        body = np.frombuffer(f.read(4 * npt * n_people), dtype="<i4")
+    if body.size != npt * n_people:
+        raise ValueError("network file is truncated")
+    links = body.reshape(n_people, npt).T.copy()
+    for t in range(npt):
+        if np.any(links[t] >= n_places[t]):
+            raise ValueError("out of bounds place link for place type %d" % t)
+    return links
+
+
+def cached(cache_dir, key, make):
+    """The population make() builds, kept as cache_dir/key.npz: generated on the
+    first call, loaded on later ones (synthetic populations reused across runs)."""
+    import os
+    if not cache_dir:
+        return make()
+    path = os.path.join(cache_dir, "%s.npz" % key)
+    if os.path.exists(path):
+        return load(path)
+    pop = make()
+    os.makedirs(cache_dir, exist_ok=True)
+    tmp = path + ".tmp.npz"
+    save(pop, tmp)
+    os.replace(tmp, path)
+    return pop
