@@ -1,0 +1,96 @@
+"""The reference's time-series output files, made from the counter blocks a run
+returns (sim.Simulation.run(..., blocks=True)): the block at t = 0 and at each day's
+end.  With the device run loop those come back in one copy at the end of the run,
+so there is no per-step host reduction (the reference's RecordSample,
+src/CovidSim.cpp:3024-3484, sums per-thread state every sample).
+
+TimeSeries[n] is the state at t = n days (n = 0 .. days), as RecordSample records
+it with a one-day output step (src/CovidSim.cpp:1411-1413, 1525); incidences are
+differences of cumulative counters between consecutive samples, the first from 0.
+Columns for features the sweep does not model (treatment, vaccination, contact
+tracing, the infection radius) are written as 0.  Files and formats follow
+SaveResults (src/CovidSim.cpp:1657-1840): `<base>.xls`, `<base>.severity.xls` and,
+with admin units, `<base>.adunit.xls`, tab-separated with "%.10f" values.
+"""
+import numpy as np
+
+from . import abi
+
+
+def _col(blocks, name, k=None):
+    off = getattr(abi.cs_counters, name).offset // 8
+    return blocks[:, off + (k or 0)].astype(np.float64)
+
+
+def _inc(x):
+    return np.diff(x, prepend=0.0)
+
+
+def time_series(blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0):
+    """TimeSeries fields [days + 1] from counter blocks [days + 1, words]."""
+    b = np.asarray(blocks, np.int64)
+    n = b.shape[0]
+    ts = {"t": np.arange(n, dtype=np.float64)}
+    for k in ("S", "L", "I", "R", "D", "Mild", "ILI", "SARI", "Critical", "CritRecov", "cumMild", "cumILI",
+              "cumSARI", "cumCritical", "cumCritRecov", "cumDeath_ILI", "cumDeath_SARI", "cumDeath_Critical", "cumDC"):
+        ts[k] = _col(b, k)
+    for k, src in (("incI", "cumI"), ("incR", "cumR"), ("incFC", "cumFC"), ("incC", "cumC"), ("incDC", "cumDC"),
+                   ("incD", "cumD"), ("incMild", "cumMild"), ("incILI", "cumILI"), ("incSARI", "cumSARI"),
+                   ("incCritical", "cumCritical"), ("incCritRecov", "cumCritRecov"),
+                   ("incDeath_ILI", "cumDeath_ILI"), ("incDeath_SARI", "cumDeath_SARI"),
+                   ("incDeath_Critical", "cumDeath_Critical"), ("incHQ", "cumHQ")):
+        ts[k] = _inc(_col(b, src))
+    ntg, tg, si = _col(b, "nTG"), _col(b, "cumTG"), _col(b, "cumSI")
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ts["meanTG"] = np.where(ntg > 0, model_timestep * tg / np.maximum(ntg, 1), 0.0)
+        ts["meanSI"] = np.where(ntg > 0, model_timestep * si / np.maximum(ntg, 1), 0.0)
+    small = (ts["R"] <= small_epidemic_cases) if small_epidemic_cases >= 0 else np.ones(n, bool)
+    ts["extinct"] = (small & (ts["I"] + ts["L"] == 0)).astype(np.float64)
+    na = min(n_adunits, abi.CS_MAX_ADUNITS)
+    for k, src in (("incI_adunit", "cumI_adunit"), ("incC_adunit", "cumC_adunit"), ("incDC_adunit", "cumDC_adunit")):
+        ts[k] = np.stack([_inc(_col(b, src, a)) for a in range(na)], axis=1) if na else np.zeros((n, 0))
+    return ts
+
+
+def _write(path, header, columns):
+    rows = np.stack(columns, axis=1)
+    with open(path, "w") as f:
+        f.write(header + "\n")
+        for r in rows:
+            f.write("\t".join("%.10f" % v for v in r) + "\n")
+
+
+def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0, adunit_names=None):
+    """Write `<base>.xls`, `<base>.severity.xls` and, with admin units,
+    `<base>.adunit.xls`; returns the TimeSeries fields."""
+    ts = time_series(blocks, model_timestep, small_epidemic_cases, n_adunits)
+    z = np.zeros_like(ts["t"])
+    # SaveResults' main table (src/CovidSim.cpp:1665-1677); its format string has
+    # "%.10ft%.10f" between cumTP and cumV, reproduced here
+    with open(base + ".xls", "w") as f:
+        f.write("t\tS\tL\tI\tR\tD\tincI\tincR\tincFC\tincC\tincDC\tincTC\tincCT\tincCC\tcumT\tcumTP\tcumV\tcumVG\t"
+                "Extinct\trmsRad\tmaxRad\n")
+        cols = [ts["t"], ts["S"], ts["L"], ts["I"], ts["R"], ts["D"], ts["incI"], ts["incR"], ts["incFC"], ts["incC"],
+                ts["incDC"], z, z, z, z, z, z, z, ts["extinct"], z, z]
+        for r in np.stack(cols, axis=1):
+            v = ["%.10f" % x for x in r]
+            f.write("\t".join(v[:15]) + "\t" + v[15] + "t" + "\t".join(v[16:]) + "\n")
+    # the severity table (src/CovidSim.cpp:1838-1851)
+    _write(base + ".severity.xls",
+           "t\tRt\tTG\tSI\tS\tI\tR\tincI\tMild\tILI\tSARI\tCritical\tCritRecov\tincMild\tincILI\tincSARI\t"
+           "incCritical\tincCritRecov\tincDeath\tincDeath_ILI\tincDeath_SARI\tincDeath_Critical\tcumMild\tcumILI\t"
+           "cumSARI\tcumCritical\tcumCritRecov\tcumDeath\tcumDeath_ILI\tcumDeath_SARI\tcumDeath_Critical",
+           [ts["t"], z, ts["meanTG"], ts["meanSI"], ts["S"], ts["I"], ts["R"], ts["incI"], ts["Mild"], ts["ILI"],
+            ts["SARI"], ts["Critical"], ts["CritRecov"], ts["incMild"], ts["incILI"], ts["incSARI"], ts["incCritical"],
+            ts["incCritRecov"], ts["incD"], ts["incDeath_ILI"], ts["incDeath_SARI"], ts["incDeath_Critical"],
+            ts["cumMild"], ts["cumILI"], ts["cumSARI"], ts["cumCritical"], ts["cumCritRecov"], ts["D"],
+            ts["cumDeath_ILI"], ts["cumDeath_SARI"], ts["cumDeath_Critical"]])
+    na = ts["incI_adunit"].shape[1]
+    if na:
+        names = list(adunit_names) if adunit_names is not None else ["%d" % a for a in range(na)]
+        header = "t" + "".join("\tI_%s" % m for m in names[:na]) + "".join("\tC_%s" % m for m in names[:na]) + \
+                 "".join("\tDC_%s" % m for m in names[:na])
+        cols = [ts["t"]] + [ts["incI_adunit"][:, a] for a in range(na)] + [ts["incC_adunit"][:, a] for a in range(na)] \
+            + [ts["incDC_adunit"][:, a] for a in range(na)]
+        _write(base + ".adunit.xls", header, cols)
+    return ts

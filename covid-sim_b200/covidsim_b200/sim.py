@@ -307,7 +307,7 @@ class Simulation:
         return rng.choice(self.pop.n_people, size=n_seed, replace=False).astype(np.int32)
 
     def run(self, seed, days, n_seed=100, policy=None, sample_every_day=True, callback=None, initial_state=None,
-            probs_every_step=False, device_loop=None):
+            probs_every_step=False, device_loop=None, blocks=False):
         """One realisation; returns daily time series of the main counters.
 
         initial_state: a cs_state_view of host arrays holding a prepared start
@@ -317,13 +317,17 @@ class Simulation:
         timestep, as the reference does, rather than at day ends.
         device_loop: run the logic between timesteps on the device (cs_gpu_run), one
         host round trip per run; the default uses it whenever the backend has it, the
-        run has whole days and there is no per-day callback.  Results are the same."""
+        run has whole days and there is no per-day callback.  Results are the same.
+        blocks: also return the whole counter block at t = 0 and at each day's end
+        (int64 [days + 1, sizeof(cs_counters) / 8]), as `(series, blocks)`; the
+        reference's output tables are made from them (covidsim_b200.output)."""
         be = self.backend
         if initial_state is not None:
             be.upload(seed, initial_state)
         else:
             be.begin_run(seed, self.choose_seeds(seed, n_seed))
         rs = _RunState(self, days, policy, callback, probs_every_step)
+        first = counter_block(be.counters()) if blocks else None
         whole = rs.nsteps == int(days) * rs.spd and float(days) == int(days)
         if device_loop is None:
             device_loop = hasattr(be, "run_device") and callback is None and whole
@@ -331,10 +335,14 @@ class Simulation:
             if not whole or callback is not None:
                 raise ValueError("the device run loop takes whole days and no callback")
             daily = be.run_device(int(days), run_policy(policy, self.pop.num_place_types, probs_every_step))
-            return {k: daily[:, _COUNTER_INDEX[k]].copy() for k in SERIES}
+            series = {k: daily[:, _COUNTER_INDEX[k]].copy() for k in SERIES}
+            return (series, np.vstack([first[None], daily])) if blocks else series
+        rs.keep_blocks = blocks
         for step in range(rs.nsteps):
             be.step(step * self.params.ModelTimeStep, 0)
             rs.after_step(step)
+        if blocks:
+            return rs.result(), np.vstack([first[None]] + rs.blocks)
         return rs.result()
 
     def _switch_interventions(self, t, policy, on, socd):
@@ -361,6 +369,11 @@ SERIES = ("S", "L", "I", "R", "D", "cumI", "cumC", "cumDC", "Critical", "cumCrit
 _COUNTER_INDEX = {k: getattr(abi.cs_counters, k).offset // 8 for k in SERIES}
 
 
+def counter_block(c):
+    """A cs_counters as its int64 words (every field of the block is int64)."""
+    return np.frombuffer(bytes(c), dtype=np.int64).copy()
+
+
 class _RunState:
     """Host side of one realisation between timesteps (src/CovidSim.cpp:1480-1530):
     daily counters, UpdateProbs when the susceptible fraction has fallen by 0.2,
@@ -374,6 +387,7 @@ class _RunState:
         self.nsteps = int(days * self.spd)
         self.prev_prop_s = 1.0
         self.series = {k: [] for k in SERIES}
+        self.keep_blocks, self.blocks = False, []
         self.iv_on_until = -1.0
         self.iv_started = False
         self.socd = np.zeros(sim.pop.n_mcells, dtype=np.uint8)
@@ -397,6 +411,8 @@ class _RunState:
         if day_end:
             for k in series:
                 series[k].append(int(getattr(c, k)))
+            if self.keep_blocks:
+                self.blocks.append(counter_block(c))
         prop_s = c.S / sim.pop.n_people
         if self.prev_prop_s - prop_s > 0.2:
             self.prev_prop_s = prop_s

@@ -1,0 +1,63 @@
+"""The reference's output tables (SaveResults, src/CovidSim.cpp:1657-1851) written
+from a run's counter blocks, here from a run of the oracle under the host loop."""
+import numpy as np
+
+from covidsim_b200 import abi, output, sim
+import oracle_py
+from tests.helpers import tiny_world
+
+DAYS = 12
+
+
+def _run(tmp_path):
+    pop, P, lk, hr = tiny_world(adunit_grid=2)
+    o = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+    series, blocks = o.run(404, DAYS, n_seed=20, blocks=True)
+    base = str(tmp_path / "run")
+    ts = output.write_results(base, blocks, P.ModelTimeStep, n_adunits=pop.n_adunits)
+    final = abi.counters_to_dict(o.backend.counters())
+    o.close()
+    return pop, series, blocks, base, ts, final
+
+
+def test_blocks_match_series_and_final_counters(tmp_path):
+    pop, series, blocks, base, ts, final = _run(tmp_path)
+    assert blocks.shape == (DAYS + 1, abi.C.sizeof(abi.cs_counters) // 8)
+    for k in ("S", "I", "cumI", "Critical"):
+        assert np.array_equal(ts[k][1:] if k in ts else output._col(blocks, k)[1:], np.asarray(series[k], float))
+    assert output._col(blocks, "cumI")[-1] == final["cumI"]
+    # t = 0 is the state after seeding: 20 infections, nobody else touched
+    assert ts["incI"][0] == 20 and ts["S"][0] == pop.n_people - 20
+
+
+def test_main_table(tmp_path):
+    pop, series, blocks, base, ts, final = _run(tmp_path)
+    lines = open(base + ".xls").read().splitlines()
+    head = lines[0].split("\t")
+    assert head[:6] == ["t", "S", "L", "I", "R", "D"] and len(head) == 21 and head[-3:] == ["Extinct", "rmsRad", "maxRad"]
+    rows = [l.split("\t") for l in lines[1:]]
+    assert len(rows) == DAYS + 1
+    # the reference's row format joins cumTP and cumV with a 't'
+    assert all(len(r) == 20 and "t" in r[15] for r in rows)
+    t = np.array([float(r[0]) for r in rows])
+    assert np.array_equal(t, np.arange(DAYS + 1))
+    SLIRD = np.array([[float(x) for x in r[1:6]] for r in rows])
+    assert np.all(SLIRD.sum(axis=1) == pop.n_people)
+    incI = np.array([float(r[6]) for r in rows])
+    assert incI.sum() == final["cumI"]
+
+
+def test_severity_and_adunit_tables(tmp_path):
+    pop, series, blocks, base, ts, final = _run(tmp_path)
+    sev = np.loadtxt(base + ".severity.xls", skiprows=1)
+    head = open(base + ".severity.xls").readline().rstrip("\n").split("\t")
+    assert len(head) == 31 and sev.shape == (DAYS + 1, 31)
+    col = {h: sev[:, i] for i, h in enumerate(head)}
+    assert col["cumCritical"][-1] == final["cumCritical"]
+    assert np.array_equal(np.cumsum(col["incCritical"]), col["cumCritical"])
+    assert col["cumDeath"][-1] == final["D"]
+    ad = np.loadtxt(base + ".adunit.xls", skiprows=1)
+    na = pop.n_adunits
+    assert ad.shape == (DAYS + 1, 1 + 3 * na)
+    # the admin units' infections add up to all infections
+    assert np.array_equal(ad[:, 1:1 + na].sum(axis=1), ts["incI"])
