@@ -30,6 +30,15 @@ def _same_series(a, b, where):
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), "%s: series %s differs" % (where, k)
 
 
+def _word_field(w):
+    """The cs_counters field holding int64 word w of the block."""
+    for name, t in abi.cs_counters._fields_:
+        f = getattr(abi.cs_counters, name)
+        if f.offset // 8 <= w < (f.offset + f.size) // 8:
+            return name
+    return "?"
+
+
 def _instrument(s):
     """Record the host loop's UpdateProbs calls and intervention switches."""
     log = {"update": 0, "switch": []}
@@ -53,14 +62,20 @@ def test_device_loop_matches_host_loop(every_step):
     pop, P, lk, hr = tiny_world()
     host = sim.Simulation(pop, P, lk, hr)
     log = _instrument(host)
-    want = host.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step, device_loop=False)
+    want, want_blocks = host.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step,
+                                 device_loop=False, blocks=True)
     want_state = snapshot(host.backend, pop)
     # the run exercised what the loop decides
     assert log["update"] >= 1, log
     assert [on for _, on in log["switch"]] == [True, False], log
     dev = host.replica()
-    got = dev.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step, device_loop=True)
+    got, got_blocks = dev.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step,
+                              device_loop=True, blocks=True)
     _same_series(got, want, "device loop")
+    # every counter of the block, at t = 0 and every day's end
+    assert got_blocks.shape == want_blocks.shape == (DAYS + 1, abi.C.sizeof(abi.cs_counters) // 8)
+    bad = np.nonzero((got_blocks != want_blocks).any(axis=0))[0]
+    assert bad.size == 0, "counters differ: %s" % sorted({_word_field(w) for w in bad})
     _same_state(snapshot(dev.backend, pop), want_state, "device loop")
     # a second run on the same context replays the same graph from a fresh start
     again = dev.run(505, DAYS, n_seed=20, policy=_policy(), probs_every_step=every_step)
