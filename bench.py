@@ -198,6 +198,34 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
+def ensemble_share(n_members, rank, world):
+    """Indices of the ensemble members rank `rank` simulates: every world-th one,
+    so each rank gets the same mix of population sizes."""
+    return list(range(rank, n_members, world))
+
+
+def gather_series(local, n_members, rank, world, dist, device):
+    """The ensemble's daily series on every rank: `local` is this rank's members'
+    [members of the rank, days] array (ensemble_share order); the result is
+    [n_members, days] in member order.  One all-gather (NCCL on the GPUs)."""
+    local = np.asarray(local, np.float64)
+    days = local.shape[1]
+    if dist is None:
+        return local
+    import torch
+    per = (n_members + world - 1) // world
+    buf = np.zeros((per, days))
+    buf[:len(local)] = local
+    t = torch.tensor(buf, dtype=torch.float64, device=device)
+    parts = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(parts, t)
+    out = np.zeros((n_members, days))
+    for r, part in enumerate(parts):
+        idx = ensemble_share(n_members, r, world)
+        out[idx] = part.cpu().numpy()[:len(idx)]
+    return out
+
+
 def run_ours(args):
     import torch
     rank = int(os.environ.get("RANK", 0))
@@ -442,68 +470,105 @@ def run_c2(args):
     """Ensemble of uneven populations stepped together (cs_gpu_batch): per size,
     `c2-per-size` realisations sharing that population's static device arrays,
     each with its own seed and R0 drawn uniformly in [1.8, 3.2], C1 interventions.
-    One step = the whole ensemble for c2-days days; one CUDA graph per timestep."""
+    One step = the whole ensemble for c2-days days, one CUDA graph per day.  Under
+    torchrun the realisations are split across the ranks (every world-th member to
+    each), the members' daily series are all-gathered at the end, and the time is the
+    slowest rank's (strong scaling: the ensemble's size is fixed)."""
     import torch
-    torch.cuda.set_device(0)
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        # the ensemble is split by realisation: each rank simulates its share, only
+        # the timing and the final series cross ranks
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     from covidsim_b200 import population, params as prm, sim
     grid = population.make_grid(cell_deg=1.0 / 120, nmcl=10)
     rng = np.random.default_rng(2024)
-    members, people = [], 0
+    n_members = len(C2_SIZES) * args.c2_per_size
+    mine = set(ensemble_share(n_members, rank, world))
+    members, people, people_all, j = [], 0, 0, 0
     for size in C2_SIZES:
         n = int(size * args.c2_scale)
-        pop = population.generate(n, grid, sigma=1.2, seed=98798150 + n)
+        draws = [float(rng.uniform(1.8, 3.2)) for _ in range(args.c2_per_size)]   # the same draws on every rank
+        people_all += n * args.c2_per_size
+        idx = [j + k for k in range(args.c2_per_size)]
+        j += args.c2_per_size
+        if not any(i in mine for i in idx):
+            continue
+        pop = population.cached(args.population_cache, "c2_%d" % n,
+                                lambda n=n: population.generate(n, grid, sigma=1.2, seed=98798150 + n))
         P, lk, hr = prm.build_params(pop.grid)
         beta24, _ = sim.calibrate_local_beta(pop, P, 2.4)
         base = None
-        for k in range(args.c2_per_size):
+        for k, i in enumerate(idx):
+            if i not in mine:
+                continue
             Pk = type(P).from_buffer_copy(P)
-            Pk.LocalBeta = beta24 * float(rng.uniform(1.8, 3.2)) / 2.4   # the coefficient scales R0 linearly
+            Pk.LocalBeta = beta24 * draws[k] / 2.4   # the coefficient scales R0 linearly
             if base is None:
                 base = sim.Simulation(pop, Pk, lk, hr)
                 members.append(base)
             else:
                 members.append(base.replica(Pk))
             people += n
+    order = sorted(mine)   # member indices of this rank, in the order of `members`
+    if not members:
+        raise SystemExit("c2: %d ranks for %d realisations leaves rank %d without any" % (world, n_members, rank))
     batch = sim.Batch(members)
     from covidsim_b200 import tune
-    tuned = tune.autotune_batch(batch, n_sm=torch.cuda.get_device_properties(0).multi_processor_count)
+    tuned = tune.autotune_batch(batch, n_sm=torch.cuda.get_device_properties(local_rank).multi_processor_count)
     days = args.c2_days
     policy = sim.InterventionPolicy()
     stream = torch.cuda.ExternalStream(batch.stream())
     for w in range(args.warmup):
-        batch.run([9000 + 100 * w + k for k in range(len(members))], min(days, 20), policy=policy)
+        batch.run([9000 + 100 * w + i for i in order], min(days, 20), policy=policy)
     batch.sync()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    finals = []
-    with ClockSampler(0) as clk:
+    last = None
+    if dist:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
         ev0.record(stream)
         for k in range(args.steps):
-            out = batch.run([17389101 + 1000 * k + j for j in range(len(members))], days, policy=policy)
-            finals.append(int(sum(o["cumI"][-1] for o in out)))
+            last = batch.run([17389101 + 1000 * k + i for i in order], days, policy=policy)
         ev1.record(stream)
         batch.sync()
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
+    # the ensemble's daily cumulative infections, gathered from the ranks
+    ens = gather_series(np.stack([o["cumI"] for o in last]), n_members, rank, world, dist, "cuda")
+    finals = [int(ens[:, -1].sum())]
     steps_per_run = int(days * members[0].params.TimeStepsPerDay)
-    person_steps = people * steps_per_run * args.steps
-    nreal = len(members) * args.steps
+    person_steps = people_all * steps_per_run * args.steps
+    nreal = n_members * args.steps
     batch.close()
     for m in members:
         m.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
     return {
-        "metric": METRIC, "value": round(person_steps / (ms / 1e3), 1), "unit": METRIC, "n_gpus": 1,
+        "metric": METRIC, "value": round(person_steps / (ms / 1e3), 1), "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64/f32 (f64 infection probabilities, f32 normaliser sums and person state)",
         "data": "synthetic (seeded generator, reference parameter set)",
         "config": {"workload": "batched ensemble: %d realisations, %d each of %s people on 240x240 cells, "
                                "R0 ~ U[1.8, 3.2], interventions, %d d"
-                               % (len(members), args.c2_per_size,
+                               % (n_members, args.c2_per_size,
                                   "/".join("%g" % (x * args.c2_scale) for x in C2_SIZES), days),
-                   "realisations_per_step": len(members), "people_total": people,
+                   "realisations_per_step": n_members, "people_total": people_all,
                    "timesteps_per_realisation": steps_per_run,
-                   "parallelism": "one graph per timestep; each kernel launched once for all realisations "
-                                  "(one grid row each); static arrays shared per population",
+                   "parallelism": "realisations split across %d GPU(s), daily series all-gathered at the end; "
+                                  "per GPU one graph per day, each kernel launched once for all of its "
+                                  "realisations (one grid row each); static arrays shared per population" % world,
                    "tuned": tuned},
         "runs_per_hour": round(nreal / (ms / 1e3) * 3600.0, 1),
         "ensemble_new_infections": finals,
@@ -617,7 +682,9 @@ def run_c4(args):
 def main():
     args = parse()
     if args.impl == "ours" and args.workload == "c2":
-        print(json.dumps(run_c2(args)))
+        out = run_c2(args)
+        if out is not None:
+            print(json.dumps(out))
         return
     if args.impl == "ours" and args.workload == "c4":
         print(json.dumps(run_c4(args)))
