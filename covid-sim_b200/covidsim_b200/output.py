@@ -8,7 +8,8 @@ TimeSeries[n] is the state at t = n days (n = 0 .. days), as RecordSample record
 it with a one-day output step (src/CovidSim.cpp:1411-1413, 1525); incidences are
 differences of cumulative counters between consecutive samples, the first from 0.
 Columns for features the sweep does not model (treatment, vaccination, contact
-tracing, the infection radius) are written as 0.  Files and formats follow
+tracing, the infection radius) are written as 0; Rt comes from the final
+per-person state when it is given.  Files and formats follow
 SaveResults (src/CovidSim.cpp:1657-1840): `<base>.xls`, `<base>.severity.xls` and,
 with admin units, `<base>.adunit.xls`, tab-separated with "%.10f" values.
 """
@@ -52,6 +53,30 @@ def time_series(blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0):
     return ts
 
 
+def reproduction_numbers(state, model_timestep, days, output_step=1.0):
+    """Rt of each output step, as the reference forms it at the end of a run
+    (src/CovidSim.cpp:3856-3973): every person ever infected (not susceptible, not
+    immune at the start) whose latent period ended by the end of the run counts once
+    in the step of that time (Rdenom); every person they infected counts once in the
+    same step of their infector; Rt is the second count over the first (over 1e-10
+    where no one's latent period ended).  `state` holds the downloaded per-person
+    arrays inf, latent_time and infector (sim.state_arrays)."""
+    inf = np.asarray(state["inf"])
+    t_lat = np.asarray(state["latent_time"], np.float64) * model_timestep
+    infector = np.asarray(state["infector"], np.int64)
+    n = int(days) + 1
+    ever = (inf != abi.CS_INF_SUSCEPTIBLE) & (inf != abi.CS_INF_IMMUNE_AT_START)
+    step = (t_lat / output_step).astype(np.int64)
+    own = ever & (t_lat <= days)
+    denom = np.bincount(step[own], minlength=n)[:n].astype(np.float64)
+    src = infector[ever]
+    src = src[src >= 0]
+    src = src[t_lat[src] <= days]
+    num = np.bincount(step[src], minlength=n)[:n].astype(np.float64)
+    denom[denom == 0] = 1e-10
+    return num / denom
+
+
 def _write(path, header, columns):
     rows = np.stack(columns, axis=1)
     with open(path, "w") as f:
@@ -60,11 +85,13 @@ def _write(path, header, columns):
             f.write("\t".join("%.10f" % v for v in r) + "\n")
 
 
-def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0, adunit_names=None):
+def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0, adunit_names=None, state=None):
     """Write `<base>.xls`, `<base>.severity.xls` and, with admin units,
-    `<base>.adunit.xls`; returns the TimeSeries fields."""
+    `<base>.adunit.xls`; returns the TimeSeries fields.  With `state` (the final
+    per-person arrays) the severity table's Rt column is filled, else it is 0."""
     ts = time_series(blocks, model_timestep, small_epidemic_cases, n_adunits)
     z = np.zeros_like(ts["t"])
+    ts["Rt"] = reproduction_numbers(state, model_timestep, len(z) - 1) if state is not None else z
     # SaveResults' main table (src/CovidSim.cpp:1665-1677); its format string has
     # "%.10ft%.10f" between cumTP and cumV, reproduced here
     with open(base + ".xls", "w") as f:
@@ -80,7 +107,7 @@ def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_aduni
            "t\tRt\tTG\tSI\tS\tI\tR\tincI\tMild\tILI\tSARI\tCritical\tCritRecov\tincMild\tincILI\tincSARI\t"
            "incCritical\tincCritRecov\tincDeath\tincDeath_ILI\tincDeath_SARI\tincDeath_Critical\tcumMild\tcumILI\t"
            "cumSARI\tcumCritical\tcumCritRecov\tcumDeath\tcumDeath_ILI\tcumDeath_SARI\tcumDeath_Critical",
-           [ts["t"], z, ts["meanTG"], ts["meanSI"], ts["S"], ts["I"], ts["R"], ts["incI"], ts["Mild"], ts["ILI"],
+           [ts["t"], ts["Rt"], ts["meanTG"], ts["meanSI"], ts["S"], ts["I"], ts["R"], ts["incI"], ts["Mild"], ts["ILI"],
             ts["SARI"], ts["Critical"], ts["CritRecov"], ts["incMild"], ts["incILI"], ts["incSARI"], ts["incCritical"],
             ts["incCritRecov"], ts["incD"], ts["incDeath_ILI"], ts["incDeath_SARI"], ts["incDeath_Critical"],
             ts["cumMild"], ts["cumILI"], ts["cumSARI"], ts["cumCritical"], ts["cumCritRecov"], ts["D"],

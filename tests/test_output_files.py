@@ -61,3 +61,34 @@ def test_severity_and_adunit_tables(tmp_path):
     assert ad.shape == (DAYS + 1, 1 + 3 * na)
     # the admin units' infections add up to all infections
     assert np.array_equal(ad[:, 1:1 + na].sum(axis=1), ts["incI"])
+
+
+def _rt_loop(inf, latent_time, infector, dt, days):
+    """The reference's loop (src/CovidSim.cpp:3882-3915, 3964-3973), person by person."""
+    n = days + 1
+    denom, num = [0.0] * n, [0.0] * n
+    for i in range(len(inf)):
+        if inf[i] in (abi.CS_INF_SUSCEPTIBLE, abi.CS_INF_IMMUNE_AT_START):
+            continue
+        if latent_time[i] * dt <= days:
+            denom[int(latent_time[i] * dt / 1.0)] += 1
+        j = infector[i]
+        if j >= 0 and latent_time[j] * dt <= days:
+            num[int(latent_time[j] * dt / 1.0)] += 1
+    return [num[k] / (denom[k] if denom[k] else 1e-10) for k in range(n)]
+
+
+def test_reproduction_numbers(tmp_path):
+    from tests.helpers import snapshot
+    pop, P, lk, hr = tiny_world()
+    o = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+    _, blocks = o.run(505, 40, n_seed=20, blocks=True)
+    st = snapshot(o.backend, pop)
+    rt = output.reproduction_numbers(st, P.ModelTimeStep, 40)
+    want = _rt_loop(st["inf"], st["latent_time"], st["infector"], P.ModelTimeStep, 40)
+    assert np.allclose(rt, want, rtol=0, atol=0)
+    assert rt[:10].max() > 1.0            # a growing epidemic early on (R0 2.4)
+    ts = output.write_results(str(tmp_path / "r"), blocks, P.ModelTimeStep, state=st)
+    sev = np.loadtxt(str(tmp_path / "r") + ".severity.xls", skiprows=1)
+    assert np.allclose(sev[:, 1], np.round(rt, 10), atol=1e-9)
+    o.close()
