@@ -10,8 +10,9 @@ differences of cumulative counters between consecutive samples, the first from 0
 Columns for features the sweep does not model (treatment, vaccination, contact
 tracing, the infection radius) are written as 0; Rt comes from the final
 per-person state when it is given.  Files and formats follow
-SaveResults (src/CovidSim.cpp:1657-1840): `<base>.xls`, `<base>.severity.xls` and,
-with admin units, `<base>.adunit.xls`, tab-separated with "%.10f" values.
+SaveResults and SaveSummaryResults (src/CovidSim.cpp:1657-2199): `<base>.xls`,
+`<base>.severity.xls`, `<base>.age.xls`, `<base>.inftype.xls` and, with admin units,
+`<base>.adunit.xls`, tab-separated.
 """
 import numpy as np
 
@@ -53,14 +54,17 @@ def time_series(blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0):
     return ts
 
 
-def reproduction_numbers(state, model_timestep, days, output_step=1.0):
-    """Rt of each output step, as the reference forms it at the end of a run
-    (src/CovidSim.cpp:3856-3973): every person ever infected (not susceptible, not
-    immune at the start) whose latent period ended by the end of the run counts once
-    in the step of that time (Rdenom); every person they infected counts once in the
-    same step of their infector; Rt is the second count over the first (over 1e-10
-    where no one's latent period ended).  `state` holds the downloaded per-person
-    arrays inf, latent_time and infector (sim.state_arrays)."""
+def infection_breakdown(state, model_timestep, days, ages=None, output_step=1.0):
+    """RecordInfTypes at the end of a run (src/CovidSim.cpp:3856-3973): every person
+    ever infected (not susceptible, not immune at the start) whose latent period
+    ended by the end of the run counts once in the output step of that time
+    (Rdenom); every person they infected counts once in the same step of their
+    infector, by the infection's type (Rtype) and by the infectee's age group
+    (Rage).  Returns (Rt, Rtype [steps, 16], Rage [steps, 17] or None), each
+    divided by Rdenom (1e-10 where no one's latent period ended), and Rt the sum
+    of Rtype over the types in type order, as the reference forms them.  `state`
+    holds the downloaded per-person arrays inf, latent_time, infector and
+    infect_type (sim.state_arrays); `ages` the people's ages in years."""
     inf = np.asarray(state["inf"])
     t_lat = np.asarray(state["latent_time"], np.float64) * model_timestep
     infector = np.asarray(state["infector"], np.int64)
@@ -69,12 +73,36 @@ def reproduction_numbers(state, model_timestep, days, output_step=1.0):
     step = (t_lat / output_step).astype(np.int64)
     own = ever & (t_lat <= days)
     denom = np.bincount(step[own], minlength=n)[:n].astype(np.float64)
-    src = infector[ever]
-    src = src[src >= 0]
-    src = src[t_lat[src] <= days]
-    num = np.bincount(step[src], minlength=n)[:n].astype(np.float64)
+    idx = np.nonzero(ever)[0]
+    src = infector[idx]
+    keep = src >= 0
+    idx, src = idx[keep], src[keep]
+    keep = t_lat[src] <= days
+    idx, src = idx[keep], src[keep]
+    bins = step[src]
     denom[denom == 0] = 1e-10
-    return num / denom
+    rtype = np.zeros((n, abi.CS_INFECT_TYPE_MASK))
+    if "infect_type" in state:
+        types = np.asarray(state["infect_type"], np.int64)[idx] % abi.CS_INFECT_TYPE_MASK
+    else:
+        types = np.zeros(len(idx), np.int64)
+    np.add.at(rtype, (bins, types), 1.0)
+    rtype /= denom[:, None]
+    rt = np.zeros(n)
+    for k in range(abi.CS_INFECT_TYPE_MASK):
+        rt += rtype[:, k]
+    rage = None
+    if ages is not None:
+        groups = np.minimum(np.asarray(ages, np.int64)[idx] // 5, abi.CS_NUM_AGE_GROUPS - 1)
+        rage = np.zeros((n, abi.CS_NUM_AGE_GROUPS))
+        np.add.at(rage, (bins, groups), 1.0)
+        rage /= denom[:, None]
+    return rt, rtype, rage
+
+
+def reproduction_numbers(state, model_timestep, days, output_step=1.0):
+    """Rt of each output step (infection_breakdown's first result)."""
+    return infection_breakdown(state, model_timestep, days, output_step=output_step)[0]
 
 
 def _write(path, header, columns):
@@ -85,13 +113,20 @@ def _write(path, header, columns):
             f.write("\t".join("%.10f" % v for v in r) + "\n")
 
 
-def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0, adunit_names=None, state=None):
-    """Write `<base>.xls`, `<base>.severity.xls` and, with admin units,
-    `<base>.adunit.xls`; returns the TimeSeries fields.  With `state` (the final
-    per-person arrays) the severity table's Rt column is filled, else it is 0."""
+def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0, adunit_names=None, state=None,
+                  ages=None):
+    """Write `<base>.xls`, `<base>.severity.xls`, `<base>.age.xls` and, with admin
+    units, `<base>.adunit.xls`; returns the TimeSeries fields.  With `state` (the
+    final per-person arrays) the severity table's Rt column is filled (else it is
+    0) and `<base>.inftype.xls` is written; `ages` (years) adds the age
+    distribution row of the age table and the Rage columns."""
     ts = time_series(blocks, model_timestep, small_epidemic_cases, n_adunits)
     z = np.zeros_like(ts["t"])
-    ts["Rt"] = reproduction_numbers(state, model_timestep, len(z) - 1) if state is not None else z
+    n = len(z)
+    if state is not None:
+        ts["Rt"], ts["Rtype"], ts["Rage"] = infection_breakdown(state, model_timestep, n - 1, ages)
+    else:
+        ts["Rt"] = z
     # SaveResults' main table (src/CovidSim.cpp:1665-1677); its format string has
     # "%.10ft%.10f" between cumTP and cumV, reproduced here
     with open(base + ".xls", "w") as f:
@@ -112,6 +147,31 @@ def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_aduni
             ts["incCritRecov"], ts["incD"], ts["incDeath_ILI"], ts["incDeath_SARI"], ts["incDeath_Critical"],
             ts["cumMild"], ts["cumILI"], ts["cumSARI"], ts["cumCritical"], ts["cumCritRecov"], ts["D"],
             ts["cumDeath_ILI"], ts["cumDeath_SARI"], ts["cumDeath_Critical"]])
+    # by age group (src/CovidSim.cpp:2035-2061), and by infection type
+    # (src/CovidSim.cpp:2184-2199, "%lf" values there)
+    b = np.asarray(blocks, np.int64)
+    ng = abi.CS_NUM_AGE_GROUPS
+    inc_age = {k: np.stack([_inc(_col(b, src, g)) for g in range(ng)], axis=1)
+               for k, src in (("I", "cumIa"), ("C", "cumCa"), ("D", "cumDa"))}
+    with open(base + ".age.xls", "w") as f:
+        f.write("t" + "".join("\t%s%d-%d" % (k, 5 * g, 5 * (g + 1)) for k in ("I", "C", "D") for g in range(ng)) + "\n")
+        for r in range(n):
+            f.write("%.10f" % ts["t"][r] + "".join("\t%.10f" % inc_age[k][r, g] for k in ("I", "C", "D")
+                                                 for g in range(ng)) + "\n")
+        if ages is not None:
+            dist = np.bincount(np.minimum(np.asarray(ages, np.int64) // 5, ng - 1), minlength=ng)[:ng]
+            f.write("dist" + "".join("\t%.10f" % v for v in dist / max(dist.sum(), 1)) + "\n")
+    if state is not None:
+        inc_type = np.stack([_inc(_col(b, "cumItype", k)) for k in range(abi.CS_INFECT_TYPE_MASK)], axis=1)
+        rage = ts["Rage"] if ts["Rage"] is not None else np.zeros((n, ng))
+        with open(base + ".inftype.xls", "w") as f:
+            f.write("t\tR\tTG\tSI" + "".join("\tRtype_%d" % k for k in range(abi.CS_INFECT_TYPE_MASK)) +
+                    "".join("\tincItype_%d" % k for k in range(abi.CS_INFECT_TYPE_MASK)) +
+                    "".join("\tRage_%d" % g for g in range(ng)) + "\n")
+            for r in range(n):
+                vals = [ts["t"][r], ts["Rt"][r], ts["meanTG"][r], ts["meanSI"][r]] + list(ts["Rtype"][r]) + \
+                       list(inc_type[r]) + list(rage[r])
+                f.write("\t".join("%f" % v for v in vals) + "\n")
     na = ts["incI_adunit"].shape[1]
     if na:
         names = list(adunit_names) if adunit_names is not None else ["%d" % a for a in range(na)]

@@ -63,10 +63,11 @@ def test_severity_and_adunit_tables(tmp_path):
     assert np.array_equal(ad[:, 1:1 + na].sum(axis=1), ts["incI"])
 
 
-def _rt_loop(inf, latent_time, infector, dt, days):
+def _rt_loop(inf, latent_time, infector, infect_type, dt, days):
     """The reference's loop (src/CovidSim.cpp:3882-3915, 3964-3973), person by person."""
-    n = days + 1
-    denom, num = [0.0] * n, [0.0] * n
+    n, M = days + 1, abi.CS_INFECT_TYPE_MASK
+    denom = [0.0] * n
+    rtype = [[0.0] * M for _ in range(n)]
     for i in range(len(inf)):
         if inf[i] in (abi.CS_INF_SUSCEPTIBLE, abi.CS_INF_IMMUNE_AT_START):
             continue
@@ -74,8 +75,15 @@ def _rt_loop(inf, latent_time, infector, dt, days):
             denom[int(latent_time[i] * dt / 1.0)] += 1
         j = infector[i]
         if j >= 0 and latent_time[j] * dt <= days:
-            num[int(latent_time[j] * dt / 1.0)] += 1
-    return [num[k] / (denom[k] if denom[k] else 1e-10) for k in range(n)]
+            rtype[int(latent_time[j] * dt / 1.0)][infect_type[i] % M] += 1
+    out = []
+    for k in range(n):
+        d = denom[k] if denom[k] else 1e-10
+        s = 0.0
+        for t in range(M):
+            s += rtype[k][t] / d
+        out.append(s)
+    return out
 
 
 def test_reproduction_numbers(tmp_path):
@@ -85,10 +93,26 @@ def test_reproduction_numbers(tmp_path):
     _, blocks = o.run(505, 40, n_seed=20, blocks=True)
     st = snapshot(o.backend, pop)
     rt = output.reproduction_numbers(st, P.ModelTimeStep, 40)
-    want = _rt_loop(st["inf"], st["latent_time"], st["infector"], P.ModelTimeStep, 40)
-    assert np.allclose(rt, want, rtol=0, atol=0)
+    want = _rt_loop(st["inf"], st["latent_time"], st["infector"], st["infect_type"], P.ModelTimeStep, 40)
+    assert np.array_equal(rt, np.array(want))
     assert rt[:10].max() > 1.0            # a growing epidemic early on (R0 2.4)
-    ts = output.write_results(str(tmp_path / "r"), blocks, P.ModelTimeStep, state=st)
+    ts = output.write_results(str(tmp_path / "r"), blocks, P.ModelTimeStep, state=st, ages=pop.person_age)
     sev = np.loadtxt(str(tmp_path / "r") + ".severity.xls", skiprows=1)
     assert np.allclose(sev[:, 1], np.round(rt, 10), atol=1e-9)
+    # the infection-type table: R is the sum of the Rtype columns, and the Rage
+    # columns split the same infections by the infectee's age group
+    it = np.loadtxt(str(tmp_path / "r") + ".inftype.xls", skiprows=1)
+    M, G = abi.CS_INFECT_TYPE_MASK, abi.CS_NUM_AGE_GROUPS
+    assert it.shape == (41, 4 + 2 * M + G)
+    assert np.allclose(it[:, 4:4 + M].sum(axis=1), it[:, 1], atol=1e-4)
+    assert np.allclose(it[:, 4 + 2 * M:].sum(axis=1), it[:, 1], atol=1e-4)
+    assert it[:, 4 + M:4 + 2 * M].sum() == output._col(blocks, "cumI")[-1]
+    # the age table: incidence by age group adds up to all infections, and the
+    # distribution row to one
+    lines = open(str(tmp_path / "r") + ".age.xls").read().splitlines()
+    assert lines[-1].startswith("dist")
+    age = np.array([[float(x) for x in l.split("\t")] for l in lines[1:-1]])
+    assert age.shape == (41, 1 + 3 * G)
+    assert np.array_equal(age[:, 1:1 + G].sum(axis=1), ts["incI"])
+    assert abs(sum(float(x) for x in lines[-1].split("\t")[1:]) - 1.0) < 1e-8
     o.close()
