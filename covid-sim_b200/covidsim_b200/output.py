@@ -181,3 +181,56 @@ def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_aduni
             + [ts["incDC_adunit"][:, a] for a in range(na)]
         _write(base + ".adunit.xls", header, cols)
     return ts
+
+
+def write_summary(base, runs, model_timestep, r0_parts=(0.0, 0.0, 0.0), small_epidemic_cases=-1):
+    """`<base>.avNE.xls`: the main table averaged over the non-extinct realisations
+    among `runs` (each a run's counter blocks), with per-time-step variances, as
+    SaveSummaryResults writes it (src/CovidSim.cpp:1960-1999; the sums over runs as
+    src/CovidSim.cpp:3978-4019).  The header line carries the realisation counts
+    (non-extinct, extinct), the three R0 parts, and the mean and variance over all
+    realisations of the peak daily case incidence and its time.  The reference's
+    column names are kept as it writes them (its ninth value is incFC under the
+    name incD, and the variance written under vincFC is that of incD).  Returns
+    the number of non-extinct realisations."""
+    series = [time_series(b, model_timestep, small_epidemic_cases) for b in runs]
+    if not series:
+        return 0
+    n = len(series[0]["t"])
+    zero = np.zeros(n)
+    ne = [ts for ts in series if not ts["extinct"][-1]]
+    n_ne, n_e = len(ne), len(series) - len(ne)
+    peaks_h, peaks_t = [], []
+    for ts in series:   # the first step with the largest case incidence
+        k = int(np.argmax(ts["incC"]))
+        peaks_h.append(ts["incC"][k] if ts["incC"][k] > 0 else 0.0)
+        peaks_t.append(float(k) if ts["incC"][k] > 0 else 0.0)
+    c = 1.0 / len(series)
+    ph, pt = np.asarray(peaks_h), np.asarray(peaks_t)
+    head = ("t\tS\tL\tI\tR\tD\tincI\tincR\tincD\tincC\tincDC\tincTC\tcumT\tcumTmax\tcumTP\tcumV\tcumVmax\tExtinct\t"
+            "rmsRad\tmaxRad\tvS\tvI\tvR\tvD\tvincI\tvincR\tvincFC\tvincC\tvincDC\tvincTC\tvrmsRad\tvmaxRad\t\t%i\t%i\t"
+            "%.10f\t%.10f\t%.10f\t\t%.10f\t%.10f\t%.10f\t%.10f\n"
+            % (n_ne, n_e, r0_parts[0], r0_parts[1], r0_parts[2], c * ph.sum(), c * (ph * ph).sum() - c * c * ph.sum() ** 2,
+               c * pt.sum(), c * (pt * pt).sum() - c * c * pt.sum() ** 2))
+    with open(base + ".avNE.xls", "w") as f:
+        f.write(head)
+        if not n_ne:
+            return 0
+        c = 1.0 / n_ne
+
+        def mean(k):
+            return c * sum(ts.get(k, zero) for ts in ne)
+
+        def var(k):
+            s1 = sum(ts.get(k, zero) for ts in ne)
+            s2 = sum(ts.get(k, zero) ** 2 for ts in ne)
+            return c * s2 - c * c * s1 * s1
+        first = ["t", "S", "L", "I", "R", "D", "incI", "incR", "incFC", "incC", "incDC", "incTC", "cumT", "cumTmax",
+                 "cumTP", "cumV", "cumVmax", "extinct", "rmsRad", "maxRad"]
+        maxed = {"cumTmax", "cumVmax"}    # written as maxima, not scaled by c
+        cols1 = [zero if k in maxed else mean(k) for k in first]
+        cols2 = [var(k) for k in ("S", "I", "R", "D", "incI", "incR", "incD", "incC", "incDC", "incTC", "rmsRad", "maxRad")]
+        for r in range(n):
+            f.write("%.10f" % cols1[0][r] + "".join("\t%10f" % col[r] for col in cols1[1:]) + "\t")
+            f.write("\t".join("%.10f" % col[r] for col in cols2) + "\n")
+    return n_ne

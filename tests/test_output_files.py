@@ -116,3 +116,25 @@ def test_reproduction_numbers(tmp_path):
     assert np.array_equal(age[:, 1:1 + G].sum(axis=1), ts["incI"])
     assert abs(sum(float(x) for x in lines[-1].split("\t")[1:]) - 1.0) < 1e-8
     o.close()
+
+
+def test_summary_over_realisations(tmp_path):
+    pop, P, lk, hr = tiny_world()
+    o = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+    runs = [o.run(900 + k, 15, n_seed=20, blocks=True)[1] for k in range(3)]
+    # a run whose epidemic dies out at once: one infection that cannot spread
+    runs.append(o.run(950, 15, n_seed=1, blocks=True)[1])
+    o.close()
+    series = [output.time_series(b, P.ModelTimeStep) for b in runs]
+    ne = [s for s in series if not s["extinct"][-1]]
+    base = str(tmp_path / "ens")
+    assert output.write_summary(base, runs, P.ModelTimeStep, (0.5, 0.7, 1.2)) == len(ne)
+    lines = open(base + ".avNE.xls").read().splitlines()
+    head = lines[0].split("\t")
+    assert head[:6] == ["t", "S", "L", "I", "R", "D"] and head[32:35] == ["", str(len(ne)), str(len(runs) - len(ne))]
+    rows = np.array([[float(x) for x in l.split("\t")] for l in lines[1:]])
+    assert rows.shape == (16, 32)
+    mean_I = np.mean([s["I"] for s in ne], axis=0)
+    var_I = np.var([s["I"] for s in ne], axis=0)
+    assert np.allclose(rows[:, 3], mean_I, atol=1e-5) and np.allclose(rows[:, 21], var_I, rtol=1e-9, atol=1e-6)
+    assert np.allclose(rows[:, 0], np.arange(16))
