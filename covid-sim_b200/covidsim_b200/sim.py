@@ -523,19 +523,26 @@ class Batch:
     def stream(self):
         return self.lib.cs_gpu_batch_stream(self.handle)
 
-    def run(self, seeds, days, n_seed=100, policy=None, callback=None, probs_every_step=False, device_loop=None):
+    def run(self, seeds, days, n_seed=100, policy=None, callback=None, probs_every_step=False, device_loop=None,
+            blocks=False):
         """One realisation per member (member k with run seed seeds[k] and, when
         `policy` is a list, policy[k]); returns the members' daily series.
         device_loop as Simulation.run: by default the logic between timesteps runs
         on the device (cs_gpu_batch_run) whenever there is no callback and the run
-        has whole days.  probs_every_step may be a list (one flag per member)."""
-        states = []
+        has whole days.  probs_every_step may be a list (one flag per member).
+        blocks: also return each member's counter blocks at t = 0 and every day's
+        end, as `(series, blocks)` (Simulation.run; output.write_summary averages
+        them over the members)."""
+        states, firsts = [], []
         policies = policy if isinstance(policy, (list, tuple)) else [policy] * len(self.sims)
         every = probs_every_step if isinstance(probs_every_step, (list, tuple)) else [probs_every_step] * len(self.sims)
         for sim, seed, pol, ev in zip(self.sims, seeds, policies, every):
             sim.backend.begin_run(seed, sim.choose_seeds(seed, n_seed))
+            if blocks:
+                firsts.append(counter_block(sim.backend.counters()))
             cb = (lambda step, c, k=len(states): callback(k, step, c)) if callback else None
             states.append(_RunState(sim, days, pol, cb, ev))
+            states[-1].keep_blocks = blocks
         whole = float(days) == int(days) and all(rs.nsteps == int(days) * rs.spd for rs in states)
         if device_loop is None:
             device_loop = callback is None and whole
@@ -547,14 +554,20 @@ class Batch:
                                              for p, s, ev in zip(policies, self.sims, every)])
             out = np.empty((n, max(nd, 1), C.sizeof(abi.cs_counters) // 8), np.int64)
             self._ck(self.lib.cs_gpu_batch_run(self.handle, nd, C.addressof(pols), out.ctypes.data), "run")
-            return [{k: out[j, :nd, _COUNTER_INDEX[k]].copy() for k in SERIES} for j in range(n)]
+            series = [{k: out[j, :nd, _COUNTER_INDEX[k]].copy() for k in SERIES} for j in range(n)]
+            if blocks:
+                return series, [np.vstack([firsts[j][None], out[j, :nd]]) for j in range(n)]
+            return series
         nsteps = max(rs.nsteps for rs in states)
         dt = self.sims[0].params.ModelTimeStep
         for step in range(nsteps):
             self.step(step * dt, 0)
             for rs in states:
                 rs.after_step(step)
-        return [rs.result() for rs in states]
+        series = [rs.result() for rs in states]
+        if blocks:
+            return series, [np.vstack([f[None]] + rs.blocks) for f, rs in zip(firsts, states)]
+        return series
 
     def close(self):
         if self.handle:

@@ -213,3 +213,22 @@ def test_batch_with_per_adunit_member():
         m.close()
     a.close()
     b.close()
+
+
+def test_batch_blocks_match_lone_runs():
+    """A batch's counter blocks (t = 0 and every day's end), member by member, equal
+    lone runs' blocks under the host loop; the summary table averages them."""
+    from covidsim_b200 import output
+    pop, P, lk, hr = tiny_world()
+    a = sim.Simulation(pop, P, lk, hr)
+    b = a.replica()
+    batch = sim.Batch([a, b])
+    _, got = batch.run([41, 42], 20, n_seed=20, policy=_policy(), blocks=True)
+    batch.close()
+    for k, seed in enumerate([41, 42]):
+        m = sim.Simulation(pop, P, lk, hr)
+        _, want = m.run(seed, 20, n_seed=20, policy=_policy(), device_loop=False, blocks=True)
+        assert np.array_equal(got[k], want), "member %d" % k
+        m.close()
+    a.close()
+    b.close()
