@@ -183,7 +183,7 @@ def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_aduni
     return ts
 
 
-def write_summary(base, runs, model_timestep, r0_parts=(0.0, 0.0, 0.0), small_epidemic_cases=-1):
+def write_summary(base, runs, model_timestep, r0_parts=(0.0, 0.0, 0.0), small_epidemic_cases=-1, last_rt=None):
     """`<base>.avNE.xls`: the main table averaged over the non-extinct realisations
     among `runs` (each a run's counter blocks), with per-time-step variances, as
     SaveSummaryResults writes it (src/CovidSim.cpp:1960-1999; the sums over runs as
@@ -191,8 +191,14 @@ def write_summary(base, runs, model_timestep, r0_parts=(0.0, 0.0, 0.0), small_ep
     (non-extinct, extinct), the three R0 parts, and the mean and variance over all
     realisations of the peak daily case incidence and its time.  The reference's
     column names are kept as it writes them (its ninth value is incFC under the
-    name incD, and the variance written under vincFC is that of incD).  Returns
-    the number of non-extinct realisations."""
+    name incD, and the variance written under vincFC is that of incD).  The peak of
+    each realisation is found as RecordInfTypes finds it (src/CovidSim.cpp:3962-
+    4016): the running maximum starts from the realisation's last-step Rt (the
+    summed Rtype the loop before leaves in it; `last_rt`, one per run, 0 when not
+    given) and a step counts when its case incidence exceeds it; the time is that
+    step's output time.  When no step exceeds it the reference keeps an
+    uninitialised time; 0 is written here.  Returns the number of non-extinct
+    realisations."""
     series = [time_series(b, model_timestep, small_epidemic_cases) for b in runs]
     if not series:
         return 0
@@ -201,10 +207,13 @@ def write_summary(base, runs, model_timestep, r0_parts=(0.0, 0.0, 0.0), small_ep
     ne = [ts for ts in series if not ts["extinct"][-1]]
     n_ne, n_e = len(ne), len(series) - len(ne)
     peaks_h, peaks_t = [], []
-    for ts in series:   # the first step with the largest case incidence
-        k = int(np.argmax(ts["incC"]))
-        peaks_h.append(ts["incC"][k] if ts["incC"][k] > 0 else 0.0)
-        peaks_t.append(float(k) if ts["incC"][k] > 0 else 0.0)
+    for i, ts in enumerate(series):
+        h, t = (float(last_rt[i]) if last_rt is not None else 0.0), 0.0
+        for k in range(n):
+            if h < ts["incC"][k]:
+                h, t = float(ts["incC"][k]), float(ts["t"][k])
+        peaks_h.append(h)
+        peaks_t.append(t)
     c = 1.0 / len(series)
     ph, pt = np.asarray(peaks_h), np.asarray(peaks_t)
     head = ("t\tS\tL\tI\tR\tD\tincI\tincR\tincD\tincC\tincDC\tincTC\tcumT\tcumTmax\tcumTP\tcumV\tcumVmax\tExtinct\t"

@@ -138,3 +138,35 @@ def test_summary_over_realisations(tmp_path):
     var_I = np.var([s["I"] for s in ne], axis=0)
     assert np.allclose(rows[:, 3], mean_I, atol=1e-5) and np.allclose(rows[:, 21], var_I, rtol=1e-9, atol=1e-6)
     assert np.allclose(rows[:, 0], np.arange(16))
+
+
+def test_summary_peak_statistics_follow_reference(tmp_path):
+    """The header's peak statistics from hand-made runs, as RecordInfTypes forms them
+    (src/CovidSim.cpp:3962-4016): the running maximum of the case incidence starts
+    from the run's last-step Rt, a later equal value does not move the peak, and
+    mean and variance are taken over all runs."""
+    import ctypes as C
+    W = C.sizeof(abi.cs_counters) // 8
+    off = {k: getattr(abi.cs_counters, k).offset // 8 for k in ("cumC", "cumI", "S", "I")}
+
+    def blocks(inc_c, infectious=3):
+        b = np.zeros((len(inc_c), W), np.int64)
+        b[:, off["cumC"]] = np.cumsum(inc_c)
+        b[:, off["cumI"]] = np.cumsum(inc_c)
+        b[:, off["S"]] = 1000
+        b[:, off["I"]] = infectious
+        return b
+
+    runs = [blocks([0, 2, 7, 7, 3, 0]),    # peak 7 first reached on day 2
+            blocks([0, 1, 1, 2, 9, 4]),    # peak 9 on day 4
+            blocks([0, 1, 2, 1, 0, 0])]    # last-step Rt 2.5 is above every day: the peak stays at it
+    last_rt = [1.5, 0.0, 2.5]
+    base = str(tmp_path / "pk")
+    output.write_summary(base, runs, 0.25, (0.0, 0.0, 0.0), last_rt=last_rt)
+    head = open(base + ".avNE.xls").readline().rstrip("\n").split("\t")
+    h = np.array([7.0, 9.0, 2.5])
+    t = np.array([2.0, 4.0, 0.0])
+    vals = [float(x) for x in head[-4:]]
+    c = 1.0 / 3
+    assert np.allclose(vals, [c * h.sum(), c * (h * h).sum() - c * c * h.sum() ** 2,
+                              c * t.sum(), c * (t * t).sum() - c * c * t.sum() ** 2], atol=1e-9)
