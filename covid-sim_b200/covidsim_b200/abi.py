@@ -100,6 +100,7 @@ cs_state_view = STRUCTS["cs_state_view"]
 cs_interventions = STRUCTS["cs_interventions"]
 cs_counters = STRUCTS["cs_counters"]
 cs_run_policy = STRUCTS["cs_run_policy"]
+cs_place_event = STRUCTS["cs_place_event"]
 
 COUNTER_FIELDS = [f for f, _ in cs_counters._fields_]
 
@@ -171,6 +172,8 @@ def load_library(path=LIB_PATH):
         "cs_sur_set_gemm": (I, [V, I]),
         "cs_gpu_set_interventions": (I, [V, P(cs_interventions)]),
         "cs_gpu_close_places": (I, [V, I, V, I, C.c_uint16, C.c_uint16]),
+        "cs_gpu_place_events": (I, [V, V, I]),
+        "cs_gpu_set_mcell_status": (I, [V, V, V, V, I]),
         "cs_gpu_get_counters": (I, [V, P(cs_counters)]),
         "cs_gpu_run": (I, [V, I, P(cs_run_policy), V]),
         "cs_gpu_batch_run": (I, [V, I, V, V]),

@@ -108,6 +108,21 @@ class GpuBackend:
             m = np.ascontiguousarray(mcells, dtype=np.int32)
             self._ck(self.lib.cs_gpu_close_places(self.ctx, place_type, m.ctypes.data, len(m), start, stop), "close_places")
 
+    def place_events(self, events):
+        """Outcomes of a host TreatSweep's DoPlaceClose / DoPlaceOpen calls (a list of
+        abi.cs_place_event)."""
+        ev = (abi.cs_place_event * len(events))(*events)
+        self._ck(self.lib.cs_gpu_place_events(self.ctx, ev, len(events)), "place_events")
+
+    def set_mcell_status(self, mcells, socdist=None, moverest=None):
+        """Microcell social-distancing / movement-restriction status (TreatStat) for
+        the listed microcells."""
+        m = np.ascontiguousarray(mcells, dtype=np.int32)
+        sd = None if socdist is None else np.ascontiguousarray(socdist, dtype=np.uint8)
+        mr = None if moverest is None else np.ascontiguousarray(moverest, dtype=np.uint8)
+        self._ck(self.lib.cs_gpu_set_mcell_status(self.ctx, m.ctypes.data, None if sd is None else sd.ctypes.data,
+                                                  None if mr is None else mr.ctypes.data, len(m)), "set_mcell_status")
+
     def counters(self):
         out = abi.cs_counters()
         self._ck(self.lib.cs_gpu_get_counters(self.ctx, C.byref(out)), "get_counters")

@@ -173,9 +173,15 @@ struct DevPop {
     int2* place_work;          // [N * NPT] (active index << 3 | place type, place) of each place pass
     uint8_t* hh_flag;          // [NH] deferred household actions
     int32_t* hh_list;          // [NH]
+    // households a place closure sends an adult home to (the host closure queue of
+    // DoPlaceClose, src/Update.cpp:1220-1231): window packed as
+    // (0xFFFF - start) << 16 | stop, 0 when none; listed once in carer_list
+    uint32_t* carer_win;       // [NH]
+    int32_t* carer_list;       // [NH]
     cs_counters* C;
 };
 
-enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntPlaceWork = 5, kCntEvents = 6, kCntN = 8 };
+enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntPlaceWork = 5, kCntEvents = 6,
+       kCntCarer = 7, kCntN = 8 };
 
 }  // namespace csb

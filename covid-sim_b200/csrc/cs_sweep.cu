@@ -219,6 +219,11 @@ struct cs_gpu_ctx {
     int day_every_step = -1;    // the probs_every_step the day graph was captured with
     long long geometry_gen = 0; // bumped when set_params replaces the kernel-row table
     size_t tp_smem[2] = {0, 0}; // dynamic shared memory enabled for k_tot_prob_rows<false>, <true>
+    // staging of cs_gpu_place_events / cs_gpu_set_mcell_status
+    cs_place_event* d_ev = nullptr;
+    int ev_cap = 0;
+    void* d_mc = nullptr;
+    size_t mc_cap = 0;
     cudaGraph_t day_graph = nullptr;
     cudaGraphExec_t day_exec = nullptr;
     long long day_launches = 0;
@@ -1615,6 +1620,115 @@ struct DayCtl {
     uint16_t a_close_start[CS_MAX_ADUNITS], a_close_stop[CS_MAX_ADUNITS];
 };
 
+// ------------------------------------------------------------ place closure
+// Is a living adult at home already (no workplace link, or quarantined)?  The test
+// DoPlaceClose and DoPlaceOpen make before sending an adult home with a child
+// (src/Update.cpp:1211-1215, 1278-1281).  It reads no absence times, so the
+// closures of one call may run in any order.
+__device__ bool adult_home_for_child(const DevPop& d, const cs_params& P, int hh, int ts)
+{
+    const HouseholdRec r = d.hhr[hh];
+    const int wp = P.PlaceTypeNoAirNum - 1;
+    for (int j = r.first; j < r.first + r.nh; j++) {
+        const PersonHot m = d.hot[j];
+        if (is_alive(m.inf) && m.age >= P.CaseAbsentChildAgeCutoff &&
+            (wp < 0 || link_of(d, wp, j) < 0 || host_quarantined(m, P, ts)))
+            return true;
+    }
+    return false;
+}
+
+// Queue household hh for an adult carer over [ws, we): the host closure queue of
+// DoPlaceClose (src/Update.cpp:1218-1231).  Windows of several closures merge as
+// UpdateHostClosure's min/max does; the household is listed once.
+__device__ void flag_carer(const DevPop& d, int hh, uint16_t ws, uint16_t we)
+{
+    if (ws >= we) return;
+    uint32_t* w = d.carer_win + hh;
+    const uint32_t add = ((uint32_t)(0xFFFFu - ws) << 16) | we;
+    uint32_t old = *w, assumed;
+    bool first = false;
+    do {
+        assumed = old;
+        const uint32_t nv = max(assumed & 0xFFFF0000u, add & 0xFFFF0000u) | max(assumed & 0xFFFFu, add & 0xFFFFu);
+        if (nv == assumed) break;
+        old = atomicCAS(w, assumed, nv);
+        first = (old == assumed) && assumed == 0u;
+    } while (old != assumed);
+    if (first) d.carer_list[append(d.counts + kCntCarer)] = hh;
+}
+
+// UpdateHostClosure (src/Update.cpp:1243-1258) for the households flag_carer
+// listed: the first living adult's absence covers the window.
+__device__ __forceinline__ void k_carer_pass_body(const DevPop& d)
+{
+    const cs_params& P = *d.P;
+    const int n = d.counts[kCntCarer];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int hh = d.carer_list[k];
+        const uint32_t win = d.carer_win[hh];
+        d.carer_win[hh] = 0u;
+        const uint16_t ws = (uint16_t)(0xFFFFu - (win >> 16)), we = (uint16_t)(win & 0xFFFFu);
+        const HouseholdRec r = d.hhr[hh];
+        for (int j = r.first; j < r.first + r.nh; j++) {
+            PersonHot* m = d.hot + j;
+            if (m->age >= P.CaseAbsentChildAgeCutoff && is_alive(m->inf)) {
+                if (m->absent_start > ws) m->absent_start = ws;
+                if (m->absent_stop < we) m->absent_stop = we;
+                break;
+            }
+        }
+    }
+}
+__global__ void k_carer_pass(DevPop d) { k_carer_pass_body(d); }
+__global__ void k_carer_pass_multi(const DevPop* __restrict__ pops) { k_carer_pass_body(pops[blockIdx.y]); }
+__global__ void k_carer_reset(DevPop d) { d.counts[kCntCarer] = 0; }
+__global__ void k_carer_reset_multi(const DevPop* __restrict__ pops) { pops[blockIdx.x].counts[kCntCarer] = 0; }
+
+// DoPlaceClose's loop over the members of a place that closed (src/Update.cpp:
+// 1196-1240) at timestep ts with absence window [ws, we), one block per place.  A
+// person is a member of one place per type, so the blocks of one launch (one place
+// type) write disjoint people; carers are only queued here.
+__device__ void close_place_members(const DevPop& d, const cs_params& P, int pt, int l, int ts, uint16_t ws, uint16_t we)
+{
+    const DevPlaces& pl = d.pl[pt];
+    const double att = P.PlaceClosePropAttending[pt];
+    for (int k = pl.member_ofs[l] + threadIdx.x; k < pl.member_ofs[l + 1]; k += blockDim.x) {
+        const int w = pl.members[k];
+        if (!((att == 0) || (d.prob_absent[w] >= att))) continue;
+        PersonHot* hw = d.hot + w;
+        const PersonHot h = *hw;
+        if (!host_absent(h, ts) && !host_quarantined(h, P, ts) && h.age < P.CaseAbsentChildAgeCutoff &&
+            d.prob_care[w] < P.CaseAbsentChildPropAdultCarers && !adult_home_for_child(d, P, h.hh, ts))
+            flag_carer(d, h.hh, ws, we);
+        if (h.absent_start > ws) hw->absent_start = ws;
+        if (h.absent_stop < we) hw->absent_stop = we;
+    }
+}
+
+// DoPlaceOpen (src/Update.cpp:1260-1294) for place l of type pt, whose closure
+// ends at ce > ts: absences that ended with the closure end at ts, also those of
+// adults who stayed home with a child of the place.
+__device__ void open_place_members(const DevPop& d, const cs_params& P, int pt, int l, int ts, uint16_t ce)
+{
+    const DevPlaces& pl = d.pl[pt];
+    for (int k = pl.member_ofs[l] + threadIdx.x; k < pl.member_ofs[l + 1]; k += blockDim.x) {
+        const int ai = pl.members[k];
+        PersonHot* ha = d.hot + ai;
+        if (ha->absent_stop == ce) ha->absent_stop = (uint16_t)ts;
+        if (!(d.prob_care[ai] < P.CaseAbsentChildPropAdultCarers)) continue;
+        const PersonHot h = *ha;
+        if (h.age >= P.CaseAbsentChildAgeCutoff || host_quarantined(h, P, ts) || adult_home_for_child(d, P, h.hh, ts)) continue;
+        const HouseholdRec r = d.hhr[h.hh];
+        for (int j = r.first; j < r.first + r.nh; j++) {
+            PersonHot* m = d.hot + j;
+            const PersonHot mh = *m;
+            if (mh.age >= P.CaseAbsentChildAgeCutoff && is_alive(mh.inf) && host_absent(mh, ts) && mh.absent_stop == ce)
+                m->absent_stop = (uint16_t)ts;
+        }
+    }
+}
+
 __device__ void k_close_places_body(const DevPop& d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop,
                                     const DayCtl* ctl)
 {
@@ -1654,15 +1768,48 @@ __device__ void k_close_places_body(const DevPop& d, int pt, const uint8_t* sel,
             }
         }
         __syncthreads();
-        if (do_members)
-            for (int k = pl.member_ofs[l] + threadIdx.x; k < pl.member_ofs[l + 1]; k += blockDim.x) {
-                int w = pl.members[k];
-                // a person can be a member of only one place per type: no race
-                PersonHot* hw = d.hot + w;
-                if (hw->absent_start > ws) hw->absent_start = ws;
-                if (hw->absent_stop < we) hw->absent_stop = we;
-            }
+        if (do_members) close_place_members(d, P, pt, l, ws, ws, we);
         __syncthreads();
+    }
+}
+
+// Outcomes of a host's DoPlaceClose / DoPlaceOpen calls (cs_gpu_place_events), one
+// block per event; every event of one launch has the same kind and place type.
+__global__ void k_place_events(DevPop d, const cs_place_event* __restrict__ ev, int n)
+{
+    const cs_params& P = *d.P;
+    for (int e = blockIdx.x; e < n; e += gridDim.x) {
+        const cs_place_event E = ev[e];
+        const DevPlaces& pl = d.pl[E.place_type];
+        if (E.kind == CS_PLACE_EV_CLOSE) {
+            if (threadIdx.x == 0) {
+                pl.close_start[E.place] = E.close_start;
+                pl.close_end[E.place] = E.close_end;
+                if (E.close_start < E.close_end) {
+                    atomicMin(d.close_window, (int32_t)E.close_start);
+                    atomicMax(d.close_window + 1, (int32_t)E.close_end);
+                }
+            }
+            if (E.members && P.DoRealSymptWithdrawal) close_place_members(d, P, E.place_type, E.place, E.ts, E.win_start, E.win_stop);
+        } else {
+            const uint16_t ce = pl.close_end[E.place];
+            __syncthreads();
+            if (E.ts < ce) {
+                if (P.DoRealSymptWithdrawal) open_place_members(d, P, E.place_type, E.place, E.ts, ce);
+                if (threadIdx.x == 0) pl.close_end[E.place] = E.ts;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Microcell status from a host's TreatSweep (cs_gpu_set_mcell_status).
+__global__ void k_mcell_status(DevPop d, const int32_t* __restrict__ m, const uint8_t* __restrict__ sd,
+                               const uint8_t* __restrict__ mr, int n)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        if (sd) d.socdist[m[k]] = sd[k];
+        if (mr) d.moverest[m[k]] = mr[k];
     }
 }
 __global__ void k_close_places(DevPop d, int pt, const uint8_t* sel, uint16_t start, uint16_t stop, const DayCtl* ctl)
@@ -1919,6 +2066,8 @@ static int alloc_dynamic(cs_gpu_ctx* c)
     AL(d.act, N); AL(d.act_cell, N); AL(d.cnt, NC); AL(d.cnt_ofs, N);
     AL(d.cmap, 2 * N); d.cmap_cap = (int32_t)(2 * N);
     AL(d.act_closed, N); AL(d.hh_flag, NH + 4); AL(d.hh_list, NH);
+    AL(d.carer_win, NH); AL(d.carer_list, NH);
+    CK(cudaMemsetAsync(d.carer_win, 0, sizeof(uint32_t) * NH, c->stream));
     AL(d.place_work, N * (size_t)(NPT > 0 ? NPT : 1));
     AL(d.close_window, 2);
     CK(cudaMemcpyAsync(d.close_window, kNoClosures, sizeof(kNoClosures), cudaMemcpyHostToDevice, c->stream));
@@ -2140,6 +2289,8 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     c->stat.reset();   // frees the static arrays when no replica still uses them
     if (c->xfer) cudaFree(c->xfer);
     if (c->d_seed_list) cudaFree(c->d_seed_list);
+    if (c->d_ev) cudaFree(c->d_ev);
+    if (c->d_mc) cudaFree(c->d_mc);
     cudaStream_t own = c->own_stream ? c->own_stream : c->stream;   // never a batch's stream
     if (own) cudaStreamDestroy(own);
     delete c;
@@ -2569,6 +2720,10 @@ static int enqueue_day(cs_gpu_ctx* c, int spd, bool every_step)
     LAUNCH(k_socdist_fill, mgrid, kThreads, d, (const DayCtl*)c->d_ctl);
     for (int pt = 0; pt < d.NPT; pt++)
         LAUNCH(k_close_places, c->grid, kThreads, d, pt, (const uint8_t*)nullptr, (uint16_t)0, (uint16_t)0, (const DayCtl*)c->d_ctl);
+    if (d.NPT > 0) {
+        LAUNCH(k_carer_pass, 64, kThreads, d);
+        LAUNCH(k_carer_reset, 1, 1, d);
+    }
     return CS_OK;
 }
 
@@ -2973,7 +3128,11 @@ static int batch_enqueue_day(cs_gpu_batch* b, int spd, bool every_step)
     const dim3 g(b->members[0]->grid, R);
     BLAUNCH(k_socdist_fill_multi, g, kThreads, pops, b->d_ctls);
     for (int pt = 0; pt < npt; pt++) BLAUNCH(k_close_places_multi, g, kThreads, pops, pt, b->d_ctls);
-    for (int k = 0; k < R; k++) b->member_day_launches[k] += 1 + b->members[k]->d.NPT;
+    if (npt > 0) {
+        BLAUNCH(k_carer_pass_multi, dim3(64, R), kThreads, pops);
+        BLAUNCH(k_carer_reset_multi, R, 1, pops);
+    }
+    for (int k = 0; k < R; k++) b->member_day_launches[k] += 1 + b->members[k]->d.NPT + (npt > 0 ? 2 : 0);
     return CS_OK;
 }
 
@@ -3135,12 +3294,83 @@ int cs_gpu_close_places(cs_gpu_ctx* c, int pt, const int32_t* mcells, int n_mcel
         CK(cudaMemcpyAsync(sel, h.data(), c->d.NM, cudaMemcpyHostToDevice, c->stream));
     }
     LAUNCH(k_close_places, c->grid, kThreads, c->d, pt, sel, start, stop, (const DayCtl*)nullptr);
+    LAUNCH(k_carer_pass, 64, kThreads, c->d);
+    LAUNCH(k_carer_reset, 1, 1, c->d);
     if (sel) {
         CK(cudaStreamSynchronize(c->stream));
         cudaFree(sel);
     }
     return CS_OK;
 }
+
+// Outcomes of a host TreatSweep's DoPlaceClose / DoPlaceOpen calls: opens first,
+// then closes, each kind place type by place type, so that one launch never has two
+// places of a person; the closures' carers follow the last close launch.
+int cs_gpu_place_events(cs_gpu_ctx* c, const cs_place_event* ev, int n)
+{
+    if (!c) return CS_E_ARG;
+    if (n < 0 || (n > 0 && !ev)) return set_err(c, CS_E_ARG, "bad event list");
+    if (n == 0) return CS_OK;
+    std::vector<cs_place_event> v(ev, ev + n);
+    for (const cs_place_event& e : v) {
+        if (e.place_type >= c->d.NPT || e.place < 0 || e.place >= c->d.pl[e.place_type].n)
+            return set_err(c, CS_E_ARG, "place event: place %d of type %d out of range", e.place, (int)e.place_type);
+        if (e.kind != CS_PLACE_EV_CLOSE && e.kind != CS_PLACE_EV_OPEN)
+            return set_err(c, CS_E_ARG, "place event: bad kind %d", (int)e.kind);
+    }
+    auto key = [](const cs_place_event& e) { return (e.kind == CS_PLACE_EV_OPEN ? 0 : 16) + (int)e.place_type; };
+    std::stable_sort(v.begin(), v.end(), [&](const cs_place_event& a, const cs_place_event& b) { return key(a) < key(b); });
+    if (c->ev_cap < n) {
+        if (c->d_ev) cudaFree(c->d_ev);
+        c->d_ev = nullptr;
+        c->ev_cap = 0;
+        CK(cudaMalloc(&c->d_ev, sizeof(cs_place_event) * (size_t)n));
+        c->ev_cap = n;
+    }
+    CK(cudaMemcpyAsync(c->d_ev, v.data(), sizeof(cs_place_event) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    bool closes = false;
+    for (int i0 = 0; i0 < n;) {
+        int i1 = i0;
+        while (i1 < n && key(v[i1]) == key(v[i0])) i1++;
+        LAUNCH(k_place_events, std::min(c->grid, i1 - i0), kThreads, c->d, c->d_ev + i0, i1 - i0);
+        closes |= v[i0].kind == CS_PLACE_EV_CLOSE;
+        i0 = i1;
+    }
+    if (closes) {
+        LAUNCH(k_carer_pass, 64, kThreads, c->d);
+        LAUNCH(k_carer_reset, 1, 1, c->d);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+int cs_gpu_set_mcell_status(cs_gpu_ctx* c, const int32_t* mcells, const uint8_t* socdist, const uint8_t* moverest, int n)
+{
+    if (!c) return CS_E_ARG;
+    if (n < 0 || (n > 0 && !mcells)) return set_err(c, CS_E_ARG, "bad microcell list");
+    if (n == 0 || (!socdist && !moverest)) return CS_OK;
+    for (int k = 0; k < n; k++)
+        if (mcells[k] < 0 || mcells[k] >= c->d.NM) return set_err(c, CS_E_ARG, "microcell %d out of range", mcells[k]);
+    const size_t need = (size_t)n * (4 + 2);
+    if (c->mc_cap < need) {
+        if (c->d_mc) cudaFree(c->d_mc);
+        c->d_mc = nullptr;
+        c->mc_cap = 0;
+        CK(cudaMalloc(&c->d_mc, need));
+        c->mc_cap = need;
+    }
+    int32_t* dm = (int32_t*)c->d_mc;
+    uint8_t* dsd = (uint8_t*)(dm + n);
+    uint8_t* dmr = dsd + n;
+    CK(cudaMemcpyAsync(dm, mcells, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    if (socdist) CK(cudaMemcpyAsync(dsd, socdist, (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    if (moverest) CK(cudaMemcpyAsync(dmr, moverest, (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    LAUNCH(k_mcell_status, std::max(1, std::min(c->grid, (n + kThreads - 1) / kThreads)), kThreads, c->d, dm,
+           socdist ? (const uint8_t*)dsd : nullptr, moverest ? (const uint8_t*)dmr : nullptr, n);
+    CK(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
 
 int cs_gpu_profile(cs_gpu_ctx* c, int enable)
 {
@@ -3357,14 +3587,10 @@ namespace {
 constexpr size_t kStaticCells = CS_STATIC_MAX_GRID_CELLS;
 constexpr size_t kStaticRows = CS_STATIC_MAX_GRID_ROWS;
 constexpr size_t kStaticBytes = 2 * sizeof(float) * kStaticCells + kStaticRows;
-constexpr int kStaticMaxDevices = 64;
 }  // namespace
 
 // [S0 on the grid: kStaticCells floats][numerators: kStaticCells floats][row flags]
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
-
-static std::mutex g_static_mu;
-static void* g_static_base[kStaticMaxDevices];  // device address of the array, per device
 
 extern "C" int cs_gpu_update_probs_static(cs_gpu_ctx* c, int do_place)
 {
@@ -3381,20 +3607,16 @@ extern "C" int cs_gpu_update_probs_static(cs_gpu_ctx* c, int do_place)
     if (dev != c->device)
         return set_err(c, CS_E_STATE, "update_probs_static: device %d is current, the context is on device %d",
                        dev, c->device);
-    if (dev < 0 || dev >= kStaticMaxDevices)
-        return set_err(c, CS_E_UNSUPPORTED, "update_probs_static: device ordinal %d above %d", dev, kStaticMaxDevices - 1);
-    // set-up, once per device, with that device current: the array's device address
-    void* base;
+    // The array's device address in the current context, looked up on every call
+    // (the lookup allocates nothing): a context made after a device reset, or
+    // another context on the same device, holds its own copy of the module.  The
+    // first lookup in a context loads the library's module there, which is why the
+    // first call should come before any stream capture.
+    void* base = nullptr;
     {
-        std::lock_guard<std::mutex> lock(g_static_mu);
-        if (!g_static_base[dev]) {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-            if (e != cudaSuccess || !p)
-                return set_err(c, CS_E_CUDA, "update_probs_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-            g_static_base[dev] = p;
-        }
-        base = g_static_base[dev];
+        cudaError_t e = cudaGetSymbolAddress(&base, g_static_scratch);
+        if (e != cudaSuccess || !base)
+            return set_err(c, CS_E_CUDA, "update_probs_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
     }
     float* S0g = (float*)base;
     float* Ag = S0g + kStaticCells;
@@ -3405,19 +3627,24 @@ extern "C" int cs_gpu_update_probs_static(cs_gpu_ctx* c, int do_place)
     CK(cudaMemsetAsync(S0g, 0, sizeof(float) * G, c->stream));
     CK(cudaMemsetAsync(rowS, 0, P.nch, c->stream));
     const int cgrid = (d.NC + kThreads - 1) / kThreads;
-    k_update_S0<<<cgrid, kThreads, 0, c->stream>>>(d, do_place);
-    k_grid_values<<<cgrid, kThreads, 0, c->stream>>>(d, S0g, nullptr, rowS, nullptr);
-    const TotProbGeom gm = tot_prob_geom(P.ncw, P.nch, false);   // all row chunks in one block
+    LAUNCH(k_update_S0, cgrid, kThreads, d, do_place);
+    LAUNCH(k_grid_values, cgrid, kThreads, d, S0g, (float*)nullptr, rowS, (uint8_t*)nullptr);
+    // All row chunks of a column block run in one block (grid z = 1): the chunked
+    // form's per-chunk partial sums would need nchunks x G more floats of scratch.
+    const TotProbGeom gm = tot_prob_geom(P.ncw, P.nch, false);
     dim3 grid;
     int tpb;
     tot_prob_launch_shape(P.ncw, P.nch, gm, &grid, &tpb);
     const size_t smem = gm.smem(false);
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_tot_prob_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int r = tot_prob_smem(c, false, smem);
+    if (r) return r;
+    if (c->prof) prof_begin(c, "k_tot_prob_rows_static");
     k_tot_prob_rows<false><<<grid, tpb, smem, c->stream>>>(d, S0g, nullptr, rowS, nullptr, Ag, nullptr, gm, c->Gtab);
-    k_tot_prob_finish<<<cgrid, kThreads, 0, c->stream>>>(d, Ag, c->Bg);
-    k_block_S0<<<(d.NB + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);
-    k_block_rows<<<(d.NB * 32 + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(d);
-    c->launches += 6;
+    if (c->prof) prof_end(c);
+    c->launches++;
     CK(cudaGetLastError());
+    LAUNCH(k_tot_prob_finish, cgrid, kThreads, d, Ag, c->Bg);
+    LAUNCH(k_block_S0, (d.NB + kThreads - 1) / kThreads, kThreads, d);
+    LAUNCH(k_block_rows, (d.NB * 32 + kThreads - 1) / kThreads, kThreads, d);
     return CS_OK;
 }

@@ -16,12 +16,26 @@
 //   every step           run the device sweeps, then copy back what RecordSample
 //                        reads: per-cell S/L/I/R/D and the StateT counters;
 //   UpdateProbs          noticed through a change of the host cells' S0, then
-//                        recomputed on the device from the device's own counts.
+//                        recomputed on the device from the device's own counts;
+//   interventions        the host's own trigger logic (RecordSample's start times,
+//                        src/CovidSim.cpp:3598-3649) and TreatSweep
+//                        (src/Sweep.cpp:1324-2004) keep running on the host; before
+//                        each step what they changed is handed to the device: the
+//                        parameter block (ControlPropCasesId, efficacies, CFR
+//                        scales), each admin unit's case-isolation and household-
+//                        quarantine start times, the microcells' social-distancing
+//                        and movement-restriction status, and the outcome of every
+//                        DoPlaceClose / DoPlaceOpen call TreatSweep made.  Those two
+//                        calls reach this file because the drop-in compiles Sweep.cpp
+//                        with them renamed (oracle/Makefile), as it does the sweeps.
 //
 // Features outside the device sweep (digital contact tracing, airports, blanket
-// movement restrictions, treatment/vaccination, false positives, holidays, and the
-// host's own intervention triggers) stop the run with ERR_CRITICAL, the reference's
-// own failure convention, rather than silently computing something else.
+// movement restrictions, treatment/vaccination/key-worker prophylaxis, false
+// positives, holidays, intervention delays by admin unit, and triggers counted per
+// microcell or place rather than globally or per admin unit) stop the run with
+// ERR_CRITICAL, the reference's own failure convention, rather than silently
+// computing something else -- at set-up when the parameters rule them in, else at
+// the first step at which they could act.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -35,6 +49,7 @@
 #include "Model.h"
 #include "Param.h"
 #include "Sweep.h"
+#include "Update.h"
 
 #include "covidsim_b200.h"
 
@@ -47,6 +62,12 @@ long long g_s0_sig = -1;
 int64_t g_tg_base = 0, g_si_base = 0, g_ntg_base = 0, g_tg_set = 0, g_si_set = 0, g_ntg_set = 0;
 std::vector<int32_t> g_S, g_L, g_I, g_R, g_D;
 cs_params g_params;
+// what the device holds of the host's intervention state
+std::vector<uint8_t> g_sd, g_mr;              // per microcell: socdist, moverest (TreatStat)
+std::vector<double> g_ci_start, g_hq_start;   // per admin unit start times
+double g_ci_dur = -1, g_hq_dur = -1;
+bool g_iv_sent = false;
+std::vector<cs_place_event> g_events;         // TreatSweep's closures since the last step
 
 void check(int rc, const char* what)
 {
@@ -143,6 +164,8 @@ cs_params params_from_reference()
     p.CaseIsolationProp = P.CaseIsolationProp; p.HQuarantinePropHouseCompliant = P.HQuarantinePropHouseCompliant;
     p.HQuarantinePropIndivCompliant = P.HQuarantinePropIndivCompliant; p.HQuarantineDelay = P.HQuarantineDelay;
     p.CaseAbsentChildPropAdultCarers = P.CaseAbsentChildPropAdultCarers;
+    for (int t = 0; t < MAX_NUM_PLACE_TYPES; t++)
+        p.PlaceClosePropAttending[t] = (t < P.NumPlaceTypes) ? P.PlaceClosePropAttending[t] : 0.0;
     p.usCaseIsolationDelay = P.usCaseIsolationDelay; p.usCaseIsolationDuration = P.usCaseIsolationDuration;
     p.usCaseAbsenteeismDelay = P.usCaseAbsenteeismDelay; p.usCaseAbsenteeismDuration = P.usCaseAbsenteeismDuration;
     p.usHQuarantineHouseDuration = P.usHQuarantineHouseDuration;
@@ -165,6 +188,29 @@ void unsupported_features()
     if (P.DoBlanketMoveRestr) ERR_CRITICAL("GPU sweep: blanket movement restrictions are not supported\n");
     if (P.FalsePositiveRate > 0) ERR_CRITICAL("GPU sweep: false-positive cases are not supported\n");
     if (P.DoHolidays && P.NumHolidays > 0) ERR_CRITICAL("GPU sweep: holidays are not supported\n");
+    if (P.DoInterventionDelaysByAdUnit) ERR_CRITICAL("GPU sweep: intervention delays by admin unit are not supported\n");
+    if (P.DoAdUnits && P.DoAdminTriggers && P.NumAdunits > CS_MAX_ADUNITS)
+        ERR_CRITICAL_FMT("GPU sweep: admin-unit triggers over more than %d admin units are not supported\n", CS_MAX_ADUNITS);
+}
+
+// Host interventions the device does not model, checked at each step against the
+// host's current start times (t is the time of the TreatSweep that just ran).
+void unsupported_at(double t)
+{
+    if (t >= P.TreatTimeStart) ERR_CRITICAL("GPU sweep: treatment is not supported\n");
+    if (t >= P.VaccTimeStart || t >= P.VaccTimeStartGeo) ERR_CRITICAL("GPU sweep: vaccination is not supported\n");
+    if (t >= P.KeyWorkerProphTimeStart) ERR_CRITICAL("GPU sweep: key-worker prophylaxis is not supported\n");
+    const bool any = t >= P.PlaceCloseTimeStart || t >= P.SocDistTimeStart || t >= P.MoveRestrTimeStart;
+    if (any && !P.DoGlobalTriggers && !P.DoAdminTriggers)
+        ERR_CRITICAL("GPU sweep: triggers counted per microcell are not supported (use global or admin-unit triggers)\n");
+    // DoDetectedCase's and DoCase's own place closures (src/Update.cpp:544-560, 821-830)
+    if (t >= P.PlaceCloseTimeStart && P.DoPlaces) {
+        if (!P.AbsenteeismPlaceClosure && !P.DoAdminTriggers && !(P.DoGlobalTriggers && P.PlaceCloseCellIncThresh < 1000000000))
+            ERR_CRITICAL("GPU sweep: place closure by detected cases is not supported\n");
+        if (P.AbsenteeismPlaceClosure && !P.DoAdminTriggers && !P.DoGlobalTriggers)
+            ERR_CRITICAL("GPU sweep: place closure by absenteeism is not supported\n");
+        if (P.PlaceCloseByAdminUnit) ERR_CRITICAL("GPU sweep: place closure by admin-unit case proportions is not supported\n");
+    }
 }
 
 void create_context()
@@ -322,6 +368,12 @@ void upload_run_state(int run)
     for (int j = 1; j < P.NumThreads; j++)
         if (StateT[j].cumI || StateT[j].cumC) ERR_CRITICAL("GPU sweep: host counters outside thread 0 at run start\n");
     std::memcpy(&g_base, &StateT[0], sizeof(PopVar));
+    // the upload reset the device's closures, microcell status and windows, as
+    // InitModel reset the host's
+    g_sd.assign(P.NumMicrocells, (uint8_t)CS_TREAT_UNTREATED);
+    g_mr.assign(P.NumMicrocells, (uint8_t)CS_TREAT_UNTREATED);
+    g_iv_sent = false;
+    g_events.clear();
     g_s0_sig = s0_signature();
     g_tg_base = g_si_base = g_ntg_base = 0;
     g_tg_set = g_si_set = g_ntg_set = 0;
@@ -358,19 +410,84 @@ void sync_back()
         s.cumI_keyworker[i] = b.cumI_keyworker[i] + (int)k.cumI_keyworker[i];
         s.cumC_keyworker[i] = b.cumC_keyworker[i] + (int)k.cumC_keyworker[i];
     }
+    // per admin unit: what RecordSample's admin-unit triggers and tables read
+    // (src/CovidSim.cpp:3433-3450)
+    if (P.DoAdUnits)
+        for (int a = 0; a < P.NumAdunits && a < CS_MAX_ADUNITS; a++) {
+            s.cumI_adunit[a] = b.cumI_adunit[a] + (int)k.cumI_adunit[a];
+            s.cumC_adunit[a] = b.cumC_adunit[a] + (int)k.cumC_adunit[a];
+            s.cumD_adunit[a] = b.cumD_adunit[a] + (int)k.cumD_adunit[a];
+            s.cumDC_adunit[a] = b.cumDC_adunit[a] + (int)k.cumDC_adunit[a];
+            s.cumCritical_adunit[a] = b.cumCritical_adunit[a] + (int)k.cumCritical_adunit[a];
+            s.Critical_adunit[a] = b.Critical_adunit[a] + (int)k.Critical_adunit[a];
+        }
     // generation-time sums are read and zeroed by each RecordSample: hand over increments
     if (s.cumTG != g_tg_set || s.nTG != g_ntg_set) { g_tg_base += g_tg_set; g_si_base += g_si_set; g_ntg_base += g_ntg_set; }
     g_tg_set = k.cumTG - g_tg_base; g_si_set = k.cumSI - g_si_base; g_ntg_set = k.nTG - g_ntg_base;
     s.cumTG = (int)g_tg_set; s.cumSI = (int)g_si_set; s.nTG = (int)g_ntg_set;
 }
 
-void interventions_idle()
+// Everything the host's run loop changed between two sweeps that the device sweep
+// reads, handed over before the next sweep (t is the coming step's time).
+void mirror_host_interventions(double t)
 {
-    // the host's trigger logic runs in TreatSweep; this drop-in supports runs in which
-    // it never switches an intervention on
-    for (int m = 0; m < P.NumMicrocells; m++)
-        if (Mcells[m].socdist == TreatStat::Treated || Mcells[m].moverest == TreatStat::Treated)
-            ERR_CRITICAL("GPU sweep: microcell interventions switched on by the host are not supported by this drop-in\n");
+    const double t_prev = t - P.ModelTimeStep;   // the time TreatSweep last ran at
+    if (t_prev >= 0) unsupported_at(t_prev);
+    // the parameter block: ControlPropCasesId after the alert, efficacies varied over
+    // time, CFR scales (UpdateCFRs), seasonality
+    cs_params cur = params_from_reference();
+    cur.kernel_delta = g_params.kernel_delta;
+    cur.Seasonality = P.DoSeasonality ? P.Seasonality[((int)t) % DAYS_PER_YEAR] : 1.0;
+    if (std::memcmp(&cur, &g_params, sizeof(cs_params)) != 0) {
+        g_params = cur;
+        check(cs_gpu_set_params(g_ctx, &g_params), "cs_gpu_set_params");
+    }
+    // case isolation and household quarantine windows of each admin unit
+    // (RecordSample, src/CovidSim.cpp:3598-3609; read by DoDetectedCase)
+    const int na = P.NumAdunits > 0 ? P.NumAdunits : 1;
+    bool iv = !g_iv_sent || g_ci_dur != P.CaseIsolationPolicyDuration || g_hq_dur != P.HQuarantinePolicyDuration;
+    g_ci_start.resize(na);
+    g_hq_start.resize(na);
+    for (int a = 0; a < na; a++) {
+        const double ci = P.NumAdunits > 0 ? AdUnits[a].CaseIsolationTimeStart : 1e10;
+        const double hq = P.NumAdunits > 0 ? AdUnits[a].HQuarantineTimeStart : 1e10;
+        iv |= ci != g_ci_start[a] || hq != g_hq_start[a];
+        g_ci_start[a] = ci;
+        g_hq_start[a] = hq;
+    }
+    if (iv) {
+        cs_interventions w;
+        std::memset(&w, 0, sizeof(w));
+        w.CaseIsolationPolicyDuration = g_ci_dur = P.CaseIsolationPolicyDuration;
+        w.HQuarantinePolicyDuration = g_hq_dur = P.HQuarantinePolicyDuration;
+        w.CaseIsolationTimeStart = g_ci_start[0];
+        w.HQuarantineTimeStart = g_hq_start[0];
+        w.adunit_CaseIsolationTimeStart = g_ci_start.data();
+        w.adunit_HQuarantineTimeStart = g_hq_start.data();
+        check(cs_gpu_set_interventions(g_ctx, &w), "cs_gpu_set_interventions");
+        g_iv_sent = true;
+    }
+    // microcell status: TreatSweep changes it only from the start times on
+    const bool sd = t_prev >= P.SocDistTimeStart, mr = t_prev >= P.MoveRestrTimeStart;
+    if (sd || mr) {
+        std::vector<int32_t> ms;
+        std::vector<uint8_t> vs, vm;
+        for (int i = 0; i < P.NumPopulatedMicrocells; i++) {
+            const int m = (int)(McellLookup[i] - Mcells);
+            const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
+            if (a == g_sd[m] && b == g_mr[m]) continue;
+            ms.push_back(m);
+            vs.push_back(g_sd[m] = a);
+            vm.push_back(g_mr[m] = b);
+        }
+        if (!ms.empty())
+            check(cs_gpu_set_mcell_status(g_ctx, ms.data(), vs.data(), vm.data(), (int)ms.size()), "cs_gpu_set_mcell_status");
+    }
+    // the closures and openings TreatSweep made
+    if (!g_events.empty()) {
+        check(cs_gpu_place_events(g_ctx, g_events.data(), (int)g_events.size()), "cs_gpu_place_events");
+        g_events.clear();
+    }
 }
 
 }  // namespace
@@ -385,16 +502,52 @@ void InfectSweep(double t, int run)
         check(cs_gpu_update_probs(g_ctx, 0), "cs_gpu_update_probs");  // the host ran UpdateProbs(0)
         g_s0_sig = s0_signature();
     }
-    if (P.DoSeasonality) {
-        double seas = P.Seasonality[((int)t) % DAYS_PER_YEAR];
-        if (seas != g_params.Seasonality) {
-            g_params.Seasonality = seas;
-            check(cs_gpu_set_params(g_ctx, &g_params), "cs_gpu_set_params");
-        }
-    }
-    if (((int)(t * P.TimeStepsPerDay)) % ((int)P.TimeStepsPerDay) == 0) interventions_idle();
+    mirror_host_interventions(t);
     check(cs_gpu_infect_sweep(g_ctx, t, run), "cs_gpu_infect_sweep");
 }
+// TreatSweep's place closures (src/Sweep.cpp:1686, 1733): the drop-in's Sweep.cpp
+// calls these in place of DoPlaceClose / DoPlaceOpen.  Each runs the reference's own
+// function on the host's Places, so the host's place state and its outputs stay the
+// reference's, and records the outcome for the device.  Members' absences are the
+// device's to apply (the host's person records are not current between steps).
+// Called from TreatSweep's OpenMP threads, one microcell's places per thread.
+void cs_shim_DoPlaceClose(int i, int j, unsigned short int TimeStepNow, int tn, int DoAnyway)
+{
+    if (!DoAnyway) ERR_CRITICAL("GPU sweep: place closure by case counts is not supported\n");
+    Place& pl = Places[i][j];
+    const unsigned short int ce0 = pl.close_end_time;
+    DoPlaceClose(i, j, TimeStepNow, tn, DoAnyway);
+    if (pl.close_end_time == ce0) return;   // DoPlaceClose changes close_end_time whenever it acts
+    cs_place_event e;
+    std::memset(&e, 0, sizeof(e));
+    e.place = j;
+    e.place_type = (uint8_t)i;
+    e.kind = CS_PLACE_EV_CLOSE;
+    e.members = pl.ProbClose >= P.Efficacies[PlaceClosure][i];   // HasPlaceClosed (src/Update.cpp:1178)
+    e.ts = TimeStepNow;
+    e.close_start = pl.close_start_time;
+    e.close_end = pl.close_end_time;
+    e.win_start = (uint16_t)(TimeStepNow + ((unsigned short int)(P.TimeStepsPerDay * P.PlaceCloseDelayMean)));
+    e.win_stop = (uint16_t)(TimeStepNow + ((unsigned short int)(P.TimeStepsPerDay * (P.PlaceCloseDelayMean + P.PlaceCloseDuration))));
+#pragma omp critical(cs_shim_place_events)
+    g_events.push_back(e);
+}
+
+void cs_shim_DoPlaceOpen(int i, int j, unsigned short int TimeStepNow)
+{
+    const unsigned short int ce0 = Places[i][j].close_end_time;
+    DoPlaceOpen(i, j, TimeStepNow);
+    if (!(TimeStepNow < ce0)) return;
+    cs_place_event e;
+    std::memset(&e, 0, sizeof(e));
+    e.place = j;
+    e.place_type = (uint8_t)i;
+    e.kind = CS_PLACE_EV_OPEN;
+    e.ts = TimeStepNow;
+#pragma omp critical(cs_shim_place_events)
+    g_events.push_back(e);
+}
+
 
 void IncubRecoverySweep(double t)
 {

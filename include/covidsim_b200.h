@@ -34,7 +34,9 @@
 extern "C" {
 #endif
 
-#define CS_ABI_VERSION 2            /* 2: per admin unit windows in cs_interventions, cs_run_policy */
+#define CS_ABI_VERSION 3            /* 2: per admin unit windows in cs_interventions, cs_run_policy;
+                                       3: PlaceClosePropAttending, cs_gpu_place_events,
+                                          cs_gpu_set_mcell_status */
 
 /* Sizes fixed by the reference (src/Constants.h, src/Country.h). */
 #define CS_MAX_PLACE_TYPES 5        /* MAX_NUM_PLACE_TYPES   (Country.h:15)   */
@@ -197,6 +199,7 @@ typedef struct cs_params {
     /* interventions consumed inside the sweep (DoCase/DoDetectedCase) */
     double CaseIsolationProp, HQuarantinePropHouseCompliant, HQuarantinePropIndivCompliant;
     double HQuarantineDelay, CaseAbsentChildPropAdultCarers;
+    double PlaceClosePropAttending[CS_MAX_PLACE_TYPES]; /* DoPlaceClose's attendance filter */
     uint16_t usCaseIsolationDelay, usCaseIsolationDuration, usCaseAbsenteeismDelay;
     uint16_t usCaseAbsenteeismDuration, usHQuarantineHouseDuration, _pad1[3];
     /* geometry: degrees relative to the bounding box's bottom-left corner */
@@ -394,8 +397,9 @@ int cs_gpu_update_probs(cs_gpu_ctx* ctx, int do_place);
  * scratch is one fixed array inside the library, 2 x 4 B x CS_STATIC_MAX_GRID_CELLS
  * + CS_STATIC_MAX_GRID_ROWS bytes (4.0 MiB), per device; grids with more cells or
  * rows are rejected with CS_E_RANGE.  The context's device must be current
- * (CS_E_STATE otherwise).  The first call on a device does the set-up (looking up
- * the array's device address), so make it before any stream capture.  All calls
+ * (CS_E_STATE otherwise).  Each call looks up the array's device address in the
+ * current CUDA context (a lookup, no allocation); the first call in a context also
+ * loads the library's device code there, so make it before any stream capture.  All calls
  * on one device share that array: calls that overlap in time, from two contexts
  * or two streams, race on it and must be serialised by the caller. */
 #define CS_STATIC_MAX_GRID_CELLS 524288
@@ -481,10 +485,50 @@ int cs_sur_train_step(cs_sur* sur, const float* x, const float* target, int n, f
 int cs_sur_set_gemm(cs_sur* sur, int impl);
 
 int cs_gpu_set_interventions(cs_gpu_ctx* ctx, const cs_interventions* iv);
-/* DoPlaceClose (src/Update.cpp:1095-1258) for every place of type t in the listed
- * microcells (all when mcells == NULL), closing [start, stop) in timesteps. */
+/* DoPlaceClose with DoAnyway = 1 (src/Update.cpp:1095-1240, as TreatSweep calls it
+ * at src/Sweep.cpp:1730-1733) for every place of type t in the listed microcells
+ * (all when mcells == NULL), closing [start, stop) in timesteps: a place closes if
+ * its ProbClose passes Efficacies[PlaceClosure][t]; then each member attending
+ * (PlaceClosePropAttending) is made absent over [start, stop) and, for a child at
+ * home with no adult there, the household's first living adult too (the host
+ * closure queue, applied as UpdateHostClosure does, src/Update.cpp:1243-1258).
+ * Members' states are evaluated at timestep `start`. */
 int cs_gpu_close_places(cs_gpu_ctx* ctx, int place_type, const int32_t* mcells, int n_mcells,
                         uint16_t start, uint16_t stop);
+
+/*
+ * Place closures decided by a host's own TreatSweep.  A host that keeps the
+ * reference's TreatSweep (src/Sweep.cpp:1324-2004) records each call it makes of
+ * DoPlaceClose (DoAnyway = 1) and DoPlaceOpen (src/Update.cpp:1095-1240, 1260-1294)
+ * and hands the outcomes over before the next sweep.  For a close the context sets
+ * the place's window to the host's result (close_start, close_end) and, when the
+ * place closed (HasPlaceClosed), runs DoPlaceClose's member loop over [win_start,
+ * win_stop) at timestep ts, as cs_gpu_close_places does.  For an open it runs
+ * DoPlaceOpen at ts on its own copy of the place (which equals the host's when
+ * every close was handed over).  Opens are applied before closes, and each kind
+ * place type by place type; the carers' absences follow the last close.  Hand
+ * over the events of one host timestep per call.
+ */
+#define CS_PLACE_EV_CLOSE 1
+#define CS_PLACE_EV_OPEN 2
+typedef struct cs_place_event {
+    int32_t place;                     /* index within its type (Places[place_type][place]) */
+    uint8_t place_type;
+    uint8_t kind;                      /* CS_PLACE_EV_CLOSE or CS_PLACE_EV_OPEN */
+    uint8_t members;                   /* close: 1 when the place closed (its members' loop runs) */
+    uint8_t _pad0;
+    uint16_t ts;                       /* TimeStepNow of the host's call */
+    uint16_t close_start, close_end;   /* close: the place's window after the host's call */
+    uint16_t win_start, win_stop;      /* close: t_start_place_close, t_stop_place_close */
+    uint16_t _pad1;
+} cs_place_event;
+int cs_gpu_place_events(cs_gpu_ctx* ctx, const cs_place_event* events, int n);
+
+/* Microcell status a host's TreatSweep set (Microcell::socdist and ::moverest,
+ * TreatStat values) for the n listed microcells; either array may be NULL to leave
+ * that status unchanged.  The sparse form of cs_interventions' full arrays. */
+int cs_gpu_set_mcell_status(cs_gpu_ctx* ctx, const int32_t* mcells, const uint8_t* socdist,
+                            const uint8_t* moverest, int n);
 
 /* Copy the device counter block (cumulative since the run began). */
 int cs_gpu_get_counters(cs_gpu_ctx* ctx, cs_counters* out);

@@ -87,6 +87,7 @@ struct cs_cpu_ctx {
     /* per step scratch */
     uint64_t* claim;
     uint8_t *hh_carer, *hh_hq;
+    uint16_t *carer_start, *carer_stop;   /* [NH] place-closure carers' windows (start > stop: none) */
     /* run */
     uint64_t seed;
     int run_started;
@@ -611,6 +612,8 @@ int cs_cpu_create(const cs_population* pop, const cs_params* params, cs_cpu_ctx*
     ALLOC(c->socdist, c->NM, uint8_t); ALLOC(c->moverest, c->NM, uint8_t);
     ALLOC(c->claim, c->N, uint64_t);
     ALLOC(c->hh_carer, c->NH, uint8_t); ALLOC(c->hh_hq, c->NH, uint8_t);
+    ALLOC(c->carer_start, c->NH, uint16_t); ALLOC(c->carer_stop, c->NH, uint16_t);
+    for (int h = 0; h < c->NH; h++) c->carer_start[h] = 0xFFFF;
     ALLOC(c->ci_start, c->NAD, double); ALLOC(c->hq_start, c->NAD, double);
     for (int a = 0; a <= c->NAD; a++) c->ci_start[a] = c->hq_start[a] = 1e10;
     for (int i = 0; i < c->N; i++) c->claim[i] = UINT64_MAX;
@@ -630,7 +633,7 @@ void cs_cpu_destroy(cs_cpu_ctx* c)
                     c->prob_absent, c->prob_care, c->infector, c->listpos, c->infect_type, c->S, c->L, c->I,
                     c->R, c->D, c->S0, c->tot_prob, c->slots, c->mark, c->socdist, c->moverest, c->claim,
                     c->hh_carer, c->hh_hq, c->cell_block, c->block_cell_ofs, c->block_cells, c->block_cum,
-                    c->block_S0, c->block_row_cum, c->ci_start, c->hq_start};
+                    c->block_S0, c->block_row_cum, c->ci_start, c->hq_start, c->carer_start, c->carer_stop};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     for (int t = 0; t < c->NPT; t++) {
         place_arrays* p = &c->pl[t];
@@ -1500,9 +1503,86 @@ int cs_cpu_set_interventions(cs_cpu_ctx* c, const cs_interventions* iv)
     return CS_OK;
 }
 
-/* DoPlaceClose (src/Update.cpp:1095-1258) with DoAnyway = 1 for the listed
- * microcells: close the place if its ProbClose passes the efficacy, and move its
- * members' absence windows (symptomatic withdrawal model). */
+/* Is a living adult at home already (no workplace link, or quarantined)?  The test
+ * DoPlaceClose and DoPlaceOpen make before sending an adult home with a child
+ * (src/Update.cpp:1211-1215, 1278-1281). */
+static int adult_home_for_child(const cs_cpu_ctx* c, int h, int ts)
+{
+    const cs_params* P = &c->P;
+    const int wp = P->PlaceTypeNoAirNum - 1;
+    for (int j = c->hh_first[h]; j < c->hh_first[h] + c->hh_nh[h]; j++)
+        if (is_alive(c, j) && c->age[j] >= P->CaseAbsentChildAgeCutoff &&
+            (wp < 0 || link_of(c, wp, j) < 0 || host_quarantined(c, j, ts)))
+            return 1;
+    return 0;
+}
+
+/* The host closure queue of DoPlaceClose (src/Update.cpp:1218-1231), one window per
+ * household merged by min/max, and its application by UpdateHostClosure
+ * (src/Update.cpp:1243-1258) to the household's first living adult. */
+static void queue_carer(cs_cpu_ctx* c, int h, uint16_t ws, uint16_t we)
+{
+    if (ws >= we) return;
+    if (c->carer_start[h] > ws) c->carer_start[h] = ws;
+    if (c->carer_stop[h] < we) c->carer_stop[h] = we;
+}
+
+static void carer_queue_apply(cs_cpu_ctx* c)
+{
+    const cs_params* P = &c->P;
+    for (int h = 0; h < c->NH; h++) {
+        if (c->carer_start[h] >= c->carer_stop[h]) continue;
+        const uint16_t ws = c->carer_start[h], we = c->carer_stop[h];
+        c->carer_start[h] = 0xFFFF;
+        c->carer_stop[h] = 0;
+        for (int j = c->hh_first[h]; j < c->hh_first[h] + c->hh_nh[h]; j++)
+            if (c->age[j] >= P->CaseAbsentChildAgeCutoff && is_alive(c, j)) {
+                if (c->absent_start[j] > ws) c->absent_start[j] = ws;
+                if (c->absent_stop[j] < we) c->absent_stop[j] = we;
+                break;
+            }
+    }
+}
+
+/* DoPlaceClose's loop over the members of a place that closed (src/Update.cpp:
+ * 1196-1240) at timestep ts with absence window [ws, we). */
+static void close_place_members(cs_cpu_ctx* c, int pt, int l, int ts, uint16_t ws, uint16_t we)
+{
+    const cs_params* P = &c->P;
+    place_arrays* pl = &c->pl[pt];
+    const double att = P->PlaceClosePropAttending[pt];
+    for (int k = pl->member_ofs[l]; k < pl->member_ofs[l + 1]; k++) {
+        const int w = pl->members[k];
+        if (!((att == 0) || (c->prob_absent[w] >= att))) continue;
+        if (!host_absent(c, w, ts) && !host_quarantined(c, w, ts) && c->age[w] < P->CaseAbsentChildAgeCutoff &&
+            c->prob_care[w] < P->CaseAbsentChildPropAdultCarers && !adult_home_for_child(c, c->hh[w], ts))
+            queue_carer(c, c->hh[w], ws, we);
+        if (c->absent_start[w] > ws) c->absent_start[w] = ws;
+        if (c->absent_stop[w] < we) c->absent_stop[w] = we;
+    }
+}
+
+/* DoPlaceOpen (src/Update.cpp:1260-1294) for place l of type pt, whose closure ends
+ * at ce > ts. */
+static void open_place_members(cs_cpu_ctx* c, int pt, int l, int ts, uint16_t ce)
+{
+    const cs_params* P = &c->P;
+    place_arrays* pl = &c->pl[pt];
+    for (int k = pl->member_ofs[l]; k < pl->member_ofs[l + 1]; k++) {
+        const int ai = pl->members[k];
+        if (c->absent_stop[ai] == ce) c->absent_stop[ai] = (uint16_t)ts;
+        if (!(c->prob_care[ai] < P->CaseAbsentChildPropAdultCarers)) continue;
+        if (c->age[ai] >= P->CaseAbsentChildAgeCutoff || host_quarantined(c, ai, ts) || adult_home_for_child(c, c->hh[ai], ts))
+            continue;
+        for (int j = c->hh_first[c->hh[ai]]; j < c->hh_first[c->hh[ai]] + c->hh_nh[c->hh[ai]]; j++)
+            if (c->age[j] >= P->CaseAbsentChildAgeCutoff && is_alive(c, j) && host_absent(c, j, ts) && c->absent_stop[j] == ce)
+                c->absent_stop[j] = (uint16_t)ts;
+    }
+}
+
+/* DoPlaceClose (src/Update.cpp:1095-1240) with DoAnyway = 1 for the listed
+ * microcells: close the place if its ProbClose passes the efficacy, run the member
+ * loop (symptomatic withdrawal model) at timestep `start`, then the carers. */
 int cs_cpu_close_places(cs_cpu_ctx* c, int pt, const int32_t* mcells, int n_mcells, uint16_t start, uint16_t stop)
 {
     const cs_params* P = &c->P;
@@ -1519,16 +1599,59 @@ int cs_cpu_close_places(cs_cpu_ctx* c, int pt, const int32_t* mcells, int n_mcel
         if (pl->prob_close[l] >= P->Efficacies[CS_NPI_PLACE_CLOSURE][pt]) {
             if (pl->close_start[l] > start) pl->close_start[l] = start;
             pl->close_end[l] = stop;
-            if (P->DoRealSymptWithdrawal)
-                for (int k = pl->member_ofs[l]; k < pl->member_ofs[l + 1]; k++) {
-                    int w = pl->members[k];
-                    if (c->absent_start[w] > start) c->absent_start[w] = start;
-                    if (c->absent_stop[w] < stop) c->absent_stop[w] = stop;
-                }
+            if (P->DoRealSymptWithdrawal) close_place_members(c, pt, l, start, start, stop);
         } else
             pl->close_start[l] = pl->close_end[l] = stop;
     }
+    carer_queue_apply(c);
     free(sel);
+    return CS_OK;
+}
+
+/* The outcomes of a host TreatSweep's DoPlaceClose / DoPlaceOpen calls, in the order
+ * the GPU library applies them: opens, then closes, each place type by place type
+ * (events of one kind and type in the order given), then the closures' carers. */
+int cs_cpu_place_events(cs_cpu_ctx* c, const cs_place_event* ev, int n)
+{
+    const cs_params* P = &c->P;
+    if (n < 0 || (n > 0 && !ev)) return fail(c, CS_E_ARG, "bad event list");
+    for (int i = 0; i < n; i++) {
+        if (ev[i].place_type >= c->NPT || ev[i].place < 0 || ev[i].place >= c->pl[ev[i].place_type].n)
+            return fail(c, CS_E_ARG, "place event out of range");
+        if (ev[i].kind != CS_PLACE_EV_CLOSE && ev[i].kind != CS_PLACE_EV_OPEN) return fail(c, CS_E_ARG, "bad place event kind");
+    }
+    int closes = 0;
+    for (int kind = 0; kind < 2; kind++)
+        for (int pt = 0; pt < c->NPT; pt++)
+            for (int i = 0; i < n; i++) {
+                const cs_place_event* e = ev + i;
+                if (e->place_type != pt || e->kind != (kind == 0 ? CS_PLACE_EV_OPEN : CS_PLACE_EV_CLOSE)) continue;
+                place_arrays* pl = &c->pl[pt];
+                if (e->kind == CS_PLACE_EV_CLOSE) {
+                    closes = 1;
+                    pl->close_start[e->place] = e->close_start;
+                    pl->close_end[e->place] = e->close_end;
+                    if (e->members && P->DoRealSymptWithdrawal) close_place_members(c, pt, e->place, e->ts, e->win_start, e->win_stop);
+                } else {
+                    const uint16_t ce = pl->close_end[e->place];
+                    if (e->ts < ce) {
+                        if (P->DoRealSymptWithdrawal) open_place_members(c, pt, e->place, e->ts, ce);
+                        pl->close_end[e->place] = e->ts;
+                    }
+                }
+            }
+    if (closes) carer_queue_apply(c);
+    return CS_OK;
+}
+
+int cs_cpu_set_mcell_status(cs_cpu_ctx* c, const int32_t* mcells, const uint8_t* socdist, const uint8_t* moverest, int n)
+{
+    if (n < 0 || (n > 0 && !mcells)) return fail(c, CS_E_ARG, "bad microcell list");
+    for (int k = 0; k < n; k++) {
+        if (mcells[k] < 0 || mcells[k] >= c->NM) return fail(c, CS_E_ARG, "microcell out of range");
+        if (socdist) c->socdist[mcells[k]] = socdist[k];
+        if (moverest) c->moverest[mcells[k]] = moverest[k];
+    }
     return CS_OK;
 }
 

@@ -40,6 +40,9 @@ int cs_cpu_step(cs_cpu_ctx* ctx, double t, int run);
 int cs_cpu_set_interventions(cs_cpu_ctx* ctx, const cs_interventions* iv);
 int cs_cpu_close_places(cs_cpu_ctx* ctx, int place_type, const int32_t* mcells, int n_mcells,
                         uint16_t start, uint16_t stop);
+int cs_cpu_place_events(cs_cpu_ctx* ctx, const cs_place_event* events, int n);
+int cs_cpu_set_mcell_status(cs_cpu_ctx* ctx, const int32_t* mcells, const uint8_t* socdist,
+                            const uint8_t* moverest, int n);
 int cs_cpu_download_state(cs_cpu_ctx* ctx, const cs_state_view* state);
 int cs_cpu_get_counters(cs_cpu_ctx* ctx, cs_counters* out);
 

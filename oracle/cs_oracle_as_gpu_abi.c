@@ -34,6 +34,12 @@ int cs_gpu_update_probs(cs_gpu_ctx* c, int do_place) { return cs_cpu_update_prob
 int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run) { return cs_cpu_infect_sweep((cs_cpu_ctx*)c, t, run); }
 int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* c, double t) { return cs_cpu_incub_recovery_sweep((cs_cpu_ctx*)c, t); }
 int cs_gpu_get_counters(cs_gpu_ctx* c, cs_counters* out) { return cs_cpu_get_counters((cs_cpu_ctx*)c, out); }
+int cs_gpu_set_interventions(cs_gpu_ctx* c, const cs_interventions* iv) { return cs_cpu_set_interventions((cs_cpu_ctx*)c, iv); }
+int cs_gpu_place_events(cs_gpu_ctx* c, const cs_place_event* ev, int n) { return cs_cpu_place_events((cs_cpu_ctx*)c, ev, n); }
+int cs_gpu_set_mcell_status(cs_gpu_ctx* c, const int32_t* m, const uint8_t* sd, const uint8_t* mr, int n)
+{
+    return cs_cpu_set_mcell_status((cs_cpu_ctx*)c, m, sd, mr, n);
+}
 
 int cs_gpu_get_cell_counts(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D)
 {

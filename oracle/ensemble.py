@@ -6,6 +6,17 @@ the reference's own set-up builds the same population (same set-up seeds) and it
 own RecordSample writes the outputs; only the sweeps differ.  Per realisation we
 keep the final size (cumulative infections), the peak day of prevalence and the
 daily incidence, critical-care and death curves.
+
+Workloads (CONFIGS):
+  plain          20,000 people on 24 x 24 cells, 120 days, no interventions;
+  interventions  the same world for 200 days with the 10M workload's interventions:
+                 the global trigger on critical-care admissions over the last 7 days
+                 (above 5 here, the 20,000-person scale of the workload's 100 per
+                 10M rounded up to a trigger that fires mid-growth in every run)
+                 switches on case isolation, household quarantine, social
+                 distancing and place closure for 90 days; the reference's own
+                 RecordSample and TreatSweep decide them, the drop-in's sweeps
+                 consume them.
 """
 import os
 import sys
@@ -17,22 +28,34 @@ ROOT = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
 sys.path.insert(0, HERE)
 
-CONFIG = dict(people=20000, width_deg=0.2, cell_deg=1.0 / 120, nmcl=10, sigma=1.2, days=120, realisations=200,
-              setup_seed=98798150)
+CONFIGS = {
+    "plain": dict(people=20000, width_deg=0.2, cell_deg=1.0 / 120, nmcl=10, sigma=1.2, days=120, realisations=200,
+                  setup_seed=98798150),
+    "interventions": dict(people=20000, width_deg=0.2, cell_deg=1.0 / 120, nmcl=10, sigma=1.2, days=200,
+                          realisations=200, setup_seed=98798150, interventions=True, threshold=5, duration=90.0),
+}
+CONFIG = CONFIGS["plain"]
+GOLDEN = {"plain": "ref_ensemble.json", "interventions": "ref_ensemble_iv.json"}
 
 
-def population():
+def population(config="plain"):
     from covidsim_b200 import population as popmod
-    c = CONFIG
+    c = CONFIGS[config]
     grid = popmod.make_grid(width_deg=c["width_deg"], height_deg=c["width_deg"], cell_deg=c["cell_deg"], nmcl=c["nmcl"])
     return popmod.generate(c["people"], grid, sigma=c["sigma"], seed=c["setup_seed"])
 
 
-def run(binary, nr=None, threads=None):
+def run(binary, nr=None, threads=None, config="plain"):
+    """Realisations of `binary` on a workload.  A drop-in binary (its sweeps on the
+    oracle or the GPU) runs with OpenMP's passive wait policy: its host threads idle
+    while the sweep runs, and spinning threads would compete with it for cores."""
     import refrun
-    c = CONFIG
-    res = refrun.run_reference(population(), c["days"], nr=nr or c["realisations"], threads=threads, binary=binary,
-                               series=True, timeout=5400)
+    c = CONFIGS[config]
+    dropin = os.path.basename(binary) != "CovidSim"
+    res = refrun.run_reference(population(config), c["days"], nr=nr or c["realisations"], threads=threads, binary=binary,
+                               series=True, timeout=5400, interventions=c.get("interventions", False),
+                               threshold=c.get("threshold", 100), duration=c.get("duration", 90.0),
+                               env={"OMP_WAIT_POLICY": "passive"} if dropin else None)
     return summarise(res["series"]), res
 
 

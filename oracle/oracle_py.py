@@ -43,6 +43,8 @@ def load():
         "cs_cpu_step": (I, [V, D, I]),
         "cs_cpu_set_interventions": (I, [V, P(abi.cs_interventions)]),
         "cs_cpu_close_places": (I, [V, I, V, I, C.c_uint16, C.c_uint16]),
+        "cs_cpu_place_events": (I, [V, V, I]),
+        "cs_cpu_set_mcell_status": (I, [V, V, V, V, I]),
         "cs_cpu_download_state": (I, [V, P(abi.cs_state_view)]),
         "cs_cpu_get_counters": (I, [V, P(abi.cs_counters)]),
         "cs_cpu_kernel_num": (D, [V, D]),
@@ -121,6 +123,17 @@ class OracleBackend:
         else:
             m = np.ascontiguousarray(mcells, dtype=np.int32)
             self._ck(self.lib.cs_cpu_close_places(self.ctx, place_type, m.ctypes.data, len(m), start, stop), "close_places")
+
+    def place_events(self, events):
+        ev = (self.abi.cs_place_event * len(events))(*events)
+        self._ck(self.lib.cs_cpu_place_events(self.ctx, ev, len(events)), "place_events")
+
+    def set_mcell_status(self, mcells, socdist=None, moverest=None):
+        m = np.ascontiguousarray(mcells, dtype=np.int32)
+        sd = None if socdist is None else np.ascontiguousarray(socdist, dtype=np.uint8)
+        mr = None if moverest is None else np.ascontiguousarray(moverest, dtype=np.uint8)
+        self._ck(self.lib.cs_cpu_set_mcell_status(self.ctx, m.ctypes.data, None if sd is None else sd.ctypes.data,
+                                                  None if mr is None else mr.ctypes.data, len(m)), "set_mcell_status")
 
     def counters(self):
         out = self.abi.cs_counters()

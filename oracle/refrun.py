@@ -49,14 +49,14 @@ def parse_timing(stderr):
 
 def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=100, workdir=None,
                   seeds=(98798150, 729101, 17389101, 4797132),
-                  binary=BIN, keep=False, timeout=3000, series=False):
+                  binary=BIN, keep=False, timeout=3000, series=False, duration=90.0, env=None, extra_args=()):
     sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
     from covidsim_b200 import refconfig
     threads = threads or os.cpu_count()
     wd = workdir or tempfile.mkdtemp(prefix="csref_")
     try:
         f = refconfig.write_workload(wd, pop, days, interventions=interventions)
-        params = refconfig.intervention_params(interventions, threshold=threshold)
+        params = refconfig.intervention_params(interventions, duration=duration, threshold=threshold)
         pre = refconfig.pre_params(days, pop.grid, 2.4, 100)
         pre["Number of realisations"] = nr
         pre["Number of non-extinct realisations"] = nr
@@ -66,13 +66,15 @@ def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=
         refconfig.write_params(f["pre"], pre)
         refconfig.write_params(f["params"], params)
         cmd = [binary, "/c:%d" % threads, "/PP:" + f["pre"], "/P:" + f["params"], "/A:" + f["admin"],
-               "/D:" + f["density"], "/O:" + os.path.join(wd, "out"), *[str(s) for s in seeds]]
+               "/D:" + f["density"], "/O:" + os.path.join(wd, "out"), *extra_args, *[str(s) for s in seeds]]
         t0 = time.time()
-        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout,
+                           env=dict(os.environ, **env) if env else None)
         wall = time.time() - t0
         if r.returncode != 0:
             raise RuntimeError("reference exited %d: %s" % (r.returncode, r.stderr[-800:]))
-        out = dict(rows=parse_timing(r.stderr), wall=wall, threads=threads, workdir=wd, stderr=r.stderr[-4000:])
+        out = dict(rows=parse_timing(r.stderr), wall=wall, threads=threads, workdir=wd, stderr=r.stderr[-4000:],
+                   stderr_head=r.stderr[:8000])
         if series:
             out["series"] = [read_severity(os.path.join(wd, "out.%d.severity.xls" % k) if nr > 1 else
                                            os.path.join(wd, "out.severity.xls")) for k in range(nr)]

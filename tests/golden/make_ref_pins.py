@@ -3,8 +3,9 @@
 Builds oracle/_ref/ref_pins (oracle/Makefile: the reference's Kernels.cpp,
 Dist.cpp, InverseCdf.cpp, CalcInfSusc.cpp, Person.cpp and Rand.cpp compiled from the
 reference checkout, plus oracle/ref_pins.cpp) and stores its JSON output.  Needs the
-reference checkout (REF=..., default /root/reference); the tests only read the
-committed JSON.
+reference checkout, named by the REF environment variable
+(REF=<path of the reference checkout> python tests/golden/make_ref_pins.py); the tests
+only read the committed JSON.
 """
 import json
 import os
@@ -16,8 +17,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 
 
 def main():
-    env = dict(os.environ)
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "pins"], check=True, env=env)
+    if not os.environ.get("REF"):
+        sys.exit("set REF=<path of the reference checkout>")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "pins", "REF=" + os.environ["REF"]], check=True)
     out = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "ref_pins")], check=True, capture_output=True, text=True).stdout
     data = json.loads(out)
     with open(os.path.join(HERE, "ref_pins.json"), "w") as f:
