@@ -14,7 +14,7 @@ import numpy as np
 from . import abi
 
 GRIDS_PER_SM = (2, 4, 8, 16)
-LANES = (4, 8, 16)
+LANES = (2, 4, 8, 16)
 
 
 def autotune(simulation, n_sm=148, grids_per_sm=GRIDS_PER_SM, lanes=LANES, steps=24, seed_frac=0.02, seed=4040):
@@ -48,7 +48,7 @@ def autotune(simulation, n_sm=148, grids_per_sm=GRIDS_PER_SM, lanes=LANES, steps
             "ms": {"%dx%d" % k: round(v, 3) for k, v in sorted(timings.items())}}
 
 
-def autotune_batch(batch, n_sm=148, grids_per_sm=(1, 2, 4, 8), lanes=(4, 8), steps=12, seed_frac=0.02, seed=4040):
+def autotune_batch(batch, n_sm=148, grids_per_sm=(1, 2, 4, 8), lanes=(2, 4, 8), steps=12, seed_frac=0.02, seed=4040):
     """autotune for a sim.Batch: every member starts a throwaway realisation
     seeded with `seed_frac` of its population; each (grid, lanes) setting is timed
     over `steps` batched timesteps and the fastest is applied."""

@@ -162,6 +162,27 @@ __device__ __forceinline__ double knum(const DevPop& d, const cs_params& P, doub
     return t;
 }
 
+// KernelLookup::num over the FP32 copies of the tables (values within 2^-24
+// relative of the doubles), interpolated in double; an out-of-table distance sets
+// *oor instead of counting an error.  The spatial pass's acceptance test reads it:
+// half the bytes of the double tables per random lookup.
+__device__ __forceinline__ double knum_f32(const DevPop& d, const cs_params& P, double r2, int* oor)
+{
+    double t = r2 / P.kernel_delta;
+    if (t > P.kernel_size) { *oor = 1; return 0.0; }
+    double s = t * P.kernel_expansion;
+    if (s < P.kernel_size) {
+        t = s - floor(s);
+        t = (1.0 - t) * (double)__ldg(d.khires_f + (int)s) + t * (double)__ldg(d.khires_f + (int)(s + 1.0));
+    } else {
+        int i0 = (int)t, i1 = (int)(t + 1.0);
+        if (i1 > P.kernel_size) i1 = P.kernel_size;
+        s = t - floor(t);
+        t = (1.0 - s) * (double)__ldg(d.klookup_f + i0) + s * (double)__ldg(d.klookup_f + i1);
+    }
+    return t;
+}
+
 // KernelLookup::num for a caller that decides later whether the evaluation counts:
 // an out-of-table distance sets *oor instead of counting an error.
 __device__ __forceinline__ double knum_flag(const DevPop& d, const cs_params& P, double r2, int* oor)
@@ -288,6 +309,40 @@ __device__ inline double block_bound(const DevPop& d, const cs_params& P, int b,
     }
     d2 = d2 * 0.98;
     return knum(d, P, d2, err);
+}
+
+// The same bound by (row of b, row of B, column distance dx in blocks): the
+// closest corners are dx - 1 blocks apart in x (none for dx = 0) and at the rows'
+// facing edges in y; the great-circle distance depends on x only through the
+// difference and on y through both latitudes.
+__device__ inline double block_bound_rel(const DevPop& d, const cs_params& P, int by, int By, int dx, unsigned long long* err)
+{
+    if (P.DoPeriodicBoundaries) return knum(d, P, 0.0, err);
+    const int bs = d.bs, g = dx > 0 ? (dx - 1) * bs : 0;
+    int ya, yb;
+    if (By > by) { ya = (by + 1) * bs; yb = By * bs; }
+    else if (By < by) { ya = by * bs; yb = (By + 1) * bs; }
+    else { ya = yb = by * bs; }
+    double d2;
+    if (P.DoUTM_coords)
+        d2 = dist2_utm(P, P.cell_width * (double)g, P.cell_height * (double)ya, 0.0, P.cell_height * (double)yb);
+    else {
+        double x = P.cell_width * (double)g, y = P.cell_height * fabs((double)(ya - yb));
+        d2 = x * x + y * y;
+    }
+    d2 = d2 * 0.98;
+    return knum(d, P, d2, err);
+}
+
+// bound(b, B) for the proposal and the acceptance test alike, so that their
+// product stays exactly K(d): the compact FP32 table, or the per-call table.
+__device__ __forceinline__ double bound_of(const DevPop& d, int b, int B)
+{
+    if (d.bounds_static) {
+        const int bx = b / d.nby, by = b % d.nby, Bx = B / d.nby, By = B % d.nby;
+        return (double)__ldg(d.bound_c + ((size_t)by * d.nby + By) * d.nbx + (bx > Bx ? bx - Bx : Bx - bx));
+    }
+    return d.block_bound_tab[(size_t)b * d.NB + B];
 }
 
 // ------------------------------------------------------------- state macros

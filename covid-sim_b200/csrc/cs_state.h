@@ -111,6 +111,8 @@ struct DevPop {
     const int32_t* cell_members;
     const double* klookup;
     const double* khires;
+    const float* klookup_f;    // the same tables in FP32, for the spatial pass's acceptance test
+    const float* khires_f;
     DevPlaces pl[CS_MAX_PLACE_TYPES];
     // cold per-person state
     uint16_t* infection_time;
@@ -152,9 +154,13 @@ struct DevPop {
     BlockCell* block_cell_info;  // [NC], rebuilt with S0
     BlockInfo* block_info;       // [NB], S0 rebuilt with S0
     double* block_row_cum;     // [NB][NB]
-    double* block_bound_tab;   // [NB][NB] bound(b, B)
-    int32_t bounds_static;     // 1: all of block_bound_tab was filled once (geometry only);
-                               // 0: k_block_rows fills the entries of blocks with people
+    // bound(b, B), which depends on the row of b, the row of B and the distance of
+    // their columns only: [nby][nby][nbx], FP32 rounded up, filled once per geometry
+    const float* bound_c;
+    double* block_bound_tab;   // [NB][NB] bound(b, B) evaluated per UpdateProbs call, when bound_c
+                               // could not be filled (a distance beyond the kernel table)
+    int32_t bounds_static;     // 1: bound_c holds every bound; 0: k_block_rows fills block_bound_tab
+                               // for the blocks with people
     int16_t* block_guide;      // [NB][NB] cut points of each row (Chen & Asau guide table)
     int16_t* cell_guide;       // [NC] cut points of each block's cell list
     // per-step scratch

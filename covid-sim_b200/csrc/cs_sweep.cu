@@ -204,7 +204,7 @@ struct cs_gpu_ctx {
     uint64_t seed = 0;
     bool run_started = false;
     int grid = 148 * 8;
-    int spatial_lanes = 8;   // lanes per spatial contact (4, 8 or 16)
+    int spatial_lanes = 8;   // lanes per spatial contact (2, 4, 8 or 16)
     // one timestep captured as a CUDA graph and replayed
     bool use_graph = true;
     cudaGraph_t graph = nullptr;
@@ -696,15 +696,18 @@ __global__ void k_block_S0(DevPop d)
     }
 }
 
-// Every bound(b, B) of the geometry, once per population; *oor counts distances
+// Every bound of the geometry by (row of b, row of B, column distance), once per
+// population, rounded up to FP32 so that it still bounds K; *oor counts distances
 // beyond the kernel table (then the bounds are evaluated per call instead, so that
 // the error counts stay those of the per-call evaluation).
-__global__ void k_block_bounds_all(DevPop d, unsigned long long* oor)
+__global__ void k_block_bounds_all(DevPop d, float* bound_c, unsigned long long* oor)
 {
     const cs_params& P = *d.P;
-    const size_t n = (size_t)d.NB * d.NB;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-        d.block_bound_tab[e] = block_bound(d, P, (int)(e / d.NB), (int)(e % d.NB), oor);
+    const size_t n = (size_t)d.nby * d.nby * d.nbx;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int dx = (int)(e % d.nbx), By = (int)((e / d.nbx) % d.nby), by = (int)(e / ((size_t)d.nbx * d.nby));
+        bound_c[e] = __double2float_ru(block_bound_rel(d, P, by, By, dx, oor));
+    }
 }
 
 // Row b of the proposal table: running sum over B of S0_B * bound(b, B), added in
@@ -718,14 +721,14 @@ __global__ void k_block_rows(DevPop d)
     int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int b = warp; b < d.NB; b += nwarps) {
         double* row = d.block_row_cum + (size_t)b * d.NB;
-        double* btab = d.block_bound_tab + (size_t)b * d.NB;
+        double* btab = d.bounds_static ? nullptr : d.block_bound_tab + (size_t)b * d.NB;
         double s = 0.0;
         for (int B0 = 0; B0 < d.NB; B0 += 32) {
             int B = B0 + lane;
             double w = 0.0;
             if (B < d.NB && d.block_info[B].S0 > 0) {
                 double bound;
-                if (d.bounds_static) bound = btab[B];
+                if (d.bounds_static) bound = bound_of(d, b, B);
                 else btab[B] = bound = block_bound(d, P, b, B, CSB_CTR(err_kernel_range));
                 w = (double)d.block_info[B].S0 * bound;
             }
@@ -1004,7 +1007,7 @@ __device__ __forceinline__ bool spatial_draw(const DevPop& d, const cs_params& P
     int p = d.slots[bc.start + slot];
     PersonHot hp = d.hot[p];
     double d2 = dist2_hh(d, P, hh_inf, hp.hh);
-    double accept = knum_flag(d, P, d2, oor) / d.block_bound_tab[(size_t)b * d.NB + B];
+    double accept = knum_f32(d, P, d2, oor) / bound_of(d, b, B);
     if ((s.next() >= accept) || !is_alive(hp.inf)) return false;
     m_out = m; slot_out = slot; p_out = p; hp_out = hp;
     return true;
@@ -2179,6 +2182,14 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     size_t ksz = (size_t)params->kernel_size + 1;
     { double* t; UP(t, pop->kernel_lookup, ksz); d.klookup = t; }
     { double* t; UP(t, pop->kernel_hi_res, ksz); d.khires = t; }
+    {
+        std::vector<float> f(ksz), g(ksz);
+        for (size_t i = 0; i < ksz; i++) f[i] = (float)pop->kernel_lookup[i];
+        for (size_t i = 0; i < ksz; i++) g[i] = (float)pop->kernel_hi_res[i];
+        { float* t; UP(t, f.data(), ksz); d.klookup_f = t; }
+        { float* t; UP(t, g.data(), ksz); d.khires_f = t; }
+        CK(cudaStreamSynchronize(c->stream));   // before f and g go out of scope
+    }
     for (size_t pt = 0; pt < NPT; pt++) {
         DevPlaces& pl = d.pl[pt];
         pl.n = pop->n_places[pt];
@@ -2225,7 +2236,8 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         AL(c->Bpart, nchunks * G);
         AL(c->rowN, (size_t)params->nch);
     }
-    AL(d.block_bound_tab, (size_t)d.NB * d.NB);
+    { float* t; AL(t, (size_t)d.nby * d.nby * d.nbx); d.bound_c = t; }
+    d.block_bound_tab = nullptr;
     d.bounds_static = 1;
     c->alloc_to = nullptr;
 #undef UP
@@ -2341,7 +2353,7 @@ static int build_block_bounds(cs_gpu_ctx* c)
     unsigned long long* oor = nullptr;
     CK(cudaMalloc(&oor, sizeof(unsigned long long)));
     CK(cudaMemsetAsync(oor, 0, sizeof(unsigned long long), c->stream));
-    LAUNCH(k_block_bounds_all, c->grid, kThreads, d, oor);
+    LAUNCH(k_block_bounds_all, c->grid, kThreads, d, (float*)d.bound_c, oor);
     unsigned long long h = 0;
     CK(cudaMemcpyAsync(&h, oor, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -2554,6 +2566,7 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
     LAUNCH(k_infector_hh_spatial, c->grid, kThreads, d);
     LAUNCH(k_infector_places, c->grid, kThreads, d);
     switch (c->spatial_lanes) {
+    case 2: LAUNCH(k_spatial<2>, c->grid, kThreads, d); break;
     case 4: LAUNCH(k_spatial<4>, c->grid, kThreads, d); break;
     case 16: LAUNCH(k_spatial<16>, c->grid, kThreads, d); break;
     default: LAUNCH(k_spatial<8>, c->grid, kThreads, d); break;
@@ -2669,7 +2682,7 @@ int cs_gpu_grid(const cs_gpu_ctx* c) { return c ? c->grid : 0; }
 int cs_gpu_set_spatial_lanes(cs_gpu_ctx* c, int lanes)
 {
     if (!c) return CS_E_ARG;
-    if (lanes != 4 && lanes != 8 && lanes != 16) return set_err(c, CS_E_ARG, "spatial lanes must be 4, 8 or 16");
+    if (lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16) return set_err(c, CS_E_ARG, "spatial lanes must be 2, 4, 8 or 16");
     CK(cudaStreamSynchronize(c->stream));
     c->spatial_lanes = lanes;
     drop_day_graph(c);
@@ -2970,6 +2983,7 @@ static int batch_enqueue(cs_gpu_batch* b, const DevPop* pops)
     BLAUNCH(k_infector_hh_spatial_multi, g, kThreads, pops);
     BLAUNCH(k_infector_places_multi, g, kThreads, pops);
     switch (b->lanes) {
+    case 2: BLAUNCH(k_spatial_multi<2>, g, kThreads, pops); break;
     case 4: BLAUNCH(k_spatial_multi<4>, g, kThreads, pops); break;
     case 16: BLAUNCH(k_spatial_multi<16>, g, kThreads, pops); break;
     default: BLAUNCH(k_spatial_multi<8>, g, kThreads, pops); break;
@@ -3060,7 +3074,7 @@ int cs_gpu_batch_set_grid(cs_gpu_batch* b, int blocks)
 int cs_gpu_batch_set_spatial_lanes(cs_gpu_batch* b, int lanes)
 {
     if (!b) return CS_E_ARG;
-    if (lanes != 4 && lanes != 8 && lanes != 16) return batch_err(b, CS_E_ARG, "spatial lanes must be 4, 8 or 16");
+    if (lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16) return batch_err(b, CS_E_ARG, "spatial lanes must be 2, 4, 8 or 16");
     BCK(cudaStreamSynchronize(b->stream));
     b->lanes = lanes;
     batch_drop_graph(b);

@@ -417,8 +417,8 @@ int cs_gpu_use_graphs(cs_gpu_ctx* ctx, int enable);
  * step graph is dropped and captured again. */
 int cs_gpu_set_grid(cs_gpu_ctx* ctx, int blocks);
 int cs_gpu_grid(const cs_gpu_ctx* ctx);
-/* Lanes that test one spatial contact's candidate draws together: 4, 8 (default)
- * or 16.  Also a launch-shape choice: results do not depend on it. */
+/* Lanes that test one spatial contact's candidate draws together: 2, 4, 8
+ * (default) or 16.  Also a launch-shape choice: results do not depend on it. */
 int cs_gpu_set_spatial_lanes(cs_gpu_ctx* ctx, int lanes);
 
 /* ---- Realisations stepped together.  No counterpart in the reference, which
@@ -444,7 +444,7 @@ int cs_gpu_batch_create(cs_gpu_ctx* const* members, int n, cs_gpu_batch** out);
 int cs_gpu_batch_step(cs_gpu_batch* batch, double t, int run);
 /* cs_gpu_set_grid for every member (members must share one launch shape). */
 int cs_gpu_batch_set_grid(cs_gpu_batch* batch, int blocks);
-/* Spatial lanes of the batched launches (4, 8 or 16). */
+/* Spatial lanes of the batched launches (2, 4, 8 or 16). */
 int cs_gpu_batch_set_spatial_lanes(cs_gpu_batch* batch, int lanes);
 int cs_gpu_batch_sync(cs_gpu_batch* batch);
 void* cs_gpu_batch_stream(cs_gpu_batch* batch);

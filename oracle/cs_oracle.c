@@ -63,6 +63,7 @@ struct cs_cpu_ctx {
     float *hh_x, *hh_y;
     place_arrays pl[CS_MAX_PLACE_TYPES];
     double *klookup, *khires;
+    float *klookup_f, *khires_f;   /* the kernel tables rounded to FP32 (the spatial acceptance test) */
     /* dynamic per person */
     int8_t* inf;
     uint8_t *sev, *dflags;
@@ -84,6 +85,8 @@ struct cs_cpu_ctx {
     int32_t *cell_block, *block_cell_ofs, *block_cells, *block_cum;
     int64_t* block_S0;
     double* block_row_cum; /* [NB][NB] */
+    float* bound_c;        /* [nby][nby][nbx] bound by (row of b, row of B, column distance), FP32 rounded up */
+    int bounds_static;     /* 1: bound_c holds every bound; 0: bounds are evaluated per call */
     /* per step scratch */
     uint64_t* claim;
     uint8_t *hh_carer, *hh_hq;
@@ -416,6 +419,104 @@ static double block_bound(const cs_cpu_ctx* c, int b, int B, int64_t* err)
     return knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta, d2, err);
 }
 
+/* The same bound by (row of b, row of B, column distance dx in blocks), as the GPU
+ * library tabulates it once per geometry: the closest corners are dx - 1 blocks
+ * apart in x (none for dx = 0) and at the rows' facing edges in y. */
+static double block_bound_rel(const cs_cpu_ctx* c, int by, int By, int dx, int64_t* err)
+{
+    const cs_params* P = &c->P;
+    if (P->DoPeriodicBoundaries) return knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta, 0.0, err);
+    const int bs = c->bs, g = dx > 0 ? (dx - 1) * bs : 0;
+    int ya, yb;
+    if (By > by) { ya = (by + 1) * bs; yb = By * bs; }
+    else if (By < by) { ya = by * bs; yb = (By + 1) * bs; }
+    else { ya = yb = by * bs; }
+    double d2;
+    if (P->DoUTM_coords)
+        d2 = dist2_utm(P, P->cell_width * (double)g, P->cell_height * (double)ya, 0.0, P->cell_height * (double)yb);
+    else {
+        double x = P->cell_width * (double)g, y = P->cell_height * fabs((double)(ya - yb));
+        d2 = x * x + y * y;
+    }
+    d2 = d2 * 0.98;
+    return knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta, d2, err);
+}
+
+/* Round up to FP32: the nearest float, or the next one up when that is below v. */
+static float f32_up(double v)
+{
+    float f = (float)v;
+    if ((double)f < v) f = nextafterf(f, INFINITY);
+    return f;
+}
+
+/* Tabulate the bounds of the geometry; if any distance falls outside the kernel
+ * table they are evaluated (and counted) per call instead, as the GPU library does. */
+static void build_bound_table(cs_cpu_ctx* c)
+{
+    int64_t err = 0;
+    const size_t n = (size_t)c->nby * c->nby * c->nbx;
+    free(c->bound_c);
+    c->bound_c = (float*)calloc(n + 1, sizeof(float));
+    for (size_t e = 0; e < n; e++) {
+        const int dx = (int)(e % c->nbx), By = (int)((e / c->nbx) % c->nby), by = (int)(e / ((size_t)c->nbx * c->nby));
+        c->bound_c[e] = f32_up(block_bound_rel(c, by, By, dx, &err));
+    }
+    c->bounds_static = err == 0;
+}
+
+/* bound(b, B) for the proposal and the acceptance test alike. */
+static double bound_of(const cs_cpu_ctx* c, int b, int B, int64_t* err)
+{
+    if (c->bounds_static) {
+        const int bx = b / c->nby, by = b % c->nby, Bx = B / c->nby, By = B % c->nby;
+        return (double)c->bound_c[((size_t)by * c->nby + By) * c->nbx + (bx > Bx ? bx - Bx : Bx - bx)];
+    }
+    return block_bound(c, b, B, err);
+}
+
+/* KernelLookup::num over FP32 copies of the tables, interpolated in double. */
+static double knum_f32_tab(const float* lk, const float* hr, int size, int expansion, double delta, double r2,
+                           int64_t* err)
+{
+    double t = r2 / delta;
+    if (t > size) { (*err)++; return 0.0; }
+    double s = t * expansion;
+    if (s < size) {
+        t = s - floor(s);
+        t = (1.0 - t) * (double)hr[(int)s] + t * (double)hr[(int)(s + 1.0)];
+    } else {
+        int i0 = (int)t, i1 = (int)(t + 1.0);
+        if (i1 > size) i1 = size;
+        s = t - floor(t);
+        t = (1.0 - s) * (double)lk[i0] + s * (double)lk[i1];
+    }
+    return t;
+}
+
+static double knum_f32(const cs_cpu_ctx* c, double r2, int64_t* err)
+{
+    const cs_params* P = &c->P;
+    return knum_f32_tab(c->klookup_f, c->khires_f, P->kernel_size, P->kernel_expansion, P->kernel_delta, r2, err);
+}
+
+double cs_cpu_block_bound(const cs_cpu_ctx* c, int b, int B)
+{
+    int64_t e = 0;
+    return bound_of(c, b, B, &e);
+}
+
+void cs_cpu_block_geometry(const cs_cpu_ctx* c, int32_t* out)
+{
+    out[0] = c->bs; out[1] = c->nbx; out[2] = c->nby; out[3] = c->bounds_static;
+}
+
+double cs_cpu_kernel_num_f32(const float* lookup, const float* hi_res, int size, int expansion, double delta, double r2)
+{
+    int64_t e = 0;
+    return knum_f32_tab(lookup, hi_res, size, expansion, delta, r2, &e);
+}
+
 /* ---------------------------------------------------------- state macros -- */
 /* src/ModelMacros.h:6-20 */
 static inline int age_group(const cs_cpu_ctx* c, int p) { return c->age[p] / CS_AGE_GROUP_WIDTH; }
@@ -552,6 +653,13 @@ static void build_blocks(cs_cpu_ctx* c)
         c->block_cells[c->block_cell_ofs[b] + fill[b]++] = m;
     }
     free(fill);
+    c->klookup_f = (float*)calloc((size_t)P->kernel_size + 2, sizeof(float));
+    c->khires_f = (float*)calloc((size_t)P->kernel_size + 2, sizeof(float));
+    for (int i = 0; i <= P->kernel_size; i++) {
+        c->klookup_f[i] = (float)c->klookup[i];
+        c->khires_f[i] = (float)c->khires[i];
+    }
+    build_bound_table(c);
 }
 
 int cs_cpu_create(const cs_population* pop, const cs_params* params, cs_cpu_ctx** out)
@@ -633,7 +741,8 @@ void cs_cpu_destroy(cs_cpu_ctx* c)
                     c->prob_absent, c->prob_care, c->infector, c->listpos, c->infect_type, c->S, c->L, c->I,
                     c->R, c->D, c->S0, c->tot_prob, c->slots, c->mark, c->socdist, c->moverest, c->claim,
                     c->hh_carer, c->hh_hq, c->cell_block, c->block_cell_ofs, c->block_cells, c->block_cum,
-                    c->block_S0, c->block_row_cum, c->ci_start, c->hq_start, c->carer_start, c->carer_stop};
+                    c->block_S0, c->block_row_cum, c->ci_start, c->hq_start, c->carer_start, c->carer_stop,
+                    c->klookup_f, c->khires_f, c->bound_c};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     for (int t = 0; t < c->NPT; t++) {
         place_arrays* p = &c->pl[t];
@@ -648,6 +757,7 @@ int cs_cpu_set_params(cs_cpu_ctx* c, const cs_params* params)
     if (params->kernel_size != c->P.kernel_size || params->NumPlaceTypes != c->P.NumPlaceTypes)
         return fail(c, CS_E_ARG, "set_params may not change the kernel table or place types");
     c->P = *params;
+    build_bound_table(c);   /* the bounds depend on the geometry the parameters carry */
     return CS_OK;
 }
 
@@ -669,7 +779,7 @@ static void rebuild_block_tables(cs_cpu_ctx* c)
         double* row = c->block_row_cum + (size_t)b * c->NB;
         double s = 0.0;
         for (int B = 0; B < c->NB; B++) {
-            double w = (c->block_S0[B] > 0) ? (double)c->block_S0[B] * block_bound(c, b, B, &err) : 0.0;
+            double w = (c->block_S0[B] > 0) ? (double)c->block_S0[B] * bound_of(c, b, B, &err) : 0.0;
             s = s + w;
             row[B] = s;
         }
@@ -994,7 +1104,6 @@ static void place_candidates(cs_cpu_ctx* c, int i, int pt, int link, double Pinf
 static int spatial_draw(cs_cpu_ctx* c, stream* s, int b, int hi_, const double* row, double total,
                         int* m_out, int* slot_out, int* p_out, int64_t* err)
 {
-    const cs_params* P = &c->P;
     double target = stream_next(s) * total;
     int lo = 0, hi = c->NB - 1;
     while (lo < hi) {
@@ -1013,8 +1122,7 @@ static int spatial_draw(cs_cpu_ctx* c, stream* s, int b, int hi_, const double* 
     int slot = (int)(r - (double)(c->block_cum[k0] - c->S0[m]));
     int p = c->slots[c->cell_start[m] + slot];
     double d2 = dist2_hh(c, hi_, c->hh[p]);
-    double accept = knum(c->klookup, c->khires, P->kernel_size, P->kernel_expansion, P->kernel_delta, d2, err)
-        / block_bound(c, b, B, err);
+    double accept = knum_f32(c, d2, err) / bound_of(c, b, B, err);
     if ((stream_next(s) >= accept) || !is_alive(c, p)) return 0;
     *m_out = m; *slot_out = slot; *p_out = p;
     return 1;

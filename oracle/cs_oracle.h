@@ -51,6 +51,11 @@ int cs_cpu_upload_state(cs_cpu_ctx* ctx, uint64_t seed, const cs_state_view* sta
 double cs_cpu_calc(const cs_cpu_ctx* ctx, int kind, int p, int q, int pt, int ts);
 int cs_cpu_sample_many(int kind, uint64_t seed, double a, double b, int n, double* out);
 double cs_cpu_kernel_num(const cs_cpu_ctx* ctx, double r2);
+/* The spatial proposal's bound(b, B) and its block geometry {bs, nbx, nby, tabulated}. */
+double cs_cpu_block_bound(const cs_cpu_ctx* ctx, int b, int B);
+void cs_cpu_block_geometry(const cs_cpu_ctx* ctx, int32_t* out);
+/* KernelLookup::num over FP32 copies of the tables (the spatial acceptance test). */
+double cs_cpu_kernel_num_f32(const float* lookup, const float* hi_res, int size, int expansion, double delta, double r2);
 double cs_cpu_dist2_raw(const cs_params* p, double ax, double ay, double bx, double by);
 double cs_cpu_dist2_cc_min(const cs_params* p, int grid_l, int grid_m);
 uint16_t cs_cpu_icdf_choose(const cs_icdf* icdf, double mean, double u, double steps_per_day);

@@ -48,6 +48,9 @@ def load():
         "cs_cpu_download_state": (I, [V, P(abi.cs_state_view)]),
         "cs_cpu_get_counters": (I, [V, P(abi.cs_counters)]),
         "cs_cpu_kernel_num": (D, [V, D]),
+        "cs_cpu_kernel_num_f32": (D, [V, V, I, I, D, D]),
+        "cs_cpu_block_bound": (D, [V, I, I]),
+        "cs_cpu_block_geometry": (None, [V, V]),
         "cs_cpu_dist2_raw": (D, [P(abi.cs_params), D, D, D, D]),
         "cs_cpu_dist2_cc_min": (D, [P(abi.cs_params), I, I]),
         "cs_cpu_icdf_choose": (C.c_uint16, [P(abi.cs_icdf), D, D, D]),

@@ -51,3 +51,55 @@ def test_update_probs_renormalises():
     tp = snap["cell_tot_prob"]
     assert np.all((tp > 0) & (tp <= 1.0))
     assert tp.min() < 1.0
+
+
+def _bound_dominates(world, n_pairs=60000, seed=3):
+    """For household pairs in every kind of block pair (same, adjacent, far), the
+    tabulated proposal bound of their blocks is at least the FP32 kernel value at
+    their distance: the acceptance probability K(d)/bound of the spatial pass never
+    exceeds 1, so the rejection sampler draws exactly in proportion to K(d)."""
+    import ctypes as C
+    pop, P, lk, hr = world
+    s = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+    lib = oracle_py.load()
+    geo = np.zeros(4, np.int32)
+    lib.cs_cpu_block_geometry(s.backend.ctx, geo.ctypes.data)
+    bs, nbx, nby, tab = (int(v) for v in geo)
+    assert tab == 1
+    lk32, hr32 = lk.astype(np.float32), hr.astype(np.float32)
+    cx = np.floor(pop.hh_x / P.cell_width).astype(np.int64)
+    cy = np.floor(pop.hh_y / P.cell_height).astype(np.int64)
+    blk = (cx // bs) * nby + (cy // bs)
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, len(blk), n_pairs)
+    # half the partners from the same or a neighbouring block, where the bound is tight
+    near = np.nonzero(rng.random(n_pairs) < 0.5)[0]
+    b = rng.integers(0, len(blk), n_pairs)
+    order = np.argsort(blk, kind="stable")
+    first = np.searchsorted(blk[order], np.arange(nbx * nby))
+    last = np.searchsorted(blk[order], np.arange(nbx * nby), side="right")
+    worst = 0.0
+    for k in near:
+        bx, by = divmod(int(blk[a[k]]), nby)
+        tx = min(max(bx + int(rng.integers(-1, 2)), 0), nbx - 1)
+        ty = min(max(by + int(rng.integers(-1, 2)), 0), nby - 1)
+        t = tx * nby + ty
+        if last[t] > first[t]:
+            b[k] = order[rng.integers(first[t], last[t])]
+    for i, j in zip(a, b):
+        d2 = lib.cs_cpu_dist2_raw(C.byref(P), float(pop.hh_x[i]), float(pop.hh_y[i]), float(pop.hh_x[j]),
+                                  float(pop.hh_y[j]))
+        kf = lib.cs_cpu_kernel_num_f32(lk32.ctypes.data, hr32.ctypes.data, P.kernel_size, P.kernel_expansion,
+                                       P.kernel_delta, d2)
+        bound = lib.cs_cpu_block_bound(s.backend.ctx, int(blk[i]), int(blk[j]))
+        worst = max(worst, kf / bound)
+    s.close()
+    assert 0.5 < worst <= 1.0, worst
+
+
+def test_spatial_bound_dominates_kernel_utm():
+    _bound_dominates(tiny_world())
+
+
+def test_spatial_bound_dominates_kernel_planar():
+    _bound_dominates(tiny_world(utm=0))

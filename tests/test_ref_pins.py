@@ -82,6 +82,23 @@ def test_kernel_lookup_bit_exact(key):
         assert got == g["num"]
 
 
+@pytest.mark.parametrize("key", ["kernel", "kernel2"])
+def test_kernel_lookup_fp32_within_1e6(key):
+    """The spatial pass's acceptance test reads FP32 copies of the kernel tables:
+    within 1e-6 relative of the reference's double KernelLookup::num."""
+    g = GOLD[key]
+    n, e = g["size"], g["expansion"]
+    olib = oracle_py.load()
+    lk, hr = np.empty(n + 1), np.empty(n + 1)
+    d = C.c_double()
+    assert olib.cs_cpu_build_kernel_table(g["type"], g["scale"], g["shape"], 0.0, 0.0, g["longest_d2"], n, e,
+                                          lk.ctypes.data, hr.ctypes.data, C.byref(d)) == 0
+    lk32, hr32 = lk.astype(np.float32), hr.astype(np.float32)
+    got = np.array([olib.cs_cpu_kernel_num_f32(lk32.ctypes.data, hr32.ctypes.data, n, e, d.value, r2) for r2 in g["r2"]])
+    want = np.array(g["num"])
+    assert np.all(np.abs(got - want) <= 1e-6 * np.abs(want)), np.max(np.abs(got - want) / np.abs(want))
+
+
 def test_inverse_cdf_bit_exact():
     g = GOLD["icdf"]
     icdf = abi.cs_icdf()
