@@ -81,6 +81,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-out", default=None, help="write per-kernel times to this JSON file")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the launch-shape autotuner (use --lanes and --blocks-per-sm), so that the timed "
+                         "realisation's k-th timestep is each kernel's k-th launch (profiling runs)")
+    ap.add_argument("--lanes", type=int, default=2, help="with --no-tune: lanes per spatial contact")
+    ap.add_argument("--blocks-per-sm", type=int, default=8, help="with --no-tune: blocks per SM of the sweep kernels")
     return ap.parse_args()
 
 
@@ -254,7 +259,13 @@ def run_ours(args):
     base_seed = replica_seed(rank)
 
     from covidsim_b200 import tune
-    tuned = tune.autotune(s, n_sm=torch.cuda.get_device_properties(local).multi_processor_count)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    if args.no_tune:
+        be.set_grid(n_sm * args.blocks_per_sm)
+        be.set_spatial_lanes(args.lanes)
+        tuned = {"grid": n_sm * args.blocks_per_sm, "spatial_lanes": args.lanes, "ms": None}
+    else:
+        tuned = tune.autotune(s, n_sm=n_sm)
     for w in range(args.warmup):
         s.run(seed=base_seed + 1000 + w, days=days, n_seed=n_seed, policy=policy)
     be.sync()
