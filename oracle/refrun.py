@@ -74,7 +74,7 @@ def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=
         if r.returncode != 0:
             raise RuntimeError("reference exited %d: %s" % (r.returncode, r.stderr[-800:]))
         out = dict(rows=parse_timing(r.stderr), wall=wall, threads=threads, workdir=wd, stderr=r.stderr[-4000:],
-                   dropin=[ln.strip() for ln in r.stderr.splitlines() if ln.startswith("GPU sweep:")])
+                   dropin=[ln[ln.index("GPU sweep:"):].strip() for ln in r.stderr.splitlines() if "GPU sweep:" in ln])
         if series:
             out["series"] = [read_severity(os.path.join(wd, "out.%d.severity.xls" % k) if nr > 1 else
                                            os.path.join(wd, "out.severity.xls")) for k in range(nr)]
