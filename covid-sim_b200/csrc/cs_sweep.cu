@@ -183,6 +183,8 @@ struct cs_gpu_ctx {
     std::vector<void*>* alloc_to = nullptr;  // where dalloc records allocations (null: allocs)
     cudaStream_t own_stream = nullptr;     // the context's stream while a batch lends it another
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;           // the place pass's branch beside the spatial pass
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     char err[512] = {0};
     long long launches = 0;
     DevPop d{};
@@ -235,6 +237,13 @@ struct cs_gpu_ctx {
     std::vector<const char*> prof_names;
     std::vector<double> prof_ms;
     std::vector<long long> prof_n;
+    // per-kernel timing inside a captured day graph: event-record nodes around each
+    // kernel, read after every replay, so that the times are device times between
+    // back-to-back graph launches rather than eager launches with host gaps
+    bool capturing_prof = false;
+    bool day_graph_prof = false;
+    std::vector<cudaEvent_t> graph_events;   // pool, reused by later captures
+    std::vector<Rec> graph_recs;             // the captured day graph's timed kernels
 };
 
 static void drop_day_graph(cs_gpu_ctx* c)
@@ -261,8 +270,25 @@ static void prof_flush(cs_gpu_ctx* c)
     c->ring_used = 0;
 }
 
+static cudaEvent_t graph_event(cs_gpu_ctx* c, size_t i)
+{
+    while (c->graph_events.size() <= i) {
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        c->graph_events.push_back(e);
+    }
+    return c->graph_events[i];
+}
+
 static void prof_begin(cs_gpu_ctx* c, const char* name)
 {
+    if (c->capturing_prof) {   // an event-record node before the kernel's node
+        const size_t i = 2 * c->graph_recs.size();
+        cs_gpu_ctx::Rec r{name, graph_event(c, i), graph_event(c, i + 1)};
+        cudaEventRecordWithFlags(r.a, c->stream, cudaEventRecordExternal);
+        c->graph_recs.push_back(r);
+        return;
+    }
     if (c->ring_used == c->ring.size()) prof_flush(c);
     cs_gpu_ctx::Rec& r = c->ring[c->ring_used];
     r.name = name;
@@ -271,8 +297,28 @@ static void prof_begin(cs_gpu_ctx* c, const char* name)
 
 static void prof_end(cs_gpu_ctx* c)
 {
+    if (c->capturing_prof) {
+        cudaEventRecordWithFlags(c->graph_recs.back().b, c->stream, cudaEventRecordExternal);
+        return;
+    }
     cudaEventRecord(c->ring[c->ring_used].b, c->stream);
     c->ring_used++;
+}
+
+// After a replay of a day graph captured with timing nodes: add its kernels' times.
+static void prof_graph_collect(cs_gpu_ctx* c)
+{
+    if (c->graph_recs.empty()) return;
+    cudaEventSynchronize(c->graph_recs.back().b);
+    for (const auto& r : c->graph_recs) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        size_t k = 0;
+        while (k < c->prof_names.size() && std::strcmp(c->prof_names[k], r.name) != 0) k++;
+        if (k == c->prof_names.size()) { c->prof_names.push_back(r.name); c->prof_ms.push_back(0); c->prof_n.push_back(0); }
+        c->prof_ms[k] += ms;
+        c->prof_n[k]++;
+    }
 }
 
 static int set_err(cs_gpu_ctx* c, int code, const char* fmt, ...)
@@ -2111,6 +2157,9 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     c->grid = nsm * 8;
@@ -2265,6 +2314,9 @@ int cs_gpu_create_replica(const cs_gpu_ctx* base, cs_gpu_ctx** out)
     c->device = base->device;
     CK(cudaSetDevice(c->device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     c->grid = base->grid;
     c->hp = base->hp;
     c->stat = base->stat;
@@ -2290,6 +2342,10 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& r : c->ring) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (cudaEvent_t e : c->graph_events) cudaEventDestroy(e);
+    if (c->side) { cudaStreamSynchronize(c->side); cudaStreamDestroy(c->side); }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->day_exec) cudaGraphExecDestroy(c->day_exec);
@@ -2564,13 +2620,28 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
     int r = build_active(c, 0);
     if (r) return r;
     LAUNCH(k_infector_hh_spatial, c->grid, kThreads, d);
-    LAUNCH(k_infector_places, c->grid, kThreads, d);
+    // The place pass and the spatial pass both read the infector pass's lists and
+    // only claim infections (atomicMin on the claim key) and add to counters, so the
+    // place pass runs on the side stream beside the spatial pass (a branch of the
+    // captured graphs).  While profiling they run one after the other.
+    const bool fork = c->side && !c->prof;
+    if (fork) {
+        CK(cudaEventRecord(c->ev_fork, c->stream));
+        CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+        k_infector_places<<<c->grid, kThreads, 0, c->side>>>(d);
+        c->launches++;
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(c->ev_join, c->side));
+    } else {
+        LAUNCH(k_infector_places, c->grid, kThreads, d);
+    }
     switch (c->spatial_lanes) {
     case 2: LAUNCH(k_spatial<2>, c->grid, kThreads, d); break;
     case 4: LAUNCH(k_spatial<4>, c->grid, kThreads, d); break;
     case 16: LAUNCH(k_spatial<16>, c->grid, kThreads, d); break;
     default: LAUNCH(k_spatial<8>, c->grid, kThreads, d); break;
     }
+    if (fork) CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     return apply_queue(c);
 }
 
@@ -2771,16 +2842,22 @@ static int capture_day(cs_gpu_ctx* c, int spd, bool every_step)
 
 static int run_days(cs_gpu_ctx* c, int days, int spd, bool every_step)
 {
-    const bool graph = c->use_graph && !c->prof;
-    if (graph && (!c->day_exec || c->day_every_step != (every_step ? 1 : 0))) {
+    const bool graph = c->use_graph;
+    if (graph && (!c->day_exec || c->day_every_step != (every_step ? 1 : 0) || c->day_graph_prof != c->prof)) {
         drop_day_graph(c);
+        prof_flush(c);
+        c->graph_recs.clear();
+        c->capturing_prof = c->prof;
         int r = capture_day(c, spd, every_step);
+        c->capturing_prof = false;
+        c->day_graph_prof = c->prof && r == CS_OK;
         if (r) return r;
     }
     for (int k = 0; k < days; k++) {
         if (graph) {
             CK(cudaGraphLaunch(c->day_exec, c->stream));
             c->launches += c->day_launches;
+            if (c->day_graph_prof) prof_graph_collect(c);
         } else {
             int r = enqueue_day(c, spd, every_step);
             if (r) return r;

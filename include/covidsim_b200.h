@@ -580,7 +580,10 @@ void* cs_gpu_stream(cs_gpu_ctx* ctx);
 int64_t cs_gpu_launch_count(const cs_gpu_ctx* ctx);
 /*
  * Per-kernel device time: with enable = 1 every launch is bracketed by CUDA events
- * on the context's stream; 2 also clears the totals; 0 stops recording.
+ * on the context's stream; 2 also clears the totals; 0 stops recording.  Inside
+ * cs_gpu_run the day graph is captured with event-record nodes around each kernel
+ * and replayed as usual, so those times are kernel times between back-to-back
+ * launches; elsewhere launches are eager while profiling.
  * cs_gpu_profile_entry reads entry i (name, summed milliseconds, launches) and
  * returns CS_E_RANGE past the last entry.
  */
