@@ -26,8 +26,14 @@
 //                        quarantine start times, the microcells' social-distancing
 //                        and movement-restriction status, and the outcome of every
 //                        DoPlaceClose / DoPlaceOpen call TreatSweep made.  Those two
-//                        calls reach this file because the drop-in compiles Sweep.cpp
-//                        with them renamed (oracle/Makefile), as it does the sweeps.
+//                        calls and TreatSweep itself reach this file because the
+//                        drop-in compiles Sweep.cpp with them renamed (oracle/Makefile),
+//                        as it does the sweeps;
+//   timing               the wall time of each realisation's sweep calls (from its
+//                        first call on, the device context's creation excluded),
+//                        written to stderr at exit as oracle/ref_timing_shim.cpp
+//                        writes the reference's:  SWEEPTIMING run=.. pop=.. threads=..
+//                        steps=.. infect_s=.. incub_s=..
 //
 // Features outside the device sweep (digital contact tracing, airports, blanket
 // movement restrictions, treatment/vaccination/key-worker prophylaxis, false
@@ -39,7 +45,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <omp.h>
 #include <vector>
 
 #include "Constants.h"
@@ -68,6 +76,16 @@ std::vector<double> g_ci_start, g_hq_start;   // per admin unit start times
 double g_ci_dur = -1, g_hq_dur = -1;
 bool g_iv_sent = false;
 std::vector<cs_place_event> g_events;         // TreatSweep's closures since the last step
+// what the last microcell scan found: populated microcells untreated / treated for
+// social distancing, and the earliest end of a treated one (TimeStepNow units)
+long long g_sd_untreated = 0, g_sd_treated = 0;
+unsigned int g_sd_min_end = 0xFFFFFFFFu;
+struct RunTiming {
+    int run;
+    long steps = 0;
+    double infect = 0.0, incub = 0.0;
+};
+std::vector<RunTiming> g_timing;
 
 void check(int rc, const char* what)
 {
@@ -372,6 +390,9 @@ void upload_run_state(int run)
     // InitModel reset the host's
     g_sd.assign(P.NumMicrocells, (uint8_t)CS_TREAT_UNTREATED);
     g_mr.assign(P.NumMicrocells, (uint8_t)CS_TREAT_UNTREATED);
+    g_sd_untreated = P.NumPopulatedMicrocells;
+    g_sd_treated = 0;
+    g_sd_min_end = 0xFFFFFFFFu;
     g_iv_sent = false;
     g_events.clear();
     g_s0_sig = s0_signature();
@@ -467,19 +488,56 @@ void mirror_host_interventions(double t)
         check(cs_gpu_set_interventions(g_ctx, &w), "cs_gpu_set_interventions");
         g_iv_sent = true;
     }
-    // microcell status: TreatSweep changes it only from the start times on
-    const bool sd = t_prev >= P.SocDistTimeStart, mr = t_prev >= P.MoveRestrTimeStart;
+}
+
+// The global trigger value as TreatSweep forms it (src/Sweep.cpp:1342-1347).
+int global_trig_value()
+{
+    if (!P.DoGlobalTriggers) return 0;
+    if (P.DoPerCapitaTriggers) return (int)floor(((double)State.trigDetectedCases) * P.GlobalIncThreshPop / ((double)P.PopSize));
+    return State.trigDetectedCases;
+}
+
+// What TreatSweep(t) changed, handed to the device right after it ran.  Microcell
+// status changes only where TreatSweep's own conditions allow (src/Sweep.cpp:
+// 1839-1912): social distancing switches on when the trigger reached its threshold
+// and untreated microcells remain, and off when a treated microcell's end time has
+// come or the trigger fell below the stop threshold; movement restrictions only
+// from their start time on.  The microcells are scanned only then: a scan touches
+// every populated microcell's record (2.7 M of them at 10 M people on 240 x 240
+// cells).  Admin-unit triggers are compared per unit, so with them every step from
+// the start time on is scanned.
+void mirror_treat_sweep(double t, int gt)
+{
+    const unsigned int ts = (unsigned short int)(P.TimeStepsPerDay * t);
+    bool sd = false;
+    if (t >= P.SocDistTimeStart) {
+        if (!P.DoGlobalTriggers) sd = true;
+        else sd = (g_sd_untreated > 0 && gt >= P.SocDistCellIncThresh) ||
+                  (g_sd_treated > 0 && (gt < P.SocDistCellIncStopThresh || ts >= g_sd_min_end));
+    }
+    const bool mr = t >= P.MoveRestrTimeStart;
     if (sd || mr) {
         std::vector<int32_t> ms;
         std::vector<uint8_t> vs, vm;
+        long long untreated = 0, treated = 0;
+        unsigned int min_end = 0xFFFFFFFFu;
         for (int i = 0; i < P.NumPopulatedMicrocells; i++) {
             const int m = (int)(McellLookup[i] - Mcells);
             const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
+            if (Mcells[m].socdist == TreatStat::Untreated) untreated++;
+            else if (Mcells[m].socdist == TreatStat::Treated) {
+                treated++;
+                if (Mcells[m].socdist_end_time < min_end) min_end = Mcells[m].socdist_end_time;
+            }
             if (a == g_sd[m] && b == g_mr[m]) continue;
             ms.push_back(m);
             vs.push_back(g_sd[m] = a);
             vm.push_back(g_mr[m] = b);
         }
+        g_sd_untreated = untreated;
+        g_sd_treated = treated;
+        g_sd_min_end = min_end;
         if (!ms.empty())
             check(cs_gpu_set_mcell_status(g_ctx, ms.data(), vs.data(), vm.data(), (int)ms.size()), "cs_gpu_set_mcell_status");
     }
@@ -490,11 +548,22 @@ void mirror_host_interventions(double t)
     }
 }
 
+void report_timing()
+{
+    for (const RunTiming& r : g_timing)
+        std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f\n", r.run, P.PopSize,
+                     P.NumThreads, r.steps, r.infect, r.incub);
+}
+
 }  // namespace
 
 void InfectSweep(double t, int run)
 {
-    if (!g_ctx) create_context();
+    if (!g_ctx) {
+        create_context();
+        std::atexit(report_timing);
+    }
+    const double t0 = omp_get_wtime();
     if (run != g_run) {
         upload_run_state(run);
         g_run = run;
@@ -504,6 +573,23 @@ void InfectSweep(double t, int run)
     }
     mirror_host_interventions(t);
     check(cs_gpu_infect_sweep(g_ctx, t, run), "cs_gpu_infect_sweep");
+    if (g_timing.empty() || g_timing.back().run != run) {
+        g_timing.push_back(RunTiming());
+        g_timing.back().run = run;
+    }
+    g_timing.back().infect += omp_get_wtime() - t0;
+    g_timing.back().steps++;
+}
+
+// TreatSweep (src/Sweep.cpp:1324-2004) runs on the host as the reference's own
+// function; the drop-in's Sweep.cpp has it renamed to ref_TreatSweep.
+int ref_TreatSweep(double t);
+int TreatSweep(double t)
+{
+    const int gt = global_trig_value();   // the value the reference's TreatSweep will use
+    const int r = ref_TreatSweep(t);
+    if (g_ctx && g_run >= 0) mirror_treat_sweep(t, gt);
+    return r;
 }
 // TreatSweep's place closures (src/Sweep.cpp:1686, 1733): the drop-in's Sweep.cpp
 // calls these in place of DoPlaceClose / DoPlaceOpen.  Each runs the reference's own
@@ -551,6 +637,8 @@ void cs_shim_DoPlaceOpen(int i, int j, unsigned short int TimeStepNow)
 
 void IncubRecoverySweep(double t)
 {
+    const double t0 = omp_get_wtime();
     check(cs_gpu_incub_recovery_sweep(g_ctx, t), "cs_gpu_incub_recovery_sweep");
     sync_back();
+    if (!g_timing.empty()) g_timing.back().incub += omp_get_wtime() - t0;
 }

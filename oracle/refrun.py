@@ -41,7 +41,8 @@ SAMPLES = {
 
 def parse_timing(stderr):
     rows = []
-    for m in re.finditer(r"REFTIMING run=(\d+) pop=(\d+) threads=(\d+) steps=(\d+) infect_s=([\d.]+) incub_s=([\d.]+)", stderr):
+    for m in re.finditer(r"(?:REF|SWEEP)TIMING run=(\d+) pop=(\d+) threads=(\d+) steps=(\d+) infect_s=([\d.]+) incub_s=([\d.]+)",
+                         stderr):
         rows.append(dict(run=int(m.group(1)), pop=int(m.group(2)), threads=int(m.group(3)), steps=int(m.group(4)),
                          infect_s=float(m.group(5)), incub_s=float(m.group(6))))
     return rows
