@@ -61,7 +61,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["c2", "c4"])
+    ap.add_argument("--workload", default="c1_240", choices=sorted(WORKLOADS) + ["c2", "c4"])
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the extra measurement of the 600x600-cell grid in the default run")
     ap.add_argument("--c2-scale", type=float, default=1.0,
                     help="c2 only: population sizes times this factor (1.0 = 1/4/10/20 M)")
     ap.add_argument("--c2-per-size", type=int, default=16, help="c2 only: realisations per population size")
@@ -349,8 +351,17 @@ def run_ours(args):
                        workload=args.workload, profiled_runs=prof_runs, tuned=tuned),
                   open(args.profile_out, "w"), indent=1)
 
-    # end to end through the C ABI with host buffers
+    # end to end through the reference-facing drop-in: the reference executable with
+    # the GPU sweep linked in, on the same network file the reference arm loads
+    # (the reference's own set-up and host code, the sweeps on this rank's GPU)
     e2e = None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    dropin = (not args.no_e2e) and refrun.SAMPLES.get(args.workload, {}).get("network")
+    if dropin:
+        e2e = e2e_dropin(args, local, world, dist, pop.n_cells)
+    # end to end through the C ABI from host buffers (the Python host)
+    e2e_py = None
     if not args.no_e2e:
         # the prepared start state (input) and the final state (output) in separate
         # pinned host buffers, so every realisation starts from the same input
@@ -375,14 +386,23 @@ def run_ours(args):
         for a in pinned:
             cudart.cudaHostUnregister(a.ctypes.data)
         import ctypes
-        e2e = {"value": round(person_steps / dt, 1), "unit": METRIC, "h2d_bytes_per_step": state_bytes,
-               "d2h_bytes_per_step": state_bytes + days * ctypes.sizeof(sim.abi.cs_counters),
-               "what": "upload prepared start state, run, daily counters, download final state"}
+        e2e_py = {"value": round(person_steps / dt, 1), "unit": METRIC, "h2d_bytes_per_step": state_bytes,
+                  "d2h_bytes_per_step": state_bytes + days * ctypes.sizeof(sim.abi.cs_counters),
+                  "what": "Python host through the C ABI: upload prepared start state, run, daily counters, "
+                          "download final state"}
+        if e2e is None:
+            e2e = e2e_py
 
     # CPU baseline: the oracle port on a bounded sample of the same workload
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(s, pop, P, lk, hr, days)
+    s.close()
+
+    # the same measurement on the 600x600-cell grid of the 10M workload
+    extra = None
+    if args.workload == "c1_240" and not args.no_extra:
+        extra = extra_600(args, local, world, dist)
 
     if dist:
         dist.barrier()
@@ -402,10 +422,72 @@ def run_ours(args):
                    "tuned": {"grid": tuned["grid"], "spatial_lanes": tuned["spatial_lanes"]}},
         "runs_per_hour": round(runs_per_hour, 1),
         "outcomes": [{"cumI": a, "deaths": b, "peak_day": c} for a, b, c in finals],
-        "clocks": clocks, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+        "clocks": clocks, "e2e": e2e, "e2e_python_host": e2e_py if e2e is not e2e_py else None,
+        "c1_600x600": extra, "roofline": roofline, "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} for r in rows[:8]],
     }
+
+
+def e2e_dropin(args, local, world, dist, n_cells):
+    """e2e through the drop-in: warm-up 1 and `steps` timed realisations of the
+    reference executable with the GPU sweep linked in, loading the workload's
+    network file; value = people x timesteps / wall time of the sweep calls (state
+    upload at each realisation's start, the device sweeps, the per-step copy of the
+    cell counts and counters back to the reference's host structures)."""
+    import ctypes
+    import refrun
+    from covidsim_b200 import abi, sim
+    res = refrun.time_dropin(args.workload, steps=args.steps, warmup=1, device=local,
+                             threads=min(os.cpu_count() or 8, 32))
+    if "unavailable" in res:
+        return {"unavailable": res["unavailable"]}
+    rows = res["rows"]
+    person_steps = sum(r["pop"] * r["steps"] for r in rows)
+    secs = sum(r["infect_s"] + r["incub_s"] for r in rows)
+    secs = max_over_ranks(secs, dist, "cuda")
+    n, steps = rows[0]["pop"], rows[0]["steps"]
+    arrs, _ = sim.state_arrays(n, n_cells)   # the grid's populated cells (every cell at 10M people)
+    h2d = sum(a.nbytes for a in arrs.values())
+    d2h = steps * (5 * 4 * n_cells + ctypes.sizeof(abi.cs_counters))
+    return {"value": round(person_steps * world / secs, 1), "unit": METRIC, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(1e3 * secs / len(rows), 3),
+            "what": "the reference executable with the GPU sweep linked in (oracle/_ref/CovidSim_b200), the same "
+                    "network file as the reference arm; wall time of the sweep calls per realisation: state upload "
+                    "from the reference's host structures at its start, device sweeps, per-step copy of cell "
+                    "counts and counters back",
+            "realisations": len(rows), "host_threads": rows[0]["threads"], "process_wall_s": round(res["wall"], 1)}
+
+
+def extra_600(args, local, world, dist):
+    """value of the 10M workload on its own 600x600-cell grid (device time, 1 warm-up
+    and 2 timed realisations)."""
+    import torch
+    from covidsim_b200 import population, params as prm, sim, tune
+    preset, days, with_iv, desc, n_seed = WORKLOADS["c1"]
+    pop = population.cached(args.population_cache, preset, lambda: population.preset(preset))
+    P, lk, hr = prm.build_params(pop.grid)
+    P.LocalBeta, _ = sim.calibrate_local_beta(pop, P, 2.4)
+    s = sim.Simulation(pop, P, lk, hr, device=local)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    tuned = tune.autotune(s, n_sm=n_sm)
+    policy = sim.InterventionPolicy()
+    base_seed = replica_seed(int(os.environ.get("RANK", 0)))
+    s.run(seed=base_seed + 999, days=days, n_seed=n_seed, policy=policy)
+    stream = torch.cuda.ExternalStream(s.backend.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for k in range(2):
+        s.run(seed=base_seed + k, days=days, n_seed=n_seed, policy=policy)
+    ev1.record(stream)
+    s.backend.sync()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
+    s.close()
+    return {"workload": desc, "value": round(pop.n_people * int(days * P.TimeStepsPerDay) * 2 * world / (ms / 1e3), 1),
+            "unit": METRIC, "ms_per_step": round(ms / 2, 3), "realisations_per_rank": 2,
+            "tuned": {"grid": tuned["grid"], "spatial_lanes": tuned["spatial_lanes"]}}
 
 
 def cpu_baseline_port(s, pop, P, lk, hr, days, budget_s=20.0):
@@ -457,7 +539,9 @@ def run_reference(args):
     import refrun
     if args.workload not in refrun.SAMPLES:
         return {"impl": "reference", "unavailable": "no reference sample defined for workload %s" % args.workload}
-    res = refrun.time_reference(args.workload, steps=args.steps, warmup=args.warmup)
+    # a CPU realisation needs no warm-up beyond touching its memory once: one
+    # warm-up realisation at most, then the `steps` timed ones
+    res = refrun.time_reference(args.workload, steps=args.steps, warmup=min(args.warmup, 1))
     if "unavailable" in res:
         return {"impl": "reference", "unavailable": res["unavailable"]}
     preset, days, with_iv, desc, n_seed = WORKLOADS[args.workload]

@@ -8,6 +8,14 @@ compiled from its sources with wall-clock timers around InfectSweep and
 IncubRecoverySweep, oracle/ref_timing_shim.cpp) runs W + K realisations in one
 process (/NR), so set-up is paid once.  person-steps/s = people x timesteps / sweep
 wall time, per realisation.
+
+At 10M people the reference's own place assignment alone runs for hours
+(single-threaded, one microcell spiral per person), so those workloads load a
+network file (/L) that oracle/_ref/CovidSim_netgen wrote once (/S): the reference's
+own set-up with a fast place assignment (oracle/ref_network_tool.cpp).  The timed
+reference and the drop-in (oracle/_ref/CovidSim_b200, the reference with the GPU
+sweep linked in) then load the same file: the same people, households, places and
+groups, and the same host code around the sweeps.
 """
 import os
 import re
@@ -21,6 +29,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 BIN = os.path.join(HERE, "_ref", "CovidSim_timed")
 STOCK = os.path.join(HERE, "_ref", "CovidSim")
+DROPIN = os.path.join(HERE, "_ref", "CovidSim_b200")
+NETGEN = os.path.join(HERE, "_ref", "CovidSim_netgen")
+NET_DIR = os.path.join(HERE, "_ref", "net")
 
 # The reference keeps two dense Ncells x Ncells float tables (src/SetupModel.cpp:
 # 1207-1216): 8 bytes per cell pair.  Its sample grids are chosen to fit in memory
@@ -36,7 +47,41 @@ SAMPLES = {
                     "10M workload), C1 interventions with the ICU trigger scaled per head, 365 d"),
     "c0": dict(people=1_000_000, cell_deg=1.0 / 120, days=120, interventions=False, threshold=100,
                note="1M people, 240x240 cells (26.5 GB of dense cell tables), 120 d"),
+    # The 10M workload itself on the 240 x 240 grid (the largest grid whose dense cell
+    # tables, 26.5 GB, the reference can hold): the same density file, parameters
+    # and interventions as the GPU's c1_240 workload, the population set up by the
+    # reference from them with its place links from the network file.
+    "c1_240": dict(people=10_000_000, preset="c1_240", days=365, interventions=True, threshold=100, network=True,
+                   note="10M people on 240x240 cells, C1 interventions (global ICU trigger at 100 weekly admissions), "
+                        "365 d; the reference's own set-up with place links loaded from a network file (/L)"),
 }
+
+
+def sample_population(s):
+    sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
+    from covidsim_b200 import population
+    if s.get("preset"):
+        return population.preset(s["preset"])
+    grid = population.make_grid(cell_deg=s["cell_deg"], nmcl=10)
+    return population.generate(s["people"], grid, sigma=1.2, seed=98798150)
+
+
+def network_file(pop, key, threads=None):
+    """The network file (person-to-place links) of the population `key`, written by
+    CovidSim_netgen (/S) when absent; /L runs of the reference and the drop-in load
+    it.  It records the population size and the set-up seeds, which /L checks."""
+    path = os.path.join(NET_DIR, key + ".net")
+    if os.path.exists(path):
+        return path
+    if not os.path.exists(NETGEN):
+        raise RuntimeError("oracle/_ref/CovidSim_netgen not built (needs the reference checkout at build time)")
+    os.makedirs(NET_DIR, exist_ok=True)
+    part = os.path.join(NET_DIR, key + ".part.net")
+    if os.path.exists(part):
+        os.remove(part)
+    run_reference(pop, 1, nr=1, binary=NETGEN, threads=threads, extra_args=("/S:" + part,), timeout=7200)
+    os.replace(part, path)
+    return path
 
 
 def parse_timing(stderr):
@@ -95,15 +140,17 @@ def read_severity(path):
     return {k: data[:, i] for i, k in enumerate(head)}
 
 
-def time_reference(workload, steps=3, warmup=3):
-    if not os.path.exists(BIN):
-        return {"unavailable": "oracle/_ref/CovidSim_timed not built (the reference checkout was absent at build time)"}
-    sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
-    from covidsim_b200 import population
+def time_reference(workload, steps=3, warmup=3, binary=BIN, threads=None, env=None, pop=None):
+    """Sweep throughput of `binary` on a workload sample: warmup + steps realisations
+    in one process, the last `steps` timed (wall time of the sweep calls)."""
+    if not os.path.exists(binary):
+        return {"unavailable": "oracle/_ref/%s not built (the reference checkout was absent at build time)"
+                               % os.path.basename(binary)}
     s = SAMPLES[workload]
-    grid = population.make_grid(cell_deg=s["cell_deg"], nmcl=10)
-    pop = population.generate(s["people"], grid, sigma=1.2, seed=98798150)
-    res = run_reference(pop, s["days"], nr=warmup + steps, interventions=s["interventions"], threshold=s["threshold"])
+    pop = pop if pop is not None else sample_population(s)
+    extra = ("/L:" + network_file(pop, workload, threads=threads),) if s.get("network") else ()
+    res = run_reference(pop, s["days"], nr=warmup + steps, interventions=s["interventions"], threshold=s["threshold"],
+                        binary=binary, threads=threads, env=env, extra_args=extra, timeout=7200)
     rows = res["rows"][warmup:warmup + steps]
     if len(rows) < steps:
         return {"unavailable": "reference produced %d timed realisations" % len(rows)}
@@ -111,4 +158,18 @@ def time_reference(workload, steps=3, warmup=3):
     secs = sum(r["infect_s"] + r["incub_s"] for r in rows)
     return {"value": person_steps / secs, "ms_per_step": 1e3 * secs / steps, "cores": res["threads"],
             "sample": s["note"] + "; %d realisations after %d warm-up, sweep wall time (omp_get_wtime), %d threads"
-                      % (steps, warmup, res["threads"]), "rows": rows}
+                      % (steps, warmup, res["threads"]), "rows": rows, "wall": res["wall"], "dropin": res.get("dropin")}
+
+
+def time_dropin(workload, steps=3, warmup=1, device=0, threads=None, pop=None):
+    """The same as time_reference through the drop-in: the reference executable with
+    the GPU sweep linked in, on this process's CUDA device `device` (the drop-in uses
+    its device 0, so it is given that one device only)."""
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if visible:
+        ids = [x for x in visible.split(",") if x.strip()]
+        visible = ids[device] if device < len(ids) else str(device)
+    else:
+        visible = str(device)
+    env = {"OMP_WAIT_POLICY": "passive", "CUDA_VISIBLE_DEVICES": visible}
+    return time_reference(workload, steps=steps, warmup=warmup, binary=DROPIN, threads=threads, env=env, pop=pop)
