@@ -438,8 +438,9 @@ def e2e_dropin(args, local, world, dist, n_cells):
     import ctypes
     import refrun
     from covidsim_b200 import abi, sim
-    res = refrun.time_dropin(args.workload, steps=args.steps, warmup=1, device=local,
-                             threads=min(os.cpu_count() or 8, 32))
+    # the host's thread count, as the reference arm: the reference's set-up, and so the
+    # population the network file fits, depends on it
+    res = refrun.time_dropin(args.workload, steps=args.steps, warmup=1, device=local, threads=os.cpu_count())
     if "unavailable" in res:
         return {"unavailable": res["unavailable"]}
     rows = res["rows"]

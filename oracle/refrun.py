@@ -66,17 +66,20 @@ def sample_population(s):
     return population.generate(s["people"], grid, sigma=1.2, seed=98798150)
 
 
-def network_file(pop, key, threads=None):
+def network_file(pop, key, threads):
     """The network file (person-to-place links) of the population `key`, written by
     CovidSim_netgen (/S) when absent; /L runs of the reference and the drop-in load
-    it.  It records the population size and the set-up seeds, which /L checks."""
-    path = os.path.join(NET_DIR, key + ".net")
+    it.  It records the population size and the set-up seeds, which /L checks.  The
+    reference generates its places thread by thread with per-thread random streams
+    (src/SetupModel.cpp:1520-1530), so its population, and the file that fits it,
+    depend on the thread count: one file per count."""
+    path = os.path.join(NET_DIR, "%s_t%d.net" % (key, threads))
     if os.path.exists(path):
         return path
     if not os.path.exists(NETGEN):
         raise RuntimeError("oracle/_ref/CovidSim_netgen not built (needs the reference checkout at build time)")
     os.makedirs(NET_DIR, exist_ok=True)
-    part = os.path.join(NET_DIR, key + ".part.net")
+    part = path[:-4] + ".part.net"
     if os.path.exists(part):
         os.remove(part)
     run_reference(pop, 1, nr=1, binary=NETGEN, threads=threads, extra_args=("/S:" + part,), timeout=7200)
@@ -148,7 +151,8 @@ def time_reference(workload, steps=3, warmup=3, binary=BIN, threads=None, env=No
                                % os.path.basename(binary)}
     s = SAMPLES[workload]
     pop = pop if pop is not None else sample_population(s)
-    extra = ("/L:" + network_file(pop, workload, threads=threads),) if s.get("network") else ()
+    threads = threads or os.cpu_count()
+    extra = ("/L:" + network_file(pop, workload, threads),) if s.get("network") else ()
     res = run_reference(pop, s["days"], nr=warmup + steps, interventions=s["interventions"], threshold=s["threshold"],
                         binary=binary, threads=threads, env=env, extra_args=extra, timeout=7200)
     rows = res["rows"][warmup:warmup + steps]
