@@ -457,7 +457,8 @@ def e2e_dropin(args, local, world, dist, n_cells):
                     "network file as the reference arm; wall time of the sweep calls per realisation: state upload "
                     "from the reference's host structures at its start, device sweeps, per-step copy of cell "
                     "counts and counters back",
-            "realisations": len(rows), "host_threads": rows[0]["threads"], "process_wall_s": round(res["wall"], 1)}
+            "realisations": len(rows), "host_threads": rows[0]["threads"], "process_wall_s": round(res["wall"], 1),
+            "network_file": res.get("network_file")}
 
 
 def extra_600(args, local, world, dist):
@@ -551,7 +552,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": METRIC, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "reference_sample": res["sample"]},
+        "config": {"workload": desc, "reference_sample": res["sample"], "network_file": res.get("network_file"),
+                   "process_wall_s": round(res["wall"], 1)},
         "cpu_baseline": {"value": round(v, 1), "unit": METRIC, "cores": res["cores"], "kind": "reference",
                          "sample": res["sample"]},
         "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

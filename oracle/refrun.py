@@ -70,10 +70,27 @@ def network_file(pop, key, threads):
     """The network file (person-to-place links) of the population `key`, written by
     CovidSim_netgen (/S) when absent; /L runs of the reference and the drop-in load
     it.  It records the population size and the set-up seeds, which /L checks.  The
-    reference generates its places thread by thread with per-thread random streams
-    (src/SetupModel.cpp:1520-1530), so its population, and the file that fits it,
-    depend on the thread count: one file per count."""
-    path = os.path.join(NET_DIR, "%s_t%d.net" % (key, threads))
+    people the reference sets up depend on the density file, and its places are
+    generated thread by thread with per-thread random streams (src/SetupModel.cpp:
+    1520-1530), so a file fits one density file and one thread count: both are in
+    its name (the density file by a hash of its bytes, which can differ between
+    machines whose floating-point library rounds the generator's draws
+    differently)."""
+    import hashlib
+    sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
+    from covidsim_b200 import refconfig
+    wd = tempfile.mkdtemp(prefix="csnet_")
+    try:
+        dens = os.path.join(wd, "density.txt")
+        refconfig.write_density(dens, pop)
+        h = hashlib.sha256()
+        with open(dens, "rb") as f:
+            for chunk in iter(lambda: f.read(1 << 24), b""):
+                h.update(chunk)
+        digest = h.hexdigest()[:12]
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+    path = os.path.join(NET_DIR, "%s_%s_t%d.net" % (key, digest, threads))
     if os.path.exists(path):
         return path
     if not os.path.exists(NETGEN):
@@ -162,7 +179,8 @@ def time_reference(workload, steps=3, warmup=3, binary=BIN, threads=None, env=No
     secs = sum(r["infect_s"] + r["incub_s"] for r in rows)
     return {"value": person_steps / secs, "ms_per_step": 1e3 * secs / steps, "cores": res["threads"],
             "sample": s["note"] + "; %d realisations after %d warm-up, sweep wall time (omp_get_wtime), %d threads"
-                      % (steps, warmup, res["threads"]), "rows": rows, "wall": res["wall"], "dropin": res.get("dropin")}
+                      % (steps, warmup, res["threads"]), "rows": rows, "wall": res["wall"], "dropin": res.get("dropin"),
+            "network_file": os.path.basename(extra[0][3:]) if extra else None}
 
 
 def time_dropin(workload, steps=3, warmup=1, device=0, threads=None, pop=None):
