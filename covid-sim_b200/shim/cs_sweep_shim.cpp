@@ -13,10 +13,15 @@
 //                        and create the device context;
 //   first call of a run  copy the host state InitModel + SeedInfection left behind
 //                        (people, cell lists, S0, tot_prob) to the device;
-//   every step           run the device sweeps, then copy back what RecordSample
-//                        reads: per-cell S/L/I/R/D and the StateT counters;
-//   UpdateProbs          noticed through a change of the host cells' S0, then
-//                        recomputed on the device from the device's own counts;
+//   every step           run the device sweeps (one replay of the captured timestep
+//                        graph: RunModel calls IncubRecoverySweep right after
+//                        InfectSweep) and wait for them;
+//   every output step    copy back what RecordSample reads on its next call:
+//                        per-cell S/L/I/R/D and the StateT counters;
+//   UpdateProbs          RunModel's own test (src/CovidSim.cpp:1515-1521: the
+//                        susceptible fraction of State.S fell by more than 0.2 since
+//                        the last call), evaluated at the same point of the step, then
+//                        UpdateProbs recomputed on the device from its own counts;
 //   interventions        the host's own trigger logic (RecordSample's start times,
 //                        src/CovidSim.cpp:3598-3649) and TreatSweep
 //                        (src/Sweep.cpp:1324-2004) keep running on the host; before
@@ -66,7 +71,9 @@ namespace {
 cs_gpu_ctx* g_ctx = nullptr;
 int g_run = -1;
 PopVar g_base;  // StateT[0] as InitModel + SeedInfection left it; device counters add to it
-long long g_s0_sig = -1;
+double g_prev_prop = 1.0;      // RunModel's PreviousProportionSusceptible (src/CovidSim.cpp:1395)
+bool g_update_probs = false;   // RunModel called UpdateProbs(0) after the last step
+long g_step_in_run = 0;        // timesteps of the current realisation so far
 int64_t g_tg_base = 0, g_si_base = 0, g_ntg_base = 0, g_tg_set = 0, g_si_set = 0, g_ntg_set = 0;
 std::vector<int32_t> g_S, g_L, g_I, g_R, g_D;
 cs_params g_params;
@@ -207,6 +214,10 @@ void unsupported_features()
     if (P.FalsePositiveRate > 0) ERR_CRITICAL("GPU sweep: false-positive cases are not supported\n");
     if (P.DoHolidays && P.NumHolidays > 0) ERR_CRITICAL("GPU sweep: holidays are not supported\n");
     if (P.DoInterventionDelaysByAdUnit) ERR_CRITICAL("GPU sweep: intervention delays by admin unit are not supported\n");
+    if (P.InfectionImportRate1 > 0 || P.InfectionImportRate2 > 0 || P.DurImportTimeProfile > 0)
+        ERR_CRITICAL("GPU sweep: importation of infections during a run is not supported\n");
+    if (P.FalsePositivePerCapitaIncidence > 0) ERR_CRITICAL("GPU sweep: false-positive cases are not supported\n");
+    if (P.DoSI) ERR_CRITICAL("GPU sweep: the SI model (no IncubRecoverySweep) is not supported\n");
     if (P.DoAdUnits && P.DoAdminTriggers && P.NumAdunits > CS_MAX_ADUNITS)
         ERR_CRITICAL_FMT("GPU sweep: admin-unit triggers over more than %d admin units are not supported\n", CS_MAX_ADUNITS);
 }
@@ -334,13 +345,6 @@ void create_context()
     std::fprintf(stderr, "GPU sweep: %d people, %d populated cells on device\n", N, NC);
 }
 
-long long s0_signature()
-{
-    long long s = 0;
-    for (int c = 0; c < P.NumPopulatedCells; c++) s = s * 1000003 + CellLookup[c]->S0;
-    return s;
-}
-
 void upload_run_state(int run)
 {
     const int N = P.PopSize, NC = P.NumPopulatedCells;
@@ -395,7 +399,9 @@ void upload_run_state(int run)
     g_sd_min_end = 0xFFFFFFFFu;
     g_iv_sent = false;
     g_events.clear();
-    g_s0_sig = s0_signature();
+    g_prev_prop = 1.0;
+    g_update_probs = false;
+    g_step_in_run = 0;
     g_tg_base = g_si_base = g_ntg_base = 0;
     g_tg_set = g_si_set = g_ntg_set = 0;
 }
@@ -404,6 +410,7 @@ void upload_run_state(int run)
 void sync_back()
 {
     check(cs_gpu_get_cell_counts(g_ctx, g_S.data(), g_L.data(), g_I.data(), g_R.data(), g_D.data()), "cs_gpu_get_cell_counts");
+#pragma omp parallel for schedule(static)
     for (int c = 0; c < P.NumPopulatedCells; c++) {
         Cell* x = CellLookup[c];
         x->S = g_S[c]; x->L = g_L[c]; x->I = g_I[c]; x->R = g_R[c]; x->D = g_D[c];
@@ -567,12 +574,14 @@ void InfectSweep(double t, int run)
     if (run != g_run) {
         upload_run_state(run);
         g_run = run;
-    } else if (s0_signature() != g_s0_sig) {
+    } else if (g_update_probs) {
         check(cs_gpu_update_probs(g_ctx, 0), "cs_gpu_update_probs");  // the host ran UpdateProbs(0)
-        g_s0_sig = s0_signature();
+        g_update_probs = false;
     }
     mirror_host_interventions(t);
-    check(cs_gpu_infect_sweep(g_ctx, t, run), "cs_gpu_infect_sweep");
+    // RunModel calls IncubRecoverySweep(t) right after this call (src/CovidSim.cpp:
+    // 1488-1490), so the whole timestep runs here as one replay of its graph
+    check(cs_gpu_step(g_ctx, t, run), "cs_gpu_step");
     if (g_timing.empty() || g_timing.back().run != run) {
         g_timing.push_back(RunTiming());
         g_timing.back().run = run;
@@ -588,7 +597,16 @@ int TreatSweep(double t)
 {
     const int gt = global_trig_value();   // the value the reference's TreatSweep will use
     const int r = ref_TreatSweep(t);
-    if (g_ctx && g_run >= 0) mirror_treat_sweep(t, gt);
+    if (g_ctx && g_run >= 0) {
+        mirror_treat_sweep(t, gt);
+        // RunModel's UpdateProbs test runs next in this timestep on the State.S the
+        // last RecordSample set, which no call in between changes
+        const double prop = ((double)(State.S)) / ((double)P.PopSize);
+        if ((g_prev_prop - prop) > 0.2) {
+            g_prev_prop = prop;
+            g_update_probs = true;
+        }
+    }
     return r;
 }
 // TreatSweep's place closures (src/Sweep.cpp:1686, 1733): the drop-in's Sweep.cpp
@@ -638,7 +656,13 @@ void cs_shim_DoPlaceOpen(int i, int j, unsigned short int TimeStepNow)
 void IncubRecoverySweep(double t)
 {
     const double t0 = omp_get_wtime();
-    check(cs_gpu_incub_recovery_sweep(g_ctx, t), "cs_gpu_incub_recovery_sweep");
-    sync_back();
+    (void)t;
+    check(cs_gpu_sync(g_ctx), "cs_gpu_sync");   // the timestep's device work, all of it timed
+    // RecordSample reads the cells and counters at the start of the next output step.
+    // RunModel stops calling the sweeps mid-output-step only once State.L + State.I
+    // was 0 at the last RecordSample, after which no sweep changes anything; a run
+    // with a limit on infections is copied back every step all the same
+    g_step_in_run++;
+    if (P.LimitNumInfections || g_step_in_run % P.NumModelTimeStepsPerOutputTimeStep == 0) sync_back();
     if (!g_timing.empty()) g_timing.back().incub += omp_get_wtime() - t0;
 }

@@ -33,6 +33,12 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v) { 
 int cs_gpu_update_probs(cs_gpu_ctx* c, int do_place) { return cs_cpu_update_probs((cs_cpu_ctx*)c, do_place); }
 int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run) { return cs_cpu_infect_sweep((cs_cpu_ctx*)c, t, run); }
 int cs_gpu_incub_recovery_sweep(cs_gpu_ctx* c, double t) { return cs_cpu_incub_recovery_sweep((cs_cpu_ctx*)c, t); }
+int cs_gpu_step(cs_gpu_ctx* c, double t, int run)
+{
+    int r = cs_cpu_infect_sweep((cs_cpu_ctx*)c, t, run);
+    return r ? r : cs_cpu_incub_recovery_sweep((cs_cpu_ctx*)c, t);
+}
+int cs_gpu_sync(cs_gpu_ctx* c) { (void)c; return 0; }
 int cs_gpu_get_counters(cs_gpu_ctx* c, cs_counters* out) { return cs_cpu_get_counters((cs_cpu_ctx*)c, out); }
 int cs_gpu_set_interventions(cs_gpu_ctx* c, const cs_interventions* iv) { return cs_cpu_set_interventions((cs_cpu_ctx*)c, iv); }
 int cs_gpu_place_events(cs_gpu_ctx* c, const cs_place_event* ev, int n) { return cs_cpu_place_events((cs_cpu_ctx*)c, ev, n); }

@@ -170,8 +170,20 @@ def time_reference(workload, steps=3, warmup=3, binary=BIN, threads=None, env=No
     pop = pop if pop is not None else sample_population(s)
     threads = threads or os.cpu_count()
     extra = ("/L:" + network_file(pop, workload, threads),) if s.get("network") else ()
-    res = run_reference(pop, s["days"], nr=warmup + steps, interventions=s["interventions"], threshold=s["threshold"],
-                        binary=binary, threads=threads, env=env, extra_args=extra, timeout=7200)
+    run = lambda: run_reference(pop, s["days"], nr=warmup + steps, interventions=s["interventions"],
+                                threshold=s["threshold"], binary=binary, threads=threads, env=env, extra_args=extra,
+                                timeout=7200)
+    try:
+        res = run()
+    except RuntimeError as e:
+        # the reference's set-up may place people differently from the run that wrote
+        # the cached file (its place generation is threaded): write the file again
+        # from this machine's set-up and retry once
+        if not extra or not re.search(r"place link|does not match|Incompatible network file", str(e)):
+            raise
+        os.remove(extra[0][3:])
+        extra = ("/L:" + network_file(pop, workload, threads),)
+        res = run()
     rows = res["rows"][warmup:warmup + steps]
     if len(rows) < steps:
         return {"unavailable": "reference produced %d timed realisations" % len(rows)}
