@@ -132,6 +132,7 @@ def load_library(path=LIB_PATH):
         "cs_sizeof_counters": (C.c_size_t, []),
         "cs_sizeof_interventions": (C.c_size_t, []),
         "cs_sizeof_run_policy": (C.c_size_t, []),
+        "cs_kernel_arch": (I, [P(I), P(I)]),
         "cs_build_kernel_table": (I, [I, D, D, D, D, D, I, I, V, V, P(D)]),
         "cs_kernel_num": (D, [V, V, I, I, D, D]),
         "cs_gpu_create": (I, [P(cs_population), P(cs_params), I, P(V)]),

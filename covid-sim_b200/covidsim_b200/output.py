@@ -42,7 +42,10 @@ def time_series(blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0):
                    ("incDeath_ILI", "cumDeath_ILI"), ("incDeath_SARI", "cumDeath_SARI"),
                    ("incDeath_Critical", "cumDeath_Critical"), ("incHQ", "cumHQ")):
         ts[k] = _inc(_col(b, src))
-    ntg, tg, si = _col(b, "nTG"), _col(b, "cumTG"), _col(b, "cumSI")
+    # RecordSample reads and zeroes the generation-time sums at every sample
+    # (src/CovidSim.cpp:3065-3068, 3141-3146): means over each output step's new
+    # infections, from the blocks' cumulative sums
+    ntg, tg, si = _inc(_col(b, "nTG")), _inc(_col(b, "cumTG")), _inc(_col(b, "cumSI"))
     with np.errstate(invalid="ignore", divide="ignore"):
         ts["meanTG"] = np.where(ntg > 0, model_timestep * tg / np.maximum(ntg, 1), 0.0)
         ts["meanSI"] = np.where(ntg > 0, model_timestep * si / np.maximum(ntg, 1), 0.0)

@@ -2067,6 +2067,18 @@ size_t cs_sizeof_interventions(void) { return sizeof(cs_interventions); }
 size_t cs_sizeof_run_policy(void) { return sizeof(cs_run_policy); }
 
 const char* cs_gpu_last_error(const cs_gpu_ctx* c) { return c ? c->err : "null context"; }
+
+int cs_kernel_arch(int* binary_version, int* ptx_version)
+{
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, (const void*)k_apply_infections) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return CS_E_CUDA;
+    }
+    if (binary_version) *binary_version = a.binaryVersion;
+    if (ptx_version) *ptx_version = a.ptxVersion;
+    return CS_OK;
+}
 void* cs_gpu_stream(cs_gpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
 int64_t cs_gpu_launch_count(const cs_gpu_ctx* c) { return c ? c->launches : 0; }
 

@@ -34,6 +34,9 @@
 //                        calls and TreatSweep itself reach this file because the
 //                        drop-in compiles Sweep.cpp with them renamed (oracle/Makefile),
 //                        as it does the sweeps;
+//   CS_DUMP_BLOCKS=<p>   (optional) each realisation's counter blocks -- t = 0 and
+//                        every output step, what RecordSample reads, in the layout
+//                        cs_gpu_run returns -- appended to <p>.<run>.blocks;
 //   timing               the wall time of each realisation's sweep calls (from its
 //                        first call on, the device context's creation excluded),
 //                        written to stderr at exit as oracle/ref_timing_shim.cpp
@@ -93,6 +96,7 @@ struct RunTiming {
     double infect = 0.0, incub = 0.0;
 };
 std::vector<RunTiming> g_timing;
+FILE* g_dump = nullptr;
 
 void check(int rc, const char* what)
 {
@@ -345,6 +349,8 @@ void create_context()
     std::fprintf(stderr, "GPU sweep: %d people, %d populated cells on device\n", N, NC);
 }
 
+void dump_block();
+
 void upload_run_state(int run)
 {
     const int N = P.PopSize, NC = P.NumPopulatedCells;
@@ -404,6 +410,14 @@ void upload_run_state(int run)
     g_step_in_run = 0;
     g_tg_base = g_si_base = g_ntg_base = 0;
     g_tg_set = g_si_set = g_ntg_set = 0;
+    if (const char* dump = std::getenv("CS_DUMP_BLOCKS")) {
+        if (g_dump) std::fclose(g_dump);
+        char path[4096];
+        std::snprintf(path, sizeof(path), "%s.%d.blocks", dump, run);
+        g_dump = std::fopen(path, "wb");
+        if (!g_dump) ERR_CRITICAL_FMT("GPU sweep: cannot write %s\n", path);
+        dump_block();
+    }
 }
 
 // RecordSample (src/CovidSim.cpp:3024-3120) reads per-cell counts and StateT[].
@@ -453,6 +467,40 @@ void sync_back()
     if (s.cumTG != g_tg_set || s.nTG != g_ntg_set) { g_tg_base += g_tg_set; g_si_base += g_si_set; g_ntg_base += g_ntg_set; }
     g_tg_set = k.cumTG - g_tg_base; g_si_set = k.cumSI - g_si_base; g_ntg_set = k.nTG - g_ntg_base;
     s.cumTG = (int)g_tg_set; s.cumSI = (int)g_si_set; s.nTG = (int)g_ntg_set;
+}
+
+// One counter block of the realisation, as RecordSample would sum it now: the
+// cells' S/L/I/R/D, thread 0's counters (the only ones the drop-in writes) and the
+// device's cumulative generation-time sums.
+void dump_block()
+{
+    if (!g_dump) return;
+    cs_counters b;
+    std::memset(&b, 0, sizeof(b));
+    for (int c = 0; c < P.NumPopulatedCells; c++) {
+        const Cell* x = CellLookup[c];
+        b.S += x->S; b.L += x->L; b.I += x->I; b.R += x->R; b.D += x->D;
+    }
+    b.cumR = b.R; b.cumD = b.D;   // as RecordSample sets them (src/CovidSim.cpp:3055-3056)
+    const PopVar& s = StateT[0];
+    b.cumI = s.cumI; b.cumC = s.cumC; b.cumDC = s.cumDC; b.cumFC = s.cumFC; b.cumHQ = s.cumHQ;
+    b.cumAC = s.cumAC; b.cumAA = s.cumAA; b.cumACS = s.cumACS;
+    for (int i = 0; i < INFECT_TYPE_MASK; i++) b.cumItype[i] = s.cumItype[i];
+    for (int a = 0; a < NUM_AGE_GROUPS; a++) { b.cumIa[a] = s.cumIa[a]; b.cumCa[a] = s.cumCa[a]; b.cumDa[a] = s.cumDa[a]; }
+    b.Mild = s.Mild; b.ILI = s.ILI; b.SARI = s.SARI; b.Critical = s.Critical; b.CritRecov = s.CritRecov;
+    b.cumMild = s.cumMild; b.cumILI = s.cumILI; b.cumSARI = s.cumSARI; b.cumCritical = s.cumCritical;
+    b.cumCritRecov = s.cumCritRecov; b.cumDeath_ILI = s.cumDeath_ILI; b.cumDeath_SARI = s.cumDeath_SARI;
+    b.cumDeath_Critical = s.cumDeath_Critical;
+    if (P.DoAdUnits)
+        for (int a = 0; a < P.NumAdunits && a < CS_MAX_ADUNITS; a++) {
+            b.cumI_adunit[a] = s.cumI_adunit[a]; b.cumC_adunit[a] = s.cumC_adunit[a];
+            b.cumD_adunit[a] = s.cumD_adunit[a]; b.cumDC_adunit[a] = s.cumDC_adunit[a];
+            b.cumCritical_adunit[a] = s.cumCritical_adunit[a]; b.Critical_adunit[a] = s.Critical_adunit[a];
+        }
+    cs_counters k;
+    check(cs_gpu_get_counters(g_ctx, &k), "cs_gpu_get_counters");
+    b.cumTG = g_base.cumTG + k.cumTG; b.cumSI = g_base.cumSI + k.cumSI; b.nTG = g_base.nTG + k.nTG;
+    if (std::fwrite(&b, sizeof(b), 1, g_dump) != 1) ERR_CRITICAL("GPU sweep: writing the counter blocks failed\n");
 }
 
 // Everything the host's run loop changed between two sweeps that the device sweep
@@ -663,6 +711,8 @@ void IncubRecoverySweep(double t)
     // was 0 at the last RecordSample, after which no sweep changes anything; a run
     // with a limit on infections is copied back every step all the same
     g_step_in_run++;
-    if (P.LimitNumInfections || g_step_in_run % P.NumModelTimeStepsPerOutputTimeStep == 0) sync_back();
+    const bool output_step = g_step_in_run % P.NumModelTimeStepsPerOutputTimeStep == 0;
+    if (P.LimitNumInfections || output_step) sync_back();
+    if (output_step) dump_block();
     if (!g_timing.empty()) g_timing.back().incub += omp_get_wtime() - t0;
 }

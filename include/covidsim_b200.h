@@ -344,6 +344,14 @@ size_t cs_sizeof_interventions(void);
 size_t cs_sizeof_run_policy(void);
 
 /*
+ * The architecture the library's sweep kernels were compiled for, as the CUDA
+ * runtime reports it for the current device (cudaFuncAttributes.binaryVersion and
+ * ptxVersion, major*10 + minor: 100 for sm_100a machine code).  Needs a device;
+ * returns CS_E_CUDA without one.
+ */
+int cs_kernel_arch(int* binary_version, int* ptx_version);
+
+/*
  * Build the spatial kernel lookup tables exactly as KernelLookup::setup/init
  * (src/Kernels.cpp:8-46) with norm 1: lookup[i] = K(i*delta), hi_res[i] =
  * K(i*delta/expansion), delta = longest_d2/size.  kernel_type follows

@@ -115,7 +115,8 @@ def parse_timing(stderr):
 
 def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=100, workdir=None,
                   seeds=(98798150, 729101, 17389101, 4797132),
-                  binary=BIN, keep=False, timeout=3000, series=False, duration=90.0, env=None, extra_args=()):
+                  binary=BIN, keep=False, timeout=3000, series=False, duration=90.0, env=None, extra_args=(),
+                  pre_extra=None):
     sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
     from covidsim_b200 import refconfig
     threads = threads or os.cpu_count()
@@ -129,6 +130,7 @@ def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=
         if series:  # one .severity.xls per realisation
             pre["OutputNonSummaryResults"] = 1
             pre["OutputSeverity"] = 1
+        pre.update(pre_extra or {})
         refconfig.write_params(f["pre"], pre)
         refconfig.write_params(f["params"], params)
         cmd = [binary, "/c:%d" % threads, "/PP:" + f["pre"], "/P:" + f["params"], "/A:" + f["admin"],

@@ -170,3 +170,51 @@ def test_summary_peak_statistics_follow_reference(tmp_path):
     c = 1.0 / 3
     assert np.allclose(vals, [c * h.sum(), c * (h * h).sum() - c * c * h.sum() ** 2,
                               c * t.sum(), c * (t * t).sum() - c * c * t.sum() ** 2], atol=1e-9)
+
+
+def test_tables_match_the_reference_written_tables(tmp_path):
+    """The writers against the reference's own SaveResults / SaveSummaryResults on
+    the same realisations: the reference executable with the oracle's sweeps linked
+    in (oracle/_ref/CovidSim_oracle, built from the reference's sources) runs two
+    realisations of a 20,000-person epidemic with interventions and writes its
+    tables; the drop-in dumps the counter blocks RecordSample read
+    (CS_DUMP_BLOCKS), and the tables written from them here must be the same bytes:
+    `<base>.<run>.xls`, `<base>.<run>.severity.xls` and the data rows and peak
+    statistics of `<base>.avNE.xls`."""
+    import ctypes as C
+    import os
+
+    import pytest
+
+    import ensemble
+    import refrun
+    binary = os.path.join(os.path.dirname(refrun.DROPIN), "CovidSim_oracle")
+    if not os.path.exists(binary):
+        pytest.skip("oracle/_ref/CovidSim_oracle not built (needs the reference checkout at build time)")
+    days, wd = 200, str(tmp_path)
+    refrun.run_reference(ensemble.population("interventions"), days, nr=2, threads=4, binary=binary, series=True,
+                         workdir=wd, interventions=True, threshold=5,
+                         env={"OMP_WAIT_POLICY": "passive", "CS_DUMP_BLOCKS": os.path.join(wd, "dump")},
+                         pre_extra={"OutputNonSeverity": 1})
+    small = 100    # "Maximum number of cases defining small outbreak" in the pre-parameters
+    W = C.sizeof(abi.cs_counters) // 8
+    runs = []
+    for r in range(2):
+        b = np.fromfile(os.path.join(wd, "dump.%d.blocks" % r), dtype=np.int64).reshape(-1, W)
+        # a run whose epidemic died out stops calling the sweeps; RecordSample then
+        # records the same state to the end
+        assert 1 <= b.shape[0] <= days + 1
+        runs.append(np.concatenate([b, np.repeat(b[-1:], days + 1 - b.shape[0], axis=0)]))
+        mine = os.path.join(wd, "mine.%d" % r)
+        output.write_results(mine, runs[-1], 0.25, small_epidemic_cases=small)
+        for suffix in (".xls", ".severity.xls"):
+            ref = open(os.path.join(wd, "out.%d%s" % (r, suffix))).read()
+            assert open(mine + suffix).read() == ref, "run %d %s differs" % (r, suffix)
+    output.write_summary(os.path.join(wd, "mine"), runs, 0.25, small_epidemic_cases=small)
+    ref = open(os.path.join(wd, "out.avNE.xls")).read().split("\n")
+    mine = open(os.path.join(wd, "mine.avNE.xls")).read().split("\n")
+    assert mine[1:] == ref[1:]
+    # the header: realisation counts and peak statistics (the R0 parts come from the
+    # reference's set-up, not from the counters)
+    hr, hm = ref[0].split("\t"), mine[0].split("\t")
+    assert hm[:-8] == hr[:-8] and hm[-5:] == hr[-5:], (hm[-11:], hr[-11:])
