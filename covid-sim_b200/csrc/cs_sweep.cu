@@ -15,7 +15,7 @@
 //     k_spatial              spatial contacts: block proposal + rejection, eight
 //                            draws of a contact evaluated together
 //     k_apply_infections     DoInfect for every claimed person (lowest key wins)
-//     k_partition_S          S -> L cell-list moves, one thread per touched cell
+//     k_partition_S          S -> L cell-list moves, one warp per touched cell
 //   IncubRecoverySweep
 //     k_build_active         latent + infectious people
 //     k_incub_scan           the people with an event this step
@@ -810,9 +810,12 @@ __global__ void k_block_rows(DevPop d)
 // entries warp by warp, so the list's order varies from launch to launch; nothing
 // that reads it depends on the order (random streams are keyed by person and
 // contact, conflicting claims resolve by key, tallies are integer sums, and cell
-// lists are reordered by position).
+// lists are reordered by position).  A block reserves the entries of its 256 cells
+// at once and copies them together, entry j by the thread whose turn it is, so a
+// cell with thousands of active people costs no more than its share of the block.
 __device__ __forceinline__ void k_build_active_body(const DevPop& d, int mode)
 {
+    __shared__ int s_first[kThreads], s_dst[kThreads], s_n[kThreads];
     for (int c0 = blockIdx.x * blockDim.x; c0 < d.NC; c0 += gridDim.x * blockDim.x) {
         const int c = c0 + threadIdx.x;
         int first = 0, n = 0;
@@ -821,10 +824,23 @@ __device__ __forceinline__ void k_build_active_body(const DevPop& d, int mode)
             n = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
         }
         const int o = block_reserve2(d.counts + kCntAct, n, nullptr, 0).x;
-        for (int k = 0; k < n; k++) {
-            d.act[o + k] = d.slots[first + k];
-            d.act_cell[o + k] = c;
+        s_first[threadIdx.x] = first;
+        s_dst[threadIdx.x] = o;
+        s_n[threadIdx.x] = n;
+        __syncthreads();
+        const int base = s_dst[0];                    // thread 0's entries start the block's range
+        const int total = s_dst[blockDim.x - 1] + s_n[blockDim.x - 1] - base;
+        for (int j = threadIdx.x; j < total; j += blockDim.x) {
+            // the last cell whose entries start at or before j holds entry j
+            int lo = 0, hi = blockDim.x - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_dst[mid] - base <= j) lo = mid; else hi = mid - 1;
+            }
+            d.act[base + j] = d.slots[s_first[lo] + (base + j - s_dst[lo])];
+            d.act_cell[base + j] = c0 + lo;
         }
+        __syncthreads();   // the shared arrays are refilled for the next 256 cells
     }
 }
 __global__ void k_build_active(DevPop d, int mode) { k_build_active_body(d, mode); }
@@ -1204,44 +1220,62 @@ __global__ void k_apply_infections(DevPop d) { k_apply_infections_body(d); }
 __global__ void k_apply_infections_multi(const DevPop* __restrict__ pops) { k_apply_infections_body(pops[blockIdx.y]); }
 
 // Swap-with-block-end removal of marked slots, high to low (src/Update.cpp:1402-1579
-// UpdateCell sequence).  Returns nothing; moved people get their new listpos.
-__device__ void partition_block(const DevPop& d, int base, int b0, int n, int nmarked, uint8_t want,
-                                bool relay_exit)
+// UpdateCell sequence).  Moved people get their new listpos.  One warp per block:
+// the warp reads the marks 32 positions at a time from the top and lane 0 applies
+// the swaps in descending position order, as a serial scan would.  A swap writes
+// only at its own position and above, so the marks the warp read for the positions
+// still below are the ones a serial scan would find there.
+__device__ void partition_block_warp(const DevPop& d, int base, int b0, int n, int nmarked, uint8_t want,
+                                     bool relay_exit)
 {
+    const int lane = threadIdx.x & 31;
     int cur = n, removed = 0;
-    for (int pos = b0 + n - 1; pos >= b0 && removed < nmarked; pos--) {
-        if (d.mark[pos] != want) continue;
-        cur--;
-        removed++;
-        int end = b0 + cur;
-        if (pos < end) {
-            int a = d.slots[pos], e = d.slots[end];
-            d.slots[pos] = e;
-            d.listpos[e] = pos - base;
-            d.slots[end] = a;
-            d.listpos[a] = end - base;
+    for (int top = b0 + n - 1; top >= b0 && removed < nmarked; top -= 32) {
+        const int pos = top - lane;
+        unsigned hits = __ballot_sync(0xffffffffu, pos >= b0 && d.mark[pos] == want);
+        if (lane == 0) {
+            while (hits && removed < nmarked) {
+                const int p = top - (__ffs(hits) - 1);   // lowest lane: highest position
+                hits &= hits - 1;
+                cur--;
+                removed++;
+                const int end = b0 + cur;
+                if (p < end) {
+                    int a = d.slots[p], e = d.slots[end];
+                    d.slots[p] = e;
+                    d.listpos[e] = p - base;
+                    d.slots[end] = a;
+                    d.listpos[a] = end - base;
+                }
+                d.mark[p] = 0;
+                d.mark[end] = 0;
+                if (relay_exit) {
+                    int a = d.slots[end];
+                    if (d.pstep[a] & kStepItoRD) d.mark[end] = 2;
+                }
+            }
         }
-        d.mark[pos] = 0;
-        d.mark[end] = 0;
-        if (relay_exit) {
-            int a = d.slots[end];
-            if (d.pstep[a] & kStepItoRD) d.mark[end] = 2;
-        }
+        removed = __shfl_sync(0xffffffffu, removed, 0);
+        __syncwarp();
     }
 }
 
-// S -> L list moves for every cell that gained latent people this step.
+// S -> L list moves for every cell that gained latent people this step, one warp
+// per cell.
 __device__ __forceinline__ void k_partition_S_body(const DevPop& d)
 {
     int nt = d.counts[kCntTouched];
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_cells_touched), nt);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < nt; k += warps) {
         int c = d.touched[k];
         int moved = d.cnt[c];
         int base = d.cell_start[c];
-        partition_block(d, base, base, d.S[c] + moved, moved, 1, false);
-        d.cnt[c] = 0;
-        d.cell_flag[c] = 0;
+        partition_block_warp(d, base, base, d.S[c] + moved, moved, 1, false);
+        if ((threadIdx.x & 31) == 0) {
+            d.cnt[c] = 0;
+            d.cell_flag[c] = 0;
+        }
     }
 }
 __global__ void k_partition_S(DevPop d) { k_partition_S_body(d); }
@@ -1554,16 +1588,19 @@ __global__ void __launch_bounds__(kThreads, 3) k_incub_events_multi(const DevPop
 __device__ __forceinline__ void k_partition_LI_body(const DevPop& d)
 {
     int nt = d.counts[kCntTouched];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < nt; k += warps) {
         int c = d.touched[k];
         int v = d.cnt[c];
         int nLI = v & 0xffff, nIR = (v >> 16) & 0xffff;
         int base = d.cell_start[c];
         int S = d.S[c], L = d.L[c], I = d.I[c];
-        if (nLI) partition_block(d, base, base + S, L + nLI, nLI, 1, true);
-        if (nIR) partition_block(d, base, base + S + L, I + nIR, nIR, 2, false);
-        d.cnt[c] = 0;
-        d.cell_flag[c] = 0;
+        if (nLI) partition_block_warp(d, base, base + S, L + nLI, nLI, 1, true);
+        if (nIR) partition_block_warp(d, base, base + S + L, I + nIR, nIR, 2, false);
+        if ((threadIdx.x & 31) == 0) {
+            d.cnt[c] = 0;
+            d.cell_flag[c] = 0;
+        }
     }
 }
 __global__ void k_partition_LI(DevPop d) { k_partition_LI_body(d); }

@@ -38,7 +38,8 @@
 //                        every output step, what RecordSample reads, in the layout
 //                        cs_gpu_run returns -- appended to <p>.<run>.blocks;
 //   timing               the wall time of each realisation's sweep calls (from its
-//                        first call on, the device context's creation excluded),
+//                        first call on, the device context's creation excluded)
+//                        and of the hand-over after TreatSweep,
 //                        written to stderr at exit as oracle/ref_timing_shim.cpp
 //                        writes the reference's:  SWEEPTIMING run=.. pop=.. threads=..
 //                        steps=.. infect_s=.. incub_s=..
@@ -643,10 +644,16 @@ void InfectSweep(double t, int run)
 int ref_TreatSweep(double t);
 int TreatSweep(double t)
 {
+    double t0 = omp_get_wtime();
     const int gt = global_trig_value();   // the value the reference's TreatSweep will use
+    double spent = omp_get_wtime() - t0;
     const int r = ref_TreatSweep(t);
     if (g_ctx && g_run >= 0) {
+        t0 = omp_get_wtime();
         mirror_treat_sweep(t, gt);
+        // the hand-over is the drop-in's own work: timed with its sweeps
+        spent += omp_get_wtime() - t0;
+        if (!g_timing.empty()) g_timing.back().infect += spent;
         // RunModel's UpdateProbs test runs next in this timestep on the State.S the
         // last RecordSample set, which no call in between changes
         const double prop = ((double)(State.S)) / ((double)P.PopSize);
