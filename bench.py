@@ -433,8 +433,10 @@ def e2e_dropin(args, local, world, dist, n_cells):
     """e2e through the drop-in: warm-up 1 and `steps` timed realisations of the
     reference executable with the GPU sweep linked in, loading the workload's
     network file; value = people x timesteps / wall time of the sweep calls (state
-    upload at each realisation's start, the device sweeps, the per-step copy of the
-    cell counts and counters back to the reference's host structures)."""
+    upload at each realisation's start, the device sweeps and the wait for them at
+    every timestep, the copy of the cell counts and counters back to the
+    reference's host structures at every output step, the hand-over of the host's
+    interventions)."""
     import ctypes
     import refrun
     from covidsim_b200 import abi, sim
@@ -450,13 +452,17 @@ def e2e_dropin(args, local, world, dist, n_cells):
     n, steps = rows[0]["pop"], rows[0]["steps"]
     arrs, _ = sim.state_arrays(n, n_cells)   # the grid's populated cells (every cell at 10M people)
     h2d = sum(a.nbytes for a in arrs.values())
-    d2h = steps * (5 * 4 * n_cells + ctypes.sizeof(abi.cs_counters))
+    days = refrun.SAMPLES[args.workload]["days"]   # one copy back per output step (a day)
+    d2h = days * (5 * 4 * n_cells + ctypes.sizeof(abi.cs_counters))
+    parts = {k: round(1e3 * sum(r.get(k, 0.0) for r in rows) / len(rows), 3) for k in ("upload_s", "copyback_s")}
     return {"value": round(person_steps * world / secs, 1), "unit": METRIC, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": round(1e3 * secs / len(rows), 3),
+            "ms_per_step_parts": {"state_upload": parts["upload_s"], "copy_back": parts["copyback_s"]},
             "what": "the reference executable with the GPU sweep linked in (oracle/_ref/CovidSim_b200), the same "
                     "network file as the reference arm; wall time of the sweep calls per realisation: state upload "
-                    "from the reference's host structures at its start, device sweeps, per-step copy of cell "
-                    "counts and counters back",
+                    "from the reference's host structures at its start, device sweeps (one graph per timestep, "
+                    "waited for), copy of cell counts and counters back at each output step, intervention "
+                    "hand-over",
             "realisations": len(rows), "host_threads": rows[0]["threads"], "process_wall_s": round(res["wall"], 1),
             "network_file": res.get("network_file")}
 

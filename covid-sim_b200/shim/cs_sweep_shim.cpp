@@ -95,6 +95,7 @@ struct RunTiming {
     int run;
     long steps = 0;
     double infect = 0.0, incub = 0.0;
+    double upload = 0.0, copyback = 0.0;   // parts of the two above
 };
 std::vector<RunTiming> g_timing;
 FILE* g_dump = nullptr;
@@ -352,45 +353,64 @@ void create_context()
 
 void dump_block();
 
+// Host staging of the start state, kept from run to run so that later runs write
+// into memory that is already mapped.
+struct Staging {
+    std::vector<int8_t> inf;
+    std::vector<uint8_t> sev, fl;
+    std::vector<uint16_t> it, lt, rt, st, ct, sd, as, ae, iso, qs, dt;
+    std::vector<float> infn, susc, pa, pc;
+    std::vector<int32_t> infector, listpos, slots, S0, cS, cL, cI, cR, cD, cell_ofs;
+    std::vector<int16_t> itype;
+    std::vector<double> tp;
+};
+Staging g_stage;
+
 void upload_run_state(int run)
 {
     const int N = P.PopSize, NC = P.NumPopulatedCells;
-    std::vector<int8_t> inf(N);
-    std::vector<uint8_t> sev(N), fl(N);
-    std::vector<uint16_t> it(N), lt(N), rt(N), st(N), ct(N), sd(N), as(N), ae(N), iso(N), qs(N), dt(N);
-    std::vector<float> infn(N), susc(N), pa(N), pc(N);
-    std::vector<int32_t> infector(N), listpos(N), slots(N), S0(NC), cS(NC), cL(NC), cI(NC), cR(NC), cD(NC);
-    std::vector<int16_t> itype(N);
-    std::vector<double> tp(NC);
+    Staging& g = g_stage;
+    if ((int)g.inf.size() != N || (int)g.tp.size() != NC) {
+        for (auto* v : {&g.sev, &g.fl}) v->resize(N);
+        for (auto* v : {&g.it, &g.lt, &g.rt, &g.st, &g.ct, &g.sd, &g.as, &g.ae, &g.iso, &g.qs, &g.dt}) v->resize(N);
+        for (auto* v : {&g.infn, &g.susc, &g.pa, &g.pc}) v->resize(N);
+        for (auto* v : {&g.infector, &g.listpos, &g.slots}) v->resize(N);
+        for (auto* v : {&g.S0, &g.cS, &g.cL, &g.cI, &g.cR, &g.cD}) v->resize(NC);
+        g.inf.resize(N); g.itype.resize(N); g.tp.resize(NC);
+        g.cell_ofs.assign(NC + 1, 0);
+        for (int c = 0; c < NC; c++) g.cell_ofs[c + 1] = g.cell_ofs[c] + CellLookup[c]->n;
+    }
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < N; i++) {
         const Person& a = Hosts[i];
-        inf[i] = inf_of(a);
-        sev[i] = (uint8_t)((int)a.Severity_Current | ((int)a.Severity_Final << 4));
-        fl[i] = (uint8_t)((a.to_die ? CS_DF_TO_DIE : 0) | (a.detected ? CS_DF_DETECTED : 0) |
-                          ((HostsQuarantine[i].comply & 3) << CS_DF_QUAR_COMPLY_SHIFT));
-        it[i] = a.infection_time; lt[i] = a.latent_time; rt[i] = a.recovery_or_death_time;
-        st[i] = a.SARI_time; ct[i] = a.Critical_time; sd[i] = a.Stepdown_time;
-        as[i] = a.absent_start_time; ae[i] = a.absent_stop_time; iso[i] = a.isolation_start_time;
-        qs[i] = HostsQuarantine[i].start_time; dt[i] = a.detected_time;
-        infn[i] = a.infectiousness; susc[i] = a.susc; pa[i] = a.ProbAbsent; pc[i] = a.ProbCare;
-        infector[i] = a.infector; itype[i] = a.infect_type; listpos[i] = a.listpos;
+        g.inf[i] = inf_of(a);
+        g.sev[i] = (uint8_t)((int)a.Severity_Current | ((int)a.Severity_Final << 4));
+        g.fl[i] = (uint8_t)((a.to_die ? CS_DF_TO_DIE : 0) | (a.detected ? CS_DF_DETECTED : 0) |
+                            ((HostsQuarantine[i].comply & 3) << CS_DF_QUAR_COMPLY_SHIFT));
+        g.it[i] = a.infection_time; g.lt[i] = a.latent_time; g.rt[i] = a.recovery_or_death_time;
+        g.st[i] = a.SARI_time; g.ct[i] = a.Critical_time; g.sd[i] = a.Stepdown_time;
+        g.as[i] = a.absent_start_time; g.ae[i] = a.absent_stop_time; g.iso[i] = a.isolation_start_time;
+        g.qs[i] = HostsQuarantine[i].start_time; g.dt[i] = a.detected_time;
+        g.infn[i] = a.infectiousness; g.susc[i] = a.susc; g.pa[i] = a.ProbAbsent; g.pc[i] = a.ProbCare;
+        g.infector[i] = a.infector; g.itype[i] = a.infect_type; g.listpos[i] = a.listpos;
     }
-    int o = 0;
+#pragma omp parallel for schedule(dynamic, 64)
     for (int c = 0; c < NC; c++) {
-        Cell* x = CellLookup[c];
-        for (int k = 0; k < x->n; k++) slots[o + k] = x->susceptible[k];
-        o += x->n;
-        cS[c] = x->S; cL[c] = x->L; cI[c] = x->I; cR[c] = x->R; cD[c] = x->D; S0[c] = x->S0; tp[c] = x->tot_prob;
+        const Cell* x = CellLookup[c];
+        std::memcpy(g.slots.data() + g.cell_ofs[c], x->susceptible, sizeof(int32_t) * (size_t)x->n);
+        g.cS[c] = x->S; g.cL[c] = x->L; g.cI[c] = x->I; g.cR[c] = x->R; g.cD[c] = x->D; g.S0[c] = x->S0;
+        g.tp[c] = x->tot_prob;
     }
     cs_state_view v;
     std::memset(&v, 0, sizeof(v));
-    v.inf = inf.data(); v.severity = sev.data(); v.flags = fl.data(); v.infection_time = it.data(); v.latent_time = lt.data();
-    v.recovery_or_death_time = rt.data(); v.SARI_time = st.data(); v.Critical_time = ct.data(); v.Stepdown_time = sd.data();
-    v.absent_start_time = as.data(); v.absent_stop_time = ae.data(); v.isolation_start_time = iso.data();
-    v.quar_start_time = qs.data(); v.detected_time = dt.data(); v.infectiousness = infn.data(); v.susc = susc.data();
-    v.ProbAbsent = pa.data(); v.ProbCare = pc.data(); v.infector = infector.data(); v.infect_type = itype.data();
-    v.listpos = listpos.data(); v.cell_S = cS.data(); v.cell_L = cL.data(); v.cell_I = cI.data(); v.cell_R = cR.data();
-    v.cell_D = cD.data(); v.cell_S0 = S0.data(); v.cell_tot_prob = tp.data(); v.cell_slots = slots.data();
+    v.inf = g.inf.data(); v.severity = g.sev.data(); v.flags = g.fl.data(); v.infection_time = g.it.data();
+    v.latent_time = g.lt.data(); v.recovery_or_death_time = g.rt.data(); v.SARI_time = g.st.data();
+    v.Critical_time = g.ct.data(); v.Stepdown_time = g.sd.data(); v.absent_start_time = g.as.data();
+    v.absent_stop_time = g.ae.data(); v.isolation_start_time = g.iso.data(); v.quar_start_time = g.qs.data();
+    v.detected_time = g.dt.data(); v.infectiousness = g.infn.data(); v.susc = g.susc.data(); v.ProbAbsent = g.pa.data();
+    v.ProbCare = g.pc.data(); v.infector = g.infector.data(); v.infect_type = g.itype.data(); v.listpos = g.listpos.data();
+    v.cell_S = g.cS.data(); v.cell_L = g.cL.data(); v.cell_I = g.cI.data(); v.cell_R = g.cR.data(); v.cell_D = g.cD.data();
+    v.cell_S0 = g.S0.data(); v.cell_tot_prob = g.tp.data(); v.cell_slots = g.slots.data();
     uint64_t seed = ((uint64_t)(uint32_t)P.runSeed1 << 32) ^ (uint32_t)P.runSeed2 ^ (0x9E3779B97F4A7C15ull * (uint64_t)(run + 1));
     check(cs_gpu_upload_state(g_ctx, seed, &v), "cs_gpu_upload_state");
     // seeding ran DoInfect on the host (thread 0's counters); the device counts from zero
@@ -607,8 +627,8 @@ void mirror_treat_sweep(double t, int gt)
 void report_timing()
 {
     for (const RunTiming& r : g_timing)
-        std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f\n", r.run, P.PopSize,
-                     P.NumThreads, r.steps, r.infect, r.incub);
+        std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f upload_s=%.6f copyback_s=%.6f\n",
+                     r.run, P.PopSize, P.NumThreads, r.steps, r.infect, r.incub, r.upload, r.copyback);
 }
 
 }  // namespace
@@ -620,9 +640,11 @@ void InfectSweep(double t, int run)
         std::atexit(report_timing);
     }
     const double t0 = omp_get_wtime();
+    double upload = 0.0;
     if (run != g_run) {
         upload_run_state(run);
         g_run = run;
+        upload = omp_get_wtime() - t0;
     } else if (g_update_probs) {
         check(cs_gpu_update_probs(g_ctx, 0), "cs_gpu_update_probs");  // the host ran UpdateProbs(0)
         g_update_probs = false;
@@ -636,6 +658,7 @@ void InfectSweep(double t, int run)
         g_timing.back().run = run;
     }
     g_timing.back().infect += omp_get_wtime() - t0;
+    g_timing.back().upload += upload;
     g_timing.back().steps++;
 }
 
@@ -719,7 +742,9 @@ void IncubRecoverySweep(double t)
     // with a limit on infections is copied back every step all the same
     g_step_in_run++;
     const bool output_step = g_step_in_run % P.NumModelTimeStepsPerOutputTimeStep == 0;
+    const double t1 = omp_get_wtime();
     if (P.LimitNumInfections || output_step) sync_back();
     if (output_step) dump_block();
+    if (!g_timing.empty()) g_timing.back().copyback += omp_get_wtime() - t1;
     if (!g_timing.empty()) g_timing.back().incub += omp_get_wtime() - t0;
 }

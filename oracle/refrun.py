@@ -106,10 +106,12 @@ def network_file(pop, key, threads):
 
 def parse_timing(stderr):
     rows = []
-    for m in re.finditer(r"(?:REF|SWEEP)TIMING run=(\d+) pop=(\d+) threads=(\d+) steps=(\d+) infect_s=([\d.]+) incub_s=([\d.]+)",
-                         stderr):
+    for m in re.finditer(r"(?:REF|SWEEP)TIMING run=(\d+) pop=(\d+) threads=(\d+) steps=(\d+) infect_s=([\d.]+) incub_s=([\d.]+)"
+                         r"(?: upload_s=([\d.]+) copyback_s=([\d.]+))?", stderr):
         rows.append(dict(run=int(m.group(1)), pop=int(m.group(2)), threads=int(m.group(3)), steps=int(m.group(4)),
                          infect_s=float(m.group(5)), incub_s=float(m.group(6))))
+        if m.group(7) is not None:   # the drop-in's parts: state upload, copies back
+            rows[-1].update(upload_s=float(m.group(7)), copyback_s=float(m.group(8)))
     return rows
 
 
