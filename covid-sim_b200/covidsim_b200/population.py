@@ -382,10 +382,19 @@ NETWORK_FILE_VERSION = 1
 def save_network_file(pop, path, setup_seed1, setup_seed2):
     npt = len(pop.places)
     links = np.asarray(pop.person_place, np.int32).reshape(npt, pop.n_people)
-    for t, pl in enumerate(pop.places):
-        if np.any(links[t] >= len(pl["mcell"])):
+    save_network_links(links, [len(pl["mcell"]) for pl in pop.places], path, setup_seed1, setup_seed2)
+
+
+def save_network_links(links, n_places, path, setup_seed1, setup_seed2):
+    """Write place links [place types, people] (-1: no place of that type) as the
+    reference's network file; n_places: places per type, for the bounds check
+    SavePeopleToPlaces makes (src/SetupModel.cpp:2661-2690)."""
+    links = np.asarray(links, np.int32)
+    npt, n_people = links.shape
+    for t in range(npt):
+        if np.any(links[t] >= n_places[t]):
             raise ValueError("out of bounds place link for place type %d" % t)
-    head = np.array([NETWORK_FILE_VERSION, npt, pop.n_people, setup_seed1, setup_seed2], dtype="<i4")
+    head = np.array([NETWORK_FILE_VERSION, npt, n_people, setup_seed1, setup_seed2], dtype="<i4")
     with open(path, "wb") as f:
         f.write(head.tobytes())
         f.write(np.ascontiguousarray(links.T, dtype="<i4").tobytes())

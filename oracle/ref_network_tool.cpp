@@ -25,11 +25,20 @@
 //     probability proportional to the type's kernel K(d) x remaining capacity, the
 //     weight the reference's searches use (src/SetupModel.cpp:2265-2290, 2404-2415).
 // Age-restricted availability (AvailByAge) is not modelled.
+//
+// With CS_NETGEN_LOAD=<file> in the environment the replacement assigns nothing
+// itself: it calls the reference's own LoadPeopleToPlaces on that file, so that a
+// /S run writes back, through the reference's SavePeopleToPlaces, exactly the links
+// the reference's loader read (the reference's command line refuses /L and /S
+// together).  Tests use it to show that a network file written elsewhere is read
+// link for link.
 #include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <random>
+#include <string>
 #include <vector>
 
 #include "Constants.h"
@@ -38,6 +47,7 @@
 #include "Kernels.h"
 #include "Model.h"
 #include "Param.h"
+#include "SetupModel.h"
 
 extern double PropPlaces[NUM_AGE_GROUPS * AGE_GROUP_WIDTH][MAX_NUM_PLACE_TYPES];
 
@@ -86,6 +96,10 @@ int capacity_draw(int tp, std::mt19937_64& rng)
 
 void AssignPeopleToPlaces()
 {
+    if (const char* load = std::getenv("CS_NETGEN_LOAD")) {
+        LoadPeopleToPlaces(std::string(load));
+        return;
+    }
     std::mt19937_64 rng(((uint64_t)(uint32_t)P.setupSeed1 << 32) ^ (uint32_t)P.setupSeed2 ^ 0x6E657467656E2121ull);
     std::uniform_real_distribution<double> U(0.0, 1.0);
     for (int i = 0; i < P.PopSize; i++)

@@ -74,3 +74,44 @@ def test_cache_generates_once(tmp_path):
     assert len(calls) == 1
     _same(a, b)
     assert population.cached(None, "x", make) is not None and len(calls) == 2
+
+
+def test_network_file_read_by_the_reference(tmp_path):
+    """A network file written here is read link for link by the reference's own
+    LoadPeopleToPlaces (src/SetupModel.cpp:2603-2659).  The reference's command line
+    refuses /L with /S, so the network tool's loader mode runs the reference's
+    set-up with LoadPeopleToPlaces on our file in place of the place assignment and
+    /S writes back what it loaded (SavePeopleToPlaces); the two files are the same
+    bytes.  The file written here carries a network the reference did not make
+    (links exchanged among the attendees of each place type), so the match cannot
+    come from the reference re-deriving its own.  The stock reference then runs a
+    realisation on our file with /L."""
+    import os
+    import refrun
+    if not (os.path.exists(refrun.NETGEN) and os.path.exists(refrun.STOCK)):
+        pytest.skip("reference executables not built (needs the reference checkout at build time)")
+    grid = population.make_grid(width_deg=0.2, height_deg=0.2, cell_deg=1.0 / 120, nmcl=10)
+    pop = population.generate(5000, grid, sigma=1.2, seed=98798150)
+    seeds = (98798150, 729101)
+    theirs = str(tmp_path / "reference.net")
+    refrun.run_reference(pop, 1, nr=1, threads=2, binary=refrun.NETGEN, extra_args=("/S:" + theirs,), timeout=600)
+    raw = np.fromfile(theirs, dtype="<i4")
+    npt, n = int(raw[1]), int(raw[2])
+    assert (raw[0], n, raw[3], raw[4]) == (population.NETWORK_FILE_VERSION, pop.n_people) + seeds
+    n_places = [int(raw[5 + t::npt].max()) + 1 for t in range(npt)]
+    links = population.load_network_file(theirs, n, n_places, *seeds)
+    assert np.array_equal(np.ascontiguousarray(links.T).ravel(), raw[5:])
+    # exchange links among each type's attendees (every link stays a valid place)
+    rng = np.random.default_rng(5)
+    mine = links.copy()
+    for t in range(npt):
+        att = np.nonzero(mine[t] >= 0)[0]
+        mine[t, att] = mine[t, rng.permutation(att)]
+    assert not np.array_equal(mine, links)
+    ours = str(tmp_path / "ours.net")
+    population.save_network_links(mine, n_places, ours, *seeds)
+    back = str(tmp_path / "back.net")
+    refrun.run_reference(pop, 1, nr=1, threads=2, binary=refrun.NETGEN, extra_args=("/S:" + back,), timeout=600,
+                         env={"CS_NETGEN_LOAD": ours})
+    assert open(back, "rb").read() == open(ours, "rb").read()
+    refrun.run_reference(pop, 1, nr=1, threads=2, binary=refrun.STOCK, extra_args=("/L:" + ours,), timeout=600)
