@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcovidsim_b200.so")
 
-SOURCES = ["cs_sweep.cu", "cs_surrogate.cu", "cs_host.cpp"]
+SOURCES = ["cs_sweep.cu", "cs_surrogate.cu", "cs_setup.cu", "cs_host.cpp"]
 HEADERS = ["cs_device.cuh", "cs_state.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -101,6 +101,8 @@ cs_interventions = STRUCTS["cs_interventions"]
 cs_counters = STRUCTS["cs_counters"]
 cs_run_policy = STRUCTS["cs_run_policy"]
 cs_place_event = STRUCTS["cs_place_event"]
+cs_setup_spec = STRUCTS["cs_setup_spec"]
+cs_setup_out = STRUCTS["cs_setup_out"]
 
 COUNTER_FIELDS = [f for f, _ in cs_counters._fields_]
 
@@ -184,6 +186,13 @@ def load_library(path=LIB_PATH):
         "cs_gpu_launch_count": (C.c_int64, [V]),
         "cs_gpu_profile": (I, [V, I]),
         "cs_gpu_profile_entry": (I, [V, I, C.c_char_p, I, P(D), P(C.c_int64)]),
+        "cs_sizeof_setup_spec": (C.c_size_t, []),
+        "cs_sizeof_setup_out": (C.c_size_t, []),
+        "cs_gpu_setup_run": (I, [P(cs_setup_spec), P(cs_params), I, P(V)]),
+        "cs_gpu_setup_sizes": (I, [V, P(cs_setup_out)]),
+        "cs_gpu_setup_download": (I, [V, P(cs_setup_out)]),
+        "cs_gpu_setup_last_error": (C.c_char_p, [V]),
+        "cs_gpu_setup_destroy": (None, [V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -192,7 +201,8 @@ def load_library(path=LIB_PATH):
         raise CovidSimError("library ABI version %d, header %d" % (lib.cs_abi_version(), CONST["CS_ABI_VERSION"]))
     for fn, st in (("cs_sizeof_params", cs_params), ("cs_sizeof_population", cs_population),
                    ("cs_sizeof_counters", cs_counters), ("cs_sizeof_interventions", cs_interventions),
-                   ("cs_sizeof_run_policy", cs_run_policy)):
+                   ("cs_sizeof_run_policy", cs_run_policy), ("cs_sizeof_setup_spec", cs_setup_spec),
+                   ("cs_sizeof_setup_out", cs_setup_out)):
         if getattr(lib, fn)() != C.sizeof(st):
             raise CovidSimError("%s: library %d bytes, Python mirror %d" % (fn, getattr(lib, fn)(), C.sizeof(st)))
     _lib = lib

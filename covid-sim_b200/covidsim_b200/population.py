@@ -66,6 +66,7 @@ class Population:
     cell_members: np.ndarray
     places: list = field(default_factory=list)  # per type: dict of arrays
     n_adunits: int = 1
+    setup_info: dict = None       # set-up on the device: timings and counts
 
     @property
     def n_households(self):
@@ -337,6 +338,126 @@ def preset(name, n_people=None, seed=98798150, adunit_grid=None):
         grid = make_grid(width_deg=0.2, height_deg=0.2, cell_deg=1.0 / 60, nmcl=4)
         return generate(n_people or 20_000, grid, sigma=1.0, seed=seed, adunit_grid=adunit_grid)
     raise ValueError("unknown preset %r" % name)
+
+
+# ------------------------------------------------------ set-up on the GPU
+# Places a person chooses among, per type: the reference's "closest places" counts
+# for the schools and universities; workplaces (0 there: every place, by kernel)
+# choose among the 24 nearest.
+PLACE_NEAREST = [3, 3, 6, 24]
+CAPACITY_SLACK = 1.125      # the reference's total capacity of 1.125 x demand (src/SetupModel.cpp:2186-2190)
+SETUP_ROUNDS = 6
+
+
+def setup_spec(n_people, grid, sigma=1.2, seed=98798150, blobs=0, blob_share=0.0, adunit_grid=None,
+               num_place_types=4, hh_dist=HH_SIZE_DIST, rounds=SETUP_ROUNDS):
+    """The cs_setup_spec of a synthetic population, and the cs_params whose geometry
+    and kernel tables it uses: (spec, params, keep) -- `keep` holds the tables the
+    spec points at."""
+    from . import params as prm
+    P, lk, hr = prm.build_params(grid, num_place_types=num_place_types)
+    S = abi.cs_setup_spec()
+    S.n_people, S.ncw, S.nch, S.nmcl = n_people, grid["ncw"], grid["nch"], grid["nmcl"]
+    S.cell_width, S.cell_height = grid["cell_width"], grid["cell_height"]
+    S.sigma = sigma
+    S.n_blobs = blobs
+    S.blob_share = blob_share if blobs else 0.0
+    S.adunit_grid = adunit_grid or 0
+    S.seed = seed
+    cdf = np.cumsum(np.asarray(hh_dist, dtype=float))
+    cdf /= cdf[-1]
+    for k in range(abi.CS_MAX_HOUSEHOLD_SIZE):
+        S.hh_cdf[k] = cdf[k] if k < len(cdf) else 1.0
+    ad = np.cumsum(np.asarray(AGE_DIST, dtype=float))
+    ad /= ad[-1]
+    for k in range(abi.CS_NUM_AGE_GROUPS):
+        S.age_cdf[k] = ad[k]
+    S.num_place_types = num_place_types
+    S.rounds = rounds
+    for t in range(num_place_types):
+        T = S.pt[t]
+        for b, (lo, hi, prop) in enumerate(PLACE_AGE_BANDS[t]):
+            T.band_lo[b], T.band_hi[b], T.band_prop[b] = lo, hi, prop
+        T.mean_size = PLACE_MEAN_SIZE[t]
+        if t == 3:
+            T.size_kind = abi.CS_SETUP_SIZE_POWER
+            T.size_offset, T.size_power, T.size_max = WORKPLACE_OFFSET, WORKPLACE_POWER, WORKPLACE_MAX
+        else:
+            T.size_kind = abi.CS_SETUP_SIZE_GAMMA
+        T.capacity_slack = CAPACITY_SLACK
+        T.nearest = PLACE_NEAREST[t]
+        T.group_size = GROUP_SIZE_PARAM1[t]
+        T.kernel_lookup = lk.ctypes.data
+        T.kernel_hi_res = hr.ctypes.data
+    return S, P, (lk, hr)
+
+
+def from_setup(sizes, download, grid):
+    """A Population from a set-up's sizes (cs_setup_out) and `download(out)`, which
+    copies the arrays into the buffers `out` points at."""
+    N, NH, NC, NM = sizes.n_people, sizes.n_households, sizes.n_cells, sizes.n_mcells
+    npt = sizes.num_place_types
+    a = dict(person_hh=np.zeros(N, np.int32), person_mcell=np.zeros(N, np.int32), person_age=np.zeros(N, np.uint8),
+             person_place=np.zeros((npt, N), np.int32), person_group=np.zeros((npt, N), np.uint16),
+             hh_first=np.zeros(NH, np.int32), hh_nh=np.zeros(NH, np.uint16), hh_x=np.zeros(NH, np.float32),
+             hh_y=np.zeros(NH, np.float32), mcell_cell=np.zeros(NM, np.int32), mcell_adunit=np.zeros(NM, np.int32),
+             mcell_grid=np.zeros(NM, np.int64), cell_grid=np.zeros(NC, np.int32),
+             cell_start=np.zeros(NC + 1, np.int32))
+    out = abi.cs_setup_out()
+    for k, v in a.items():
+        setattr(out, k, v.ctypes.data)
+    places = []
+    for t in range(npt):
+        np_, na, ng = sizes.n_places[t], sizes.n_attendees[t], sizes.n_groups[t]
+        pl = dict(mcell=np.zeros(np_, np.int32), x=np.zeros(np_, np.float32), y=np.zeros(np_, np.float32),
+                  member_ofs=np.zeros(np_ + 1, np.int32), members=np.zeros(na, np.int32),
+                  group_ofs=np.zeros(np_ + 1, np.int32), group_start=np.zeros(ng, np.int32),
+                  group_size=np.zeros(ng, np.int32))
+        out.place_mcell[t], out.place_x[t], out.place_y[t] = pl["mcell"].ctypes.data, pl["x"].ctypes.data, pl["y"].ctypes.data
+        out.place_member_ofs[t], out.place_members[t] = pl["member_ofs"].ctypes.data, pl["members"].ctypes.data
+        out.place_group_ofs[t] = pl["group_ofs"].ctypes.data
+        out.group_start[t], out.group_size[t] = pl["group_start"].ctypes.data, pl["group_size"].ctypes.data
+        places.append(pl)
+    download(out)
+    info = dict(device_ms=float(sizes.device_ms), forced=[int(sizes.forced[t]) for t in range(npt)],
+                attendees=[int(sizes.n_attendees[t]) for t in range(npt)])
+    return Population(
+        n_people=N, grid=grid, person_hh=a["person_hh"], person_mcell=a["person_mcell"], person_age=a["person_age"],
+        person_flags=np.zeros(N, dtype=np.uint8), person_place=a["person_place"], person_group=a["person_group"],
+        hh_first=a["hh_first"], hh_nh=a["hh_nh"], hh_nhr=a["hh_nh"].copy(), hh_x=a["hh_x"], hh_y=a["hh_y"],
+        mcell_cell=a["mcell_cell"], mcell_adunit=a["mcell_adunit"], mcell_grid=a["mcell_grid"],
+        cell_grid=a["cell_grid"], cell_start=a["cell_start"], cell_members=np.arange(N, dtype=np.int32),
+        places=places, n_adunits=sizes.n_adunits, setup_info=info)
+
+
+def generate_on_device(n_people, grid, sigma=1.2, seed=98798150, blobs=0, blob_share=0.0, adunit_grid=None,
+                       num_place_types=4, hh_dist=HH_SIZE_DIST, rounds=SETUP_ROUNDS, device=0):
+    """A synthetic population built by the set-up kernels on CUDA device `device`
+    (cs_gpu_setup_run) and copied to host arrays.  The same spec always gives the
+    same population; its distributions follow generate(), its numbering the
+    reference's (people cell by cell)."""
+    import time
+    lib = abi.load_library()
+    S, P, keep = setup_spec(n_people, grid, sigma, seed, blobs, blob_share, adunit_grid, num_place_types, hh_dist,
+                            rounds)
+    h = C.c_void_p()
+    t0 = time.perf_counter()
+    rc = lib.cs_gpu_setup_run(C.byref(S), C.byref(P), device, C.byref(h))
+    try:
+        if rc != 0:
+            raise abi.CovidSimError("cs_gpu_setup_run: %s" % lib.cs_gpu_setup_last_error(h).decode())
+        sizes = abi.cs_setup_out()
+        lib.cs_gpu_setup_sizes(h, C.byref(sizes))
+
+        def download(out):
+            if lib.cs_gpu_setup_download(h, C.byref(out)) != 0:
+                raise abi.CovidSimError("cs_gpu_setup_download: %s" % lib.cs_gpu_setup_last_error(h).decode())
+        pop = from_setup(sizes, download, grid)
+    finally:
+        lib.cs_gpu_setup_destroy(h)
+    pop.setup_info["wall_s"] = time.perf_counter() - t0
+    del keep
+    return pop
 
 
 # ------------------------------------------------------------ files

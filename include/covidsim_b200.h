@@ -34,9 +34,10 @@
 extern "C" {
 #endif
 
-#define CS_ABI_VERSION 3            /* 2: per admin unit windows in cs_interventions, cs_run_policy;
+#define CS_ABI_VERSION 4            /* 2: per admin unit windows in cs_interventions, cs_run_policy;
                                        3: PlaceClosePropAttending, cs_gpu_place_events,
-                                          cs_gpu_set_mcell_status */
+                                          cs_gpu_set_mcell_status;
+                                       4: population set-up (cs_gpu_setup_*) */
 
 /* Sizes fixed by the reference (src/Constants.h, src/Country.h). */
 #define CS_MAX_PLACE_TYPES 5        /* MAX_NUM_PLACE_TYPES   (Country.h:15)   */
@@ -113,6 +114,19 @@ extern "C" {
 #define CS_RNG_HQ 10              /* entity household                     */
 #define CS_RNG_RUN_INIT 11        /* entity person, timestep 0            */
 #define CS_RNG_PLACE_INIT 12      /* entity place, sub place type         */
+/* Population set-up (cs_gpu_setup_run); timestep field = round where noted. */
+#define CS_RNG_SETUP_DENSITY 20   /* entity microcell grid index          */
+#define CS_RNG_SETUP_BLOB 21      /* entity blob                          */
+#define CS_RNG_SETUP_PERSON 22    /* entity draw k (64-bit integer)       */
+#define CS_RNG_SETUP_HH 23        /* entity microcell grid index          */
+#define CS_RNG_SETUP_HH_LOC 24    /* entity microcell grid index, sub household ordinal */
+#define CS_RNG_SETUP_AGE 25       /* entity person                        */
+#define CS_RNG_SETUP_ATTEND 26    /* entity person, sub 4 * place type + band */
+#define CS_RNG_SETUP_PLACE_SIZE 27 /* entity place draw, sub place type   */
+#define CS_RNG_SETUP_PLACE_LOC 28 /* entity place, sub place type (block 0: 64-bit person draw) */
+#define CS_RNG_SETUP_CHOOSE 29    /* entity person, sub place type, timestep round */
+#define CS_RNG_SETUP_ACCEPT 30    /* entity person, sub place type, timestep round */
+#define CS_RNG_SETUP_SHUFFLE 31   /* entity person, sub place type (32-bit key) */
 
 /* Static per-person flag bits (cs_population.person_flags). */
 #define CS_PF_CARE_HOME_RESIDENT 0x01u
@@ -597,6 +611,123 @@ int64_t cs_gpu_launch_count(const cs_gpu_ctx* ctx);
  */
 int cs_gpu_profile(cs_gpu_ctx* ctx, int enable);
 int cs_gpu_profile_entry(cs_gpu_ctx* ctx, int i, char* name, int cap, double* total_ms, int64_t* launches);
+
+/*
+ * Population set-up on the GPU: the steps of the reference's SetupModel that build
+ * the hot path's inputs (src/SetupModel.cpp:1137-1290 microcell populations,
+ * households and their locations; :1989-2466 AssignPeopleToPlaces), restated as
+ * parallel kernels on the counter-based streams (CS_RNG_SETUP_*), so the result
+ * depends on the spec and its seed only.
+ *
+ *  - microcell weights lognormal(0, sigma) per microcell (optionally blended with
+ *    Gaussian urban blobs holding blob_share of the weight), quantised to integers;
+ *    every person then draws its microcell by inverse CDF over the integer prefix
+ *    sums: the counts are multinomial, the law of the reference's sequential
+ *    binomial allocation (:1137-1156);
+ *  - people numbered as the reference numbers Hosts[]: populated cells in grid
+ *    order, within a cell its microcells x-major (:1163-1185), within a microcell
+ *    household by household;
+ *  - households per microcell with the reference's rule (:1224-1253): a size drawn
+ *    from the cumulative distribution hh_cdf, cut at the microcell's remaining
+ *    people and at CS_MAX_HOUSEHOLD_SIZE; located uniformly in the microcell
+ *    (:1272-1290);
+ *  - ages: a 5-year band from age_cdf, a year uniform in it, at most 84;
+ *  - per place type: attendance by age band (at most one place per person, types
+ *    in order), place sizes drawn until they cover the attendees (gamma(4) about
+ *    mean_size, or the offset power law of :2100-2108), places located in
+ *    microcells drawn in proportion to their people, capacity = ceil(size *
+ *    capacity_slack);
+ *  - assignment: in each of `rounds` rounds every attendee without a place looks at
+ *    the `nearest` nearest places with room (rings of buckets until that many are
+ *    in hand, then one ring more, as the reference's microcell spiral gathers them)
+ *    and proposes to one with probability proportional to K(d) * room, the weight of
+ *    the reference's searches (:2265-2290); a place with more proposals than room
+ *    accepts each with probability room / proposals.  A last round ignores
+ *    capacity.  K is the type's kernel table (cs_build_kernel_table layout, with
+ *    the size, expansion and delta of the cs_params passed in);
+ *  - member lists in a random order, groups of about group_size members.
+ */
+#define CS_SETUP_SIZE_GAMMA 0
+#define CS_SETUP_SIZE_POWER 1
+#define CS_SETUP_MAX_BLOBS 64
+#define CS_SETUP_MAX_NEAREST 32
+typedef struct cs_setup_place_type {
+    double band_lo[3], band_hi[3], band_prop[3];   /* attendance: age in [lo, hi) years, probability */
+    double mean_size;                  /* PlaceTypeMeanSize                   */
+    double size_offset, size_power, size_max;      /* CS_SETUP_SIZE_POWER: P(S > s) = ((off+1)/(off+s))^power */
+    double capacity_slack;             /* capacity = ceil(size * slack)       */
+    int32_t size_kind;                 /* CS_SETUP_SIZE_GAMMA or CS_SETUP_SIZE_POWER */
+    int32_t nearest;                   /* places the choice is among (1..CS_SETUP_MAX_NEAREST) */
+    int32_t group_size;                /* PlaceTypeGroupSizeParam1            */
+    int32_t _pad;
+    const double* kernel_lookup;       /* K over distance^2 (cs_build_kernel_table)  */
+    const double* kernel_hi_res;
+} cs_setup_place_type;
+
+typedef struct cs_setup_spec {
+    int32_t n_people;
+    int32_t ncw, nch, nmcl;            /* grid cells, microcells per cell side   */
+    double cell_width, cell_height;    /* degrees                                */
+    double sigma;                      /* lognormal sigma of microcell weights   */
+    double blob_share;                 /* weight share of the blobs (0: none)    */
+    int32_t n_blobs;                   /* <= CS_SETUP_MAX_BLOBS                  */
+    int32_t adunit_grid;               /* admin units on an a x a grid (0: one)  */
+    uint64_t seed;
+    double hh_cdf[CS_MAX_HOUSEHOLD_SIZE];   /* cumulative household size distribution */
+    double age_cdf[CS_NUM_AGE_GROUPS];      /* cumulative age band distribution       */
+    int32_t num_place_types;
+    int32_t rounds;                    /* capacity-respecting assignment rounds  */
+    cs_setup_place_type pt[CS_MAX_PLACE_TYPES];
+} cs_setup_spec;
+
+/* What a set-up produced.  cs_gpu_setup_sizes fills the counts; for
+ * cs_gpu_setup_download the caller points the arrays at buffers of those sizes
+ * (any may be NULL to skip it).  person_place and person_group are
+ * [num_place_types][n_people].  People are numbered cell by cell, so a cell's
+ * members are [cell_start[c], cell_start[c+1]) in order. */
+typedef struct cs_setup_out {
+    int32_t n_people, n_households, n_cells, n_mcells, n_adunits, num_place_types;
+    int32_t n_places[CS_MAX_PLACE_TYPES];
+    int32_t n_groups[CS_MAX_PLACE_TYPES];
+    int32_t n_attendees[CS_MAX_PLACE_TYPES];
+    int32_t forced[CS_MAX_PLACE_TYPES];   /* attendees placed by the capacity-free last round */
+    double device_ms;                  /* device time of the set-up's kernels    */
+    int32_t* person_hh;
+    int32_t* person_mcell;
+    uint8_t* person_age;
+    int32_t* person_place;
+    uint16_t* person_group;
+    int32_t* hh_first;
+    uint16_t* hh_nh;
+    float* hh_x;
+    float* hh_y;
+    int32_t* mcell_cell;
+    int32_t* mcell_adunit;
+    int64_t* mcell_grid;               /* microcell grid index mx * nch * nmcl + my */
+    int32_t* cell_grid;
+    int32_t* cell_start;               /* n_cells + 1 */
+    int32_t* place_mcell[CS_MAX_PLACE_TYPES];
+    float* place_x[CS_MAX_PLACE_TYPES];
+    float* place_y[CS_MAX_PLACE_TYPES];
+    int32_t* place_member_ofs[CS_MAX_PLACE_TYPES];   /* n_places + 1 */
+    int32_t* place_members[CS_MAX_PLACE_TYPES];
+    int32_t* place_group_ofs[CS_MAX_PLACE_TYPES];    /* n_places + 1 */
+    int32_t* group_start[CS_MAX_PLACE_TYPES];
+    int32_t* group_size[CS_MAX_PLACE_TYPES];
+} cs_setup_out;
+
+typedef struct cs_setup cs_setup;
+/* Run the set-up on CUDA device `device`; the result stays in device memory until
+ * cs_gpu_setup_destroy.  `params` supplies the geometry (DoUTM_coords, the distance
+ * tables, bbox) and the kernel table's size, expansion and delta.  On failure *out
+ * may still hold a handle whose last error says why (destroy it). */
+size_t cs_sizeof_setup_spec(void);
+size_t cs_sizeof_setup_out(void);
+int cs_gpu_setup_run(const cs_setup_spec* spec, const cs_params* params, int device, cs_setup** out);
+int cs_gpu_setup_sizes(cs_setup* setup, cs_setup_out* sizes);
+int cs_gpu_setup_download(cs_setup* setup, const cs_setup_out* dst);
+const char* cs_gpu_setup_last_error(const cs_setup* setup);
+void cs_gpu_setup_destroy(cs_setup* setup);
 
 #ifdef __cplusplus
 }

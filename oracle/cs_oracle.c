@@ -1862,3 +1862,619 @@ int cs_cpu_sample_many(int kind, uint64_t seed, double a, double b, int n, doubl
     }
     return err ? CS_E_OVERFLOW : CS_OK;
 }
+
+/* ================================================================== set-up ==
+ * Population set-up (the GPU's cs_gpu_setup_*), restated sequentially: the steps
+ * of the reference's SetupModel that build the sweep's inputs -- microcell
+ * populations (src/SetupModel.cpp:1137-1156), people numbered cell by cell
+ * (:1163-1185), households and their locations (:1224-1290), people assigned to
+ * places (:1989-2466) -- on the same counter-based streams as the device, with
+ * the same arithmetic, so the two agree array for array. */
+typedef struct cs_cpu_setup {
+    char err[256];
+    cs_setup_out o;              /* sizes and arrays (owned) */
+} cs_cpu_setup;
+
+static int setup_fail(cs_cpu_setup* s, int code, const char* msg)
+{
+    snprintf(s->err, sizeof s->err, "%s", msg);
+    return code;
+}
+
+static uint64_t setup_rand64(uint64_t seed, int purpose, uint32_t ts, uint32_t entity, uint32_t sub)
+{
+    uint32_t ctr[4] = {0u, entity, (ts & 0xffffu) | ((uint32_t)purpose << 16), sub}, x[4];
+    cs_cpu_philox((uint32_t)seed, (uint32_t)(seed >> 32), ctr, x);
+    return ((uint64_t)x[1] << 32) | x[0];
+}
+
+static uint64_t mulhi64(uint64_t a, uint64_t b)
+{
+    return (uint64_t)(((unsigned __int128)a * (unsigned __int128)b) >> 64);
+}
+
+static double setup_knum(const double* lk, const double* hr, const cs_params* P, double r2)
+{
+    double t = r2 / P->kernel_delta;
+    if (t > P->kernel_size) return 0.0;
+    double s = t * P->kernel_expansion;
+    if (s < P->kernel_size) {
+        t = s - floor(s);
+        return (1.0 - t) * hr[(int)s] + t * hr[(int)(s + 1.0)];
+    }
+    int i0 = (int)t, i1 = (int)(t + 1.0);
+    if (i1 > P->kernel_size) i1 = P->kernel_size;
+    s = t - floor(t);
+    return (1.0 - s) * lk[i0] + s * lk[i1];
+}
+
+static double setup_dist2(const cs_params* P, float ax, float ay, float bx, float by)
+{
+    if (P->DoUTM_coords) return dist2_utm(P, ax, ay, bx, by);
+    float dx = ax - bx, dy = ay - by;
+    return periodic_xy(P, fabs(dx), fabs(dy));
+}
+
+static int setup_hh_size(stream* s, const double* cdf, int k, int n)
+{
+    double u = stream_next(s);
+    int m = 1;
+    while ((u > cdf[m - 1]) && (k + m < n) && (m < CS_MAX_HOUSEHOLD_SIZE)) m++;
+    return m;
+}
+
+static int64_t setup_place_size(uint64_t seed, int t, int i, const cs_setup_place_type* T, int64_t* err)
+{
+    stream s;
+    stream_init(&s, seed, CS_RNG_SETUP_PLACE_SIZE, 0, (uint32_t)i, (uint32_t)t);
+    double v;
+    if (T->size_kind == CS_SETUP_SIZE_POWER) {
+        double u = 1.0 - stream_next(&s);
+        v = floor((T->size_offset + 1.0) * pow(u, -1.0 / T->size_power) - T->size_offset);
+        v = fmin(fmax(v, 1.0), T->size_max);
+    } else {
+        v = floor(sample_gamma(&s, 4.0 / T->mean_size, 4.0, err) + 0.5);
+        v = fmax(v, 1.0);
+    }
+    return (int64_t)v;
+}
+
+typedef struct { double d2; int32_t pl; } setup_cand;
+
+static int setup_cand_less(double d2, int pl, const setup_cand* c)
+{
+    return d2 < c->d2 || (d2 == c->d2 && pl < c->pl);
+}
+
+typedef struct { uint64_t key; int32_t a; } setup_key;
+
+static int setup_key_cmp(const void* x, const void* y)
+{
+    const setup_key* a = (const setup_key*)x;
+    const setup_key* b = (const setup_key*)y;
+    if (a->key != b->key) return a->key < b->key ? -1 : 1;
+    return (a->a > b->a) - (a->a < b->a);
+}
+
+#define SETUP_ALLOC(p, n, T)                                                   \
+    do {                                                                       \
+        (p) = (T*)calloc((size_t)((n) > 0 ? (n) : 1), sizeof(T));              \
+        if (!(p)) { rc = setup_fail(s, CS_E_ARG, "setup: out of memory"); goto done; } \
+    } while (0)
+
+static int setup_run(cs_cpu_setup* s, const cs_setup_spec* S, const cs_params* P)
+{
+    int rc = CS_OK;
+    int64_t err = 0;
+    const uint64_t seed = S->seed;
+    const int nmcl = S->nmcl, nch = S->nch, ncw = S->ncw;
+    const int th = nch * nmcl, tw = ncw * nmcl;
+    const int64_t M = (int64_t)tw * th;
+    const int G = ncw * nch, N = S->n_people;
+    const double mcw = S->cell_width / nmcl, mch = S->cell_height / nmcl;
+    cs_setup_out* o = &s->o;
+    uint64_t *q = NULL, *qb = NULL, *pref = NULL;
+    int32_t *cnt = NULL, *mcell_start = NULL, *mcell_n = NULL;
+    uint8_t* taken_p = NULL;
+    int32_t* list = NULL;
+    double bl[CS_SETUP_MAX_BLOBS][4];
+    if (N <= 0 || ncw <= 0 || nch <= 0 || nmcl <= 0) return setup_fail(s, CS_E_ARG, "setup: bad sizes");
+    if (S->n_blobs < 0 || S->n_blobs > CS_SETUP_MAX_BLOBS) return setup_fail(s, CS_E_ARG, "setup: bad n_blobs");
+    if (S->num_place_types < 0 || S->num_place_types > CS_MAX_PLACE_TYPES)
+        return setup_fail(s, CS_E_ARG, "setup: bad num_place_types");
+    for (int t = 0; t < S->num_place_types; t++)
+        if (S->pt[t].nearest < 1 || S->pt[t].nearest > CS_SETUP_MAX_NEAREST)
+            return setup_fail(s, CS_E_ARG, "setup: bad nearest");
+    o->n_people = N;
+    o->num_place_types = S->num_place_types;
+    o->n_adunits = S->adunit_grid > 0 ? S->adunit_grid * S->adunit_grid : 1;
+
+    /* 1. microcell weights (lognormal, optionally blended with blobs), integer prefix */
+    for (int k = 0; k < S->n_blobs; k++) {
+        stream b;
+        stream_init(&b, seed, CS_RNG_SETUP_BLOB, 0, (uint32_t)k, 0);
+        bl[k][0] = 0.05 + 0.9 * stream_next(&b);
+        bl[k][1] = 0.05 + 0.9 * stream_next(&b);
+        bl[k][2] = 0.004 + 0.016 * stream_next(&b);
+        bl[k][3] = exp(0.7 * sample_normal(&b, &err));
+    }
+    SETUP_ALLOC(q, M, uint64_t);
+    SETUP_ALLOC(pref, M, uint64_t);
+    if (S->n_blobs > 0) SETUP_ALLOC(qb, M, uint64_t);
+    for (int64_t j = 0; j < M; j++) {
+        stream d;
+        stream_init(&d, seed, CS_RNG_SETUP_DENSITY, 0, (uint32_t)j, 0);
+        double w = exp(S->sigma * sample_normal(&d, &err));
+        q[j] = (uint64_t)floor(w * 1048576.0);
+        if (S->n_blobs > 0) {
+            const double xs = ((double)(j / th) + 0.5) / (double)tw;
+            const double ys = ((double)(j % th) + 0.5) / (double)th;
+            double b = 0.0;
+            for (int k = 0; k < S->n_blobs; k++) {
+                const double ax = (xs - bl[k][0]) / bl[k][2], ay = (ys - bl[k][1]) / bl[k][2];
+                b = b + bl[k][3] * exp(-0.5 * ax * ax) * exp(-0.5 * ay * ay);
+            }
+            qb[j] = (uint64_t)floor(b * 1048576.0);
+        }
+    }
+    if (S->n_blobs > 0) {
+        uint64_t QW = 0, QB = 0;
+        for (int64_t j = 0; j < M; j++) { QW += q[j]; QB += qb[j]; }
+        for (int64_t j = 0; j < M; j++) {
+            const double a = (double)q[j] / (double)QW, b = (double)qb[j] / (double)QB;
+            q[j] = (uint64_t)floor(((1.0 - S->blob_share) * a + S->blob_share * b) * 4503599627370496.0);
+        }
+    }
+    {
+        uint64_t run = 0;
+        for (int64_t j = 0; j < M; j++) pref[j] = run += q[j];
+    }
+    if (pref[M - 1] == 0) { rc = setup_fail(s, CS_E_ARG, "setup: every microcell weight is zero"); goto done; }
+
+    /* 2. people to microcells */
+    SETUP_ALLOC(cnt, M, int32_t);
+    for (int k = 0; k < N; k++) {
+        const uint64_t r = mulhi64(setup_rand64(seed, CS_RNG_SETUP_PERSON, 0, (uint32_t)k, 0), pref[M - 1]);
+        int64_t lo = 0, hi = M - 1;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if (pref[mid] > r) hi = mid; else lo = mid + 1;
+        }
+        cnt[lo]++;
+    }
+
+    /* 3. populated cells and microcells, the reference's order */
+    {
+        int NC = 0, NM = 0;
+        for (int c = 0; c < G; c++) {
+            int n = 0;
+            for (int l = 0; l < nmcl; l++)
+                for (int m = 0; m < nmcl; m++) {
+                    int v = cnt[(int64_t)((c / nch) * nmcl + l) * th + (int64_t)(c % nch) * nmcl + m];
+                    n += v;
+                    NM += v > 0;
+                }
+            NC += n > 0;
+        }
+        o->n_cells = NC;
+        o->n_mcells = NM;
+        SETUP_ALLOC(o->cell_grid, NC, int32_t);
+        SETUP_ALLOC(o->cell_start, NC + 1, int32_t);
+        SETUP_ALLOC(o->mcell_cell, NM, int32_t);
+        SETUP_ALLOC(o->mcell_grid, NM, int64_t);
+        SETUP_ALLOC(o->mcell_adunit, NM, int32_t);
+        SETUP_ALLOC(mcell_start, NM, int32_t);
+        SETUP_ALLOC(mcell_n, NM, int32_t);
+        int pid = 0, mid = 0, run = 0;
+        for (int c = 0; c < G; c++) {
+            const int first_mid = mid, first_run = run;
+            for (int l = 0; l < nmcl; l++)
+                for (int m = 0; m < nmcl; m++) {
+                    const int64_t j = (int64_t)((c / nch) * nmcl + l) * th + (int64_t)(c % nch) * nmcl + m;
+                    const int v = cnt[j];
+                    if (v == 0) continue;
+                    o->mcell_cell[mid] = pid;
+                    o->mcell_grid[mid] = j;
+                    mcell_start[mid] = run;
+                    mcell_n[mid] = v;
+                    int au = 0;
+                    if (S->adunit_grid > 0) {
+                        const int64_t mx = j / th, my = j % th;
+                        int64_t ax = (mx * S->adunit_grid) / tw, ay = (my * S->adunit_grid) / th;
+                        if (ax > S->adunit_grid - 1) ax = S->adunit_grid - 1;
+                        if (ay > S->adunit_grid - 1) ay = S->adunit_grid - 1;
+                        au = (int)(ax * S->adunit_grid + ay);
+                    }
+                    o->mcell_adunit[mid] = au;
+                    run += v;
+                    mid++;
+                }
+            if (run > first_run) {
+                o->cell_grid[pid] = c;
+                o->cell_start[pid] = first_run;
+                pid++;
+            }
+            (void)first_mid;
+        }
+        o->cell_start[NC] = N;
+    }
+
+    /* 4. households */
+    {
+        const int NM = o->n_mcells;
+        int NH = 0;
+        for (int i = 0; i < NM; i++) {
+            stream h;
+            stream_init(&h, seed, CS_RNG_SETUP_HH, 0, (uint32_t)o->mcell_grid[i], 0);
+            int k = 0;
+            while (k < mcell_n[i]) { k += setup_hh_size(&h, S->hh_cdf, k, mcell_n[i]); NH++; }
+        }
+        o->n_households = NH;
+        SETUP_ALLOC(o->hh_first, NH, int32_t);
+        SETUP_ALLOC(o->hh_nh, NH, uint16_t);
+        SETUP_ALLOC(o->hh_x, NH, float);
+        SETUP_ALLOC(o->hh_y, NH, float);
+        SETUP_ALLOC(o->person_hh, N, int32_t);
+        SETUP_ALLOC(o->person_mcell, N, int32_t);
+        int hh = 0;
+        for (int i = 0; i < NM; i++) {
+            const int64_t j = o->mcell_grid[i];
+            stream h;
+            stream_init(&h, seed, CS_RNG_SETUP_HH, 0, (uint32_t)j, 0);
+            const int n = mcell_n[i], first = mcell_start[i];
+            const double x = (double)(j / th), y = (double)(j % th);
+            int k = 0;
+            uint32_t ord = 0;
+            while (k < n) {
+                const int m = setup_hh_size(&h, S->hh_cdf, k, n);
+                stream sl;
+                stream_init(&sl, seed, CS_RNG_SETUP_HH_LOC, 0, (uint32_t)j, ord++);
+                const double ux = stream_next(&sl), uy = stream_next(&sl);
+                o->hh_first[hh] = first + k;
+                o->hh_nh[hh] = (uint16_t)m;
+                o->hh_x[hh] = (float)(mcw * (ux + x));
+                o->hh_y[hh] = (float)(mch * (uy + y));
+                for (int r = 0; r < m; r++) {
+                    o->person_hh[first + k + r] = hh;
+                    o->person_mcell[first + k + r] = i;
+                }
+                k += m;
+                hh++;
+            }
+        }
+    }
+
+    /* 5. ages */
+    SETUP_ALLOC(o->person_age, N, uint8_t);
+    for (int p = 0; p < N; p++) {
+        stream a;
+        stream_init(&a, seed, CS_RNG_SETUP_AGE, 0, (uint32_t)p, 0);
+        const double u = stream_next(&a);
+        int b = 0;
+        while (b < CS_NUM_AGE_GROUPS - 1 && !(u < S->age_cdf[b])) b++;
+        int age = b * CS_AGE_GROUP_WIDTH + (int)floor(stream_next(&a) * CS_AGE_GROUP_WIDTH);
+        o->person_age[p] = (uint8_t)(age < 84 ? age : 84);
+    }
+
+    /* 6. places */
+    {
+        const int npt = S->num_place_types;
+        SETUP_ALLOC(o->person_place, (int64_t)(npt > 0 ? npt : 1) * N, int32_t);
+        SETUP_ALLOC(o->person_group, (int64_t)(npt > 0 ? npt : 1) * N, uint16_t);
+        for (int64_t i = 0; i < (int64_t)npt * N; i++) o->person_place[i] = -1;
+        SETUP_ALLOC(taken_p, N, uint8_t);
+        SETUP_ALLOC(list, N, int32_t);
+        for (int t = 0; t < npt; t++) {
+            const cs_setup_place_type* T = &S->pt[t];
+            int n_att = 0;
+            for (int p = 0; p < N; p++) {
+                if (taken_p[p]) continue;
+                const double a = (double)o->person_age[p];
+                int f = 0;
+                for (int b = 0; b < 3 && !f; b++) {
+                    if (!(T->band_prop[b] > 0) || a < T->band_lo[b] || !(a < T->band_hi[b])) continue;
+                    stream sa;
+                    stream_init(&sa, seed, CS_RNG_SETUP_ATTEND, 0, (uint32_t)p, (uint32_t)(4 * t + b));
+                    if (stream_next(&sa) < T->band_prop[b]) f = 1;
+                }
+                if (f) { taken_p[p] = 1; list[n_att++] = p; }
+            }
+            o->n_attendees[t] = n_att;
+            if (n_att == 0) {
+                o->n_places[t] = 0;
+                SETUP_ALLOC(o->place_member_ofs[t], 1, int32_t);
+                SETUP_ALLOC(o->place_group_ofs[t], 1, int32_t);
+                continue;
+            }
+            /* sizes until they cover the attendees */
+            int n_est = (int)((double)n_att / T->mean_size * 1.2) + 8;
+            if (n_est < 1) n_est = 1;
+            int64_t* sz = (int64_t*)calloc((size_t)n_est, sizeof(int64_t));
+            int64_t* cum = (int64_t*)calloc((size_t)n_est, sizeof(int64_t));
+            if (!sz || !cum) { free(sz); free(cum); rc = setup_fail(s, CS_E_ARG, "setup: out of memory"); goto done; }
+            int64_t run = 0;
+            for (int i = 0; i < n_est; i++) { sz[i] = setup_place_size(seed, t, i, T, &err); cum[i] = run += sz[i]; }
+            int lo = 0, hi = n_est;
+            while (lo < hi) { int mid = (lo + hi) >> 1; if (cum[mid] >= n_att) hi = mid; else lo = mid + 1; }
+            const int npl = (lo < n_est) ? lo + 1 : n_est + 1;
+            o->n_places[t] = npl;
+            int32_t* rem = (int32_t*)calloc((size_t)npl, sizeof(int32_t));
+            SETUP_ALLOC(o->place_mcell[t], npl, int32_t);
+            SETUP_ALLOC(o->place_x[t], npl, float);
+            SETUP_ALLOC(o->place_y[t], npl, float);
+            for (int i = 0; i < npl; i++) {
+                int64_t size;
+                if (i < n_est) { size = sz[i]; if (cum[i] > n_att) size -= cum[i] - n_att; }
+                else size = n_att - cum[n_est - 1];
+                rem[i] = (int32_t)ceil((double)size * T->capacity_slack);
+                const uint64_t r = mulhi64(setup_rand64(seed, CS_RNG_SETUP_PLACE_LOC, 0, (uint32_t)i, (uint32_t)t),
+                                           (uint64_t)N);
+                const int mid = o->person_mcell[r];
+                const int64_t j = o->mcell_grid[mid];
+                stream sp;
+                stream_init(&sp, seed, CS_RNG_SETUP_PLACE_LOC, 0, (uint32_t)i, (uint32_t)t);
+                sp.block = 1;
+                const double ux = stream_next(&sp), uy = stream_next(&sp);
+                o->place_mcell[t][i] = mid;
+                o->place_x[t][i] = (float)(mcw * ((double)(j / th) + ux));
+                o->place_y[t][i] = (float)(mch * ((double)(j % th) + uy));
+            }
+            free(sz);
+            free(cum);
+            /* buckets of about four places (order within a bucket is immaterial) */
+            int bs = (int)floor(sqrt(4.0 * (double)G / (double)npl));
+            if (bs < 1) bs = 1;
+            const int nbx = (ncw + bs - 1) / bs, nby = (nch + bs - 1) / bs, NBK = nbx * nby;
+            int32_t* bstart = (int32_t*)calloc((size_t)NBK + 1, sizeof(int32_t));
+            int32_t* items = (int32_t*)calloc((size_t)npl, sizeof(int32_t));
+            int32_t* pb = (int32_t*)calloc((size_t)npl, sizeof(int32_t));
+            int32_t* link = (int32_t*)malloc(sizeof(int32_t) * (size_t)n_att);
+            int32_t* prop = (int32_t*)malloc(sizeof(int32_t) * (size_t)n_att);
+            int32_t* nprop = (int32_t*)calloc((size_t)npl, sizeof(int32_t));
+            int32_t* taken = (int32_t*)calloc((size_t)npl, sizeof(int32_t));
+            for (int i = 0; i < npl; i++) {
+                int cx = (int)(o->place_x[t][i] / S->cell_width), cy = (int)(o->place_y[t][i] / S->cell_height);
+                cx = cx < 0 ? 0 : (cx > ncw - 1 ? ncw - 1 : cx);
+                cy = cy < 0 ? 0 : (cy > nch - 1 ? nch - 1 : cy);
+                pb[i] = (cx / bs) * nby + (cy / bs);
+                bstart[pb[i] + 1]++;
+            }
+            for (int b = 0; b < NBK; b++) bstart[b + 1] += bstart[b];
+            {
+                int32_t* cur = (int32_t*)malloc(sizeof(int32_t) * (size_t)NBK);
+                memcpy(cur, bstart, sizeof(int32_t) * (size_t)NBK);
+                for (int i = 0; i < npl; i++) items[cur[pb[i]]++] = i;
+                free(cur);
+            }
+            for (int a = 0; a < n_att; a++) link[a] = -1;
+            int forced = 0;
+            const int nn = T->nearest;
+            for (int rd = 0; rd <= S->rounds; rd++) {
+                const int free_round = rd == S->rounds;
+                for (int a = 0; a < n_att; a++) {
+                    prop[a] = -1;
+                    if (link[a] >= 0) continue;
+                    const int p = list[a];
+                    const int h = o->person_hh[p];
+                    const float hx = o->hh_x[h], hy = o->hh_y[h];
+                    int cx = (int)(hx / S->cell_width), cy = (int)(hy / S->cell_height);
+                    cx = cx < 0 ? 0 : (cx > ncw - 1 ? ncw - 1 : cx);
+                    cy = cy < 0 ? 0 : (cy > nch - 1 ? nch - 1 : cy);
+                    const int bx = cx / bs, by = cy / bs;
+                    setup_cand top[CS_SETUP_MAX_NEAREST];
+                    int ntop = 0, found = 0, extra = -1;
+                    const int rmax = nbx > nby ? nbx : nby;
+                    for (int r = 0; r < rmax && extra != 0; r++) {
+                        /* the square ring at Chebyshev distance r, any order */
+                        for (int x = bx - r; x <= bx + r; x++)
+                            for (int y = by - r; y <= by + r; y++) {
+                                if (x != bx - r && x != bx + r && y != by - r && y != by + r) continue;
+                                if (x < 0 || y < 0 || x >= nbx || y >= nby) continue;
+                                const int bk = x * nby + y;
+                                for (int e = bstart[bk]; e < bstart[bk + 1]; e++) {
+                                    const int pl = items[e];
+                                    if (!free_round && rem[pl] <= 0) continue;
+                                    found++;
+                                    const double d2 = setup_dist2(P, hx, hy, o->place_x[t][pl], o->place_y[t][pl]);
+                                    if (ntop == nn && !setup_cand_less(d2, pl, &top[nn - 1])) continue;
+                                    int k = (ntop < nn) ? ntop++ : nn - 1;
+                                    while (k > 0 && setup_cand_less(d2, pl, &top[k - 1])) { top[k] = top[k - 1]; k--; }
+                                    top[k].d2 = d2;
+                                    top[k].pl = pl;
+                                }
+                            }
+                        if (extra > 0) extra--;
+                        else if (extra < 0 && found >= nn) extra = 1;
+                    }
+                    if (ntop == 0) continue;
+                    double w[CS_SETUP_MAX_NEAREST], tot = 0.0;
+                    for (int k = 0; k < ntop; k++) {
+                        w[k] = setup_knum(T->kernel_lookup, T->kernel_hi_res, P, top[k].d2) *
+                               (free_round ? 1.0 : (double)rem[top[k].pl]);
+                        tot = tot + w[k];
+                    }
+                    int k = 0;
+                    if (tot > 0) {
+                        stream sc;
+                        stream_init(&sc, seed, CS_RNG_SETUP_CHOOSE, (uint32_t)rd, (uint32_t)p, (uint32_t)t);
+                        double u = stream_next(&sc) * tot;
+                        while (k + 1 < ntop && u >= w[k]) { u -= w[k]; k++; }
+                    } else if (!free_round) {
+                        continue;
+                    }
+                    prop[a] = top[k].pl;
+                }
+                for (int a = 0; a < n_att; a++)
+                    if (prop[a] >= 0) nprop[prop[a]]++;
+                for (int a = 0; a < n_att; a++) {
+                    const int pl = prop[a];
+                    if (pl < 0) continue;
+                    int ok = 1;
+                    if (!free_round && nprop[pl] > rem[pl]) {
+                        stream sa;
+                        stream_init(&sa, seed, CS_RNG_SETUP_ACCEPT, (uint32_t)rd, (uint32_t)list[a], (uint32_t)t);
+                        ok = stream_next(&sa) * (double)nprop[pl] < (double)rem[pl];
+                    }
+                    if (!ok) continue;
+                    link[a] = pl;
+                    taken[pl]++;
+                    if (free_round) forced++;
+                }
+                for (int i = 0; i < npl; i++) {
+                    rem[i] = rem[i] - taken[i] > 0 ? rem[i] - taken[i] : 0;
+                    taken[i] = 0;
+                    nprop[i] = 0;
+                }
+            }
+            o->forced[t] = forced;
+            /* member lists by (place, random key), then groups */
+            setup_key* keys = (setup_key*)malloc(sizeof(setup_key) * (size_t)n_att);
+            int32_t* mcount = (int32_t*)calloc((size_t)npl, sizeof(int32_t));
+            for (int a = 0; a < n_att; a++) {
+                const int p = list[a];
+                const uint32_t hsh = (uint32_t)setup_rand64(seed, CS_RNG_SETUP_SHUFFLE, 0, (uint32_t)p, (uint32_t)t);
+                keys[a].key = ((uint64_t)(uint32_t)link[a] << 32) | hsh;
+                keys[a].a = a;
+                mcount[link[a]]++;
+                o->person_place[(int64_t)t * N + p] = link[a];
+            }
+            qsort(keys, (size_t)n_att, sizeof(setup_key), setup_key_cmp);
+            SETUP_ALLOC(o->place_members[t], n_att, int32_t);
+            for (int a = 0; a < n_att; a++) o->place_members[t][a] = list[keys[a].a];
+            free(keys);
+            SETUP_ALLOC(o->place_member_ofs[t], npl + 1, int32_t);
+            SETUP_ALLOC(o->place_group_ofs[t], npl + 1, int32_t);
+            int ngt = 0;
+            for (int i = 0; i < npl; i++) {
+                o->place_member_ofs[t][i + 1] = o->place_member_ofs[t][i] + mcount[i];
+                int g = (int)floor((double)mcount[i] / (double)T->group_size + 0.5);
+                if (g < 1) g = 1;
+                o->place_group_ofs[t][i + 1] = o->place_group_ofs[t][i] + g;
+                ngt += g;
+            }
+            o->n_groups[t] = ngt;
+            SETUP_ALLOC(o->group_start[t], ngt, int32_t);
+            SETUP_ALLOC(o->group_size[t], ngt, int32_t);
+            for (int i = 0; i < npl; i++) {
+                const int64_t n = mcount[i], g = o->place_group_ofs[t][i + 1] - o->place_group_ofs[t][i];
+                for (int64_t k = 0; k < g; k++) {
+                    const int64_t st = (k * n) / g, en = ((k + 1) * n) / g;
+                    o->group_start[t][o->place_group_ofs[t][i] + k] = (int32_t)st;
+                    o->group_size[t][o->place_group_ofs[t][i] + k] = (int32_t)(en - st);
+                    for (int64_t r = st; r < en; r++)
+                        o->person_group[(int64_t)t * N + o->place_members[t][o->place_member_ofs[t][i] + r]] =
+                            (uint16_t)k;
+                }
+            }
+            free(mcount);
+            free(rem);
+            free(bstart);
+            free(items);
+            free(pb);
+            free(link);
+            free(prop);
+            free(nprop);
+            free(taken);
+        }
+    }
+    if (err) rc = setup_fail(s, CS_E_OVERFLOW, "setup: a bounded sampling loop gave up");
+done:
+    free(q);
+    free(qb);
+    free(pref);
+    free(cnt);
+    free(mcell_start);
+    free(mcell_n);
+    free(taken_p);
+    free(list);
+    return rc;
+}
+
+int cs_cpu_setup_run(const cs_setup_spec* spec, const cs_params* params, cs_cpu_setup** out)
+{
+    if (!out) return CS_E_ARG;
+    *out = NULL;
+    if (!spec || !params) return CS_E_ARG;
+    cs_cpu_setup* s = (cs_cpu_setup*)calloc(1, sizeof(cs_cpu_setup));
+    if (!s) return CS_E_ARG;
+    *out = s;
+    return setup_run(s, spec, params);
+}
+
+int cs_cpu_setup_sizes(cs_cpu_setup* s, cs_setup_out* o)
+{
+    if (!s || !o) return CS_E_ARG;
+    const cs_setup_out* a = &s->o;
+    o->n_people = a->n_people;
+    o->n_households = a->n_households;
+    o->n_cells = a->n_cells;
+    o->n_mcells = a->n_mcells;
+    o->n_adunits = a->n_adunits;
+    o->num_place_types = a->num_place_types;
+    for (int t = 0; t < CS_MAX_PLACE_TYPES; t++) {
+        o->n_places[t] = a->n_places[t];
+        o->n_groups[t] = a->n_groups[t];
+        o->n_attendees[t] = a->n_attendees[t];
+        o->forced[t] = a->forced[t];
+    }
+    o->device_ms = 0;
+    return CS_OK;
+}
+
+static void setup_get(void* dst, const void* src, size_t bytes)
+{
+    if (dst && src && bytes) memcpy(dst, src, bytes);
+}
+
+int cs_cpu_setup_download(cs_cpu_setup* s, const cs_setup_out* o)
+{
+    if (!s || !o) return CS_E_ARG;
+    const cs_setup_out* a = &s->o;
+    const size_t N = (size_t)a->n_people, NH = (size_t)a->n_households, NM = (size_t)a->n_mcells,
+                 NC = (size_t)a->n_cells, npt = (size_t)a->num_place_types;
+    setup_get(o->person_hh, a->person_hh, 4 * N);
+    setup_get(o->person_mcell, a->person_mcell, 4 * N);
+    setup_get(o->person_age, a->person_age, N);
+    setup_get(o->person_place, a->person_place, 4 * N * npt);
+    setup_get(o->person_group, a->person_group, 2 * N * npt);
+    setup_get(o->hh_first, a->hh_first, 4 * NH);
+    setup_get(o->hh_nh, a->hh_nh, 2 * NH);
+    setup_get(o->hh_x, a->hh_x, 4 * NH);
+    setup_get(o->hh_y, a->hh_y, 4 * NH);
+    setup_get(o->mcell_cell, a->mcell_cell, 4 * NM);
+    setup_get(o->mcell_adunit, a->mcell_adunit, 4 * NM);
+    setup_get(o->mcell_grid, a->mcell_grid, 8 * NM);
+    setup_get(o->cell_grid, a->cell_grid, 4 * NC);
+    setup_get(o->cell_start, a->cell_start, 4 * (NC + 1));
+    for (size_t t = 0; t < npt; t++) {
+        const size_t np = (size_t)a->n_places[t], na = (size_t)a->n_attendees[t], ng = (size_t)a->n_groups[t];
+        setup_get(o->place_mcell[t], a->place_mcell[t], 4 * np);
+        setup_get(o->place_x[t], a->place_x[t], 4 * np);
+        setup_get(o->place_y[t], a->place_y[t], 4 * np);
+        setup_get(o->place_member_ofs[t], a->place_member_ofs[t], 4 * (np + 1));
+        setup_get(o->place_members[t], a->place_members[t], 4 * na);
+        setup_get(o->place_group_ofs[t], a->place_group_ofs[t], 4 * (np + 1));
+        setup_get(o->group_start[t], a->group_start[t], 4 * ng);
+        setup_get(o->group_size[t], a->group_size[t], 4 * ng);
+    }
+    return CS_OK;
+}
+
+const char* cs_cpu_setup_last_error(const cs_cpu_setup* s)
+{
+    return s ? s->err : "null set-up handle";
+}
+
+void cs_cpu_setup_destroy(cs_cpu_setup* s)
+{
+    if (!s) return;
+    cs_setup_out* a = &s->o;
+    free(a->person_hh); free(a->person_mcell); free(a->person_age); free(a->person_place); free(a->person_group);
+    free(a->hh_first); free(a->hh_nh); free(a->hh_x); free(a->hh_y);
+    free(a->mcell_cell); free(a->mcell_adunit); free(a->mcell_grid); free(a->cell_grid); free(a->cell_start);
+    for (int t = 0; t < CS_MAX_PLACE_TYPES; t++) {
+        free(a->place_mcell[t]); free(a->place_x[t]); free(a->place_y[t]); free(a->place_member_ofs[t]);
+        free(a->place_members[t]); free(a->place_group_ofs[t]); free(a->group_start[t]); free(a->group_size[t]);
+    }
+    free(s);
+}

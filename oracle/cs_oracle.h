@@ -64,6 +64,15 @@ int cs_cpu_build_kernel_table(int kernel_type, double scale, double shape, doubl
                               double longest_d2, int size, int expansion, double* lookup_out,
                               double* hi_res_out, double* delta_out);
 
+/* Population set-up, restated: the same results as cs_gpu_setup_run on the same
+ * spec, array for array. */
+typedef struct cs_cpu_setup cs_cpu_setup;
+int cs_cpu_setup_run(const cs_setup_spec* spec, const cs_params* params, cs_cpu_setup** out);
+int cs_cpu_setup_sizes(cs_cpu_setup* setup, cs_setup_out* sizes);
+int cs_cpu_setup_download(cs_cpu_setup* setup, const cs_setup_out* dst);
+const char* cs_cpu_setup_last_error(const cs_cpu_setup* setup);
+void cs_cpu_setup_destroy(cs_cpu_setup* setup);
+
 #ifdef __cplusplus
 }
 #endif

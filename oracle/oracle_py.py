@@ -58,6 +58,11 @@ def load():
         "cs_cpu_build_kernel_table": (I, [I, D, D, D, D, D, I, I, V, V, P(D)]),
         "cs_cpu_upload_state": (I, [V, C.c_uint64, P(abi.cs_state_view)]),
         "cs_cpu_calc": (D, [V, I, I, I, I, I]),
+        "cs_cpu_setup_run": (I, [P(abi.cs_setup_spec), P(abi.cs_params), P(V)]),
+        "cs_cpu_setup_sizes": (I, [V, P(abi.cs_setup_out)]),
+        "cs_cpu_setup_download": (I, [V, P(abi.cs_setup_out)]),
+        "cs_cpu_setup_last_error": (C.c_char_p, [V]),
+        "cs_cpu_setup_destroy": (None, [V]),
         "cs_cpu_sample_many": (I, [I, C.c_uint64, D, D, I, V]),
     }
     for name, (res, args) in sig.items():
@@ -157,3 +162,24 @@ class OracleBackend:
 
     def kernel_num(self, r2):
         return self.lib.cs_cpu_kernel_num(self.ctx, r2)
+
+
+def setup_population(n_people, grid, **kw):
+    """The oracle's restatement of the set-up kernels (cs_cpu_setup_run) on the spec
+    covidsim_b200.population.generate_on_device builds: a Population to compare
+    with the GPU's array for array."""
+    from covidsim_b200 import abi, population
+    lib = load()
+    S, P, keep = population.setup_spec(n_people, grid, **kw)
+    h = C.c_void_p()
+    rc = lib.cs_cpu_setup_run(C.byref(S), C.byref(P), C.byref(h))
+    try:
+        if rc != 0:
+            raise RuntimeError("cs_cpu_setup_run: %s" % lib.cs_cpu_setup_last_error(h).decode())
+        sizes = abi.cs_setup_out()
+        lib.cs_cpu_setup_sizes(h, C.byref(sizes))
+        pop = population.from_setup(sizes, lambda out: lib.cs_cpu_setup_download(h, C.byref(out)), grid)
+    finally:
+        lib.cs_cpu_setup_destroy(h)
+    del keep
+    return pop
