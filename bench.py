@@ -78,6 +78,8 @@ def parse():
                     help="c4 only: scenarios drawn at random from the sweep to measure accuracy on")
     ap.add_argument("--c4-save", default=None, help="c4 only: write the simulated data sets to this .npz")
     ap.add_argument("--c4-people", type=int, default=1_000_000, help="c4 only: population size")
+    ap.add_argument("--setup", default="host", choices=["host", "gpu"],
+                    help="build the population with the host generator or the set-up kernels on the GPU")
     ap.add_argument("--population-cache", default=None,
                     help="directory keeping generated populations (.npz) for later runs")
     ap.add_argument("--no-e2e", action="store_true")
@@ -249,7 +251,12 @@ def run_ours(args):
     from covidsim_b200 import population, params as prm, sim
 
     preset, days, with_iv, desc, n_seed = WORKLOADS[args.workload]
-    pop = population.cached(args.population_cache, preset, lambda: population.preset(preset))
+    t_setup = time.perf_counter()
+    if args.setup == "gpu":
+        pop = population.cached(args.population_cache, preset + "_gpu", lambda: population.preset(preset, device=local))
+    else:
+        pop = population.cached(args.population_cache, preset, lambda: population.preset(preset))
+    t_setup = time.perf_counter() - t_setup
     P, lk, hr = prm.build_params(pop.grid)
     beta, r0parts = sim.calibrate_local_beta(pop, P, 2.4)
     P.LocalBeta = beta
@@ -419,7 +426,9 @@ def run_ours(args):
                    "realisations_per_rank": args.steps, "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2 (%.0f MB resident)" % (pop.nbytes() / 1e6),
                    "local_beta": round(beta, 6), "r0_parts": {k: round(float(v), 4) for k, v in r0parts.items()},
-                   "tuned": {"grid": tuned["grid"], "spatial_lanes": tuned["spatial_lanes"]}},
+                   "tuned": {"grid": tuned["grid"], "spatial_lanes": tuned["spatial_lanes"]},
+                   "setup": {"kind": args.setup, "seconds": round(t_setup, 2),
+                             "device_ms": round(pop.setup_info["device_ms"], 1) if pop.setup_info else None}},
         "runs_per_hour": round(runs_per_hour, 1),
         "outcomes": [{"cumI": a, "deaths": b, "peak_day": c} for a, b, c in finals],
         "clocks": clocks, "e2e": e2e, "e2e_python_host": e2e_py if e2e is not e2e_py else None,

@@ -181,6 +181,9 @@ def load_library(path=LIB_PATH):
         "cs_gpu_run": (I, [V, I, P(cs_run_policy), V]),
         "cs_gpu_batch_run": (I, [V, I, V, V]),
         "cs_gpu_get_cell_counts": (I, [V, V, V, V, V, V]),
+        "cs_gpu_get_sample": (I, [V, V, V, V, V, V, P(cs_counters)]),
+        "cs_host_alloc": (V, [C.c_size_t]),
+        "cs_host_free": (None, [V]),
         "cs_gpu_sync": (I, [V]),
         "cs_gpu_stream": (V, [V]),
         "cs_gpu_launch_count": (C.c_int64, [V]),

@@ -319,24 +319,25 @@ def generate(n_people, grid, sigma=1.2, seed=98798150, blobs=0, blob_share=0.0, 
 
 
 # ------------------------------------------------------------------ presets
-def preset(name, n_people=None, seed=98798150, adunit_grid=None):
-    """Geography and population of a named workload: c0, c1, c1_240, c3 or tiny."""
+def preset(name, n_people=None, seed=98798150, adunit_grid=None, device=None):
+    """Geography and population of a named workload: c0, c1, c1_240, c3 or tiny;
+    built by the host generator, or by the set-up kernels on CUDA device `device`."""
+    gen = generate if device is None else (lambda *a, **k: generate_on_device(*a, device=device, **k))
     if name == "c0":   # 1 M people, 2 x 2 degrees, 240 x 240 cells, 10 x 10 microcells
         grid = make_grid(cell_deg=1.0 / 120, nmcl=10)
-        return generate(n_people or 1_000_000, grid, sigma=1.2, seed=seed)
+        return gen(n_people or 1_000_000, grid, sigma=1.2, seed=seed)
     if name == "c1":   # 10 M people, 600 x 600 cells
         grid = make_grid(cell_deg=1.0 / 300, nmcl=10)
-        return generate(n_people or 10_000_000, grid, sigma=1.2, seed=seed)
+        return gen(n_people or 10_000_000, grid, sigma=1.2, seed=seed)
     if name == "c1_240":  # 10 M people on the 240 x 240 grid the reference can allocate
         grid = make_grid(cell_deg=1.0 / 120, nmcl=10)
-        return generate(n_people or 10_000_000, grid, sigma=1.2, seed=seed)
+        return gen(n_people or 10_000_000, grid, sigma=1.2, seed=seed)
     if name == "c3":   # 66 M people, 1500 x 1500 cells, urban blobs, 10 x 10 admin units
         grid = make_grid(width_deg=5.0, height_deg=5.0, cell_deg=1.0 / 300, nmcl=4)
-        return generate(n_people or 66_000_000, grid, sigma=1.5, seed=seed, blobs=30, blob_share=0.4,
-                        adunit_grid=10)
+        return gen(n_people or 66_000_000, grid, sigma=1.5, seed=seed, blobs=30, blob_share=0.4, adunit_grid=10)
     if name == "tiny":  # parity-test scale (optionally with adunit_grid^2 admin units)
         grid = make_grid(width_deg=0.2, height_deg=0.2, cell_deg=1.0 / 60, nmcl=4)
-        return generate(n_people or 20_000, grid, sigma=1.0, seed=seed, adunit_grid=adunit_grid)
+        return gen(n_people or 20_000, grid, sigma=1.0, seed=seed, adunit_grid=adunit_grid)
     raise ValueError("unknown preset %r" % name)
 
 

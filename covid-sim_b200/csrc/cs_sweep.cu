@@ -3560,6 +3560,41 @@ int cs_gpu_get_counters(cs_gpu_ctx* c, cs_counters* out)
     return CS_OK;
 }
 
+// The cell counts and the counter block together, waited for once: what the
+// reference's RecordSample reads at every output step.  From page-locked buffers
+// (cs_host_alloc) the six copies run at the link's rate.
+int cs_gpu_get_sample(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D, cs_counters* out)
+{
+    if (!c || !out) return CS_E_ARG;
+    DevPop& d = c->d;
+    const size_t n = sizeof(int32_t) * d.NC;
+    if (S) CK(cudaMemcpyAsync(S, d.S, n, cudaMemcpyDeviceToHost, c->stream));
+    if (L) CK(cudaMemcpyAsync(L, d.L, n, cudaMemcpyDeviceToHost, c->stream));
+    if (I) CK(cudaMemcpyAsync(I, d.I, n, cudaMemcpyDeviceToHost, c->stream));
+    if (R) CK(cudaMemcpyAsync(R, d.R, n, cudaMemcpyDeviceToHost, c->stream));
+    if (D) CK(cudaMemcpyAsync(D, d.D, n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemsetAsync(d.C, 0, 5 * sizeof(int64_t), c->stream));  // S..D recomputed below
+    LAUNCH(k_cell_totals, 64, kThreads, d);
+    CK(cudaMemcpyAsync(out, d.C, sizeof(cs_counters), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (out->err_queue_overflow || out->err_spatial_tries || out->err_kernel_range)
+        return set_err(c, CS_E_OVERFLOW, "bounded device loop gave up (spatial %lld, queue %lld, kernel range %lld)",
+                       (long long)out->err_spatial_tries, (long long)out->err_queue_overflow, (long long)out->err_kernel_range);
+    return CS_OK;
+}
+
+void* cs_host_alloc(size_t bytes)
+{
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void cs_host_free(void* p)
+{
+    if (p) cudaFreeHost(p);
+}
+
 int cs_gpu_get_cell_counts(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D)
 {
     if (!c) return CS_E_ARG;

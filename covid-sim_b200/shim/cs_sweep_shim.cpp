@@ -79,7 +79,36 @@ double g_prev_prop = 1.0;      // RunModel's PreviousProportionSusceptible (src/
 bool g_update_probs = false;   // RunModel called UpdateProbs(0) after the last step
 long g_step_in_run = 0;        // timesteps of the current realisation so far
 int64_t g_tg_base = 0, g_si_base = 0, g_ntg_base = 0, g_tg_set = 0, g_si_set = 0, g_ntg_set = 0;
-std::vector<int32_t> g_S, g_L, g_I, g_R, g_D;
+// A page-locked host array (cs_host_alloc): the state upload at a realisation's
+// start and the copies back at output steps run at the link's rate from it.
+template <typename T>
+struct Pinned {
+    T* p = nullptr;
+    size_t n = 0;
+    Pinned() = default;
+    Pinned(const Pinned&) = delete;
+    Pinned& operator=(const Pinned&) = delete;
+    ~Pinned() { cs_host_free(p); }
+    void resize(size_t m)
+    {
+        if (m == n) return;
+        cs_host_free(p);
+        p = (T*)cs_host_alloc(sizeof(T) * (m ? m : 1));
+        if (!p) ERR_CRITICAL("GPU sweep: page-locked host allocation failed\n");
+        n = m;
+    }
+    void assign(size_t m, T v)
+    {
+        resize(m);
+        for (size_t i = 0; i < m; i++) p[i] = v;
+    }
+    size_t size() const { return n; }
+    T* data() { return p; }
+    T& operator[](size_t i) { return p[i]; }
+    const T& operator[](size_t i) const { return p[i]; }
+};
+
+Pinned<int32_t> g_S, g_L, g_I, g_R, g_D;
 cs_params g_params;
 // what the device holds of the host's intervention state
 std::vector<uint8_t> g_sd, g_mr;              // per microcell: socdist, moverest (TreatStat)
@@ -356,13 +385,14 @@ void dump_block();
 // Host staging of the start state, kept from run to run so that later runs write
 // into memory that is already mapped.
 struct Staging {
-    std::vector<int8_t> inf;
-    std::vector<uint8_t> sev, fl;
-    std::vector<uint16_t> it, lt, rt, st, ct, sd, as, ae, iso, qs, dt;
-    std::vector<float> infn, susc, pa, pc;
-    std::vector<int32_t> infector, listpos, slots, S0, cS, cL, cI, cR, cD, cell_ofs;
-    std::vector<int16_t> itype;
-    std::vector<double> tp;
+    Pinned<int8_t> inf;
+    Pinned<uint8_t> sev, fl;
+    Pinned<uint16_t> it, lt, rt, st, ct, sd, as, ae, iso, qs, dt;
+    Pinned<float> infn, susc, pa, pc;
+    Pinned<int32_t> infector, listpos, slots, S0, cS, cL, cI, cR, cD;
+    std::vector<int32_t> cell_ofs;
+    Pinned<int16_t> itype;
+    Pinned<double> tp;
 };
 Staging g_stage;
 
@@ -444,14 +474,13 @@ void upload_run_state(int run)
 // RecordSample (src/CovidSim.cpp:3024-3120) reads per-cell counts and StateT[].
 void sync_back()
 {
-    check(cs_gpu_get_cell_counts(g_ctx, g_S.data(), g_L.data(), g_I.data(), g_R.data(), g_D.data()), "cs_gpu_get_cell_counts");
+    cs_counters k;
+    check(cs_gpu_get_sample(g_ctx, g_S.data(), g_L.data(), g_I.data(), g_R.data(), g_D.data(), &k), "cs_gpu_get_sample");
 #pragma omp parallel for schedule(static)
     for (int c = 0; c < P.NumPopulatedCells; c++) {
         Cell* x = CellLookup[c];
         x->S = g_S[c]; x->L = g_L[c]; x->I = g_I[c]; x->R = g_R[c]; x->D = g_D[c];
     }
-    cs_counters k;
-    check(cs_gpu_get_counters(g_ctx, &k), "cs_gpu_get_counters");
     PopVar& s = StateT[0];
     const PopVar& b = g_base;
     s.cumI = b.cumI + (int)k.cumI; s.cumC = b.cumC + (int)k.cumC; s.cumDC = b.cumDC + (int)k.cumDC;
@@ -530,14 +559,25 @@ void mirror_host_interventions(double t)
 {
     const double t_prev = t - P.ModelTimeStep;   // the time TreatSweep last ran at
     if (t_prev >= 0) unsupported_at(t_prev);
-    // the parameter block: ControlPropCasesId after the alert, efficacies varied over
-    // time, CFR scales (UpdateCFRs), seasonality
-    cs_params cur = params_from_reference();
-    cur.kernel_delta = g_params.kernel_delta;
-    cur.Seasonality = P.DoSeasonality ? P.Seasonality[((int)t) % DAYS_PER_YEAR] : 1.0;
-    if (std::memcmp(&cur, &g_params, sizeof(cs_params)) != 0) {
-        g_params = cur;
-        check(cs_gpu_set_params(g_ctx, &g_params), "cs_gpu_set_params");
+    // the parameter block.  The reference changes parameters only in RecordSample
+    // (ControlPropCasesId after the alert, src/CovidSim.cpp:3592) and UpdateCFRs (the
+    // CFR scales, :2840-2867), both run just before an output step's first
+    // timestep, and seasonality is read per day (src/Sweep.cpp:296).  The whole block
+    // is rebuilt and compared at a realisation's first step and at each output
+    // step's first; every step compares the fields that can move.
+    const double seas = P.DoSeasonality ? P.Seasonality[((int)t) % DAYS_PER_YEAR] : 1.0;
+    const bool boundary = g_step_in_run % P.NumModelTimeStepsPerOutputTimeStep == 0;
+    if (boundary || seas != g_params.Seasonality || P.ControlPropCasesId != g_params.ControlPropCasesId ||
+        P.CFR_Critical_Scale_Current != g_params.CFR_Critical_Scale_Current ||
+        P.CFR_SARI_Scale_Current != g_params.CFR_SARI_Scale_Current ||
+        P.CFR_ILI_Scale_Current != g_params.CFR_ILI_Scale_Current) {
+        cs_params cur = params_from_reference();
+        cur.kernel_delta = g_params.kernel_delta;
+        cur.Seasonality = seas;
+        if (std::memcmp(&cur, &g_params, sizeof(cs_params)) != 0) {
+            g_params = cur;
+            check(cs_gpu_set_params(g_ctx, &g_params), "cs_gpu_set_params");
+        }
     }
     // case isolation and household quarantine windows of each admin unit
     // (RecordSample, src/CovidSim.cpp:3598-3609; read by DoDetectedCase)

@@ -594,6 +594,16 @@ int cs_gpu_run(cs_gpu_ctx* ctx, int days, const cs_run_policy* policy, cs_counte
 int cs_gpu_batch_run(cs_gpu_batch* batch, int days, const cs_run_policy* policies, cs_counters* daily);
 /* Per-cell S, L, I, R, D (each n_cells) for RecordSample (src/CovidSim.cpp:3044-3056). */
 int cs_gpu_get_cell_counts(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D);
+/* cs_gpu_get_cell_counts and cs_gpu_get_counters in one call, with one wait: what
+ * RecordSample (src/CovidSim.cpp:3024-3120) reads at each output step.  Any of the
+ * five cell arrays may be NULL. */
+int cs_gpu_get_sample(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D,
+                      cs_counters* out);
+/* Page-locked host memory (NULL on failure) for a host's staging buffers: copies
+ * between it and the device run at the link's full rate and never through an
+ * intermediate buffer.  Free with cs_host_free. */
+void* cs_host_alloc(size_t bytes);
+void cs_host_free(void* p);
 /* Wait for the context's stream; returns a deferred device error if any. */
 int cs_gpu_sync(cs_gpu_ctx* ctx);
 /* The CUDA stream the context launches on (a cudaStream_t), for host-side timing. */

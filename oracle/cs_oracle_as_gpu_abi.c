@@ -8,6 +8,7 @@
  * oracle's whole-epidemic behaviour can be compared with the reference's own on
  * the CPU.
  */
+#include <stdlib.h>
 #include <string.h>
 
 #include "cs_oracle.h"
@@ -54,3 +55,12 @@ int cs_gpu_get_cell_counts(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, in
     v.cell_S = S; v.cell_L = L; v.cell_I = I; v.cell_R = R; v.cell_D = D;
     return cs_cpu_download_state((cs_cpu_ctx*)c, &v);
 }
+
+int cs_gpu_get_sample(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D, cs_counters* out)
+{
+    int r = cs_gpu_get_cell_counts(c, S, L, I, R, D);
+    return r ? r : cs_cpu_get_counters((cs_cpu_ctx*)c, out);
+}
+
+void* cs_host_alloc(size_t bytes) { return malloc(bytes ? bytes : 1); }
+void cs_host_free(void* p) { free(p); }
