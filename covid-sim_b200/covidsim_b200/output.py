@@ -8,8 +8,8 @@ TimeSeries[n] is the state at t = n days (n = 0 .. days), as RecordSample record
 it with a one-day output step (src/CovidSim.cpp:1411-1413, 1525); incidences are
 differences of cumulative counters between consecutive samples, the first from 0.
 Columns for features the sweep does not model (treatment, vaccination, contact
-tracing, the infection radius) are written as 0; Rt comes from the final
-per-person state when it is given.  Files and formats follow
+tracing) are written as 0; Rt comes from the final per-person state when it is
+given.  Files and formats follow
 SaveResults and SaveSummaryResults (src/CovidSim.cpp:1657-2199): `<base>.xls`,
 `<base>.severity.xls`, `<base>.age.xls`, `<base>.inftype.xls` and, with admin units,
 `<base>.adunit.xls`, tab-separated.
@@ -49,6 +49,15 @@ def time_series(blocks, model_timestep, small_epidemic_cases=-1, n_adunits=0):
     with np.errstate(invalid="ignore", divide="ignore"):
         ts["meanTG"] = np.where(ntg > 0, model_timestep * tg / np.maximum(ntg, 1), 0.0)
         ts["meanSI"] = np.where(ntg > 0, model_timestep * si / np.maximum(ntg, 1), 0.0)
+    # infection radii as RecordSample forms them (src/CovidSim.cpp:3059-3074, 3107,
+    # 3389-3390): it adds each thread's sum of squared radii twice, takes the root
+    # mean over all infections, and the largest radius so far
+    s2 = _col(b, "sumRad2_q") / 4294967296.0
+    cum_i = _col(b, "cumI")
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ts["rmsRad"] = np.where(cum_i > 0, np.sqrt((s2 + s2) / np.maximum(cum_i, 1.0)), 0.0)
+    off = getattr(abi.cs_counters, "maxRad2_bits").offset // 8
+    ts["maxRad"] = np.sqrt(np.ascontiguousarray(b[:, off]).view(np.float64))
     small = (ts["R"] <= small_epidemic_cases) if small_epidemic_cases >= 0 else np.ones(n, bool)
     ts["extinct"] = (small & (ts["I"] + ts["L"] == 0)).astype(np.float64)
     na = min(n_adunits, abi.CS_MAX_ADUNITS)
@@ -136,7 +145,7 @@ def write_results(base, blocks, model_timestep, small_epidemic_cases=-1, n_aduni
         f.write("t\tS\tL\tI\tR\tD\tincI\tincR\tincFC\tincC\tincDC\tincTC\tincCT\tincCC\tcumT\tcumTP\tcumV\tcumVG\t"
                 "Extinct\trmsRad\tmaxRad\n")
         cols = [ts["t"], ts["S"], ts["L"], ts["I"], ts["R"], ts["D"], ts["incI"], ts["incR"], ts["incFC"], ts["incC"],
-                ts["incDC"], z, z, z, z, z, z, z, ts["extinct"], z, z]
+                ts["incDC"], z, z, z, z, z, z, z, ts["extinct"], ts["rmsRad"], ts["maxRad"]]
         for r in np.stack(cols, axis=1):
             v = ["%.10f" % x for x in r]
             f.write("\t".join(v[:15]) + "\t" + v[15] + "t" + "\t".join(v[16:]) + "\n")

@@ -250,6 +250,24 @@ __device__ __forceinline__ double dist2_hh(const DevPop& d, const cs_params& P, 
     return periodic_xy(P, fabs(dx), fabs(dy));
 }
 
+// dist2_raw (src/Dist.cpp:163-170), in double from float locations: from a
+// household to a point (a place), and between two households.
+__device__ __forceinline__ double dist2_raw(const cs_params& P, double ax, double ay, double bx, double by)
+{
+    if (P.DoUTM_coords) return dist2_utm(P, ax, ay, bx, by);
+    return periodic_xy(P, fabs(ax - bx), fabs(ay - by));
+}
+__device__ __forceinline__ double dist2_hh_pt(const DevPop& d, const cs_params& P, int32_t ha, float bx, float by)
+{
+    float2 a = __ldg(reinterpret_cast<const float2*>(d.hhr + ha));
+    return dist2_raw(P, a.x, a.y, bx, by);
+}
+__device__ __forceinline__ double dist2_hh_raw(const DevPop& d, const cs_params& P, int32_t ha, int32_t hb)
+{
+    float2 b = __ldg(reinterpret_cast<const float2*>(d.hhr + hb));
+    return dist2_hh_pt(d, P, ha, b.x, b.y);
+}
+
 // dist2_cc_min (src/Dist.cpp:78-144) on grid cell indices.
 __device__ inline double dist2_cc_min(const cs_params& P, int l, int m)
 {

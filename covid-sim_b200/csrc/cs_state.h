@@ -72,6 +72,8 @@ struct DevPlaces {
     const int32_t* group_ofs;
     const int32_t* group_start;
     const int32_t* group_size;
+    const float* x;            // location (blanket movement restrictions measure to it)
+    const float* y;
     uint16_t* close_start;
     uint16_t* close_end;
     float* prob_close;
@@ -89,7 +91,8 @@ struct DevIv {
 // captured step graph needs only that one kernel's arguments changed per replay.
 struct DevStep {
     double t, fp, seas, sp_beta, hh_beta;
-    int32_t ts, pad;
+    int32_t ts;
+    int32_t blanket;           // blanket movement restrictions in place (src/Sweep.cpp:301)
     unsigned long long seed;
 };
 
@@ -184,6 +187,7 @@ struct DevPop {
     // (0xFFFF - start) << 16 | stop, 0 when none; listed once in carer_list
     uint32_t* carer_win;       // [NH]
     int32_t* carer_list;       // [NH]
+    double* rad_origin;        // [2] where infection radii are measured from
     cs_counters* C;
 };
 

@@ -870,7 +870,7 @@ __device__ __forceinline__ void k_set_step_body(const DevPop& d, double t, unsig
     DevStep st;
     st.t = t;
     st.ts = (int)(uint16_t)(P.TimeStepsPerDay * t);
-    st.pad = 0;
+    st.blanket = P.DoBlanketMoveRestr && (t >= P.MoveRestrTimeStart) && (t < P.MoveRestrTimeStart + P.MoveRestrDuration);
     st.fp = P.ModelTimeStep / (1 - P.FalsePositiveRate);
     st.seas = P.Seasonality;
     st.sp_beta = P.DoSpatial ? st.seas * st.fp * P.LocalBeta : 0.0;
@@ -916,7 +916,10 @@ __device__ void place_candidates(const DevPop& d, const cs_params& P, const Step
         if ((pt == P.CareHomePlaceType) && ((!ich) || (!is_ch(hm)))) sc *= P.CareHomeWorkerGroupScaling;
         if (hm.inf == CS_INF_SUSCEPTIBLE && !host_absent(hm, st.ts)) {
             sc *= calc_person_susc(hm, iag, P) * p / p;
-            if (moverest_differs(d, hm.mcell, mc_place)) sc *= P.MoveRestrEffect;
+            if (st.blanket) {
+                if (dist2_hh_pt(d, P, hm.hh, pl.x[link], pl.y[link]) > P.MoveRestrRadius2) sc *= P.MoveRestrEffect;
+            } else if (moverest_differs(d, hm.mcell, mc_place))
+                sc *= P.MoveRestrEffect;
             if ((sc == 1) || (s.next() < sc)) claim_infection(d, m, i, between ? 2 + pt + CS_MAX_PLACE_TYPES : 2 + pt);
         }
     }
@@ -1017,7 +1020,11 @@ __device__ __forceinline__ void k_infector_places_body(const DevPop& d)
         int i = d.act[idx];
         PersonHot hi = d.hot[i];
         double PI = st.fp * st.seas * calc_place_inf(hi, P, pt, st.ts);
-        if (moverest_differs(d, hi.mcell, d.pl[pt].mcell[link])) PI *= P.MoveRestrEffect;
+        if (st.blanket) {
+            if (dist2_hh_pt(d, P, hi.hh, d.pl[pt].x[link], d.pl[pt].y[link]) > P.MoveRestrRadius2)
+                PI *= P.MoveRestrEffect;
+        } else if (moverest_differs(d, hi.mcell, d.pl[pt].mcell[link]))
+            PI *= P.MoveRestrEffect;
         if (pt != P.HotelPlaceType) {
             double p1 = PI;
             if (p1 > 1) p1 = 1;
@@ -1045,7 +1052,7 @@ constexpr uint32_t kSpatialBlocksPerDraw = 2;
 __device__ __forceinline__ bool spatial_draw(const DevPop& d, const cs_params& P, Stream& s, int b,
                                              const double* row, const int16_t* guide_row, double total,
                                              int hh_inf, int& m_out, int& slot_out, int& p_out,
-                                             PersonHot& hp_out, int* oor)
+                                             PersonHot& hp_out, double& d2_out, int* oor)
 {
     // smallest B with target < row[B]: guide-table start, then walk
     double u1 = s.next();
@@ -1071,7 +1078,7 @@ __device__ __forceinline__ bool spatial_draw(const DevPop& d, const cs_params& P
     double d2 = dist2_hh(d, P, hh_inf, hp.hh);
     double accept = knum_f32(d, P, d2, oor) / bound_of(d, b, B);
     if ((s.next() >= accept) || !is_alive(hp.inf)) return false;
-    m_out = m; slot_out = slot; p_out = p; hp_out = hp;
+    m_out = m; slot_out = slot; p_out = p; hp_out = hp; d2_out = d2;
     return true;
 }
 
@@ -1101,6 +1108,7 @@ __device__ __forceinline__ void k_spatial_body(const DevPop& d)
         double total = row[d.NB - 1];
         if (!(total > 0)) { if (lane == 0) give_ups++; continue; }
         int m = 0, slot = 0, p = 0, won = -1;
+        double d2w = 0.0;
         PersonHot hp;
         Stream s(seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)st.ts, (uint32_t)i, (uint32_t)j);
         for (int t0 = 0; t0 < kMaxSpatialTries; t0 += kSpatialLanes) {
@@ -1108,7 +1116,7 @@ __device__ __forceinline__ void k_spatial_body(const DevPop& d)
             s = Stream(seed, CS_RNG_SPATIAL_CONTACT, (uint32_t)st.ts, (uint32_t)i, (uint32_t)j);
             s.block = kSpatialBlocksPerDraw * (uint32_t)t;
             bool acc = (t < kMaxSpatialTries) && spatial_draw(d, P, s, b, row, guide_row, total, hinf.hh,
-                                                              m, slot, p, hp, &oor);
+                                                              m, slot, p, hp, d2w, &oor);
             unsigned mask = tile.ballot(acc);
             int w = mask ? __ffs(mask) - 1 : kSpatialLanes;
             if (lane < w) oor_count += oor;   // draws up to the winner count, as in a sequential loop
@@ -1125,7 +1133,11 @@ __device__ __forceinline__ void k_spatial_body(const DevPop& d)
             if (slot < d.S[m]) {
                 ss *= calc_person_susc(hp, iag, P);
                 ss *= P.WAIFW_Matrix_SpatialOnly[age_group(hp)][iag];
-                if (moverest_differs(d, hp.mcell, hinf.mcell)) ss *= P.MoveRestrEffect;
+                if (st.blanket) {   // the draw's distance is dist2_raw's with UTM coordinates
+                    const double d2b = P.DoUTM_coords ? d2w : dist2_hh_raw(d, P, hinf.hh, hp.hh);
+                    if (d2b > P.MoveRestrRadius2) ss *= P.MoveRestrEffect;
+                } else if (moverest_differs(d, hp.mcell, hinf.mcell))
+                    ss *= P.MoveRestrEffect;
                 if ((!closed_i) && closures_possible(d, st.ts) && host_absent(hp, st.ts)) {
                     bool f = false;
                     for (int pt = 0; (pt < d.NPT) && (!f); pt++) {
@@ -1165,7 +1177,8 @@ __device__ __forceinline__ void k_apply_infections_body(const DevPop& d)
     const bool staged = nq >= kStageMinItems;
     stage_begin(d.C, staged);
     // single-address tallies, summed per thread and added once per warp
-    long long n_inf = 0, n_kw = 0, n_tg = 0, sum_tg = 0, sum_si = 0;
+    long long n_inf = 0, n_kw = 0, n_tg = 0, sum_tg = 0, sum_si = 0, rad_q = 0, rad_max = 0;
+    const double ox = d.rad_origin[0], oy = d.rad_origin[1];
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
         int p = d.queue[q];
         unsigned long long key = d.claim[p];
@@ -1187,6 +1200,13 @@ __device__ __forceinline__ void k_apply_infections_body(const DevPop& d)
         atomicAdd(d.cnt + cell, 1);  // transitions out of this cell's S block
         mark_cell(d, cell);
         n_inf++;
+        if (infector != -2) {   // a seed's radius is 0 (the origin moved to it)
+            const HouseholdRec hr = load_household(d, h.hh);
+            const double x = (double)hr.x - ox, y = (double)hr.y - oy;
+            const double r2 = x * x + y * y;
+            rad_q += (long long)(r2 * 4294967296.0);
+            rad_max = max(rad_max, __double_as_longlong(r2));
+        }
         cnt_add(CSB_STAGED(cumItype[it % CS_INFECT_TYPE_MASK]), 1);
         cnt_add(CSB_STAGED(cumIa[age_group(h)]), 1);
         if (h.pflags & CS_PF_KEYWORKER) n_kw++;
@@ -1213,6 +1233,12 @@ __device__ __forceinline__ void k_apply_infections_body(const DevPop& d)
     cnt_add_warp(CSB_CTR(cumTG), sum_tg);
     cnt_add_warp(CSB_CTR(cumSI), sum_si);
     cnt_add_warp(CSB_CTR(nTG), n_tg);
+    cnt_add_warp(CSB_CTR(sumRad2_q), rad_q);
+    {
+        long long m = rad_max;
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0 && m > 0) atomicMax((long long*)CSB_CTR(maxRad2_bits), m);
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_STAGED(work_new_infections), nq);
     stage_flush(d.C, staged);
 }
@@ -1674,6 +1700,12 @@ __global__ void k_seed_claims(DevPop d, const int32_t* list, int n)
         if (d.hot[p].inf != CS_INF_SUSCEPTIBLE) continue;
         unsigned long long key = ((unsigned long long)(uint32_t)(-2) << 8) | (unsigned long long)(CS_INFECT_TYPE_MASK - 1);
         if (atomicCAS(d.claim + p, ~0ull, key) == ~0ull) d.queue[append(d.counts + kCntQueue)] = p;
+        // radii are measured from the last seed's household (src/CovidSim.cpp:1358-1359)
+        if (k == n - 1) {
+            const HouseholdRec hr = load_household(d, d.hot[p].hh);
+            d.rad_origin[0] = (double)hr.x;
+            d.rad_origin[1] = (double)hr.y;
+        }
     }
 }
 
@@ -2188,6 +2220,7 @@ static int alloc_dynamic(cs_gpu_ctx* c)
     { unsigned long long* t; AL(t, 1); c->d_seed = t; d.seed_src = t; CK(cudaMemsetAsync(t, 0, sizeof(*t), c->stream)); }
     d.t_src = nullptr;
     { cs_counters* t; AL(t, 1); c->dC = t; d.C = t; CK(cudaMemsetAsync(t, 0, sizeof(cs_counters), c->stream)); }
+    { double* t; UP(t, params->LocationInitialInfection, 2); d.rad_origin = t; }
 #undef UP
 #undef AL
     CK(cudaStreamSynchronize(c->stream));   // the parameter and window copies came from the stack
@@ -2299,6 +2332,8 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
         { int32_t* t; UP(t, pop->place_group_ofs[pt], np + 1); pl.group_ofs = t; }
         { int32_t* t; UP(t, pop->group_start[pt], ng); pl.group_start = t; }
         { int32_t* t; UP(t, pop->group_size[pt], ng); pl.group_size = t; }
+        { float* t; UP(t, pop->place_x[pt], np); pl.x = t; }
+        { float* t; UP(t, pop->place_y[pt], np); pl.y = t; }
     }
     // proposal blocks
     int bs = params->block_cells;
@@ -3735,6 +3770,9 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
     CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
     CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
+    // the host seeded the run: its LocationInitialInfection is where radii start
+    CK(cudaMemcpyAsync(d.rad_origin, c->hp.LocationInitialInfection, sizeof(double) * 2, cudaMemcpyHostToDevice,
+                       c->stream));
     c->seed = seed;
     CK(cudaMemcpyAsync(c->d_seed, &c->seed, sizeof(c->seed), cudaMemcpyHostToDevice, c->stream));
     int r = reset_run_level(c, seed);

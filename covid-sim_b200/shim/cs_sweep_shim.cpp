@@ -208,6 +208,11 @@ cs_params params_from_reference()
     for (int i = 0; i < CS_NUM_NPI; i++)
         for (int j = 0; j < CS_NUM_SETTINGS; j++) p.Efficacies[i][j] = P.Efficacies[i][j];
     p.MoveRestrEffect = P.MoveRestrEffect;
+    p.DoBlanketMoveRestr = P.DoBlanketMoveRestr;
+    p.MoveRestrTimeStart = P.MoveRestrTimeStart; p.MoveRestrDuration = P.MoveRestrDuration;
+    p.MoveRestrRadius2 = P.MoveRestrRadius2;
+    p.LocationInitialInfection[0] = P.LocationInitialInfection[0][0];
+    p.LocationInitialInfection[1] = P.LocationInitialInfection[0][1];
     p.LatentPeriod = P.LatentPeriod; p.InfectiousPeriod = P.InfectiousPeriod; p.LatentToSymptDelay = P.LatentToSymptDelay;
     p.SymptInfectiousness = P.SymptInfectiousness; p.AsymptInfectiousness = P.AsymptInfectiousness;
     p.InfectiousnessSD = P.InfectiousnessSD;
@@ -245,7 +250,6 @@ void unsupported_features()
 {
     if (P.DoDigitalContactTracing) ERR_CRITICAL("GPU sweep: digital contact tracing is not supported\n");
     if (P.DoAirports) ERR_CRITICAL("GPU sweep: airports / travel are not supported\n");
-    if (P.DoBlanketMoveRestr) ERR_CRITICAL("GPU sweep: blanket movement restrictions are not supported\n");
     if (P.FalsePositiveRate > 0) ERR_CRITICAL("GPU sweep: false-positive cases are not supported\n");
     if (P.DoHolidays && P.NumHolidays > 0) ERR_CRITICAL("GPU sweep: holidays are not supported\n");
     if (P.DoInterventionDelaysByAdUnit) ERR_CRITICAL("GPU sweep: intervention delays by admin unit are not supported\n");
@@ -513,6 +517,13 @@ void sync_back()
             s.cumCritical_adunit[a] = b.cumCritical_adunit[a] + (int)k.cumCritical_adunit[a];
             s.Critical_adunit[a] = b.Critical_adunit[a] + (int)k.Critical_adunit[a];
         }
+    // infection radii (DoInfect, src/Update.cpp:116-127): the device's since the upload
+    s.sumRad2 = b.sumRad2 + (double)k.sumRad2_q / 4294967296.0;
+    {
+        double m;
+        std::memcpy(&m, &k.maxRad2_bits, sizeof m);
+        s.maxRad2 = m > b.maxRad2 ? m : b.maxRad2;
+    }
     // generation-time sums are read and zeroed by each RecordSample: hand over increments
     if (s.cumTG != g_tg_set || s.nTG != g_ntg_set) { g_tg_base += g_tg_set; g_si_base += g_si_set; g_ntg_base += g_ntg_set; }
     g_tg_set = k.cumTG - g_tg_base; g_si_set = k.cumSI - g_si_base; g_ntg_set = k.nTG - g_ntg_base;
@@ -550,6 +561,8 @@ void dump_block()
     cs_counters k;
     check(cs_gpu_get_counters(g_ctx, &k), "cs_gpu_get_counters");
     b.cumTG = g_base.cumTG + k.cumTG; b.cumSI = g_base.cumSI + k.cumSI; b.nTG = g_base.nTG + k.nTG;
+    b.sumRad2_q = (int64_t)(s.sumRad2 * 4294967296.0);
+    std::memcpy(&b.maxRad2_bits, &s.maxRad2, sizeof(double));
     if (std::fwrite(&b, sizeof(b), 1, g_dump) != 1) ERR_CRITICAL("GPU sweep: writing the counter blocks failed\n");
 }
 

@@ -189,6 +189,15 @@ typedef struct cs_params {
     double CareHomeWorkerGroupScaling, CareHomeResidentPlaceScaling, CareHomeRelProbHosp;
     double Efficacies[CS_NUM_NPI][CS_NUM_SETTINGS];    /* P.Efficacies[npi][setting] */
     double MoveRestrEffect;
+    /* blanket movement restrictions (P.DoBlanketMoveRestr, src/Sweep.cpp:300-301):
+     * from MoveRestrTimeStart for MoveRestrDuration days, a contact whose two ends
+     * lie more than sqrt(MoveRestrRadius2) apart (dist2_raw) is scaled by
+     * MoveRestrEffect, in place of the microcells' movement-restriction test */
+    int32_t DoBlanketMoveRestr, _pad3;
+    double MoveRestrTimeStart, MoveRestrDuration, MoveRestrRadius2;
+    /* the point infection radii are measured from (P.LocationInitialInfection[0];
+     * seeding moves it to the last seed's household, src/CovidSim.cpp:1358-1359) */
+    double LocationInitialInfection[2];
     /* natural history */
     double LatentPeriod, InfectiousPeriod, LatentToSymptDelay;
     double SymptInfectiousness, AsymptInfectiousness, InfectiousnessSD;
@@ -339,6 +348,11 @@ typedef struct cs_counters {
     int64_t cumI_adunit[CS_MAX_ADUNITS], cumC_adunit[CS_MAX_ADUNITS], cumD_adunit[CS_MAX_ADUNITS];
     int64_t cumDC_adunit[CS_MAX_ADUNITS], cumCritical_adunit[CS_MAX_ADUNITS];
     int64_t Critical_adunit[CS_MAX_ADUNITS];
+    /* infection radii from LocationInitialInfection (DoInfect, src/Update.cpp:116-127,
+     * 1477): the sum of squared radii in units of 2^-32 square degrees (an integer, so
+     * the sum does not depend on order) and the largest squared radius as the bits of
+     * a non-negative double; a seed's own radius is 0, as the reference measures it */
+    int64_t sumRad2_q, maxRad2_bits;
     /* work done by the sweeps (for the HBM roofline) */
     int64_t work_infectors, work_hh_members, work_place_candidates;
     int64_t work_spatial_contacts, work_spatial_draws, work_new_infections;

@@ -62,6 +62,8 @@ struct cs_cpu_ctx {
     uint8_t *age, *pflags;
     float *hh_x, *hh_y;
     place_arrays pl[CS_MAX_PLACE_TYPES];
+    int blanket;                 /* blanket movement restrictions in place this step */
+    double rad_origin[2];        /* where infection radii are measured from */
     double *klookup, *khires;
     float *klookup_f, *khires_f;   /* the kernel tables rounded to FP32 (the spatial acceptance test) */
     /* dynamic per person */
@@ -353,6 +355,12 @@ static double dist2_hh(const cs_cpu_ctx* c, int32_t ha, int32_t hb)
     float dx = c->hh_x[ha] - c->hh_x[hb];
     float dy = c->hh_y[ha] - c->hh_y[hb];
     return periodic_xy(&c->P, fabs(dx), fabs(dy));
+}
+
+/* dist2_raw (src/Dist.cpp:163-170) from household ha to a point, in double. */
+static double dist2_hh_pt(const cs_cpu_ctx* c, int32_t ha, double bx, double by)
+{
+    return cs_cpu_dist2_raw(&c->P, c->hh_x[ha], c->hh_y[ha], bx, by);
 }
 
 /* dist2_cc_min (src/Dist.cpp:78-144) on grid cell indices. */
@@ -667,6 +675,8 @@ int cs_cpu_create(const cs_population* pop, const cs_params* params, cs_cpu_ctx*
     if (!pop || !params || !out) return CS_E_ARG;
     cs_cpu_ctx* c = (cs_cpu_ctx*)calloc(1, sizeof(cs_cpu_ctx));
     c->P = *params;
+    c->rad_origin[0] = params->LocationInitialInfection[0];
+    c->rad_origin[1] = params->LocationInitialInfection[1];
     c->N = pop->n_people; c->NH = pop->n_households; c->NC = pop->n_cells; c->NM = pop->n_mcells;
     c->NPT = pop->num_place_types; c->NAD = pop->n_adunits;
     if (c->NPT > CS_MAX_PLACE_TYPES || c->NPT != params->NumPlaceTypes) { *out = c; return fail(c, CS_E_ARG, "place type count mismatch"); }
@@ -895,6 +905,14 @@ static void do_infect(cs_cpu_ctx* c, int p, double t, int ts, int32_t infector, 
     c->S[cell]--; c->L[cell]++;
     c->mark[c->cell_start[cell] + c->listpos[p]] = 1;
     c->C.cumI++;
+    if (infector != -2) {   /* a seed's radius is 0: the origin moved to it */
+        const double x = (double)c->hh_x[c->hh[p]] - c->rad_origin[0], y = (double)c->hh_y[c->hh[p]] - c->rad_origin[1];
+        const double r2 = x * x + y * y;
+        int64_t bits;
+        c->C.sumRad2_q += (int64_t)(r2 * 4294967296.0);
+        memcpy(&bits, &r2, sizeof bits);
+        if (bits > c->C.maxRad2_bits) c->C.maxRad2_bits = bits;
+    }
     c->C.cumItype[infect_type % CS_INFECT_TYPE_MASK]++;
     c->C.cumIa[age_group(c, p)]++;
     c->C.cumI_keyworker[(c->pflags[p] & CS_PF_KEYWORKER) ? 1 : 0]++;
@@ -945,6 +963,11 @@ int cs_cpu_seed_infections(cs_cpu_ctx* c, double t, const int32_t* people, int n
         if (c->inf[p] != CS_INF_SUSCEPTIBLE) continue;
         do_infect(c, p, t, ts, -2, (int16_t)(CS_INFECT_TYPE_MASK - 1));
         touched[nt++] = cell_of(c, p);
+    }
+    /* radii are measured from the last seed's household (src/CovidSim.cpp:1358-1359) */
+    if (n > 0) {
+        c->rad_origin[0] = (double)c->hh_x[c->hh[people[n - 1]]];
+        c->rad_origin[1] = (double)c->hh_y[c->hh[people[n - 1]]];
     }
     /* unique cells */
     for (int i = 0; i < nt; i++)
@@ -1089,7 +1112,10 @@ static void place_candidates(cs_cpu_ctx* c, int i, int pt, int link, double Pinf
         if ((pt == P->CareHomePlaceType) && ((!is_ch(c, i)) || (!is_ch(c, m)))) sc *= P->CareHomeWorkerGroupScaling;
         if (c->inf[m] == CS_INF_SUSCEPTIBLE && !host_absent(c, m, ts)) {
             sc *= calc_person_susc(c, m, i) * p / p;
-            if (moverest_differs(c, c->mcell[m], mc_place)) sc *= P->MoveRestrEffect;
+            if (c->blanket) {
+                if (dist2_hh_pt(c, c->hh[m], pl->x[link], pl->y[link]) > P->MoveRestrRadius2) sc *= P->MoveRestrEffect;
+            } else if (moverest_differs(c, c->mcell[m], mc_place))
+                sc *= P->MoveRestrEffect;
             if ((sc == 1) || (stream_next(&s) < sc)) claim(c, m, i, between ? 2 + pt + CS_MAX_PLACE_TYPES : 2 + pt);
         }
     }
@@ -1153,7 +1179,10 @@ static void spatial_contact(cs_cpu_ctx* c, int i, int ci, int j, int closed_i, i
         if (slot < c->S[m]) {
             ss *= calc_person_susc(c, p, i);
             ss *= P->WAIFW_Matrix_SpatialOnly[age_group(c, p)][age_group(c, i)];
-            if (moverest_differs(c, c->mcell[p], c->mcell[i])) ss *= P->MoveRestrEffect;
+            if (c->blanket) {
+                if (dist2_hh_pt(c, hi_, c->hh_x[c->hh[p]], c->hh_y[c->hh[p]]) > P->MoveRestrRadius2) ss *= P->MoveRestrEffect;
+            } else if (moverest_differs(c, c->mcell[p], c->mcell[i]))
+                ss *= P->MoveRestrEffect;
             if ((!closed_i) && host_absent(c, p, ts)) {
                 int f = 0;
                 for (int pt = 0; (pt < c->NPT) && (!f); pt++)
@@ -1198,7 +1227,10 @@ static void infector_pass(cs_cpu_ctx* c, int i, int ci, double hh_beta, double s
             if (link < 0) continue;
             double PI = fp * seas * calc_place_inf(c, i, pt, ts);
             int mc_place = c->pl[pt].mcell[link];
-            if (moverest_differs(c, c->mcell[i], mc_place)) PI *= P->MoveRestrEffect;
+            if (c->blanket) {
+                if (dist2_hh_pt(c, h, c->pl[pt].x[link], c->pl[pt].y[link]) > P->MoveRestrRadius2) PI *= P->MoveRestrEffect;
+            } else if (moverest_differs(c, c->mcell[i], mc_place))
+                PI *= P->MoveRestrEffect;
             if (pt != P->HotelPlaceType) {
                 double p1 = PI;
                 if (p1 > 1) p1 = 1;
@@ -1241,6 +1273,7 @@ int cs_cpu_infect_sweep(cs_cpu_ctx* c, double t, int run)
     int ts = (int)(uint16_t)(P->TimeStepsPerDay * t);
     double fp = P->ModelTimeStep / (1 - P->FalsePositiveRate);
     double seas = P->Seasonality;
+    c->blanket = P->DoBlanketMoveRestr && (t >= P->MoveRestrTimeStart) && (t < P->MoveRestrTimeStart + P->MoveRestrDuration);
     double sp_beta = (P->DoSpatial ? seas * fp * P->LocalBeta : 0.0);
     double hh_beta = P->DoHouseholds ? seas * fp * P->HouseholdTrans : 0;
     for (int ci = 0; ci < c->NC; ci++) {
@@ -1796,6 +1829,8 @@ int cs_cpu_get_counters(cs_cpu_ctx* c, cs_counters* out)
 int cs_cpu_upload_state(cs_cpu_ctx* c, uint64_t seed, const cs_state_view* v)
 {
     size_t N = (size_t)c->N, NC = (size_t)c->NC;
+    c->rad_origin[0] = c->P.LocationInitialInfection[0];
+    c->rad_origin[1] = c->P.LocationInitialInfection[1];
 #define CPI(src, dst, n) do { if (v->src) memcpy(c->dst, v->src, sizeof(*c->dst) * (n)); } while (0)
     CPI(inf, inf, N); CPI(severity, sev, N); CPI(flags, dflags, N);
     CPI(infection_time, infection_time, N); CPI(latent_time, latent_time, N);

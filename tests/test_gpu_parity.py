@@ -111,3 +111,17 @@ def test_parity_graph_replayed_steps():
     _compare(pop, g, o, "second run")
     g.close()
     o.close()
+
+
+def test_parity_blanket_movement_restrictions():
+    """Blanket movement restrictions from day 8 for 20 days: the place, place-group
+    and spatial passes scale contacts longer than the radius (src/Sweep.cpp:397-403,
+    516-521, 823-827); the radius counters compare as well."""
+    pop, P, lk, hr = tiny_world()
+    Q = type(P).from_buffer_copy(P)
+    Q.DoBlanketMoveRestr = 1
+    Q.MoveRestrTimeStart, Q.MoveRestrDuration = 8.0, 20.0
+    Q.MoveRestrRadius2 = 1500.0 ** 2
+    Q.MoveRestrEffect = 0.25
+    c = _run_pair((pop, Q, lk, hr), seed=707, steps=160, check_every=8)
+    assert c.cumI > 200 and c.sumRad2_q > 0

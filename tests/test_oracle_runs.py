@@ -103,3 +103,39 @@ def test_spatial_bound_dominates_kernel_utm():
 
 def test_spatial_bound_dominates_kernel_planar():
     _bound_dominates(tiny_world(utm=0))
+
+
+def test_infection_radii_follow_their_definition():
+    """The oracle's radius counters against the definition restated here: every
+    infection but a seed's adds (int)(r^2 * 2^32), r the distance in degrees from
+    its household to the last seed's (src/Update.cpp:116-127, src/CovidSim.cpp:
+    1358-1359), and the largest r^2 is kept."""
+    pop, P, lk, hr = tiny_world()
+    s, be, out = _run(21, 120)
+    snap = snapshot(be, pop)
+    seeds = s.choose_seeds(21, 20)
+    o = np.array([pop.hh_x[pop.person_hh[seeds[-1]]], pop.hh_y[pop.person_hh[seeds[-1]]]], np.float64)
+    inf = np.nonzero((snap["inf"] != 0) & (snap["infector"] != -2))[0]
+    h = pop.person_hh[inf]
+    r2 = (pop.hh_x[h].astype(np.float64) - o[0]) ** 2 + (pop.hh_y[h].astype(np.float64) - o[1]) ** 2
+    c = be.counters()
+    assert len(inf) > 300
+    assert c.sumRad2_q == int(np.sum((r2 * 4294967296.0).astype(np.int64)))
+    assert np.array([c.maxRad2_bits], np.int64).view(np.float64)[0] == r2.max()
+
+
+def test_blanket_movement_restrictions_cut_long_contacts():
+    """Blanket movement restrictions (src/Sweep.cpp:300-301): with the effect 0 and a
+    radius of a few hundred metres, contacts beyond the radius cannot infect while
+    the restriction lasts, so the epidemic grows more slowly than without it and
+    the infections in the window stay near their infectors."""
+    pop, P, lk, hr = tiny_world()
+    Q = type(P).from_buffer_copy(P)
+    Q.DoBlanketMoveRestr = 1
+    Q.MoveRestrTimeStart, Q.MoveRestrDuration = 10.0, 20.0
+    Q.MoveRestrRadius2 = 500.0 ** 2          # dist2 is in square metres
+    Q.MoveRestrEffect = 0.0
+    _, be0, a = _run(31, 120, world=(pop, P, lk, hr))
+    _, be1, b = _run(31, 120, world=(pop, Q, lk, hr))
+    assert a[39] == b[39]                    # identical until the restriction starts
+    assert b[-1][5] < 0.8 * a[-1][5]         # fewer infections by day 30
