@@ -672,11 +672,15 @@ __global__ void k_take(int npl, int32_t* __restrict__ rem, int32_t* __restrict__
 __global__ void k_member_keys(uint64_t seed, int t, int n_att, const int32_t* __restrict__ list,
                               const int32_t* __restrict__ link, uint64_t* __restrict__ keys,
                               int32_t* __restrict__ vals, int32_t* __restrict__ mcount,
-                              int32_t* __restrict__ person_place)
+                              int32_t* __restrict__ person_place, unsigned long long* err)
 {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n_att) return;
     const int p = list[a], pl = link[a];
+    if (pl < 0) {   // the last round reaches every place, so this does not happen; counted if it does
+        atomicAdd(err, 1ull);
+        return;
+    }
     const uint32_t h = (uint32_t)rand64(seed, CS_RNG_SETUP_SHUFFLE, 0, (uint32_t)p, (uint32_t)t);
     keys[a] = ((uint64_t)(uint32_t)pl << 32) | h;
     vals[a] = p;
@@ -994,8 +998,27 @@ int run_setup(cs_setup* s, const cs_setup_spec& S, const cs_params& P)
     SALLOC(s->person_age, N);
     SLAUNCH(k_ages, nblk(N), kT, seed, N, ar, s->person_age);
 
-    // 6. places
+    // 6. places.  The spec's kernel tables are host arrays: each distinct one is
+    // copied to the device once.
     const int npt = S.num_place_types;
+    const size_t ktab = (size_t)P.kernel_size + 1;
+    const double* klk[CS_MAX_PLACE_TYPES] = {};
+    const double* khr[CS_MAX_PLACE_TYPES] = {};
+    for (int t = 0; t < npt; t++) {
+        for (int u = 0; u < t && !klk[t]; u++)
+            if (S.pt[u].kernel_lookup == S.pt[t].kernel_lookup && S.pt[u].kernel_hi_res == S.pt[t].kernel_hi_res) {
+                klk[t] = klk[u];
+                khr[t] = khr[u];
+            }
+        if (klk[t]) continue;
+        double *a, *b;
+        SALLOC(a, ktab);
+        SALLOC(b, ktab);
+        SK(cudaMemcpyAsync(a, S.pt[t].kernel_lookup, sizeof(double) * ktab, cudaMemcpyHostToDevice, s->stream));
+        SK(cudaMemcpyAsync(b, S.pt[t].kernel_hi_res, sizeof(double) * ktab, cudaMemcpyHostToDevice, s->stream));
+        klk[t] = a;
+        khr[t] = b;
+    }
     SALLOC(s->person_place, (long long)std::max(npt, 1) * N);
     SALLOC(s->person_group, (long long)std::max(npt, 1) * N);
     SLAUNCH(k_fill_i32, nblk((long long)npt * N), kT, s->person_place, (long long)npt * N, -1);
@@ -1081,9 +1104,8 @@ int run_setup(cs_setup* s, const cs_setup_spec& S, const cs_params& P)
         SK(cudaMemsetAsync(forced, 0, sizeof(int32_t), s->stream));
         for (int rd = 0; rd <= S.rounds; rd++) {
             const int free_round = rd == S.rounds;
-            SLAUNCH(k_propose, nblk(n_att, 128), 128, seed, t, rd, free_round, n_att, T.nearest, B, Pd,
-                    T.kernel_lookup, T.kernel_hi_res, list, s->person_hh, s->hh_x, s->hh_y, O.x, O.y, bstart, items,
-                    rem, link, prop);
+            SLAUNCH(k_propose, nblk(n_att, 128), 128, seed, t, rd, free_round, n_att, T.nearest, B, Pd, klk[t],
+                    khr[t], list, s->person_hh, s->hh_x, s->hh_y, O.x, O.y, bstart, items, rem, link, prop);
             SLAUNCH(k_count_props, nblk(n_att), kT, n_att, prop, nprop);
             SLAUNCH(k_accept, nblk(n_att), kT, seed, t, rd, free_round, n_att, list, prop, nprop, rem, link, taken,
                     forced);
@@ -1101,7 +1123,7 @@ int run_setup(cs_setup* s, const cs_setup_spec& S, const cs_params& P)
         SALLOC(O.group_ofs, npl + 1);
         SK(cudaMemsetAsync(mcount, 0, sizeof(int32_t) * npl, s->stream));
         SLAUNCH(k_member_keys, nblk(n_att), kT, seed, t, n_att, list, link, keys, vals, mcount,
-                s->person_place + (long long)t * N);
+                s->person_place + (long long)t * N, err);
         int bits = 32;
         while (bits < 64 && ((uint64_t)npl >> (bits - 32)) != 0) bits++;
         r = radix_sort(s, keys, vals, n_att, bits);

@@ -169,7 +169,7 @@ struct DevPop {
     // per-step scratch
     unsigned long long* claim; // [N], UINT64_MAX when unclaimed
     int32_t* queue;            // [N] newly infected people
-    int32_t* counts;           // [8] device-side sizes (see kCnt*)
+    int32_t* counts;           // [kCntN] device-side sizes (see kCnt*)
     int32_t* touched;          // [NC] cells whose lists change this phase
     uint8_t* cell_flag;        // [NC]
     int32_t* act;              // [N] active people (infectors / latent+infectious)
@@ -188,10 +188,15 @@ struct DevPop {
     uint32_t* carer_win;       // [NH]
     int32_t* carer_list;       // [NH]
     double* rad_origin;        // [2] where infection radii are measured from
+    uint32_t* fc_flag;         // [N/32 + 1] people with a false-positive entry this step
+    int32_t* fc_queue;         // [N] those people, once each
     cs_counters* C;
 };
 
-enum { kCntQueue = 0, kCntTouched = 1, kCntHH = 2, kCntAct = 3, kCntContacts = 4, kCntPlaceWork = 5, kCntEvents = 6,
-       kCntCarer = 7, kCntN = 8 };
+// kCntHH is last: the infect sweep zeroes the counters before it (kCntN - 1 of
+// them) and leaves the household list, which its false cases may have filled, to
+// the incub sweep's household pass.
+enum { kCntQueue = 0, kCntTouched = 1, kCntAct = 2, kCntContacts = 3, kCntPlaceWork = 4, kCntEvents = 5,
+       kCntCarer = 6, kCntFalse = 7, kCntHH = 8, kCntN = 9 };
 
 }  // namespace csb

@@ -847,14 +847,27 @@ __global__ void k_build_active(DevPop d, int mode) { k_build_active_body(d, mode
 __global__ void k_build_active_multi(const DevPop* __restrict__ pops, int mode) { k_build_active_body(pops[blockIdx.y], mode); }
 
 // =============================================================== InfectSweep
-__device__ __forceinline__ void claim_infection(const DevPop& d, int person, int infector, int code)
+typedef DevStep StepScalars;
+
+// AddInfections (src/Sweep.cpp:2031-2065): with probability FalsePositiveRate the
+// entry is a false positive (DoFalseCase for the person) instead of an infection.
+// The draw is keyed by (infector, infectee, infection type), one per entry.
+__device__ __forceinline__ void claim_infection(const DevPop& d, const cs_params& P, const StepScalars& st, int person,
+                                                int infector, int code)
 {
+    if (P.FalsePositiveRate > 0) {
+        Stream s(st.seed, CS_RNG_FALSE_POSITIVE, (uint32_t)st.ts, (uint32_t)infector, (uint32_t)person);
+        s.block = (uint32_t)code;
+        if (s.next() < P.FalsePositiveRate) {
+            const uint32_t bit = 1u << (person & 31);
+            if (!(atomicOr(d.fc_flag + (person >> 5), bit) & bit)) d.fc_queue[append(d.counts + kCntFalse)] = person;
+            return;
+        }
+    }
     unsigned long long key = ((unsigned long long)(uint32_t)infector << 8) | (unsigned long long)code;
     unsigned long long old = atomicMin(d.claim + person, key);
     if (old == ~0ull) d.queue[append(d.counts + kCntQueue)] = person;
 }
-
-typedef DevStep StepScalars;
 
 // The step's scalars from the parameters, on the device (src/Sweep.cpp:292-301).
 __device__ __forceinline__ void k_set_step_body(const DevPop& d, double t, unsigned long long seed)
@@ -920,7 +933,7 @@ __device__ void place_candidates(const DevPop& d, const cs_params& P, const Step
                 if (dist2_hh_pt(d, P, hm.hh, pl.x[link], pl.y[link]) > P.MoveRestrRadius2) sc *= P.MoveRestrEffect;
             } else if (moverest_differs(d, hm.mcell, mc_place))
                 sc *= P.MoveRestrEffect;
-            if ((sc == 1) || (s.next() < sc)) claim_infection(d, m, i, between ? 2 + pt + CS_MAX_PLACE_TYPES : 2 + pt);
+            if ((sc == 1) || (s.next() < sc)) claim_infection(d, P, st, m, i, between ? 2 + pt + CS_MAX_PLACE_TYPES : 2 + pt);
         }
     }
     cnt_add_warp(CSB_CTR(work_place_candidates), ncand);
@@ -968,7 +981,7 @@ __device__ __forceinline__ void k_infector_hh_spatial_body(const DevPop& d)
                     PersonHot hm = d.hot[m];
                     if (hm.inf == CS_INF_SUSCEPTIBLE) {
                         double foi = HI * calc_house_susc(d, hm, iag, P);
-                        if (s.next() < foi) claim_infection(d, m, i, 1);
+                        if (s.next() < foi) claim_infection(d, P, st, m, i, 1);
                     }
                 }
             }
@@ -1147,7 +1160,7 @@ __device__ __forceinline__ void k_spatial_body(const DevPop& d)
                     if (f) ss *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL];
                 }
                 if ((ss == 1) || (s.next() < ss))
-                    if (hp.inf == CS_INF_SUSCEPTIBLE) claim_infection(d, p, i, 2 + 2 * CS_MAX_PLACE_TYPES);
+                    if (hp.inf == CS_INF_SUSCEPTIBLE) claim_infection(d, P, st, p, i, 2 + 2 * CS_MAX_PLACE_TYPES);
             }
         }
     }
@@ -1565,6 +1578,47 @@ __global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d) { k_incub_sca
 __global__ void __launch_bounds__(kThreads) k_incub_scan_multi(const DevPop* __restrict__ pops) { k_incub_scan_body(pops[blockIdx.y]); }
 
 // cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
+// DoFalseCase (src/Update.cpp:896-905) for every person with a false-positive
+// entry this step, after the step's infections: detected with probability
+// ControlPropCasesId (counted once the detected cases at the last sample reached
+// the alert threshold) and then treated as a detected case; every false case is
+// counted.  A person the step did not infect takes the false entry's labels
+// (infector and infection type -1, as the reference's queue drain writes them,
+// src/Sweep.cpp:866-869); an infected one keeps the infection's.
+__device__ __forceinline__ void k_apply_false_cases_body(const DevPop& d)
+{
+    const cs_params& P = *d.P;
+    const double t = d.step->t;
+    const int ts = d.step->ts;
+    const uint64_t seed = d.step->seed;
+    const DevIv iv = *d.iv;
+    const int n = d.counts[kCntFalse];
+    if (blockIdx.x * blockDim.x >= n) return;
+    stage_begin(d.C, false);
+    long long nfc = 0, ndc = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int p = d.fc_queue[q];
+        d.fc_flag[p >> 5] = 0;   // every flagged person of the word is in the queue
+        PersonHot h = d.hot[p];
+        if (h.inf == CS_INF_SUSCEPTIBLE) {
+            d.infector[p] = -1;
+            d.infect_type[p] = -1;
+        }
+        Stream s(seed, CS_RNG_FALSE_CASE, (uint32_t)ts, (uint32_t)p, 0);
+        if ((P.ControlPropCasesId == 1) || (s.next() < P.ControlPropCasesId)) {
+            if (P.cumDC_at_sample >= P.CaseOrDeathThresholdBeforeAlert) ndc++;
+            do_detected_case(d, P, iv, p, h, t, ts, seed);
+            d.hot[p] = h;
+        }
+        nfc++;
+    }
+    cnt_add_warp(CSB_CTR(cumFC), nfc);
+    cnt_add_warp(CSB_CTR(cumDC), ndc);
+    stage_flush(d.C, false);
+}
+__global__ void k_apply_false_cases(DevPop d) { k_apply_false_cases_body(d); }
+__global__ void k_apply_false_cases_multi(const DevPop* __restrict__ pops) { k_apply_false_cases_body(pops[blockIdx.y]); }
+
 __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
@@ -2221,6 +2275,8 @@ static int alloc_dynamic(cs_gpu_ctx* c)
     d.t_src = nullptr;
     { cs_counters* t; AL(t, 1); c->dC = t; d.C = t; CK(cudaMemsetAsync(t, 0, sizeof(cs_counters), c->stream)); }
     { double* t; UP(t, params->LocationInitialInfection, 2); d.rad_origin = t; }
+    AL(d.fc_flag, N / 32 + 1); AL(d.fc_queue, N);
+    CK(cudaMemsetAsync(d.fc_flag, 0, sizeof(uint32_t) * (N / 32 + 1), c->stream));
 #undef UP
 #undef AL
     CK(cudaStreamSynchronize(c->stream));   // the parameter and window copies came from the stack
@@ -2467,6 +2523,14 @@ int cs_gpu_set_params(cs_gpu_ctx* c, const cs_params* params)
     if (geometry && c->stat.use_count() > 1)
         return set_err(c, CS_E_UNSUPPORTED, "set_params may not change the geometry of a population shared by replicas");
     drop_day_graph(c);   // captured with this kernel-row table and steps per day
+    if ((params->FalsePositiveRate > 0) != (o.FalsePositiveRate > 0) && c->graph_exec) {
+        // the captured step has the false-case pass only while false positives are on
+        CK(cudaStreamSynchronize(c->stream));
+        cudaGraphExecDestroy(c->graph_exec);
+        cudaGraphDestroy(c->graph);
+        c->graph_exec = nullptr;
+        c->graph = nullptr;
+    }
     c->hp = *params;
     CK(cudaMemcpyAsync(c->dP, params, sizeof(cs_params), cudaMemcpyHostToDevice, c->stream));
     if (geometry) {   // the kernel rows and the n-weighted denominators depend on it
@@ -2628,8 +2692,10 @@ static int apply_queue(cs_gpu_ctx* c)
     DevPop& d = c->d;
     LAUNCH(k_apply_infections, c->grid, kThreads, d);
     LAUNCH(k_partition_S, c->grid, kThreads, d);
-    // every sweep leaves all list counters at zero for the next one
-    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
+    if (c->hp.FalsePositiveRate > 0) LAUNCH(k_apply_false_cases, c->grid, kThreads, d);
+    // every sweep leaves its list counters at zero for the next one; the household
+    // list (last) is the incub sweep's
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * (kCntN - 1), c->stream));
     return CS_OK;
 }
 
@@ -3028,9 +3094,9 @@ int cs_gpu_run(cs_gpu_ctx* c, int days, const cs_run_policy* policy, cs_counters
 }
 
 // List counters of every member of a batch back to zero (the end-of-sweep reset).
-__global__ void k_zero_counts_multi(const DevPop* __restrict__ pops)
+__global__ void k_zero_counts_multi(const DevPop* __restrict__ pops, int n)
 {
-    if (threadIdx.x < kCntN) pops[blockIdx.x].counts[threadIdx.x] = 0;
+    if (threadIdx.x < n) pops[blockIdx.x].counts[threadIdx.x] = 0;
 }
 
 // ------------------------------------------------------------ batched steps
@@ -3151,13 +3217,16 @@ static int batch_enqueue(cs_gpu_batch* b, const DevPop* pops)
     }
     BLAUNCH(k_apply_infections_multi, g, kThreads, pops);
     BLAUNCH(k_partition_S_multi, g, kThreads, pops);
-    BLAUNCH(k_zero_counts_multi, R, 32, pops);
+    bool fpr = false;
+    for (const cs_gpu_ctx* m : b->members) fpr |= m->hp.FalsePositiveRate > 0;
+    if (fpr) BLAUNCH(k_apply_false_cases_multi, g, kThreads, pops);
+    BLAUNCH(k_zero_counts_multi, R, 32, pops, (int)(kCntN - 1));   // the household list is the incub sweep's
     BLAUNCH(k_build_active_multi, g, kThreads, pops, 1);
     BLAUNCH(k_incub_scan_multi, g, kThreads, pops);
     BLAUNCH(k_incub_events_multi, g, kThreads, pops);
     BLAUNCH(k_partition_LI_multi, g, kThreads, pops);
     BLAUNCH(k_household_after_multi, g, kThreads, pops);
-    BLAUNCH(k_zero_counts_multi, R, 32, pops);
+    BLAUNCH(k_zero_counts_multi, R, 32, pops, (int)kCntN);
     return CS_OK;
 }
 

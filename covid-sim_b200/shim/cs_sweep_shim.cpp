@@ -168,6 +168,8 @@ cs_params params_from_reference()
     p.PlaceTypeNoAirNum = P.PlaceTypeNoAirNum; p.IncludeStepDownToDeath = P.IncludeStepDownToDeath;
     p.CaseAbsentChildAgeCutoff = P.CaseAbsentChildAgeCutoff; p.DoHQretrigger = P.DoHQretrigger;
     p.LocalBeta = P.LocalBeta; p.HouseholdTrans = P.HouseholdTrans; p.FalsePositiveRate = P.FalsePositiveRate;
+    p.CaseOrDeathThresholdBeforeAlert = P.CaseOrDeathThresholdBeforeAlert;
+    p.cumDC_at_sample = P.FalsePositiveRate > 0 ? State.cumDC : 0;   // RecordSample's, read by DoFalseCase
     p.Seasonality = 1.0;
     for (int i = 0; i < MAX_HOUSEHOLD_SIZE; i++) p.HouseholdDenomLookup[i] = P.HouseholdDenomLookup[i];
     for (int i = 0; i < MAX_INFECTIOUS_STEPS; i++) p.infectiousness[i] = P.infectiousness[i];
@@ -250,12 +252,12 @@ void unsupported_features()
 {
     if (P.DoDigitalContactTracing) ERR_CRITICAL("GPU sweep: digital contact tracing is not supported\n");
     if (P.DoAirports) ERR_CRITICAL("GPU sweep: airports / travel are not supported\n");
-    if (P.FalsePositiveRate > 0) ERR_CRITICAL("GPU sweep: false-positive cases are not supported\n");
     if (P.DoHolidays && P.NumHolidays > 0) ERR_CRITICAL("GPU sweep: holidays are not supported\n");
     if (P.DoInterventionDelaysByAdUnit) ERR_CRITICAL("GPU sweep: intervention delays by admin unit are not supported\n");
     if (P.InfectionImportRate1 > 0 || P.InfectionImportRate2 > 0 || P.DurImportTimeProfile > 0)
         ERR_CRITICAL("GPU sweep: importation of infections during a run is not supported\n");
-    if (P.FalsePositivePerCapitaIncidence > 0) ERR_CRITICAL("GPU sweep: false-positive cases are not supported\n");
+    if (P.FalsePositivePerCapitaIncidence > 0)
+        ERR_CRITICAL("GPU sweep: false-positive cases drawn at a per-capita incidence are not supported\n");
     if (P.DoSI) ERR_CRITICAL("GPU sweep: the SI model (no IncubRecoverySweep) is not supported\n");
     if (P.DoAdUnits && P.DoAdminTriggers && P.NumAdunits > CS_MAX_ADUNITS)
         ERR_CRITICAL_FMT("GPU sweep: admin-unit triggers over more than %d admin units are not supported\n", CS_MAX_ADUNITS);

@@ -114,6 +114,8 @@ extern "C" {
 #define CS_RNG_HQ 10              /* entity household                     */
 #define CS_RNG_RUN_INIT 11        /* entity person, timestep 0            */
 #define CS_RNG_PLACE_INIT 12      /* entity place, sub place type         */
+#define CS_RNG_FALSE_POSITIVE 13  /* entity infector, sub infectee, block infection type */
+#define CS_RNG_FALSE_CASE 14      /* entity person                        */
 /* Population set-up (cs_gpu_setup_run); timestep field = round where noted. */
 #define CS_RNG_SETUP_DENSITY 20   /* entity microcell grid index          */
 #define CS_RNG_SETUP_BLOB 21      /* entity blob                          */
@@ -171,6 +173,10 @@ typedef struct cs_params {
     int32_t IncludeStepDownToDeath, CaseAbsentChildAgeCutoff, DoHQretrigger, _pad0;
     /* transmission */
     double LocalBeta, HouseholdTrans, FalsePositiveRate, Seasonality;
+    /* DoFalseCase counts a false case as detected only once the detected cases at the
+     * last sample (State.cumDC) reached P.CaseOrDeathThresholdBeforeAlert
+     * (src/Update.cpp:901); the host refreshes cumDC_at_sample at each sample */
+    int32_t CaseOrDeathThresholdBeforeAlert, cumDC_at_sample;
     double HouseholdDenomLookup[CS_MAX_HOUSEHOLD_SIZE];
     double infectiousness[CS_MAX_INFECTIOUS_STEPS];     /* P.infectiousness[] */
     double PlaceTypeTrans[CS_MAX_PLACE_TYPES];

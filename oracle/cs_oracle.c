@@ -63,6 +63,8 @@ struct cs_cpu_ctx {
     float *hh_x, *hh_y;
     place_arrays pl[CS_MAX_PLACE_TYPES];
     int blanket;                 /* blanket movement restrictions in place this step */
+    int cur_ts;                  /* the infect sweep's timestep (false-positive draws) */
+    uint8_t* fc;                 /* [N] a false-positive entry this step */
     double rad_origin[2];        /* where infection radii are measured from */
     double *klookup, *khires;
     float *klookup_f, *khires_f;   /* the kernel tables rounded to FP32 (the spatial acceptance test) */
@@ -730,6 +732,7 @@ int cs_cpu_create(const cs_population* pop, const cs_params* params, cs_cpu_ctx*
     ALLOC(c->socdist, c->NM, uint8_t); ALLOC(c->moverest, c->NM, uint8_t);
     ALLOC(c->claim, c->N, uint64_t);
     ALLOC(c->hh_carer, c->NH, uint8_t); ALLOC(c->hh_hq, c->NH, uint8_t);
+    ALLOC(c->fc, c->N, uint8_t);
     ALLOC(c->carer_start, c->NH, uint16_t); ALLOC(c->carer_stop, c->NH, uint16_t);
     for (int h = 0; h < c->NH; h++) c->carer_start[h] = 0xFFFF;
     ALLOC(c->ci_start, c->NAD, double); ALLOC(c->hq_start, c->NAD, double);
@@ -752,7 +755,7 @@ void cs_cpu_destroy(cs_cpu_ctx* c)
                     c->R, c->D, c->S0, c->tot_prob, c->slots, c->mark, c->socdist, c->moverest, c->claim,
                     c->hh_carer, c->hh_hq, c->cell_block, c->block_cell_ofs, c->block_cells, c->block_cum,
                     c->block_S0, c->block_row_cum, c->ci_start, c->hq_start, c->carer_start, c->carer_stop,
-                    c->klookup_f, c->khires_f, c->bound_c};
+                    c->klookup_f, c->khires_f, c->bound_c, c->fc};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     for (int t = 0; t < c->NPT; t++) {
         place_arrays* p = &c->pl[t];
@@ -891,6 +894,7 @@ int cs_cpu_update_probs(cs_cpu_ctx* c, int do_place)
 
 /* ------------------------------------------------------------ run start -- */
 static void partition_block(cs_cpu_ctx* c, int cell, int b0, int n, int* removed_out);
+static void do_detected_case(cs_cpu_ctx* c, int p, double t, int ts);
 
 /* ToInfected + DoInfect (src/Update.cpp:100-195, 1531-1538) for one person, without
  * the cell-list move (done per cell afterwards). */
@@ -1068,8 +1072,20 @@ static void partition_block(cs_cpu_ctx* c, int cell, int b0, int n, int* removed
 }
 
 /* ------------------------------------------------------------- InfectSweep -- */
+/* AddInfections (src/Sweep.cpp:2031-2065): with probability FalsePositiveRate the
+ * entry is a false positive (DoFalseCase for the person) instead of an infection,
+ * one draw per entry keyed by (infector, infectee, infection type). */
 static inline void claim(cs_cpu_ctx* c, int person, int infector, int code)
 {
+    if (c->P.FalsePositiveRate > 0) {
+        stream s;
+        stream_init(&s, c->seed, CS_RNG_FALSE_POSITIVE, (uint32_t)c->cur_ts, (uint32_t)infector, (uint32_t)person);
+        s.block = (uint32_t)code;
+        if (stream_next(&s) < c->P.FalsePositiveRate) {
+            c->fc[person] = 1;
+            return;
+        }
+    }
     uint64_t key = ((uint64_t)(uint32_t)infector << 8) | (uint64_t)code;
     if (key < c->claim[person]) c->claim[person] = key;
 }
@@ -1269,8 +1285,8 @@ int cs_cpu_infect_sweep(cs_cpu_ctx* c, double t, int run)
     (void)run;
     const cs_params* P = &c->P;
     if (!c->run_started) return fail(c, CS_E_STATE, "infect sweep before begin_run");
-    if (P->FalsePositiveRate != 0) return fail(c, CS_E_UNSUPPORTED, "FalsePositiveRate must be 0");
     int ts = (int)(uint16_t)(P->TimeStepsPerDay * t);
+    c->cur_ts = ts;
     double fp = P->ModelTimeStep / (1 - P->FalsePositiveRate);
     double seas = P->Seasonality;
     c->blanket = P->DoBlanketMoveRestr && (t >= P->MoveRestrTimeStart) && (t < P->MoveRestrTimeStart + P->MoveRestrDuration);
@@ -1297,6 +1313,25 @@ int cs_cpu_infect_sweep(cs_cpu_ctx* c, double t, int run)
     partition_S_blocks(c, touched, nt);
     free(touched);
     free(seen);
+    /* DoFalseCase (src/Update.cpp:896-905) for every person with a false-positive
+     * entry, after the step's infections; a person the step did not infect takes
+     * the false entry's labels (src/Sweep.cpp:866-869) */
+    if (P->FalsePositiveRate > 0)
+        for (int p = 0; p < c->N; p++) {
+            if (!c->fc[p]) continue;
+            c->fc[p] = 0;
+            if (c->inf[p] == CS_INF_SUSCEPTIBLE) {
+                c->infector[p] = -1;
+                c->infect_type[p] = -1;
+            }
+            stream s;
+            stream_init(&s, c->seed, CS_RNG_FALSE_CASE, (uint32_t)ts, (uint32_t)p, 0);
+            if ((P->ControlPropCasesId == 1) || (stream_next(&s) < P->ControlPropCasesId)) {
+                if (P->cumDC_at_sample >= P->CaseOrDeathThresholdBeforeAlert) c->C.cumDC++;
+                do_detected_case(c, p, t, ts);
+            }
+            c->C.cumFC++;
+        }
     return CS_OK;
 }
 
@@ -2365,6 +2400,8 @@ static int setup_run(cs_cpu_setup* s, const cs_setup_spec* S, const cs_params* P
             /* member lists by (place, random key), then groups */
             setup_key* keys = (setup_key*)malloc(sizeof(setup_key) * (size_t)n_att);
             int32_t* mcount = (int32_t*)calloc((size_t)npl, sizeof(int32_t));
+            for (int a = 0; a < n_att; a++)
+                if (link[a] < 0) { rc = setup_fail(s, CS_E_OVERFLOW, "setup: an attendee has no place"); goto done; }
             for (int a = 0; a < n_att; a++) {
                 const int p = list[a];
                 const uint32_t hsh = (uint32_t)setup_rand64(seed, CS_RNG_SETUP_SHUFFLE, 0, (uint32_t)p, (uint32_t)t);

@@ -125,3 +125,16 @@ def test_parity_blanket_movement_restrictions():
     Q.MoveRestrEffect = 0.25
     c = _run_pair((pop, Q, lk, hr), seed=707, steps=160, check_every=8)
     assert c.cumI > 200 and c.sumRad2_q > 0
+
+
+def test_parity_false_positives_with_interventions():
+    """False positives (AddInfections' false branch and DoFalseCase, src/Sweep.cpp:
+    2046, src/Update.cpp:896-905) with case isolation and household quarantine on
+    from day 10: false cases are detected in the infect sweep, and the households
+    they quarantine are handled by the incub sweep's household pass."""
+    pop, P, lk, hr = tiny_world()
+    Q = type(P).from_buffer_copy(P)
+    Q.FalsePositiveRate = 0.2
+    Q.ControlPropCasesId = 0.8
+    c = _run_pair((pop, Q, lk, hr), seed=808, steps=160, check_every=8, policy_day=10)
+    assert c.cumFC > 50 and c.cumHQ > 0

@@ -139,3 +139,22 @@ def test_blanket_movement_restrictions_cut_long_contacts():
     _, be1, b = _run(31, 120, world=(pop, Q, lk, hr))
     assert a[39] == b[39]                    # identical until the restriction starts
     assert b[-1][5] < 0.8 * a[-1][5]         # fewer infections by day 30
+
+
+def test_false_positives_are_counted_and_detected():
+    """False positives (src/Sweep.cpp:2046, src/Update.cpp:896-905): a fraction of
+    the entries that would infect become false cases instead, every one counted in
+    cumFC and, with ControlPropCasesId 1, detected (cumDC) and so isolated when case
+    isolation is on; the infections fall by about that fraction."""
+    pop, P, lk, hr = tiny_world()
+    Q = type(P).from_buffer_copy(P)
+    Q.FalsePositiveRate = 0.3
+    Q.ControlPropCasesId = 1.0
+    _, be0, a = _run(41, 80, world=(pop, P, lk, hr))
+    _, be1, b = _run(41, 80, world=(pop, Q, lk, hr))
+    c0, c1 = be0.counters(), be1.counters()
+    assert c0.cumFC == 0 and c1.cumFC > 100
+    assert c1.cumDC >= c1.cumFC            # every false case detected, besides the real ones
+    # the transmission rate is scaled by 1 / (1 - rate) (src/Sweep.cpp:295), so the
+    # infections per generation stay about the same
+    assert 0.5 * c0.cumI < c1.cumI < 2.0 * c0.cumI
