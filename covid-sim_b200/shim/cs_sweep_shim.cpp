@@ -125,6 +125,9 @@ struct RunTiming {
     long steps = 0;
     double infect = 0.0, incub = 0.0;
     double upload = 0.0, copyback = 0.0;   // parts of the two above
+    double wait = 0.0, scatter = 0.0, handover = 0.0;   // finer parts: the wait for the device's
+                                                        // timestep, the copy into the host's cells,
+                                                        // the hand-over after TreatSweep
 };
 std::vector<RunTiming> g_timing;
 FILE* g_dump = nullptr;
@@ -482,11 +485,13 @@ void sync_back()
 {
     cs_counters k;
     check(cs_gpu_get_sample(g_ctx, g_S.data(), g_L.data(), g_I.data(), g_R.data(), g_D.data(), &k), "cs_gpu_get_sample");
+    const double t_sc = omp_get_wtime();
 #pragma omp parallel for schedule(static)
     for (int c = 0; c < P.NumPopulatedCells; c++) {
         Cell* x = CellLookup[c];
         x->S = g_S[c]; x->L = g_L[c]; x->I = g_I[c]; x->R = g_R[c]; x->D = g_D[c];
     }
+    if (!g_timing.empty()) g_timing.back().scatter += omp_get_wtime() - t_sc;
     PopVar& s = StateT[0];
     const PopVar& b = g_base;
     s.cumI = b.cumI + (int)k.cumI; s.cumC = b.cumC + (int)k.cumC; s.cumDC = b.cumDC + (int)k.cumDC;
@@ -682,8 +687,10 @@ void mirror_treat_sweep(double t, int gt)
 void report_timing()
 {
     for (const RunTiming& r : g_timing)
-        std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f upload_s=%.6f copyback_s=%.6f\n",
-                     r.run, P.PopSize, P.NumThreads, r.steps, r.infect, r.incub, r.upload, r.copyback);
+        std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f upload_s=%.6f copyback_s=%.6f"
+                             " wait_s=%.6f scatter_s=%.6f handover_s=%.6f\n",
+                     r.run, P.PopSize, P.NumThreads, r.steps, r.infect, r.incub, r.upload, r.copyback, r.wait, r.scatter,
+                     r.handover);
 }
 
 }  // namespace
@@ -731,7 +738,7 @@ int TreatSweep(double t)
         mirror_treat_sweep(t, gt);
         // the hand-over is the drop-in's own work: timed with its sweeps
         spent += omp_get_wtime() - t0;
-        if (!g_timing.empty()) g_timing.back().infect += spent;
+        if (!g_timing.empty()) { g_timing.back().infect += spent; g_timing.back().handover += spent; }
         // RunModel's UpdateProbs test runs next in this timestep on the State.S the
         // last RecordSample set, which no call in between changes
         const double prop = ((double)(State.S)) / ((double)P.PopSize);
@@ -791,6 +798,7 @@ void IncubRecoverySweep(double t)
     const double t0 = omp_get_wtime();
     (void)t;
     check(cs_gpu_sync(g_ctx), "cs_gpu_sync");   // the timestep's device work, all of it timed
+    if (!g_timing.empty()) g_timing.back().wait += omp_get_wtime() - t0;
     // RecordSample reads the cells and counters at the start of the next output step.
     // RunModel stops calling the sweeps mid-output-step only once State.L + State.I
     // was 0 at the last RecordSample, after which no sweep changes anything; a run

@@ -107,11 +107,13 @@ def network_file(pop, key, threads):
 def parse_timing(stderr):
     rows = []
     for m in re.finditer(r"(?:REF|SWEEP)TIMING run=(\d+) pop=(\d+) threads=(\d+) steps=(\d+) infect_s=([\d.]+) incub_s=([\d.]+)"
-                         r"(?: upload_s=([\d.]+) copyback_s=([\d.]+))?", stderr):
+                         r"((?: \w+_s=[\d.]+)*)", stderr):
         rows.append(dict(run=int(m.group(1)), pop=int(m.group(2)), threads=int(m.group(3)), steps=int(m.group(4)),
                          infect_s=float(m.group(5)), incub_s=float(m.group(6))))
-        if m.group(7) is not None:   # the drop-in's parts: state upload, copies back
-            rows[-1].update(upload_s=float(m.group(7)), copyback_s=float(m.group(8)))
+        # the drop-in's parts: state upload, copies back, the wait for the device, the
+        # copy into the host's cells, the hand-over after TreatSweep
+        for k, v in re.findall(r" (\w+_s)=([\d.]+)", m.group(7)):
+            rows[-1][k] = float(v)
     return rows
 
 
@@ -209,5 +211,8 @@ def time_dropin(workload, steps=3, warmup=1, device=0, threads=None, pop=None):
         visible = ids[device] if device < len(ids) else str(device)
     else:
         visible = str(device)
-    env = {"OMP_WAIT_POLICY": "passive", "CUDA_VISIBLE_DEVICES": visible}
+    # OpenMP's wait policy as the reference arm runs with (the runtime's default)
+    env = {"CUDA_VISIBLE_DEVICES": visible}
+    if os.environ.get("CS_DROPIN_OMP_WAIT_POLICY"):
+        env["OMP_WAIT_POLICY"] = os.environ["CS_DROPIN_OMP_WAIT_POLICY"]
     return time_reference(workload, steps=steps, warmup=warmup, binary=DROPIN, threads=threads, env=env, pop=pop)
