@@ -1945,15 +1945,30 @@ __device__ void k_close_places_body(const DevPop& d, int pt, const uint8_t* sel,
     }
 }
 
-// Outcomes of a host's DoPlaceClose / DoPlaceOpen calls (cs_gpu_place_events), one
-// block per event; every event of one launch has the same kind and place type.
+// Outcomes of a host's DoPlaceClose / DoPlaceOpen calls and holiday closures
+// (cs_gpu_place_events), one block per event; every event of one launch has the
+// same kind and place type.
 __global__ void k_place_events(DevPop d, const cs_place_event* __restrict__ ev, int n)
 {
     const cs_params& P = *d.P;
     for (int e = blockIdx.x; e < n; e += gridDim.x) {
         const cs_place_event E = ev[e];
         const DevPlaces& pl = d.pl[E.place_type];
-        if (E.kind == CS_PLACE_EV_CLOSE) {
+        if (E.kind == CS_PLACE_EV_HOLIDAY) {   // src/Sweep.cpp:904-913
+            if (threadIdx.x == 0) {
+                if (pl.close_start[E.place] > E.win_start) pl.close_start[E.place] = E.win_start;
+                if (pl.close_end[E.place] < E.win_stop) pl.close_end[E.place] = E.win_stop;
+                if (pl.close_start[E.place] < pl.close_end[E.place]) {
+                    atomicMin(d.close_window, (int32_t)pl.close_start[E.place]);
+                    atomicMax(d.close_window + 1, (int32_t)pl.close_end[E.place]);
+                }
+            }
+            for (int k = pl.member_ofs[E.place] + threadIdx.x; k < pl.member_ofs[E.place + 1]; k += blockDim.x) {
+                PersonHot* hw = d.hot + pl.members[k];
+                if (hw->absent_start > E.win_start) hw->absent_start = E.win_start;
+                if (hw->absent_stop < E.win_stop) hw->absent_stop = E.win_stop;
+            }
+        } else if (E.kind == CS_PLACE_EV_CLOSE) {
             if (threadIdx.x == 0) {
                 pl.close_start[E.place] = E.close_start;
                 pl.close_end[E.place] = E.close_end;
@@ -3559,10 +3574,13 @@ int cs_gpu_place_events(cs_gpu_ctx* c, const cs_place_event* ev, int n)
     for (const cs_place_event& e : v) {
         if (e.place_type >= c->d.NPT || e.place < 0 || e.place >= c->d.pl[e.place_type].n)
             return set_err(c, CS_E_ARG, "place event: place %d of type %d out of range", e.place, (int)e.place_type);
-        if (e.kind != CS_PLACE_EV_CLOSE && e.kind != CS_PLACE_EV_OPEN)
+        if (e.kind != CS_PLACE_EV_CLOSE && e.kind != CS_PLACE_EV_OPEN && e.kind != CS_PLACE_EV_HOLIDAY)
             return set_err(c, CS_E_ARG, "place event: bad kind %d", (int)e.kind);
     }
-    auto key = [](const cs_place_event& e) { return (e.kind == CS_PLACE_EV_OPEN ? 0 : 16) + (int)e.place_type; };
+    // opens, closes, holidays; each kind place type by place type
+    auto key = [](const cs_place_event& e) {
+        return (e.kind == CS_PLACE_EV_OPEN ? 0 : e.kind == CS_PLACE_EV_CLOSE ? 16 : 32) + (int)e.place_type;
+    };
     std::stable_sort(v.begin(), v.end(), [&](const cs_place_event& a, const cs_place_event& b) { return key(a) < key(b); });
     if (c->ev_cap < n) {
         if (c->d_ev) cudaFree(c->d_ev);
@@ -3576,6 +3594,11 @@ int cs_gpu_place_events(cs_gpu_ctx* c, const cs_place_event* ev, int n)
     for (int i0 = 0; i0 < n;) {
         int i1 = i0;
         while (i1 < n && key(v[i1]) == key(v[i0])) i1++;
+        if (v[i0].kind == CS_PLACE_EV_HOLIDAY && closes) {   // the closures' carers before the holidays
+            LAUNCH(k_carer_pass, 64, kThreads, c->d);
+            LAUNCH(k_carer_reset, 1, 1, c->d);
+            closes = false;
+        }
         LAUNCH(k_place_events, std::min(c->grid, i1 - i0), kThreads, c->d, c->d_ev + i0, i1 - i0);
         closes |= v[i0].kind == CS_PLACE_EV_CLOSE;
         i0 = i1;

@@ -65,6 +65,7 @@
 #include "InfStat.h"
 #include "Model.h"
 #include "Param.h"
+#include "Rand.h"
 #include "Sweep.h"
 #include "Update.h"
 
@@ -255,7 +256,6 @@ void unsupported_features()
 {
     if (P.DoDigitalContactTracing) ERR_CRITICAL("GPU sweep: digital contact tracing is not supported\n");
     if (P.DoAirports) ERR_CRITICAL("GPU sweep: airports / travel are not supported\n");
-    if (P.DoHolidays && P.NumHolidays > 0) ERR_CRITICAL("GPU sweep: holidays are not supported\n");
     if (P.DoInterventionDelaysByAdUnit) ERR_CRITICAL("GPU sweep: intervention delays by admin unit are not supported\n");
     if (P.InfectionImportRate1 > 0 || P.InfectionImportRate2 > 0 || P.DurImportTimeProfile > 0)
         ERR_CRITICAL("GPU sweep: importation of infections during a run is not supported\n");
@@ -684,6 +684,49 @@ void mirror_treat_sweep(double t, int gt)
     }
 }
 
+// Holidays (the start of IncubRecoverySweep, src/Sweep.cpp:889-918): at the timestep
+// a holiday starts in, each place of a type the holiday affects is chosen (all of
+// them when HolidayEffect is 0, else with probability 1 - HolidayEffect), its window
+// on the host widens as the reference's loop widens it, and the device receives the
+// same choice as CS_PLACE_EV_HOLIDAY events, which widen the members' absences.  The
+// events go to the device before the timestep's sweeps: the holiday starts at
+// HolidayStart = (int)(ht * TimeStepsPerDay), which is past the timestep when the
+// holiday begins on a timestep boundary (ht in (t, t + dt]), so the timestep's
+// InfectSweep sees no difference.
+std::vector<cs_place_event> g_holiday;
+
+void holidays(double t)
+{
+    if (!P.DoPlaces || P.NumHolidays <= 0) return;
+    g_holiday.clear();
+    const unsigned short int ts = (unsigned short int)(P.TimeStepsPerDay * t);
+    for (int h = 0; h < P.NumHolidays; h++) {
+        const double ht = P.HolidayStartTime[h] + P.HolidaysStartDay_SimTime;
+        if (!((t + P.ModelTimeStep >= ht) && (t < ht))) continue;
+        const int hs = (int)(ht * P.TimeStepsPerDay), he = (int)((ht + P.HolidayDuration[h]) * P.TimeStepsPerDay);
+        for (int pt = 0; pt < P.NumPlaceTypes; pt++) {
+            if (!(P.HolidayEffect[pt] < 1)) continue;
+            for (int i = 0; i < P.Nplace[pt]; i++) {
+                if (!((P.HolidayEffect[pt] == 0) || (ranf_mt(0) >= P.HolidayEffect[pt]))) continue;
+                Place& pl = Places[pt][i];
+                if (pl.close_start_time > hs) pl.close_start_time = (unsigned short)hs;
+                if (pl.close_end_time < he) pl.close_end_time = (unsigned short)he;
+                cs_place_event e;
+                std::memset(&e, 0, sizeof(e));
+                e.place = i;
+                e.place_type = (uint8_t)pt;
+                e.kind = CS_PLACE_EV_HOLIDAY;
+                e.ts = ts;
+                e.win_start = (uint16_t)hs;
+                e.win_stop = (uint16_t)he;
+                g_holiday.push_back(e);
+            }
+        }
+    }
+    if (!g_holiday.empty())
+        check(cs_gpu_place_events(g_ctx, g_holiday.data(), (int)g_holiday.size()), "cs_gpu_place_events (holidays)");
+}
+
 void report_timing()
 {
     for (const RunTiming& r : g_timing)
@@ -712,6 +755,7 @@ void InfectSweep(double t, int run)
         g_update_probs = false;
     }
     mirror_host_interventions(t);
+    holidays(t);
     // RunModel calls IncubRecoverySweep(t) right after this call (src/CovidSim.cpp:
     // 1488-1490), so the whole timestep runs here as one replay of its graph
     check(cs_gpu_step(g_ctx, t, run), "cs_gpu_step");

@@ -553,10 +553,14 @@ int cs_gpu_close_places(cs_gpu_ctx* ctx, int place_type, const int32_t* mcells, 
  */
 #define CS_PLACE_EV_CLOSE 1
 #define CS_PLACE_EV_OPEN 2
+/* A holiday closure (IncubRecoverySweep, src/Sweep.cpp:889-918): the place's window
+ * widens to include [win_start, win_stop) and so does every member's absence,
+ * whatever their state.  Applied after the call's opens and closes. */
+#define CS_PLACE_EV_HOLIDAY 3
 typedef struct cs_place_event {
     int32_t place;                     /* index within its type (Places[place_type][place]) */
     uint8_t place_type;
-    uint8_t kind;                      /* CS_PLACE_EV_CLOSE or CS_PLACE_EV_OPEN */
+    uint8_t kind;                      /* CS_PLACE_EV_CLOSE, _OPEN or _HOLIDAY */
     uint8_t members;                   /* close: 1 when the place closed (its members' loop runs) */
     uint8_t _pad0;
     uint16_t ts;                       /* TimeStepNow of the host's call */

@@ -1794,16 +1794,29 @@ int cs_cpu_place_events(cs_cpu_ctx* c, const cs_place_event* ev, int n)
     for (int i = 0; i < n; i++) {
         if (ev[i].place_type >= c->NPT || ev[i].place < 0 || ev[i].place >= c->pl[ev[i].place_type].n)
             return fail(c, CS_E_ARG, "place event out of range");
-        if (ev[i].kind != CS_PLACE_EV_CLOSE && ev[i].kind != CS_PLACE_EV_OPEN) return fail(c, CS_E_ARG, "bad place event kind");
+        if (ev[i].kind != CS_PLACE_EV_CLOSE && ev[i].kind != CS_PLACE_EV_OPEN && ev[i].kind != CS_PLACE_EV_HOLIDAY)
+            return fail(c, CS_E_ARG, "bad place event kind");
     }
     int closes = 0;
-    for (int kind = 0; kind < 2; kind++)
+    /* opens, closes, then holidays (the holiday part of IncubRecoverySweep,
+     * src/Sweep.cpp:889-918); closes' carers after the last close */
+    static const int kinds[3] = {CS_PLACE_EV_OPEN, CS_PLACE_EV_CLOSE, CS_PLACE_EV_HOLIDAY};
+    for (int kind = 0; kind < 3; kind++) {
+        if (kind == 2 && closes) { carer_queue_apply(c); closes = 0; }
         for (int pt = 0; pt < c->NPT; pt++)
             for (int i = 0; i < n; i++) {
                 const cs_place_event* e = ev + i;
-                if (e->place_type != pt || e->kind != (kind == 0 ? CS_PLACE_EV_OPEN : CS_PLACE_EV_CLOSE)) continue;
+                if (e->place_type != pt || e->kind != kinds[kind]) continue;
                 place_arrays* pl = &c->pl[pt];
-                if (e->kind == CS_PLACE_EV_CLOSE) {
+                if (e->kind == CS_PLACE_EV_HOLIDAY) {
+                    if (pl->close_start[e->place] > e->win_start) pl->close_start[e->place] = e->win_start;
+                    if (pl->close_end[e->place] < e->win_stop) pl->close_end[e->place] = e->win_stop;
+                    for (int k = pl->member_ofs[e->place]; k < pl->member_ofs[e->place + 1]; k++) {
+                        const int w = pl->members[k];
+                        if (c->absent_start[w] > e->win_start) c->absent_start[w] = e->win_start;
+                        if (c->absent_stop[w] < e->win_stop) c->absent_stop[w] = e->win_stop;
+                    }
+                } else if (e->kind == CS_PLACE_EV_CLOSE) {
                     closes = 1;
                     pl->close_start[e->place] = e->close_start;
                     pl->close_end[e->place] = e->close_end;
@@ -1816,6 +1829,7 @@ int cs_cpu_place_events(cs_cpu_ctx* c, const cs_place_event* ev, int n)
                     }
                 }
             }
+    }
     if (closes) carer_queue_apply(c);
     return CS_OK;
 }

@@ -9,6 +9,9 @@ daily incidence, critical-care and death curves.
 
 Workloads (CONFIGS):
   plain          20,000 people on 24 x 24 cells, 120 days, no interventions;
+  holidays       the plain workload with a 30-day holiday from day 25 that closes
+                 every school and university (the drop-in hands the reference's
+                 holiday choices to the device);
   interventions  the same world for 200 days with the 10M workload's interventions:
                  the global trigger on critical-care admissions over the last 7 days
                  (above 5 here, the 20,000-person scale of the workload's 100 per
@@ -34,8 +37,14 @@ CONFIGS = {
     "interventions": dict(people=20000, width_deg=0.2, cell_deg=1.0 / 120, nmcl=10, sigma=1.2, days=200,
                           realisations=200, setup_seed=98798150, interventions=True, threshold=5, duration=90.0),
 }
+# the plain world for 120 days with one 30-day holiday from day 25 that closes every
+# school and university (the proportion of places of each type that stays open:
+# primary, secondary, university, workplace), src/Sweep.cpp:889-918
+CONFIGS["holidays"] = dict(CONFIGS["plain"], admin_extra={
+    "Include holidays": 1, "Proportion of places remaining open during holidays by place type": [0.0, 0.0, 0.0, 1.0],
+    "Number of holidays": 1, "Holiday start times": [25.0], "Holiday durations": [30.0]})
 CONFIG = CONFIGS["plain"]
-GOLDEN = {"plain": "ref_ensemble.json", "interventions": "ref_ensemble_iv.json"}
+GOLDEN = {"plain": "ref_ensemble.json", "interventions": "ref_ensemble_iv.json", "holidays": "ref_ensemble_hol.json"}
 
 
 def population(config="plain"):
@@ -55,7 +64,7 @@ def run(binary, nr=None, threads=None, config="plain"):
     res = refrun.run_reference(population(config), c["days"], nr=nr or c["realisations"], threads=threads, binary=binary,
                                series=True, timeout=5400, interventions=c.get("interventions", False),
                                threshold=c.get("threshold", 100), duration=c.get("duration", 90.0),
-                               env={"OMP_WAIT_POLICY": "passive"} if dropin else None)
+                               env={"OMP_WAIT_POLICY": "passive"} if dropin else None, admin_extra=c.get("admin_extra"))
     return summarise(res["series"]), res
 
 

@@ -120,7 +120,7 @@ def parse_timing(stderr):
 def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=100, workdir=None,
                   seeds=(98798150, 729101, 17389101, 4797132),
                   binary=BIN, keep=False, timeout=3000, series=False, duration=90.0, env=None, extra_args=(),
-                  pre_extra=None):
+                  pre_extra=None, admin_extra=None):
     sys.path.insert(0, os.path.join(ROOT, "covid-sim_b200"))
     from covidsim_b200 import refconfig
     threads = threads or os.cpu_count()
@@ -136,6 +136,10 @@ def run_reference(pop, days, nr=1, threads=None, interventions=False, threshold=
             pre["OutputSeverity"] = 1
         pre.update(pre_extra or {})
         refconfig.write_params(f["pre"], pre)
+        if admin_extra:
+            adm = refconfig.admin_params(pop.n_people, 100)
+            adm.update(admin_extra)
+            refconfig.write_params(f["admin"], adm)
         refconfig.write_params(f["params"], params)
         cmd = [binary, "/c:%d" % threads, "/PP:" + f["pre"], "/P:" + f["params"], "/A:" + f["admin"],
                "/D:" + f["density"], "/O:" + os.path.join(wd, "out"), *extra_args, *[str(s) for s in seeds]]

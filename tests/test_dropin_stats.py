@@ -7,7 +7,8 @@ Two-sample KS on final size and peak day (p > 0.01); ensemble-mean daily
 incidence, critical-care and death curves within 2 standard errors on at least
 90% of days.
 
-Two workloads (oracle/ensemble.py): `plain`, and `interventions`, where the
+Three workloads (oracle/ensemble.py): `plain`; `holidays`, the plain one with a
+30-day holiday closing every school and university; and `interventions`, where the
 reference's own trigger logic and TreatSweep switch case isolation, household
 quarantine, social distancing and place closure on and the drop-in's sweeps consume
 what they decided.  The drop-in runs with the host thread count the reference ran
@@ -63,6 +64,12 @@ def test_oracle_sweep_with_interventions_matches_reference():
     _check(summary, "interventions")
 
 
+@pytest.mark.slow
+def test_oracle_sweep_with_holidays_matches_reference():
+    summary, _ = _run(_binary("CovidSim_oracle"), "holidays")
+    _check(summary, "holidays")
+
+
 @pytest.mark.gpu
 def test_gpu_sweep_in_reference_matches_reference():
     summary, res = _run(_binary("CovidSim_b200"), "plain")
@@ -74,4 +81,11 @@ def test_gpu_sweep_in_reference_matches_reference():
 def test_gpu_sweep_with_interventions_matches_reference():
     summary, res = _run(_binary("CovidSim_b200"), "interventions")
     _check(summary, "interventions")
+    assert any("people" in ln for ln in res["dropin"]), res["dropin"]
+
+
+@pytest.mark.gpu
+def test_gpu_sweep_with_holidays_matches_reference():
+    summary, res = _run(_binary("CovidSim_b200"), "holidays")
+    _check(summary, "holidays")
     assert any("people" in ln for ln in res["dropin"]), res["dropin"]

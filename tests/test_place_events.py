@@ -45,6 +45,8 @@ def _events(pop, rng, ts, kind, frac, types, members=None, window=None):
                 e.members = int(rng.random() < 0.8) if members is None else members
                 e.win_start, e.win_stop = window
                 e.close_start, e.close_end = (window if e.members else (window[1], window[1]))
+            elif kind == abi.CS_PLACE_EV_HOLIDAY:
+                e.win_start, e.win_stop = window
             out.append(e)
     return out
 
@@ -117,19 +119,33 @@ class _Ref:
                                 s["absent_stop_time"][l] = e.ts
         self.close_end[(e.place_type, e.place)] = e.ts
 
+    def holiday(self, e):
+        """IncubRecoverySweep's holiday loop for one chosen place (src/Sweep.cpp:
+        904-913): the place's window and every member's absence widen."""
+        s = self.s
+        self.close_end[(e.place_type, e.place)] = max(self.close_end.get((e.place_type, e.place), 0), e.win_stop)
+        for w in self.members(e.place_type, e.place):
+            if s["absent_start_time"][w] > e.win_start:
+                s["absent_start_time"][w] = e.win_start
+            if s["absent_stop_time"][w] < e.win_stop:
+                s["absent_stop_time"][w] = e.win_stop
+
     def apply(self, events):
-        order = sorted(range(len(events)), key=lambda i: ((0 if events[i].kind == abi.CS_PLACE_EV_OPEN else 1),
-                                                          events[i].place_type, i))
+        rank = {abi.CS_PLACE_EV_OPEN: 0, abi.CS_PLACE_EV_CLOSE: 1}
+        order = sorted(range(len(events)), key=lambda i: (rank.get(events[i].kind, 2), events[i].place_type, i))
         queue = []
         for i in order:
             e = events[i]
             if e.kind == abi.CS_PLACE_EV_OPEN:
                 self.open(e)
-            else:
+            elif e.kind == abi.CS_PLACE_EV_CLOSE:
                 self.close(e, queue)
         for j, a, b in queue:   # UpdateHostClosure
             self.s["absent_start_time"][j] = min(self.s["absent_start_time"][j], a)
             self.s["absent_stop_time"][j] = max(self.s["absent_stop_time"][j], b)
+        for i in order:
+            if events[i].kind == abi.CS_PLACE_EV_HOLIDAY:
+                self.holiday(events[i])
         return len(queue)
 
 
@@ -188,6 +204,28 @@ def test_oracle_close_places_follows_reference():
     o.close()
 
 
+def test_oracle_holidays_follow_reference():
+    """Holiday closures (CS_PLACE_EV_HOLIDAY) against the reference's holiday loop
+    restated over the state, mixed with closures in one call (holidays after the
+    closures' carers)."""
+    pop, P, lk, hr = _world((0.0, 0.0, 0.0, 0.0))
+    o = sim.Simulation(pop, P, lk, hr, backend=oracle_py.OracleBackend)
+    o.backend.begin_run(79, o.choose_seeds(79, 40))
+    _advance([o], P, 0, 100, policy_at=40)
+    rng = np.random.default_rng(8)
+    ts = 100
+    hol = _events(pop, rng, ts, abi.CS_PLACE_EV_HOLIDAY, 0.7, (0, 1, 2, 3), window=(ts + 1, ts + 57))
+    closes = _events(pop, rng, ts, abi.CS_PLACE_EV_CLOSE, 0.3, (0, 1), window=(ts, ts + 120))
+    ref = _Ref(pop, P, snapshot(o.backend, pop))
+    ref.apply(hol + closes)
+    o.backend.place_events(hol + closes)
+    got = snapshot(o.backend, pop)
+    for k in ("absent_start_time", "absent_stop_time"):
+        assert np.array_equal(got[k], ref.s[k]), k
+    assert np.sum(got["absent_start_time"] == ts + 1) > 1000, "few members on holiday: weak test"
+    o.close()
+
+
 @pytest.mark.gpu
 def test_gpu_place_events_match_oracle():
     pop, P, lk, hr = _world((0.0, 0.5, 0.0, 0.0))
@@ -204,6 +242,8 @@ def test_gpu_place_events_match_oracle():
         _advance([g, o], P, done, ts_close)
         done = ts_close
         ev = _events(pop, rng, ts_close, abi.CS_PLACE_EV_CLOSE, 0.3, (0, 1, 2, 3), window=(ts_close, ts_close + 160))
+        if round_ == 1:   # holidays among the closures and openings
+            ev += _events(pop, rng, ts_close, abi.CS_PLACE_EV_HOLIDAY, 0.5, (0, 1, 3), window=(ts_close + 1, ts_close + 41))
         if ts_open is not None:
             ev += [abi.cs_place_event(place=int(l), place_type=pt, kind=abi.CS_PLACE_EV_OPEN, ts=ts_open)
                    for pt in (0, 1) for l in np.nonzero(rng.random(len(pop.places[pt]["mcell"])) < 0.3)[0]]
