@@ -159,9 +159,10 @@ def peaks():
 
 def kernel_bytes(name, w, n_cells_steps):
     """Algorithmic bytes a kernel moved over the timed region, from the work counters
-    (per-unit costs: transition scan 16 B per latent/infectious person, infector
-    record 40 B, household member 12 B, place candidate 20 B, spatial draw 33 B,
-    accepted infection 24 B, active-list entry 12 B, per-cell counts 16 B)."""
+    (per-unit costs: transition gather 16 B per latent/infectious person and 16 B per
+    cell, infector record 40 B, household member 12 B, place candidate 20 B, spatial
+    draw 33 B, accepted infection 24 B, infector-list entry 12 B, per-cell counts
+    16 B)."""
     if name == "k_infector_hh_spatial":
         return 40 * w["work_infectors"] + 12 * w["work_hh_members"]
     if name == "k_infector_places":
@@ -170,14 +171,14 @@ def kernel_bytes(name, w, n_cells_steps):
         return 33 * w["work_spatial_draws"]
     if name in ("k_apply_infections", "k_partition_S"):
         return 12 * w["work_new_infections"]
-    if name == "k_incub_scan":
-        return 16 * w["work_incub_people"]
+    if name == "k_incub_gather":
+        return 16 * w["work_incub_people"] + 16 * n_cells_steps
     if name == "k_incub_events":
         return 32 * w["work_transitions"]
-    if name in ("k_partition_LI", "k_clear_pstep"):
+    if name == "k_incub_finish":
         return 8 * w["work_transitions"]
-    if name == "k_build_active":   # two launches per timestep
-        return 12 * (w["work_infectors"] + w["work_incub_people"]) + 2 * 16 * n_cells_steps
+    if name == "k_build_active":   # the infectors, once per timestep
+        return 12 * w["work_infectors"] + 16 * n_cells_steps
     return None
 
 

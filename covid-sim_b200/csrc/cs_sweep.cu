@@ -17,11 +17,11 @@
 //     k_apply_infections     DoInfect for every claimed person (lowest key wins)
 //     k_partition_S          S -> L cell-list moves, one warp per touched cell
 //   IncubRecoverySweep
-//     k_build_active         latent + infectious people
-//     k_incub_scan           the people with an event this step
+//     k_incub_gather         the latent and infectious people with an event this step,
+//                            read from the cells' lists
 //     k_incub_events         DoIncub / DoCase / severity / recovery / death per person
-//     k_partition_LI     L -> I and I -> R/D cell-list moves per touched cell
-//     k_household_after  deferred adult-carer absence and household quarantine
+//     k_incub_finish         L -> I and I -> R/D cell-list moves per touched cell, then
+//                            the deferred adult-carer absence and household quarantine
 //
 // Determinism: all random numbers come from Philox streams keyed by
 // (seed, step, entity, purpose); conflicting infections resolve by atomicMin on a
@@ -1551,33 +1551,65 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
 // Which latent / infectious people have an event this step (latent period ends,
 // case onset, severity change, recovery or death): a light scan that compacts
 // them into cmap so the heavy transition kernel runs only on those.
-__device__ __forceinline__ void k_incub_scan_body(const DevPop& d)
+// IncubRecoverySweep's scan (src/Sweep.cpp:920-977) over the cells' lists: every
+// latent and infectious person (slots [S, S+L+I) of each cell, read block-
+// cooperatively as k_build_active reads a cell's slots, so a dense cell costs no more
+// than its share of the block) joins the step's event list when one of its times is
+// now.  The list holds (person, cell) in act / act_cell, in no particular order:
+// k_incub_events treats each person on its own.
+__device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const int ts = d.step->ts;
-    int nact = d.counts[kCntAct];
-    if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_CTR(work_incub_people), nact);
     const int delay = (int)(P.LatentToSymptDelay / P.ModelTimeStep);
-    for (int base = blockIdx.x * blockDim.x; base < nact; base += gridDim.x * blockDim.x) {
-        const int idx = base + threadIdx.x;
-        bool ev = false;
-        if (idx < nact) {
-            int p = d.act[idx];
-            PersonHot h = d.hot[p];
-            if (h.inf == CS_INF_LATENT)
-                ev = h.latent_time == ts;
-            else
-                ev = (ts == (uint16_t)(h.latent_time + delay)) || (ts == d.recovery_time[p]) ||
-                     (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
+    __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads];
+    long long people = 0;
+    for (int c0 = blockIdx.x * blockDim.x; c0 < d.NC; c0 += gridDim.x * blockDim.x) {
+        const int c = c0 + threadIdx.x;
+        int first = 0, n = 0;
+        if (c < d.NC) {
+            first = d.cell_start[c] + d.S[c];
+            n = d.L[c] + d.I[c];
         }
-        const int o = block_reserve2(d.counts + kCntEvents, ev ? 1 : 0, nullptr, 0).x;
-        if (ev) d.cmap[o] = idx;
+        const int o = block_reserve2(nullptr, n, nullptr, 0).x;   // the block's own prefix of n
+        s_first[threadIdx.x] = first;
+        s_ofs[threadIdx.x] = o;
+        s_n[threadIdx.x] = n;
+        __syncthreads();
+        const int total = s_ofs[blockDim.x - 1] + s_n[blockDim.x - 1];
+        if (threadIdx.x == 0) people += total;
+        for (int j0 = 0; j0 < total; j0 += blockDim.x) {   // block-uniform: every thread reserves
+            const int j = j0 + (int)threadIdx.x;
+            bool ev = false;
+            int p = 0, cell = 0;
+            if (j < total) {
+                int lo = 0, hi = blockDim.x - 1;   // the last cell whose entries start at or before j
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_ofs[mid] <= j) lo = mid; else hi = mid - 1;
+                }
+                p = d.slots[s_first[lo] + (j - s_ofs[lo])];
+                cell = c0 + lo;
+                const PersonHot h = d.hot[p];
+                if (h.inf == CS_INF_LATENT)
+                    ev = h.latent_time == ts;
+                else
+                    ev = (ts == (uint16_t)(h.latent_time + delay)) || (ts == d.recovery_time[p]) ||
+                         (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
+            }
+            const int e = block_reserve2(d.counts + kCntEvents, ev ? 1 : 0, nullptr, 0).x;
+            if (ev) {
+                d.act[e] = p;
+                d.act_cell[e] = cell;
+            }
+        }
+        __syncthreads();   // the shared arrays are refilled for the next cells
     }
+    if (threadIdx.x == 0 && people) cnt_add(CSB_CTR(work_incub_people), people);
 }
-__global__ void __launch_bounds__(kThreads) k_incub_scan(DevPop d) { k_incub_scan_body(d); }
-__global__ void __launch_bounds__(kThreads) k_incub_scan_multi(const DevPop* __restrict__ pops) { k_incub_scan_body(pops[blockIdx.y]); }
+__global__ void __launch_bounds__(kThreads) k_incub_gather(DevPop d) { k_incub_gather_body(d); }
+__global__ void __launch_bounds__(kThreads) k_incub_gather_multi(const DevPop* __restrict__ pops) { k_incub_gather_body(pops[blockIdx.y]); }
 
-// cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
 // DoFalseCase (src/Update.cpp:896-905) for every person with a false-positive
 // entry this step, after the step's infections: detected with probability
 // ControlPropCasesId (counted once the detected cases at the last sample reached
@@ -1619,6 +1651,7 @@ __device__ __forceinline__ void k_apply_false_cases_body(const DevPop& d)
 __global__ void k_apply_false_cases(DevPop d) { k_apply_false_cases_body(d); }
 __global__ void k_apply_false_cases_multi(const DevPop* __restrict__ pops) { k_apply_false_cases_body(pops[blockIdx.y]); }
 
+// cnt[c] low 16 bits: L -> I moves of cell c; high 16 bits: I -> R/D moves.
 __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
@@ -1631,8 +1664,7 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
     const bool staged = nev >= kStageMinItems;
     stage_begin(d.C, staged);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) {
-        int idx = d.cmap[e];
-        int p = d.act[idx], c = d.act_cell[idx];
+        const int p = d.act[e], c = d.act_cell[e];
         PersonHot h = d.hot[p];
         int pos = d.cell_start[c] + d.listpos[p];
         if (h.inf == CS_INF_LATENT) {
@@ -1696,7 +1728,7 @@ __device__ __forceinline__ void k_household_after_body(const DevPop& d)
     const uint64_t seed = d.step->seed;
     // the step's transition flags are only set on event people: clear them
     int nev = d.counts[kCntEvents];
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) d.pstep[d.act[d.cmap[e]]] = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) d.pstep[d.act[e]] = 0;
     int nh = d.counts[kCntHH];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
         int h = d.hh_list[k];
@@ -1744,6 +1776,20 @@ __device__ __forceinline__ void k_household_after_body(const DevPop& d)
 }
 __global__ void k_household_after(DevPop d) { k_household_after_body(d); }
 __global__ void k_household_after_multi(const DevPop* __restrict__ pops) { k_household_after_body(pops[blockIdx.y]); }
+
+// The cell-list moves and the household actions in one launch: the moves touch the
+// cells' slots and list positions, the household actions people's absences and
+// quarantine, flags and household lists, so neither waits for the other.
+__global__ void k_incub_finish(DevPop d)
+{
+    k_partition_LI_body(d);
+    k_household_after_body(d);
+}
+__global__ void k_incub_finish_multi(const DevPop* __restrict__ pops)
+{
+    k_partition_LI_body(pops[blockIdx.y]);
+    k_household_after_body(pops[blockIdx.y]);
+}
 
 // ============================================================ seeding
 __global__ void k_seed_claims(DevPop d, const int32_t* list, int n)
@@ -2222,7 +2268,7 @@ int64_t cs_gpu_launch_count(const cs_gpu_ctx* c) { return c ? c->launches : 0; }
 
 static int check_params(cs_gpu_ctx* c, const cs_params* P)
 {
-    if (P->FalsePositiveRate != 0) return set_err(c, CS_E_UNSUPPORTED, "FalsePositiveRate must be 0 (false-positive cases are not modelled)");
+    if (!(P->FalsePositiveRate >= 0 && P->FalsePositiveRate < 1)) return set_err(c, CS_E_ARG, "FalsePositiveRate outside [0, 1)");
     if (P->NumPlaceTypes < 0 || P->NumPlaceTypes > CS_MAX_PLACE_TYPES) return set_err(c, CS_E_ARG, "NumPlaceTypes out of range");
     if (P->kernel_size < 2 || P->kernel_expansion < 1 || !(P->kernel_delta > 0)) return set_err(c, CS_E_ARG, "kernel table not set");
     if (P->ncw <= 0 || P->nch <= 0) return set_err(c, CS_E_ARG, "grid size not set");
@@ -2246,7 +2292,12 @@ static int alloc_dynamic(cs_gpu_ctx* c)
     AL(d.infection_time, N); AL(d.recovery_time, N); AL(d.sari_time, N); AL(d.critical_time, N);
     AL(d.stepdown_time, N); AL(d.detected_time, N); AL(d.prob_absent, N); AL(d.prob_care, N);
     AL(d.infector, N); AL(d.listpos, N); AL(d.infect_type, N); AL(d.pstep, N);
-    AL(d.S, NC); AL(d.L, NC); AL(d.I, NC); AL(d.R, NC); AL(d.D, NC); AL(d.S0, NC);
+    {   // S, L, I, R, D side by side, so that a host can copy all five at once
+        int32_t* cells5;
+        AL(cells5, 5 * NC);
+        d.S = cells5; d.L = cells5 + NC; d.I = cells5 + 2 * NC; d.R = cells5 + 3 * NC; d.D = cells5 + 4 * NC;
+    }
+    AL(d.S0, NC);
     AL(d.tot_prob, NC); AL(d.slots, N); AL(d.mark, N);
     AL(d.socdist, NM); AL(d.moverest, NM);
     CK(cudaMemsetAsync(d.socdist, 0, NM, c->stream));
@@ -2816,12 +2867,9 @@ static int incub_sweep(cs_gpu_ctx* c, double t, bool set_step)
 {
     DevPop& d = c->d;
     if (set_step) LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
-    int r = build_active(c, 1);
-    if (r) return r;
-    LAUNCH(k_incub_scan, c->grid, kThreads, d);
+    LAUNCH(k_incub_gather, (d.NC + kThreads - 1) / kThreads, kThreads, d);
     LAUNCH(k_incub_events, c->grid, kThreads, d);
-    LAUNCH(k_partition_LI, c->grid, kThreads, d);
-    LAUNCH(k_household_after, c->grid, kThreads, d);
+    LAUNCH(k_incub_finish, c->grid, kThreads, d);
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));   // all list counters
     return CS_OK;
 }
@@ -3236,11 +3284,9 @@ static int batch_enqueue(cs_gpu_batch* b, const DevPop* pops)
     for (const cs_gpu_ctx* m : b->members) fpr |= m->hp.FalsePositiveRate > 0;
     if (fpr) BLAUNCH(k_apply_false_cases_multi, g, kThreads, pops);
     BLAUNCH(k_zero_counts_multi, R, 32, pops, (int)(kCntN - 1));   // the household list is the incub sweep's
-    BLAUNCH(k_build_active_multi, g, kThreads, pops, 1);
-    BLAUNCH(k_incub_scan_multi, g, kThreads, pops);
+    BLAUNCH(k_incub_gather_multi, g, kThreads, pops);
     BLAUNCH(k_incub_events_multi, g, kThreads, pops);
-    BLAUNCH(k_partition_LI_multi, g, kThreads, pops);
-    BLAUNCH(k_household_after_multi, g, kThreads, pops);
+    BLAUNCH(k_incub_finish_multi, g, kThreads, pops);
     BLAUNCH(k_zero_counts_multi, R, 32, pops, (int)kCntN);
     return CS_OK;
 }
@@ -3695,11 +3741,15 @@ int cs_gpu_get_sample(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t
     if (!c || !out) return CS_E_ARG;
     DevPop& d = c->d;
     const size_t n = sizeof(int32_t) * d.NC;
-    if (S) CK(cudaMemcpyAsync(S, d.S, n, cudaMemcpyDeviceToHost, c->stream));
-    if (L) CK(cudaMemcpyAsync(L, d.L, n, cudaMemcpyDeviceToHost, c->stream));
-    if (I) CK(cudaMemcpyAsync(I, d.I, n, cudaMemcpyDeviceToHost, c->stream));
-    if (R) CK(cudaMemcpyAsync(R, d.R, n, cudaMemcpyDeviceToHost, c->stream));
-    if (D) CK(cudaMemcpyAsync(D, d.D, n, cudaMemcpyDeviceToHost, c->stream));
+    if (S && L == S + d.NC && I == L + d.NC && R == I + d.NC && D == R + d.NC) {
+        CK(cudaMemcpyAsync(S, d.S, 5 * n, cudaMemcpyDeviceToHost, c->stream));   // the five arrays lie side by side
+    } else {
+        if (S) CK(cudaMemcpyAsync(S, d.S, n, cudaMemcpyDeviceToHost, c->stream));
+        if (L) CK(cudaMemcpyAsync(L, d.L, n, cudaMemcpyDeviceToHost, c->stream));
+        if (I) CK(cudaMemcpyAsync(I, d.I, n, cudaMemcpyDeviceToHost, c->stream));
+        if (R) CK(cudaMemcpyAsync(R, d.R, n, cudaMemcpyDeviceToHost, c->stream));
+        if (D) CK(cudaMemcpyAsync(D, d.D, n, cudaMemcpyDeviceToHost, c->stream));
+    }
     CK(cudaMemsetAsync(d.C, 0, 5 * sizeof(int64_t), c->stream));  // S..D recomputed below
     LAUNCH(k_cell_totals, 64, kThreads, d);
     CK(cudaMemcpyAsync(out, d.C, sizeof(cs_counters), cudaMemcpyDeviceToHost, c->stream));

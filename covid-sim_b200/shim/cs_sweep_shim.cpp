@@ -109,7 +109,8 @@ struct Pinned {
     const T& operator[](size_t i) const { return p[i]; }
 };
 
-Pinned<int32_t> g_S, g_L, g_I, g_R, g_D;
+Pinned<int32_t> g_cells5;                     // S, L, I, R, D of every cell, side by side
+int32_t *g_S = nullptr, *g_L = nullptr, *g_I = nullptr, *g_R = nullptr, *g_D = nullptr;
 cs_params g_params;
 // what the device holds of the host's intervention state
 std::vector<uint8_t> g_sd, g_mr;              // per microcell: socdist, moverest (TreatStat)
@@ -129,6 +130,7 @@ struct RunTiming {
     double wait = 0.0, scatter = 0.0, handover = 0.0;   // finer parts: the wait for the device's
                                                         // timestep, the copy into the host's cells,
                                                         // the hand-over after TreatSweep
+    long scans = 0;                                     // microcell scans of the hand-over
 };
 std::vector<RunTiming> g_timing;
 FILE* g_dump = nullptr;
@@ -385,7 +387,8 @@ void create_context()
     pop.kernel_lookup = klook.data(); pop.kernel_hi_res = khi.data();
     int rc = cs_gpu_create(&pop, &g_params, 0, &g_ctx);
     check(rc, "cs_gpu_create");
-    g_S.resize(NC); g_L.resize(NC); g_I.resize(NC); g_R.resize(NC); g_D.resize(NC);
+    g_cells5.resize(5 * (size_t)NC);
+    g_S = g_cells5.data(); g_L = g_S + NC; g_I = g_L + NC; g_R = g_I + NC; g_D = g_R + NC;
     std::fprintf(stderr, "GPU sweep: %d people, %d populated cells on device\n", N, NC);
 }
 
@@ -484,7 +487,7 @@ void upload_run_state(int run)
 void sync_back()
 {
     cs_counters k;
-    check(cs_gpu_get_sample(g_ctx, g_S.data(), g_L.data(), g_I.data(), g_R.data(), g_D.data(), &k), "cs_gpu_get_sample");
+    check(cs_gpu_get_sample(g_ctx, g_S, g_L, g_I, g_R, g_D, &k), "cs_gpu_get_sample");
     const double t_sc = omp_get_wtime();
 #pragma omp parallel for schedule(static)
     for (int c = 0; c < P.NumPopulatedCells; c++) {
@@ -654,11 +657,15 @@ void mirror_treat_sweep(double t, int gt)
     }
     const bool mr = t >= P.MoveRestrTimeStart;
     if (sd || mr) {
-        std::vector<int32_t> ms;
-        std::vector<uint8_t> vs, vm;
+        // the scan over every populated microcell runs on the host's OpenMP threads;
+        // the changed ones are then listed in microcell order
+        const int npm = P.NumPopulatedMicrocells;
+        static std::vector<uint8_t> chg;
+        chg.resize(npm);
         long long untreated = 0, treated = 0;
         unsigned int min_end = 0xFFFFFFFFu;
-        for (int i = 0; i < P.NumPopulatedMicrocells; i++) {
+#pragma omp parallel for schedule(static) reduction(+ : untreated, treated) reduction(min : min_end)
+        for (int i = 0; i < npm; i++) {
             const int m = (int)(McellLookup[i] - Mcells);
             const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
             if (Mcells[m].socdist == TreatStat::Untreated) untreated++;
@@ -666,11 +673,18 @@ void mirror_treat_sweep(double t, int gt)
                 treated++;
                 if (Mcells[m].socdist_end_time < min_end) min_end = Mcells[m].socdist_end_time;
             }
-            if (a == g_sd[m] && b == g_mr[m]) continue;
-            ms.push_back(m);
-            vs.push_back(g_sd[m] = a);
-            vm.push_back(g_mr[m] = b);
+            chg[i] = (a != g_sd[m] || b != g_mr[m]);
         }
+        std::vector<int32_t> ms;
+        std::vector<uint8_t> vs, vm;
+        for (int i = 0; i < npm; i++) {
+            if (!chg[i]) continue;
+            const int m = (int)(McellLookup[i] - Mcells);
+            ms.push_back(m);
+            vs.push_back(g_sd[m] = (uint8_t)Mcells[m].socdist);
+            vm.push_back(g_mr[m] = (uint8_t)Mcells[m].moverest);
+        }
+        if (!g_timing.empty()) g_timing.back().scans++;
         g_sd_untreated = untreated;
         g_sd_treated = treated;
         g_sd_min_end = min_end;
@@ -731,9 +745,9 @@ void report_timing()
 {
     for (const RunTiming& r : g_timing)
         std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f upload_s=%.6f copyback_s=%.6f"
-                             " wait_s=%.6f scatter_s=%.6f handover_s=%.6f\n",
+                             " wait_s=%.6f scatter_s=%.6f handover_s=%.6f mcell_scans=%ld\n",
                      r.run, P.PopSize, P.NumThreads, r.steps, r.infect, r.incub, r.upload, r.copyback, r.wait, r.scatter,
-                     r.handover);
+                     r.handover, r.scans);
 }
 
 }  // namespace

@@ -620,7 +620,8 @@ int cs_gpu_batch_run(cs_gpu_batch* batch, int days, const cs_run_policy* policie
 int cs_gpu_get_cell_counts(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D);
 /* cs_gpu_get_cell_counts and cs_gpu_get_counters in one call, with one wait: what
  * RecordSample (src/CovidSim.cpp:3024-3120) reads at each output step.  Any of the
- * five cell arrays may be NULL. */
+ * five cell arrays may be NULL; when they lie side by side in one buffer (L = S +
+ * n_cells, ..., D = R + n_cells) they arrive in a single copy. */
 int cs_gpu_get_sample(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D,
                       cs_counters* out);
 /* Page-locked host memory (NULL on failure) for a host's staging buffers: copies

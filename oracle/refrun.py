@@ -107,12 +107,12 @@ def network_file(pop, key, threads):
 def parse_timing(stderr):
     rows = []
     for m in re.finditer(r"(?:REF|SWEEP)TIMING run=(\d+) pop=(\d+) threads=(\d+) steps=(\d+) infect_s=([\d.]+) incub_s=([\d.]+)"
-                         r"((?: \w+_s=[\d.]+)*)", stderr):
+                         r"((?: \w+=[\d.]+)*)", stderr):
         rows.append(dict(run=int(m.group(1)), pop=int(m.group(2)), threads=int(m.group(3)), steps=int(m.group(4)),
                          infect_s=float(m.group(5)), incub_s=float(m.group(6))))
         # the drop-in's parts: state upload, copies back, the wait for the device, the
         # copy into the host's cells, the hand-over after TreatSweep
-        for k, v in re.findall(r" (\w+_s)=([\d.]+)", m.group(7)):
+        for k, v in re.findall(r" (\w+)=([\d.]+)", m.group(7)):
             rows[-1][k] = float(v)
     return rows
 
