@@ -466,12 +466,14 @@ def e2e_dropin(args, local, world, dist, n_cells):
     d2h = days * (5 * 4 * n_cells + ctypes.sizeof(abi.cs_counters))
     parts = {k: round(1e3 * sum(r.get(k, 0.0) for r in rows) / len(rows), 3)
              for k in ("upload_s", "copyback_s", "wait_s", "scatter_s", "handover_s", "infect_s", "incub_s")}
+    scans = sum(r.get("mcell_scans", 0) for r in rows) / len(rows)
     return {"value": round(person_steps * world / secs, 1), "unit": METRIC, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": round(1e3 * secs / len(rows), 3),
             "ms_per_step_parts": {"state_upload": parts["upload_s"], "copy_back": parts["copyback_s"],
                                   "copy_back_into_cells": parts["scatter_s"], "wait_for_device": parts["wait_s"],
                                   "handover_after_treatsweep": parts["handover_s"], "infect_calls": parts["infect_s"],
                                   "incub_calls": parts["incub_s"]},
+            "handover_microcell_scans_per_step": scans,
             "what": "the reference executable with the GPU sweep linked in (oracle/_ref/CovidSim_b200), the same "
                     "network file as the reference arm; wall time of the sweep calls per realisation: state upload "
                     "from the reference's host structures at its start, device sweeps (one graph per timestep, "

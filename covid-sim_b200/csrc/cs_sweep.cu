@@ -1555,8 +1555,11 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
 // latent and infectious person (slots [S, S+L+I) of each cell, read block-
 // cooperatively as k_build_active reads a cell's slots, so a dense cell costs no more
 // than its share of the block) joins the step's event list when one of its times is
-// now.  The list holds (person, cell) in act / act_cell, in no particular order:
-// k_incub_events treats each person on its own.
+// now.  The cells come in tiles of blockDim.x; Q = gridDim.x / tiles blocks share a
+// tile, block q taking its chunks q, q + Q, ... of blockDim.x entries, so the launch
+// has the parallelism of a flat list without building one.  The list holds (person,
+// cell) in act / act_cell, in no particular order: k_incub_events treats each person
+// on its own.
 __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
@@ -1564,7 +1567,10 @@ __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
     const int delay = (int)(P.LatentToSymptDelay / P.ModelTimeStep);
     __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads];
     long long people = 0;
-    for (int c0 = blockIdx.x * blockDim.x; c0 < d.NC; c0 += gridDim.x * blockDim.x) {
+    const int ntiles = (d.NC + blockDim.x - 1) / blockDim.x;
+    const int Q = max(1, (int)gridDim.x / ntiles), part = blockIdx.x % Q;
+    for (int tile = blockIdx.x / Q; tile < ntiles; tile += max(1, (int)gridDim.x / Q)) {
+        const int c0 = tile * blockDim.x;
         const int c = c0 + threadIdx.x;
         int first = 0, n = 0;
         if (c < d.NC) {
@@ -1577,8 +1583,8 @@ __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
         s_n[threadIdx.x] = n;
         __syncthreads();
         const int total = s_ofs[blockDim.x - 1] + s_n[blockDim.x - 1];
-        if (threadIdx.x == 0) people += total;
-        for (int j0 = 0; j0 < total; j0 += blockDim.x) {   // block-uniform: every thread reserves
+        if (threadIdx.x == 0 && part == 0) people += total;
+        for (int j0 = part * blockDim.x; j0 < total; j0 += Q * blockDim.x) {   // block-uniform: every thread reserves
             const int j = j0 + (int)threadIdx.x;
             bool ev = false;
             int p = 0, cell = 0;
@@ -2867,7 +2873,10 @@ static int incub_sweep(cs_gpu_ctx* c, double t, bool set_step)
 {
     DevPop& d = c->d;
     if (set_step) LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
-    LAUNCH(k_incub_gather, (d.NC + kThreads - 1) / kThreads, kThreads, d);
+    {   // every tile of kThreads cells shared by enough blocks to fill the grid
+        const int ntiles = (d.NC + kThreads - 1) / kThreads;
+        LAUNCH(k_incub_gather, ntiles * std::max(1, c->grid / ntiles), kThreads, d);
+    }
     LAUNCH(k_incub_events, c->grid, kThreads, d);
     LAUNCH(k_incub_finish, c->grid, kThreads, d);
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));   // all list counters

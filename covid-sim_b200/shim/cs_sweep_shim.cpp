@@ -659,31 +659,51 @@ void mirror_treat_sweep(double t, int gt)
     if (sd || mr) {
         // the scan over every populated microcell runs on the host's OpenMP threads;
         // the changed ones are then listed in microcell order
+        // Each thread scans one contiguous share of the populated microcells, counts
+        // its changes, and after a prefix over the threads writes them to its own
+        // range of the change list, so the list stays in microcell order.
         const int npm = P.NumPopulatedMicrocells;
-        static std::vector<uint8_t> chg;
-        chg.resize(npm);
-        long long untreated = 0, treated = 0;
+        static std::vector<int32_t> ms;
+        static std::vector<uint8_t> vs, vm;
+        static std::vector<long long> thread_n;
+        ms.resize(npm); vs.resize(npm); vm.resize(npm);
+        long long untreated = 0, treated = 0, nchg = 0;
         unsigned int min_end = 0xFFFFFFFFu;
-#pragma omp parallel for schedule(static) reduction(+ : untreated, treated) reduction(min : min_end)
-        for (int i = 0; i < npm; i++) {
-            const int m = (int)(McellLookup[i] - Mcells);
-            const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
-            if (Mcells[m].socdist == TreatStat::Untreated) untreated++;
-            else if (Mcells[m].socdist == TreatStat::Treated) {
-                treated++;
-                if (Mcells[m].socdist_end_time < min_end) min_end = Mcells[m].socdist_end_time;
+#pragma omp parallel reduction(+ : untreated, treated) reduction(min : min_end)
+        {
+            const int T = omp_get_num_threads(), k = omp_get_thread_num();
+#pragma omp single
+            thread_n.assign((size_t)T + 1, 0);
+            const int i0 = (int)((long long)npm * k / T), i1 = (int)((long long)npm * (k + 1) / T);
+            long long mine = 0;
+            for (int i = i0; i < i1; i++) {
+                const int m = (int)(McellLookup[i] - Mcells);
+                const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
+                if (Mcells[m].socdist == TreatStat::Untreated) untreated++;
+                else if (Mcells[m].socdist == TreatStat::Treated) {
+                    treated++;
+                    if (Mcells[m].socdist_end_time < min_end) min_end = Mcells[m].socdist_end_time;
+                }
+                mine += (a != g_sd[m] || b != g_mr[m]);
             }
-            chg[i] = (a != g_sd[m] || b != g_mr[m]);
+            thread_n[k + 1] = mine;
+#pragma omp barrier
+#pragma omp single
+            for (int j = 0; j < T; j++) thread_n[j + 1] += thread_n[j];
+            long long o = thread_n[k];
+            for (int i = i0; i < i1 && o < thread_n[k + 1]; i++) {
+                const int m = (int)(McellLookup[i] - Mcells);
+                const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
+                if (a == g_sd[m] && b == g_mr[m]) continue;
+                ms[o] = m;
+                vs[o] = g_sd[m] = a;
+                vm[o] = g_mr[m] = b;
+                o++;
+            }
+#pragma omp single
+            nchg = thread_n[T];
         }
-        std::vector<int32_t> ms;
-        std::vector<uint8_t> vs, vm;
-        for (int i = 0; i < npm; i++) {
-            if (!chg[i]) continue;
-            const int m = (int)(McellLookup[i] - Mcells);
-            ms.push_back(m);
-            vs.push_back(g_sd[m] = (uint8_t)Mcells[m].socdist);
-            vm.push_back(g_mr[m] = (uint8_t)Mcells[m].moverest);
-        }
+        ms.resize(nchg); vs.resize(nchg); vm.resize(nchg);
         if (!g_timing.empty()) g_timing.back().scans++;
         g_sd_untreated = untreated;
         g_sd_treated = treated;
