@@ -182,6 +182,7 @@ def load_library(path=LIB_PATH):
         "cs_gpu_batch_run": (I, [V, I, V, V]),
         "cs_gpu_get_cell_counts": (I, [V, V, V, V, V, V]),
         "cs_gpu_get_sample": (I, [V, V, V, V, V, V, P(cs_counters)]),
+        "cs_gpu_get_sample16": (I, [V, V, P(cs_counters)]),
         "cs_host_alloc": (V, [C.c_size_t]),
         "cs_host_free": (None, [V]),
         "cs_gpu_sync": (I, [V]),

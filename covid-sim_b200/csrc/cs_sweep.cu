@@ -181,6 +181,8 @@ struct cs_gpu_ctx {
     int device = 0;
     std::shared_ptr<StaticStore> stat;     // static population arrays (possibly shared)
     std::vector<void*>* alloc_to = nullptr;  // where dalloc records allocations (null: allocs)
+    int max_cell_people = 0;   // the largest cell's population (cs_gpu_get_sample16's limit)
+    void* pack16 = nullptr;    // device staging of cs_gpu_get_sample16
     cudaStream_t own_stream = nullptr;     // the context's stream while a batch lends it another
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;           // the place pass's branch beside the spatial pass
@@ -806,41 +808,53 @@ __global__ void k_block_rows(DevPop d)
 
 // ======================================================== active-list build
 // The step's active people, cell by cell: infectious, slots [S+L, S+L+I) (mode 0),
-// or latent and infectious, slots [S, S+L+I) (mode 1).  Each cell reserves its
-// entries warp by warp, so the list's order varies from launch to launch; nothing
-// that reads it depends on the order (random streams are keyed by person and
-// contact, conflicting claims resolve by key, tallies are integer sums, and cell
-// lists are reordered by position).  A block reserves the entries of its 256 cells
-// at once and copies them together, entry j by the thread whose turn it is, so a
-// cell with thousands of active people costs no more than its share of the block.
+// or latent and infectious, slots [S, S+L+I) (mode 1).  The cells come in tiles of
+// blockDim.x; Q = gridDim.x / tiles blocks share a tile, block q copying its chunks
+// q, q + Q, ... of blockDim.x entries (entry j by the thread whose turn it is), so a
+// cell with thousands of active people costs no more than its share and the launch
+// has the parallelism of the list.  Each chunk reserves its entries at once, so the
+// list's order varies from launch to launch; nothing that reads it depends on the
+// order (random streams are keyed by person and contact, conflicting claims resolve
+// by key, tallies are integer sums, and cell lists are reordered by position).
 __device__ __forceinline__ void k_build_active_body(const DevPop& d, int mode)
 {
-    __shared__ int s_first[kThreads], s_dst[kThreads], s_n[kThreads];
-    for (int c0 = blockIdx.x * blockDim.x; c0 < d.NC; c0 += gridDim.x * blockDim.x) {
+    __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads];
+    const int ntiles = (d.NC + blockDim.x - 1) / blockDim.x;
+    const int Q = max(1, (int)gridDim.x / ntiles), part = blockIdx.x % Q;
+    for (int tile = blockIdx.x / Q; tile < ntiles; tile += max(1, (int)gridDim.x / Q)) {
+        const int c0 = tile * blockDim.x;
         const int c = c0 + threadIdx.x;
         int first = 0, n = 0;
         if (c < d.NC) {
             first = d.cell_start[c] + d.S[c] + (mode == 0 ? d.L[c] : 0);
             n = mode == 0 ? d.I[c] : d.L[c] + d.I[c];
         }
-        const int o = block_reserve2(d.counts + kCntAct, n, nullptr, 0).x;
+        const int o = block_reserve2(nullptr, n, nullptr, 0).x;   // the block's own prefix of n
         s_first[threadIdx.x] = first;
-        s_dst[threadIdx.x] = o;
+        s_ofs[threadIdx.x] = o;
         s_n[threadIdx.x] = n;
         __syncthreads();
-        const int base = s_dst[0];                    // thread 0's entries start the block's range
-        const int total = s_dst[blockDim.x - 1] + s_n[blockDim.x - 1] - base;
-        for (int j = threadIdx.x; j < total; j += blockDim.x) {
-            // the last cell whose entries start at or before j holds entry j
-            int lo = 0, hi = blockDim.x - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_dst[mid] - base <= j) lo = mid; else hi = mid - 1;
+        const int total = s_ofs[blockDim.x - 1] + s_n[blockDim.x - 1];
+        for (int j0 = part * blockDim.x; j0 < total; j0 += Q * blockDim.x) {   // block-uniform: every thread reserves
+            const int j = j0 + (int)threadIdx.x;
+            const bool valid = j < total;
+            int p = 0, cell = 0;
+            if (valid) {
+                int lo = 0, hi = blockDim.x - 1;   // the last cell whose entries start at or before j
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_ofs[mid] <= j) lo = mid; else hi = mid - 1;
+                }
+                p = d.slots[s_first[lo] + (j - s_ofs[lo])];
+                cell = c0 + lo;
             }
-            d.act[base + j] = d.slots[s_first[lo] + (base + j - s_dst[lo])];
-            d.act_cell[base + j] = c0 + lo;
+            const int e = block_reserve2(d.counts + kCntAct, valid ? 1 : 0, nullptr, 0).x;
+            if (valid) {
+                d.act[e] = p;
+                d.act_cell[e] = cell;
+            }
         }
-        __syncthreads();   // the shared arrays are refilled for the next 256 cells
+        __syncthreads();   // the shared arrays are refilled for the next cells
     }
 }
 __global__ void k_build_active(DevPop d, int mode) { k_build_active_body(d, mode); }
@@ -2437,6 +2451,8 @@ int cs_gpu_create(const cs_population* pop, const cs_params* params, int device,
     { int32_t* t; UP(t, pop->mcell_adunit, NM); d.mcell_adunit = t; }
     { int32_t* t; UP(t, pop->cell_grid, NC); d.cell_grid = t; }
     { int32_t* t; UP(t, pop->cell_start, NC + 1); d.cell_start = t; }
+    for (size_t m = 0; m < NC; m++)
+        c->max_cell_people = std::max(c->max_cell_people, pop->cell_start[m + 1] - pop->cell_start[m]);
     { int32_t* t; UP(t, pop->cell_members, N); d.cell_members = t; }
     size_t ksz = (size_t)params->kernel_size + 1;
     { double* t; UP(t, pop->kernel_lookup, ksz); d.klookup = t; }
@@ -2535,6 +2551,7 @@ int cs_gpu_create_replica(const cs_gpu_ctx* base, cs_gpu_ctx** out)
     c->d = base->d;           // static pointers and sizes; dynamic ones are replaced below
     c->Ng = base->Ng; c->Bg = base->Bg; c->Bpart = base->Bpart; c->rowN = base->rowN;
     c->Gtab = base->Gtab;
+    c->max_cell_people = base->max_cell_people;
     DevPop& d = c->d;
     {
         PersonHot* ph;
@@ -2571,6 +2588,7 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     if (c->d_seed_list) cudaFree(c->d_seed_list);
     if (c->d_ev) cudaFree(c->d_ev);
     if (c->d_mc) cudaFree(c->d_mc);
+    if (c->pack16) cudaFree(c->pack16);
     cudaStream_t own = c->own_stream ? c->own_stream : c->stream;   // never a batch's stream
     if (own) cudaStreamDestroy(own);
     delete c;
@@ -2828,7 +2846,8 @@ static int build_active(cs_gpu_ctx* c, int mode)
     DevPop& d = c->d;
     // the list counters are zero here: every sweep (and begin_run, upload_state,
     // seed_infections) ends by zeroing them
-    LAUNCH(k_build_active, (d.NC + kThreads - 1) / kThreads, kThreads, d, mode);
+    const int ntiles = (d.NC + kThreads - 1) / kThreads;
+    LAUNCH(k_build_active, ntiles * std::max(1, c->grid / ntiles), kThreads, d, mode);
     return CS_OK;
 }
 
@@ -3759,6 +3778,39 @@ int cs_gpu_get_sample(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t
         if (R) CK(cudaMemcpyAsync(R, d.R, n, cudaMemcpyDeviceToHost, c->stream));
         if (D) CK(cudaMemcpyAsync(D, d.D, n, cudaMemcpyDeviceToHost, c->stream));
     }
+    CK(cudaMemsetAsync(d.C, 0, 5 * sizeof(int64_t), c->stream));  // S..D recomputed below
+    LAUNCH(k_cell_totals, 64, kThreads, d);
+    CK(cudaMemcpyAsync(out, d.C, sizeof(cs_counters), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (out->err_queue_overflow || out->err_spatial_tries || out->err_kernel_range)
+        return set_err(c, CS_E_OVERFLOW, "bounded device loop gave up (spatial %lld, queue %lld, kernel range %lld)",
+                       (long long)out->err_spatial_tries, (long long)out->err_queue_overflow, (long long)out->err_kernel_range);
+    return CS_OK;
+}
+
+// S, L, I, R, D of every cell as 16-bit values side by side: half the bytes of
+// cs_gpu_get_sample's copy, for populations whose cells hold at most 65,535 people.
+__global__ void k_pack_cells16(DevPop d, uint16_t* __restrict__ out)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        out[c] = (uint16_t)d.S[c];
+        out[d.NC + c] = (uint16_t)d.L[c];
+        out[2 * d.NC + c] = (uint16_t)d.I[c];
+        out[3 * d.NC + c] = (uint16_t)d.R[c];
+        out[4 * d.NC + c] = (uint16_t)d.D[c];
+    }
+}
+
+int cs_gpu_get_sample16(cs_gpu_ctx* c, uint16_t* cells, cs_counters* out)
+{
+    if (!c || !cells || !out) return CS_E_ARG;
+    DevPop& d = c->d;
+    if (c->max_cell_people > 65535)
+        return set_err(c, CS_E_RANGE, "get_sample16: a cell holds %d people, more than 16 bits count",
+                       c->max_cell_people);
+    if (!c->pack16) CK(cudaMalloc(&c->pack16, sizeof(uint16_t) * 5 * (size_t)d.NC));
+    LAUNCH(k_pack_cells16, (d.NC + kThreads - 1) / kThreads, kThreads, d, (uint16_t*)c->pack16);
+    CK(cudaMemcpyAsync(cells, c->pack16, sizeof(uint16_t) * 5 * (size_t)d.NC, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemsetAsync(d.C, 0, 5 * sizeof(int64_t), c->stream));  // S..D recomputed below
     LAUNCH(k_cell_totals, 64, kThreads, d);
     CK(cudaMemcpyAsync(out, d.C, sizeof(cs_counters), cudaMemcpyDeviceToHost, c->stream));

@@ -111,6 +111,8 @@ struct Pinned {
 
 Pinned<int32_t> g_cells5;                     // S, L, I, R, D of every cell, side by side
 int32_t *g_S = nullptr, *g_L = nullptr, *g_I = nullptr, *g_R = nullptr, *g_D = nullptr;
+Pinned<uint16_t> g_cells16;                   // the same as 16-bit values, when every cell fits
+bool g_use16 = false;
 cs_params g_params;
 // what the device holds of the host's intervention state
 std::vector<uint8_t> g_sd, g_mr;              // per microcell: socdist, moverest (TreatStat)
@@ -389,6 +391,12 @@ void create_context()
     check(rc, "cs_gpu_create");
     g_cells5.resize(5 * (size_t)NC);
     g_S = g_cells5.data(); g_L = g_S + NC; g_I = g_L + NC; g_R = g_I + NC; g_D = g_R + NC;
+    {   // the copies back travel as 16-bit counts when no cell holds more than 65,535 people
+        int most = 0;
+        for (int c = 0; c < NC; c++) most = CellLookup[c]->n > most ? CellLookup[c]->n : most;
+        g_use16 = most <= 65535;
+        if (g_use16) g_cells16.resize(5 * (size_t)NC);
+    }
     std::fprintf(stderr, "GPU sweep: %d people, %d populated cells on device\n", N, NC);
 }
 
@@ -487,12 +495,23 @@ void upload_run_state(int run)
 void sync_back()
 {
     cs_counters k;
-    check(cs_gpu_get_sample(g_ctx, g_S, g_L, g_I, g_R, g_D, &k), "cs_gpu_get_sample");
+    const int NC = P.NumPopulatedCells;
+    if (g_use16) check(cs_gpu_get_sample16(g_ctx, g_cells16.data(), &k), "cs_gpu_get_sample16");
+    else check(cs_gpu_get_sample(g_ctx, g_S, g_L, g_I, g_R, g_D, &k), "cs_gpu_get_sample");
     const double t_sc = omp_get_wtime();
+    if (g_use16) {
+        const uint16_t* v = g_cells16.data();
 #pragma omp parallel for schedule(static)
-    for (int c = 0; c < P.NumPopulatedCells; c++) {
-        Cell* x = CellLookup[c];
-        x->S = g_S[c]; x->L = g_L[c]; x->I = g_I[c]; x->R = g_R[c]; x->D = g_D[c];
+        for (int c = 0; c < NC; c++) {
+            Cell* x = CellLookup[c];
+            x->S = v[c]; x->L = v[NC + c]; x->I = v[2 * NC + c]; x->R = v[3 * NC + c]; x->D = v[4 * NC + c];
+        }
+    } else {
+#pragma omp parallel for schedule(static)
+        for (int c = 0; c < NC; c++) {
+            Cell* x = CellLookup[c];
+            x->S = g_S[c]; x->L = g_L[c]; x->I = g_I[c]; x->R = g_R[c]; x->D = g_D[c];
+        }
     }
     if (!g_timing.empty()) g_timing.back().scatter += omp_get_wtime() - t_sc;
     PopVar& s = StateT[0];
@@ -582,18 +601,15 @@ void mirror_host_interventions(double t)
 {
     const double t_prev = t - P.ModelTimeStep;   // the time TreatSweep last ran at
     if (t_prev >= 0) unsupported_at(t_prev);
-    // the parameter block.  The reference changes parameters only in RecordSample
-    // (ControlPropCasesId after the alert, src/CovidSim.cpp:3592) and UpdateCFRs (the
-    // CFR scales, :2840-2867), both run just before an output step's first
-    // timestep, and seasonality is read per day (src/Sweep.cpp:296).  The whole block
-    // is rebuilt and compared at a realisation's first step and at each output
-    // step's first; every step compares the fields that can move.
+    // the parameter block.  During a run the reference changes parameters only in
+    // RecordSample (ControlPropCasesId after the alert, src/CovidSim.cpp:3592) and
+    // UpdateCFRs (the CFR scales, :2840-2867), and seasonality is read per day
+    // (src/Sweep.cpp:296); the efficacies are fixed after reading.  The whole block
+    // is built at a realisation's first timestep; every timestep compares the
+    // fields that can move and hands over a change.
     const double seas = P.DoSeasonality ? P.Seasonality[((int)t) % DAYS_PER_YEAR] : 1.0;
-    const bool boundary = g_step_in_run % P.NumModelTimeStepsPerOutputTimeStep == 0;
-    if (boundary || seas != g_params.Seasonality || P.ControlPropCasesId != g_params.ControlPropCasesId ||
-        P.CFR_Critical_Scale_Current != g_params.CFR_Critical_Scale_Current ||
-        P.CFR_SARI_Scale_Current != g_params.CFR_SARI_Scale_Current ||
-        P.CFR_ILI_Scale_Current != g_params.CFR_ILI_Scale_Current) {
+    const int dc_gate = P.FalsePositiveRate > 0 ? State.cumDC : 0;   // RecordSample's, read by DoFalseCase
+    if (g_step_in_run == 0) {   // a realisation's first timestep: the whole block
         cs_params cur = params_from_reference();
         cur.kernel_delta = g_params.kernel_delta;
         cur.Seasonality = seas;
@@ -601,6 +617,18 @@ void mirror_host_interventions(double t)
             g_params = cur;
             check(cs_gpu_set_params(g_ctx, &g_params), "cs_gpu_set_params");
         }
+    } else if (seas != g_params.Seasonality || P.ControlPropCasesId != g_params.ControlPropCasesId ||
+               P.CFR_Critical_Scale_Current != g_params.CFR_Critical_Scale_Current ||
+               P.CFR_SARI_Scale_Current != g_params.CFR_SARI_Scale_Current ||
+               P.CFR_ILI_Scale_Current != g_params.CFR_ILI_Scale_Current || dc_gate != g_params.cumDC_at_sample) {
+        // the fields the run loop moves; nothing else in the block changes during a run
+        g_params.Seasonality = seas;
+        g_params.ControlPropCasesId = P.ControlPropCasesId;
+        g_params.CFR_Critical_Scale_Current = P.CFR_Critical_Scale_Current;
+        g_params.CFR_SARI_Scale_Current = P.CFR_SARI_Scale_Current;
+        g_params.CFR_ILI_Scale_Current = P.CFR_ILI_Scale_Current;
+        g_params.cumDC_at_sample = dc_gate;
+        check(cs_gpu_set_params(g_ctx, &g_params), "cs_gpu_set_params");
     }
     // case isolation and household quarantine windows of each admin unit
     // (RecordSample, src/CovidSim.cpp:3598-3609; read by DoDetectedCase)

@@ -624,6 +624,10 @@ int cs_gpu_get_cell_counts(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, 
  * n_cells, ..., D = R + n_cells) they arrive in a single copy. */
 int cs_gpu_get_sample(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32_t* R, int32_t* D,
                       cs_counters* out);
+/* cs_gpu_get_sample with the five cell arrays as 16-bit values side by side in
+ * cells[5 * n_cells] (S, L, I, R, D): half the bytes to copy.  CS_E_RANGE when a cell
+ * holds more than 65,535 people. */
+int cs_gpu_get_sample16(cs_gpu_ctx* ctx, uint16_t* cells, cs_counters* out);
 /* Page-locked host memory (NULL on failure) for a host's staging buffers: copies
  * between it and the device run at the link's full rate and never through an
  * intermediate buffer.  Free with cs_host_free. */

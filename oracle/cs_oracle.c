@@ -2564,3 +2564,18 @@ void cs_cpu_setup_destroy(cs_cpu_setup* s)
     }
     free(s);
 }
+
+/* S, L, I, R, D of every cell as 16-bit values side by side (cs_gpu_get_sample16). */
+int cs_cpu_get_cells16(cs_cpu_ctx* c, uint16_t* out)
+{
+    const int NC = c->NC;
+    for (int k = 0; k < NC; k++) {
+        if (c->cell_start[k + 1] - c->cell_start[k] > 65535) return fail(c, CS_E_RANGE, "a cell holds more than 65535 people");
+        out[k] = (uint16_t)c->S[k];
+        out[NC + k] = (uint16_t)c->L[k];
+        out[2 * NC + k] = (uint16_t)c->I[k];
+        out[3 * NC + k] = (uint16_t)c->R[k];
+        out[4 * NC + k] = (uint16_t)c->D[k];
+    }
+    return CS_OK;
+}

@@ -64,6 +64,8 @@ int cs_cpu_build_kernel_table(int kernel_type, double scale, double shape, doubl
                               double longest_d2, int size, int expansion, double* lookup_out,
                               double* hi_res_out, double* delta_out);
 
+int cs_cpu_get_cells16(cs_cpu_ctx* ctx, uint16_t* out);
+
 /* Population set-up, restated: the same results as cs_gpu_setup_run on the same
  * spec, array for array. */
 typedef struct cs_cpu_setup cs_cpu_setup;

@@ -64,3 +64,9 @@ int cs_gpu_get_sample(cs_gpu_ctx* c, int32_t* S, int32_t* L, int32_t* I, int32_t
 
 void* cs_host_alloc(size_t bytes) { return malloc(bytes ? bytes : 1); }
 void cs_host_free(void* p) { free(p); }
+
+int cs_gpu_get_sample16(cs_gpu_ctx* c, uint16_t* cells, cs_counters* out)
+{
+    int r = cs_cpu_get_cells16((cs_cpu_ctx*)c, cells);
+    return r ? r : cs_cpu_get_counters((cs_cpu_ctx*)c, out);
+}

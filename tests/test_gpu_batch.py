@@ -110,3 +110,42 @@ def test_autotuner_picks_a_setting_and_keeps_results():
     s.run(41, days=10, n_seed=20)
     _same(snapshot(s.backend, pop), want, "after tuning")
     s.close()
+
+
+def test_ensemble_split_by_realisation_gives_the_same_members():
+    """The multi-GPU ensemble split (bench.py ensemble_share: every world-th member to
+    each rank) on one GPU: two batches, one per rank's share, yield each member's
+    daily series exactly as one batch holding every member does, so gathering the
+    ranks' series reproduces the single-process ensemble."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location("_bench", os.path.join(os.path.dirname(os.path.dirname(
+        os.path.abspath(__file__))), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    pop, P, lk, hr = tiny_world()
+    n, world, days = 5, 2, 25
+    seeds = [3100 + 7 * k for k in range(n)]
+    policy = sim.InterventionPolicy(threshold=2, duration=10.0)
+
+    def members(idx):
+        base = sim.Simulation(pop, P, lk, hr)
+        return [base] + [base.replica() for _ in idx[1:]]
+    everyone = members(list(range(n)))
+    whole = sim.Batch(everyone).run(seeds, days, n_seed=20, policy=policy)
+    shares = [bench.ensemble_share(n, r, world) for r in range(world)]
+    got = [None] * n
+    for share in shares:
+        ms = members(share)
+        out = sim.Batch(ms).run([seeds[k] for k in share], days, n_seed=20, policy=policy)
+        for k, ser in zip(share, out):
+            got[k] = ser
+        for m in ms:
+            m.close()
+    for k in range(n):
+        for key in whole[k]:
+            assert np.array_equal(whole[k][key], got[k][key]), "member %d: %s differs" % (k, key)
+    assert sorted(sum(shares, [])) == list(range(n))
+    assert max(int(whole[k]["cumI"][-1]) for k in range(n)) > 500
+    for m in everyone:
+        m.close()
