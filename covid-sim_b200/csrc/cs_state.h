@@ -124,6 +124,14 @@ struct DevPop {
     uint16_t* critical_time;
     uint16_t* stepdown_time;
     uint16_t* detected_time;
+    // Each latent or infectious person's next transition time: the least of the
+    // times IncubRecoverySweep tests (latent_time; case onset, recovery and the
+    // severity times) that is not yet past, 0xFFFF when none is.  The transition
+    // gather reads it alone; k_incub_events re-tests the person's own times.
+    // ev_init, when nonzero, has the next gather form it from those times (set by
+    // a state upload or run reset).
+    uint16_t* next_ev;
+    int32_t* ev_init;
     float* prob_absent;
     float* prob_care;
     int32_t* infector;

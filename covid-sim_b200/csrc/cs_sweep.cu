@@ -183,6 +183,7 @@ struct cs_gpu_ctx {
     std::vector<void*>* alloc_to = nullptr;  // where dalloc records allocations (null: allocs)
     int max_cell_people = 0;   // the largest cell's population (cs_gpu_get_sample16's limit)
     void* pack16 = nullptr;    // device staging of cs_gpu_get_sample16
+    void* packed = nullptr;    // device staging of cs_gpu_get_sample_packed
     cudaStream_t own_stream = nullptr;     // the context's stream while a batch lends it another
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;           // the place pass's branch beside the spatial pass
@@ -214,6 +215,7 @@ struct cs_gpu_ctx {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<cudaGraphNode_t> set_step_nodes;
+    std::vector<cudaKernelNodeParams> set_step_params;   // their launch parameters, read once at capture
     long long graph_launches = 0;
     // device-side run loop: one graph per day (cs_gpu_run)
     DayCtl* d_ctl = nullptr;
@@ -382,6 +384,7 @@ static int build_block_bounds(cs_gpu_ctx* c);
 // ================================================================ run start
 __global__ void k_reset_people(DevPop d, uint64_t seed)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.ev_init = 1;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.N; p += gridDim.x * blockDim.x) {
         Stream s(seed, CS_RNG_RUN_INIT, 0, (uint32_t)p, 0);
         PersonHot h = d.hot[p];
@@ -399,6 +402,7 @@ __global__ void k_reset_people(DevPop d, uint64_t seed)
         d.infection_time[p] = 0;
         d.recovery_time[p] = 0;
         d.sari_time[p] = d.critical_time[p] = d.stepdown_time[p] = kNever;
+        d.next_ev[p] = 0xFFFF;
         d.detected_time[p] = 0;
         d.prob_absent[p] = (float)s.next();
         d.prob_care[p] = (float)s.next();
@@ -1248,6 +1252,7 @@ __device__ __forceinline__ void k_apply_infections_body(const DevPop& d)
         } else
             h.latent_time = (uint16_t)(t * P.TimeStepsPerDay);
         d.hot[p] = h;
+        d.next_ev[p] = h.latent_time;
         if (infector >= 0) {
             sum_tg += ((int)(uint16_t)ts) - ((int)d.infection_time[infector]);
             sum_si += ((int)h.latent_time) - ((int)d.hot[infector].latent_time);
@@ -1562,6 +1567,53 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
     return 2;
 }
 
+// An infectious person's next transition time after (strict) or from step ts: the
+// least of the times infectious_events tests that is above (or at) ts, 0xFFFF when
+// none is.  The times are compared as IncubRecoverySweep compares them, 16-bit.
+__device__ __forceinline__ uint16_t next_infectious_time(const DevPop& d, const cs_params& P, int p, uint16_t latent_time,
+                                                         int ts, bool strict)
+{
+    const int lo = strict ? ts + 1 : ts;
+    const int delay = (int)(P.LatentToSymptDelay / P.ModelTimeStep);
+    int best = 0xFFFF;
+    auto take = [&](int x) { if (x >= lo && x < best) best = x; };
+    take((uint16_t)(latent_time + delay));
+    take(d.recovery_time[p]);
+    if (P.DoSeverity) {
+        take(d.sari_time[p]);
+        take(d.critical_time[p]);
+        take(d.stepdown_time[p]);
+    }
+    return (uint16_t)best;
+}
+
+// The gather's test from the person's own times, forming next_ev on the way (the
+// first gather after an upload or reset); kept out of line, off the common path.
+// (The arrays come as pointers: a DevPop passed by reference to an out-of-line
+// function would be copied to every thread's stack.)
+__device__ __noinline__ bool gather_test_from_times(const cs_params* __restrict__ P, const PersonHot* hot,
+                                                    const uint16_t* const* times, uint16_t* next_ev, int p, int ts)
+{
+    const int delay = (int)(P->LatentToSymptDelay / P->ModelTimeStep);
+    const PersonHot h = hot[p];
+    if (h.inf == CS_INF_LATENT) {
+        next_ev[p] = h.latent_time;
+        return h.latent_time == ts;
+    }
+    // times: recovery, SARI, critical, stepdown
+    const int v[5] = {(uint16_t)(h.latent_time + delay), times[0][p], P->DoSeverity ? times[1][p] : 0xFFFF,
+                      P->DoSeverity ? times[2][p] : 0xFFFF, P->DoSeverity ? times[3][p] : 0xFFFF};
+    int best = 0xFFFF;
+    bool ev = false;
+    for (int k = 0; k < 5; k++) {
+        if (k >= 2 && !P->DoSeverity) break;
+        if (v[k] == ts) ev = true;
+        if (v[k] >= ts && v[k] < best) best = v[k];
+    }
+    next_ev[p] = (uint16_t)best;
+    return ev;
+}
+
 // Which latent / infectious people have an event this step (latent period ends,
 // case onset, severity change, recovery or death): a light scan that compacts
 // them into cmap so the heavy transition kernel runs only on those.
@@ -1578,7 +1630,7 @@ __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const int ts = d.step->ts;
-    const int delay = (int)(P.LatentToSymptDelay / P.ModelTimeStep);
+    const bool init = *d.ev_init != 0;   // next_ev is formed from the people's own times
     __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads];
     long long people = 0;
     const int ntiles = (d.NC + blockDim.x - 1) / blockDim.x;
@@ -1610,12 +1662,12 @@ __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
                 }
                 p = d.slots[s_first[lo] + (j - s_ofs[lo])];
                 cell = c0 + lo;
-                const PersonHot h = d.hot[p];
-                if (h.inf == CS_INF_LATENT)
-                    ev = h.latent_time == ts;
-                else
-                    ev = (ts == (uint16_t)(h.latent_time + delay)) || (ts == d.recovery_time[p]) ||
-                         (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
+                if (init) {
+                    const uint16_t* times[4] = {d.recovery_time, d.sari_time, d.critical_time, d.stepdown_time};
+                    ev = gather_test_from_times(d.P, d.hot, times, d.next_ev, p, ts);
+                } else {
+                    ev = d.next_ev[p] == ts;
+                }
             }
             const int e = block_reserve2(d.counts + kCntEvents, ev ? 1 : 0, nullptr, 0).x;
             if (ev) {
@@ -1680,6 +1732,7 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
     const uint64_t seed = d.step->seed;
     const DevIv iv = *d.iv;
     int nev = d.counts[kCntEvents];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.ev_init = 0;   // the gather before this formed next_ev
     if (blockIdx.x * blockDim.x >= nev) return;   // a block without work stages nothing
     const bool staged = nev >= kStageMinItems;
     stage_begin(d.C, staged);
@@ -1698,6 +1751,9 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
             if (infectious_events(d, P, iv, p, h, c, t, ts, seed) & 1) {
                 d.pstep[p] = kStepItoRD;
                 add += 1 << 16;
+                d.next_ev[p] = 0xFFFF;
+            } else {
+                d.next_ev[p] = next_infectious_time(d, P, p, h.latent_time, ts, true);
             }
             d.hot[p] = h;
             atomicAdd(d.cnt + c, add);
@@ -1709,6 +1765,9 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
                 d.mark[pos] = 2;
                 atomicAdd(d.cnt + c, 1 << 16);
                 mark_cell(d, c);
+                d.next_ev[p] = 0xFFFF;
+            } else {
+                d.next_ev[p] = next_infectious_time(d, P, p, h.latent_time, ts, true);
             }
         }
     }
@@ -2312,6 +2371,8 @@ static int alloc_dynamic(cs_gpu_ctx* c)
     AL(d.infection_time, N); AL(d.recovery_time, N); AL(d.sari_time, N); AL(d.critical_time, N);
     AL(d.stepdown_time, N); AL(d.detected_time, N); AL(d.prob_absent, N); AL(d.prob_care, N);
     AL(d.infector, N); AL(d.listpos, N); AL(d.infect_type, N); AL(d.pstep, N);
+    AL(d.next_ev, N); AL(d.ev_init, 1);
+    CK(cudaMemsetAsync(d.ev_init, 0xff, sizeof(int32_t), c->stream));
     {   // S, L, I, R, D side by side, so that a host can copy all five at once
         int32_t* cells5;
         AL(cells5, 5 * NC);
@@ -2589,6 +2650,7 @@ void cs_gpu_destroy(cs_gpu_ctx* c)
     if (c->d_ev) cudaFree(c->d_ev);
     if (c->d_mc) cudaFree(c->d_mc);
     if (c->pack16) cudaFree(c->pack16);
+    if (c->packed) cudaFree(c->packed);
     cudaStream_t own = c->own_stream ? c->own_stream : c->stream;   // never a batch's stream
     if (own) cudaStreamDestroy(own);
     delete c;
@@ -2937,13 +2999,17 @@ static int capture_step(cs_gpu_ctx* c, double t, int run)
     std::vector<cudaGraphNode_t> nodes(n);
     CK(cudaGraphGetNodes(g, nodes.data(), &n));
     c->set_step_nodes.clear();
+    c->set_step_params.clear();
     for (cudaGraphNode_t nd : nodes) {
         cudaGraphNodeType ty;
         CK(cudaGraphNodeGetType(nd, &ty));
         if (ty != cudaGraphNodeTypeKernel) continue;
         cudaKernelNodeParams kp;
         CK(cudaGraphKernelNodeGetParams(nd, &kp));
-        if (kp.func == (void*)k_set_step) c->set_step_nodes.push_back(nd);
+        if (kp.func == (void*)k_set_step) {
+            c->set_step_nodes.push_back(nd);
+            c->set_step_params.push_back(kp);
+        }
     }
     CK(cudaGraphInstantiate(&c->graph_exec, g, 0));
     c->graph = g;
@@ -2963,13 +3029,12 @@ int cs_gpu_step(cs_gpu_ctx* c, double t, int run)
     }
     DevPop d = c->d;
     unsigned long long seed = c->seed;
-    for (cudaGraphNode_t nd : c->set_step_nodes) {
+    for (size_t k = 0; k < c->set_step_nodes.size(); k++) {
         void* args[] = {&d, &t, &seed};
-        cudaKernelNodeParams kp;
-        CK(cudaGraphKernelNodeGetParams(nd, &kp));
+        cudaKernelNodeParams kp = c->set_step_params[k];
         kp.kernelParams = args;
         kp.extra = nullptr;
-        CK(cudaGraphExecKernelNodeSetParams(c->graph_exec, nd, &kp));
+        CK(cudaGraphExecKernelNodeSetParams(c->graph_exec, c->set_step_nodes[k], &kp));
     }
     CK(cudaGraphLaunch(c->graph_exec, c->stream));
     c->launches += c->graph_launches;
@@ -3801,6 +3866,50 @@ __global__ void k_pack_cells16(DevPop d, uint16_t* __restrict__ out)
     }
 }
 
+// The counter block (S..D left 0) followed by S, L, I, R, D of every cell as 16-bit
+// values, written by one kernel into one device buffer: one copy per sample.
+__global__ void k_pack_sample(DevPop d, unsigned char* __restrict__ out)
+{
+    if (blockIdx.x == 0) {   // the counters, 8-byte words, S..D (the first five) zero
+        const int64_t* src = reinterpret_cast<const int64_t*>(d.C);
+        int64_t* dst = reinterpret_cast<int64_t*>(out);
+        for (int k = threadIdx.x; k < (int)(sizeof(cs_counters) / 8); k += blockDim.x) dst[k] = k < 5 ? 0 : src[k];
+    }
+    uint16_t* cells = reinterpret_cast<uint16_t*>(out + sizeof(cs_counters));
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.NC; c += gridDim.x * blockDim.x) {
+        cells[c] = (uint16_t)d.S[c];
+        cells[d.NC + c] = (uint16_t)d.L[c];
+        cells[2 * d.NC + c] = (uint16_t)d.I[c];
+        cells[3 * d.NC + c] = (uint16_t)d.R[c];
+        cells[4 * d.NC + c] = (uint16_t)d.D[c];
+    }
+}
+
+size_t cs_gpu_sample_packed_bytes(const cs_gpu_ctx* c)
+{
+    return c ? sizeof(cs_counters) + sizeof(uint16_t) * 5 * (size_t)c->d.NC : 0;
+}
+
+int cs_gpu_get_sample_packed(cs_gpu_ctx* c, void* buf, size_t bytes)
+{
+    if (!c || !buf) return CS_E_ARG;
+    DevPop& d = c->d;
+    const size_t need = cs_gpu_sample_packed_bytes(c);
+    if (bytes < need) return set_err(c, CS_E_ARG, "get_sample_packed: %zu bytes, %zu needed", bytes, need);
+    if (c->max_cell_people > 65535)
+        return set_err(c, CS_E_RANGE, "get_sample_packed: a cell holds %d people, more than 16 bits count",
+                       c->max_cell_people);
+    if (!c->packed) CK(cudaMalloc(&c->packed, need));
+    LAUNCH(k_pack_sample, (d.NC + kThreads - 1) / kThreads, kThreads, d, (unsigned char*)c->packed);
+    CK(cudaMemcpyAsync(buf, c->packed, need, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const cs_counters* out = (const cs_counters*)buf;
+    if (out->err_queue_overflow || out->err_spatial_tries || out->err_kernel_range)
+        return set_err(c, CS_E_OVERFLOW, "bounded device loop gave up (spatial %lld, queue %lld, kernel range %lld)",
+                       (long long)out->err_spatial_tries, (long long)out->err_queue_overflow, (long long)out->err_kernel_range);
+    return CS_OK;
+}
+
 int cs_gpu_get_sample16(cs_gpu_ctx* c, uint16_t* cells, cs_counters* out)
 {
     if (!c || !cells || !out) return CS_E_ARG;
@@ -3973,6 +4082,7 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));
     CK(cudaMemsetAsync(d.cnt, 0, sizeof(int32_t) * d.NC, c->stream));
     CK(cudaMemsetAsync(d.C, 0, sizeof(cs_counters), c->stream));
+    CK(cudaMemsetAsync(d.ev_init, 0xff, sizeof(int32_t), c->stream));   // next_ev from the uploaded times
     // the host seeded the run: its LocationInitialInfection is where radii start
     CK(cudaMemcpyAsync(d.rad_origin, c->hp.LocationInitialInfection, sizeof(double) * 2, cudaMemcpyHostToDevice,
                        c->stream));

@@ -111,7 +111,11 @@ struct Pinned {
 
 Pinned<int32_t> g_cells5;                     // S, L, I, R, D of every cell, side by side
 int32_t *g_S = nullptr, *g_L = nullptr, *g_I = nullptr, *g_R = nullptr, *g_D = nullptr;
-Pinned<uint16_t> g_cells16;                   // the same as 16-bit values, when every cell fits
+// When every cell fits 16 bits: the counter block and S, L, I, R, D of every cell as
+// 16-bit values in one page-locked buffer (one copy per sample), and what the host's
+// cells hold, so that a sample writes only the cells whose counts changed
+Pinned<unsigned char> g_packed;
+std::vector<uint16_t> g_host16;
 bool g_use16 = false;
 cs_params g_params;
 // what the device holds of the host's intervention state
@@ -133,7 +137,9 @@ struct RunTiming {
                                                         // timestep, the copy into the host's cells,
                                                         // the hand-over after TreatSweep
     long scans = 0;                                     // microcell scans of the hand-over
+    double upload_device = 0.0;                         // the upload's part in cs_gpu_upload_state
 };
+double g_upload_device = 0.0;   // the last upload's time in cs_gpu_upload_state
 std::vector<RunTiming> g_timing;
 FILE* g_dump = nullptr;
 
@@ -395,7 +401,10 @@ void create_context()
         int most = 0;
         for (int c = 0; c < NC; c++) most = CellLookup[c]->n > most ? CellLookup[c]->n : most;
         g_use16 = most <= 65535;
-        if (g_use16) g_cells16.resize(5 * (size_t)NC);
+        if (g_use16) {
+            g_packed.resize(cs_gpu_sample_packed_bytes(g_ctx));
+            g_host16.assign(5 * (size_t)NC, 0);
+        }
     }
     std::fprintf(stderr, "GPU sweep: %d people, %d populated cells on device\n", N, NC);
 }
@@ -450,6 +459,11 @@ void upload_run_state(int run)
         std::memcpy(g.slots.data() + g.cell_ofs[c], x->susceptible, sizeof(int32_t) * (size_t)x->n);
         g.cS[c] = x->S; g.cL[c] = x->L; g.cI[c] = x->I; g.cR[c] = x->R; g.cD[c] = x->D; g.S0[c] = x->S0;
         g.tp[c] = x->tot_prob;
+        if (g_use16) {   // what the host's cells hold: the copies back compare against it
+            uint16_t* h = g_host16.data();
+            h[c] = (uint16_t)x->S; h[NC + c] = (uint16_t)x->L; h[2 * NC + c] = (uint16_t)x->I;
+            h[3 * NC + c] = (uint16_t)x->R; h[4 * NC + c] = (uint16_t)x->D;
+        }
     }
     cs_state_view v;
     std::memset(&v, 0, sizeof(v));
@@ -462,7 +476,9 @@ void upload_run_state(int run)
     v.cell_S = g.cS.data(); v.cell_L = g.cL.data(); v.cell_I = g.cI.data(); v.cell_R = g.cR.data(); v.cell_D = g.cD.data();
     v.cell_S0 = g.S0.data(); v.cell_tot_prob = g.tp.data(); v.cell_slots = g.slots.data();
     uint64_t seed = ((uint64_t)(uint32_t)P.runSeed1 << 32) ^ (uint32_t)P.runSeed2 ^ (0x9E3779B97F4A7C15ull * (uint64_t)(run + 1));
+    const double t_up = omp_get_wtime();
     check(cs_gpu_upload_state(g_ctx, seed, &v), "cs_gpu_upload_state");
+    g_upload_device = omp_get_wtime() - t_up;
     // seeding ran DoInfect on the host (thread 0's counters); the device counts from zero
     for (int j = 1; j < P.NumThreads; j++)
         if (StateT[j].cumI || StateT[j].cumC) ERR_CRITICAL("GPU sweep: host counters outside thread 0 at run start\n");
@@ -496,15 +512,26 @@ void sync_back()
 {
     cs_counters k;
     const int NC = P.NumPopulatedCells;
-    if (g_use16) check(cs_gpu_get_sample16(g_ctx, g_cells16.data(), &k), "cs_gpu_get_sample16");
-    else check(cs_gpu_get_sample(g_ctx, g_S, g_L, g_I, g_R, g_D, &k), "cs_gpu_get_sample");
+    if (g_use16) {
+        check(cs_gpu_get_sample_packed(g_ctx, g_packed.data(), g_packed.size()), "cs_gpu_get_sample_packed");
+        std::memcpy(&k, g_packed.data(), sizeof k);
+    } else {
+        check(cs_gpu_get_sample(g_ctx, g_S, g_L, g_I, g_R, g_D, &k), "cs_gpu_get_sample");
+    }
     const double t_sc = omp_get_wtime();
     if (g_use16) {
-        const uint16_t* v = g_cells16.data();
+        // only the cells whose counts changed since the last sample are written: the
+        // host's cells change through these writes alone between uploads
+        const uint16_t* v = reinterpret_cast<const uint16_t*>(g_packed.data() + sizeof(cs_counters));
+        uint16_t* h = g_host16.data();
 #pragma omp parallel for schedule(static)
         for (int c = 0; c < NC; c++) {
+            if (v[c] == h[c] && v[NC + c] == h[NC + c] && v[2 * NC + c] == h[2 * NC + c] &&
+                v[3 * NC + c] == h[3 * NC + c] && v[4 * NC + c] == h[4 * NC + c])
+                continue;
             Cell* x = CellLookup[c];
-            x->S = v[c]; x->L = v[NC + c]; x->I = v[2 * NC + c]; x->R = v[3 * NC + c]; x->D = v[4 * NC + c];
+            x->S = h[c] = v[c]; x->L = h[NC + c] = v[NC + c]; x->I = h[2 * NC + c] = v[2 * NC + c];
+            x->R = h[3 * NC + c] = v[3 * NC + c]; x->D = h[4 * NC + c] = v[4 * NC + c];
         }
     } else {
 #pragma omp parallel for schedule(static)
@@ -793,9 +820,9 @@ void report_timing()
 {
     for (const RunTiming& r : g_timing)
         std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f upload_s=%.6f copyback_s=%.6f"
-                             " wait_s=%.6f scatter_s=%.6f handover_s=%.6f mcell_scans=%ld\n",
+                             " wait_s=%.6f scatter_s=%.6f handover_s=%.6f mcell_scans=%ld upload_device_s=%.6f cell_bytes=%d\n",
                      r.run, P.PopSize, P.NumThreads, r.steps, r.infect, r.incub, r.upload, r.copyback, r.wait, r.scatter,
-                     r.handover, r.scans);
+                     r.handover, r.scans, r.upload_device, g_use16 ? 2 : 4);
 }
 
 }  // namespace
@@ -827,6 +854,7 @@ void InfectSweep(double t, int run)
     }
     g_timing.back().infect += omp_get_wtime() - t0;
     g_timing.back().upload += upload;
+    if (upload > 0.0) g_timing.back().upload_device += g_upload_device;
     g_timing.back().steps++;
 }
 

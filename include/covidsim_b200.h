@@ -628,6 +628,13 @@ int cs_gpu_get_sample(cs_gpu_ctx* ctx, int32_t* S, int32_t* L, int32_t* I, int32
  * cells[5 * n_cells] (S, L, I, R, D): half the bytes to copy.  CS_E_RANGE when a cell
  * holds more than 65,535 people. */
 int cs_gpu_get_sample16(cs_gpu_ctx* ctx, uint16_t* cells, cs_counters* out);
+/* What RecordSample reads, in one copy into one buffer of
+ * cs_gpu_sample_packed_bytes(ctx) bytes (page-locked, from cs_host_alloc, for the
+ * link's rate): the counter block with S..D left 0, then S, L, I, R, D of every cell
+ * as 16-bit values side by side.  CS_E_RANGE when a cell holds more than 65,535
+ * people. */
+size_t cs_gpu_sample_packed_bytes(const cs_gpu_ctx* ctx);
+int cs_gpu_get_sample_packed(cs_gpu_ctx* ctx, void* buf, size_t bytes);
 /* Page-locked host memory (NULL on failure) for a host's staging buffers: copies
  * between it and the device run at the link's full rate and never through an
  * intermediate buffer.  Free with cs_host_free. */

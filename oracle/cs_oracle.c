@@ -2579,3 +2579,8 @@ int cs_cpu_get_cells16(cs_cpu_ctx* c, uint16_t* out)
     }
     return CS_OK;
 }
+
+size_t cs_cpu_sample_packed_bytes(const cs_cpu_ctx* c)
+{
+    return sizeof(cs_counters) + sizeof(uint16_t) * 5 * (size_t)c->NC;
+}

@@ -65,6 +65,7 @@ int cs_cpu_build_kernel_table(int kernel_type, double scale, double shape, doubl
                               double* hi_res_out, double* delta_out);
 
 int cs_cpu_get_cells16(cs_cpu_ctx* ctx, uint16_t* out);
+size_t cs_cpu_sample_packed_bytes(const cs_cpu_ctx* ctx);
 
 /* Population set-up, restated: the same results as cs_gpu_setup_run on the same
  * spec, array for array. */

@@ -70,3 +70,14 @@ int cs_gpu_get_sample16(cs_gpu_ctx* c, uint16_t* cells, cs_counters* out)
     int r = cs_cpu_get_cells16((cs_cpu_ctx*)c, cells);
     return r ? r : cs_cpu_get_counters((cs_cpu_ctx*)c, out);
 }
+
+size_t cs_gpu_sample_packed_bytes(const cs_gpu_ctx* c) { return cs_cpu_sample_packed_bytes((const cs_cpu_ctx*)c); }
+int cs_gpu_get_sample_packed(cs_gpu_ctx* c, void* buf, size_t bytes)
+{
+    if (bytes < cs_cpu_sample_packed_bytes((const cs_cpu_ctx*)c)) return CS_E_ARG;
+    cs_counters* k = (cs_counters*)buf;
+    int r = cs_cpu_get_counters((cs_cpu_ctx*)c, k);
+    if (r) return r;
+    k->S = k->L = k->I = k->R = k->D = 0;
+    return cs_cpu_get_cells16((cs_cpu_ctx*)c, (uint16_t*)((char*)buf + sizeof(cs_counters)));
+}

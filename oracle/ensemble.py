@@ -9,6 +9,8 @@ daily incidence, critical-care and death curves.
 
 Workloads (CONFIGS):
   plain          20,000 people on 24 x 24 cells, 120 days, no interventions;
+  medium         200,000 people at the 1M workload's cell density with the
+                 interventions, people linked to places by a network file;
   holidays       the plain workload with a 30-day holiday from day 25 that closes
                  every school and university (the drop-in hands the reference's
                  holiday choices to the device);
@@ -43,8 +45,16 @@ CONFIGS = {
 CONFIGS["holidays"] = dict(CONFIGS["plain"], admin_extra={
     "Include holidays": 1, "Proportion of places remaining open during holidays by place type": [0.0, 0.0, 0.0, 1.0],
     "Number of holidays": 1, "Holiday start times": [25.0], "Holiday durations": [30.0]})
+# 200,000 people at the 1M workload's cell density (1 x 1 degree, 120 x 120 cells of
+# 10 x 10 microcells) for 200 days with the interventions (trigger above 20 weekly
+# critical-care admissions); people linked to places by a network file (/L) written
+# once per thread count by the network tool, so both arms hold the same network
+CONFIGS["medium"] = dict(people=200000, width_deg=1.0, cell_deg=1.0 / 120, nmcl=10, sigma=1.2, days=200,
+                         realisations=200, setup_seed=98798150, interventions=True, threshold=20, duration=90.0,
+                         network=True)
 CONFIG = CONFIGS["plain"]
-GOLDEN = {"plain": "ref_ensemble.json", "interventions": "ref_ensemble_iv.json", "holidays": "ref_ensemble_hol.json"}
+GOLDEN = {"plain": "ref_ensemble.json", "interventions": "ref_ensemble_iv.json", "holidays": "ref_ensemble_hol.json",
+          "medium": "ref_ensemble_200k.json"}
 
 
 def population(config="plain"):
@@ -61,7 +71,11 @@ def run(binary, nr=None, threads=None, config="plain"):
     import refrun
     c = CONFIGS[config]
     dropin = os.path.basename(binary) != "CovidSim"
-    res = refrun.run_reference(population(config), c["days"], nr=nr or c["realisations"], threads=threads, binary=binary,
+    pop = population(config)
+    extra = ()
+    if c.get("network"):
+        extra = ("/L:" + refrun.network_file(pop, "ensemble_" + config, threads or os.cpu_count()),)
+    res = refrun.run_reference(pop, c["days"], nr=nr or c["realisations"], threads=threads, binary=binary, extra_args=extra,
                                series=True, timeout=5400, interventions=c.get("interventions", False),
                                threshold=c.get("threshold", 100), duration=c.get("duration", 90.0),
                                env={"OMP_WAIT_POLICY": "passive"} if dropin else None, admin_extra=c.get("admin_extra"))

@@ -3,10 +3,10 @@
 oracle/ensemble.py, summarised as final sizes, peak days and ensemble-mean daily
 curves.
 
-    python tests/golden/make_ref_ensemble.py [plain|interventions|holidays]
+    python tests/golden/make_ref_ensemble.py [plain|interventions|holidays|medium]
 
-writes tests/golden/ref_ensemble.json (plain, the default), ref_ensemble_iv.json or
-ref_ensemble_hol.json;
+writes tests/golden/ref_ensemble.json (plain, the default), ref_ensemble_iv.json,
+ref_ensemble_hol.json or ref_ensemble_200k.json;
 CS_THREADS sets the reference's thread count (default: every core)."""
 import json
 import os

@@ -89,3 +89,12 @@ def test_gpu_sweep_with_holidays_matches_reference():
     summary, res = _run(_binary("CovidSim_b200"), "holidays")
     _check(summary, "holidays")
     assert any("people" in ln for ln in res["dropin"]), res["dropin"]
+
+
+@pytest.mark.gpu
+def test_gpu_sweep_at_200k_people_matches_reference():
+    """200,000 people at the 1M workload's cell density with the interventions, 200
+    realisations against 200 of the reference on the same network file."""
+    summary, res = _run(_binary("CovidSim_b200"), "medium")
+    _check(summary, "medium")
+    assert any("people" in ln for ln in res["dropin"]), res["dropin"]
