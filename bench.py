@@ -489,11 +489,16 @@ def e2e_dropin(args, local, world, dist, n_cells):
                                   "handover_after_treatsweep": parts["handover_s"], "infect_calls": parts["infect_s"],
                                   "incub_calls": parts["incub_s"]},
             "handover_microcell_scans_per_step": scans,
+            # RunModel's time stepping per realisation with the host code between the
+            # sweeps (TreatSweep, RecordSample, output), beside the sweep calls alone
+            "run_loop_ms_per_step": round(1e3 * sum(r.get("loop_s", 0.0) for r in rows) / len(rows), 3),
             "what": "the reference executable with the GPU sweep linked in (oracle/_ref/CovidSim_b200), the same "
                     "network file as the reference arm; wall time of the sweep calls per realisation: state upload "
-                    "from the reference's host structures at its start, device sweeps (one graph per timestep, "
-                    "waited for), copy of cell counts and counters back at each output step, intervention "
-                    "hand-over",
+                    "from the reference's host structures at its start, device sweeps (one graph per timestep; "
+                    "the host waits for the device at the last timestep of each output step, the timesteps "
+                    "before it run on while the host runs TreatSweep), copy of cell counts and counters back "
+                    "at each output step, intervention hand-over; run_loop_ms_per_step is RunModel's whole "
+                    "time stepping, the host code between sweeps included, as the reference arm reports it",
             "realisations": len(rows), "host_threads": rows[0]["threads"], "process_wall_s": round(res["wall"], 1),
             "network_file": res.get("network_file")}
 
@@ -590,7 +595,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": desc, "reference_sample": res["sample"], "network_file": res.get("network_file"),
-                   "process_wall_s": round(res["wall"], 1)},
+                   "process_wall_s": round(res["wall"], 1), "run_loop_ms_per_step": res.get("run_loop_ms_per_step")},
         "cpu_baseline": {"value": round(v, 1), "unit": METRIC, "cores": res["cores"], "kind": "reference",
                          "sample": res["sample"]},
         "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -138,6 +138,9 @@ struct RunTiming {
                                                         // the hand-over after TreatSweep
     long scans = 0;                                     // microcell scans of the hand-over
     double upload_device = 0.0;                         // the upload's part in cs_gpu_upload_state
+    double loop_start = -1.0, loop_end = -1.0;          // wall clock at the run's first sweep call and
+                                                        // at the end of its last: RunModel's time
+                                                        // stepping with the host code between sweeps
 };
 double g_upload_device = 0.0;   // the last upload's time in cs_gpu_upload_state
 std::vector<RunTiming> g_timing;
@@ -507,6 +510,10 @@ void upload_run_state(int run)
     }
 }
 
+// Below this many cells the copy into the host's cells runs on one thread: waking
+// the team costs more than the loop.
+constexpr int kParallelCells = 16384;
+
 // RecordSample (src/CovidSim.cpp:3024-3120) reads per-cell counts and StateT[].
 void sync_back()
 {
@@ -524,7 +531,7 @@ void sync_back()
         // host's cells change through these writes alone between uploads
         const uint16_t* v = reinterpret_cast<const uint16_t*>(g_packed.data() + sizeof(cs_counters));
         uint16_t* h = g_host16.data();
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (NC >= kParallelCells)
         for (int c = 0; c < NC; c++) {
             if (v[c] == h[c] && v[NC + c] == h[NC + c] && v[2 * NC + c] == h[2 * NC + c] &&
                 v[3 * NC + c] == h[3 * NC + c] && v[4 * NC + c] == h[4 * NC + c])
@@ -534,7 +541,7 @@ void sync_back()
             x->R = h[3 * NC + c] = v[3 * NC + c]; x->D = h[4 * NC + c] = v[4 * NC + c];
         }
     } else {
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (NC >= kParallelCells)
         for (int c = 0; c < NC; c++) {
             Cell* x = CellLookup[c];
             x->S = g_S[c]; x->L = g_L[c]; x->I = g_I[c]; x->R = g_R[c]; x->D = g_D[c];
@@ -820,9 +827,9 @@ void report_timing()
 {
     for (const RunTiming& r : g_timing)
         std::fprintf(stderr, "\nSWEEPTIMING run=%d pop=%d threads=%d steps=%ld infect_s=%.6f incub_s=%.6f upload_s=%.6f copyback_s=%.6f"
-                             " wait_s=%.6f scatter_s=%.6f handover_s=%.6f mcell_scans=%ld upload_device_s=%.6f cell_bytes=%d\n",
+                             " wait_s=%.6f scatter_s=%.6f handover_s=%.6f mcell_scans=%ld upload_device_s=%.6f cell_bytes=%d loop_s=%.6f\n",
                      r.run, P.PopSize, P.NumThreads, r.steps, r.infect, r.incub, r.upload, r.copyback, r.wait, r.scatter,
-                     r.handover, r.scans, r.upload_device, g_use16 ? 2 : 4);
+                     r.handover, r.scans, r.upload_device, g_use16 ? 2 : 4, r.loop_end - r.loop_start);
 }
 
 }  // namespace
@@ -851,6 +858,7 @@ void InfectSweep(double t, int run)
     if (g_timing.empty() || g_timing.back().run != run) {
         g_timing.push_back(RunTiming());
         g_timing.back().run = run;
+        g_timing.back().loop_start = t0;
     }
     g_timing.back().infect += omp_get_wtime() - t0;
     g_timing.back().upload += upload;
@@ -927,21 +935,32 @@ void cs_shim_DoPlaceOpen(int i, int j, unsigned short int TimeStepNow)
 }
 
 
+// The timestep's device work runs on while the host goes on to TreatSweep: the host
+// reads nothing the sweeps change until RecordSample, at the start of the next
+// output step, so the wait for the device comes at the last timestep of each output
+// step (and at every step of a run with a limit on infections, whose test reads
+// State.cumI each step).  What the host hands the device in between (parameters,
+// place events, microcell status) is copied from pageable memory in stream order,
+// behind the work in flight.  RunModel stops calling the sweeps mid-output-step only
+// once State.L + State.I was 0 at the last RecordSample, after which no sweep changes
+// anything.
 void IncubRecoverySweep(double t)
 {
     const double t0 = omp_get_wtime();
     (void)t;
-    check(cs_gpu_sync(g_ctx), "cs_gpu_sync");   // the timestep's device work, all of it timed
-    if (!g_timing.empty()) g_timing.back().wait += omp_get_wtime() - t0;
-    // RecordSample reads the cells and counters at the start of the next output step.
-    // RunModel stops calling the sweeps mid-output-step only once State.L + State.I
-    // was 0 at the last RecordSample, after which no sweep changes anything; a run
-    // with a limit on infections is copied back every step all the same
     g_step_in_run++;
     const bool output_step = g_step_in_run % P.NumModelTimeStepsPerOutputTimeStep == 0;
-    const double t1 = omp_get_wtime();
-    if (P.LimitNumInfections || output_step) sync_back();
-    if (output_step) dump_block();
-    if (!g_timing.empty()) g_timing.back().copyback += omp_get_wtime() - t1;
-    if (!g_timing.empty()) g_timing.back().incub += omp_get_wtime() - t0;
+    const bool read_back = P.LimitNumInfections || output_step;
+    if (read_back) {
+        check(cs_gpu_sync(g_ctx), "cs_gpu_sync");   // the output step's device work, all of it timed
+        if (!g_timing.empty()) g_timing.back().wait += omp_get_wtime() - t0;
+        const double t1 = omp_get_wtime();
+        sync_back();
+        if (output_step) dump_block();
+        if (!g_timing.empty()) g_timing.back().copyback += omp_get_wtime() - t1;
+    }
+    if (!g_timing.empty()) {
+        g_timing.back().incub += omp_get_wtime() - t0;
+        g_timing.back().loop_end = omp_get_wtime();
+    }
 }

@@ -199,7 +199,10 @@ def time_reference(workload, steps=3, warmup=3, binary=BIN, threads=None, env=No
         return {"unavailable": "reference produced %d timed realisations" % len(rows)}
     person_steps = sum(r["pop"] * r["steps"] for r in rows)
     secs = sum(r["infect_s"] + r["incub_s"] for r in rows)
+    # RunModel's time stepping per realisation, the host code between sweeps included
+    loop = [r["loop_s"] for r in rows if "loop_s" in r]
     return {"value": person_steps / secs, "ms_per_step": 1e3 * secs / steps, "cores": res["threads"],
+            "run_loop_ms_per_step": round(1e3 * sum(loop) / len(loop), 3) if loop else None,
             "sample": s["note"] + "; %d realisations after %d warm-up, sweep wall time (omp_get_wtime), %d threads"
                       % (steps, warmup, res["threads"]), "rows": rows, "wall": res["wall"], "dropin": res.get("dropin"),
             "network_file": os.path.basename(extra[0][3:]) if extra else None}
