@@ -1357,9 +1357,37 @@ __device__ __forceinline__ void sev_add(const DevPop& d, int ad, int which, int 
     }
 }
 
-// DoIncub (src/Update.cpp:408-523) for one person, on a register copy of the record.
-__device__ void do_incub(const DevPop& d, const cs_params& P, int p, PersonHot& h, int ts, uint64_t seed)
+// An infectious person's times that IncubRecoverySweep tests besides case onset
+// (latent_time + delay), held in registers through the person's transitions.
+struct PersonTimes {
+    uint16_t rec, sari, crit, sd;
+};
+
+__device__ __forceinline__ PersonTimes load_times(const DevPop& d, const cs_params& P, int p)
 {
+    PersonTimes tm;
+    tm.rec = d.recovery_time[p];
+    if (P.DoSeverity) {
+        tm.sari = d.sari_time[p];
+        tm.crit = d.critical_time[p];
+        tm.sd = d.stepdown_time[p];
+    } else {
+        tm.sari = tm.crit = tm.sd = 0xFFFF;
+    }
+    return tm;
+}
+
+// DoIncub (src/Update.cpp:408-523) for one person, on a register copy of the record;
+// tm returns the person's times as written.
+__device__ void do_incub(const DevPop& d, const cs_params& P, int p, PersonHot& h, int ts, uint64_t seed, PersonTimes& tm)
+{
+    if (P.DoSeverity) {   // the times this call leaves unset keep their values
+        tm.sari = d.sari_time[p];
+        tm.crit = d.critical_time[p];
+        tm.sd = d.stepdown_time[p];
+    } else {
+        tm.sari = tm.crit = tm.sd = 0xFFFF;
+    }
     int age = age_group(h);
     if (age >= CS_NUM_AGE_GROUPS) age = CS_NUM_AGE_GROUPS - 1;
     Stream s(seed, CS_RNG_INCUB, (uint32_t)ts, (uint32_t)p, 0);
@@ -1380,9 +1408,9 @@ __device__ void do_incub(const DevPop& d, const cs_params& P, int p, PersonHot& 
     double spd = P.TimeStepsPerDay;
     if (!P.DoSeverity || h.inf == CS_INF_INFECTIOUS_ASYMPTOMATIC_NOT_CASE) {
         if (P.DoInfectiousnessProfile)
-            d.recovery_time[p] = (uint16_t)(h.latent_time + (uint16_t)(P.InfectiousPeriod * spd));
+            d.recovery_time[p] = tm.rec = (uint16_t)(h.latent_time + (uint16_t)(P.InfectiousPeriod * spd));
         else
-            d.recovery_time[p] = (uint16_t)(h.latent_time + icdf_choose(P.infectious_icdf, P.InfectiousPeriod, s.next(), spd));
+            d.recovery_time[p] = tm.rec = (uint16_t)(h.latent_time + icdf_choose(P.infectious_icdf, P.InfectiousPeriod, s.next(), spd));
     } else {
         int CaseTime = h.latent_time + ((int)(P.LatentToSymptDelay / P.ModelTimeStep));
         double x = s.next();
@@ -1407,30 +1435,30 @@ __device__ void do_incub(const DevPop& d, const cs_params& P, int p, PersonHot& 
         else if (fin == CS_SEV_CRITICAL) {
             uint16_t sari = (uint16_t)(CaseTime + icdf_choose(P.ILIToSARI_icdf, P.Mean_ILIToSARI[age], s.next(), spd));
             uint16_t crit = (uint16_t)(sari + icdf_choose(P.SARIToCritical_icdf, P.Mean_SARIToCritical[age], s.next(), spd));
-            d.sari_time[p] = sari;
-            d.critical_time[p] = crit;
+            d.sari_time[p] = tm.sari = sari;
+            d.critical_time[p] = tm.crit = crit;
             if (to_die) {
                 if (P.IncludeStepDownToDeath == 1) {
                     uint16_t sd = (uint16_t)(crit + icdf_choose(P.CriticalToCritRecov_icdf, P.Mean_CriticalToCritRecov[age], s.next(), spd));
-                    d.stepdown_time[p] = sd;
+                    d.stepdown_time[p] = tm.sd = sd;
                     rec = (uint16_t)(sd + icdf_choose(P.StepdownToDeath_icdf, P.Mean_StepdownToDeath[age], s.next(), spd));
                 } else
                     rec = (uint16_t)(crit + icdf_choose(P.CriticalToDeath_icdf, P.Mean_CriticalToDeath[age], s.next(), spd));
             } else {
                 uint16_t sd = (uint16_t)(crit + icdf_choose(P.CriticalToCritRecov_icdf, P.Mean_CriticalToCritRecov[age], s.next(), spd));
-                d.stepdown_time[p] = sd;
+                d.stepdown_time[p] = tm.sd = sd;
                 rec = (uint16_t)(sd + icdf_choose(P.CritRecovToRecov_icdf, P.Mean_CritRecovToRecov[age], s.next(), spd));
             }
         } else if (fin == CS_SEV_SARI) {
             uint16_t sari = (uint16_t)(CaseTime + icdf_choose(P.ILIToSARI_icdf, P.Mean_ILIToSARI[age], s.next(), spd));
-            d.sari_time[p] = sari;
+            d.sari_time[p] = tm.sari = sari;
             if (to_die) rec = (uint16_t)(sari + icdf_choose(P.SARIToDeath_icdf, P.Mean_SARIToDeath[age], s.next(), spd));
             else rec = (uint16_t)(sari + icdf_choose(P.SARIToRecovery_icdf, P.Mean_SARIToRecovery[age], s.next(), spd));
         } else {
             if (to_die) rec = (uint16_t)(CaseTime + icdf_choose(P.ILIToDeath_icdf, P.Mean_ILIToDeath[age], s.next(), spd));
             else rec = (uint16_t)(CaseTime + icdf_choose(P.ILIToRecovery_icdf, P.Mean_ILIToRecovery[age], s.next(), spd));
         }
-        d.recovery_time[p] = rec;
+        d.recovery_time[p] = tm.rec = rec;
     }
     if (h.inf == CS_INF_INFECTIOUS_ALMOST_SYMPTOMATIC && ((P.ControlPropCasesId == 1) || (s.next() < P.ControlPropCasesId))) {
         h.dflags |= CS_DF_DETECTED;
@@ -1519,21 +1547,21 @@ __device__ void do_case(const DevPop& d, const cs_params& P, const DevIv& iv, in
 // Returns bit 0 when the person leaves the infectious block this step and bit 1
 // when any event fired (the record must be written back).
 __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevIv& iv, int p, PersonHot& h, int cell,
-                                 double t, int ts, uint64_t seed)
+                                 double t, int ts, uint64_t seed, const PersonTimes& tm)
 {
     int CaseTime = h.latent_time + ((int)(P.LatentToSymptDelay / P.ModelTimeStep));
-    uint16_t rec = d.recovery_time[p];
+    const uint16_t rec = tm.rec;
     bool any = (ts == (uint16_t)CaseTime) || (ts == rec) ||
-               (P.DoSeverity && (ts == d.sari_time[p] || ts == d.critical_time[p] || ts == d.stepdown_time[p]));
+               (P.DoSeverity && (ts == tm.sari || ts == tm.crit || ts == tm.sd));
     if (!any) return 0;
     if (P.DoSymptoms && ts == (uint16_t)CaseTime) do_case(d, P, iv, p, h, t, ts, seed);
     bool to_die = (h.dflags & CS_DF_TO_DIE) != 0;
     int ad = d.mcell_adunit[h.mcell];
     if (P.DoSeverity) {
         int cur = h.sev & 0x0f;
-        if (ts == d.sari_time[p] && cur == CS_SEV_ILI) { cur = CS_SEV_SARI; sev_add(d, ad, CS_SEV_ILI, -1, false); sev_add(d, ad, CS_SEV_SARI, 1, true); }
-        if (ts == d.critical_time[p] && cur == CS_SEV_SARI) { cur = CS_SEV_CRITICAL; sev_add(d, ad, CS_SEV_SARI, -1, false); sev_add(d, ad, CS_SEV_CRITICAL, 1, true); }
-        if (ts == d.stepdown_time[p] && cur == CS_SEV_CRITICAL && !to_die) { cur = CS_SEV_STEPDOWN; sev_add(d, ad, CS_SEV_CRITICAL, -1, false); sev_add(d, ad, CS_SEV_STEPDOWN, 1, true); }
+        if (ts == tm.sari && cur == CS_SEV_ILI) { cur = CS_SEV_SARI; sev_add(d, ad, CS_SEV_ILI, -1, false); sev_add(d, ad, CS_SEV_SARI, 1, true); }
+        if (ts == tm.crit && cur == CS_SEV_SARI) { cur = CS_SEV_CRITICAL; sev_add(d, ad, CS_SEV_SARI, -1, false); sev_add(d, ad, CS_SEV_CRITICAL, 1, true); }
+        if (ts == tm.sd && cur == CS_SEV_CRITICAL && !to_die) { cur = CS_SEV_STEPDOWN; sev_add(d, ad, CS_SEV_CRITICAL, -1, false); sev_add(d, ad, CS_SEV_STEPDOWN, 1, true); }
         if (ts == rec) {
             if (to_die) {
                 if (cur == CS_SEV_CRITICAL) { sev_add(d, ad, CS_SEV_CRITICAL, -1, false); cnt_add(CSB_STAGED(cumDeath_Critical), 1); cur = CS_SEV_DEAD; }
@@ -1570,7 +1598,7 @@ __device__ int infectious_events(const DevPop& d, const cs_params& P, const DevI
 // An infectious person's next transition time after (strict) or from step ts: the
 // least of the times infectious_events tests that is above (or at) ts, 0xFFFF when
 // none is.  The times are compared as IncubRecoverySweep compares them, 16-bit.
-__device__ __forceinline__ uint16_t next_infectious_time(const DevPop& d, const cs_params& P, int p, uint16_t latent_time,
+__device__ __forceinline__ uint16_t next_infectious_time(const cs_params& P, uint16_t latent_time, const PersonTimes& tm,
                                                          int ts, bool strict)
 {
     const int lo = strict ? ts + 1 : ts;
@@ -1578,11 +1606,11 @@ __device__ __forceinline__ uint16_t next_infectious_time(const DevPop& d, const 
     int best = 0xFFFF;
     auto take = [&](int x) { if (x >= lo && x < best) best = x; };
     take((uint16_t)(latent_time + delay));
-    take(d.recovery_time[p]);
+    take(tm.rec);
     if (P.DoSeverity) {
-        take(d.sari_time[p]);
-        take(d.critical_time[p]);
-        take(d.stepdown_time[p]);
+        take(tm.sari);
+        take(tm.crit);
+        take(tm.sd);
     }
     return (uint16_t)best;
 }
@@ -1742,24 +1770,26 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
         int pos = d.cell_start[c] + d.listpos[p];
         if (h.inf == CS_INF_LATENT) {
             if (h.latent_time != ts) continue;
-            do_incub(d, P, p, h, ts, seed);
+            PersonTimes tm;
+            do_incub(d, P, p, h, ts, seed, tm);
             atomicSub(d.L + c, 1);
             atomicAdd(d.I + c, 1);
             int add = 1;
             d.mark[pos] = 1;
             cnt_add(CSB_STAGED(work_transitions), 1);
-            if (infectious_events(d, P, iv, p, h, c, t, ts, seed) & 1) {
+            if (infectious_events(d, P, iv, p, h, c, t, ts, seed, tm) & 1) {
                 d.pstep[p] = kStepItoRD;
                 add += 1 << 16;
                 d.next_ev[p] = 0xFFFF;
             } else {
-                d.next_ev[p] = next_infectious_time(d, P, p, h.latent_time, ts, true);
+                d.next_ev[p] = next_infectious_time(P, h.latent_time, tm, ts, true);
             }
             d.hot[p] = h;
             atomicAdd(d.cnt + c, add);
             mark_cell(d, c);
         } else {
-            int r = infectious_events(d, P, iv, p, h, c, t, ts, seed);
+            const PersonTimes tm = load_times(d, P, p);
+            int r = infectious_events(d, P, iv, p, h, c, t, ts, seed, tm);
             if (r & 2) d.hot[p] = h;
             if (r & 1) {
                 d.mark[pos] = 2;
@@ -1767,7 +1797,7 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
                 mark_cell(d, c);
                 d.next_ev[p] = 0xFFFF;
             } else {
-                d.next_ev[p] = next_infectious_time(d, P, p, h.latent_time, ts, true);
+                d.next_ev[p] = next_infectious_time(P, h.latent_time, tm, ts, true);
             }
         }
     }
