@@ -203,8 +203,11 @@ struct DevPop {
 
 // kCntHH is last: the infect sweep zeroes the counters before it (kCntN - 1 of
 // them) and leaves the household list, which its false cases may have filled, to
-// the incub sweep's household pass.
+// the incub sweep's household pass.  The step's transition events are two lists in
+// act / act_cell: latent people from the front (kCntEvents), infectious people
+// from the back (kCntEventsInf), so that a warp of the transition kernel mostly
+// takes one branch.
 enum { kCntQueue = 0, kCntTouched = 1, kCntAct = 2, kCntContacts = 3, kCntPlaceWork = 4, kCntEvents = 5,
-       kCntCarer = 6, kCntFalse = 7, kCntHH = 8, kCntN = 9 };
+       kCntCarer = 6, kCntFalse = 7, kCntEventsInf = 8, kCntHH = 9, kCntN = 10 };
 
 }  // namespace csb

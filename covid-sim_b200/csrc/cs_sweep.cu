@@ -1644,43 +1644,46 @@ __device__ __noinline__ bool gather_test_from_times(const cs_params* __restrict_
 
 // Which latent / infectious people have an event this step (latent period ends,
 // case onset, severity change, recovery or death): a light scan that compacts
-// them into cmap so the heavy transition kernel runs only on those.
+// them so the heavy transition kernel runs only on those.
 // IncubRecoverySweep's scan (src/Sweep.cpp:920-977) over the cells' lists: every
 // latent and infectious person (slots [S, S+L+I) of each cell, read block-
 // cooperatively as k_build_active reads a cell's slots, so a dense cell costs no more
 // than its share of the block) joins the step's event list when one of its times is
 // now.  The cells come in tiles of blockDim.x; Q = gridDim.x / tiles blocks share a
 // tile, block q taking its chunks q, q + Q, ... of blockDim.x entries, so the launch
-// has the parallelism of a flat list without building one.  The list holds (person,
-// cell) in act / act_cell, in no particular order: k_incub_events treats each person
-// on its own.
+// has the parallelism of a flat list without building one.  The lists hold (person,
+// cell) in act / act_cell, latent people from the front and infectious people from
+// the back, in no particular order within each: k_incub_events treats each person on
+// its own.
 __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
 {
     const cs_params& P = *d.P;
     const int ts = d.step->ts;
     const bool init = *d.ev_init != 0;   // next_ev is formed from the people's own times
-    __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads];
+    __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads], s_L[kThreads];
     long long people = 0;
     const int ntiles = (d.NC + blockDim.x - 1) / blockDim.x;
     const int Q = max(1, (int)gridDim.x / ntiles), part = blockIdx.x % Q;
     for (int tile = blockIdx.x / Q; tile < ntiles; tile += max(1, (int)gridDim.x / Q)) {
         const int c0 = tile * blockDim.x;
         const int c = c0 + threadIdx.x;
-        int first = 0, n = 0;
+        int first = 0, n = 0, nl = 0;
         if (c < d.NC) {
             first = d.cell_start[c] + d.S[c];
-            n = d.L[c] + d.I[c];
+            nl = d.L[c];
+            n = nl + d.I[c];
         }
         const int o = block_reserve2(nullptr, n, nullptr, 0).x;   // the block's own prefix of n
         s_first[threadIdx.x] = first;
         s_ofs[threadIdx.x] = o;
         s_n[threadIdx.x] = n;
+        s_L[threadIdx.x] = nl;
         __syncthreads();
         const int total = s_ofs[blockDim.x - 1] + s_n[blockDim.x - 1];
         if (threadIdx.x == 0 && part == 0) people += total;
         for (int j0 = part * blockDim.x; j0 < total; j0 += Q * blockDim.x) {   // block-uniform: every thread reserves
             const int j = j0 + (int)threadIdx.x;
-            bool ev = false;
+            bool ev = false, latent = false;
             int p = 0, cell = 0;
             if (j < total) {
                 int lo = 0, hi = blockDim.x - 1;   // the last cell whose entries start at or before j
@@ -1688,6 +1691,7 @@ __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
                     const int mid = (lo + hi + 1) >> 1;
                     if (s_ofs[mid] <= j) lo = mid; else hi = mid - 1;
                 }
+                latent = j - s_ofs[lo] < s_L[lo];   // the cell's slots run latent, then infectious
                 p = d.slots[s_first[lo] + (j - s_ofs[lo])];
                 cell = c0 + lo;
                 if (init) {
@@ -1697,10 +1701,12 @@ __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
                     ev = d.next_ev[p] == ts;
                 }
             }
-            const int e = block_reserve2(d.counts + kCntEvents, ev ? 1 : 0, nullptr, 0).x;
+            const int2 e = block_reserve2(d.counts + kCntEvents, (ev && latent) ? 1 : 0, d.counts + kCntEventsInf,
+                                          (ev && !latent) ? 1 : 0);
             if (ev) {
-                d.act[e] = p;
-                d.act_cell[e] = cell;
+                const int at = latent ? e.x : d.N - 1 - e.y;
+                d.act[at] = p;
+                d.act_cell[at] = cell;
             }
         }
         __syncthreads();   // the shared arrays are refilled for the next cells
@@ -1759,13 +1765,14 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
     const int ts = d.step->ts;
     const uint64_t seed = d.step->seed;
     const DevIv iv = *d.iv;
-    int nev = d.counts[kCntEvents];
+    const int nlat = d.counts[kCntEvents], nev = nlat + d.counts[kCntEventsInf];
     if (blockIdx.x == 0 && threadIdx.x == 0) *d.ev_init = 0;   // the gather before this formed next_ev
     if (blockIdx.x * blockDim.x >= nev) return;   // a block without work stages nothing
     const bool staged = nev >= kStageMinItems;
     stage_begin(d.C, staged);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) {
-        const int p = d.act[e], c = d.act_cell[e];
+        const int at = e < nlat ? e : d.N - 1 - (e - nlat);   // latent events, then infectious ones
+        const int p = d.act[at], c = d.act_cell[at];
         PersonHot h = d.hot[p];
         int pos = d.cell_start[c] + d.listpos[p];
         if (h.inf == CS_INF_LATENT) {
@@ -1836,8 +1843,9 @@ __device__ __forceinline__ void k_household_after_body(const DevPop& d)
     const int ts = d.step->ts;
     const uint64_t seed = d.step->seed;
     // the step's transition flags are only set on event people: clear them
-    int nev = d.counts[kCntEvents];
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) d.pstep[d.act[e]] = 0;
+    const int nlat = d.counts[kCntEvents], nev = nlat + d.counts[kCntEventsInf];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x)
+        d.pstep[d.act[e < nlat ? e : d.N - 1 - (e - nlat)]] = 0;
     int nh = d.counts[kCntHH];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
         int h = d.hh_list[k];
