@@ -92,13 +92,6 @@ __device__ __forceinline__ void cnt_add_warp(unsigned long long* p, long long v)
     if (g.thread_rank() == 0 && sum != 0) atomicAdd(p, (unsigned long long)sum);
 }
 
-// Programmatic dependent launch (griddepcontrol, sm_90 and later).  pdl_wait
-// returns once every grid this one depends on has completed and its memory
-// operations are visible (at once for a grid launched without the attribute);
-// pdl_trigger lets the dependent grid's blocks be dispatched before this grid ends.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
 // Warp-aggregated append to a device list.
 __device__ __forceinline__ int32_t append(int32_t* count)
 {
@@ -240,9 +233,6 @@ struct cs_gpu_ctx {
     cudaGraph_t day_graph = nullptr;
     cudaGraphExec_t day_exec = nullptr;
     long long day_launches = 0;
-    // programmatic dependent launch of the chained step kernels (off with
-    // CS_B200_NO_PDL=1 in the environment, and while profiling)
-    bool pdl = std::getenv("CS_B200_NO_PDL") == nullptr;
     // optional per-launch timing with events on the context's stream
     bool prof = false;
     struct Rec { const char* name; cudaEvent_t a, b; };
@@ -360,32 +350,6 @@ static int set_err(cs_gpu_ctx* c, int code, const char* fmt, ...)
         c->launches++;                                                                             \
         cudaError_t e_ = cudaGetLastError();                                                       \
         if (e_ != cudaSuccess) return set_err(c, CS_E_CUDA, "launch %s: %s", #kernel, cudaGetErrorString(e_)); \
-    } while (0)
-
-// A launch that may start while the kernel before it in the stream finishes
-// (programmatic dependent launch): its blocks are dispatched during the earlier
-// kernel's last blocks and wait, at their first instruction (pdl_wait), until that
-// kernel has completed and its memory is visible.  Only kernels that begin with
-// pdl_wait are launched this way; in a captured graph the launch becomes a
-// programmatic edge from the kernel node before it.
-#define LAUNCH_PDL(kernel, grid, block, ...)                                                       \
-    do {                                                                                           \
-        if (c->prof || !c->pdl) {                                                                  \
-            LAUNCH(kernel, grid, block, __VA_ARGS__);                                              \
-        } else {                                                                                   \
-            cudaLaunchConfig_t cfg_ = {};                                                          \
-            cfg_.gridDim = dim3((unsigned)(grid));                                                 \
-            cfg_.blockDim = dim3((unsigned)(block));                                               \
-            cfg_.stream = c->stream;                                                               \
-            cudaLaunchAttribute at_[1];                                                            \
-            at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                        \
-            at_[0].val.programmaticStreamSerializationAllowed = 1;                                 \
-            cfg_.attrs = at_;                                                                      \
-            cfg_.numAttrs = 1;                                                                     \
-            cudaError_t e_ = cudaLaunchKernelEx(&cfg_, kernel, __VA_ARGS__);                       \
-            c->launches++;                                                                         \
-            if (e_ != cudaSuccess) return set_err(c, CS_E_CUDA, "launch %s: %s", #kernel, cudaGetErrorString(e_)); \
-        }                                                                                          \
     } while (0)
 
 template <typename T>
@@ -897,7 +861,7 @@ __device__ __forceinline__ void k_build_active_body(const DevPop& d, int mode)
         __syncthreads();   // the shared arrays are refilled for the next cells
     }
 }
-__global__ void k_build_active(DevPop d, int mode) { pdl_wait(); pdl_trigger(); k_build_active_body(d, mode); }
+__global__ void k_build_active(DevPop d, int mode) { k_build_active_body(d, mode); }
 __global__ void k_build_active_multi(const DevPop* __restrict__ pops, int mode) { k_build_active_body(pops[blockIdx.y], mode); }
 
 // =============================================================== InfectSweep
@@ -945,7 +909,7 @@ __device__ __forceinline__ void k_set_step_body(const DevPop& d, double t, unsig
     st.seed = seed;
     *d.step = st;
 }
-__global__ void k_set_step(DevPop d, double t, unsigned long long seed) { pdl_trigger(); k_set_step_body(d, t, seed); }
+__global__ void k_set_step(DevPop d, double t, unsigned long long seed) { k_set_step_body(d, t, seed); }
 __global__ void k_set_step_multi(const DevPop* __restrict__ pops, double t, unsigned long long seed) { k_set_step_body(pops[blockIdx.y], t, seed); }
 
 // Geometric-skip enumeration of the Bernoulli(p) trials over a member list
@@ -1070,7 +1034,7 @@ __device__ __forceinline__ void k_infector_hh_spatial_body(const DevPop& d)
     }
     cnt_add_warp(CSB_CTR(work_hh_members), hh_members);
 }
-__global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d) { pdl_wait(); pdl_trigger(); k_infector_hh_spatial_body(d); }
+__global__ void __launch_bounds__(kThreads) k_infector_hh_spatial(DevPop d) { k_infector_hh_spatial_body(d); }
 __global__ void __launch_bounds__(kThreads) k_infector_hh_spatial_multi(const DevPop* __restrict__ pops) { k_infector_hh_spatial_body(pops[blockIdx.y]); }
 
 // Place passes (src/Sweep.cpp:379-647): one thread per (infector, place) work
@@ -1228,7 +1192,7 @@ __device__ __forceinline__ void k_spatial_body(const DevPop& d)
     }
 }
 template <int kSpatialLanes>
-__global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d) { pdl_wait(); k_spatial_body<kSpatialLanes>(d); }
+__global__ void __launch_bounds__(kThreads, 3) k_spatial(DevPop d) { k_spatial_body<kSpatialLanes>(d); }
 template <int kSpatialLanes>
 __global__ void __launch_bounds__(kThreads, 3) k_spatial_multi(const DevPop* __restrict__ pops) { k_spatial_body<kSpatialLanes>(pops[blockIdx.y]); }
 
@@ -1310,7 +1274,7 @@ __device__ __forceinline__ void k_apply_infections_body(const DevPop& d)
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt_add(CSB_STAGED(work_new_infections), nq);
     stage_flush(d.C, staged);
 }
-__global__ void k_apply_infections(DevPop d) { pdl_trigger(); k_apply_infections_body(d); }
+__global__ void k_apply_infections(DevPop d) { k_apply_infections_body(d); }
 __global__ void k_apply_infections_multi(const DevPop* __restrict__ pops) { k_apply_infections_body(pops[blockIdx.y]); }
 
 // Swap-with-block-end removal of marked slots, high to low (src/Update.cpp:1402-1579
@@ -1372,7 +1336,7 @@ __device__ __forceinline__ void k_partition_S_body(const DevPop& d)
         }
     }
 }
-__global__ void k_partition_S(DevPop d) { pdl_wait(); k_partition_S_body(d); }
+__global__ void k_partition_S(DevPop d) { k_partition_S_body(d); }
 __global__ void k_partition_S_multi(const DevPop* __restrict__ pops) { k_partition_S_body(pops[blockIdx.y]); }
 
 // ====================================================== IncubRecoverySweep
@@ -1693,6 +1657,7 @@ __device__ __noinline__ bool gather_test_from_times(const cs_params* __restrict_
 // its own.
 __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
 {
+    const cs_params& P = *d.P;
     const int ts = d.step->ts;
     const bool init = *d.ev_init != 0;   // next_ev is formed from the people's own times
     __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads], s_L[kThreads];
@@ -1748,7 +1713,7 @@ __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
     }
     if (threadIdx.x == 0 && people) cnt_add(CSB_CTR(work_incub_people), people);
 }
-__global__ void __launch_bounds__(kThreads) k_incub_gather(DevPop d) { pdl_trigger(); k_incub_gather_body(d); }
+__global__ void __launch_bounds__(kThreads) k_incub_gather(DevPop d) { k_incub_gather_body(d); }
 __global__ void __launch_bounds__(kThreads) k_incub_gather_multi(const DevPop* __restrict__ pops) { k_incub_gather_body(pops[blockIdx.y]); }
 
 // DoFalseCase (src/Update.cpp:896-905) for every person with a false-positive
@@ -1845,7 +1810,7 @@ __device__ __forceinline__ void k_incub_events_body(const DevPop& d)
     }
     stage_flush(d.C, staged);
 }
-__global__ void __launch_bounds__(kThreads, 3) k_incub_events(DevPop d) { pdl_wait(); pdl_trigger(); k_incub_events_body(d); }
+__global__ void __launch_bounds__(kThreads, 3) k_incub_events(DevPop d) { k_incub_events_body(d); }
 __global__ void __launch_bounds__(kThreads, 3) k_incub_events_multi(const DevPop* __restrict__ pops) { k_incub_events_body(pops[blockIdx.y]); }
 
 __device__ __forceinline__ void k_partition_LI_body(const DevPop& d)
@@ -1934,7 +1899,6 @@ __global__ void k_household_after_multi(const DevPop* __restrict__ pops) { k_hou
 // quarantine, flags and household lists, so neither waits for the other.
 __global__ void k_incub_finish(DevPop d)
 {
-    pdl_wait();
     k_partition_LI_body(d);
     k_household_after_body(d);
 }
@@ -2917,7 +2881,7 @@ static int apply_queue(cs_gpu_ctx* c)
 {
     DevPop& d = c->d;
     LAUNCH(k_apply_infections, c->grid, kThreads, d);
-    LAUNCH_PDL(k_partition_S, c->grid, kThreads, d);
+    LAUNCH(k_partition_S, c->grid, kThreads, d);
     if (c->hp.FalsePositiveRate > 0) LAUNCH(k_apply_false_cases, c->grid, kThreads, d);
     // every sweep leaves its list counters at zero for the next one; the household
     // list (last) is the incub sweep's
@@ -2983,7 +2947,7 @@ static int build_active(cs_gpu_ctx* c, int mode)
     // the list counters are zero here: every sweep (and begin_run, upload_state,
     // seed_infections) ends by zeroing them
     const int ntiles = (d.NC + kThreads - 1) / kThreads;
-    LAUNCH_PDL(k_build_active, ntiles * std::max(1, c->grid / ntiles), kThreads, d, mode);
+    LAUNCH(k_build_active, ntiles * std::max(1, c->grid / ntiles), kThreads, d, mode);
     return CS_OK;
 }
 
@@ -2996,7 +2960,7 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
     LAUNCH(k_set_step, 1, 1, d, t, (unsigned long long)c->seed);
     int r = build_active(c, 0);
     if (r) return r;
-    LAUNCH_PDL(k_infector_hh_spatial, c->grid, kThreads, d);
+    LAUNCH(k_infector_hh_spatial, c->grid, kThreads, d);
     // The place pass and the spatial pass both read the infector pass's lists and
     // only claim infections (atomicMin on the claim key) and add to counters, so the
     // place pass runs on the side stream beside the spatial pass (a branch of the
@@ -3013,10 +2977,10 @@ int cs_gpu_infect_sweep(cs_gpu_ctx* c, double t, int run)
         LAUNCH(k_infector_places, c->grid, kThreads, d);
     }
     switch (c->spatial_lanes) {
-    case 2: LAUNCH_PDL(k_spatial<2>, c->grid, kThreads, d); break;
-    case 4: LAUNCH_PDL(k_spatial<4>, c->grid, kThreads, d); break;
-    case 16: LAUNCH_PDL(k_spatial<16>, c->grid, kThreads, d); break;
-    default: LAUNCH_PDL(k_spatial<8>, c->grid, kThreads, d); break;
+    case 2: LAUNCH(k_spatial<2>, c->grid, kThreads, d); break;
+    case 4: LAUNCH(k_spatial<4>, c->grid, kThreads, d); break;
+    case 16: LAUNCH(k_spatial<16>, c->grid, kThreads, d); break;
+    default: LAUNCH(k_spatial<8>, c->grid, kThreads, d); break;
     }
     if (fork) CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     return apply_queue(c);
@@ -3032,8 +2996,8 @@ static int incub_sweep(cs_gpu_ctx* c, double t, bool set_step)
         const int ntiles = (d.NC + kThreads - 1) / kThreads;
         LAUNCH(k_incub_gather, ntiles * std::max(1, c->grid / ntiles), kThreads, d);
     }
-    LAUNCH_PDL(k_incub_events, c->grid, kThreads, d);
-    LAUNCH_PDL(k_incub_finish, c->grid, kThreads, d);
+    LAUNCH(k_incub_events, c->grid, kThreads, d);
+    LAUNCH(k_incub_finish, c->grid, kThreads, d);
     CK(cudaMemsetAsync(d.counts, 0, sizeof(int32_t) * kCntN, c->stream));   // all list counters
     return CS_OK;
 }
