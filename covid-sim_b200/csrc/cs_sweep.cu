@@ -1657,7 +1657,6 @@ __device__ __noinline__ bool gather_test_from_times(const cs_params* __restrict_
 // its own.
 __device__ __forceinline__ void k_incub_gather_body(const DevPop& d)
 {
-    const cs_params& P = *d.P;
     const int ts = d.step->ts;
     const bool init = *d.ev_init != 0;   // next_ev is formed from the people's own times
     __shared__ int s_first[kThreads], s_ofs[kThreads], s_n[kThreads], s_L[kThreads];
