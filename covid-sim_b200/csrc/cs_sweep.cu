@@ -942,10 +942,12 @@ __device__ void place_candidates(const DevPop& d, const cs_params& P, const Step
         int m = pl.members[base + (int)pos];
         ncand++;
         PersonHot hm = d.hot[m];
-        double sc = calc_place_susc(d, hm, P, pt, st.ts);
-        if (between && ich && is_ch(hm) && gi != group_of(d, pt, m)) sc *= P.CareHomeResidentPlaceScaling;
-        if ((pt == P.CareHomePlaceType) && ((!ich) || (!is_ch(hm)))) sc *= P.CareHomeWorkerGroupScaling;
         if (hm.inf == CS_INF_SUSCEPTIBLE && !host_absent(hm, st.ts)) {
+            // the susceptibility is formed only for a candidate it can matter to (the
+            // same factors in the same order as for every candidate)
+            double sc = calc_place_susc(d, hm, P, pt, st.ts);
+            if (between && ich && is_ch(hm) && gi != group_of(d, pt, m)) sc *= P.CareHomeResidentPlaceScaling;
+            if ((pt == P.CareHomePlaceType) && ((!ich) || (!is_ch(hm)))) sc *= P.CareHomeWorkerGroupScaling;
             sc *= calc_person_susc(hm, iag, P) * p / p;
             if (st.blanket) {
                 if (dist2_hh_pt(d, P, hm.hh, pl.x[link], pl.y[link]) > P.MoveRestrRadius2) sc *= P.MoveRestrEffect;
@@ -986,10 +988,11 @@ __device__ __forceinline__ void k_infector_hh_spatial_body(const DevPop& d)
                 double HI = st.hh_beta * calc_house_inf(hi, hr.nhr, P, st.ts);
                 bool absent = false;
                 for (int m = f0; anyc && (m < f1) && (!absent); m++) {
-                    bool ma = host_absent(d.hot[m], st.ts);
+                    // a member counts only when absent: its places are read only then
+                    if (!host_absent(d.hot[m], st.ts)) continue;
                     for (int pt = 0; (pt < d.NPT) && (!absent); pt++) {
                         int lk = link_of(d, pt, m);
-                        if (lk >= 0) absent = place_closed(d, pt, lk, st.ts) && ma;
+                        if (lk >= 0) absent = place_closed(d, pt, lk, st.ts);
                     }
                 }
                 if (absent) HI *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_HOUSE];
@@ -1012,8 +1015,8 @@ __device__ __forceinline__ void k_infector_hh_spatial_body(const DevPop& d)
             }
             if (st.sp_beta > 0) {
                 double si = calc_spatial_inf(hi, P, st.ts);
-                bool closed = false;
-                for (int pt = 0; anyc && (pt < d.NPT) && (!closed); pt++)
+                bool closed = false;   // counts only for an absent infector
+                for (int pt = 0; anyc && absent_i && (pt < d.NPT) && (!closed); pt++)
                     if (links[pt] >= 0) closed = place_closed(d, pt, links[pt], st.ts);
                 if (closed && absent_i) { si *= P.Efficacies[CS_NPI_PLACE_CLOSURE][CS_SETTING_SPATIAL]; closed_i = 1; }
                 double lambda = si * st.sp_beta * d.tot_prob[ci];
