@@ -185,6 +185,8 @@ def load_library(path=LIB_PATH):
         "cs_gpu_get_sample16": (I, [V, V, P(cs_counters)]),
         "cs_gpu_sample_packed_bytes": (C.c_size_t, [V]),
         "cs_gpu_get_sample_packed": (I, [V, V, C.c_size_t]),
+        "cs_gpu_sample_packed_begin": (I, [V, V, C.c_size_t]),
+        "cs_gpu_sample_packed_end": (I, [V, V]),
         "cs_host_alloc": (V, [C.c_size_t]),
         "cs_host_free": (None, [V]),
         "cs_gpu_sync": (I, [V]),

@@ -3930,24 +3930,36 @@ size_t cs_gpu_sample_packed_bytes(const cs_gpu_ctx* c)
     return c ? sizeof(cs_counters) + sizeof(uint16_t) * 5 * (size_t)c->d.NC : 0;
 }
 
-int cs_gpu_get_sample_packed(cs_gpu_ctx* c, void* buf, size_t bytes)
+int cs_gpu_sample_packed_begin(cs_gpu_ctx* c, void* buf, size_t bytes)
 {
     if (!c || !buf) return CS_E_ARG;
     DevPop& d = c->d;
     const size_t need = cs_gpu_sample_packed_bytes(c);
-    if (bytes < need) return set_err(c, CS_E_ARG, "get_sample_packed: %zu bytes, %zu needed", bytes, need);
+    if (bytes < need) return set_err(c, CS_E_ARG, "sample_packed: %zu bytes, %zu needed", bytes, need);
     if (c->max_cell_people > 65535)
-        return set_err(c, CS_E_RANGE, "get_sample_packed: a cell holds %d people, more than 16 bits count",
+        return set_err(c, CS_E_RANGE, "sample_packed: a cell holds %d people, more than 16 bits count",
                        c->max_cell_people);
     if (!c->packed) CK(cudaMalloc(&c->packed, need));
     LAUNCH(k_pack_sample, (d.NC + kThreads - 1) / kThreads, kThreads, d, (unsigned char*)c->packed);
     CK(cudaMemcpyAsync(buf, c->packed, need, cudaMemcpyDeviceToHost, c->stream));
+    return CS_OK;
+}
+
+int cs_gpu_sample_packed_end(cs_gpu_ctx* c, const void* buf)
+{
+    if (!c || !buf) return CS_E_ARG;
     CK(cudaStreamSynchronize(c->stream));
     const cs_counters* out = (const cs_counters*)buf;
     if (out->err_queue_overflow || out->err_spatial_tries || out->err_kernel_range)
         return set_err(c, CS_E_OVERFLOW, "bounded device loop gave up (spatial %lld, queue %lld, kernel range %lld)",
                        (long long)out->err_spatial_tries, (long long)out->err_queue_overflow, (long long)out->err_kernel_range);
     return CS_OK;
+}
+
+int cs_gpu_get_sample_packed(cs_gpu_ctx* c, void* buf, size_t bytes)
+{
+    const int r = cs_gpu_sample_packed_begin(c, buf, bytes);
+    return r ? r : cs_gpu_sample_packed_end(c, buf);
 }
 
 int cs_gpu_get_sample16(cs_gpu_ctx* c, uint16_t* cells, cs_counters* out)

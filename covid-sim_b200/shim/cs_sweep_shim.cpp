@@ -117,6 +117,7 @@ int32_t *g_S = nullptr, *g_L = nullptr, *g_I = nullptr, *g_R = nullptr, *g_D = n
 Pinned<unsigned char> g_packed;
 std::vector<uint16_t> g_host16;
 bool g_use16 = false;
+bool g_sample_queued = false;   // the packed copy back of the timestep in flight is queued
 cs_params g_params;
 // what the device holds of the host's intervention state
 std::vector<uint8_t> g_sd, g_mr;              // per microcell: socdist, moverest (TreatStat)
@@ -520,7 +521,9 @@ void sync_back()
     cs_counters k;
     const int NC = P.NumPopulatedCells;
     if (g_use16) {
-        check(cs_gpu_get_sample_packed(g_ctx, g_packed.data(), g_packed.size()), "cs_gpu_get_sample_packed");
+        if (g_sample_queued) check(cs_gpu_sample_packed_end(g_ctx, g_packed.data()), "cs_gpu_sample_packed_end");
+        else check(cs_gpu_get_sample_packed(g_ctx, g_packed.data(), g_packed.size()), "cs_gpu_get_sample_packed");
+        g_sample_queued = false;
         std::memcpy(&k, g_packed.data(), sizeof k);
     } else {
         check(cs_gpu_get_sample(g_ctx, g_S, g_L, g_I, g_R, g_D, &k), "cs_gpu_get_sample");
@@ -855,6 +858,13 @@ void InfectSweep(double t, int run)
     // RunModel calls IncubRecoverySweep(t) right after this call (src/CovidSim.cpp:
     // 1488-1490), so the whole timestep runs here as one replay of its graph
     check(cs_gpu_step(g_ctx, t, run), "cs_gpu_step");
+    // a timestep whose results RecordSample reads: the packed copy back is queued
+    // behind it now, so it follows the timestep on the device without a round trip
+    g_sample_queued = false;
+    if (g_use16 && (P.LimitNumInfections || (g_step_in_run + 1) % P.NumModelTimeStepsPerOutputTimeStep == 0)) {
+        check(cs_gpu_sample_packed_begin(g_ctx, g_packed.data(), g_packed.size()), "cs_gpu_sample_packed_begin");
+        g_sample_queued = true;
+    }
     if (g_timing.empty() || g_timing.back().run != run) {
         g_timing.push_back(RunTiming());
         g_timing.back().run = run;

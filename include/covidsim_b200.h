@@ -635,6 +635,12 @@ int cs_gpu_get_sample16(cs_gpu_ctx* ctx, uint16_t* cells, cs_counters* out);
  * people. */
 size_t cs_gpu_sample_packed_bytes(const cs_gpu_ctx* ctx);
 int cs_gpu_get_sample_packed(cs_gpu_ctx* ctx, void* buf, size_t bytes);
+/* The same in two halves: _begin queues the packing and the copy behind the work
+ * already on the context's stream (a timestep just launched) and returns at once;
+ * _end waits for the stream and checks the counter block's error fields.  buf is
+ * not to be read or reused between the two. */
+int cs_gpu_sample_packed_begin(cs_gpu_ctx* ctx, void* buf, size_t bytes);
+int cs_gpu_sample_packed_end(cs_gpu_ctx* ctx, const void* buf);
 /* Page-locked host memory (NULL on failure) for a host's staging buffers: copies
  * between it and the device run at the link's full rate and never through an
  * intermediate buffer.  Free with cs_host_free. */

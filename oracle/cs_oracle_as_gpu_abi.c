@@ -81,3 +81,5 @@ int cs_gpu_get_sample_packed(cs_gpu_ctx* c, void* buf, size_t bytes)
     k->S = k->L = k->I = k->R = k->D = 0;
     return cs_cpu_get_cells16((cs_cpu_ctx*)c, (uint16_t*)((char*)buf + sizeof(cs_counters)));
 }
+int cs_gpu_sample_packed_begin(cs_gpu_ctx* c, void* buf, size_t bytes) { return cs_gpu_get_sample_packed(c, buf, bytes); }
+int cs_gpu_sample_packed_end(cs_gpu_ctx* c, const void* buf) { (void)c; (void)buf; return CS_OK; }

@@ -1,7 +1,8 @@
 """The three ways a host reads what RecordSample needs agree with each other and with
 the oracle: cs_gpu_get_sample (32-bit cell counts), cs_gpu_get_sample16 (16-bit) and
 cs_gpu_get_sample_packed (the counter block and the 16-bit counts in one buffer,
-S..D of the block left 0), into page-locked memory from cs_host_alloc."""
+S..D of the block left 0, also in two halves queued behind a timestep), into
+page-locked memory from cs_host_alloc."""
 import ctypes as C
 
 import numpy as np
@@ -44,6 +45,18 @@ def test_sample_copies_agree_with_each_other_and_the_oracle():
         assert lib.cs_gpu_get_sample_packed(ctx, buf, nbytes - 1) != 0   # too small a buffer is refused
         assert lib.cs_gpu_get_sample_packed(ctx, buf, nbytes) == 0
         raw = np.ctypeslib.as_array(C.cast(buf, C.POINTER(C.c_uint8)), shape=(nbytes,)).copy()
+        # the two halves, queued behind a timestep: the same bytes as the timestep's
+        # own copy afterwards
+        C.memset(buf, 0, nbytes)
+        t = 60 * P.ModelTimeStep
+        be.infect_sweep(t, 0)
+        be.incub_recovery_sweep(t)
+        assert lib.cs_gpu_sample_packed_begin(ctx, buf, nbytes) == 0
+        assert lib.cs_gpu_sample_packed_end(ctx, buf) == 0
+        queued = np.ctypeslib.as_array(C.cast(buf, C.POINTER(C.c_uint8)), shape=(nbytes,)).copy()
+        assert lib.cs_gpu_get_sample_packed(ctx, buf, nbytes) == 0
+        after = np.ctypeslib.as_array(C.cast(buf, C.POINTER(C.c_uint8)), shape=(nbytes,)).copy()
+        assert np.array_equal(queued, after)
     finally:
         lib.cs_host_free(buf)
     kp = abi.cs_counters.from_buffer_copy(raw[:C.sizeof(abi.cs_counters)].tobytes())
