@@ -455,10 +455,12 @@ def e2e_dropin(args, local, world, dist, n_cells):
     """e2e through the drop-in: warm-up 1 and `steps` timed realisations of the
     reference executable with the GPU sweep linked in, loading the workload's
     network file; value = people x timesteps / wall time of the sweep calls (state
-    upload at each realisation's start, the device sweeps and the wait for them at
-    every timestep, the copy of the cell counts and counters back to the
-    reference's host structures at every output step, the hand-over of the host's
-    interventions)."""
+    upload at each realisation's start, the launch of every timestep's graph, the
+    wait for the device at the last timestep of each output step -- the timesteps
+    before it run on while the host runs TreatSweep --, the copy of the cell counts
+    and counters back to the reference's host structures there, the hand-over of the
+    host's interventions).  run_loop_ms_per_step is RunModel's whole loop per
+    realisation, the host code between sweeps included."""
     import ctypes
     import refrun
     from covidsim_b200 import abi, sim
