@@ -143,6 +143,7 @@ def load_library(path=LIB_PATH):
         "cs_gpu_set_params": (I, [V, P(cs_params)]),
         "cs_gpu_begin_run": (I, [V, C.c_uint64, V, I, I]),
         "cs_gpu_upload_state": (I, [V, C.c_uint64, P(cs_state_view)]),
+        "cs_gpu_upload_people": (I, [V, P(cs_state_view), C.c_int64, C.c_int64]),
         "cs_gpu_download_state": (I, [V, P(cs_state_view)]),
         "cs_gpu_seed_infections": (I, [V, D, V, I]),
         "cs_gpu_infect_sweep": (I, [V, D, I]),

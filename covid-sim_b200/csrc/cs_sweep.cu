@@ -228,6 +228,7 @@ struct cs_gpu_ctx {
     // staging of cs_gpu_place_events / cs_gpu_set_mcell_status
     cs_place_event* d_ev = nullptr;
     int ev_cap = 0;
+    size_t people_sent = 0;   // people whose arrays cs_gpu_upload_people has queued
     void* d_mc = nullptr;
     size_t mc_cap = 0;
     cudaGraph_t day_graph = nullptr;
@@ -4098,6 +4099,51 @@ int cs_gpu_download_state(cs_gpu_ctx* c, const cs_state_view* v)
     return rc;
 }
 
+// The per-person arrays of a state upload for people [first, first + n), queued on
+// the context's stream from the view's host arrays: the record fields into the
+// staging slices (k_pack_hot packs them later), the rest into place.
+static int upload_people_slice(cs_gpu_ctx* c, const cs_state_view* v, const XferSlices& x, size_t first, size_t n)
+{
+    DevPop& d = c->d;
+    if (n == 0) return CS_OK;
+#define SL(dst, src, w)                                                                                       \
+    CK(cudaMemcpyAsync((char*)(dst) + (size_t)(w) * first, (const char*)v->src + (size_t)(w) * first,        \
+                       (size_t)(w) * n, cudaMemcpyHostToDevice, c->stream))
+    SL(x.inf, inf, 1); SL(x.sev, severity, 1); SL(x.fl, flags, 1); SL(x.lt, latent_time, 2);
+    SL(x.as, absent_start_time, 2); SL(x.ae, absent_stop_time, 2); SL(x.iso, isolation_start_time, 2);
+    SL(x.qs, quar_start_time, 2); SL(x.infn, infectiousness, 4); SL(x.susc, susc, 4);
+    SL(d.infection_time, infection_time, 2); SL(d.recovery_time, recovery_or_death_time, 2);
+    SL(d.sari_time, SARI_time, 2); SL(d.critical_time, Critical_time, 2); SL(d.stepdown_time, Stepdown_time, 2);
+    SL(d.detected_time, detected_time, 2); SL(d.prob_absent, ProbAbsent, 4); SL(d.prob_care, ProbCare, 4);
+    SL(d.infector, infector, 4); SL(d.infect_type, infect_type, 2); SL(d.listpos, listpos, 4);
+#undef SL
+    return CS_OK;
+}
+
+static bool people_fields(const cs_state_view* v)
+{
+    return v->inf && v->severity && v->flags && v->latent_time && v->absent_start_time && v->absent_stop_time &&
+           v->isolation_start_time && v->quar_start_time && v->infectiousness && v->susc && v->infection_time &&
+           v->recovery_or_death_time && v->SARI_time && v->Critical_time && v->Stepdown_time && v->detected_time &&
+           v->ProbAbsent && v->ProbCare && v->infector && v->infect_type && v->listpos;
+}
+
+int cs_gpu_upload_people(cs_gpu_ctx* c, const cs_state_view* v, int64_t first, int64_t n)
+{
+    if (!c || !v) return CS_E_ARG;
+    if (!people_fields(v)) return set_err(c, CS_E_ARG, "upload_people needs every per-person field of the view");
+    if (first != (int64_t)c->people_sent || n < 0 || first + n > (int64_t)c->d.N)
+        return set_err(c, CS_E_ARG, "upload_people: people [%lld, %lld) do not follow the %zu sent (of %d)",
+                       (long long)first, (long long)(first + n), c->people_sent, c->d.N);
+    XferSlices x;
+    int r = xfer_slices(c, &x);
+    if (r) return r;
+    r = upload_people_slice(c, v, x, (size_t)first, (size_t)n);
+    if (r) return r;
+    c->people_sent += (size_t)n;
+    return CS_OK;
+}
+
 int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
 {
     if (!c || !v) return CS_E_ARG;
@@ -4112,21 +4158,19 @@ int cs_gpu_upload_state(cs_gpu_ctx* c, uint64_t seed, const cs_state_view* v)
     XferSlices x;
     int r0 = xfer_slices(c, &x);
     if (r0) return r0;
-#define STG(dst, src, bytes) CK(cudaMemcpyAsync(dst, v->src, bytes, cudaMemcpyHostToDevice, c->stream))
-    STG(x.inf, inf, N); STG(x.sev, severity, N); STG(x.fl, flags, N); STG(x.lt, latent_time, 2 * N);
-    STG(x.as, absent_start_time, 2 * N); STG(x.ae, absent_stop_time, 2 * N); STG(x.iso, isolation_start_time, 2 * N);
-    STG(x.qs, quar_start_time, 2 * N); STG(x.infn, infectiousness, 4 * N); STG(x.susc, susc, 4 * N);
-#undef STG
+    {   // the people cs_gpu_upload_people has not sent yet
+        const size_t sent = c->people_sent;
+        c->people_sent = 0;
+        if (sent > N) return set_err(c, CS_E_STATE, "upload_state: %zu people sent ahead, %zu in the population", sent, N);
+        r0 = upload_people_slice(c, v, x, sent, N - sent);
+        if (r0) return r0;
+    }
     int8_t* dinf = x.inf; uint8_t* dsev = x.sev; uint8_t* dfl = x.fl;
     uint16_t *dlt = x.lt, *das = x.as, *dae = x.ae, *diso = x.iso, *dqs = x.qs;
     float *dinfn = x.infn, *dsusc = x.susc;
     k_pack_hot<<<c->grid, kThreads, 0, c->stream>>>(d, dinf, dsev, dfl, dlt, das, dae, diso, dqs, dinfn, dsusc);
     c->launches++;
 #define UL(src, dst, bytes) CK(cudaMemcpyAsync(dst, v->src, bytes, cudaMemcpyHostToDevice, c->stream))
-    UL(infection_time, d.infection_time, 2 * N); UL(recovery_or_death_time, d.recovery_time, 2 * N);
-    UL(SARI_time, d.sari_time, 2 * N); UL(Critical_time, d.critical_time, 2 * N); UL(Stepdown_time, d.stepdown_time, 2 * N);
-    UL(detected_time, d.detected_time, 2 * N); UL(ProbAbsent, d.prob_absent, 4 * N); UL(ProbCare, d.prob_care, 4 * N);
-    UL(infector, d.infector, 4 * N); UL(infect_type, d.infect_type, 2 * N); UL(listpos, d.listpos, 4 * N);
     UL(cell_S, d.S, 4 * NC); UL(cell_L, d.L, 4 * NC); UL(cell_I, d.I, 4 * NC); UL(cell_R, d.R, 4 * NC);
     UL(cell_D, d.D, 4 * NC); UL(cell_S0, d.S0, 4 * NC); UL(cell_tot_prob, d.tot_prob, 8 * NC); UL(cell_slots, d.slots, 4 * N);
 #undef UL

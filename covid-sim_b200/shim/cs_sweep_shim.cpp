@@ -443,19 +443,39 @@ void upload_run_state(int run)
         g.cell_ofs.assign(NC + 1, 0);
         for (int c = 0; c < NC; c++) g.cell_ofs[c + 1] = g.cell_ofs[c] + CellLookup[c]->n;
     }
+    cs_state_view v;
+    std::memset(&v, 0, sizeof(v));
+    v.inf = g.inf.data(); v.severity = g.sev.data(); v.flags = g.fl.data(); v.infection_time = g.it.data();
+    v.latent_time = g.lt.data(); v.recovery_or_death_time = g.rt.data(); v.SARI_time = g.st.data();
+    v.Critical_time = g.ct.data(); v.Stepdown_time = g.sd.data(); v.absent_start_time = g.as.data();
+    v.absent_stop_time = g.ae.data(); v.isolation_start_time = g.iso.data(); v.quar_start_time = g.qs.data();
+    v.detected_time = g.dt.data(); v.infectiousness = g.infn.data(); v.susc = g.susc.data(); v.ProbAbsent = g.pa.data();
+    v.ProbCare = g.pc.data(); v.infector = g.infector.data(); v.infect_type = g.itype.data(); v.listpos = g.listpos.data();
+    v.cell_S = g.cS.data(); v.cell_L = g.cL.data(); v.cell_I = g.cI.data(); v.cell_R = g.cR.data(); v.cell_D = g.cD.data();
+    v.cell_S0 = g.S0.data(); v.cell_tot_prob = g.tp.data(); v.cell_slots = g.slots.data();
+    // the people in slices: each is sent (cs_gpu_upload_people) as soon as it is
+    // filled, so its copy to the device runs while the next slice is filled
+    double t_sent = 0.0;
+    const int kSlices = 8;
+    for (int q = 0; q < kSlices; q++) {
+        const int lo = (int)((long long)N * q / kSlices), hi = (int)((long long)N * (q + 1) / kSlices);
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < N; i++) {
-        const Person& a = Hosts[i];
-        g.inf[i] = inf_of(a);
-        g.sev[i] = (uint8_t)((int)a.Severity_Current | ((int)a.Severity_Final << 4));
-        g.fl[i] = (uint8_t)((a.to_die ? CS_DF_TO_DIE : 0) | (a.detected ? CS_DF_DETECTED : 0) |
-                            ((HostsQuarantine[i].comply & 3) << CS_DF_QUAR_COMPLY_SHIFT));
-        g.it[i] = a.infection_time; g.lt[i] = a.latent_time; g.rt[i] = a.recovery_or_death_time;
-        g.st[i] = a.SARI_time; g.ct[i] = a.Critical_time; g.sd[i] = a.Stepdown_time;
-        g.as[i] = a.absent_start_time; g.ae[i] = a.absent_stop_time; g.iso[i] = a.isolation_start_time;
-        g.qs[i] = HostsQuarantine[i].start_time; g.dt[i] = a.detected_time;
-        g.infn[i] = a.infectiousness; g.susc[i] = a.susc; g.pa[i] = a.ProbAbsent; g.pc[i] = a.ProbCare;
-        g.infector[i] = a.infector; g.itype[i] = a.infect_type; g.listpos[i] = a.listpos;
+        for (int i = lo; i < hi; i++) {
+            const Person& a = Hosts[i];
+            g.inf[i] = inf_of(a);
+            g.sev[i] = (uint8_t)((int)a.Severity_Current | ((int)a.Severity_Final << 4));
+            g.fl[i] = (uint8_t)((a.to_die ? CS_DF_TO_DIE : 0) | (a.detected ? CS_DF_DETECTED : 0) |
+                                ((HostsQuarantine[i].comply & 3) << CS_DF_QUAR_COMPLY_SHIFT));
+            g.it[i] = a.infection_time; g.lt[i] = a.latent_time; g.rt[i] = a.recovery_or_death_time;
+            g.st[i] = a.SARI_time; g.ct[i] = a.Critical_time; g.sd[i] = a.Stepdown_time;
+            g.as[i] = a.absent_start_time; g.ae[i] = a.absent_stop_time; g.iso[i] = a.isolation_start_time;
+            g.qs[i] = HostsQuarantine[i].start_time; g.dt[i] = a.detected_time;
+            g.infn[i] = a.infectiousness; g.susc[i] = a.susc; g.pa[i] = a.ProbAbsent; g.pc[i] = a.ProbCare;
+            g.infector[i] = a.infector; g.itype[i] = a.infect_type; g.listpos[i] = a.listpos;
+        }
+        const double t0 = omp_get_wtime();
+        check(cs_gpu_upload_people(g_ctx, &v, lo, hi - lo), "cs_gpu_upload_people");
+        t_sent += omp_get_wtime() - t0;
     }
 #pragma omp parallel for schedule(dynamic, 64)
     for (int c = 0; c < NC; c++) {
@@ -469,20 +489,10 @@ void upload_run_state(int run)
             h[3 * NC + c] = (uint16_t)x->R; h[4 * NC + c] = (uint16_t)x->D;
         }
     }
-    cs_state_view v;
-    std::memset(&v, 0, sizeof(v));
-    v.inf = g.inf.data(); v.severity = g.sev.data(); v.flags = g.fl.data(); v.infection_time = g.it.data();
-    v.latent_time = g.lt.data(); v.recovery_or_death_time = g.rt.data(); v.SARI_time = g.st.data();
-    v.Critical_time = g.ct.data(); v.Stepdown_time = g.sd.data(); v.absent_start_time = g.as.data();
-    v.absent_stop_time = g.ae.data(); v.isolation_start_time = g.iso.data(); v.quar_start_time = g.qs.data();
-    v.detected_time = g.dt.data(); v.infectiousness = g.infn.data(); v.susc = g.susc.data(); v.ProbAbsent = g.pa.data();
-    v.ProbCare = g.pc.data(); v.infector = g.infector.data(); v.infect_type = g.itype.data(); v.listpos = g.listpos.data();
-    v.cell_S = g.cS.data(); v.cell_L = g.cL.data(); v.cell_I = g.cI.data(); v.cell_R = g.cR.data(); v.cell_D = g.cD.data();
-    v.cell_S0 = g.S0.data(); v.cell_tot_prob = g.tp.data(); v.cell_slots = g.slots.data();
     uint64_t seed = ((uint64_t)(uint32_t)P.runSeed1 << 32) ^ (uint32_t)P.runSeed2 ^ (0x9E3779B97F4A7C15ull * (uint64_t)(run + 1));
     const double t_up = omp_get_wtime();
     check(cs_gpu_upload_state(g_ctx, seed, &v), "cs_gpu_upload_state");
-    g_upload_device = omp_get_wtime() - t_up;
+    g_upload_device = omp_get_wtime() - t_up + t_sent;
     // seeding ran DoInfect on the host (thread 0's counters); the device counts from zero
     for (int j = 1; j < P.NumThreads; j++)
         if (StateT[j].cumI || StateT[j].cumC) ERR_CRITICAL("GPU sweep: host counters outside thread 0 at run start\n");

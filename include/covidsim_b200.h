@@ -421,6 +421,14 @@ int cs_gpu_begin_run(cs_gpu_ctx* ctx, uint64_t seed, const int32_t* seed_people,
  * outside the view (place closures and closure thresholds, social-distancing and
  * movement flags, intervention windows) is reset as cs_gpu_begin_run resets it. */
 int cs_gpu_upload_state(cs_gpu_ctx* ctx, uint64_t seed, const cs_state_view* state);
+/* The per-person arrays of the next cs_gpu_upload_state, sent ahead in slices that
+ * follow one another from person 0: people [first, first + n) of every per-person
+ * array of `state` are queued for copying and the call returns at once, so a host
+ * can fill the next slice while this one crosses (page-locked arrays, from
+ * cs_host_alloc, copy without a staging pass).  The slices' memory must stay as it
+ * is until that cs_gpu_upload_state returns; it sends the people not sent yet.
+ * A slice out of order is CS_E_ARG. */
+int cs_gpu_upload_people(cs_gpu_ctx* ctx, const cs_state_view* state, int64_t first, int64_t n);
 int cs_gpu_download_state(cs_gpu_ctx* ctx, const cs_state_view* state);
 
 /* Infect people chosen by the host at time t (importation, SeedInfection). */

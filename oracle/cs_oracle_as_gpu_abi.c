@@ -83,3 +83,9 @@ int cs_gpu_get_sample_packed(cs_gpu_ctx* c, void* buf, size_t bytes)
 }
 int cs_gpu_sample_packed_begin(cs_gpu_ctx* c, void* buf, size_t bytes) { return cs_gpu_get_sample_packed(c, buf, bytes); }
 int cs_gpu_sample_packed_end(cs_gpu_ctx* c, const void* buf) { (void)c; (void)buf; return CS_OK; }
+/* The oracle reads the whole view in cs_gpu_upload_state: slices sent ahead need no work. */
+int cs_gpu_upload_people(cs_gpu_ctx* c, const cs_state_view* v, int64_t first, int64_t n)
+{
+    (void)c; (void)v; (void)first; (void)n;
+    return CS_OK;
+}

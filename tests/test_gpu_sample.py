@@ -76,3 +76,39 @@ def test_sample_copies_agree_with_each_other_and_the_oracle():
         assert np.array_equal(cells32[j * nc:(j + 1) * nc], snap[key]), key
     assert a["cumI"] == abi.counters_to_dict(o.backend.counters())["cumI"]
     assert a["cumI"] > 100
+
+
+def test_state_uploaded_in_slices_equals_whole_upload():
+    """cs_gpu_upload_people: the per-person arrays sent ahead in three slices, then
+    cs_gpu_upload_state, give the context the same state as one whole upload, and the
+    run goes on identically; a slice that does not follow the last one is refused."""
+    from covidsim_b200 import sim as simmod
+    pop, P, lk, hr = tiny_world()
+    g = sim.Simulation(pop, P, lk, hr)
+    seeds = g.choose_seeds(9, 20)
+    g.backend.begin_run(9, seeds)
+    for k in range(40):
+        t = k * P.ModelTimeStep
+        g.backend.infect_sweep(t, 0)
+        g.backend.incub_recovery_sweep(t)
+    arrs, view = simmod.state_arrays(pop.n_people, pop.n_cells)
+    g.backend.download(view)
+    results = []
+    lib, ctx = g.backend.lib, g.backend.ctx
+    for sliced in (False, True):
+        if sliced:
+            n = pop.n_people
+            cuts = [0, n // 3, (2 * n) // 3, n]
+            assert lib.cs_gpu_upload_people(ctx, C.byref(view), 5, 10) != 0   # not from person 0
+            for a, b in zip(cuts[:-1], cuts[1:]):
+                assert lib.cs_gpu_upload_people(ctx, C.byref(view), a, b - a) == 0
+        g.backend.upload(77, view)
+        for k in range(40, 60):
+            t = k * P.ModelTimeStep
+            g.backend.infect_sweep(t, 0)
+            g.backend.incub_recovery_sweep(t)
+        results.append((snapshot(g.backend, pop), abi.counters_to_dict(g.backend.counters())))
+    (a, ca), (b, cb) = results
+    for key in a:
+        assert np.array_equal(a[key], b[key]), key
+    assert ca == cb
