@@ -1,4 +1,4 @@
-// TEST AND BASELINE INFRASTRUCTURE: the reference's own set-up with a fast place
+// TEST AND CPU-BASELINE INFRASTRUCTURE: the reference's own set-up with a fast place
 // assignment, used once per population to write a network file (/S) that the
 // reference executable and the drop-in then load with /L.
 //
