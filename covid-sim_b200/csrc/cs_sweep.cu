@@ -3019,9 +3019,10 @@ static int step_eager(cs_gpu_ctx* c, double t, int run)
     return incub_sweep(c, t, false);
 }
 
-// Capture one whole timestep (both sweeps, ~25 kernels and memsets) as a CUDA graph.
-// Every kernel reads the step's scalars from device memory written by k_set_step,
-// so a replay only needs the two k_set_step nodes' arguments changed.
+// Capture one whole timestep (both sweeps: ten kernels and two memsets, one more
+// kernel with false positives on) as a CUDA graph.  Every kernel reads the step's
+// scalars from device memory written by k_set_step, so a replay only needs the
+// k_set_step node's arguments changed.
 static int capture_step(cs_gpu_ctx* c, double t, int run)
 {
     cudaGraph_t g = nullptr;
