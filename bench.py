@@ -165,8 +165,9 @@ def peaks():
 
 def kernel_bytes(name, w, n_cells_steps):
     """Algorithmic bytes a kernel moved over the timed region, from the work counters
-    (per-unit costs: transition gather 6 B per latent/infectious person -- its list
-    entry and its next transition time -- and 16 B per cell, infector record 40 B, household member 12 B, place candidate 20 B, spatial
+    (per-unit costs, the shared counting convention: transition scan 16 B per
+    latent/infectious person -- the kernel itself reads 6 B of it, the list entry and
+    the next-event time -- and 16 B per cell, infector record 40 B, household member 12 B, place candidate 20 B, spatial
     draw 33 B, accepted infection 24 B, infector-list entry 12 B, per-cell counts
     16 B)."""
     if name == "k_infector_hh_spatial":
@@ -178,7 +179,7 @@ def kernel_bytes(name, w, n_cells_steps):
     if name in ("k_apply_infections", "k_partition_S"):
         return 12 * w["work_new_infections"]
     if name == "k_incub_gather":
-        return 6 * w["work_incub_people"] + 16 * n_cells_steps
+        return 16 * w["work_incub_people"] + 16 * n_cells_steps
     if name == "k_incub_events":
         return 32 * w["work_transitions"]
     if name == "k_incub_finish":
