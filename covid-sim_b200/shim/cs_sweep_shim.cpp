@@ -733,14 +733,15 @@ void mirror_treat_sweep(double t, int gt)
     const bool mr = t >= P.MoveRestrTimeStart;
     if (sd || mr) {
         // the scan over every populated microcell runs on the host's OpenMP threads;
-        // the changed ones are then listed in microcell order
-        // Each thread scans one contiguous share of the populated microcells, counts
-        // its changes, and after a prefix over the threads writes them to its own
-        // range of the change list, so the list stays in microcell order.
+        // the changed ones are then listed in microcell order.  Each thread scans one
+        // contiguous share of the populated microcells and keeps its changes in its
+        // own list; after a prefix over the threads the lists are copied into the
+        // change list, so it stays in microcell order and each microcell is read once.
         const int npm = P.NumPopulatedMicrocells;
         static std::vector<int32_t> ms;
         static std::vector<uint8_t> vs, vm;
         static std::vector<long long> thread_n;
+        static std::vector<std::vector<int32_t>> local;
         ms.resize(npm); vs.resize(npm); vm.resize(npm);
         long long untreated = 0, treated = 0, nchg = 0;
         unsigned int min_end = 0xFFFFFFFFu;
@@ -748,9 +749,13 @@ void mirror_treat_sweep(double t, int gt)
         {
             const int T = omp_get_num_threads(), k = omp_get_thread_num();
 #pragma omp single
-            thread_n.assign((size_t)T + 1, 0);
+            {
+                thread_n.assign((size_t)T + 1, 0);
+                local.resize((size_t)T);
+            }
+            std::vector<int32_t>& mine = local[k];
+            mine.clear();
             const int i0 = (int)((long long)npm * k / T), i1 = (int)((long long)npm * (k + 1) / T);
-            long long mine = 0;
             for (int i = i0; i < i1; i++) {
                 const int m = (int)(McellLookup[i] - Mcells);
                 const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
@@ -759,20 +764,21 @@ void mirror_treat_sweep(double t, int gt)
                     treated++;
                     if (Mcells[m].socdist_end_time < min_end) min_end = Mcells[m].socdist_end_time;
                 }
-                mine += (a != g_sd[m] || b != g_mr[m]);
+                if (a != g_sd[m] || b != g_mr[m]) {
+                    g_sd[m] = a;
+                    g_mr[m] = b;
+                    mine.push_back(m);
+                }
             }
-            thread_n[k + 1] = mine;
+            thread_n[k + 1] = (long long)mine.size();
 #pragma omp barrier
 #pragma omp single
             for (int j = 0; j < T; j++) thread_n[j + 1] += thread_n[j];
             long long o = thread_n[k];
-            for (int i = i0; i < i1 && o < thread_n[k + 1]; i++) {
-                const int m = (int)(McellLookup[i] - Mcells);
-                const uint8_t a = (uint8_t)Mcells[m].socdist, b = (uint8_t)Mcells[m].moverest;
-                if (a == g_sd[m] && b == g_mr[m]) continue;
+            for (const int32_t m : mine) {
                 ms[o] = m;
-                vs[o] = g_sd[m] = a;
-                vm[o] = g_mr[m] = b;
+                vs[o] = g_sd[m];
+                vm[o] = g_mr[m];
                 o++;
             }
 #pragma omp single
