@@ -453,8 +453,11 @@ def run_ours(args):
     }
 
 
+E2E_MAX_STEPS = 3   # realisations the drop-in's end-to-end figure times at most
+
+
 def e2e_dropin(args, local, world, dist, n_cells):
-    """e2e through the drop-in: warm-up 1 and `steps` timed realisations of the
+    """e2e through the drop-in: warm-up 1 and up to three timed realisations of the
     reference executable with the GPU sweep linked in, loading the workload's
     network file; value = people x timesteps / wall time of the sweep calls (state
     upload at each realisation's start, the launch of every timestep's graph, the
@@ -468,7 +471,12 @@ def e2e_dropin(args, local, world, dist, n_cells):
     from covidsim_b200 import abi, sim
     # the host's thread count, as the reference arm: the reference's set-up, and so the
     # population the network file fits, depends on it
-    res = refrun.time_dropin(args.workload, steps=args.steps, warmup=1, device=local, threads=os.cpu_count())
+    # a realisation through the drop-in runs the reference's RunModel loop, about
+    # 30 s of host code (TreatSweep's microcell loop) around 0.2 s of sweeps: at most
+    # E2E_MAX_STEPS realisations are timed (one per rank when several ranks share the
+    # host's cores), after one warm-up, so the run stays within a few minutes
+    steps = max(1, min(args.steps, E2E_MAX_STEPS if world == 1 else 1))
+    res = refrun.time_dropin(args.workload, steps=steps, warmup=1, device=local, threads=os.cpu_count())
     if "unavailable" in res:
         return {"unavailable": res["unavailable"]}
     rows = res["rows"]
